@@ -1,0 +1,167 @@
+/*
+ * spider_b200.h -- C ABI of the B200 (sm_100a) implementation of SPIDER's
+ * Fourier gridding back-projection (BP 3F, BP 32F, BP 3F P, BP 3F M), its
+ * trilinear projector (PJ 3Q) and conjugate-gradient reconstruction (BP CG).
+ *
+ * These entry points are what SPIDER's operation subroutines would bind
+ * through ISO_C_BINDING in place of their compute loops; each comment names
+ * the reference subroutine (file:line, paths inside the SPIDER source tree)
+ * whose computation it replaces.  The Fortran side keeps its prompts, file
+ * I/O and RESULTS output; it passes arrays and receives arrays.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = success, otherwise an
+ *    IRTFLG-style code (46 = allocation failure, 101 = invalid argument,
+ *    102 = missing data / radius too large, 200+ = CUDA or cuFFT error);
+ *    spi_last_error() returns the message of the last failure on the
+ *    calling host thread.
+ *  - Arrays are Fortran column-major, i.e. C row-major with the dimensions
+ *    reversed: an image is float[nx*nx] with x fastest, a volume
+ *    float[nz*ny*nx] with x fastest.
+ *  - Angles are triples (psi, theta, phi) in degrees per image: registers
+ *    1-3 of SPIDER's angle document, the order BUILDM1 reads them
+ *    (bp3f.f:1287).  Symmetries use the same triple order (builds.f:52).
+ *  - `half` masks hold one byte per image: nonzero routes the image to the
+ *    first sample volume (BP 32F RANDLIST .TRUE., bp32f.f:802-913).
+ *  - Buffers are caller-owned.  `on_device` flags say whether a pointer is a
+ *    device (cudaMalloc'd, same device as the context) or host pointer.
+ *  - A context is bound to one device and one CUDA stream and must be used
+ *    from one host thread at a time.  Calls are synchronous unless the name
+ *    ends in _async.  `stream` arguments are cudaStream_t values (NULL = the
+ *    context's own stream).
+ */
+#ifndef SPIDER_B200_H
+#define SPIDER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spi_ctx spi_ctx;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int spi_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* spi_last_error(void);
+
+/* Create / destroy a context on CUDA device `device`. */
+int spi_ctx_create(int device, spi_ctx** out);
+int spi_ctx_destroy(spi_ctx* ctx);
+
+/* Number of kernels this library has launched through `ctx` so far. */
+long long spi_ctx_launch_count(const spi_ctx* ctx);
+
+/* Device memory the context currently holds, in bytes. */
+long long spi_ctx_device_bytes(const spi_ctx* ctx);
+
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void* spi_ctx_stream(const spi_ctx* ctx);
+
+/* Per-phase device timing (CUDA events on the context stream).  When on,
+ * every phase of the back-projection is bracketed by events and its device
+ * milliseconds accumulated; spi_ctx_timing copies SPI_NPHASE totals and
+ * resets them.  Phases: 0 stage (PADD2), 1 2D FFT, 2 insert (ONELINE),
+ * 3 SYMPLANE0, 4 NRMW2, 5 3D FFT, 6 WINDKB2A, 7 host-to-device copies. */
+#define SPI_NPHASE 8
+int spi_ctx_set_timing(spi_ctx* ctx, int on);
+int spi_ctx_timing(spi_ctx* ctx, double* ms_out, long long* count_out);
+
+/* ------------------------------------------------------------------ *
+ * Fourier gridding back-projection, streaming form.
+ * Replaces BP3FQ's per-image loop (bp3f.f:298-515) and BP32FQ's
+ * (bp32f.f:433-939): PADD2 + FMRS_2 + phase + ONELINE per image, then
+ * SYMPLANE0 + NRMW2 + FMRS_3 + WINDKB2A per volume.
+ * ------------------------------------------------------------------ */
+
+/* Allocate and zero `ngrids` (1 = BP 3F, 2 = BP 32F) Fourier grids for box
+ * size nx (even, 8 <= nx <= 512) and set the symmetry list (sym_angles may
+ * be NULL when nsym <= 1).  Replaces the grid setup of BP3F (bp3f.f:160-178,
+ * 386-394) and BP32F (bp32f.f:163-179, 490-500). */
+int spi_bp_open(spi_ctx* ctx, int nx, int ngrids, const float* sym_angles, int nsym);
+
+/* Spectrum storage for subsequent inserts: 0 = FP32 (default), 1 = BF16. */
+int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
+
+/* Insert `nimg` images (float[nimg*nx*nx]) with their angles
+ * (float[nimg*3], host) and optional half mask (uint8[nimg], host; NULL
+ * routes every image to grid 0).  Replaces the body of the BP3FQ image loop
+ * (bp3f.f:403-493) and of BP32FQ's (bp32f.f:809-913).  Images may be host or
+ * device memory (`imgs_on_device`). */
+int spi_bp_insert(spi_ctx* ctx, const float* imgs, int nimg, const float* angles,
+                  const uint8_t* half, int imgs_on_device);
+
+/* Finish the open grids: SYMPLANE0 (bp32f.f:1051-1088), NRMW2
+ * (bp3f.f:1347-1371), inverse FFT (fmrs_3.f:54-59) and WINDKB2A
+ * (bp32f.f:945-1045).  With one grid, vol_all receives the BP 3F volume.
+ * With two, vol_all receives XE+XO (ADDADA, bp32f.f:345-351), vol_1 the
+ * first and vol_2 the second sample volume; any of them may be NULL.
+ * Volumes are float[nx*nx*nx]. */
+int spi_bp_finish(spi_ctx* ctx, float* vol_all, float* vol_1, float* vol_2, int out_on_device);
+
+/* Copy grid `g` after SYMPLANE0 in BP 3F P's file layout: x_out =
+ * float[2nx*2nx*2(nx+1)] (interleaved complex X(0:NX,2NX,2NX)), w_out =
+ * float[2nx*2nx*(nx+1)] (W).  Replaces BP3F's HALT branch
+ * (bp3f.f:191-248).  Host pointers. */
+int spi_bp_partial_out(spi_ctx* ctx, int g, float* x_out, float* w_out);
+
+/* Add a partial X,W pair (layout as spi_bp_partial_out) into grid `g`.
+ * With spi_bp_finish this is BP 3F M (BP3F_MERGE, bp3f.f:531-739).
+ * Partials are already plane-0 symmetrised, so finishing after merges
+ * skips SYMPLANE0 for inputs added this way. */
+int spi_bp_partial_add(spi_ctx* ctx, int g, const float* x_in, const float* w_in);
+
+/* Release the grids and chunk buffers of the open reconstruction. */
+int spi_bp_close(spi_ctx* ctx);
+
+/* One-shot BP 3F on host arrays (BP3F(.FALSE.,.FALSE.), bp3f.f:79). */
+int spi_bp3f(spi_ctx* ctx, const float* imgs, int nx, int nang, const float* angles,
+             const float* sym_angles, int nsym, float* vol_out);
+
+/* One-shot BP 32F on host arrays (BP32F(.FALSE.), bp32f.f:57). */
+int spi_bp32f(spi_ctx* ctx, const float* imgs, int nx, int nang, const float* angles,
+              const float* sym_angles, int nsym, const uint8_t* half,
+              float* vol_all, float* vol_1, float* vol_2);
+
+/* ------------------------------------------------------------------ *
+ * PJ 3Q: trilinear projection of a volume (PJ3Q_N, pj3q_n.f:41 ->
+ * WRITPRO_N, writpro_n.f:60 -> WPRO_N, wpro_n.f:44-150).
+ * vol = float[nz*ny*nx]; proj_out = float[nang*ny*nx]; ri = object radius
+ * (the reference's default is min(nx,ny,nz)/2 - 2, pj3q_n.f:82).
+ * ------------------------------------------------------------------ */
+int spi_pj3q(spi_ctx* ctx, const float* vol, int nx, int ny, int nz, float ri,
+             const float* angles, int nang, float* proj_out, int on_device);
+
+/* Exact adjoint of spi_pj3q: scatters projections back into a volume with
+ * the transposed trilinear weights (vol_out is overwritten). */
+int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, float ri,
+                     const float* angles, int nang, float* vol_out, int on_device);
+
+/* ------------------------------------------------------------------ *
+ * BP CG, linear interpolation (BPCG, bpcg.f:70 -> BPCG_2 bpcg.f:425,
+ * HIANG hiang.f:40, BPCG_3_LIN bpcg.f:818).  projs = float[nang*n*n];
+ * vol_out = float[n*n*n]; log_out (may be NULL) = float[3*maxit] receiving
+ * (iteration, DIFFERENCE, CHISQ) as the RESULTS lines (bpcg.f:1213-1216);
+ * niter_out receives the iterations run.  mode = 1, 2 or 3 (order of the
+ * regulariser); lambda = LAMBDA.  Returns 102 for 'RADIUS TOO LARGE'.
+ * ------------------------------------------------------------------ */
+int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* angles,
+             float ri, float errm, float chim, int maxit, int mode, float lambda,
+             float* vol_out, float* log_out, int* niter_out);
+
+/* One application of the BP CG operators on device arrays, for the
+ * differentiable wrapper and adjointness checks.  spi_cg_project: PRJCQ_N
+ * (prjcq.f:48-82) of vol into projs (overwritten).  spi_cg_backproject:
+ * BCKPJ_LIN (bckpj.f:59-94) of projs summed into vol (overwritten). */
+int spi_cg_project(spi_ctx* ctx, const float* vol, int n, float ri, const float* angles,
+                   int nang, float* projs, int on_device);
+int spi_cg_backproject(spi_ctx* ctx, const float* projs, int n, float ri, const float* angles,
+                       int nang, float* vol, int on_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPIDER_B200_H */

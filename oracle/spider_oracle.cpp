@@ -1,0 +1,1082 @@
+// SPIDER reconstruction oracle -- TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement, in C++17 + OpenMP, of the Fortran routines of SPIDER's
+// Fourier gridding back-projection (BP 3F / BP 32F), its trilinear projector
+// (PJ 3Q) and its conjugate-gradient reconstruction (BP CG, linear mode).
+// Every function names the reference file:line it restates.  Only the test
+// suite, the smoke check and the CPU-baseline leg of the benchmark load this
+// library; the product path never links, calls or falls back to it.
+//
+// Parity status: UNPINNED against outputs of the reference itself.  The
+// reference is Fortran 77/90 + FFTW3 and neither gfortran nor libfftw3f exist
+// on this machine, and the reference ships no golden volumes for this path
+// (its KATs need the angle document `savangbprp`, absent from the tree).  The
+// sub-functions are pinned to independent implementations instead: the
+// Kaiser-Bessel table and the gridding-correction Bessel values against
+// scipy.special, the FFT against numpy.fft, the Euler matrix against an
+// independent rotation composition (tests/test_oracle_pins.py).
+//
+// Arithmetic rules (kept identical in the CUDA path so that every index,
+// interpolation weight and table entry is bit-identical, and only the
+// summation order of accumulations differs):
+//   * coordinates, table indices and weights are IEEE float, evaluated left
+//     to right without contraction (built with -ffp-contract=off);
+//   * Fortran NINT = round half away from zero, IFIX = truncation;
+//   * SPIDER's `QUADPI = 3.14159...` literals are default-REAL constants, so
+//     pi enters the Euler-angle code rounded to single precision
+//     (cang.f:62-63, wpro_n.f:62-63, hiang.f:45-46).
+// The `prec` argument selects the accumulation type: 0 = REAL (FP32, the
+// reference's storage types), 1 = DOUBLE (FP64 oracle).  FFTs are computed in
+// double in both modes and rounded to the storage type.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+typedef std::complex<double> cd;
+
+// pi as the reference's Euler-angle routines see it (single-precision literal)
+const double QUADPI_F = (double)3.14159265358979323846f;
+
+inline int nint_pos(float v) {            // Fortran NINT for v >= 0
+  float f = std::floor(v);
+  return (int)f + ((v - f) >= 0.5f ? 1 : 0);
+}
+
+inline int ifix(float v) { return (int)v; }   // truncation toward zero
+
+// ---------------------------------------------------------------- FFT ------
+// Mixed-radix recursive Cooley-Tukey in double (radices 2,3,4,5,7 and a
+// generic DFT for any other prime).  sign = -1 forward (e^-i), +1 backward.
+struct FFT1 {
+  int n = 0;
+  int sign = -1;
+  std::vector<cd> w;  // w[j] = exp(sign*2*pi*i*j/n)
+  std::vector<int> fac;
+  FFT1() {}
+  FFT1(int n_, int sign_) : n(n_), sign(sign_), w(n_) {
+    for (int j = 0; j < n; ++j) {
+      double a = 2.0 * M_PI * (double)j / (double)n * (double)sign;
+      w[j] = cd(std::cos(a), std::sin(a));
+    }
+    int m = n;
+    while (m > 1) {
+      int p = 0;
+      if (m % 4 == 0) p = 4;
+      else if (m % 2 == 0) p = 2;
+      else if (m % 3 == 0) p = 3;
+      else if (m % 5 == 0) p = 5;
+      else if (m % 7 == 0) p = 7;
+      else { for (int q = 11; q <= m; q += 2) if (m % q == 0) { p = q; break; } }
+      fac.push_back(p);
+      m /= p;
+    }
+  }
+  // out[k] = sum_j in[j*istride] w^(j k)
+  void rec(const cd* in, int istride, cd* out, int len, int fi, int tstride, cd* tmp) const {
+    if (len == 1) { out[0] = in[0]; return; }
+    int p = fac[fi];
+    int m = len / p;
+    for (int q = 0; q < p; ++q)
+      rec(in + q * istride, istride * p, out + q * m, m, fi + 1, tstride * p, tmp);
+    // butterflies: X[k + r m] = sum_q w_len^{q (k + r m)} Y_q[k]
+    for (int k = 0; k < m; ++k) {
+      cd y[64];
+      cd* yy = (p <= 64) ? y : tmp;
+      for (int q = 0; q < p; ++q) {
+        long e = (long)q * k * tstride % n;
+        yy[q] = out[q * m + k] * w[e];
+      }
+      for (int r = 0; r < p; ++r) {
+        cd s = 0;
+        for (int q = 0; q < p; ++q) {
+          long e = (long)q * r * m * tstride % n;
+          s += yy[q] * w[e];
+        }
+        tmp[p + r] = s;   // staged to avoid clobbering yy
+      }
+      for (int r = 0; r < p; ++r) out[k + r * m] = tmp[p + r];
+    }
+  }
+  void exec(const cd* in, int istride, cd* out) const {
+    std::vector<cd> tmp(2 * n + 130);
+    rec(in, istride, out, n, 0, 1, tmp.data());
+  }
+};
+
+// ---------------------------------------------------- KB table (A4) -------
+// FILLBESSIL, fillbessi0.f:88-125 (inline copy bp32f.f:193-214)
+struct KBTable {
+  float tab[5000];
+  float fltb, alpha, aaaa;
+  int ln2;
+};
+
+void fill_kb(int n2, KBTable& t) {
+  const int ltab = 4999, ln = 5;
+  t.ln2 = ln / 2;
+  float v = (float)(ln - 1) / 2.0f / (float)n2;
+  t.alpha = 6.5f;
+  t.aaaa = 0.9f * v;
+  float b0 = std::sqrt(t.alpha) * (float)std::cyl_bessel_i(1.0, (double)t.alpha);
+  t.fltb = (float)ltab / (float)(t.ln2 + 1);
+  for (int i = 0; i <= ltab; ++i) {
+    float s = (float)i / t.fltb / (float)n2;
+    if (s <= t.aaaa) {
+      float q = s / t.aaaa;
+      float xt = std::sqrt(1.0f - q * q);
+      float ax = t.alpha * xt;
+      t.tab[i] = std::sqrt(ax) * (float)std::cyl_bessel_i(1.0, (double)ax) / b0;
+    } else {
+      t.tab[i] = 0.0f;
+    }
+  }
+}
+
+// ---------------------------------------------------- Euler (A2) ----------
+// CANG, cang.f:44-81
+void cang(float phi, float theta, float psi, float* dm) {
+  const double d2r = QUADPI_F / 180.0;
+  double cphi = std::cos((double)phi * d2r), sphi = std::sin((double)phi * d2r);
+  double cthe = std::cos((double)theta * d2r), sthe = std::sin((double)theta * d2r);
+  double cpsi = std::cos((double)psi * d2r), spsi = std::sin((double)psi * d2r);
+  dm[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+  dm[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+  dm[2] = (float)(-sthe * cpsi);
+  dm[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+  dm[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+  dm[5] = (float)(sthe * spsi);
+  dm[6] = (float)(sthe * cphi);
+  dm[7] = (float)(sthe * sphi);
+  dm[8] = (float)(cthe);
+}
+
+// DMS = MATMUL(SM, DM) of two column-major 3x3 REAL matrices (bp3f.f:460-466)
+void matmul33(const float* sm, const float* dm, float* out) {
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      float s = sm[i] * dm[3 * j];
+      s = s + sm[i + 3] * dm[1 + 3 * j];
+      s = s + sm[i + 6] * dm[2 + 3 * j];
+      out[i + 3 * j] = s;
+    }
+}
+
+// ------------------------------------------------ Fourier grid ------------
+template <class R>
+struct Grid {
+  int nx, n;
+  std::vector<std::complex<R>> X;  // X[(k*n + j)*(nx+1) + i]
+  std::vector<R> W;
+  Grid(int nx_) : nx(nx_), n(2 * nx_), X((size_t)(nx_ + 1) * 4 * nx_ * nx_), W((size_t)(nx_ + 1) * 4 * nx_ * nx_) {}
+  size_t idx(int i, int j, int k) const { return ((size_t)k * n + j) * (nx + 1) + i; }
+};
+
+// PADD2 + ASTA_D (bp3f.f:1307-1343, asta.f:61-92), FMRS_2 forward with the
+// SPIDER sign (fftw3.f:409-419), phase (-1)^(I+J+1) (bp3f.f:453-458).
+// Output bi[jrow*(nx+1) + i], jrow 0-based, i = 0..nx.
+template <class R>
+void stage_image(const float* proj, int nx, std::vector<std::complex<R>>& bi,
+                 const FFT1& fx, const FFT1& fy) {
+  const int n = 2 * nx;
+  // ASTA_D: mean of pixels outside radius L/2 (integer division, then REAL)
+  float r = (float)(nx / 2);
+  float rr = r * r;
+  int nc = nx / 2 + 1;
+  double aba = 0.0, klp = 0.0;
+  for (int j = 1; j <= nx; ++j) {
+    float t = (float)(j - nc);
+    float xx = t * t;
+    for (int i = 1; i <= nx; ++i) {
+      float t2 = (float)(i - nc);
+      if (xx + t2 * t2 > rr) { aba += (double)proj[(j - 1) * nx + (i - 1)]; klp += 1.0; }
+    }
+  }
+  double qs = aba / (double)(float)klp;
+  int ip = (n - nx) / 2 + nx % 2;
+  std::vector<cd> img((size_t)n * n, cd(0, 0));
+  for (int j = 1; j <= nx; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      float v = (float)((double)proj[(j - 1) * nx + (i - 1)] - qs);
+      img[(size_t)(ip + j - 1) * n + (ip + i - 1)] = cd(v, 0.0);
+    }
+  // 2D forward FFT: rows (x) then columns (y)
+  std::vector<cd> row(n), col(n), tmp(n);
+  for (int y = 0; y < n; ++y) {
+    fx.exec(&img[(size_t)y * n], 1, row.data());
+    for (int x = 0; x < n; ++x) img[(size_t)y * n + x] = row[x];
+  }
+  bi.assign((size_t)(nx + 1) * n, std::complex<R>(0, 0));
+  for (int x = 0; x <= nx; ++x) {
+    fy.exec(&img[x], n, col.data());
+    for (int y = 0; y < n; ++y) {
+      // SPIDER sign: negate imaginary part; store in REAL or DOUBLE
+      std::complex<R> v((R)col[y].real(), (R)(-col[y].imag()));
+      // (-1)**(I+J+1) with J 1-based == (-1)**(i+y) with y 0-based
+      if (((x + y) & 1) != 0) v = -v;
+      bi[(size_t)y * (nx + 1) + x] = v;
+    }
+  }
+}
+
+// ONELINE, oneline.f:38-200 (called as ONELINE(J,N2,NX,...), bp3f.f:477:
+// callee N = 2*NX, callee N2 = NX)
+template <class R>
+void oneline(int J, Grid<R>& g, const std::complex<R>* bi, const float* dm, const KBTable& kb) {
+  const int N = g.n, N2 = g.nx, LN2 = kb.ln2;
+  const int JP = (J >= 0) ? J : N + J;
+  const float fltb = kb.fltb;
+  for (int I = 0; I <= N2; ++I) {
+    if (!((I * I + J * J) < (N * N / 4) && !(I == 0 && J < 0))) continue;
+    float xnew = (float)I * dm[0] + (float)J * dm[3];
+    float ynew = (float)I * dm[1] + (float)J * dm[4];
+    float znew = (float)I * dm[2] + (float)J * dm[5];
+    std::complex<R> btq;
+    if (xnew < 0.0f) {
+      xnew = -xnew; ynew = -ynew; znew = -znew;
+      btq = std::conj(bi[(size_t)JP * (N2 + 1) + I]);
+    } else {
+      btq = bi[(size_t)JP * (N2 + 1) + I];
+    }
+    int ixn = ifix((xnew + 0.5f) + (float)N) - N;
+    int iyn = ifix((ynew + 0.5f) + (float)N) - N;
+    int izn = ifix((znew + 0.5f) + (float)N) - N;
+    if (!(ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+          izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1)))
+      continue;
+    if (ixn >= 0) {
+      int lb = -std::min(ixn, LN2);
+      for (int lz = -LN2; lz <= LN2; ++lz) {
+        int izp = izn + lz;
+        int iza = (izp >= 0) ? izp : N + izp;
+        float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
+        if (tz == 0.0f) continue;
+        for (int ly = -LN2; ly <= LN2; ++ly) {
+          int iyp = iyn + ly;
+          int iya = (iyp >= 0) ? iyp : N + iyp;
+          float ty = kb.tab[nint_pos(std::fabs(ynew - (float)iyp) * fltb)] * tz;
+          if (ty == 0.0f) continue;
+          for (int ixp = lb + ixn; ixp <= LN2 + ixn; ++ixp) {
+            float wg = kb.tab[nint_pos(std::fabs(xnew - (float)ixp) * fltb)] * ty;
+            if (wg != 0.0f) {
+              size_t q = g.idx(ixp, iya, iza);
+              g.X[q] += btq * (R)wg;
+              g.W[q] += (R)wg;
+            }
+          }
+        }
+      }
+    }
+    if (ixn < LN2) {  // reflected points, oneline.f:118-150
+      for (int lz = -LN2; lz <= LN2; ++lz) {
+        int izp = izn + lz;
+        int izt = (izp > 0) ? N - izp : -izp;
+        float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
+        if (tz == 0.0f) continue;
+        for (int ly = -LN2; ly <= LN2; ++ly) {
+          int iyp = iyn + ly;
+          int iyt = (iyp > 0) ? N - iyp : -iyp;
+          float ty = kb.tab[nint_pos(std::fabs(ynew - (float)iyp) * fltb)] * tz;
+          if (ty == 0.0f) continue;
+          for (int ixp = ixn - LN2; ixp <= -1; ++ixp) {
+            float wg = kb.tab[nint_pos(std::fabs(xnew - (float)ixp) * fltb)] * ty;
+            if (wg != 0.0f) {
+              size_t q = g.idx(-ixp, iyt, izt);
+              g.X[q] += std::conj(btq) * (R)wg;
+              g.W[q] += (R)wg;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// SYMPLANE0, bp32f.f:1051-1088 (called as SYMPLANE0(X,W,NX,N2): callee
+// N2 = NX, callee N = 2*NX).  1-based IYA/IZA mapped to 0-based a-1.
+template <class R>
+void symplane0(Grid<R>& g) {
+  const int N2 = g.nx, N = g.n;
+  auto X = [&](int a, int b) -> std::complex<R>& { return g.X[g.idx(0, a - 1, b - 1)]; };
+  auto W = [&](int a, int b) -> R& { return g.W[g.idx(0, a - 1, b - 1)]; };
+  for (int iza = 2; iza <= N2; ++iza)
+    for (int iya = 2; iya <= N2; ++iya) {
+      X(iya, iza) = X(iya, iza) + std::conj(X(N - iya + 2, N - iza + 2));
+      W(iya, iza) = W(iya, iza) + W(N - iya + 2, N - iza + 2);
+      X(N - iya + 2, N - iza + 2) = std::conj(X(iya, iza));
+      W(N - iya + 2, N - iza + 2) = W(iya, iza);
+      X(N - iya + 2, iza) = X(N - iya + 2, iza) + std::conj(X(iya, N - iza + 2));
+      W(N - iya + 2, iza) = W(N - iya + 2, iza) + W(iya, N - iza + 2);
+      X(iya, N - iza + 2) = std::conj(X(N - iya + 2, iza));
+      W(iya, N - iza + 2) = W(N - iya + 2, iza);
+    }
+  for (int iya = 2; iya <= N2; ++iya) {
+    X(iya, 1) = X(iya, 1) + std::conj(X(N - iya + 2, 1));
+    W(iya, 1) = W(iya, 1) + W(N - iya + 2, 1);
+    X(N - iya + 2, 1) = std::conj(X(iya, 1));
+    W(N - iya + 2, 1) = W(iya, 1);
+  }
+  for (int iza = 2; iza <= N2; ++iza) {
+    X(1, iza) = X(1, iza) + std::conj(X(1, N - iza + 2));
+    W(1, iza) = W(1, iza) + W(1, N - iza + 2);
+    X(1, N - iza + 2) = std::conj(X(1, iza));
+    W(1, N - iza + 2) = W(1, iza);
+  }
+}
+
+// Gridding-correction radial table: WKB as a function of the integer squared
+// radius LR (WINDKB2A, bp32f.f:964-1005).  nu = NNN/2 = 1.5.  I_nu(x)/x^nu and
+// J_nu(x)/x^nu from their power series (exact mathematics of RIBSL/RJBSL,
+// besi1.f:276-1239, at order 3/2).
+double inu_over_xnu(double x, double nu) {   // I_nu(x)/x^nu
+  double q = x * x / 4.0, term = 1.0 / std::tgamma(nu + 1.0), s = term;
+  for (int k = 1; k < 200; ++k) { term *= q / ((double)k * (nu + k)); s += term; if (term < 1e-18 * s) break; }
+  return s / std::pow(2.0, nu);
+}
+double jnu_over_xnu(double x, double nu) {   // J_nu(x)/x^nu
+  double q = -x * x / 4.0, term = 1.0 / std::tgamma(nu + 1.0), s = term;
+  for (int k = 1; k < 400; ++k) { term *= q / ((double)k * (nu + k)); s += term; if (std::fabs(term) < 1e-18 * std::fabs(s)) break; }
+  return s / std::pow(2.0, nu);
+}
+
+void windkb_table(int nx, const KBTable& kb, std::vector<float>& wkb) {
+  const float quadpi = 3.14159265358979323846f;
+  const float twopi = 2.0f * quadpi;
+  int l2 = (nx / 2) * (nx / 2);
+  const double xnu = 1.5;
+  const float alpha = kb.alpha;
+  double wkb0 = std::pow((double)alpha, xnu) / (inu_over_xnu(alpha, xnu) * std::pow((double)alpha, xnu));
+  float qrt = (twopi * kb.aaaa) * (twopi * kb.aaaa);
+  wkb.assign(l2 + 1, 1.0f);
+  for (int lr = 0; lr <= l2; ++lr) {
+    float sigma = qrt * (float)lr - alpha * alpha;
+    double w;
+    if (std::fabs(sigma) < 1.0e-7f) w = 1.0;
+    else if (sigma > 0.0f) w = wkb0 * jnu_over_xnu(std::sqrt((double)sigma), xnu);
+    else w = wkb0 * inu_over_xnu(std::sqrt((double)std::fabs(sigma)), xnu);
+    wkb[lr] = (float)std::fabs(w);
+  }
+}
+
+// NRMW2 (bp3f.f:1347-1371) + FMRS_3 inverse (fftw3.f:426-449) + WINDKB2A
+// (bp32f.f:945-1045).  Consumes the grid; writes vol (nx^3, x fastest).
+template <class R>
+void finish_volume(Grid<R>& g, const KBTable& kb, float* vol) {
+  const int nx = g.nx, n = g.n, h = nx + 1;
+  // NRMW2: X = X * (-1)**(I+J+K) / W  if W > 0.1 else 0   (J,K 1-based)
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        size_t q = g.idx(i, j, k);
+        if (g.W[q] > (R)0.1f) {
+          std::complex<R> v = g.X[q];
+          if (((i + j + k) & 1) != 0) v = -v;
+          g.X[q] = std::complex<R>(v.real() / g.W[q], v.imag() / g.W[q]);
+        } else {
+          g.X[q] = std::complex<R>(0, 0);
+        }
+      }
+  // inverse: SPIDER sign (negate Im), c2c along z and y, c2r along x
+  FFT1 fb(n, +1);
+  std::vector<cd> G((size_t)h * n * n);
+  #pragma omp parallel
+  {
+    std::vector<cd> line(n), out(n);
+    #pragma omp for collapse(2)
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= nx; ++i) {
+          std::complex<R> v = g.X[g.idx(i, j, k)];
+          G[((size_t)k * n + j) * h + i] = cd((double)v.real(), -(double)v.imag());
+        }
+    #pragma omp for collapse(2)
+    for (int k = 0; k < n; ++k)
+      for (int i = 0; i <= nx; ++i) {
+        for (int j = 0; j < n; ++j) line[j] = G[((size_t)k * n + j) * h + i];
+        fb.exec(line.data(), 1, out.data());
+        for (int j = 0; j < n; ++j) G[((size_t)k * n + j) * h + i] = out[j];
+      }
+    #pragma omp for collapse(2)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        for (int k = 0; k < n; ++k) line[k] = G[((size_t)k * n + j) * h + i];
+        fb.exec(line.data(), 1, out.data());
+        for (int k = 0; k < n; ++k) G[((size_t)k * n + j) * h + i] = out[k];
+      }
+  }
+  // c2r along x: only the crop [ip, ip+nx) in every dimension is needed
+  const int ip = (n - nx) / 2 + nx % 2;  // WINDKB2A IP (0-based start of crop)
+  const R pix = (sizeof(R) == 4) ? (R)(1.0f / (float)((long)n * n * n)) : (R)(1.0 / ((double)n * n * n));
+  std::vector<R> crop((size_t)nx * nx * nx);
+  #pragma omp parallel
+  {
+    std::vector<cd> line(n), out(n);
+    #pragma omp for collapse(2)
+    for (int k = 0; k < nx; ++k)
+      for (int j = 0; j < nx; ++j) {
+        const cd* gr = &G[((size_t)(ip + k) * n + (ip + j)) * h];
+        line[0] = cd(gr[0].real(), 0.0);
+        line[nx] = cd(gr[nx].real(), 0.0);
+        for (int i = 1; i < nx; ++i) { line[i] = gr[i]; line[n - i] = std::conj(gr[i]); }
+        fb.exec(line.data(), 1, out.data());
+        for (int i = 0; i < nx; ++i) {
+          R v = (R)out[ip + i].real();
+          crop[((size_t)k * nx + j) * nx + i] = v * pix;
+        }
+      }
+  }
+  // WINDKB2A: divide by |WKB(LR)|, shell mean, subtract, mask
+  std::vector<float> wkb;
+  windkb_table(nx, kb, wkb);
+  const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1), c = nx / 2 + 1;
+  R tnr = 0;
+  long m = 0;
+  for (int k = 1; k <= nx; ++k)
+    for (int j = 1; j <= nx; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        int lr = (k - c) * (k - c) + (j - c) * (j - c) + (i - c) * (i - c);
+        if (lr <= l2) {
+          R& v = crop[((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1)];
+          v = v / (R)wkb[lr];
+          if (lr >= l2p) { tnr += v; ++m; }
+        }
+      }
+  tnr = tnr / (R)(float)m;
+  for (int k = 1; k <= nx; ++k)
+    for (int j = 1; j <= nx; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        int lr = (k - c) * (k - c) + (j - c) * (j - c) + (i - c) * (i - c);
+        size_t q = ((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1);
+        vol[q] = (lr <= l2) ? (float)(crop[q] - tnr) : 0.0f;
+      }
+}
+
+// BP3FQ image loop (bp3f.f:298-515) / BP32FQ (bp32f.f:433-939): every image
+// is staged and inserted row by row into grid `route[img]`, rows striped by
+// LN1 = 6 under OpenMP exactly like the reference's SP_MP build.
+template <class R>
+void insert_images(std::vector<Grid<R>*>& grids, const float* imgs, int nx, int nang,
+                   const float* dm9, const float* sm9, int nsym, const uint8_t* route,
+                   const KBTable& kb, int nthreads) {
+  const int n = 2 * nx;
+  FFT1 fx(n, -1), fy(n, -1);
+  std::vector<std::complex<R>> bi;
+  for (int a = 0; a < nang; ++a) {
+    stage_image<R>(imgs + (size_t)a * nx * nx, nx, bi, fx, fy);
+    Grid<R>& g = *grids[route ? route[a] : 0];
+    for (int is = 0; is < std::max(1, nsym); ++is) {
+      float dms[9];
+      if (nsym > 1) matmul33(sm9 + 9 * is, dm9 + 9 * a, dms);
+      else std::memcpy(dms, dm9 + 9 * a, sizeof(dms));
+      const int ln1 = 6;
+      for (int jt = 1; jt <= ln1; ++jt) {
+        #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+        for (int J = -nx + jt; J <= nx; J += ln1) oneline<R>(J, g, bi.data(), dms, kb);
+      }
+    }
+  }
+}
+
+template <class R>
+void grid_out(const Grid<R>& g, double* x_out, double* w_out) {
+  size_t nv = g.W.size();
+  for (size_t q = 0; q < nv; ++q) {
+    if (x_out) { x_out[2 * q] = (double)g.X[q].real(); x_out[2 * q + 1] = (double)g.X[q].imag(); }
+    if (w_out) w_out[q] = (double)g.W[q];
+  }
+}
+
+template <class R>
+int bp_run(const float* imgs, int nx, int nang, const float* angles, const float* symang,
+           int nsym, const uint8_t* half, int halt, float* vol_all, float* vol_1, float* vol_2,
+           double* x_out, double* w_out, int nthreads) {
+  if (nx < 8 || nx % 2 != 0) return 101;
+  KBTable kb;
+  fill_kb(2 * nx, kb);
+  std::vector<float> dm((size_t)9 * nang), sm((size_t)9 * std::max(1, nsym));
+  for (int a = 0; a < nang; ++a)  // BUILDM1: CANG(phi, theta, psi), bp3f.f:1287
+    cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], &dm[9 * a]);
+  for (int s = 0; s < nsym; ++s)  // BUILDS, builds.f:52
+    cang(symang[3 * s + 2], symang[3 * s + 1], symang[3 * s + 0], &sm[9 * s]);
+  Grid<R> ge(nx);
+  std::vector<Grid<R>*> grids{&ge};
+  Grid<R>* go = nullptr;
+  if (half) { go = new Grid<R>(nx); grids.push_back(go); }
+  std::vector<uint8_t> route;
+  if (half) { route.resize(nang); for (int a = 0; a < nang; ++a) route[a] = half[a] ? 0 : 1; }
+  insert_images<R>(grids, imgs, nx, nang, dm.data(), sm.data(), nsym, half ? route.data() : nullptr, kb, nthreads);
+  symplane0<R>(ge);
+  if (go) symplane0<R>(*go);
+  if (halt) {  // BP 3F P: partial X and W after SYMPLANE0
+    grid_out(ge, x_out, w_out);
+    delete go;
+    return 0;
+  }
+  if (!half) {
+    finish_volume<R>(ge, kb, vol_all);
+    return 0;
+  }
+  // BP 32F: first sample = XE, both = XE+XO (ADDADA), second = XO
+  Grid<R> both(nx);
+  for (size_t q = 0; q < ge.W.size(); ++q) { both.X[q] = ge.X[q] + go->X[q]; both.W[q] = ge.W[q] + go->W[q]; }
+  if (vol_1) finish_volume<R>(ge, kb, vol_1);
+  if (vol_all) finish_volume<R>(both, kb, vol_all);
+  if (vol_2) finish_volume<R>(*go, kb, vol_2);
+  delete go;
+  return 0;
+}
+
+// ------------------------------------------------ PJ 3Q (A14) -------------
+// PREPCUB (prepcub.f:54-109): runs of voxels inside the sphere, centred.
+struct RunC { int i1, i2, x, y, z; };
+void prepcub(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<RunC>& runs) {
+  float r = ri * ri;
+  runs.clear();
+  for (int i1 = 1; i1 <= nslice; ++i1) {
+    float t = (float)(i1 - ldpz);
+    float xx = t * t;
+    for (int i2 = 1; i2 <= nrow; ++i2) {
+      float t2 = (float)(i2 - ldpy);
+      float yy = t2 * t2 + xx;
+      bool first = true;
+      for (int i3 = 1; i3 <= nsam; ++i3) {
+        float t3 = (float)(i3 - ldpx);
+        float rc = t3 * t3 + yy;
+        if (first) {
+          if (rc > r) continue;
+          first = false;
+          runs.push_back(RunC{i3, i3, i3 - ldpx, i2 - ldpy, i1 - ldpz});
+        } else if (rc <= r) {
+          runs.back().i2 = i3;
+        }
+      }
+    }
+  }
+}
+
+// WPRO_N (wpro_n.f:44-150): one projection, trilinear gather along z.
+template <class R>
+void wpro_n(R* b, int nsam, int nrow, int nslice, const float* cube, const std::vector<RunC>& runs,
+            float phi, float theta, float psi, float ri, int ldpx, int ldpy, int ldpz) {
+  const double d2r = QUADPI_F / 180.0;
+  double cphi = std::cos((double)phi * d2r), sphi = std::sin((double)phi * d2r);
+  double cthe = std::cos((double)theta * d2r), sthe = std::sin((double)theta * d2r);
+  double cpsi = std::cos((double)psi * d2r), spsi = std::sin((double)psi * d2r);
+  float dm[9];
+  dm[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+  dm[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+  dm[2] = (float)(-sthe * cpsi);
+  dm[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+  dm[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+  dm[5] = (float)(sthe * spsi);
+  dm[6] = (float)(sthe * cphi);
+  dm[7] = (float)(sthe * sphi);
+  dm[8] = (float)(cthe);
+  const float dm1 = dm[0], dm2 = dm[1], dm3 = dm[2];
+  std::fill(b, b + (size_t)nsam * nrow, (R)0);
+  int dim = std::min(nsam, std::min(nrow, nslice));
+  bool nocheck = (2.0f * (ri + 1.0f) + 1.0f) <= (float)dim;
+  auto C = [&](int x, int y, int z) -> R { return (R)cube[((size_t)(z - 1) * nrow + (y - 1)) * nsam + (x - 1)]; };
+  for (const RunC& rn : runs) {
+    int k = rn.y + ldpy;
+    float xb = (float)rn.x * dm[0] + (float)rn.y * dm[3] + (float)rn.z * dm[6] + (float)ldpx;
+    float yb = (float)rn.x * dm[1] + (float)rn.y * dm[4] + (float)rn.z * dm[7] + (float)ldpy;
+    float zb = (float)rn.x * dm[2] + (float)rn.y * dm[5] + (float)rn.z * dm[8] + (float)ldpz;
+    for (int j = rn.i1; j <= rn.i2; ++j) {
+      int iox = ifix(xb), ioy = ifix(yb), ioz = ifix(zb);
+      bool ok = nocheck || (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice);
+      if (ok) {
+        R dx = (R)(xb - (float)iox), dy = (R)(yb - (float)ioy), dz = (R)(zb - (float)ioz);
+        R a1 = C(iox, ioy, ioz);
+        R a2 = C(iox + 1, ioy, ioz) - a1;
+        R a3 = C(iox, ioy + 1, ioz) - a1;
+        R a4 = C(iox, ioy, ioz + 1) - a1;
+        R a5 = -a2 - C(iox, ioy + 1, ioz) + C(iox + 1, ioy + 1, ioz);
+        R a61 = -C(iox, ioy, ioz + 1) + C(iox + 1, ioy, ioz + 1);
+        R a6 = -a2 + a61;
+        R a7 = -a3 - C(iox, ioy, ioz + 1) + C(iox, ioy + 1, ioz + 1);
+        R a8 = -a5 - a61 - C(iox, ioy + 1, ioz + 1) + C(iox + 1, ioy + 1, ioz + 1);
+        R& o = b[(size_t)(k - 1) * nsam + (j - 1)];
+        o = o + a1 + dz * (a4 + a6 * dx + (a7 + a8 * dx) * dy) + a3 * dy + dx * (a2 + a5 * dy);
+      }
+      xb = xb + dm1;
+      yb = yb + dm2;
+      zb = zb + dm3;
+    }
+  }
+}
+
+// ------------------------------------------------ BP CG (A15, A16) --------
+// PREPCUB_S (prepcub_s.f:54-111): runs with 1-based linear indices.
+struct RunS { int l1, l2, x, y, z; };
+void prepcub_s(int n, float ri, int ldp, std::vector<RunS>& runs) {
+  float r = ri * ri;
+  int nmat = 0;
+  runs.clear();
+  for (int i1 = 1; i1 <= n; ++i1) {
+    float t = (float)(i1 - ldp);
+    float xx = t * t;
+    for (int i2 = 1; i2 <= n; ++i2) {
+      float t2 = (float)(i2 - ldp);
+      float yy = t2 * t2 + xx;
+      bool first = true;
+      for (int i3 = 1; i3 <= n; ++i3) {
+        ++nmat;
+        float t3 = (float)(i3 - ldp);
+        float rc = t3 * t3 + yy;
+        if (first) {
+          if (rc > r) continue;
+          first = false;
+          runs.push_back(RunS{nmat, nmat, i3, i2, i1});
+        } else if (rc <= r) {
+          runs.back().l2 = nmat;
+        }
+      }
+    }
+  }
+}
+
+// PROJT difference table (bpcg.f:732-742): projt[4*(I-1) + c], I 1-based.
+template <class R>
+void make_projt(const R* proj, int n, std::vector<R>& projt) {
+  projt.assign((size_t)4 * n * n, (R)0);
+  for (int I = 1; I <= n * n - n - 1; ++I) {
+    R pt = proj[I - 1];
+    projt[4 * (I - 1) + 0] = pt;
+    projt[4 * (I - 1) + 1] = proj[I + n - 1] - pt;
+    projt[4 * (I - 1) + 2] = proj[I] - pt;
+    projt[4 * (I - 1) + 3] = proj[I + n] - proj[I] - projt[4 * (I - 1) + 1];
+  }
+}
+
+// BCKPJ_LIN, SP_MP branch (bckpj.f:59-94): voxel gather, direct XBB formula.
+template <class R>
+void bckpj_lin(R* cube, const float* dm, const R* projt, int n, const std::vector<RunS>& runs, int ldp, int ldpnm, int nthreads) {
+  #pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (long r = 0; r < (long)runs.size(); ++r) {
+    const RunS& rn = runs[r];
+    float xb = ((float)(rn.x - ldp) * dm[0] + (float)(rn.y - ldp) * dm[1] + (float)(rn.z - ldp) * dm[2]) + (float)ldpnm;
+    float yb = ((float)(rn.x - ldp) * dm[3] + (float)(rn.y - ldp) * dm[4] + (float)(rn.z - ldp) * dm[5]) + (float)ldpnm;
+    for (int j = rn.l1; j <= rn.l2; ++j) {
+      int jt = j - rn.l1;
+      float xbb = xb + (float)jt * dm[0];
+      float ybb = yb + (float)jt * dm[3];
+      int iqx = ifix(xbb), iqy = ifix(ybb);
+      const R* B = &projt[4 * ((size_t)(iqy - 1) * n + (iqx - 1))];
+      R dy = (R)(ybb - (float)iqy), dx = (R)(xbb - (float)iqx);
+      cube[j - 1] = cube[j - 1] + B[0] + dy * B[1] + dx * (B[2] + dy * B[3]);
+    }
+  }
+}
+
+// PRJCQ_N (prjcq.f:48-82): voxel splat with sequential XB accumulation.
+template <class R>
+void prjcq_n(const R* cube, const float* dm, R* prj, int n, const std::vector<RunS>& runs, int ldp, int ldpnm) {
+  for (const RunS& rn : runs) {
+    float xb = (float)(rn.x - ldp) * dm[0] + (float)(rn.y - ldp) * dm[1] + (float)(rn.z - ldp) * dm[2] + (float)ldpnm;
+    float yb = (float)(rn.x - ldp) * dm[3] + (float)(rn.y - ldp) * dm[4] + (float)(rn.z - ldp) * dm[5] + (float)ldpnm;
+    for (int j = rn.l1; j <= rn.l2; ++j) {
+      int iqx = ifix(xb), iqy = ifix(yb);
+      R c = cube[j - 1];
+      R dx = (R)(xb - (float)iqx);
+      R dy = (R)(yb - (float)iqy) * c;
+      R dx1m = (R)1 - dx;
+      R dy1m = c - dy;
+      R* p = &prj[(size_t)(iqy - 1) * n + (iqx - 1)];
+      p[0] += dx1m * dy1m;
+      p[1] += dx * dy1m;
+      p[n] += dx1m * dy;
+      p[n + 1] += dx * dy;
+      xb = xb + dm[0];
+      yb = yb + dm[3];
+    }
+  }
+}
+
+// HIANG (hiang.f:40-112): fold theta >= 90, truncate phi to 0.01 deg, merge
+// duplicates into weights LB, psi := 0, rebuild DM in double.
+// ang[3*i] = phi, ang[3*i+1] = theta, ang[3*i+2] = psi.  Returns LO.
+int hiang(std::vector<float>& ang, int nang, std::vector<float>& dm, std::vector<int>& lb) {
+  lb.assign(nang, 1);
+  for (int i = 0; i < nang; ++i) {
+    if (ang[3 * i + 1] >= 90.0f) {
+      ang[3 * i + 1] = 180.0f - ang[3 * i + 1];
+      ang[3 * i] = ang[3 * i] + 180.0f;
+      if (ang[3 * i] >= 360.0f) ang[3 * i] = ang[3 * i] - 360.0f;
+    }
+  }
+  for (int i = 0; i < nang; ++i) {
+    int jjj = (int)(100.0f * ang[3 * i]);
+    ang[3 * i] = (float)jjj / 100.0f;
+  }
+  for (int i = 0; i < nang - 1; ++i) {
+    if (lb[i] != 0) {
+      for (int j = i + 1; j < nang; ++j) {
+        if (lb[i] != 0) {   // the reference tests LB(I) here (hiang.f:66)
+          if (ang[3 * i] == ang[3 * j] && ang[3 * i + 1] == ang[3 * j + 1]) { lb[i] += 1; lb[j] = 0; }
+        }
+      }
+    }
+  }
+  int lo = 0;
+  for (int i = 0; i < nang; ++i) {
+    if (lb[i] != 0) {
+      ang[3 * lo] = ang[3 * i];
+      ang[3 * lo + 1] = ang[3 * i + 1];
+      ang[3 * lo + 2] = 0.0f;
+      lb[lo] = lb[i];
+      ++lo;
+    }
+  }
+  const double d2r = QUADPI_F / 180.0;
+  dm.assign((size_t)9 * lo, 0.0f);
+  for (int i = 0; i < lo; ++i) {
+    double cphi = std::cos((double)ang[3 * i] * d2r), sphi = std::sin((double)ang[3 * i] * d2r);
+    double cthe = std::cos((double)ang[3 * i + 1] * d2r), sthe = std::sin((double)ang[3 * i + 1] * d2r);
+    double cpsi = 1.0, spsi = 0.0;
+    float* d = &dm[9 * i];
+    d[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+    d[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+    d[2] = (float)(-sthe * cpsi);
+    d[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+    d[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+    d[5] = (float)(sthe * spsi);
+    d[6] = (float)(sthe * cphi);
+    d[7] = (float)(sthe * sphi);
+    d[8] = (float)(cthe);
+  }
+  return lo;
+}
+
+// FIXEDGE1/2/3 (bpcg.f:1278-1517): zero outside the runs, then extend the
+// edge values by `w` voxels along x, then y, then z.
+template <class R>
+void fixedge(R* p, int n, const std::vector<RunS>& runs, int mode) {
+  const long nnn = (long)n * n * n;
+  size_t nt = 0;
+  for (long i = 1; i <= nnn; ++i) {
+    if (nt >= runs.size()) p[i - 1] = 0;
+    else if (i < runs[nt].l1) p[i - 1] = 0;
+    else if (i == runs[nt].l2) ++nt;
+  }
+  auto at = [&](int i, int j, int k) -> R& { return p[((size_t)(k - 1) * n + (j - 1)) * n + (i - 1)]; };
+  // axis passes; `get(line, t)` addresses element t (1-based) of a line
+  for (int axis = 0; axis < 3; ++axis) {
+    for (int a = 1; a <= n; ++a)
+      for (int b = 1; b <= n; ++b) {
+        auto L = [&](int t) -> R& {
+          if (axis == 0) return at(t, b, a);      // K=a, J=b, I=t
+          if (axis == 1) return at(b, t, a);      // K=a, I=b, J=t
+          return at(b, a, t);                     // J=a, I=b, K=t
+        };
+        if (mode == 1) {
+          for (int t = 1; t <= n - 1; ++t) if (L(t + 1) != (R)0) { L(t) = L(t + 1); break; }
+          for (int t = n; t >= 2; --t) if (L(t - 1) != (R)0) { L(t) = L(t - 1); break; }
+        } else if (mode == 2) {
+          for (int t = 2; t <= n - 1; ++t) if (L(t + 1) != (R)0) { L(t) = L(t + 1); L(t - 1) = L(t + 1); break; }
+          for (int t = n - 1; t >= 2; --t) if (L(t - 1) != (R)0) { L(t) = L(t - 1); L(t + 1) = L(t - 1); break; }
+        } else {
+          for (int t = 3; t <= n - 1; ++t) if (L(t + 1) != (R)0) { L(t) = L(t + 1); L(t - 1) = L(t + 1); L(t - 2) = L(t + 1); break; }
+          for (int t = n - 2; t >= 2; --t) if (L(t - 1) != (R)0) { L(t) = L(t - 1); L(t + 1) = L(t - 1); L(t + 2) = L(t - 1); break; }
+        }
+      }
+  }
+}
+
+// BFIRSTS / BSECOND / BTHIRD (bpcg.f:1521-1588)
+template <class R>
+void regularize(R* bcke, const R* p, int n, R anoise, const std::vector<RunS>& runs, int mode) {
+  auto P = [&](long q) -> R { return p[q]; };
+  const long sx = 1, sy = n, sz = (long)n * n;
+  for (const RunS& rn : runs)
+    for (int j = rn.l1; j <= rn.l2; ++j) {
+      long q = j - 1;
+      R v;
+      if (mode == 1) {
+        v = (R)6 * P(q) - (+P(q + sx) + P(q + sy) + P(q + sz) + P(q - sx) + P(q - sy) + P(q - sz));
+      } else if (mode == 2) {
+        v = (R)18 * P(q) - (R)4.0f * P(q + sx) + P(q + 2 * sx) - (R)4.0f * P(q - sx) + P(q - 2 * sx)
+            - (R)4.0f * P(q + sy) + P(q + 2 * sy) - (R)4.0f * P(q - sy) + P(q - 2 * sy)
+            - (R)4.0f * P(q + sz) + P(q + 2 * sz) - (R)4.0f * P(q - sz) + P(q - 2 * sz);
+      } else {
+        v = (R)60 * P(q) - (R)15.0f * P(q + sx) + (R)6.0f * P(q + 2 * sx) - P(q + 3 * sx)
+            - (R)15.0f * P(q - sx) + (R)6.0f * P(q - 2 * sx) - P(q - 3 * sx)
+            - (R)15.0f * P(q + sy) + (R)6.0f * P(q + 2 * sy) - P(q + 3 * sy)
+            - (R)15.0f * P(q - sy) + (R)6.0f * P(q - 2 * sy) - P(q - 3 * sy)
+            - (R)15.0f * P(q + sz) + (R)6.0f * P(q + 2 * sz) - P(q + 3 * sz)
+            - (R)15.0f * P(q - sz) + (R)6.0f * P(q - 2 * sz) - P(q - 3 * sz);
+      }
+      bcke[q] = bcke[q] + anoise * v;
+    }
+}
+
+// BPCG (bpcg.f:70-411) -> BPCG_2 (bpcg.f:425-814) -> HIANG -> BPCG_3_LIN
+// (bpcg.f:818-1238), linear interpolation, non-MPI.  `logv` receives
+// (iteration, err, chi2) triples.  Returns IRTFLG-style status.
+template <class R>
+int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
+             int maxit, int mode, float anoise, float* vol, float* logv, int* niter, int* nang_eff,
+             double* stats, int nthreads) {
+  const int ldp = n / 2 + 1, ldpnm = ldp;
+  std::vector<RunS> runs;
+  prepcub_s(n, ri, ldp, runs);
+  const long nnn = (long)n * n * n;
+  std::vector<R> cb(nnn, (R)0);
+  std::vector<float> ang((size_t)3 * nang), dm((size_t)9 * nang);
+  double d_aba = 0, d_sus = 0, d_ssq = 0, d_klp = 0, d_kls = 0;
+  std::vector<R> proj((size_t)n * n), projt;
+  for (int k = 0; k < nang; ++k) {
+    ang[3 * k + 2] = angles[3 * k + 0];   // psi
+    ang[3 * k + 1] = angles[3 * k + 1];   // theta
+    ang[3 * k + 0] = angles[3 * k + 2];   // phi
+    cang(ang[3 * k], ang[3 * k + 1], ang[3 * k + 2], &dm[9 * k]);
+    const float* x = projs + (size_t)k * n * n;
+    // ASTASQ (bpcg.f:1244-1274)
+    float r = ri * ri;
+    int nc = n / 2 + 1;
+    for (int j = 1; j <= n; ++j) {
+      float t = (float)(j - nc);
+      float xx = t * t;
+      for (int i = 1; i <= n; ++i) {
+        float t2 = (float)(i - nc);
+        float v = x[(j - 1) * n + (i - 1)];
+        if ((xx + t2 * t2) > r) { d_aba += (double)v; d_klp += 1; }
+        else { d_ssq += (double)v * (double)v; d_sus += (double)v; d_kls += 1; }
+      }
+    }
+    for (int i = 0; i < n * n; ++i) proj[i] = (R)x[i];
+    make_projt<R>(proj.data(), n, projt);
+    bckpj_lin<R>(cb.data(), &dm[9 * k], projt.data(), n, runs, ldp, ldpnm, nthreads);
+  }
+  d_aba = d_aba / d_klp;
+  R bnorm = 0;
+  R qt = (sizeof(R) == 4) ? (R)(float)(d_aba * nang) : (R)(d_aba * nang);
+  for (const RunS& rn : runs)
+    for (int j = rn.l1; j <= rn.l2; ++j) {
+      R c = (sizeof(R) == 4) ? (R)(float)((double)cb[j - 1] - (double)qt) : cb[j - 1] - qt;
+      cb[j - 1] = c;
+      bnorm = bnorm + c * c;
+    }
+  d_ssq = d_ssq - d_aba * (2 * d_sus - d_aba * d_kls);
+  R chi2 = (R)d_ssq;
+  if (stats) { stats[0] = d_klp; stats[1] = d_aba; stats[2] = (double)bnorm; stats[3] = (double)chi2; }
+  std::vector<int> lb;
+  int lo = hiang(ang, nang, dm, lb);
+  if (nang_eff) *nang_eff = lo;
+  float di = (float)(n / 2);
+  if ((mode == 1 && (ri + 1.0f + 1.0f) > di) || (mode == 2 && (ri + 2.0f + 1.0f) > di) ||
+      (mode == 3 && (ri + 3.0f + 1.0f) > di))
+    return 102;  // 'RADIUS TOO LARGE', bpcg.f:272-277
+  // BPCG_3_LIN
+  std::vector<R> bckn(nnn, (R)0), bckp(nnn, (R)0), bcke(nnn, (R)0);
+  R q = 0;
+  int it_done = 0;
+  std::vector<std::vector<R>> pbuf(nthreads > 0 ? nthreads : 1);
+  for (int iter = 1; iter <= maxit; ++iter) {
+    R delsq = 0;
+    for (const RunS& rn : runs)
+      for (int j = rn.l1; j <= rn.l2; ++j) delsq = delsq + cb[j - 1] * cb[j - 1];
+    q = q * delsq;
+    for (const RunS& rn : runs)
+      for (int j = rn.l1; j <= rn.l2; ++j) bckp[j - 1] = cb[j - 1] - q * bckp[j - 1];
+    q = (R)-1 / delsq;
+    std::fill(bcke.begin(), bcke.end(), (R)0);
+    int numth = nthreads > 0 ? nthreads : 1;
+    for (int k0 = 0; k0 < lo; k0 += numth) {
+      int lnum = std::min(numth, lo - k0);
+      std::vector<std::vector<R>> projs_k(lnum, std::vector<R>((size_t)n * n, (R)0));
+      #pragma omp parallel for num_threads(numth) schedule(static)
+      for (int t = 0; t < lnum; ++t) prjcq_n<R>(bckp.data(), &dm[9 * (k0 + t)], projs_k[t].data(), n, runs, ldp, ldpnm);
+      for (int t = 0; t < lnum; ++t) {
+        std::vector<R>& pj = projs_k[t];
+        if (lb[k0 + t] > 1)
+          for (auto& v : pj) v = v * (R)lb[k0 + t];
+        make_projt<R>(pj.data(), n, projt);
+        bckpj_lin<R>(bcke.data(), &dm[9 * (k0 + t)], projt.data(), n, runs, ldp, ldpnm, nthreads);
+      }
+    }
+    fixedge<R>(bckp.data(), n, runs, mode);
+    regularize<R>(bcke.data(), bckp.data(), n, (R)anoise, runs, mode);
+    R akden = 0;
+    for (const RunS& rn : runs)
+      for (int j = rn.l1; j <= rn.l2; ++j) akden = akden + bckp[j - 1] * bcke[j - 1];
+    R p = delsq / akden;
+    for (const RunS& rn : runs)
+      for (int j = rn.l1; j <= rn.l2; ++j) {
+        bckn[j - 1] = bckn[j - 1] + p * bckp[j - 1];
+        cb[j - 1] = cb[j - 1] - p * bcke[j - 1];
+      }
+    R err = delsq / bnorm;
+    chi2 = chi2 - p * delsq;
+    if (logv) { logv[3 * (iter - 1)] = (float)iter; logv[3 * (iter - 1) + 1] = (float)err; logv[3 * (iter - 1) + 2] = (float)chi2; }
+    it_done = iter;
+    if (std::fabs((double)err) <= errm || std::fabs((double)chi2) <= chim) break;
+  }
+  if (niter) *niter = it_done;
+  for (long i = 0; i < nnn; ++i) vol[i] = (float)bckn[i];
+  return 0;
+}
+
+}  // namespace
+
+// ============================================================ C ABI =======
+extern "C" {
+
+void orc_fillbessil(int n2, float* tab, float* fltb, float* alpha, float* aaaa) {
+  KBTable t;
+  fill_kb(n2, t);
+  std::memcpy(tab, t.tab, sizeof(t.tab));
+  *fltb = t.fltb; *alpha = t.alpha; *aaaa = t.aaaa;
+}
+
+void orc_windkb_table(int nx, float* out) {
+  KBTable t;
+  fill_kb(2 * nx, t);
+  std::vector<float> w;
+  windkb_table(nx, t, w);
+  std::memcpy(out, w.data(), w.size() * sizeof(float));
+}
+
+void orc_cang(float phi, float theta, float psi, float* dm) { cang(phi, theta, psi, dm); }
+
+// forward (sign=-1) or backward (+1) complex DFT of length n, interleaved re/im
+void orc_fft_c2c(const double* in, double* out, int n, int sign) {
+  FFT1 f(n, sign);
+  f.exec(reinterpret_cast<const cd*>(in), 1, reinterpret_cast<cd*>(out));
+}
+
+// One image through PADD2/FFT/phase: bi_out [2nx][nx+1] complex (re,im)
+void orc_stage_image(const float* proj, int nx, double* bi_out) {
+  FFT1 fx(2 * nx, -1), fy(2 * nx, -1);
+  std::vector<std::complex<double>> bi;
+  stage_image<double>(proj, nx, bi, fx, fy);
+  std::memcpy(bi_out, bi.data(), bi.size() * sizeof(cd));
+}
+
+// BP 3F (halt=0: volume; halt=1: BP 3F P partial X,W) and BP 32F (half!=NULL).
+// angles: 3 per image (psi, theta, phi, degrees); symang: 3 per symmetry.
+int orc_bp3f(const float* imgs, int nx, int nang, const float* angles, const float* symang, int nsym,
+             const uint8_t* half, int halt, int prec, float* vol_all, float* vol_1, float* vol_2,
+             double* x_out, double* w_out, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (prec == 1)
+    return bp_run<double>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
+  return bp_run<float>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
+}
+
+// PJ 3Q: vol (nx,ny,nz x fastest), angles 3 per projection (psi,theta,phi)
+void orc_pj3q(const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
+              int prec, float* proj_out, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  int ldpx = nx / 2 + 1, ldpy = ny / 2 + 1, ldpz = nz / 2 + 1;
+  std::vector<RunC> runs;
+  prepcub(nx, ny, nz, ri, ldpx, ldpy, ldpz, runs);
+  #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int a = 0; a < nang; ++a) {
+    float* out = proj_out + (size_t)a * nx * ny;
+    if (prec == 1) {
+      std::vector<double> b((size_t)nx * ny);
+      wpro_n<double>(b.data(), nx, ny, nz, vol, runs, angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], ri, ldpx, ldpy, ldpz);
+      for (size_t i = 0; i < b.size(); ++i) out[i] = (float)b[i];
+    } else {
+      wpro_n<float>(out, nx, ny, nz, vol, runs, angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], ri, ldpx, ldpy, ldpz);
+    }
+  }
+}
+
+// Number of voxel runs PREPCUB produces (for tests of the run lists)
+int orc_prepcub_count(int nx, int ny, int nz, float ri) {
+  std::vector<RunC> runs;
+  prepcub(nx, ny, nz, ri, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1, runs);
+  return (int)runs.size();
+}
+
+int orc_bpcg(const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
+             int maxit, int mode, float lambda, int prec, float* vol, float* logv, int* niter, int* nang_eff,
+             double* stats, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (prec == 1)
+    return bpcg_run<double>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff, stats, nthreads);
+  return bpcg_run<float>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff, stats, nthreads);
+}
+
+// Single operator applications, for adjointness and parity tests.
+// A (PRJCQ_N) of vol into proj for each angle triple (psi,theta,phi) with DM
+// built by CANG; At (BCKPJ_LIN via PROJT) of projections into vol (summed).
+void orc_prjcq(const float* vol, int n, float ri, const float* angles, int nang, int prec, float* proj_out) {
+  const int ldp = n / 2 + 1;
+  std::vector<RunS> runs;
+  prepcub_s(n, ri, ldp, runs);
+  long nnn = (long)n * n * n;
+  for (int a = 0; a < nang; ++a) {
+    float dm[9];
+    cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);
+    if (prec == 1) {
+      std::vector<double> c(vol, vol + nnn), p((size_t)n * n, 0.0);
+      prjcq_n<double>(c.data(), dm, p.data(), n, runs, ldp, ldp);
+      for (size_t i = 0; i < p.size(); ++i) proj_out[(size_t)a * n * n + i] = (float)p[i];
+    } else {
+      std::vector<float> p((size_t)n * n, 0.0f);
+      prjcq_n<float>(vol, dm, p.data(), n, runs, ldp, ldp);
+      std::memcpy(proj_out + (size_t)a * n * n, p.data(), p.size() * sizeof(float));
+    }
+  }
+}
+
+void orc_bckpj(const float* projs, int n, float ri, const float* angles, int nang, int prec, float* vol_out) {
+  const int ldp = n / 2 + 1;
+  std::vector<RunS> runs;
+  prepcub_s(n, ri, ldp, runs);
+  long nnn = (long)n * n * n;
+  if (prec == 1) {
+    std::vector<double> c(nnn, 0.0), pj((size_t)n * n), pt;
+    for (int a = 0; a < nang; ++a) {
+      float dm[9];
+      cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);
+      for (int i = 0; i < n * n; ++i) pj[i] = projs[(size_t)a * n * n + i];
+      make_projt<double>(pj.data(), n, pt);
+      bckpj_lin<double>(c.data(), dm, pt.data(), n, runs, ldp, ldp, 1);
+    }
+    for (long i = 0; i < nnn; ++i) vol_out[i] = (float)c[i];
+  } else {
+    std::vector<float> c(nnn, 0.0f), pt;
+    for (int a = 0; a < nang; ++a) {
+      float dm[9];
+      cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);
+      make_projt<float>(projs + (size_t)a * n * n, n, pt);
+      bckpj_lin<float>(c.data(), dm, pt.data(), n, runs, ldp, ldp, 1);
+    }
+    std::memcpy(vol_out, c.data(), nnn * sizeof(float));
+  }
+}
+
+// HIANG on angle triples (psi,theta,phi) -> effective (phi,theta) list + LB
+int orc_hiang(const float* angles, int nang, float* phi_theta_out, int* lb_out, float* dm_out) {
+  std::vector<float> ang((size_t)3 * nang), dm;
+  for (int k = 0; k < nang; ++k) { ang[3 * k] = angles[3 * k + 2]; ang[3 * k + 1] = angles[3 * k + 1]; ang[3 * k + 2] = angles[3 * k]; }
+  std::vector<int> lb;
+  int lo = hiang(ang, nang, dm, lb);
+  for (int i = 0; i < lo; ++i) { phi_theta_out[2 * i] = ang[3 * i]; phi_theta_out[2 * i + 1] = ang[3 * i + 1]; lb_out[i] = lb[i]; }
+  if (dm_out) std::memcpy(dm_out, dm.data(), dm.size() * sizeof(float));
+  return lo;
+}
+
+void orc_fixedge(float* p, int n, float ri, int mode) {
+  std::vector<RunS> runs;
+  prepcub_s(n, ri, n / 2 + 1, runs);
+  fixedge<float>(p, n, runs, mode);
+}
+
+int orc_prepcub_s_count(int n, float ri) {
+  std::vector<RunS> runs;
+  prepcub_s(n, ri, n / 2 + 1, runs);
+  return (int)runs.size();
+}
+
+}  // extern "C"

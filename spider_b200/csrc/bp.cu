@@ -1,0 +1,891 @@
+// Fourier gridding back-projection (SPIDER BP 3F / BP 32F) on sm_100a.
+//
+// Per chunk of images:   stage (PADD2 + phase as a circular shift, FP64 mean)
+//                        -> batched cuFFT R2C
+//                        -> insert (ONELINE, one persistent launch per chunk)
+// Per volume:            SYMPLANE0 -> NRMW2 (+ADDADA) -> cuFFT C2R -> WINDKB2A
+//
+// The grid is an array of float4 {Re X, Im X, W, 0} voxels laid out
+// [k][j][i], i = 0..nx fastest (Fortran X(0:NX,N,N) with W interleaved), so
+// each gridding tap is one 16-byte vector atomic in L2.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "../../include/spider_b200.h"
+#include "ctx.h"
+
+namespace spi {
+
+struct SliceDesc {
+  float dm[6];  // DMS(1:6): first two columns of the (symmetrised) rotation
+  int img;      // image index inside the chunk
+  int grid;     // target grid (BP 32F half set)
+};
+static_assert(sizeof(SliceDesc) == 32, "slice descriptor is 32 bytes");
+
+// ----------------------------------------------------------------------------
+// helpers
+__device__ __forceinline__ int nint_pos(float v) {  // Fortran NINT, v >= 0
+  float f = floorf(v);
+  return (int)f + ((__fsub_rn(v, f) >= 0.5f) ? 1 : 0);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ----------------------------------------------------------------------------
+// Stage: PADD2 (bp3f.f:1307-1343) with ASTA_D's FP64 mean outside radius
+// nx/2 (asta.f:61-92).  The phase BI*(-1)**(I+J+1) (bp3f.f:453-458) equals a
+// circular shift of the padded image by n/2 in both axes, so the padded
+// image is written already shifted: pixel i lands at (ip + i - nx) mod n.
+// One CTA per image; images beyond `nvalid` are written as zeros.
+__global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
+                                                    int nvalid, double klp, float* __restrict__ padded) {
+  const int b = blockIdx.x;
+  float* out = padded + (size_t)b * n * n;
+  __shared__ double red[8];
+  __shared__ double qs_sh;
+  const bool valid = b < nvalid;
+  const float* img = imgs + (size_t)b * nx * nx;
+  if (valid) {
+    const float rr = (float)(nx / 2) * (float)(nx / 2);
+    const int nc = nx / 2 + 1;
+    double s = 0.0;
+    for (int p = threadIdx.x; p < nx * nx; p += blockDim.x) {
+      int i = p % nx, j = p / nx;
+      float t = (float)(j + 1 - nc);
+      float t2 = (float)(i + 1 - nc);
+      float r2 = __fadd_rn(__fmul_rn(t, t), __fmul_rn(t2, t2));
+      if (r2 > rr) s += (double)img[p];
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+      qs_sh = t / klp;
+    }
+    __syncthreads();
+  }
+  const double qs = valid ? qs_sh : 0.0;
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+    int x = q % n, y = q / n;
+    int i = x + nx - ip;
+    if (i >= n) i -= n;
+    int j = y + nx - ip;
+    if (j >= n) j -= n;
+    float v = 0.0f;
+    if (valid && i < nx && j < nx) v = __double2float_rn(__dsub_rn((double)img[(size_t)j * nx + i], qs));
+    out[q] = v;
+  }
+}
+
+// FP32 spectrum -> BF16 spectrum (reduced-precision storage mode)
+__global__ void to_bf16_kernel(const float2* __restrict__ in, __nv_bfloat162* __restrict__ out, size_t count) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count; q += (size_t)gridDim.x * blockDim.x)
+    out[q] = __floats2bfloat162_rn(in[q].x, in[q].y);
+}
+
+template <bool BF16>
+__device__ __forceinline__ float2 load_spec(const void* spec, size_t q) {
+  if (BF16) {
+    __nv_bfloat162 v = static_cast<const __nv_bfloat162*>(spec)[q];
+    return make_float2(__low2float(v), __high2float(v));
+  } else {
+    return static_cast<const float2*>(spec)[q];
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Insert: ONELINE (oneline.f:38-200) for every row J of every slice.
+// One warp per (slice, row); lanes stride over I.  Coordinates, rounding,
+// bounds and table lookups follow the Fortran statement by statement with
+// explicit round-to-nearest intrinsics (no contraction), so each tap's voxel
+// and weight are bit-identical to the CPU restatement; the accumulation is an
+// FP32 vector atomic per tap.
+template <bool BF16>
+__global__ void __launch_bounds__(256) insert_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
+                                                     int nslices, int nx, const float* __restrict__ kbtab, float fltb,
+                                                     float4* __restrict__ g0, float4* __restrict__ g1) {
+  extern __shared__ float tab[];
+  for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
+  __syncthreads();
+
+  const int N = 2 * nx;          // callee N of ONELINE
+  const int N2 = nx;             // callee N2 of ONELINE
+  const int LN2 = 2;
+  const float fN = (float)N;
+  const int lane = threadIdx.x & 31;
+  const int warps_per_block = blockDim.x >> 5;
+  const long long nitems = (long long)nslices * N;
+  const size_t rowlen = (size_t)(nx + 1);
+  const size_t plane = (size_t)N * rowlen;
+
+  for (long long item = (long long)blockIdx.x * warps_per_block + (threadIdx.x >> 5); item < nitems;
+       item += (long long)gridDim.x * warps_per_block) {
+    const int s = (int)(item / N);
+    const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
+    const SliceDesc sd = slices[s];
+    float4* G = sd.grid ? g1 : g0;
+    const int JP = (J >= 0) ? J : N + J;
+    const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
+    const float fJ = (float)J;
+    const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
+    for (int I = lane; I <= N2; I += 32) {
+      if (!((I * I + J * J) < (N * N / 4)) || (I == 0 && J < 0)) continue;
+      const float fI = (float)I;
+      float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
+      float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
+      float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
+      const float2 sp = load_spec<BF16>(spec, specrow + I);
+      // SPIDER forward sign = conjugate of the cuFFT R2C output
+      float br = sp.x, bi = -sp.y;
+      if (xnew < 0.0f) {
+        xnew = -xnew; ynew = -ynew; znew = -znew;
+        bi = -bi;
+      }
+      const int ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
+      const int iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
+      const int izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
+      if (!(ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+            izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1)))
+        continue;
+      float tz[5], ty[5], tx[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        tz[l] = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(znew, (float)(izn + l - 2))), fltb))];
+        ty[l] = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(ynew, (float)(iyn + l - 2))), fltb))];
+        tx[l] = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(xnew, (float)(ixn + l - 2))), fltb))];
+      }
+      if (ixn >= 0) {
+        const int lb = -min(ixn, LN2);
+#pragma unroll
+        for (int lz = 0; lz < 5; ++lz) {
+          if (tz[lz] == 0.0f) continue;
+          const int izp = izn + lz - 2;
+          const int iza = (izp >= 0) ? izp : N + izp;
+#pragma unroll
+          for (int ly = 0; ly < 5; ++ly) {
+            const float tyz = __fmul_rn(ty[ly], tz[lz]);
+            if (tyz == 0.0f) continue;
+            const int iyp = iyn + ly - 2;
+            const int iya = (iyp >= 0) ? iyp : N + iyp;
+            float4* row = G + ((size_t)iza * N + iya) * rowlen;
+#pragma unroll
+            for (int lx = 0; lx < 5; ++lx) {
+              if (lx - 2 < lb) continue;
+              const float wg = __fmul_rn(tx[lx], tyz);
+              if (wg != 0.0f)
+                atomicAdd(row + (ixn + lx - 2), make_float4(__fmul_rn(br, wg), __fmul_rn(bi, wg), wg, 0.0f));
+            }
+          }
+        }
+      }
+      if (ixn < LN2) {  // reflected points (oneline.f:118-150)
+#pragma unroll
+        for (int lz = 0; lz < 5; ++lz) {
+          if (tz[lz] == 0.0f) continue;
+          const int izp = izn + lz - 2;
+          const int izt = (izp > 0) ? N - izp : -izp;
+#pragma unroll
+          for (int ly = 0; ly < 5; ++ly) {
+            const float tyz = __fmul_rn(ty[ly], tz[lz]);
+            if (tyz == 0.0f) continue;
+            const int iyp = iyn + ly - 2;
+            const int iyt = (iyp > 0) ? N - iyp : -iyp;
+            float4* row = G + ((size_t)izt * N + iyt) * rowlen;
+#pragma unroll
+            for (int lx = 0; lx < 2; ++lx) {     // ixp = ixn-2 .. -1
+              const int ixp = ixn + lx - 2;
+              if (ixp > -1) continue;
+              const float wg = __fmul_rn(tx[lx], tyz);
+              if (wg != 0.0f)
+                atomicAdd(row + (-ixp), make_float4(__fmul_rn(br, wg), __fmul_rn(-bi, wg), wg, 0.0f));
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// SYMPLANE0 (bp32f.f:1051-1088) on plane I = 0.  The updated positions of
+// different (IYA, IZA) are disjoint, so every pair runs in its own thread.
+__device__ __forceinline__ float4 conj4(float4 v) { return make_float4(v.x, -v.y, v.z, v.w); }
+__device__ __forceinline__ float4 addconj4(float4 a, float4 b) {  // a + conj(b), W added
+  return make_float4(__fadd_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fadd_rn(a.z, b.z), 0.0f);
+}
+
+__global__ void symplane0_kernel(float4* __restrict__ G, int nx) {
+  const int N = 2 * nx, m = nx - 1;
+  const size_t rowlen = (size_t)(nx + 1);
+  auto at = [&](int a, int b) -> float4& { return G[((size_t)(b - 1) * N + (a - 1)) * rowlen]; };
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < m * m) {
+    int a = 2 + t % m, b = 2 + t / m;
+    int ar = N - a + 2, br = N - b + 2;
+    float4 v1 = addconj4(at(a, b), at(ar, br));
+    at(a, b) = v1;
+    at(ar, br) = conj4(v1);
+    float4 v3 = addconj4(at(ar, b), at(a, br));
+    at(ar, b) = v3;
+    at(a, br) = conj4(v3);
+  } else if (t < m * m + m) {
+    int a = 2 + (t - m * m);
+    float4 v = addconj4(at(a, 1), at(N - a + 2, 1));
+    at(a, 1) = v;
+    at(N - a + 2, 1) = conj4(v);
+  } else if (t < m * m + 2 * m) {
+    int b = 2 + (t - m * m - m);
+    float4 v = addconj4(at(1, b), at(1, N - b + 2));
+    at(1, b) = v;
+    at(1, N - b + 2) = conj4(v);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// NRMW2 (bp3f.f:1347-1371): X*(-1)**(I+J+K)/W where W > 0.1, else 0, with
+// the division in FP64; optional ADDADA of a second grid first
+// (bp32f.f:345-346); output conjugated for SPIDER's inverse sign
+// (fftw3.f:426-437).  The DC imaginary part, which a real inverse transform
+// ignores, is written as zero so the C2R input is exactly Hermitian.
+__global__ void nrmw2_kernel(const float4* __restrict__ g0, const float4* __restrict__ g1, float2* __restrict__ out,
+                             int nx) {
+  const int N = 2 * nx;
+  const size_t h = (size_t)(nx + 1);
+  const size_t nvox = h * N * N;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
+    float4 g = g0[q];
+    if (g1) {
+      float4 o = g1[q];
+      g.x = __fadd_rn(g.x, o.x);
+      g.y = __fadd_rn(g.y, o.y);
+      g.z = __fadd_rn(g.z, o.z);
+    }
+    float2 r = make_float2(0.0f, 0.0f);
+    if (g.z > 0.1f) {
+      int i = (int)(q % h);
+      size_t t = q / h;
+      int j = (int)(t % N), k = (int)(t / N);
+      double s = ((i + j + k) & 1) ? -1.0 : 1.0;
+      double w = (double)g.z;
+      r.x = __double2float_rn(__ddiv_rn(s * (double)g.x, w));
+      r.y = -__double2float_rn(__ddiv_rn(s * (double)g.y, w));
+    }
+    if (q == 0) r.y = 0.0f;
+    out[q] = r;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// WINDKB2A (bp32f.f:945-1045).  The padded inverse transform R[n][n][n] is
+// cropped at offset ip, scaled by 1/n^3 (FFTW3_USEPLAN's SPIDER scale,
+// fftw3.f:443-449), divided by |WKB(LR)|; the mean TNR of the shell
+// (nx/2-1)^2 <= LR <= (nx/2)^2 is subtracted inside the sphere, and the
+// outside is zeroed.  Pass 1 sums the shell in FP64 into acc[0].
+__global__ void windkb_shell_kernel(const float* __restrict__ R, int nx, int ip, float pix,
+                                    const float* __restrict__ wkb, double* __restrict__ acc) {
+  const int N = 2 * nx, c = nx / 2 + 1;
+  const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1);
+  const size_t total = (size_t)nx * nx * nx;
+  double s = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(q % nx);
+    size_t t = q / nx;
+    int j = (int)(t % nx), k = (int)(t / nx);
+    int lr = (k + 1 - c) * (k + 1 - c) + (j + 1 - c) * (j + 1 - c) + (i + 1 - c) * (i + 1 - c);
+    if (lr >= l2p && lr <= l2) {
+      float v = __fmul_rn(R[((size_t)(ip + k) * N + (ip + j)) * N + (ip + i)], pix);
+      v = __fdiv_rn(v, wkb[lr]);
+      s += (double)v;
+    }
+  }
+  __shared__ double red[32];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) atomicAdd(acc, v);
+  }
+}
+
+__global__ void windkb_out_kernel(const float* __restrict__ R, int nx, int ip, float pix,
+                                  const float* __restrict__ wkb, const double* __restrict__ acc, double m,
+                                  float* __restrict__ vol) {
+  const int N = 2 * nx, c = nx / 2 + 1;
+  const int l2 = (nx / 2) * (nx / 2);
+  const size_t total = (size_t)nx * nx * nx;
+  const float tnr = __double2float_rn(acc[0] / m);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(q % nx);
+    size_t t = q / nx;
+    int j = (int)(t % nx), k = (int)(t / nx);
+    int lr = (k + 1 - c) * (k + 1 - c) + (j + 1 - c) * (j + 1 - c) + (i + 1 - c) * (i + 1 - c);
+    float o = 0.0f;
+    if (lr <= l2) {
+      float v = __fmul_rn(R[((size_t)(ip + k) * N + (ip + j)) * N + (ip + i)], pix);
+      v = __fdiv_rn(v, wkb[lr]);
+      o = __fsub_rn(v, tnr);
+    }
+    vol[q] = o;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// BP 3F P / M helpers: float4 grid <-> (X interleaved complex, W)
+__global__ void grid_split_kernel(const float4* __restrict__ G, float2* __restrict__ X, float* __restrict__ W, size_t nvox) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
+    float4 g = G[q];
+    X[q] = make_float2(g.x, g.y);
+    W[q] = g.z;
+  }
+}
+__global__ void grid_add_kernel(float4* __restrict__ G, const float2* __restrict__ X, const float* __restrict__ W, size_t nvox) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
+    float4 g = G[q];
+    float2 x = X[q];
+    g.x = __fadd_rn(g.x, x.x);
+    g.y = __fadd_rn(g.y, x.y);
+    g.z = __fadd_rn(g.z, W[q]);
+    G[q] = g;
+  }
+}
+
+// ============================================================================
+// host side
+
+int check_kernel(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(kCuda, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return 0;
+}
+
+int DevBuf::ensure(size_t want) {
+  if (want <= bytes && p) return 0;
+  release();
+  if (want == 0) return 0;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return fail(kAlloc, "cudaMalloc(%zu bytes) failed: %s", want, cudaGetErrorString(e));
+  }
+  bytes = want;
+  return 0;
+}
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+int HostBuf::ensure(size_t want) {
+  if (want <= bytes && p) return 0;
+  release();
+  if (want == 0) return 0;
+  cudaError_t e = cudaMallocHost(&p, want);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return fail(kAlloc, "cudaMallocHost(%zu bytes) failed: %s", want, cudaGetErrorString(e));
+  }
+  bytes = want;
+  return 0;
+}
+void HostBuf::release() {
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+void bp_release(spi_ctx* c) {
+  for (auto& g : c->grid) g.release();
+  c->imgs.release();
+  c->padded.release();
+  c->spectra.release();
+  c->spec_tmp.release();
+  c->slices.release();
+  c->cplx.release();
+  c->real3.release();
+  c->wkb.release();
+  c->volbuf.release();
+  c->hslices.release();
+  if (c->plan2d) cufftDestroy(c->plan2d);
+  if (c->plan3d) cufftDestroy(c->plan3d);
+  c->plan2d = 0;
+  c->plan3d = 0;
+  c->plan2d_n = c->plan2d_batch = c->plan3d_n = 0;
+  c->nx = c->n = c->ngrids = 0;
+  c->pending_sym0[0] = c->pending_sym0[1] = false;
+  c->merged = false;
+}
+
+static int grid_blocks(const spi_ctx* c, size_t work, int threads) {
+  size_t b = (work + threads - 1) / threads;
+  size_t cap = (size_t)c->sm_count * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static size_t grid_voxels(const spi_ctx* c) { return (size_t)(c->nx + 1) * c->n * c->n; }
+
+static int env_int(const char* name, int dflt) {
+  const char* s = getenv(name);
+  if (!s || !*s) return dflt;
+  return atoi(s);
+}
+
+}  // namespace spi
+
+using namespace spi;
+
+int spi_ctx::phase_begin(int phase) {
+  if (!timing) return -1;
+  cudaEvent_t a, b;
+  if (ev_pool.size() >= 2) {
+    a = ev_pool.back(); ev_pool.pop_back();
+    b = ev_pool.back(); ev_pool.pop_back();
+  } else {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  cudaEventRecord(a, stream);
+  ev_pending.push_back(PhaseEv{a, b, phase});
+  return (int)ev_pending.size() - 1;
+}
+
+void spi_ctx::phase_end(int slot) {
+  if (slot < 0) return;
+  cudaEventRecord(ev_pending[slot].b, stream);
+}
+
+void spi_ctx::phase_collect() {
+  for (auto& e : ev_pending) {
+    float ms = 0.0f;
+    cudaEventSynchronize(e.b);
+    if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+      phase_ms[e.phase] += ms;
+      phase_n[e.phase] += 1;
+    }
+    ev_pool.push_back(e.a);
+    ev_pool.push_back(e.b);
+  }
+  ev_pending.clear();
+}
+
+long long spi_ctx::device_bytes() const {
+  long long t = 0;
+  const DevBuf* bufs[] = {&grid[0], &grid[1], &kbtab, &imgs, &padded, &spectra, &spec_tmp, &slices, &cplx, &real3,
+                          &wkb, &acc, &volbuf, &pj_vol, &pj_out, &pj_runs, &pj_dm};
+  for (auto b : bufs) t += (long long)b->bytes;
+  for (auto& b : cg_buf) t += (long long)b.bytes;
+  return t;
+}
+
+extern "C" {
+
+int spi_version(void) { return 100; }
+
+const char* spi_last_error(void) { return last_error_cstr(); }
+
+int spi_ctx_create(int device, spi_ctx** out) {
+  if (!out) return fail(kInvalid, "spi_ctx_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  SPI_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(kInvalid, "spi_ctx_create: device %d of %d", device, ndev);
+  SPI_CUDA(cudaSetDevice(device));
+  spi_ctx* c = new spi_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sm_count = prop.multiProcessorCount;
+  if (prop.major < 10) {
+    delete c;
+    return fail(kDevice, "spi_ctx_create: device %d is sm_%d%d; this library is built for sm_100a", device,
+                prop.major, prop.minor);
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(kCuda, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  int st = c->acc.ensure(64);
+  if (st) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return st;
+  }
+  *out = c;
+  return 0;
+}
+
+int spi_ctx_destroy(spi_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  bp_release(c);
+  pj_release(c);
+  cg_release(c);
+  c->kbtab.release();
+  c->acc.release();
+  c->hbuf.release();
+  c->phase_collect();
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+long long spi_ctx_launch_count(const spi_ctx* c) { return c ? c->launches : 0; }
+
+void* spi_ctx_stream(const spi_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int spi_ctx_set_timing(spi_ctx* c, int on) {
+  if (!c) return fail(kInvalid, "NULL context");
+  c->phase_collect();
+  c->timing = on != 0;
+  return 0;
+}
+
+int spi_ctx_timing(spi_ctx* c, double* ms_out, long long* count_out) {
+  if (!c) return fail(kInvalid, "NULL context");
+  SPI_CUDA(cudaSetDevice(c->device));
+  c->phase_collect();
+  for (int i = 0; i < 8; ++i) {
+    if (ms_out) ms_out[i] = c->phase_ms[i];
+    if (count_out) count_out[i] = c->phase_n[i];
+    c->phase_ms[i] = 0.0;
+    c->phase_n[i] = 0;
+  }
+  return 0;
+}
+long long spi_ctx_device_bytes(const spi_ctx* c) { return c ? c->device_bytes() : 0; }
+
+int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsym) {
+  if (!c) return fail(kInvalid, "spi_bp_open: NULL context");
+  if (nx < 8 || nx > 512 || (nx & 1)) return fail(kInvalid, "spi_bp_open: nx = %d must be even, 8..512", nx);
+  if (ngrids != 1 && ngrids != 2) return fail(kInvalid, "spi_bp_open: ngrids = %d must be 1 or 2", ngrids);
+  if (nsym > 1 && !sym_angles) return fail(kInvalid, "spi_bp_open: nsym = %d but no symmetry angles", nsym);
+  SPI_CUDA(cudaSetDevice(c->device));
+  bp_release(c);
+  c->nx = nx;
+  c->n = 2 * nx;
+  c->ngrids = ngrids;
+  c->nsym = nsym > 1 ? nsym : 1;
+  c->sym_dm.assign((size_t)9 * c->nsym, 0.0f);
+  if (nsym > 1)
+    for (int s = 0; s < nsym; ++s)  // BUILDS: CANG(phi, theta, psi) per symmetry (builds.f:52)
+      cang(sym_angles[3 * s + 2], sym_angles[3 * s + 1], sym_angles[3 * s + 0], &c->sym_dm[9 * s]);
+  fill_kb(c->n, c->kb);
+  SPI_TRY(c->kbtab.ensure(sizeof(c->kb.tab)));
+  SPI_CUDA(cudaMemcpyAsync(c->kbtab.p, c->kb.tab, sizeof(c->kb.tab), cudaMemcpyHostToDevice, c->stream));
+  const size_t gbytes = grid_voxels(c) * sizeof(float4);
+  for (int g = 0; g < ngrids; ++g) {
+    SPI_TRY(c->grid[g].ensure(gbytes));
+    SPI_CUDA(cudaMemsetAsync(c->grid[g].p, 0, gbytes, c->stream));
+  }
+  // chunk sizes: spectra of one chunk <= ~4.3 GB FP32, FFT sub-batch <= ~256 MB padded
+  const size_t spec_per_img = (size_t)c->n * (nx + 1) * sizeof(float2);
+  int chunk = (int)std::min<size_t>(8192, std::max<size_t>(64, (size_t)4400000000ull / spec_per_img));
+  chunk = env_int("SPI_BP_CHUNK", chunk);
+  int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)268435456ull / ((size_t)c->n * c->n * 4)));
+  c->sub = sub;
+  c->chunk = ((chunk + sub - 1) / sub) * sub;
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_set_spectrum_precision(spi_ctx* c, int bf16) {
+  if (!c) return fail(kInvalid, "NULL context");
+  c->bf16 = bf16 ? 1 : 0;
+  return 0;
+}
+
+static int ensure_chunk_buffers(spi_ctx* c) {
+  const int nx = c->nx, n = c->n;
+  SPI_TRY(c->imgs.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
+  SPI_TRY(c->padded.ensure((size_t)c->sub * n * n * sizeof(float)));
+  const size_t plane = (size_t)n * (nx + 1);
+  if (c->bf16) {
+    SPI_TRY(c->spectra.ensure((size_t)c->chunk * plane * sizeof(__nv_bfloat162)));
+    SPI_TRY(c->spec_tmp.ensure((size_t)c->sub * plane * sizeof(float2)));
+  } else {
+    SPI_TRY(c->spectra.ensure((size_t)c->chunk * plane * sizeof(float2)));
+  }
+  SPI_TRY(c->slices.ensure((size_t)c->chunk * c->nsym * sizeof(SliceDesc)));
+  if (c->plan2d == 0 || c->plan2d_n != n || c->plan2d_batch != c->sub) {
+    if (c->plan2d) cufftDestroy(c->plan2d);
+    c->plan2d = 0;
+    int dims[2] = {n, n};
+    SPI_CUFFT(cufftPlanMany(&c->plan2d, 2, dims, nullptr, 1, n * n, nullptr, 1, n * (n / 2 + 1), CUFFT_R2C, c->sub));
+    SPI_CUFFT(cufftSetStream(c->plan2d, c->stream));
+    c->plan2d_n = n;
+    c->plan2d_batch = c->sub;
+  }
+  return 0;
+}
+
+int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, const uint8_t* half,
+                  int imgs_on_device) {
+  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert: no open reconstruction (spi_bp_open)");
+  if (nimg < 0 || (nimg > 0 && (!imgs || !angles))) return fail(kInvalid, "spi_bp_insert: bad image arguments");
+  if (c->merged) return fail(kInvalid, "spi_bp_insert: images cannot follow spi_bp_partial_add");
+  if (nimg == 0) return 0;
+  SPI_CUDA(cudaSetDevice(c->device));
+  SPI_TRY(ensure_chunk_buffers(c));
+  const int nx = c->nx, n = c->n, nsym = c->nsym;
+  // slice descriptors for the whole call (host, pinned)
+  const size_t nsl = (size_t)nimg * nsym;
+  SPI_TRY(c->hslices.ensure(nsl * sizeof(SliceDesc)));
+  SliceDesc* hs = c->hslices.as<SliceDesc>();
+  for (int a = 0; a < nimg; ++a) {
+    float dm[9];
+    cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);  // BUILDM1 (bp3f.f:1287)
+    int g = (c->ngrids == 2 && half) ? (half[a] ? 0 : 1) : 0;
+    for (int s = 0; s < nsym; ++s) {
+      float dms[9];
+      if (nsym > 1) matmul33(&c->sym_dm[9 * s], dm, dms);
+      else memcpy(dms, dm, sizeof(dms));
+      SliceDesc& d = hs[(size_t)a * nsym + s];
+      memcpy(d.dm, dms, 6 * sizeof(float));
+      d.img = a;  // rebased per chunk below
+      d.grid = g;
+    }
+  }
+  for (int a = 0; a < nimg; ++a)
+    for (int s = 0; s < nsym; ++s) hs[(size_t)a * nsym + s].img = a % c->chunk;
+  int klp_count = 0;
+  {
+    float rr = (float)(nx / 2) * (float)(nx / 2);
+    int nc = nx / 2 + 1;
+    for (int j = 1; j <= nx; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        float t = (float)(j - nc), t2 = (float)(i - nc);
+        if (t * t + t2 * t2 > rr) ++klp_count;
+      }
+  }
+  const double klp = (double)(float)klp_count;
+  const int ip = (n - nx) / 2 + nx % 2;
+  const size_t spec_plane = (size_t)n * (nx + 1);
+  for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
+    const int nb = std::min(c->chunk, nimg - a0);
+    const float* src = imgs + (size_t)a0 * nx * nx;
+    if (!imgs_on_device) {
+      int ev = c->phase_begin(7);
+      SPI_CUDA(cudaMemcpyAsync(c->imgs.p, src, (size_t)nb * nx * nx * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+      c->phase_end(ev);
+      src = c->imgs.as<float>();
+    }
+    for (int b0 = 0; b0 < nb; b0 += c->sub) {
+      const int nvalid = std::min(c->sub, nb - b0);
+      int ev = c->phase_begin(0);
+      stage_kernel<<<c->sub, 256, 0, c->stream>>>(src + (size_t)b0 * nx * nx, nx, n, ip, nvalid, klp,
+                                                 c->padded.as<float>());
+      SPI_TRY(check_kernel("stage_kernel"));
+      c->phase_end(ev);
+      c->count();
+      float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + (size_t)b0 * spec_plane;
+      ev = c->phase_begin(1);
+      SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      c->phase_end(ev);
+      if (c->bf16) {
+        const size_t cnt = (size_t)nvalid * spec_plane;
+        to_bf16_kernel<<<grid_blocks(c, cnt, 256), 256, 0, c->stream>>>(
+            fout, reinterpret_cast<__nv_bfloat162*>(c->spectra.p) + (size_t)b0 * spec_plane, cnt);
+        SPI_TRY(check_kernel("to_bf16_kernel"));
+        c->count();
+      }
+    }
+    const void* spec = c->spectra.p;
+    SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
+                             cudaMemcpyHostToDevice, c->stream));
+    const int nslices = nb * nsym;
+    const size_t smem = 5000 * sizeof(float);
+    int per_sm = 1;
+    if (c->bf16)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, 256, smem);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, 256, smem);
+    const int blocks = c->sm_count * std::max(per_sm, 1);
+    float4* g1 = c->ngrids == 2 ? c->grid[1].as<float4>() : c->grid[0].as<float4>();
+    int ev_ins = c->phase_begin(2);
+    if (c->bf16)
+      insert_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                           c->kbtab.as<float>(), c->kb.fltb, c->grid[0].as<float4>(), g1);
+    else
+      insert_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                            c->kbtab.as<float>(), c->kb.fltb, c->grid[0].as<float4>(), g1);
+    SPI_TRY(check_kernel("insert_kernel"));
+    c->phase_end(ev_ins);
+    c->count();
+  }
+  c->pending_sym0[0] = true;
+  if (c->ngrids == 2) c->pending_sym0[1] = true;
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static int apply_sym0(spi_ctx* c, int g) {
+  if (!c->pending_sym0[g]) return 0;
+  const int m = c->nx - 1;
+  const int work = m * m + 2 * m;
+  int ev = c->phase_begin(3);
+  symplane0_kernel<<<(work + 255) / 256, 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->nx);
+  SPI_TRY(check_kernel("symplane0_kernel"));
+  c->phase_end(ev);
+  c->count();
+  c->pending_sym0[g] = false;
+  return 0;
+}
+
+// NRMW2 + inverse FFT + WINDKB2A of (grid ga [+ grid gb]) into vol (device)
+static int finish_one(spi_ctx* c, int ga, int gb, float* dvol) {
+  const int nx = c->nx, n = c->n;
+  const size_t nvox = grid_voxels(c);
+  SPI_TRY(c->cplx.ensure(nvox * sizeof(float2)));
+  SPI_TRY(c->real3.ensure((size_t)n * n * n * sizeof(float)));
+  if (c->plan3d == 0 || c->plan3d_n != n) {
+    if (c->plan3d) cufftDestroy(c->plan3d);
+    c->plan3d = 0;
+    SPI_CUFFT(cufftPlan3d(&c->plan3d, n, n, n, CUFFT_C2R));
+    SPI_CUFFT(cufftSetStream(c->plan3d, c->stream));
+    c->plan3d_n = n;
+  }
+  int ev = c->phase_begin(4);
+  nrmw2_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(
+      c->grid[ga].as<float4>(), gb >= 0 ? c->grid[gb].as<float4>() : nullptr, c->cplx.as<float2>(), nx);
+  SPI_TRY(check_kernel("nrmw2_kernel"));
+  c->phase_end(ev);
+  c->count();
+  ev = c->phase_begin(5);
+  SPI_CUFFT(cufftExecC2R(c->plan3d, reinterpret_cast<cufftComplex*>(c->cplx.p), c->real3.as<cufftReal>()));
+  c->phase_end(ev);
+  // WINDKB2A
+  std::vector<float> wkb;
+  windkb_table(nx, c->kb, wkb);
+  SPI_TRY(c->wkb.ensure(wkb.size() * sizeof(float)));
+  SPI_CUDA(cudaMemcpyAsync(c->wkb.p, wkb.data(), wkb.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1), cc = nx / 2 + 1;
+  long m = 0;
+  for (int k = 1; k <= nx; ++k)
+    for (int j = 1; j <= nx; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        int lr = (k - cc) * (k - cc) + (j - cc) * (j - cc) + (i - cc) * (i - cc);
+        if (lr >= l2p && lr <= l2) ++m;
+      }
+  const int ip = (n - nx) / 2 + nx % 2;
+  const float pix = 1.0f / (float)((long long)n * n * n);
+  const size_t total = (size_t)nx * nx * nx;
+  ev = c->phase_begin(6);
+  SPI_CUDA(cudaMemsetAsync(c->acc.p, 0, sizeof(double), c->stream));
+  windkb_shell_kernel<<<grid_blocks(c, total, 256), 256, 0, c->stream>>>(c->real3.as<float>(), nx, ip, pix,
+                                                                         c->wkb.as<float>(), c->acc.as<double>());
+  SPI_TRY(check_kernel("windkb_shell_kernel"));
+  windkb_out_kernel<<<grid_blocks(c, total, 256), 256, 0, c->stream>>>(c->real3.as<float>(), nx, ip, pix,
+                                                                       c->wkb.as<float>(), c->acc.as<double>(),
+                                                                       (double)(float)m, dvol);
+  SPI_TRY(check_kernel("windkb_out_kernel"));
+  c->phase_end(ev);
+  c->count(2);
+  // the wkb host vector must outlive the async copy
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_finish(spi_ctx* c, float* vol_all, float* vol_1, float* vol_2, int out_on_device) {
+  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_finish: no open reconstruction");
+  SPI_CUDA(cudaSetDevice(c->device));
+  for (int g = 0; g < c->ngrids; ++g) SPI_TRY(apply_sym0(c, g));
+  const size_t vbytes = (size_t)c->nx * c->nx * c->nx * sizeof(float);
+  struct Job { float* out; int ga, gb; } jobs[3];
+  int nj = 0;
+  if (c->ngrids == 1) {
+    if (vol_all) jobs[nj++] = {vol_all, 0, -1};
+  } else {
+    if (vol_1) jobs[nj++] = {vol_1, 0, -1};
+    if (vol_all) jobs[nj++] = {vol_all, 0, 1};
+    if (vol_2) jobs[nj++] = {vol_2, 1, -1};
+  }
+  for (int t = 0; t < nj; ++t) {
+    float* dst = jobs[t].out;
+    if (!out_on_device) {
+      SPI_TRY(c->volbuf.ensure(vbytes));
+      dst = c->volbuf.as<float>();
+    }
+    SPI_TRY(finish_one(c, jobs[t].ga, jobs[t].gb, dst));
+    if (!out_on_device) SPI_CUDA(cudaMemcpy(jobs[t].out, dst, vbytes, cudaMemcpyDeviceToHost));
+  }
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_partial_out(spi_ctx* c, int g, float* x_out, float* w_out) {
+  if (!c || c->ngrids == 0 || g < 0 || g >= c->ngrids) return fail(kInvalid, "spi_bp_partial_out: bad grid");
+  SPI_CUDA(cudaSetDevice(c->device));
+  SPI_TRY(apply_sym0(c, g));
+  const size_t nvox = grid_voxels(c);
+  SPI_TRY(c->cplx.ensure(nvox * sizeof(float2)));
+  SPI_TRY(c->real3.ensure(std::max(nvox * sizeof(float), (size_t)c->n * c->n * c->n * sizeof(float))));
+  grid_split_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->cplx.as<float2>(),
+                                                                      c->real3.as<float>(), nvox);
+  SPI_TRY(check_kernel("grid_split_kernel"));
+  c->count();
+  if (x_out) SPI_CUDA(cudaMemcpyAsync(x_out, c->cplx.p, nvox * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+  if (w_out) SPI_CUDA(cudaMemcpyAsync(w_out, c->real3.p, nvox * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_partial_add(spi_ctx* c, int g, const float* x_in, const float* w_in) {
+  if (!c || c->ngrids == 0 || g < 0 || g >= c->ngrids) return fail(kInvalid, "spi_bp_partial_add: bad grid");
+  if (!x_in || !w_in) return fail(kInvalid, "spi_bp_partial_add: NULL partial");
+  SPI_CUDA(cudaSetDevice(c->device));
+  SPI_TRY(apply_sym0(c, g));  // inserted images are symmetrised before the merge
+  const size_t nvox = grid_voxels(c);
+  SPI_TRY(c->cplx.ensure(nvox * sizeof(float2)));
+  SPI_TRY(c->real3.ensure(std::max(nvox * sizeof(float), (size_t)c->n * c->n * c->n * sizeof(float))));
+  SPI_CUDA(cudaMemcpyAsync(c->cplx.p, x_in, nvox * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(c->real3.p, w_in, nvox * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  grid_add_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->cplx.as<float2>(),
+                                                                    c->real3.as<float>(), nvox);
+  SPI_TRY(check_kernel("grid_add_kernel"));
+  c->count();
+  c->merged = true;
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_close(spi_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  bp_release(c);
+  return 0;
+}
+
+int spi_bp3f(spi_ctx* c, const float* imgs, int nx, int nang, const float* angles, const float* sym_angles,
+             int nsym, float* vol_out) {
+  SPI_TRY(spi_bp_open(c, nx, 1, sym_angles, nsym));
+  SPI_TRY(spi_bp_insert(c, imgs, nang, angles, nullptr, 0));
+  SPI_TRY(spi_bp_finish(c, vol_out, nullptr, nullptr, 0));
+  return spi_bp_close(c);
+}
+
+int spi_bp32f(spi_ctx* c, const float* imgs, int nx, int nang, const float* angles, const float* sym_angles,
+              int nsym, const uint8_t* half, float* vol_all, float* vol_1, float* vol_2) {
+  if (!half) return fail(kInvalid, "spi_bp32f: half-set mask is required");
+  SPI_TRY(spi_bp_open(c, nx, 2, sym_angles, nsym));
+  SPI_TRY(spi_bp_insert(c, imgs, nang, angles, half, 0));
+  SPI_TRY(spi_bp_finish(c, vol_all, vol_1, vol_2, 0));
+  return spi_bp_close(c);
+}
+
+}  // extern "C"

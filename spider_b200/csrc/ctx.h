@@ -1,0 +1,65 @@
+// Context object behind the opaque spi_ctx handle.
+#pragma once
+
+#include "common.h"
+
+struct spi_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+
+  // ---- Fourier gridding back-projection state ----
+  int nx = 0, n = 0, ngrids = 0, nsym = 1;
+  std::vector<float> sym_dm;          // 9 * nsym (column-major 3x3 each)
+  bool pending_sym0[2] = {false, false};
+  bool merged = false;
+  int bf16 = 0;
+  int chunk = 0;                      // images per persistent insert launch
+  int sub = 0;                        // images per batched 2D FFT
+  spi::KBTab kb;
+  spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
+  spi::DevBuf kbtab;                  // float[5000]
+  spi::DevBuf imgs;                   // float [chunk][nx][nx]
+  spi::DevBuf padded;                 // float [sub][n][n]
+  spi::DevBuf spectra;                // float2 or bf16x2 [chunk][n][nx+1]
+  spi::DevBuf spec_tmp;               // float2 [sub][n][nx+1] (BF16 mode FFT output)
+  spi::DevBuf slices;                 // SliceDesc [chunk * nsym]
+  spi::DevBuf cplx;                   // float2 [n][n][nx+1] (inverse FFT input)
+  spi::DevBuf real3;                  // float [n][n][n]
+  spi::DevBuf wkb;                    // float[(nx/2)^2 + 1]
+  spi::DevBuf acc;                    // double[8] reduction scratch
+  spi::DevBuf volbuf;                 // float [nx^3] (finish output staging)
+  spi::HostBuf hslices;
+  cufftHandle plan2d = 0;
+  int plan2d_n = 0, plan2d_batch = 0;
+  cufftHandle plan3d = 0;
+  int plan3d_n = 0;
+
+  // ---- PJ 3Q / BP CG scratch ----
+  spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
+  spi::DevBuf cg_buf[8];
+  spi::HostBuf hbuf;
+
+  // per-phase event timing
+  bool timing = false;
+  struct PhaseEv { cudaEvent_t a, b; int phase; };
+  std::vector<PhaseEv> ev_pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double phase_ms[8] = {0};
+  long long phase_n[8] = {0};
+  int phase_begin(int phase);   // returns slot or -1
+  void phase_end(int slot);
+  void phase_collect();         // synchronises on recorded events
+
+  long long device_bytes() const;
+  int count(int k = 1) { launches += k; return 0; }
+};
+
+namespace spi {
+// Release every cuFFT plan and device buffer of the reconstruction state.
+void bp_release(spi_ctx* c);
+void pj_release(spi_ctx* c);
+void cg_release(spi_ctx* c);
+int check_kernel(const char* what);
+}  // namespace spi

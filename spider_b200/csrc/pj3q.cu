@@ -1,0 +1,245 @@
+// PJ 3Q: real-space trilinear projection (WPRO_N, wpro_n.f:44-150) and its
+// exact adjoint (trilinear insertion), on sm_100a.
+//
+// PREPCUB (prepcub.f:54-109) turns the sphere of radius RI into runs of
+// voxels along x.  WPRO_N walks each run accumulating the sample position
+// with XB = XB + DM(1) (sequential float additions), so one thread owns one
+// (projection, run) pair and walks it in the same order: every sample
+// position and every trilinear weight is bit-identical to the CPU form.
+// Runs are ordered (z, y); consecutive threads of a warp hold consecutive y
+// and therefore write different output rows K = y + LDPY.
+#include <cmath>
+#include <cstring>
+
+#include "../../include/spider_b200.h"
+#include "ctx.h"
+
+namespace spi {
+
+struct PjRun {
+  int i1, i2;     // first/last x (1-based) of the run
+  int x, y, z;    // centred coordinates of the first voxel
+};
+
+struct PjDM {
+  float d[9];
+};
+
+static void prepcub(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<PjRun>& runs) {
+  const float r = ri * ri;
+  runs.clear();
+  for (int i1 = 1; i1 <= nslice; ++i1) {
+    float t = (float)(i1 - ldpz);
+    float xx = t * t;
+    for (int i2 = 1; i2 <= nrow; ++i2) {
+      float t2 = (float)(i2 - ldpy);
+      float yy = t2 * t2 + xx;
+      bool first = true;
+      for (int i3 = 1; i3 <= nsam; ++i3) {
+        float t3 = (float)(i3 - ldpx);
+        float rc = t3 * t3 + yy;
+        if (first) {
+          if (rc > r) continue;
+          first = false;
+          runs.push_back(PjRun{i3, i3, i3 - ldpx, i2 - ldpy, i1 - ldpz});
+        } else if (rc <= r) {
+          runs.back().i2 = i3;
+        }
+      }
+    }
+  }
+}
+
+// Start position of a run: IPCUBE(3)*DM(1) + IPCUBE(4)*DM(4) + IPCUBE(5)*DM(7) + LDPX
+__device__ __forceinline__ float run_start(const PjRun& r, float a, float b, float c, int ldp) {
+  return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn((float)r.x, a), __fmul_rn((float)r.y, b)), __fmul_rn((float)r.z, c)),
+                   (float)ldp);
+}
+
+__global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cube, int nsam, int nrow, int nslice,
+                                                   const PjRun* __restrict__ runs, int nruns,
+                                                   const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
+                                                   int ldpz, float* __restrict__ out) {
+  const long long total = (long long)nruns * nang;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nruns);
+    const PjRun r = runs[t % nruns];
+    const PjDM dm = dms[a];
+    float* b = out + (size_t)a * nsam * nrow;
+    const int k = r.y + ldpy;
+    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
+    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
+    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+    for (int j = r.i1; j <= r.i2; ++j) {
+      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
+        const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
+        const float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
+        const float c000 = __ldg(c0), c100 = __ldg(c0 + 1), c010 = __ldg(c0 + sy), c110 = __ldg(c0 + sy + 1);
+        const float c001 = __ldg(c0 + sz), c101 = __ldg(c0 + sz + 1), c011 = __ldg(c0 + sz + sy),
+                    c111 = __ldg(c0 + sz + sy + 1);
+        // A1..A8 exactly as wpro_n.f:103-114
+        const float a1 = c000;
+        const float a2 = __fsub_rn(c100, a1);
+        const float a3 = __fsub_rn(c010, a1);
+        const float a4 = __fsub_rn(c001, a1);
+        const float a5 = __fadd_rn(__fsub_rn(-a2, c010), c110);
+        const float a61 = __fadd_rn(-c001, c101);
+        const float a6 = __fadd_rn(-a2, a61);
+        const float a7 = __fadd_rn(__fsub_rn(-a3, c001), c011);
+        const float a8 = __fadd_rn(__fsub_rn(__fsub_rn(-a5, a61), c011), c111);
+        // A1 + DZ*(A4 + A6*DX + (A7 + A8*DX)*DY) + A3*DY + DX*(A2 + A5*DY)
+        const float inner = __fadd_rn(__fadd_rn(a4, __fmul_rn(a6, dx)), __fmul_rn(__fadd_rn(a7, __fmul_rn(a8, dx)), dy));
+        float v = __fadd_rn(a1, __fmul_rn(dz, inner));
+        v = __fadd_rn(v, __fmul_rn(a3, dy));
+        v = __fadd_rn(v, __fmul_rn(dx, __fadd_rn(a2, __fmul_rn(a5, dy))));
+        atomicAdd(b + (size_t)(k - 1) * nsam + (j - 1), v);
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[1]);
+      zb = __fadd_rn(zb, dm.d[2]);
+    }
+  }
+}
+
+// Transpose of wpro_kernel: every sample spreads its projection value into
+// the 8 neighbouring voxels with the trilinear weights of the same position.
+__global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restrict__ proj, int nsam, int nrow, int nslice,
+                                                           const PjRun* __restrict__ runs, int nruns,
+                                                           const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
+                                                           int ldpz, float* __restrict__ cube) {
+  const long long total = (long long)nruns * nang;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nruns);
+    const PjRun r = runs[t % nruns];
+    const PjDM dm = dms[a];
+    const float* b = proj + (size_t)a * nsam * nrow;
+    const int k = r.y + ldpy;
+    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
+    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
+    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+    for (int j = r.i1; j <= r.i2; ++j) {
+      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
+        const float p = __ldg(b + (size_t)(k - 1) * nsam + (j - 1));
+        if (p != 0.0f) {
+          const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
+          const float ex = 1.0f - dx, ey = 1.0f - dy, ez = 1.0f - dz;
+          float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
+          atomicAdd(c0, p * ex * ey * ez);
+          atomicAdd(c0 + 1, p * dx * ey * ez);
+          atomicAdd(c0 + sy, p * ex * dy * ez);
+          atomicAdd(c0 + sy + 1, p * dx * dy * ez);
+          atomicAdd(c0 + sz, p * ex * ey * dz);
+          atomicAdd(c0 + sz + 1, p * dx * ey * dz);
+          atomicAdd(c0 + sz + sy, p * ex * dy * dz);
+          atomicAdd(c0 + sz + sy + 1, p * dx * dy * dz);
+        }
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[1]);
+      zb = __fadd_rn(zb, dm.d[2]);
+    }
+  }
+}
+
+void pj_release(spi_ctx* c) {
+  c->pj_vol.release();
+  c->pj_out.release();
+  c->pj_runs.release();
+  c->pj_dm.release();
+}
+
+static int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang,
+                     int* nruns_out) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (nx < 4 || ny < 4 || nz < 4) return fail(kInvalid, "PJ 3Q: volume %dx%dx%d too small", nx, ny, nz);
+  if (nang < 0 || (nang > 0 && !angles)) return fail(kInvalid, "PJ 3Q: bad angle list");
+  if (!(ri > 0.0f)) return fail(kInvalid, "PJ 3Q: radius %g must be positive", (double)ri);
+  SPI_CUDA(cudaSetDevice(c->device));
+  const int ldpx = nx / 2 + 1, ldpy = ny / 2 + 1, ldpz = nz / 2 + 1;
+  std::vector<PjRun> runs;
+  prepcub(nx, ny, nz, ri, ldpx, ldpy, ldpz, runs);
+  std::vector<PjDM> dms((size_t)std::max(nang, 1));
+  for (int a = 0; a < nang; ++a)  // WPRO_N(PHI=reg3, THETA=reg2, PSI=reg1), writpro_n.f:214-216
+    cang_pj(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dms[a].d);
+  SPI_TRY(c->pj_runs.ensure(std::max<size_t>(1, runs.size()) * sizeof(PjRun)));
+  SPI_TRY(c->pj_dm.ensure(dms.size() * sizeof(PjDM)));
+  if (!runs.empty())
+    SPI_CUDA(cudaMemcpy(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice));
+  SPI_CUDA(cudaMemcpy(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice));
+  *nruns_out = (int)runs.size();
+  return 0;
+}
+
+}  // namespace spi
+
+using namespace spi;
+
+extern "C" {
+
+int spi_pj3q(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
+             float* proj_out, int on_device) {
+  int nruns = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));
+  if (!vol || !proj_out) return fail(kInvalid, "PJ 3Q: NULL buffer");
+  const size_t vbytes = (size_t)nx * ny * nz * sizeof(float);
+  const size_t pbytes = (size_t)nang * nx * ny * sizeof(float);
+  const float* dvol = vol;
+  float* dout = proj_out;
+  if (!on_device) {
+    SPI_TRY(c->pj_vol.ensure(vbytes));
+    SPI_TRY(c->pj_out.ensure(std::max<size_t>(pbytes, 4)));
+    SPI_CUDA(cudaMemcpyAsync(c->pj_vol.p, vol, vbytes, cudaMemcpyHostToDevice, c->stream));
+    dvol = c->pj_vol.as<float>();
+    dout = c->pj_out.as<float>();
+  }
+  if (nang == 0) return 0;
+  SPI_CUDA(cudaMemsetAsync(dout, 0, pbytes, c->stream));
+  const long long total = (long long)nruns * nang;
+  int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
+  if (blocks > 0) {
+    wpro_kernel<<<blocks, 128, 0, c->stream>>>(dvol, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns, c->pj_dm.as<PjDM>(),
+                                               nang, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1, dout);
+    SPI_TRY(check_kernel("wpro_kernel"));
+    c->count();
+  }
+  if (!on_device) SPI_CUDA(cudaMemcpyAsync(proj_out, dout, pbytes, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_pj3q_adjoint(spi_ctx* c, const float* projs, int nx, int ny, int nz, float ri, const float* angles,
+                     int nang, float* vol_out, int on_device) {
+  int nruns = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));
+  if (!projs || !vol_out) return fail(kInvalid, "PJ 3Q adjoint: NULL buffer");
+  const size_t vbytes = (size_t)nx * ny * nz * sizeof(float);
+  const size_t pbytes = (size_t)nang * nx * ny * sizeof(float);
+  const float* dp = projs;
+  float* dvol = vol_out;
+  if (!on_device) {
+    SPI_TRY(c->pj_vol.ensure(vbytes));
+    SPI_TRY(c->pj_out.ensure(std::max<size_t>(pbytes, 4)));
+    if (pbytes) SPI_CUDA(cudaMemcpyAsync(c->pj_out.p, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
+    dp = c->pj_out.as<float>();
+    dvol = c->pj_vol.as<float>();
+  }
+  SPI_CUDA(cudaMemsetAsync(dvol, 0, vbytes, c->stream));
+  const long long total = (long long)nruns * nang;
+  int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
+  if (blocks > 0) {
+    wpro_adjoint_kernel<<<blocks, 128, 0, c->stream>>>(dp, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
+                                                       c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1,
+                                                       dvol);
+    SPI_TRY(check_kernel("wpro_adjoint_kernel"));
+    c->count();
+  }
+  if (!on_device) SPI_CUDA(cudaMemcpyAsync(vol_out, dvol, vbytes, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,313 @@
+"""Host-side mirror of SPIDER's reconstruction operations on the CUDA library.
+
+Each function carries the name of the SPIDER operation it replaces and takes
+the values that operation prompts for, in the same order and meaning:
+
+=================  ==================================================  =========================
+function           SPIDER operation (dispatch in vtil2.f)              reference subroutine
+=================  ==================================================  =========================
+``bp3f``           ``BP 3F``        (vtil2.f:301-313)                  BP3F, bp3f.f:79
+``bp3f_partial``   ``BP 3F P``      partial Fourier volume + weights   BP3F(HALT), bp3f.f:191-248
+``bp3f_merge``     ``BP 3F M``      merge partial volumes              BP3F_MERGE, bp3f.f:531
+``bp32f``          ``BP 32F``       (vtil2.f:316-322)                  BP32F, bp32f.f:57
+``pj3q``           ``PJ 3Q``        (vtil2.f:218-220)                  PJ3Q_N, pj3q_n.f:41
+``bpcg``           ``BP CG``        (vtil2.f:324)                      BPCG, bpcg.f:70
+=================  ==================================================  =========================
+
+Arrays are numpy (host) or torch CUDA tensors (device, no host copy).  Images
+are ``[nimg, nx, nx]`` float32 (x fastest), volumes ``[nz, ny, nx]``, angles
+``[nimg, 3]`` = (psi, theta, phi) in degrees (angle-document registers 1-3).
+Errors raise :class:`spider_b200._lib.SpiderError` carrying the IRTFLG-style
+code (101 invalid argument, 102 missing data / radius too large, 46 memory).
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import SpiderError, check
+
+try:  # torch is plumbing for device memory; optional for host use
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+__all__ = ["Context", "default_context", "bp3f", "bp32f", "bp3f_partial", "bp3f_merge", "pj3q",
+           "pj3q_adjoint", "bpcg", "cg_project", "cg_backproject", "SpiderError"]
+
+
+def _is_dev(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_dev(a):
+        if a.dtype != torch.float32 and a.dtype != torch.uint8:
+            raise SpiderError(101, f"device tensor dtype {a.dtype} (float32 expected)")
+        if not a.is_contiguous():
+            raise SpiderError(101, "device tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _host_f32(a):
+    if torch is not None and isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Context:
+    """One CUDA device + stream + reusable buffers (an ``spi_ctx``)."""
+
+    def __init__(self, device: int = 0):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        check(L.spi_ctx_create(device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+        self._L = L
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            self._L.spi_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(self._L.spi_ctx_launch_count(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.spi_ctx_device_bytes(self._h))
+
+    # -------- streaming back-projection (BP 3F / BP 32F) --------
+    def bp_open(self, nx: int, ngrids: int = 1, sym=None, bf16: bool = False):
+        sym_a = None if sym is None else _host_f32(sym)
+        nsym = 0 if sym_a is None else sym_a.shape[0]
+        check(self._L.spi_bp_open(self._h, nx, ngrids, _ptr(sym_a), nsym))
+        check(self._L.spi_bp_set_spectrum_precision(self._h, 1 if bf16 else 0))
+        self._nx = nx
+        self._ngrids = ngrids
+
+    def bp_insert(self, imgs, angles, half=None):
+        ang = _host_f32(angles)
+        h = None if half is None else np.ascontiguousarray(
+            half.detach().cpu().numpy() if (torch is not None and isinstance(half, torch.Tensor)) else half,
+            dtype=np.uint8)
+        dev = _is_dev(imgs)
+        if not dev:
+            imgs = _host_f32(imgs)
+        n = int(imgs.shape[0])
+        if ang.shape[0] != n:
+            raise SpiderError(101, f"{n} images but {ang.shape[0]} angle triples")
+        check(self._L.spi_bp_insert(self._h, _ptr(imgs), n, _ptr(ang), _ptr(h), 1 if dev else 0))
+
+    def bp_finish(self, want=("all",), device: bool = False):
+        nx = self._nx
+        outs = {}
+        for k in want:
+            if device:
+                outs[k] = torch.empty((nx, nx, nx), dtype=torch.float32, device=f"cuda:{self.device}")
+            else:
+                outs[k] = np.zeros((nx, nx, nx), np.float32)
+        check(self._L.spi_bp_finish(self._h, _ptr(outs.get("all")), _ptr(outs.get("1")), _ptr(outs.get("2")),
+                                    1 if device else 0))
+        return outs
+
+    def bp_partial_out(self, g: int = 0):
+        nx = self._nx
+        n = 2 * nx
+        x = np.zeros((n, n, nx + 1, 2), np.float32)
+        w = np.zeros((n, n, nx + 1), np.float32)
+        check(self._L.spi_bp_partial_out(self._h, g, _ptr(x), _ptr(w)))
+        return x, w
+
+    def bp_partial_add(self, x, w, g: int = 0):
+        x = _host_f32(x)
+        w = _host_f32(w)
+        check(self._L.spi_bp_partial_add(self._h, g, _ptr(x), _ptr(w)))
+
+    def bp_close(self):
+        check(self._L.spi_bp_close(self._h))
+
+
+_tls = threading.local()
+
+
+def default_context(device: int = 0) -> Context:
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    if device not in ctxs:
+        ctxs[device] = Context(device)
+    return ctxs[device]
+
+
+def _nx_of(imgs) -> int:
+    if imgs.ndim != 3 or imgs.shape[1] != imgs.shape[2]:
+        raise SpiderError(101, "ONLY WORKS ON SQUARE IMAGES")  # bp3f.f:135-138
+    return int(imgs.shape[1])
+
+
+def bp3f(imgs, angles, sym=None, *, ctx: Context | None = None, device_out: bool = False):
+    """``BP 3F``: Fourier gridding back-projection -> volume [nx, nx, nx]."""
+    ctx = ctx or default_context()
+    nx = _nx_of(imgs)
+    ctx.bp_open(nx, 1, sym)
+    try:
+        ctx.bp_insert(imgs, angles)
+        return ctx.bp_finish(("all",), device=device_out)["all"]
+    finally:
+        ctx.bp_close()
+
+
+def bp32f(imgs, angles, half, sym=None, *, ctx: Context | None = None, bf16: bool = False,
+          device_out: bool = False):
+    """``BP 32F``: returns (reconstructed volume, first sample volume, second sample volume)."""
+    ctx = ctx or default_context()
+    nx = _nx_of(imgs)
+    ctx.bp_open(nx, 2, sym, bf16=bf16)
+    try:
+        ctx.bp_insert(imgs, angles, half)
+        o = ctx.bp_finish(("all", "1", "2"), device=device_out)
+        return o["all"], o["1"], o["2"]
+    finally:
+        ctx.bp_close()
+
+
+def bp3f_partial(imgs, angles, sym=None, *, ctx: Context | None = None):
+    """``BP 3F P``: returns (X [2nx, 2nx, nx+1, 2] re/im, W [2nx, 2nx, nx+1]) after plane-0 symmetry."""
+    ctx = ctx or default_context()
+    nx = _nx_of(imgs)
+    ctx.bp_open(nx, 1, sym)
+    try:
+        ctx.bp_insert(imgs, angles)
+        return ctx.bp_partial_out(0)
+    finally:
+        ctx.bp_close()
+
+
+def bp3f_merge(partials, *, ctx: Context | None = None):
+    """``BP 3F M``: sum partial (X, W) pairs and finish -> volume [nx, nx, nx]."""
+    ctx = ctx or default_context()
+    partials = list(partials)
+    if not partials:
+        raise SpiderError(101, "no partial volumes")
+    nx = int(partials[0][1].shape[2]) - 1
+    ctx.bp_open(nx, 1)
+    try:
+        for x, w in partials:
+            ctx.bp_partial_add(x, w)
+        return ctx.bp_finish(("all",))["all"]
+    finally:
+        ctx.bp_close()
+
+
+def _vol_shape(vol):
+    if vol.ndim != 3:
+        raise SpiderError(101, "volume must be 3-D")
+    return int(vol.shape[2]), int(vol.shape[1]), int(vol.shape[0])
+
+
+def pj3q(vol, angles, ri=None, *, ctx: Context | None = None):
+    """``PJ 3Q``: trilinear projections [nang, ny, nx] of vol [nz, ny, nx]."""
+    ctx = ctx or default_context()
+    nx, ny, nz = _vol_shape(vol)
+    if ri is None:
+        ri = float(min(nx, ny, nz) // 2 - 2)  # pj3q_n.f:82
+    ang = _host_f32(angles)
+    nang = ang.shape[0]
+    dev = _is_dev(vol)
+    if dev:
+        out = torch.empty((nang, ny, nx), dtype=torch.float32, device=vol.device)
+    else:
+        vol = _host_f32(vol)
+        out = np.zeros((nang, ny, nx), np.float32)
+    check(ctx._L.spi_pj3q(ctx.handle, _ptr(vol), nx, ny, nz, float(ri), _ptr(ang), nang, _ptr(out), 1 if dev else 0))
+    return out
+
+
+def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
+    """Exact adjoint of :func:`pj3q`: volume [nz, ny, nx] from projections [nang, ny, nx]."""
+    ctx = ctx or default_context()
+    nz, ny, nx = shape
+    if ri is None:
+        ri = float(min(nx, ny, nz) // 2 - 2)
+    ang = _host_f32(angles)
+    nang = ang.shape[0]
+    dev = _is_dev(projs)
+    if dev:
+        out = torch.empty((nz, ny, nx), dtype=torch.float32, device=projs.device)
+    else:
+        projs = _host_f32(projs)
+        out = np.zeros((nz, ny, nx), np.float32)
+    check(ctx._L.spi_pj3q_adjoint(ctx.handle, _ptr(projs), nx, ny, nz, float(ri), _ptr(ang), nang, _ptr(out),
+                                  1 if dev else 0))
+    return out
+
+
+def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
+         ctx: Context | None = None):
+    """``BP CG`` (linear interpolation).  Prompts in reference order: radius
+    (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
+    Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
+    ctx = ctx or default_context()
+    projs = _host_f32(projs)
+    n = _nx_of(projs)
+    if ri is None:
+        ri = float(n // 2 - 2)  # bpcg.f:161
+    ang = _host_f32(angles)
+    vol = np.zeros((n, n, n), np.float32)
+    logv = np.zeros((max(maxit, 1), 3), np.float32)
+    niter = ctypes.c_int(0)
+    check(ctx._L.spi_bpcg(ctx.handle, _ptr(projs), n, projs.shape[0], _ptr(ang), float(ri), float(errm),
+                          float(chim), int(maxit), int(mode), float(lam), _ptr(vol), _ptr(logv),
+                          ctypes.cast(ctypes.byref(niter), ctypes.c_void_p)))
+    return vol, logv[: niter.value].copy()
+
+
+def cg_project(vol, angles, ri, *, ctx: Context | None = None):
+    """PRJCQ_N (the BP CG projector A) of vol [n,n,n] -> [nang, n, n]."""
+    ctx = ctx or default_context()
+    ang = _host_f32(angles)
+    n = int(vol.shape[0])
+    dev = _is_dev(vol)
+    if dev:
+        out = torch.empty((ang.shape[0], n, n), dtype=torch.float32, device=vol.device)
+    else:
+        vol = _host_f32(vol)
+        out = np.zeros((ang.shape[0], n, n), np.float32)
+    check(ctx._L.spi_cg_project(ctx.handle, _ptr(vol), n, float(ri), _ptr(ang), ang.shape[0], _ptr(out),
+                                1 if dev else 0))
+    return out
+
+
+def cg_backproject(projs, angles, ri, *, ctx: Context | None = None):
+    """BCKPJ_LIN (the BP CG back-projector A^T) of [nang, n, n] -> [n, n, n]."""
+    ctx = ctx or default_context()
+    ang = _host_f32(angles)
+    n = int(projs.shape[1])
+    dev = _is_dev(projs)
+    if dev:
+        out = torch.empty((n, n, n), dtype=torch.float32, device=projs.device)
+    else:
+        projs = _host_f32(projs)
+        out = np.zeros((n, n, n), np.float32)
+    check(ctx._L.spi_cg_backproject(ctx.handle, _ptr(projs), n, float(ri), _ptr(ang), ang.shape[0], _ptr(out),
+                                    1 if dev else 0))
+    return out
