@@ -1,18 +1,738 @@
-// BP CG (linear interpolation) -- kernels land in the next revision.
+// BP CG, linear interpolation (BPCG bpcg.f:70 -> BPCG_2 bpcg.f:425-814 ->
+// HIANG hiang.f:40-112 -> BPCG_3_LIN bpcg.f:818-1238) on sm_100a.
+//
+// Operators (voxel runs from PREPCUB_S, prepcub_s.f:54-111):
+//   A   = PRJCQ_N (prjcq.f:48-82): every sphere voxel splats bilinearly into
+//         the projection.  One CTA per projection keeps the image in shared
+//         memory (n <= 224) and walks whole runs with the reference's
+//         sequential XB = XB + DM(1) accumulation, so sample positions are
+//         bit-identical; shared-memory atomics accumulate.
+//   A^T = BCKPJ_LIN (bckpj.f:59-94, SP_MP branch): every sphere voxel
+//         gathers from each projection through the PROJT difference table
+//         (bpcg.f:732-742), computed on the fly from four pixels with the
+//         same float operations.  One thread per voxel sums the projections
+//         in image order, the order of the reference's image loop, so the
+//         back-projection is bit-identical to the CPU form.
+// CG scalars (DELSQ, AKDEN, P, Q) are FP64 device scalars; vectors are FP32.
+// One CG iteration is a fixed kernel sequence captured once as a CUDA graph.
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+
 #include "../../include/spider_b200.h"
 #include "ctx.h"
+
 namespace spi {
-void cg_release(spi_ctx* c) { for (auto& b : c->cg_buf) b.release(); }
+
+struct CgRun {
+  int l1, l2;   // first/last 1-based linear index of the run
+  int x, y, z;  // 1-based coordinates of the first voxel
+};
+
+struct CgDM {
+  float d[6];
+};
+
+static void prepcub_s(int n, float ri, int ldp, std::vector<CgRun>& runs) {
+  const float r = ri * ri;
+  int nmat = 0;
+  runs.clear();
+  for (int i1 = 1; i1 <= n; ++i1) {
+    float t = (float)(i1 - ldp);
+    float xx = t * t;
+    for (int i2 = 1; i2 <= n; ++i2) {
+      float t2 = (float)(i2 - ldp);
+      float yy = t2 * t2 + xx;
+      bool first = true;
+      for (int i3 = 1; i3 <= n; ++i3) {
+        ++nmat;
+        float t3 = (float)(i3 - ldp);
+        float rc = t3 * t3 + yy;
+        if (first) {
+          if (rc > r) continue;
+          first = false;
+          runs.push_back(CgRun{nmat, nmat, i3, i2, i1});
+        } else if (rc <= r) {
+          runs.back().l2 = nmat;
+        }
+      }
+    }
+  }
 }
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void block_add_d(double v, double* dst) {
+  __shared__ double red[32];
+  v = warp_sum_d(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double w = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    w = warp_sum_d(w);
+    if (threadIdx.x == 0) atomicAdd(dst, w);
+  }
+  __syncthreads();
+}
+
+// run of a voxel: index of the run containing linear voxel q (0-based), via
+// the per-line run table line_run[(z-1)*n + (y-1)] (-1 when the line is empty)
+
+// ---------------------------------------------------------------------------
+// ASTASQ (bpcg.f:1244-1274): FP64 sums per image; counts are host constants.
+__global__ void astasq_kernel(const float* __restrict__ projs, int n, float r2, double* __restrict__ acc) {
+  const float* x = projs + (size_t)blockIdx.x * n * n;
+  const int nc = n / 2 + 1;
+  double aba = 0.0, ssq = 0.0, sus = 0.0;
+  for (int p = threadIdx.x; p < n * n; p += blockDim.x) {
+    int i = p % n + 1, j = p / n + 1;
+    float t = (float)(j - nc), t2 = (float)(i - nc);
+    float rr = __fadd_rn(__fmul_rn(t, t), __fmul_rn(t2, t2));
+    float v = x[p];
+    if (rr > r2) aba += (double)v;
+    else { ssq += (double)v * (double)v; sus += (double)v; }
+  }
+  block_add_d(aba, acc + 0);
+  block_add_d(ssq, acc + 1);
+  block_add_d(sus, acc + 2);
+}
+
+// ---------------------------------------------------------------------------
+// A^T: BCKPJ_LIN gather.  Threads own voxels of the run list (flattened
+// through run_of[]); each adds projections [k0, k1) in order.
+__global__ void __launch_bounds__(256) bckpj_kernel(float* __restrict__ cube, const CgRun* __restrict__ runs,
+                                                    const int* __restrict__ vox_run, const int* __restrict__ vox_off,
+                                                    long long nvox, const float* __restrict__ projs,
+                                                    const CgDM* __restrict__ dms, const int* __restrict__ lb,
+                                                    int k0, int k1, int n, int ldp) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const CgRun r = runs[vox_run[v]];
+    const int jt = vox_off[v];
+    const size_t lin = (size_t)r.l1 - 1 + jt;
+    float c = cube[lin];
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp), fj = (float)jt;
+    for (int k = k0; k < k1; ++k) {
+      const CgDM dm = dms[k];
+      // XB = ((X-LDP)*DM1 + (Y-LDP)*DM2 + (Z-LDP)*DM3) + LDPNM ; XBB = XB + JT*DM1
+      const float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+      const float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+      const float xbb = __fadd_rn(xb, __fmul_rn(fj, dm.d[0]));
+      const float ybb = __fadd_rn(yb, __fmul_rn(fj, dm.d[3]));
+      const int iqx = __float2int_rz(xbb), iqy = __float2int_rz(ybb);
+      const float* P = projs + (size_t)k * n * n;
+      const int I = (iqy - 1) * n + iqx;  // PROJT column, 1-based
+      float b1 = 0.0f, b2 = 0.0f, b3 = 0.0f, b4 = 0.0f;
+      if (I >= 1 && I <= n * n - n - 1) {
+        float p00 = __ldg(P + I - 1), p01 = __ldg(P + I + n - 1), p10 = __ldg(P + I), p11 = __ldg(P + I + n);
+        if (lb) {
+          const int w = lb[k];
+          if (w > 1) {
+            const float fw = (float)w;
+            p00 = __fmul_rn(p00, fw); p01 = __fmul_rn(p01, fw); p10 = __fmul_rn(p10, fw); p11 = __fmul_rn(p11, fw);
+          }
+        }
+        b1 = p00;
+        b2 = __fsub_rn(p01, p00);
+        b3 = __fsub_rn(p10, p00);
+        b4 = __fsub_rn(__fsub_rn(p11, p10), b2);
+      }
+      const float dy = __fsub_rn(ybb, (float)iqy), dx = __fsub_rn(xbb, (float)iqx);
+      c = __fadd_rn(__fadd_rn(__fadd_rn(c, b1), __fmul_rn(dy, b2)), __fmul_rn(dx, __fadd_rn(b3, __fmul_rn(dy, b4))));
+    }
+    cube[lin] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// A: PRJCQ_N splat, one CTA per projection, image privatised in shared memory.
+__global__ void __launch_bounds__(512) prjcq_smem_kernel(const float* __restrict__ cube, const CgRun* __restrict__ runs,
+                                                         int nruns, const CgDM* __restrict__ dms, int n, int ldp,
+                                                         float* __restrict__ projs) {
+  extern __shared__ float img[];
+  const int k = blockIdx.x;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = 0.0f;
+  __syncthreads();
+  const CgDM dm = dms[k];
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
+    const CgRun r = runs[ri];
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
+    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    for (int j = r.l1; j <= r.l2; ++j) {
+      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
+      const float cv = __ldg(cube + (size_t)j - 1);
+      const float dx = __fsub_rn(xb, (float)iqx);
+      const float dy = __fmul_rn(__fsub_rn(yb, (float)iqy), cv);
+      const float dx1m = __fsub_rn(1.0f, dx);
+      const float dy1m = __fsub_rn(cv, dy);
+      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+        float* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, __fmul_rn(dx1m, dy1m));
+        atomicAdd(p + 1, __fmul_rn(dx, dy1m));
+        atomicAdd(p + n, __fmul_rn(dx1m, dy));
+        atomicAdd(p + n + 1, __fmul_rn(dx, dy));
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[3]);
+    }
+  }
+  __syncthreads();
+  float* out = projs + (size_t)k * n * n;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = img[i];
+}
+
+// Same splat with global atomics, for boxes whose image exceeds shared memory.
+__global__ void __launch_bounds__(256) prjcq_global_kernel(const float* __restrict__ cube, const CgRun* __restrict__ runs,
+                                                           int nruns, const CgDM* __restrict__ dms, int nang, int n,
+                                                           int ldp, float* __restrict__ projs) {
+  const long long total = (long long)nruns * nang;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t / nruns);
+    const CgRun r = runs[t % nruns];
+    const CgDM dm = dms[k];
+    float* img = projs + (size_t)k * n * n;
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
+    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    for (int j = r.l1; j <= r.l2; ++j) {
+      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
+      const float cv = __ldg(cube + (size_t)j - 1);
+      const float dx = __fsub_rn(xb, (float)iqx);
+      const float dy = __fmul_rn(__fsub_rn(yb, (float)iqy), cv);
+      const float dx1m = __fsub_rn(1.0f, dx);
+      const float dy1m = __fsub_rn(cv, dy);
+      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+        float* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, __fmul_rn(dx1m, dy1m));
+        atomicAdd(p + 1, __fmul_rn(dx, dy1m));
+        atomicAdd(p + n, __fmul_rn(dx1m, dy));
+        atomicAdd(p + n + 1, __fmul_rn(dx, dy));
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[3]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels over the sphere voxels (flattened run list)
+__device__ __forceinline__ size_t vox_lin(const CgRun* runs, const int* vr, const int* vo, long long v) {
+  return (size_t)runs[vr[v]].l1 - 1 + vo[v];
+}
+
+// CB -= QT inside the sphere (bpcg.f:780-790); acc[0] += CB^2 (BNORM)
+__global__ void cb_background_kernel(float* __restrict__ cb, const CgRun* __restrict__ runs, const int* __restrict__ vr,
+                                     const int* __restrict__ vo, long long nvox, float qt, double* __restrict__ acc) {
+  double s = 0.0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const size_t q = vox_lin(runs, vr, vo, v);
+    const float c = __fsub_rn(cb[q], qt);
+    cb[q] = c;
+    s += (double)c * (double)c;
+  }
+  block_add_d(s, acc);
+}
+
+// acc[0] += sum a*b over the sphere
+__global__ void dot_kernel(const float* __restrict__ a, const float* __restrict__ b, const CgRun* __restrict__ runs,
+                           const int* __restrict__ vr, const int* __restrict__ vo, long long nvox,
+                           double* __restrict__ acc) {
+  double s = 0.0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const size_t q = vox_lin(runs, vr, vo, v);
+    s += (double)a[q] * (double)b[q];
+  }
+  block_add_d(s, acc);
+}
+
+// CG scalar state, all FP64, on the device
+struct CgScal {
+  double delsq, akden, q, p, err, chi2, bnorm, pad;
+};
+
+// Q = Q*DELSQ (bpcg.f:1195), then BCKP = CB - Q*BCKP inside the sphere
+__global__ void dir_update_kernel(float* __restrict__ p, const float* __restrict__ cb, const CgRun* __restrict__ runs,
+                                  const int* __restrict__ vr, const int* __restrict__ vo, long long nvox,
+                                  const CgScal* __restrict__ sc) {
+  const double qd = sc->q * sc->delsq;
+  const float q = (float)qd;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const size_t i = vox_lin(runs, vr, vo, v);
+    p[i] = (float)((double)cb[i] - qd * (double)p[i]);
+  }
+  (void)q;
+}
+
+// after the direction update: Q = -1/DELSQ (kept as the product form above)
+__global__ void scal_after_dir_kernel(CgScal* sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) sc->q = -1.0 / sc->delsq;
+}
+
+// P = DELSQ/AKDEN; ERR = DELSQ/BNORM; CHI2 = CHI2 - P*DELSQ (bpcg.f:1197-1212)
+__global__ void scal_step_kernel(CgScal* sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    sc->p = sc->delsq / sc->akden;
+    sc->err = sc->delsq / sc->bnorm;
+    sc->chi2 = sc->chi2 - sc->p * sc->delsq;
+  }
+}
+
+// BCKN += P*BCKP ; CB -= P*BCKE inside the sphere
+__global__ void step_kernel(float* __restrict__ x, float* __restrict__ cb, const float* __restrict__ p,
+                            const float* __restrict__ e, const CgRun* __restrict__ runs, const int* __restrict__ vr,
+                            const int* __restrict__ vo, long long nvox, const CgScal* __restrict__ sc) {
+  const double s = sc->p;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const size_t i = vox_lin(runs, vr, vo, v);
+    x[i] = (float)((double)x[i] + s * (double)p[i]);
+    cb[i] = (float)((double)cb[i] - s * (double)e[i]);
+  }
+}
+
+// FIXEDGE (bpcg.f:1278-1517), part 1: zero outside the sphere runs
+__global__ void zero_outside_kernel(float* __restrict__ p, int n, int ldp, float r2) {
+  const size_t nnn = (size_t)n * n * n;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nnn; q += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(q % n) + 1;
+    const size_t t = q / n;
+    const int y = (int)(t % n) + 1, z = (int)(t / n) + 1;
+    const float tz = (float)(z - ldp), ty = (float)(y - ldp), tx = (float)(x - ldp);
+    const float rc = __fadd_rn(__fmul_rn(tx, tx), __fadd_rn(__fmul_rn(ty, ty), __fmul_rn(tz, tz)));
+    if (rc > r2) p[q] = 0.0f;
+  }
+}
+
+// FIXEDGE part 2: extend the first/last nonzero of every line along `axis`
+// by `w` voxels (mode 1/2/3); one thread per line, exact reference scans.
+__global__ void fixedge_axis_kernel(float* __restrict__ p, int n, int axis, int mode) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= n * n) return;
+  const int a = line / n, b = line % n;  // a, b: the other two coordinates (0-based)
+  size_t base, stride;
+  if (axis == 0) { base = ((size_t)a * n + b) * n; stride = 1; }                       // K=a, J=b
+  else if (axis == 1) { base = (size_t)a * n * n + b; stride = (size_t)n; }             // K=a, I=b
+  else { base = (size_t)a * n + b; stride = (size_t)n * n; }                            // J=a, I=b
+  auto L = [&](int t) -> float& { return p[base + (size_t)(t - 1) * stride]; };
+  if (mode == 1) {
+    for (int t = 1; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { L(t) = L(t + 1); break; }
+    for (int t = n; t >= 2; --t) if (L(t - 1) != 0.0f) { L(t) = L(t - 1); break; }
+  } else if (mode == 2) {
+    for (int t = 2; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { float v = L(t + 1); L(t) = v; L(t - 1) = v; break; }
+    for (int t = n - 1; t >= 2; --t) if (L(t - 1) != 0.0f) { float v = L(t - 1); L(t) = v; L(t + 1) = v; break; }
+  } else {
+    for (int t = 3; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { float v = L(t + 1); L(t) = v; L(t - 1) = v; L(t - 2) = v; break; }
+    for (int t = n - 2; t >= 2; --t) if (L(t - 1) != 0.0f) { float v = L(t - 1); L(t) = v; L(t + 1) = v; L(t + 2) = v; break; }
+  }
+}
+
+// BFIRSTS / BSECOND / BTHIRD (bpcg.f:1521-1588): BCKE += lambda * D^k BCKP
+__global__ void regularize_kernel(float* __restrict__ e, const float* __restrict__ p, const CgRun* __restrict__ runs,
+                                  const int* __restrict__ vr, const int* __restrict__ vo, long long nvox, int n,
+                                  float lam, int mode) {
+  const long sx = 1, sy = n, sz = (long)n * n;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const long q = (long)vox_lin(runs, vr, vo, v);
+    float t;
+    if (mode == 1) {
+      float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p[q + sx], p[q + sy]), p[q + sz]), p[q - sx]), p[q - sy]), p[q - sz]);
+      t = __fsub_rn(__fmul_rn(6.0f, p[q]), s);
+    } else if (mode == 2) {
+      t = __fmul_rn(18.0f, p[q]);
+      const long st[3] = {sx, sy, sz};
+      for (int d = 0; d < 3; ++d) {
+        t = __fadd_rn(__fsub_rn(t, __fmul_rn(4.0f, p[q + st[d]])), p[q + 2 * st[d]]);
+        t = __fadd_rn(__fsub_rn(t, __fmul_rn(4.0f, p[q - st[d]])), p[q - 2 * st[d]]);
+      }
+    } else {
+      t = __fmul_rn(60.0f, p[q]);
+      const long st[3] = {sx, sy, sz};
+      for (int d = 0; d < 3; ++d) {
+        t = __fsub_rn(__fadd_rn(__fsub_rn(t, __fmul_rn(15.0f, p[q + st[d]])), __fmul_rn(6.0f, p[q + 2 * st[d]])), p[q + 3 * st[d]]);
+        t = __fsub_rn(__fadd_rn(__fsub_rn(t, __fmul_rn(15.0f, p[q - st[d]])), __fmul_rn(6.0f, p[q - 2 * st[d]])), p[q - 3 * st[d]]);
+      }
+    }
+    e[q] = __fadd_rn(e[q], __fmul_rn(lam, t));
+  }
+}
+
+void cg_release(spi_ctx* c) {
+  for (auto& b : c->cg_buf) b.release();
+}
+
+// Device-side problem description shared by the entry points
+struct CgProblem {
+  int n, ldp;
+  float ri;
+  std::vector<CgRun> runs;
+  long long nvox = 0;
+};
+
+static int cg_setup(spi_ctx* c, int n, float ri, CgProblem& pb) {
+  pb.n = n;
+  pb.ldp = n / 2 + 1;
+  pb.ri = ri;
+  prepcub_s(n, ri, pb.ldp, pb.runs);
+  std::vector<int> vr, vo;
+  for (size_t r = 0; r < pb.runs.size(); ++r)
+    for (int j = pb.runs[r].l1; j <= pb.runs[r].l2; ++j) {
+      vr.push_back((int)r);
+      vo.push_back(j - pb.runs[r].l1);
+    }
+  pb.nvox = (long long)vr.size();
+  // cg_buf[0] runs, [1] vox_run, [2] vox_off
+  SPI_TRY(c->cg_buf[0].ensure(std::max<size_t>(1, pb.runs.size()) * sizeof(CgRun)));
+  SPI_TRY(c->cg_buf[1].ensure(std::max<size_t>(1, vr.size()) * sizeof(int)));
+  SPI_TRY(c->cg_buf[2].ensure(std::max<size_t>(1, vo.size()) * sizeof(int)));
+  if (!pb.runs.empty()) {
+    SPI_CUDA(cudaMemcpy(c->cg_buf[0].p, pb.runs.data(), pb.runs.size() * sizeof(CgRun), cudaMemcpyHostToDevice));
+    SPI_CUDA(cudaMemcpy(c->cg_buf[1].p, vr.data(), vr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SPI_CUDA(cudaMemcpy(c->cg_buf[2].p, vo.data(), vo.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+static int blocks_for(const spi_ctx* c, long long work, int threads) {
+  long long b = (work + threads - 1) / threads;
+  long long cap = (long long)c->sm_count * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// A: projections of `cube` for dms[0..nang) into projs (zeroed here)
+static int launch_project(spi_ctx* c, const CgProblem& pb, const float* cube, const CgDM* dms, int nang, float* projs) {
+  const int n = pb.n;
+  const size_t smem = (size_t)n * n * sizeof(float);
+  if (nang <= 0) return 0;
+  if (smem <= 200 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(prjcq_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr_set = true;
+    }
+    prjcq_smem_kernel<<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, n,
+                                                       pb.ldp, projs);
+    SPI_TRY(check_kernel("prjcq_smem_kernel"));
+  } else {
+    SPI_CUDA(cudaMemsetAsync(projs, 0, (size_t)nang * n * n * sizeof(float), c->stream));
+    long long work = (long long)pb.runs.size() * nang;
+    prjcq_global_kernel<<<blocks_for(c, work, 256), 256, 0, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(),
+                                                                        (int)pb.runs.size(), dms, nang, n, pb.ldp,
+                                                                        projs);
+    SPI_TRY(check_kernel("prjcq_global_kernel"));
+  }
+  c->count();
+  return 0;
+}
+
+// A^T: cube += back-projection of projs (image order, chunks of 64 images)
+static int launch_backproject(spi_ctx* c, const CgProblem& pb, float* cube, const float* projs, const CgDM* dms,
+                              const int* lb, int nang) {
+  const int kchunk = 64;
+  for (int k0 = 0; k0 < nang; k0 += kchunk) {
+    int k1 = std::min(nang, k0 + kchunk);
+    bckpj_kernel<<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
+        cube, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(), pb.nvox, projs, dms, lb, k0,
+        k1, pb.n, pb.ldp);
+    SPI_TRY(check_kernel("bckpj_kernel"));
+    c->count();
+  }
+  return 0;
+}
+
+static void dms_from_angles(const float* angles, int nang, std::vector<CgDM>& out) {
+  out.resize((size_t)std::max(nang, 1));
+  for (int k = 0; k < nang; ++k) {
+    float dm[9];
+    cang(angles[3 * k + 2], angles[3 * k + 1], angles[3 * k + 0], dm);  // CANG(phi, theta, psi)
+    memcpy(out[k].d, dm, 6 * sizeof(float));
+  }
+}
+
+// HIANG (hiang.f:40-112).  ang[3*i] = phi, [3*i+1] = theta, [3*i+2] = psi.
+// Duplicates (after the fold and the 0.01 degree truncation of phi) merge into
+// their first occurrence, exactly as the reference's pairwise scan does.
+static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std::vector<int>& lb) {
+  for (int i = 0; i < nang; ++i) {
+    if (ang[3 * i + 1] >= 90.0f) {
+      ang[3 * i + 1] = 180.0f - ang[3 * i + 1];
+      ang[3 * i] = ang[3 * i] + 180.0f;
+      if (ang[3 * i] >= 360.0f) ang[3 * i] = ang[3 * i] - 360.0f;
+    }
+  }
+  for (int i = 0; i < nang; ++i) {
+    int jjj = (int)(100.0f * ang[3 * i]);
+    ang[3 * i] = (float)jjj / 100.0f;
+  }
+  std::unordered_map<uint64_t, int> first;
+  std::vector<int> order;
+  lb.clear();
+  for (int i = 0; i < nang; ++i) {
+    uint32_t a, b;
+    float fa = ang[3 * i], fb = ang[3 * i + 1];
+    if (fa == 0.0f) fa = 0.0f;  // +0 and -0 compare equal in the reference
+    if (fb == 0.0f) fb = 0.0f;
+    memcpy(&a, &fa, 4);
+    memcpy(&b, &fb, 4);
+    uint64_t key = ((uint64_t)a << 32) | b;
+    auto it = first.find(key);
+    if (it == first.end()) {
+      first.emplace(key, (int)order.size());
+      order.push_back(i);
+      lb.push_back(1);
+    } else {
+      lb[it->second] += 1;
+    }
+  }
+  const int lo = (int)order.size();
+  const double quadpi = (double)3.14159265358979323846f;
+  const double d2r = quadpi / 180.0;
+  dms.resize((size_t)std::max(lo, 1));
+  for (int o = 0; o < lo; ++o) {
+    const int i = order[o];
+    double cphi = std::cos((double)ang[3 * i] * d2r), sphi = std::sin((double)ang[3 * i] * d2r);
+    double cthe = std::cos((double)ang[3 * i + 1] * d2r), sthe = std::sin((double)ang[3 * i + 1] * d2r);
+    double cpsi = 1.0, spsi = 0.0;
+    float* d = dms[o].d;
+    d[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+    d[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+    d[2] = (float)(-sthe * cpsi);
+    d[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+    d[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+    d[5] = (float)(sthe * spsi);
+  }
+  return lo;
+}
+
+}  // namespace spi
+
 using namespace spi;
+
 extern "C" {
-int spi_bpcg(spi_ctx*, const float*, int, int, const float*, float, float, float, int, int, float, float*, float*, int*) {
-  return fail(kInvalid, "spi_bpcg: not built in this revision");
+
+int spi_cg_project(spi_ctx* c, const float* vol, int n, float ri, const float* angles, int nang, float* projs,
+                   int on_device) {
+  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_project: bad arguments");
+  if (n < 8) return fail(kInvalid, "spi_cg_project: n = %d too small", n);
+  SPI_CUDA(cudaSetDevice(c->device));
+  CgProblem pb;
+  SPI_TRY(cg_setup(c, n, ri, pb));
+  std::vector<CgDM> dms;
+  dms_from_angles(angles, nang, dms);
+  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
+  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  SPI_CUDA(cudaMemcpy(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice));
+  const float* dv = vol;
+  float* dp = projs;
+  if (!on_device) {
+    SPI_TRY(c->cg_buf[4].ensure(vb));
+    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
+    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[4].p, vol, vb, cudaMemcpyHostToDevice, c->stream));
+    dv = c->cg_buf[4].as<float>();
+    dp = c->cg_buf[5].as<float>();
+  }
+  SPI_TRY(launch_project(c, pb, dv, c->cg_buf[3].as<CgDM>(), nang, dp));
+  if (!on_device && pbytes) SPI_CUDA(cudaMemcpyAsync(projs, dp, pbytes, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
 }
-int spi_cg_project(spi_ctx*, const float*, int, float, const float*, int, float*, int) {
-  return fail(kInvalid, "spi_cg_project: not built in this revision");
+
+int spi_cg_backproject(spi_ctx* c, const float* projs, int n, float ri, const float* angles, int nang, float* vol,
+                       int on_device) {
+  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_backproject: bad arguments");
+  if (n < 8) return fail(kInvalid, "spi_cg_backproject: n = %d too small", n);
+  SPI_CUDA(cudaSetDevice(c->device));
+  CgProblem pb;
+  SPI_TRY(cg_setup(c, n, ri, pb));
+  std::vector<CgDM> dms;
+  dms_from_angles(angles, nang, dms);
+  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
+  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  SPI_CUDA(cudaMemcpy(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice));
+  const float* dp = projs;
+  float* dv = vol;
+  if (!on_device) {
+    SPI_TRY(c->cg_buf[4].ensure(vb));
+    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
+    if (pbytes) SPI_CUDA(cudaMemcpyAsync(c->cg_buf[5].p, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
+    dv = c->cg_buf[4].as<float>();
+    dp = c->cg_buf[5].as<float>();
+  }
+  SPI_CUDA(cudaMemsetAsync(dv, 0, vb, c->stream));
+  SPI_TRY(launch_backproject(c, pb, dv, dp, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  if (!on_device) SPI_CUDA(cudaMemcpyAsync(vol, dv, vb, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
 }
-int spi_cg_backproject(spi_ctx*, const float*, int, float, const float*, int, float*, int) {
-  return fail(kInvalid, "spi_cg_backproject: not built in this revision");
+
+int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
+             int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out) {
+  if (!c || !projs || !angles || !vol_out) return fail(kInvalid, "spi_bpcg: NULL argument");
+  if (n < 8 || nang <= 0) return fail(kInvalid, "spi_bpcg: n = %d, nang = %d", n, nang);
+  if (mode < 1 || mode > 3) return fail(kInvalid, "spi_bpcg: mode %d must be 1, 2 or 3", mode);
+  SPI_CUDA(cudaSetDevice(c->device));
+  if (niter_out) *niter_out = 0;
+  CgProblem pb;
+  SPI_TRY(cg_setup(c, n, ri, pb));
+  const size_t nnn = (size_t)n * n * n;
+  const size_t vb = nnn * sizeof(float);
+  const size_t pbytes = (size_t)nang * n * n * sizeof(float);
+  // buffers: [3] dms, [4] CB, [5] projections, [6] BCKN|BCKP|BCKE, [7] scalars + lb
+  std::vector<CgDM> dms;
+  dms_from_angles(angles, nang, dms);
+  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  SPI_TRY(c->cg_buf[4].ensure(vb));
+  SPI_TRY(c->cg_buf[5].ensure(pbytes));
+  SPI_TRY(c->cg_buf[6].ensure(3 * vb));
+  SPI_TRY(c->cg_buf[7].ensure(sizeof(CgScal) + 64 + (size_t)nang * sizeof(int)));
+  float* cb = c->cg_buf[4].as<float>();
+  float* pj = c->cg_buf[5].as<float>();
+  float* bckn = c->cg_buf[6].as<float>();
+  float* bckp = bckn + nnn;
+  float* bcke = bckp + nnn;
+  CgScal* sc = c->cg_buf[7].as<CgScal>();
+  double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal));
+  int* dlb = reinterpret_cast<int*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal) + 64);
+  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(pj, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
+  // ---- BPCG_2: statistics, CB = A^T b, background correction
+  SPI_CUDA(cudaMemsetAsync(acc, 0, 64, c->stream));
+  astasq_kernel<<<nang, 256, 0, c->stream>>>(pj, n, ri * ri, acc);
+  SPI_TRY(check_kernel("astasq_kernel"));
+  c->count();
+  SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
+  SPI_TRY(launch_backproject(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  double hacc[3];
+  SPI_CUDA(cudaMemcpyAsync(hacc, acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  // pixel counts outside / inside the circle (ASTASQ's D_KLP, D_KLS)
+  double klp = 0, kls = 0;
+  {
+    const float r2 = ri * ri;
+    const int nc = n / 2 + 1;
+    for (int j = 1; j <= n; ++j)
+      for (int i = 1; i <= n; ++i) {
+        float t = (float)(j - nc), t2 = (float)(i - nc);
+        if (t * t + t2 * t2 > r2) klp += 1; else kls += 1;
+      }
+    klp *= nang;
+    kls *= nang;
+  }
+  double d_aba = hacc[0] / klp;
+  const double d_ssq = hacc[1], d_sus = hacc[2];
+  const float qt = (float)(d_aba * nang);
+  SPI_CUDA(cudaMemsetAsync(acc, 0, 64, c->stream));
+  cb_background_kernel<<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(cb, c->cg_buf[0].as<CgRun>(),
+                                                                           c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(),
+                                                                           pb.nvox, qt, acc);
+  SPI_TRY(check_kernel("cb_background_kernel"));
+  c->count();
+  double bnorm = 0;
+  SPI_CUDA(cudaMemcpyAsync(&bnorm, acc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  double chi2 = d_ssq - d_aba * (2 * d_sus - d_aba * kls);
+  // ---- HIANG
+  std::vector<float> ang((size_t)3 * nang);
+  for (int k = 0; k < nang; ++k) {
+    ang[3 * k] = angles[3 * k + 2];
+    ang[3 * k + 1] = angles[3 * k + 1];
+    ang[3 * k + 2] = angles[3 * k];
+  }
+  std::vector<int> lb;
+  const int lo = hiang(ang, nang, dms, lb);
+  const float di = (float)(n / 2);
+  if ((mode == 1 && (ri + 1.0f + 1.0f) > di) || (mode == 2 && (ri + 2.0f + 1.0f) > di) ||
+      (mode == 3 && (ri + 3.0f + 1.0f) > di))
+    return fail(kMissing, "RADIUS TOO LARGE (%d)", (int)ri);
+  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), (size_t)lo * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(dlb, lb.data(), (size_t)lo * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  // ---- BPCG_3_LIN
+  SPI_CUDA(cudaMemsetAsync(bckn, 0, 2 * vb, c->stream));  // BCKN, BCKP
+  CgScal hs{};
+  hs.q = 0.0;
+  hs.chi2 = chi2;
+  hs.bnorm = bnorm;
+  SPI_CUDA(cudaMemcpyAsync(sc, &hs, sizeof(CgScal), cudaMemcpyHostToDevice, c->stream));
+  const CgRun* runs = c->cg_buf[0].as<CgRun>();
+  const int* vr = c->cg_buf[1].as<int>();
+  const int* vo = c->cg_buf[2].as<int>();
+  const int nb = blocks_for(c, pb.nvox, 256);
+  const float r2 = ri * ri;
+  const size_t nnn_b = (size_t)blocks_for(c, (long long)nnn, 256);
+  auto iteration = [&]() -> int {
+    // DELSQ = sum CB^2
+    SPI_CUDA(cudaMemsetAsync(&sc->delsq, 0, sizeof(double), c->stream));
+    dot_kernel<<<nb, 256, 0, c->stream>>>(cb, cb, runs, vr, vo, pb.nvox, &sc->delsq);
+    dir_update_kernel<<<nb, 256, 0, c->stream>>>(bckp, cb, runs, vr, vo, pb.nvox, sc);
+    scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
+    SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
+    c->count(3);
+    SPI_TRY(launch_project(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
+    SPI_TRY(launch_backproject(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
+    zero_outside_kernel<<<(int)nnn_b, 256, 0, c->stream>>>(bckp, n, pb.ldp, r2);
+    for (int axis = 0; axis < 3; ++axis)
+      fixedge_axis_kernel<<<(n * n + 127) / 128, 128, 0, c->stream>>>(bckp, n, axis, mode);
+    regularize_kernel<<<nb, 256, 0, c->stream>>>(bcke, bckp, runs, vr, vo, pb.nvox, n, lambda, mode);
+    SPI_CUDA(cudaMemsetAsync(&sc->akden, 0, sizeof(double), c->stream));
+    dot_kernel<<<nb, 256, 0, c->stream>>>(bckp, bcke, runs, vr, vo, pb.nvox, &sc->akden);
+    scal_step_kernel<<<1, 32, 0, c->stream>>>(sc);
+    step_kernel<<<nb, 256, 0, c->stream>>>(bckn, cb, bckp, bcke, runs, vr, vo, pb.nvox, sc);
+    SPI_TRY(check_kernel("cg iteration"));
+    c->count(9);
+    return 0;
+  };
+  // capture one iteration as a CUDA graph, then replay it
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool use_graph = getenv("SPI_CG_NOGRAPH") == nullptr;
+  if (use_graph) {
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) use_graph = false;
+  }
+  if (use_graph) {
+    long long before = c->launches;
+    int st = iteration();
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (st != 0) return st;
+    if (e != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      graph = nullptr;
+      use_graph = false;
+      cudaGetLastError();
+    }
+    c->launches = before;  // counted per replay below
+  }
+  const long long per_iter_launches = [&]() {
+    long long k = 13 + (lo + 63) / 64 + 1;
+    return k;
+  }();
+  int done = 0;
+  for (int iter = 1; iter <= maxit; ++iter) {
+    if (use_graph) {
+      SPI_CUDA(cudaGraphLaunch(exec, c->stream));
+      c->launches += per_iter_launches;
+    } else {
+      SPI_TRY(iteration());
+    }
+    CgScal s;
+    SPI_CUDA(cudaMemcpyAsync(&s, sc, sizeof(CgScal), cudaMemcpyDeviceToHost, c->stream));
+    SPI_CUDA(cudaStreamSynchronize(c->stream));
+    if (log_out) {
+      log_out[3 * (iter - 1)] = (float)iter;
+      log_out[3 * (iter - 1) + 1] = (float)s.err;
+      log_out[3 * (iter - 1) + 2] = (float)s.chi2;
+    }
+    done = iter;
+    if (std::fabs(s.err) <= errm || std::fabs(s.chi2) <= chim) break;
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (niter_out) *niter_out = done;
+  SPI_CUDA(cudaMemcpyAsync(vol_out, bckn, vb, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
 }
-}
+
+}  // extern "C"
