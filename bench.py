@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Benchmark: SPIDER BP 32F Fourier gridding back-projection at 256^3.
+
+Metric: images back-projected per second at 256^3 (BP 32F: two half-set
+grids, FP32 spectra, FP32 vector-atomic accumulation).  A step is one
+persistent insertion launch over one chunk of 4,096 images (stage + batched
+2D FFT + ONELINE insertion).  Inputs are synthetic: PJ 3Q projections of a
+200-blob 256^3 phantom (sigma 1.5-10 voxels) at uniform SO(3) angles with
+additive noise at SNR 0.05, and a Bernoulli(1/2) half-set mask.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank inserts its own chunks into private grids
+(weak scaling); the grids are summed with one NCCL all-reduce before the
+volumes are finished, the exchange the reference does with MPI_ALLREDUCE.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "images backprojected/s at 256³"
+UNIT = "images/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--nx", type=int, default=256)
+    p.add_argument("--chunk", type=int, default=4096)
+    p.add_argument("--bf16", action="store_true", help="BF16 spectra (reduced precision variant)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample time")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_image():
+    """DRAM bytes per image of the insert kernel, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "insert_kernel_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_image"):
+                    return float(line.split("=")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------------ data
+def make_phantom_gpu(nx, nblobs, sigma, amp, rng, device):
+    import torch
+    g = torch.arange(nx, device=device, dtype=torch.float32) - nx // 2
+    vol = torch.zeros((nx, nx, nx), device=device, dtype=torch.float32)
+    radius = 0.375 * nx
+    for _ in range(nblobs):
+        while True:
+            p = rng.uniform(-radius, radius, 3)
+            if p @ p <= radius * radius:
+                break
+        s = rng.uniform(*sigma)
+        a = rng.uniform(*amp)
+        ez = torch.exp(-(g - p[2]) ** 2 / (2 * s * s))
+        ey = torch.exp(-(g - p[1]) ** 2 / (2 * s * s))
+        ex = torch.exp(-(g - p[0]) ** 2 / (2 * s * s))
+        vol += a * ez[:, None, None] * ey[None, :, None] * ex[None, None, :]
+    return vol
+
+
+def make_chunk(ctx, vol, angles, snr, gen):
+    import torch
+    from spider_b200 import ops
+    pr = ops.pj3q(vol, angles, ctx=ctx)                    # [n, nx, nx] on device
+    v = pr.var(dim=(1, 2), keepdim=True)
+    noise = torch.randn(pr.shape, device=pr.device, generator=gen) * torch.sqrt(v / snr)
+    return (pr + noise).contiguous()
+
+
+# ------------------------------------------------------------------ arms
+def cpu_baseline(nx, seconds, imgs_host, angles, half):
+    """The oracle (CPU restatement of bp32f.f / oneline.f with the reference's
+    OpenMP row striping) inserting a bounded sample on all host cores."""
+    import oracle
+    nthreads = os.cpu_count() or 1
+    sess = oracle.BpSession(nx)            # grids allocated and zeroed once, as BP32FQ does
+    # calibrate on a few images, then size the sample to ~`seconds`
+    t0 = time.perf_counter()
+    sess.insert(imgs_host[:4], angles[:4], half[:4], nthreads=nthreads)
+    per = (time.perf_counter() - t0) / 4
+    n = int(max(4, min(len(imgs_host), seconds / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    sess.insert(imgs_host[:n], angles[:n], half[:n], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    sess.close()
+    return {"value": n / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{n} images at {nx}^3 (BP 32F per-image work: PADD2 + FFT + ONELINE, FP32, "
+                      f"the reference's OpenMP row striping), {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    nx = args.nx
+    rng = np.random.default_rng(1005)
+    from spider_b200 import synth
+    nthreads = os.cpu_count() or 1
+    pool = 256
+    imgs = rng.standard_normal((pool, nx, nx)).astype(np.float32)
+    ang = synth.so3_angles(pool, rng)
+    half = synth.half_mask(pool, rng)
+    sess = oracle.BpSession(nx)
+    # calibrate: size each step to ~ 8 s of CPU work
+    t0 = time.perf_counter()
+    sess.insert(imgs[:4], ang[:4], half[:4], nthreads=nthreads)
+    per = (time.perf_counter() - t0) / 4
+    per_step = int(max(2, min(pool, 8.0 / max(per, 1e-6))))
+    for _ in range(min(args.warmup, 1)):
+        sess.insert(imgs[:per_step], ang[:per_step], half[:per_step], nthreads=nthreads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sess.insert(imgs[:per_step], ang[:per_step], half[:per_step], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    sess.close()
+    value = per_step * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"BP 32F insertion at {nx}^3, {per_step} images per step (CPU sample)",
+                   "nx": nx},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"{per_step} images per step x {args.steps} steps; the reference is "
+                                   "Fortran+FFTW and cannot be built here, its C++ restatement is timed"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    from spider_b200 import ops, roofline, synth
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    nx, chunk = args.nx, args.chunk
+    ctx = ops.Context(local)
+    L = ctx._L
+    stream = torch.cuda.ExternalStream(L.spi_ctx_stream(ctx.handle), device=dev)
+
+    # ---- synthetic data (config: 200 blobs, sigma 1.5-10, SNR 0.05)
+    rng = np.random.default_rng(1005 + 7919 * rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1005 + rank)
+    vol = make_phantom_gpu(nx, 200, (1.5, 10.0), (0.5, 1.0), rng, dev)
+    nsteps = args.warmup + args.steps
+    angles = [synth.so3_angles(chunk, rng) for _ in range(nsteps)]
+    halves = [synth.half_mask(chunk, rng) for _ in range(nsteps)]
+    chunks = [make_chunk(ctx, vol, angles[i], 0.05, gen) for i in range(2)]
+    del vol
+    torch.cuda.synchronize()
+
+    # ---- grids: library-owned at N=1, caller-owned (for the all-reduce) at N>1
+    grids = None
+    if world > 1:
+        gb = ctypes.c_longlong()
+        L.spi_bp_grid_bytes(nx, ctypes.byref(gb))
+        grids = [torch.zeros(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
+        ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
+                                        ctypes.c_void_p(grids[1].data_ptr())))
+    ctx.bp_open(nx, 2, bf16=args.bf16)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for i in range(args.warmup):
+        ctx.bp_insert(chunks[i % 2], angles[i], halves[i])
+    torch.cuda.synchronize()
+    L.spi_ctx_set_timing(ctx.handle, 1)
+    ms = (ctypes.c_double * 8)()
+    cnt = (ctypes.c_longlong * 8)()
+    L.spi_ctx_timing(ctx.handle, ms, cnt)   # reset
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.warmup, nsteps):
+        ctx.bp_insert(chunks[i % 2], angles[i], halves[i])
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.launches - launches0
+    t_ms = e0.elapsed_time(e1)
+    L.spi_ctx_timing(ctx.handle, ms, cnt)
+    insert_ms = ms[2]
+    n_insert = max(int(cnt[2]), 1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    value = world * chunk * args.steps / (t_ms / 1e3)
+
+    # ---- exchange + finish (per reconstruction)
+    torch.cuda.synchronize()
+    f0 = time.perf_counter()
+    if world > 1:
+        import torch.distributed as dist
+        for g in grids:
+            dist.all_reduce(g)
+    outs = ctx.bp_finish(("all", "1", "2"), device=True)
+    torch.cuda.synchronize()
+    finish_ms = (time.perf_counter() - f0) * 1e3
+    L.spi_ctx_timing(ctx.handle, ms, cnt)
+    finish_phase_ms = {"symplane0": ms[3], "nrmw2": ms[4], "fft3d": ms[5], "windkb2a": ms[6]}
+    del outs
+
+    # ---- roofline of the insert kernel
+    tab, fltb = roofline.kb_table(2 * nx)
+    dms = []
+    from spider_b200._lib import load as _load  # noqa: F401
+    for a in angles[args.warmup][:16]:
+        dms.append(_cang_host(a))
+    taps = roofline.mean_taps(nx, np.array(dms), tab, fltb)
+    bytes_per_img = roofline.BYTES_PER_TAP * taps + roofline.spectrum_bytes(nx, args.bf16)
+    per_launch_s = insert_ms / n_insert / 1e3
+    achieved = bytes_per_img * chunk / per_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    tpi = traffic_per_image()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": (tpi * chunk) if tpi else None,
+            "kernel": "insert_kernel", "peak_kind": peak_kind,
+            "algorithmic_bytes_per_image": bytes_per_img, "taps_per_image": taps,
+            "launch_ms": insert_ms / n_insert}
+
+    # ---- e2e through the C ABI with host buffers (pinned), H2D/D2H inside
+    e2e = None
+    if not args.no_e2e:
+        host_chunks = [c.cpu().pin_memory() for c in chunks]
+        ctx.bp_close()
+        if world > 1:
+            ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
+                                            ctypes.c_void_p(grids[1].data_ptr())))
+        hvol = [torch.empty((nx, nx, nx), dtype=torch.float32).pin_memory() for _ in range(3)]
+        ctx.bp_open(nx, 2, bf16=args.bf16)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(args.warmup, nsteps):
+            ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
+                                      angles[i].ctypes.data_as(ctypes.c_void_p),
+                                      halves[i].ctypes.data_as(ctypes.c_void_p), 0))
+        if world > 1:
+            import torch.distributed as dist
+            for g in grids:
+                dist.all_reduce(g)
+            torch.cuda.synchronize()
+        ops.check(L.spi_bp_finish(ctx.handle, ctypes.c_void_p(hvol[0].data_ptr()), ctypes.c_void_p(hvol[1].data_ptr()),
+                                  ctypes.c_void_p(hvol[2].data_ptr()), 0))
+        e1.record(stream)
+        e1.synchronize()
+        te = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([te], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": world * chunk * args.steps / (te / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": chunk * nx * nx * 4 + chunk * (12 + 1),
+               "d2h_bytes_per_step": 3 * nx ** 3 * 4 / args.steps,
+               "note": "spi_bp_insert on pinned host images per step, then one spi_bp_finish "
+                       "to three host volumes; device-timed on the library stream"}
+    ctx.bp_close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        hc = chunks[0][:256].cpu().numpy()
+        cpu = cpu_baseline(nx, args.cpu_seconds, hc, angles[0][:256], halves[0][:256])
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"BP 32F insertion at {nx}^3 (two half-set grids), "
+                                   f"{chunk} images per step in one persistent launch",
+                       "nx": nx, "images_per_step": chunk, "spectra": "bf16" if args.bf16 else "f32",
+                       "phantom": "200 Gaussian blobs, sigma 1.5-10, SNR 0.05, uniform SO(3)",
+                       "l2": "inputs larger than L2 (1.07 GB images + 2.16 GB grids per step)",
+                       "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "finish_ms": finish_ms,
+            "finish_phase_ms": finish_phase_ms,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def _cang_host(a):
+    """DM(1:6) of CANG(phi, theta, psi) for an angle triple (psi, theta, phi)."""
+    q = float(np.float32(3.14159265358979323846)) / 180.0
+    phi, theta, psi = float(a[2]), float(a[1]), float(a[0])
+    cphi, sphi = np.cos(phi * q), np.sin(phi * q)
+    cthe, sthe = np.cos(theta * q), np.sin(theta * q)
+    cpsi, spsi = np.cos(psi * q), np.sin(psi * q)
+    return np.array([cphi * cthe * cpsi - sphi * spsi, sphi * cthe * cpsi + cphi * spsi, -sthe * cpsi,
+                     -cphi * cthe * spsi - sphi * cpsi, -sphi * cthe * spsi + cphi * cpsi, sthe * spsi],
+                    dtype=np.float32)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -48,6 +48,11 @@ int spi_version(void);
 /* Message of the last failed call on this host thread ("" if none). */
 const char* spi_last_error(void);
 
+/* The generalised Kaiser-Bessel interpolation table of FILLBESSIL
+ * (fillbessi0.f:88-125) for padded size n2 = 2*nx: tab = float[5000],
+ * fltb receives FLTB.  Host-only, needs no device. */
+int spi_kb_table(int n2, float* tab, float* fltb);
+
 /* Create / destroy a context on CUDA device `device`. */
 int spi_ctx_create(int device, spi_ctx** out);
 int spi_ctx_destroy(spi_ctx* ctx);
@@ -82,6 +87,16 @@ int spi_ctx_timing(spi_ctx* ctx, double* ms_out, long long* count_out);
  * be NULL when nsym <= 1).  Replaces the grid setup of BP3F (bp3f.f:160-178,
  * 386-394) and BP32F (bp32f.f:163-179, 490-500). */
 int spi_bp_open(spi_ctx* ctx, int nx, int ngrids, const float* sym_angles, int nsym);
+
+/* Use caller-owned device memory for the grids of the next spi_bp_open
+ * (g1 may be NULL for one grid; NULL, NULL returns to library-owned grids).
+ * Each grid is spi_bp_grid_bytes(nx) bytes of float4 {Re X, Im X, W, 0}
+ * voxels, [2nx][2nx][nx+1] with i fastest.  Lets a multi-GPU caller sum the
+ * per-rank grids with a collective before spi_bp_finish, the step the
+ * reference performs with MPI_ALLREDUCE (bp3f.f:1171-1187,
+ * bp32f.f:764-774). */
+int spi_bp_attach_grids(spi_ctx* ctx, void* g0, void* g1);
+int spi_bp_grid_bytes(int nx, long long* bytes);
 
 /* Spectrum storage for subsequent inserts: 0 = FP32 (default), 1 = BF16. */
 int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);

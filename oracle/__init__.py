@@ -54,6 +54,13 @@ def lib():
                                _u8p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
                                _f64p, _f64p, ctypes.c_int]
         L.orc_bp3f.restype = ctypes.c_int
+        L.orc_bp_insert_only.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _f32p, _u8p, ctypes.c_int]
+        L.orc_bp_insert_only.restype = ctypes.c_int
+        L.orc_bp_session_open.argtypes = [ctypes.c_int]
+        L.orc_bp_session_open.restype = ctypes.c_void_p
+        L.orc_bp_session_free.argtypes = [ctypes.c_void_p]
+        L.orc_bp_session_insert.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int, _f32p, _u8p, ctypes.c_int]
+        L.orc_bp_session_insert.restype = ctypes.c_int
         L.orc_pj3q.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                _f32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int]
         L.orc_prepcub_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
@@ -169,6 +176,39 @@ def bp32f(imgs, angles, half, *, sym=None, prec=0, nthreads=0):
     if rc != 0:
         raise RuntimeError(f"oracle bp32f failed: {rc}")
     return tuple(vols)
+
+
+def bp32f_insert_only(imgs, angles, half, *, nthreads=0):
+    """BP 32F insertion (PADD2 + FFT + ONELINE) of a sample, FP32, timing use."""
+    imgs = _f32(imgs)
+    ang = _f32(angles)
+    h = np.ascontiguousarray(half, dtype=np.uint8)
+    rc = lib().orc_bp_insert_only(_p(imgs, _f32p), imgs.shape[1], imgs.shape[0], _p(ang, _f32p), _p(h, _u8p),
+                                  nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle insert failed: {rc}")
+
+
+class BpSession:
+    """Two FP32 grids zeroed once; insert() times the per-image work only."""
+
+    def __init__(self, nx: int):
+        self.nx = nx
+        self._h = lib().orc_bp_session_open(nx)
+
+    def insert(self, imgs, angles, half, nthreads=0):
+        imgs = _f32(imgs)
+        ang = _f32(angles)
+        h = np.ascontiguousarray(half, dtype=np.uint8)
+        lib().orc_bp_session_insert(self._h, _p(imgs, _f32p), imgs.shape[0], _p(ang, _f32p), _p(h, _u8p), nthreads)
+
+    def close(self):
+        if self._h:
+            lib().orc_bp_session_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def pj3q(vol, angles, ri=None, *, prec=0, nthreads=0):

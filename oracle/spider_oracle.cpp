@@ -105,8 +105,28 @@ struct FFT1 {
     }
   }
   void exec(const cd* in, int istride, cd* out) const {
+    if ((n & (n - 1)) == 0) { pow2(in, istride, out); return; }
     std::vector<cd> tmp(2 * n + 130);
     rec(in, istride, out, n, 0, 1, tmp.data());
+  }
+  // iterative radix-2 decimation in time for power-of-two lengths
+  void pow2(const cd* in, int istride, cd* out) const {
+    int lg = 0;
+    while ((1 << lg) < n) ++lg;
+    for (int i = 0; i < n; ++i) {
+      int r = 0;
+      for (int b = 0; b < lg; ++b) r |= ((i >> b) & 1) << (lg - 1 - b);
+      out[r] = in[(size_t)i * istride];
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+      const int half = len >> 1, step = n / len;
+      for (int i = 0; i < n; i += len)
+        for (int k = 0; k < half; ++k) {
+          cd t = out[i + k + half] * w[k * step];
+          out[i + k + half] = out[i + k] - t;
+          out[i + k] = out[i + k] + t;
+        }
+    }
   }
 };
 
@@ -183,7 +203,7 @@ struct Grid {
 // Output bi[jrow*(nx+1) + i], jrow 0-based, i = 0..nx.
 template <class R>
 void stage_image(const float* proj, int nx, std::vector<std::complex<R>>& bi,
-                 const FFT1& fx, const FFT1& fy) {
+                 const FFT1& fx, const FFT1& fy, int nthreads = 1) {
   const int n = 2 * nx;
   // ASTA_D: mean of pixels outside radius L/2 (integer division, then REAL)
   float r = (float)(nx / 2);
@@ -206,13 +226,18 @@ void stage_image(const float* proj, int nx, std::vector<std::complex<R>>& bi,
       float v = (float)((double)proj[(j - 1) * nx + (i - 1)] - qs);
       img[(size_t)(ip + j - 1) * n + (ip + i - 1)] = cd(v, 0.0);
     }
-  // 2D forward FFT: rows (x) then columns (y)
-  std::vector<cd> row(n), col(n), tmp(n);
+  // 2D forward FFT: rows (x) then columns (y); threads as FFTW's plan uses
+  bi.assign((size_t)(nx + 1) * n, std::complex<R>(0, 0));
+  #pragma omp parallel num_threads(nthreads)
+  {
+  std::vector<cd> row(n), col(n);
+  #pragma omp for schedule(static)
   for (int y = 0; y < n; ++y) {
+    if (y < ip || y >= ip + nx) continue;  // zero-padding rows transform to zero
     fx.exec(&img[(size_t)y * n], 1, row.data());
     for (int x = 0; x < n; ++x) img[(size_t)y * n + x] = row[x];
   }
-  bi.assign((size_t)(nx + 1) * n, std::complex<R>(0, 0));
+  #pragma omp for schedule(static)
   for (int x = 0; x <= nx; ++x) {
     fy.exec(&img[x], n, col.data());
     for (int y = 0; y < n; ++y) {
@@ -222,6 +247,7 @@ void stage_image(const float* proj, int nx, std::vector<std::complex<R>>& bi,
       if (((x + y) & 1) != 0) v = -v;
       bi[(size_t)y * (nx + 1) + x] = v;
     }
+  }
   }
 }
 
@@ -468,7 +494,7 @@ void insert_images(std::vector<Grid<R>*>& grids, const float* imgs, int nx, int 
   FFT1 fx(n, -1), fy(n, -1);
   std::vector<std::complex<R>> bi;
   for (int a = 0; a < nang; ++a) {
-    stage_image<R>(imgs + (size_t)a * nx * nx, nx, bi, fx, fy);
+    stage_image<R>(imgs + (size_t)a * nx * nx, nx, bi, fx, fy, nthreads);
     Grid<R>& g = *grids[route ? route[a] : 0];
     for (int is = 0; is < std::max(1, nsym); ++is) {
       float dms[9];
@@ -968,6 +994,48 @@ int orc_bp3f(const float* imgs, int nx, int nang, const float* angles, const flo
   if (prec == 1)
     return bp_run<double>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
   return bp_run<float>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
+}
+
+// A BP 32F insertion session: two FP32 grids allocated and zeroed once (as
+// BP32FQ does before its image loop, bp32f.f:490-500), then images inserted.
+struct BpSession {
+  int nx;
+  KBTable kb;
+  Grid<float> ge, go;
+  BpSession(int n) : nx(n), ge(n), go(n) { fill_kb(2 * n, kb); }
+};
+
+void* orc_bp_session_open(int nx) { return new BpSession(nx); }
+void orc_bp_session_free(void* s) { delete static_cast<BpSession*>(s); }
+int orc_bp_session_insert(void* sp, const float* imgs, int nang, const float* angles, const uint8_t* half,
+                          int nthreads) {
+  BpSession* S = static_cast<BpSession*>(sp);
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  std::vector<float> dm((size_t)9 * nang);
+  for (int a = 0; a < nang; ++a) cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], &dm[9 * a]);
+  std::vector<Grid<float>*> grids{&S->ge, &S->go};
+  std::vector<uint8_t> route(nang);
+  for (int a = 0; a < nang; ++a) route[a] = (half && !half[a]) ? 1 : 0;
+  insert_images<float>(grids, imgs, S->nx, nang, dm.data(), nullptr, 0, route.data(), S->kb, nthreads);
+  return 0;
+}
+
+// BP 32F insertion only (PADD2 + FFT + ONELINE into two FP32 grids), the
+// timed CPU baseline: with nthreads > 1 it uses the reference's OpenMP row
+// striping (LN1 = 6), race included.
+int orc_bp_insert_only(const float* imgs, int nx, int nang, const float* angles, const uint8_t* half,
+                       int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  KBTable kb;
+  fill_kb(2 * nx, kb);
+  std::vector<float> dm((size_t)9 * nang);
+  for (int a = 0; a < nang; ++a) cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], &dm[9 * a]);
+  Grid<float> ge(nx), go(nx);
+  std::vector<Grid<float>*> grids{&ge, &go};
+  std::vector<uint8_t> route(nang);
+  for (int a = 0; a < nang; ++a) route[a] = (half && !half[a]) ? 1 : 0;
+  insert_images<float>(grids, imgs, nx, nang, dm.data(), nullptr, 0, route.data(), kb, nthreads);
+  return 0;
 }
 
 // PJ 3Q: vol (nx,ny,nz x fastest), angles 3 per projection (psi,theta,phi)

@@ -20,6 +20,7 @@ _vp = ctypes.c_void_p
 SIGNATURES = [
     ("spi_version", ctypes.c_int, []),
     ("spi_last_error", ctypes.c_char_p, []),
+    ("spi_kb_table", ctypes.c_int, [ctypes.c_int, _vp, _vp]),
     ("spi_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("spi_ctx_destroy", ctypes.c_int, [_vp]),
     ("spi_ctx_launch_count", ctypes.c_longlong, [_vp]),
@@ -28,6 +29,8 @@ SIGNATURES = [
     ("spi_ctx_set_timing", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_ctx_timing", ctypes.c_int, [_vp, _vp, _vp]),
     ("spi_bp_open", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]),
+    ("spi_bp_attach_grids", ctypes.c_int, [_vp, _vp, _vp]),
+    ("spi_bp_grid_bytes", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
     ("spi_bp_set_spectrum_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_bp_insert", ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
     ("spi_bp_finish", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),

@@ -407,6 +407,8 @@ void HostBuf::release() {
 
 void bp_release(spi_ctx* c) {
   for (auto& g : c->grid) g.release();
+  c->gptr[0] = c->gptr[1] = nullptr;
+  c->wkb_nx = 0;
   c->imgs.release();
   c->padded.release();
   c->spectra.release();
@@ -494,6 +496,15 @@ extern "C" {
 
 int spi_version(void) { return 100; }
 
+int spi_kb_table(int n2, float* tab, float* fltb) {
+  if (!tab || n2 < 16) return fail(kInvalid, "spi_kb_table: n2 = %d", n2);
+  KBTab t;
+  fill_kb(n2, t);
+  memcpy(tab, t.tab, sizeof(t.tab));
+  if (fltb) *fltb = t.fltb;
+  return 0;
+}
+
 const char* spi_last_error(void) { return last_error_cstr(); }
 
 int spi_ctx_create(int device, spi_ctx** out) {
@@ -575,7 +586,12 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   if (ngrids != 1 && ngrids != 2) return fail(kInvalid, "spi_bp_open: ngrids = %d must be 1 or 2", ngrids);
   if (nsym > 1 && !sym_angles) return fail(kInvalid, "spi_bp_open: nsym = %d but no symmetry angles", nsym);
   SPI_CUDA(cudaSetDevice(c->device));
-  bp_release(c);
+  if (c->nx != nx) {
+    bp_release(c);   // buffers are sized by nx; same-size reopens keep them
+  } else {
+    c->pending_sym0[0] = c->pending_sym0[1] = false;
+    c->merged = false;
+  }
   c->nx = nx;
   c->n = 2 * nx;
   c->ngrids = ngrids;
@@ -589,8 +605,13 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   SPI_CUDA(cudaMemcpyAsync(c->kbtab.p, c->kb.tab, sizeof(c->kb.tab), cudaMemcpyHostToDevice, c->stream));
   const size_t gbytes = grid_voxels(c) * sizeof(float4);
   for (int g = 0; g < ngrids; ++g) {
-    SPI_TRY(c->grid[g].ensure(gbytes));
-    SPI_CUDA(cudaMemsetAsync(c->grid[g].p, 0, gbytes, c->stream));
+    if (c->ext_grid[g]) {
+      c->gptr[g] = c->ext_grid[g];
+    } else {
+      SPI_TRY(c->grid[g].ensure(gbytes));
+      c->gptr[g] = c->grid[g].as<float4>();
+    }
+    SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
   }
   // chunk sizes: spectra of one chunk <= ~4.3 GB FP32, FFT sub-batch <= ~256 MB padded
   const size_t spec_per_img = (size_t)c->n * (nx + 1) * sizeof(float2);
@@ -600,6 +621,20 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   c->sub = sub;
   c->chunk = ((chunk + sub - 1) / sub) * sub;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bp_attach_grids(spi_ctx* c, void* g0, void* g1) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (c->ngrids) return fail(kInvalid, "spi_bp_attach_grids: call before spi_bp_open");
+  c->ext_grid[0] = static_cast<float4*>(g0);
+  c->ext_grid[1] = static_cast<float4*>(g1);
+  return 0;
+}
+
+int spi_bp_grid_bytes(int nx, long long* bytes) {
+  if (!bytes || nx < 8 || nx > 512 || (nx & 1)) return fail(kInvalid, "spi_bp_grid_bytes: nx = %d", nx);
+  *bytes = (long long)(nx + 1) * (2LL * nx) * (2LL * nx) * 16;
   return 0;
 }
 
@@ -715,14 +750,14 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, 256, smem);
     const int blocks = c->sm_count * std::max(per_sm, 1);
-    float4* g1 = c->ngrids == 2 ? c->grid[1].as<float4>() : c->grid[0].as<float4>();
+    float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
     int ev_ins = c->phase_begin(2);
     if (c->bf16)
       insert_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                           c->kbtab.as<float>(), c->kb.fltb, c->grid[0].as<float4>(), g1);
+                                                           c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
     else
       insert_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                            c->kbtab.as<float>(), c->kb.fltb, c->grid[0].as<float4>(), g1);
+                                                            c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
     SPI_TRY(check_kernel("insert_kernel"));
     c->phase_end(ev_ins);
     c->count();
@@ -738,7 +773,7 @@ static int apply_sym0(spi_ctx* c, int g) {
   const int m = c->nx - 1;
   const int work = m * m + 2 * m;
   int ev = c->phase_begin(3);
-  symplane0_kernel<<<(work + 255) / 256, 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->nx);
+  symplane0_kernel<<<(work + 255) / 256, 256, 0, c->stream>>>(c->gptr[g], c->nx);
   SPI_TRY(check_kernel("symplane0_kernel"));
   c->phase_end(ev);
   c->count();
@@ -761,26 +796,34 @@ static int finish_one(spi_ctx* c, int ga, int gb, float* dvol) {
   }
   int ev = c->phase_begin(4);
   nrmw2_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(
-      c->grid[ga].as<float4>(), gb >= 0 ? c->grid[gb].as<float4>() : nullptr, c->cplx.as<float2>(), nx);
+      c->gptr[ga], gb >= 0 ? c->gptr[gb] : nullptr, c->cplx.as<float2>(), nx);
   SPI_TRY(check_kernel("nrmw2_kernel"));
   c->phase_end(ev);
   c->count();
   ev = c->phase_begin(5);
   SPI_CUFFT(cufftExecC2R(c->plan3d, reinterpret_cast<cufftComplex*>(c->cplx.p), c->real3.as<cufftReal>()));
   c->phase_end(ev);
-  // WINDKB2A
-  std::vector<float> wkb;
-  windkb_table(nx, c->kb, wkb);
-  SPI_TRY(c->wkb.ensure(wkb.size() * sizeof(float)));
-  SPI_CUDA(cudaMemcpyAsync(c->wkb.p, wkb.data(), wkb.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1), cc = nx / 2 + 1;
-  long m = 0;
-  for (int k = 1; k <= nx; ++k)
-    for (int j = 1; j <= nx; ++j)
-      for (int i = 1; i <= nx; ++i) {
-        int lr = (k - cc) * (k - cc) + (j - cc) * (j - cc) + (i - cc) * (i - cc);
-        if (lr >= l2p && lr <= l2) ++m;
+  // WINDKB2A: |WKB| table and shell voxel count depend on nx only
+  if (c->wkb_nx != nx) {
+    std::vector<float> wkb;
+    windkb_table(nx, c->kb, wkb);
+    SPI_TRY(c->wkb.ensure(wkb.size() * sizeof(float)));
+    SPI_CUDA(cudaMemcpy(c->wkb.p, wkb.data(), wkb.size() * sizeof(float), cudaMemcpyHostToDevice));
+    const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1), cc = nx / 2 + 1;
+    long m = 0;
+    for (int k = 1; k <= nx; ++k)
+      for (int j = 1; j <= nx; ++j) {
+        const int base = (k - cc) * (k - cc) + (j - cc) * (j - cc);
+        if (base > l2) continue;
+        for (int i = 1; i <= nx; ++i) {
+          int lr = base + (i - cc) * (i - cc);
+          if (lr >= l2p && lr <= l2) ++m;
+        }
       }
+    c->wkb_m = m;
+    c->wkb_nx = nx;
+  }
+  const long m = c->wkb_m;
   const int ip = (n - nx) / 2 + nx % 2;
   const float pix = 1.0f / (float)((long long)n * n * n);
   const size_t total = (size_t)nx * nx * nx;
@@ -795,8 +838,6 @@ static int finish_one(spi_ctx* c, int ga, int gb, float* dvol) {
   SPI_TRY(check_kernel("windkb_out_kernel"));
   c->phase_end(ev);
   c->count(2);
-  // the wkb host vector must outlive the async copy
-  SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -834,7 +875,7 @@ int spi_bp_partial_out(spi_ctx* c, int g, float* x_out, float* w_out) {
   const size_t nvox = grid_voxels(c);
   SPI_TRY(c->cplx.ensure(nvox * sizeof(float2)));
   SPI_TRY(c->real3.ensure(std::max(nvox * sizeof(float), (size_t)c->n * c->n * c->n * sizeof(float))));
-  grid_split_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->cplx.as<float2>(),
+  grid_split_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->gptr[g], c->cplx.as<float2>(),
                                                                       c->real3.as<float>(), nvox);
   SPI_TRY(check_kernel("grid_split_kernel"));
   c->count();
@@ -854,7 +895,7 @@ int spi_bp_partial_add(spi_ctx* c, int g, const float* x_in, const float* w_in) 
   SPI_TRY(c->real3.ensure(std::max(nvox * sizeof(float), (size_t)c->n * c->n * c->n * sizeof(float))));
   SPI_CUDA(cudaMemcpyAsync(c->cplx.p, x_in, nvox * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(c->real3.p, w_in, nvox * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  grid_add_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->grid[g].as<float4>(), c->cplx.as<float2>(),
+  grid_add_kernel<<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(c->gptr[g], c->cplx.as<float2>(),
                                                                     c->real3.as<float>(), nvox);
   SPI_TRY(check_kernel("grid_add_kernel"));
   c->count();

@@ -19,6 +19,10 @@ struct spi_ctx {
   int sub = 0;                        // images per batched 2D FFT
   spi::KBTab kb;
   spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
+  float4* gptr[2] = {nullptr, nullptr};      // grids in use (owned or attached)
+  float4* ext_grid[2] = {nullptr, nullptr};  // caller-owned grids (spi_bp_attach_grids)
+  int wkb_nx = 0;                     // nx the cached |WKB| table belongs to
+  long wkb_m = 0;                     // shell voxel count M of WINDKB2A
   spi::DevBuf kbtab;                  // float[5000]
   spi::DevBuf imgs;                   // float [chunk][nx][nx]
   spi::DevBuf padded;                 // float [sub][n][n]
