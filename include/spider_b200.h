@@ -167,6 +167,13 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
              float ri, float errm, float chim, int maxit, int mode, float lambda,
              float* vol_out, float* log_out, int* niter_out);
 
+/* Storage and accumulation type of the BP CG vectors and projections:
+ * fp64 = 1 (default) keeps CB, BCKP, BCKE, BCKN and the projections in
+ * FP64 (the reference keeps them in REAL; its FP32 CG drifts from the exact
+ * iteration by more than 1e-2 at small LAMBDA); fp64 = 0 uses FP32 as the
+ * reference does.  Scalars (DELSQ, AKDEN, P, Q) are FP64 in both. */
+int spi_ctx_set_cg_precision(spi_ctx* ctx, int fp64);
+
 /* One application of the BP CG operators on device arrays, for the
  * differentiable wrapper and adjointness checks.  spi_cg_project: PRJCQ_N
  * (prjcq.f:48-82) of vol into projs (overwritten).  spi_cg_backproject:

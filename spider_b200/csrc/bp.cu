@@ -10,6 +10,7 @@
 // each gridding tap is one 16-byte vector atomic in L2.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -211,6 +212,192 @@ __global__ void __launch_bounds__(256) insert_kernel(const void* __restrict__ sp
         }
       }
     }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Insert, tile-privatised form.  A CTA takes a 16 (I) x 8 (J) tile of pixels
+// of one slice; 256 threads = 2 per pixel, splitting the z taps (LZ = -2..0
+// and 1..2).  The tile's taps land in a thin slab whose bounding box (at most
+// 7182 voxels over all orientations for this tile shape) is accumulated in
+// shared memory with FP32 shared atomics and flushed with one global vector
+// atomic per touched voxel, instead of one per tap (each voxel receives ~13
+// taps per image).  Tiles whose pixels straddle the x = 0 flip (two separate
+// clusters) or whose box would not fit use direct global atomics; reflected
+// taps (IXN < LN2, oneline.f:118-150) always do.  Every tap's voxel and weight
+// are computed exactly as in insert_kernel.
+constexpr int kTileI = 16, kTileJ = 8, kTileCap = 7296;
+
+template <bool BF16>
+__global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
+                                                             int nslices, int nx, const float* __restrict__ tab, float fltb,
+                                                             float4* __restrict__ g0, float4* __restrict__ g1) {
+  extern __shared__ float sm[];
+  float* s_re = sm;
+  float* s_im = sm + kTileCap;
+  float* s_w = sm + 2 * kTileCap;
+  __shared__ int s_box[8];   // xmin,ymin,zmin,-xmax,-ymax,-zmax, flipped-any, unflipped-any
+
+  const int N = 2 * nx, N2 = nx, LN2 = 2;
+  const float fN = (float)N;
+  const size_t rowlen = (size_t)(nx + 1);
+  const size_t plane = (size_t)N * rowlen;
+  const int tiles_i = (nx + 1 + kTileI - 1) / kTileI;
+  const int tiles_j = (N + kTileJ - 1) / kTileJ;
+  const int tiles_per_slice = tiles_i * tiles_j;
+  const long long nitems = (long long)nslices * tiles_per_slice;
+  const int t = threadIdx.x;
+  const int p = t & 127, half = t >> 7;
+  const int lz0 = half ? 3 : 0, lz1 = half ? 5 : 3;
+
+  for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int s = (int)(item / tiles_per_slice);
+    const int tl = (int)(item % tiles_per_slice);
+    const int I0 = (tl % tiles_i) * kTileI;
+    const int J0 = (tl / tiles_i) * kTileJ - nx + 1;
+    // skip tiles entirely outside the disk I^2 + J^2 < NX^2
+    {
+      const int ci = I0, cj = (J0 > 0) ? J0 : ((J0 + kTileJ - 1 < 0) ? J0 + kTileJ - 1 : 0);
+      if (ci * ci + cj * cj >= N * N / 4) continue;   // uniform across the CTA
+    }
+    const SliceDesc sd = slices[s];
+    float4* G = sd.grid ? g1 : g0;
+    const int I = I0 + (p & (kTileI - 1));
+    const int J = J0 + (p >> 4);
+    bool ok = (I <= N2) && (J <= nx) && ((I * I + J * J) < (N * N / 4)) && !(I == 0 && J < 0);
+    float xnew = 0.f, ynew = 0.f, znew = 0.f, br = 0.f, bi = 0.f;
+    int ixn = 0, iyn = 0, izn = 0;
+    bool flipped = false;
+    if (ok) {
+      const float fI = (float)I, fJ = (float)J;
+      xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), __fmul_rn(fJ, sd.dm[3]));
+      ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), __fmul_rn(fJ, sd.dm[4]));
+      znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), __fmul_rn(fJ, sd.dm[5]));
+      const int JP = (J >= 0) ? J : N + J;
+      const float2 sp = load_spec<BF16>(spec, (size_t)sd.img * plane + (size_t)JP * rowlen + I);
+      br = sp.x;
+      bi = -sp.y;
+      if (xnew < 0.0f) {
+        xnew = -xnew; ynew = -ynew; znew = -znew;
+        bi = -bi;
+        flipped = true;
+      }
+      ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
+      iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
+      izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
+      ok = (ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+            izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1));
+    }
+    // tile bounding box of the main taps
+    if (t < 8) s_box[t] = (t < 6) ? 0x7fffffff : 0;
+    __syncthreads();
+    if (ok && half == 0) {
+      atomicMin(&s_box[0], ixn);
+      atomicMin(&s_box[1], iyn);
+      atomicMin(&s_box[2], izn);
+      atomicMin(&s_box[3], -ixn);
+      atomicMin(&s_box[4], -iyn);
+      atomicMin(&s_box[5], -izn);
+      if (flipped) s_box[6] = 1; else s_box[7] = 1;
+    }
+    __syncthreads();
+    const int bx0 = max(s_box[0] - 2, 0), by0 = s_box[1] - 2, bz0 = s_box[2] - 2;
+    const int bx = -s_box[3] + 2 - bx0 + 1, by = -s_box[4] + 2 - by0 + 1, bz = -s_box[5] + 2 - bz0 + 1;
+    const bool any = s_box[0] != 0x7fffffff;
+    const bool mixed = s_box[6] && s_box[7];
+    const bool priv = any && !mixed && (long long)bx * by * bz <= kTileCap;
+    __syncthreads();      // every thread has read the box before it is reused
+    if (!any) continue;   // uniform: no valid pixel in this tile
+    const int bsize = priv ? bx * by * bz : 0;
+    if (priv) {
+      for (int q = t; q < bsize; q += blockDim.x) { s_re[q] = 0.f; s_im[q] = 0.f; s_w[q] = 0.f; }
+      __syncthreads();
+    }
+    if (ok) {
+      float tz[5], ty[5], tx[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        tz[l] = __ldg(tab + nint_pos(__fmul_rn(fabsf(__fsub_rn(znew, (float)(izn + l - 2))), fltb)));
+        ty[l] = __ldg(tab + nint_pos(__fmul_rn(fabsf(__fsub_rn(ynew, (float)(iyn + l - 2))), fltb)));
+        tx[l] = __ldg(tab + nint_pos(__fmul_rn(fabsf(__fsub_rn(xnew, (float)(ixn + l - 2))), fltb)));
+      }
+      const int lb = -min(ixn, LN2);
+#pragma unroll
+      for (int lz = 0; lz < 5; ++lz) {
+        if (lz < lz0 || lz >= lz1 || tz[lz] == 0.0f) continue;
+        const int izp = izn + lz - 2;
+#pragma unroll
+        for (int ly = 0; ly < 5; ++ly) {
+          const float tyz = __fmul_rn(ty[ly], tz[lz]);
+          if (tyz == 0.0f) continue;
+          const int iyp = iyn + ly - 2;
+          if (priv) {
+            const int rowq = ((izp - bz0) * by + (iyp - by0)) * bx - bx0;
+#pragma unroll
+            for (int lx = 0; lx < 5; ++lx) {
+              if (lx - 2 < lb) continue;
+              const float wg = __fmul_rn(tx[lx], tyz);
+              if (wg != 0.0f) {
+                const int q = rowq + ixn + lx - 2;
+                atomicAdd(s_re + q, __fmul_rn(br, wg));
+                atomicAdd(s_im + q, __fmul_rn(bi, wg));
+                atomicAdd(s_w + q, wg);
+              }
+            }
+          } else {
+            const int iza = (izp >= 0) ? izp : N + izp;
+            const int iya = (iyp >= 0) ? iyp : N + iyp;
+            float4* row = G + ((size_t)iza * N + iya) * rowlen;
+#pragma unroll
+            for (int lx = 0; lx < 5; ++lx) {
+              if (lx - 2 < lb) continue;
+              const float wg = __fmul_rn(tx[lx], tyz);
+              if (wg != 0.0f)
+                atomicAdd(row + (ixn + lx - 2), make_float4(__fmul_rn(br, wg), __fmul_rn(bi, wg), wg, 0.0f));
+            }
+          }
+        }
+      }
+      if (ixn < LN2) {  // reflected points (oneline.f:118-150), direct
+#pragma unroll
+        for (int lz = 0; lz < 5; ++lz) {
+          if (lz < lz0 || lz >= lz1 || tz[lz] == 0.0f) continue;
+          const int izp = izn + lz - 2;
+          const int izt = (izp > 0) ? N - izp : -izp;
+#pragma unroll
+          for (int ly = 0; ly < 5; ++ly) {
+            const float tyz = __fmul_rn(ty[ly], tz[lz]);
+            if (tyz == 0.0f) continue;
+            const int iyp = iyn + ly - 2;
+            const int iyt = (iyp > 0) ? N - iyp : -iyp;
+            float4* row = G + ((size_t)izt * N + iyt) * rowlen;
+#pragma unroll
+            for (int lx = 0; lx < 2; ++lx) {
+              const int ixp = ixn + lx - 2;
+              if (ixp > -1) continue;
+              const float wg = __fmul_rn(tx[lx], tyz);
+              if (wg != 0.0f)
+                atomicAdd(row + (-ixp), make_float4(__fmul_rn(br, wg), __fmul_rn(-bi, wg), wg, 0.0f));
+            }
+          }
+        }
+      }
+    }
+    if (priv) {
+      __syncthreads();
+      for (int q = t; q < bsize; q += blockDim.x) {
+        const float w = s_w[q];
+        if (w != 0.0f) {
+          const int ix = q % bx;
+          const int r = q / bx;
+          const int iyp = by0 + r % by, izp = bz0 + r / by;
+          const int iza = (izp >= 0) ? izp : N + izp;
+          const int iya = (iyp >= 0) ? iyp : N + iyp;
+          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + (bx0 + ix), make_float4(s_re[q], s_im[q], w, 0.0f));
+        }
+      }
+    }
+    __syncthreads();   // shared box and accumulators are reused by the next tile
   }
 }
 
@@ -617,6 +804,12 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   const size_t spec_per_img = (size_t)c->n * (nx + 1) * sizeof(float2);
   int chunk = (int)std::min<size_t>(8192, std::max<size_t>(64, (size_t)4400000000ull / spec_per_img));
   chunk = env_int("SPI_BP_CHUNK", chunk);
+  {
+    const char* m = getenv("SPI_INSERT");
+    c->insert_mode = (m && strcmp(m, "tile") == 0) ? 0 : 1;
+    const char* o = getenv("SPI_SLICE_ORDER");
+    c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
+  }
   int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)268435456ull / ((size_t)c->n * c->n * 4)));
   c->sub = sub;
   c->chunk = ((chunk + sub - 1) / sub) * sub;
@@ -697,6 +890,35 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
   }
   for (int a = 0; a < nimg; ++a)
     for (int s = 0; s < nsym; ++s) hs[(size_t)a * nsym + s].img = a % c->chunk;
+  if (c->slice_order) {
+    // Within each chunk, order slices by the normal of their central plane
+    // (boustrophedon over rings of the polar angle) so that the slices in
+    // flight together touch overlapping voxels and their atomics hit in L2.
+    // The order only changes the FP32 summation order.
+    for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
+      const int nb = std::min(c->chunk, nimg - a0);
+      SliceDesc* base = hs + (size_t)a0 * nsym;
+      const int m = nb * nsym;
+      const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
+      std::vector<std::pair<double, int>> key(m);
+      for (int q = 0; q < m; ++q) {
+        const float* d = base[q].dm;
+        double cx = (double)d[1] * d[5] - (double)d[2] * d[4];
+        double cy = (double)d[2] * d[3] - (double)d[0] * d[5];
+        double cz = (double)d[0] * d[4] - (double)d[1] * d[3];
+        if (cz < 0 || (cz == 0 && (cy < 0 || (cy == 0 && cx < 0)))) { cx = -cx; cy = -cy; cz = -cz; }
+        const double th = std::acos(std::min(1.0, std::max(-1.0, cz)));      // 0..pi/2
+        const double ph = std::atan2(cy, cx);                                 // -pi..pi
+        int ring = std::min(rings - 1, (int)(th / (M_PI / 2) * rings));
+        double u = (ph + M_PI) / (2 * M_PI);
+        if (ring & 1) u = 1.0 - u;
+        key[q] = {ring + u, q};
+      }
+      std::sort(key.begin(), key.end());
+      std::vector<SliceDesc> tmp(base, base + m);
+      for (int q = 0; q < m; ++q) base[q] = tmp[key[q].second];
+    }
+  }
   int klp_count = 0;
   {
     float rr = (float)(nx / 2) * (float)(nx / 2);
@@ -743,21 +965,43 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
     SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
                              cudaMemcpyHostToDevice, c->stream));
     const int nslices = nb * nsym;
-    const size_t smem = 5000 * sizeof(float);
-    int per_sm = 1;
-    if (c->bf16)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, 256, smem);
-    else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, 256, smem);
-    const int blocks = c->sm_count * std::max(per_sm, 1);
     float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
     int ev_ins = c->phase_begin(2);
-    if (c->bf16)
-      insert_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                           c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
-    else
-      insert_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                            c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+    if (c->insert_mode == 1) {
+      const size_t smem = 5000 * sizeof(float);
+      int per_sm = 1;
+      if (c->bf16)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, 256, smem);
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, 256, smem);
+      const int blocks = c->sm_count * std::max(per_sm, 1);
+      if (c->bf16)
+        insert_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                             c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+      else
+        insert_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                              c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+    } else {
+      const size_t smem = 3 * kTileCap * sizeof(float);
+      static bool attr_done = false;
+      if (!attr_done) {
+        cudaFuncSetAttribute(insert_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(insert_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_done = true;
+      }
+      int per_sm = 1;
+      if (c->bf16)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_tile_kernel<true>, 256, smem);
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_tile_kernel<false>, 256, smem);
+      const int blocks = c->sm_count * std::max(per_sm, 1);
+      if (c->bf16)
+        insert_tile_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                                  c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+      else
+        insert_tile_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                                   c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+    }
     SPI_TRY(check_kernel("insert_kernel"));
     c->phase_end(ev_ins);
     c->count();
@@ -808,7 +1052,7 @@ static int finish_one(spi_ctx* c, int ga, int gb, float* dvol) {
     std::vector<float> wkb;
     windkb_table(nx, c->kb, wkb);
     SPI_TRY(c->wkb.ensure(wkb.size() * sizeof(float)));
-    SPI_CUDA(cudaMemcpy(c->wkb.p, wkb.data(), wkb.size() * sizeof(float), cudaMemcpyHostToDevice));
+    SPI_CUDA(cudaMemcpyAsync(c->wkb.p, wkb.data(), wkb.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     const int l2 = (nx / 2) * (nx / 2), l2p = (nx / 2 - 1) * (nx / 2 - 1), cc = nx / 2 + 1;
     long m = 0;
     for (int k = 1; k <= nx; ++k)
@@ -862,7 +1106,10 @@ int spi_bp_finish(spi_ctx* c, float* vol_all, float* vol_1, float* vol_2, int ou
       dst = c->volbuf.as<float>();
     }
     SPI_TRY(finish_one(c, jobs[t].ga, jobs[t].gb, dst));
-    if (!out_on_device) SPI_CUDA(cudaMemcpy(jobs[t].out, dst, vbytes, cudaMemcpyDeviceToHost));
+    if (!out_on_device) {
+      SPI_CUDA(cudaMemcpyAsync(jobs[t].out, dst, vbytes, cudaMemcpyDeviceToHost, c->stream));
+      SPI_CUDA(cudaStreamSynchronize(c->stream));  // volbuf is reused by the next job
+    }
   }
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;

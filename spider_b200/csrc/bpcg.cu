@@ -81,6 +81,14 @@ __device__ __forceinline__ void block_add_d(double v, double* dst) {
 // run of a voxel: index of the run containing linear voxel q (0-based), via
 // the per-line run table line_run[(z-1)*n + (y-1)] (-1 when the line is empty)
 
+// round-to-nearest arithmetic without contraction, for FP32 and FP64
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+
 // ---------------------------------------------------------------------------
 // ASTASQ (bpcg.f:1244-1274): FP64 sums per image; counts are host constants.
 __global__ void astasq_kernel(const float* __restrict__ projs, int n, float r2, double* __restrict__ acc) {
@@ -103,16 +111,17 @@ __global__ void astasq_kernel(const float* __restrict__ projs, int n, float r2, 
 // ---------------------------------------------------------------------------
 // A^T: BCKPJ_LIN gather.  Threads own voxels of the run list (flattened
 // through run_of[]); each adds projections [k0, k1) in order.
-__global__ void __launch_bounds__(256) bckpj_kernel(float* __restrict__ cube, const CgRun* __restrict__ runs,
+template <class T>
+__global__ void __launch_bounds__(256) bckpj_kernel(T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                     const int* __restrict__ vox_run, const int* __restrict__ vox_off,
-                                                    long long nvox, const float* __restrict__ projs,
+                                                    long long nvox, const T* __restrict__ projs,
                                                     const CgDM* __restrict__ dms, const int* __restrict__ lb,
                                                     int k0, int k1, int n, int ldp) {
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const CgRun r = runs[vox_run[v]];
     const int jt = vox_off[v];
     const size_t lin = (size_t)r.l1 - 1 + jt;
-    float c = cube[lin];
+    T c = cube[lin];
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp), fj = (float)jt;
     for (int k = k0; k < k1; ++k) {
       const CgDM dm = dms[k];
@@ -122,25 +131,25 @@ __global__ void __launch_bounds__(256) bckpj_kernel(float* __restrict__ cube, co
       const float xbb = __fadd_rn(xb, __fmul_rn(fj, dm.d[0]));
       const float ybb = __fadd_rn(yb, __fmul_rn(fj, dm.d[3]));
       const int iqx = __float2int_rz(xbb), iqy = __float2int_rz(ybb);
-      const float* P = projs + (size_t)k * n * n;
+      const T* P = projs + (size_t)k * n * n;
       const int I = (iqy - 1) * n + iqx;  // PROJT column, 1-based
-      float b1 = 0.0f, b2 = 0.0f, b3 = 0.0f, b4 = 0.0f;
+      T b1 = 0, b2 = 0, b3 = 0, b4 = 0;
       if (I >= 1 && I <= n * n - n - 1) {
-        float p00 = __ldg(P + I - 1), p01 = __ldg(P + I + n - 1), p10 = __ldg(P + I), p11 = __ldg(P + I + n);
+        T p00 = P[I - 1], p01 = P[I + n - 1], p10 = P[I], p11 = P[I + n];
         if (lb) {
           const int w = lb[k];
           if (w > 1) {
-            const float fw = (float)w;
-            p00 = __fmul_rn(p00, fw); p01 = __fmul_rn(p01, fw); p10 = __fmul_rn(p10, fw); p11 = __fmul_rn(p11, fw);
+            const T fw = (T)w;
+            p00 = rmul(p00, fw); p01 = rmul(p01, fw); p10 = rmul(p10, fw); p11 = rmul(p11, fw);
           }
         }
         b1 = p00;
-        b2 = __fsub_rn(p01, p00);
-        b3 = __fsub_rn(p10, p00);
-        b4 = __fsub_rn(__fsub_rn(p11, p10), b2);
+        b2 = rsub(p01, p00);
+        b3 = rsub(p10, p00);
+        b4 = rsub(rsub(p11, p10), b2);
       }
-      const float dy = __fsub_rn(ybb, (float)iqy), dx = __fsub_rn(xbb, (float)iqx);
-      c = __fadd_rn(__fadd_rn(__fadd_rn(c, b1), __fmul_rn(dy, b2)), __fmul_rn(dx, __fadd_rn(b3, __fmul_rn(dy, b4))));
+      const T dy = (T)__fsub_rn(ybb, (float)iqy), dx = (T)__fsub_rn(xbb, (float)iqx);
+      c = radd(radd(radd(c, b1), rmul(dy, b2)), rmul(dx, radd(b3, rmul(dy, b4))));
     }
     cube[lin] = c;
   }
@@ -148,12 +157,14 @@ __global__ void __launch_bounds__(256) bckpj_kernel(float* __restrict__ cube, co
 
 // ---------------------------------------------------------------------------
 // A: PRJCQ_N splat, one CTA per projection, image privatised in shared memory.
-__global__ void __launch_bounds__(512) prjcq_smem_kernel(const float* __restrict__ cube, const CgRun* __restrict__ runs,
+template <class T>
+__global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                          int nruns, const CgDM* __restrict__ dms, int n, int ldp,
-                                                         float* __restrict__ projs) {
-  extern __shared__ float img[];
+                                                         T* __restrict__ projs) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* img = reinterpret_cast<T*>(smraw);
   const int k = blockIdx.x;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = 0.0f;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (T)0;
   __syncthreads();
   const CgDM dm = dms[k];
   for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
@@ -163,53 +174,54 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const float* __restrict
     float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
     for (int j = r.l1; j <= r.l2; ++j) {
       const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
-      const float cv = __ldg(cube + (size_t)j - 1);
-      const float dx = __fsub_rn(xb, (float)iqx);
-      const float dy = __fmul_rn(__fsub_rn(yb, (float)iqy), cv);
-      const float dx1m = __fsub_rn(1.0f, dx);
-      const float dy1m = __fsub_rn(cv, dy);
+      const T cv = cube[(size_t)j - 1];
+      const T dx = (T)__fsub_rn(xb, (float)iqx);
+      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+      const T dx1m = rsub((T)1, dx);
+      const T dy1m = rsub(cv, dy);
       if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        float* p = img + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, __fmul_rn(dx1m, dy1m));
-        atomicAdd(p + 1, __fmul_rn(dx, dy1m));
-        atomicAdd(p + n, __fmul_rn(dx1m, dy));
-        atomicAdd(p + n + 1, __fmul_rn(dx, dy));
+        T* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, rmul(dx1m, dy1m));
+        atomicAdd(p + 1, rmul(dx, dy1m));
+        atomicAdd(p + n, rmul(dx1m, dy));
+        atomicAdd(p + n + 1, rmul(dx, dy));
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
     }
   }
   __syncthreads();
-  float* out = projs + (size_t)k * n * n;
+  T* out = projs + (size_t)k * n * n;
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = img[i];
 }
 
-// Same splat with global atomics, for boxes whose image exceeds shared memory.
-__global__ void __launch_bounds__(256) prjcq_global_kernel(const float* __restrict__ cube, const CgRun* __restrict__ runs,
+// Same splat with global atomics, for images that exceed shared memory.
+template <class T>
+__global__ void __launch_bounds__(256) prjcq_global_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                            int nruns, const CgDM* __restrict__ dms, int nang, int n,
-                                                           int ldp, float* __restrict__ projs) {
+                                                           int ldp, T* __restrict__ projs) {
   const long long total = (long long)nruns * nang;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(t / nruns);
     const CgRun r = runs[t % nruns];
     const CgDM dm = dms[k];
-    float* img = projs + (size_t)k * n * n;
+    T* img = projs + (size_t)k * n * n;
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
     float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
     float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
     for (int j = r.l1; j <= r.l2; ++j) {
       const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
-      const float cv = __ldg(cube + (size_t)j - 1);
-      const float dx = __fsub_rn(xb, (float)iqx);
-      const float dy = __fmul_rn(__fsub_rn(yb, (float)iqy), cv);
-      const float dx1m = __fsub_rn(1.0f, dx);
-      const float dy1m = __fsub_rn(cv, dy);
+      const T cv = cube[(size_t)j - 1];
+      const T dx = (T)__fsub_rn(xb, (float)iqx);
+      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+      const T dx1m = rsub((T)1, dx);
+      const T dy1m = rsub(cv, dy);
       if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        float* p = img + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, __fmul_rn(dx1m, dy1m));
-        atomicAdd(p + 1, __fmul_rn(dx, dy1m));
-        atomicAdd(p + n, __fmul_rn(dx1m, dy));
-        atomicAdd(p + n + 1, __fmul_rn(dx, dy));
+        T* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, rmul(dx1m, dy1m));
+        atomicAdd(p + 1, rmul(dx, dy1m));
+        atomicAdd(p + n, rmul(dx1m, dy));
+        atomicAdd(p + n + 1, rmul(dx, dy));
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
@@ -224,20 +236,22 @@ __device__ __forceinline__ size_t vox_lin(const CgRun* runs, const int* vr, cons
 }
 
 // CB -= QT inside the sphere (bpcg.f:780-790); acc[0] += CB^2 (BNORM)
-__global__ void cb_background_kernel(float* __restrict__ cb, const CgRun* __restrict__ runs, const int* __restrict__ vr,
-                                     const int* __restrict__ vo, long long nvox, float qt, double* __restrict__ acc) {
+template <class T>
+__global__ void cb_background_kernel(T* __restrict__ cb, const CgRun* __restrict__ runs, const int* __restrict__ vr,
+                                     const int* __restrict__ vo, long long nvox, T qt, double* __restrict__ acc) {
   double s = 0.0;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const size_t q = vox_lin(runs, vr, vo, v);
-    const float c = __fsub_rn(cb[q], qt);
+    const T c = rsub(cb[q], qt);
     cb[q] = c;
     s += (double)c * (double)c;
   }
   block_add_d(s, acc);
 }
 
-// acc[0] += sum a*b over the sphere
-__global__ void dot_kernel(const float* __restrict__ a, const float* __restrict__ b, const CgRun* __restrict__ runs,
+// acc[0] += sum a*b over the sphere (FP64)
+template <class T>
+__global__ void dot_kernel(const T* __restrict__ a, const T* __restrict__ b, const CgRun* __restrict__ runs,
                            const int* __restrict__ vr, const int* __restrict__ vo, long long nvox,
                            double* __restrict__ acc) {
   double s = 0.0;
@@ -253,20 +267,19 @@ struct CgScal {
   double delsq, akden, q, p, err, chi2, bnorm, pad;
 };
 
-// Q = Q*DELSQ (bpcg.f:1195), then BCKP = CB - Q*BCKP inside the sphere
-__global__ void dir_update_kernel(float* __restrict__ p, const float* __restrict__ cb, const CgRun* __restrict__ runs,
+// Q = Q*DELSQ (bpcg.f:1160), then BCKP = CB - Q*BCKP inside the sphere
+template <class T>
+__global__ void dir_update_kernel(T* __restrict__ p, const T* __restrict__ cb, const CgRun* __restrict__ runs,
                                   const int* __restrict__ vr, const int* __restrict__ vo, long long nvox,
                                   const CgScal* __restrict__ sc) {
   const double qd = sc->q * sc->delsq;
-  const float q = (float)qd;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const size_t i = vox_lin(runs, vr, vo, v);
-    p[i] = (float)((double)cb[i] - qd * (double)p[i]);
+    p[i] = (T)((double)cb[i] - qd * (double)p[i]);
   }
-  (void)q;
 }
 
-// after the direction update: Q = -1/DELSQ (kept as the product form above)
+// after the direction update: Q = -1/DELSQ (bpcg.f:1168)
 __global__ void scal_after_dir_kernel(CgScal* sc) {
   if (threadIdx.x == 0 && blockIdx.x == 0) sc->q = -1.0 / sc->delsq;
 }
@@ -281,19 +294,21 @@ __global__ void scal_step_kernel(CgScal* sc) {
 }
 
 // BCKN += P*BCKP ; CB -= P*BCKE inside the sphere
-__global__ void step_kernel(float* __restrict__ x, float* __restrict__ cb, const float* __restrict__ p,
-                            const float* __restrict__ e, const CgRun* __restrict__ runs, const int* __restrict__ vr,
-                            const int* __restrict__ vo, long long nvox, const CgScal* __restrict__ sc) {
+template <class T>
+__global__ void step_kernel(T* __restrict__ x, T* __restrict__ cb, const T* __restrict__ p, const T* __restrict__ e,
+                            const CgRun* __restrict__ runs, const int* __restrict__ vr, const int* __restrict__ vo,
+                            long long nvox, const CgScal* __restrict__ sc) {
   const double s = sc->p;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const size_t i = vox_lin(runs, vr, vo, v);
-    x[i] = (float)((double)x[i] + s * (double)p[i]);
-    cb[i] = (float)((double)cb[i] - s * (double)e[i]);
+    x[i] = (T)((double)x[i] + s * (double)p[i]);
+    cb[i] = (T)((double)cb[i] - s * (double)e[i]);
   }
 }
 
 // FIXEDGE (bpcg.f:1278-1517), part 1: zero outside the sphere runs
-__global__ void zero_outside_kernel(float* __restrict__ p, int n, int ldp, float r2) {
+template <class T>
+__global__ void zero_outside_kernel(T* __restrict__ p, int n, int ldp, float r2) {
   const size_t nnn = (size_t)n * n * n;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nnn; q += (size_t)gridDim.x * blockDim.x) {
     const int x = (int)(q % n) + 1;
@@ -301,13 +316,14 @@ __global__ void zero_outside_kernel(float* __restrict__ p, int n, int ldp, float
     const int y = (int)(t % n) + 1, z = (int)(t / n) + 1;
     const float tz = (float)(z - ldp), ty = (float)(y - ldp), tx = (float)(x - ldp);
     const float rc = __fadd_rn(__fmul_rn(tx, tx), __fadd_rn(__fmul_rn(ty, ty), __fmul_rn(tz, tz)));
-    if (rc > r2) p[q] = 0.0f;
+    if (rc > r2) p[q] = (T)0;
   }
 }
 
 // FIXEDGE part 2: extend the first/last nonzero of every line along `axis`
-// by `w` voxels (mode 1/2/3); one thread per line, exact reference scans.
-__global__ void fixedge_axis_kernel(float* __restrict__ p, int n, int axis, int mode) {
+// by 1, 2 or 3 voxels (mode 1/2/3); one thread per line, the reference scans.
+template <class T>
+__global__ void fixedge_axis_kernel(T* __restrict__ p, int n, int axis, int mode) {
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
   if (line >= n * n) return;
   const int a = line / n, b = line % n;  // a, b: the other two coordinates (0-based)
@@ -315,47 +331,56 @@ __global__ void fixedge_axis_kernel(float* __restrict__ p, int n, int axis, int 
   if (axis == 0) { base = ((size_t)a * n + b) * n; stride = 1; }                       // K=a, J=b
   else if (axis == 1) { base = (size_t)a * n * n + b; stride = (size_t)n; }             // K=a, I=b
   else { base = (size_t)a * n + b; stride = (size_t)n * n; }                            // J=a, I=b
-  auto L = [&](int t) -> float& { return p[base + (size_t)(t - 1) * stride]; };
+  auto L = [&](int t) -> T& { return p[base + (size_t)(t - 1) * stride]; };
+  const T z = (T)0;
   if (mode == 1) {
-    for (int t = 1; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { L(t) = L(t + 1); break; }
-    for (int t = n; t >= 2; --t) if (L(t - 1) != 0.0f) { L(t) = L(t - 1); break; }
+    for (int t = 1; t <= n - 1; ++t) if (L(t + 1) != z) { L(t) = L(t + 1); break; }
+    for (int t = n; t >= 2; --t) if (L(t - 1) != z) { L(t) = L(t - 1); break; }
   } else if (mode == 2) {
-    for (int t = 2; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { float v = L(t + 1); L(t) = v; L(t - 1) = v; break; }
-    for (int t = n - 1; t >= 2; --t) if (L(t - 1) != 0.0f) { float v = L(t - 1); L(t) = v; L(t + 1) = v; break; }
+    for (int t = 2; t <= n - 1; ++t) if (L(t + 1) != z) { T v = L(t + 1); L(t) = v; L(t - 1) = v; break; }
+    for (int t = n - 1; t >= 2; --t) if (L(t - 1) != z) { T v = L(t - 1); L(t) = v; L(t + 1) = v; break; }
   } else {
-    for (int t = 3; t <= n - 1; ++t) if (L(t + 1) != 0.0f) { float v = L(t + 1); L(t) = v; L(t - 1) = v; L(t - 2) = v; break; }
-    for (int t = n - 2; t >= 2; --t) if (L(t - 1) != 0.0f) { float v = L(t - 1); L(t) = v; L(t + 1) = v; L(t + 2) = v; break; }
+    for (int t = 3; t <= n - 1; ++t) if (L(t + 1) != z) { T v = L(t + 1); L(t) = v; L(t - 1) = v; L(t - 2) = v; break; }
+    for (int t = n - 2; t >= 2; --t) if (L(t - 1) != z) { T v = L(t - 1); L(t) = v; L(t + 1) = v; L(t + 2) = v; break; }
   }
 }
 
 // BFIRSTS / BSECOND / BTHIRD (bpcg.f:1521-1588): BCKE += lambda * D^k BCKP
-__global__ void regularize_kernel(float* __restrict__ e, const float* __restrict__ p, const CgRun* __restrict__ runs,
+template <class T>
+__global__ void regularize_kernel(T* __restrict__ e, const T* __restrict__ p, const CgRun* __restrict__ runs,
                                   const int* __restrict__ vr, const int* __restrict__ vo, long long nvox, int n,
-                                  float lam, int mode) {
+                                  T lam, int mode) {
   const long sx = 1, sy = n, sz = (long)n * n;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const long q = (long)vox_lin(runs, vr, vo, v);
-    float t;
+    T t;
     if (mode == 1) {
-      float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p[q + sx], p[q + sy]), p[q + sz]), p[q - sx]), p[q - sy]), p[q - sz]);
-      t = __fsub_rn(__fmul_rn(6.0f, p[q]), s);
+      T s = radd(radd(radd(radd(radd(p[q + sx], p[q + sy]), p[q + sz]), p[q - sx]), p[q - sy]), p[q - sz]);
+      t = rsub(rmul((T)6, p[q]), s);
     } else if (mode == 2) {
-      t = __fmul_rn(18.0f, p[q]);
+      t = rmul((T)18, p[q]);
       const long st[3] = {sx, sy, sz};
       for (int d = 0; d < 3; ++d) {
-        t = __fadd_rn(__fsub_rn(t, __fmul_rn(4.0f, p[q + st[d]])), p[q + 2 * st[d]]);
-        t = __fadd_rn(__fsub_rn(t, __fmul_rn(4.0f, p[q - st[d]])), p[q - 2 * st[d]]);
+        t = radd(rsub(t, rmul((T)4, p[q + st[d]])), p[q + 2 * st[d]]);
+        t = radd(rsub(t, rmul((T)4, p[q - st[d]])), p[q - 2 * st[d]]);
       }
     } else {
-      t = __fmul_rn(60.0f, p[q]);
+      t = rmul((T)60, p[q]);
       const long st[3] = {sx, sy, sz};
       for (int d = 0; d < 3; ++d) {
-        t = __fsub_rn(__fadd_rn(__fsub_rn(t, __fmul_rn(15.0f, p[q + st[d]])), __fmul_rn(6.0f, p[q + 2 * st[d]])), p[q + 3 * st[d]]);
-        t = __fsub_rn(__fadd_rn(__fsub_rn(t, __fmul_rn(15.0f, p[q - st[d]])), __fmul_rn(6.0f, p[q - 2 * st[d]])), p[q - 3 * st[d]]);
+        t = rsub(radd(rsub(t, rmul((T)15, p[q + st[d]])), rmul((T)6, p[q + 2 * st[d]])), p[q + 3 * st[d]]);
+        t = rsub(radd(rsub(t, rmul((T)15, p[q - st[d]])), rmul((T)6, p[q - 2 * st[d]])), p[q - 3 * st[d]]);
       }
     }
-    e[q] = __fadd_rn(e[q], __fmul_rn(lam, t));
+    e[q] = radd(e[q], rmul(lam, t));
   }
+}
+
+// float -> T widening copy
+template <class T>
+__global__ void widen_kernel(const float* __restrict__ in, T* __restrict__ out, size_t count) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count; q += (size_t)gridDim.x * blockDim.x)
+    out[q] = (T)in[q];
 }
 
 void cg_release(spi_ctx* c) {
@@ -387,9 +412,9 @@ static int cg_setup(spi_ctx* c, int n, float ri, CgProblem& pb) {
   SPI_TRY(c->cg_buf[1].ensure(std::max<size_t>(1, vr.size()) * sizeof(int)));
   SPI_TRY(c->cg_buf[2].ensure(std::max<size_t>(1, vo.size()) * sizeof(int)));
   if (!pb.runs.empty()) {
-    SPI_CUDA(cudaMemcpy(c->cg_buf[0].p, pb.runs.data(), pb.runs.size() * sizeof(CgRun), cudaMemcpyHostToDevice));
-    SPI_CUDA(cudaMemcpy(c->cg_buf[1].p, vr.data(), vr.size() * sizeof(int), cudaMemcpyHostToDevice));
-    SPI_CUDA(cudaMemcpy(c->cg_buf[2].p, vo.data(), vo.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[0].p, pb.runs.data(), pb.runs.size() * sizeof(CgRun), cudaMemcpyHostToDevice, c->stream));
+    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[1].p, vr.data(), vr.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[2].p, vo.data(), vo.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   }
   return 0;
 }
@@ -402,26 +427,28 @@ static int blocks_for(const spi_ctx* c, long long work, int threads) {
   return (int)b;
 }
 
-// A: projections of `cube` for dms[0..nang) into projs (zeroed here)
-static int launch_project(spi_ctx* c, const CgProblem& pb, const float* cube, const CgDM* dms, int nang, float* projs) {
+// A: projections of `cube` for dms[0..nang) into projs
+template <class T>
+static int launch_project(spi_ctx* c, const CgProblem& pb, const T* cube, const CgDM* dms, int nang, T* projs) {
   const int n = pb.n;
-  const size_t smem = (size_t)n * n * sizeof(float);
+  const size_t smem = (size_t)n * n * sizeof(T);
   if (nang <= 0) return 0;
-  if (smem <= 200 * 1024) {
+  const size_t smem_cap = 200 * 1024;
+  if (smem <= smem_cap) {
     static bool attr_set = false;
     if (!attr_set) {
-      cudaFuncSetAttribute(prjcq_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      cudaFuncSetAttribute(prjcq_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
       attr_set = true;
     }
-    prjcq_smem_kernel<<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, n,
-                                                       pb.ldp, projs);
+    prjcq_smem_kernel<T><<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
+                                                          n, pb.ldp, projs);
     SPI_TRY(check_kernel("prjcq_smem_kernel"));
   } else {
-    SPI_CUDA(cudaMemsetAsync(projs, 0, (size_t)nang * n * n * sizeof(float), c->stream));
+    SPI_CUDA(cudaMemsetAsync(projs, 0, (size_t)nang * n * n * sizeof(T), c->stream));
     long long work = (long long)pb.runs.size() * nang;
-    prjcq_global_kernel<<<blocks_for(c, work, 256), 256, 0, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(),
-                                                                        (int)pb.runs.size(), dms, nang, n, pb.ldp,
-                                                                        projs);
+    prjcq_global_kernel<T><<<blocks_for(c, work, 256), 256, 0, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(),
+                                                                           (int)pb.runs.size(), dms, nang, n,
+                                                                           pb.ldp, projs);
     SPI_TRY(check_kernel("prjcq_global_kernel"));
   }
   c->count();
@@ -429,12 +456,13 @@ static int launch_project(spi_ctx* c, const CgProblem& pb, const float* cube, co
 }
 
 // A^T: cube += back-projection of projs (image order, chunks of 64 images)
-static int launch_backproject(spi_ctx* c, const CgProblem& pb, float* cube, const float* projs, const CgDM* dms,
+template <class T>
+static int launch_backproject(spi_ctx* c, const CgProblem& pb, T* cube, const T* projs, const CgDM* dms,
                               const int* lb, int nang) {
   const int kchunk = 64;
   for (int k0 = 0; k0 < nang; k0 += kchunk) {
     int k1 = std::min(nang, k0 + kchunk);
-    bckpj_kernel<<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
+    bckpj_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
         cube, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(), pb.nvox, projs, dms, lb, k0,
         k1, pb.n, pb.ldp);
     SPI_TRY(check_kernel("bckpj_kernel"));
@@ -442,6 +470,8 @@ static int launch_backproject(spi_ctx* c, const CgProblem& pb, float* cube, cons
   }
   return 0;
 }
+
+static int bp_kernel_count(int nang) { return (nang + 63) / 64; }
 
 static void dms_from_angles(const float* angles, int nang, std::vector<CgDM>& out) {
   out.resize((size_t)std::max(nang, 1));
@@ -507,104 +537,46 @@ static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std:
   return lo;
 }
 
-}  // namespace spi
-
-using namespace spi;
-
-extern "C" {
-
-int spi_cg_project(spi_ctx* c, const float* vol, int n, float ri, const float* angles, int nang, float* projs,
-                   int on_device) {
-  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_project: bad arguments");
-  if (n < 8) return fail(kInvalid, "spi_cg_project: n = %d too small", n);
-  SPI_CUDA(cudaSetDevice(c->device));
-  CgProblem pb;
-  SPI_TRY(cg_setup(c, n, ri, pb));
-  std::vector<CgDM> dms;
-  dms_from_angles(angles, nang, dms);
-  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
-  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
-  SPI_CUDA(cudaMemcpy(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice));
-  const float* dv = vol;
-  float* dp = projs;
-  if (!on_device) {
-    SPI_TRY(c->cg_buf[4].ensure(vb));
-    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
-    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[4].p, vol, vb, cudaMemcpyHostToDevice, c->stream));
-    dv = c->cg_buf[4].as<float>();
-    dp = c->cg_buf[5].as<float>();
-  }
-  SPI_TRY(launch_project(c, pb, dv, c->cg_buf[3].as<CgDM>(), nang, dp));
-  if (!on_device && pbytes) SPI_CUDA(cudaMemcpyAsync(projs, dp, pbytes, cudaMemcpyDeviceToHost, c->stream));
-  SPI_CUDA(cudaStreamSynchronize(c->stream));
-  return 0;
-}
-
-int spi_cg_backproject(spi_ctx* c, const float* projs, int n, float ri, const float* angles, int nang, float* vol,
-                       int on_device) {
-  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_backproject: bad arguments");
-  if (n < 8) return fail(kInvalid, "spi_cg_backproject: n = %d too small", n);
-  SPI_CUDA(cudaSetDevice(c->device));
-  CgProblem pb;
-  SPI_TRY(cg_setup(c, n, ri, pb));
-  std::vector<CgDM> dms;
-  dms_from_angles(angles, nang, dms);
-  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
-  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
-  SPI_CUDA(cudaMemcpy(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice));
-  const float* dp = projs;
-  float* dv = vol;
-  if (!on_device) {
-    SPI_TRY(c->cg_buf[4].ensure(vb));
-    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
-    if (pbytes) SPI_CUDA(cudaMemcpyAsync(c->cg_buf[5].p, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
-    dv = c->cg_buf[4].as<float>();
-    dp = c->cg_buf[5].as<float>();
-  }
-  SPI_CUDA(cudaMemsetAsync(dv, 0, vb, c->stream));
-  SPI_TRY(launch_backproject(c, pb, dv, dp, c->cg_buf[3].as<CgDM>(), nullptr, nang));
-  if (!on_device) SPI_CUDA(cudaMemcpyAsync(vol, dv, vb, cudaMemcpyDeviceToHost, c->stream));
-  SPI_CUDA(cudaStreamSynchronize(c->stream));
-  return 0;
-}
-
-int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
-             int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out) {
-  if (!c || !projs || !angles || !vol_out) return fail(kInvalid, "spi_bpcg: NULL argument");
-  if (n < 8 || nang <= 0) return fail(kInvalid, "spi_bpcg: n = %d, nang = %d", n, nang);
-  if (mode < 1 || mode > 3) return fail(kInvalid, "spi_bpcg: mode %d must be 1, 2 or 3", mode);
-  SPI_CUDA(cudaSetDevice(c->device));
-  if (niter_out) *niter_out = 0;
+// BPCG_2 + HIANG + BPCG_3_LIN with vectors and projections stored as T
+template <class T>
+static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float* angles, float ri, float errm,
+                    float chim, int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out) {
   CgProblem pb;
   SPI_TRY(cg_setup(c, n, ri, pb));
   const size_t nnn = (size_t)n * n * n;
-  const size_t vb = nnn * sizeof(float);
-  const size_t pbytes = (size_t)nang * n * n * sizeof(float);
-  // buffers: [3] dms, [4] CB, [5] projections, [6] BCKN|BCKP|BCKE, [7] scalars + lb
+  const size_t vb = nnn * sizeof(T);
+  const size_t pcount = (size_t)nang * n * n;
+  // buffers: [3] dms, [4] CB, [5] projections (T) + float staging, [6] BCKN|BCKP|BCKE, [7] scalars + lb
   std::vector<CgDM> dms;
   dms_from_angles(angles, nang, dms);
   SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
   SPI_TRY(c->cg_buf[4].ensure(vb));
-  SPI_TRY(c->cg_buf[5].ensure(pbytes));
+  SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
   SPI_TRY(c->cg_buf[6].ensure(3 * vb));
   SPI_TRY(c->cg_buf[7].ensure(sizeof(CgScal) + 64 + (size_t)nang * sizeof(int)));
-  float* cb = c->cg_buf[4].as<float>();
-  float* pj = c->cg_buf[5].as<float>();
-  float* bckn = c->cg_buf[6].as<float>();
-  float* bckp = bckn + nnn;
-  float* bcke = bckp + nnn;
+  T* cb = c->cg_buf[4].as<T>();
+  T* pj = c->cg_buf[5].as<T>();
+  float* pj32 = (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
+  T* bckn = c->cg_buf[6].as<T>();
+  T* bckp = bckn + nnn;
+  T* bcke = bckp + nnn;
   CgScal* sc = c->cg_buf[7].as<CgScal>();
   double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal));
   int* dlb = reinterpret_cast<int*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal) + 64);
   SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
-  SPI_CUDA(cudaMemcpyAsync(pj, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(pj32, projs, pcount * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   // ---- BPCG_2: statistics, CB = A^T b, background correction
   SPI_CUDA(cudaMemsetAsync(acc, 0, 64, c->stream));
-  astasq_kernel<<<nang, 256, 0, c->stream>>>(pj, n, ri * ri, acc);
+  astasq_kernel<<<nang, 256, 0, c->stream>>>(pj32, n, ri * ri, acc);
   SPI_TRY(check_kernel("astasq_kernel"));
   c->count();
+  if (sizeof(T) != sizeof(float)) {
+    widen_kernel<T><<<blocks_for(c, (long long)pcount, 256), 256, 0, c->stream>>>(pj32, pj, pcount);
+    SPI_TRY(check_kernel("widen_kernel"));
+    c->count();
+  }
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
-  SPI_TRY(launch_backproject(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  SPI_TRY(launch_backproject<T>(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
   double hacc[3];
   SPI_CUDA(cudaMemcpyAsync(hacc, acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -621,19 +593,18 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
     klp *= nang;
     kls *= nang;
   }
-  double d_aba = hacc[0] / klp;
+  const double d_aba = hacc[0] / klp;
   const double d_ssq = hacc[1], d_sus = hacc[2];
-  const float qt = (float)(d_aba * nang);
+  const T qt = (sizeof(T) == sizeof(float)) ? (T)(float)(d_aba * nang) : (T)(d_aba * nang);
   SPI_CUDA(cudaMemsetAsync(acc, 0, 64, c->stream));
-  cb_background_kernel<<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(cb, c->cg_buf[0].as<CgRun>(),
-                                                                           c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(),
-                                                                           pb.nvox, qt, acc);
+  cb_background_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
+      cb, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(), pb.nvox, qt, acc);
   SPI_TRY(check_kernel("cb_background_kernel"));
   c->count();
   double bnorm = 0;
   SPI_CUDA(cudaMemcpyAsync(&bnorm, acc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
-  double chi2 = d_ssq - d_aba * (2 * d_sus - d_aba * kls);
+  const double chi2 = d_ssq - d_aba * (2 * d_sus - d_aba * kls);
   // ---- HIANG
   std::vector<float> ang((size_t)3 * nang);
   for (int k = 0; k < nang; ++k) {
@@ -661,25 +632,26 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
   const int* vo = c->cg_buf[2].as<int>();
   const int nb = blocks_for(c, pb.nvox, 256);
   const float r2 = ri * ri;
-  const size_t nnn_b = (size_t)blocks_for(c, (long long)nnn, 256);
+  const int nnn_b = blocks_for(c, (long long)nnn, 256);
+  const T lam = (T)lambda;
   auto iteration = [&]() -> int {
     // DELSQ = sum CB^2
     SPI_CUDA(cudaMemsetAsync(&sc->delsq, 0, sizeof(double), c->stream));
-    dot_kernel<<<nb, 256, 0, c->stream>>>(cb, cb, runs, vr, vo, pb.nvox, &sc->delsq);
-    dir_update_kernel<<<nb, 256, 0, c->stream>>>(bckp, cb, runs, vr, vo, pb.nvox, sc);
+    dot_kernel<T><<<nb, 256, 0, c->stream>>>(cb, cb, runs, vr, vo, pb.nvox, &sc->delsq);
+    dir_update_kernel<T><<<nb, 256, 0, c->stream>>>(bckp, cb, runs, vr, vo, pb.nvox, sc);
     scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
-    SPI_TRY(launch_project(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
-    SPI_TRY(launch_backproject(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
-    zero_outside_kernel<<<(int)nnn_b, 256, 0, c->stream>>>(bckp, n, pb.ldp, r2);
+    SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
+    SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
+    zero_outside_kernel<T><<<nnn_b, 256, 0, c->stream>>>(bckp, n, pb.ldp, r2);
     for (int axis = 0; axis < 3; ++axis)
-      fixedge_axis_kernel<<<(n * n + 127) / 128, 128, 0, c->stream>>>(bckp, n, axis, mode);
-    regularize_kernel<<<nb, 256, 0, c->stream>>>(bcke, bckp, runs, vr, vo, pb.nvox, n, lambda, mode);
+      fixedge_axis_kernel<T><<<(n * n + 127) / 128, 128, 0, c->stream>>>(bckp, n, axis, mode);
+    regularize_kernel<T><<<nb, 256, 0, c->stream>>>(bcke, bckp, runs, vr, vo, pb.nvox, n, lam, mode);
     SPI_CUDA(cudaMemsetAsync(&sc->akden, 0, sizeof(double), c->stream));
-    dot_kernel<<<nb, 256, 0, c->stream>>>(bckp, bcke, runs, vr, vo, pb.nvox, &sc->akden);
+    dot_kernel<T><<<nb, 256, 0, c->stream>>>(bckp, bcke, runs, vr, vo, pb.nvox, &sc->akden);
     scal_step_kernel<<<1, 32, 0, c->stream>>>(sc);
-    step_kernel<<<nb, 256, 0, c->stream>>>(bckn, cb, bckp, bcke, runs, vr, vo, pb.nvox, sc);
+    step_kernel<T><<<nb, 256, 0, c->stream>>>(bckn, cb, bckp, bcke, runs, vr, vo, pb.nvox, sc);
     SPI_TRY(check_kernel("cg iteration"));
     c->count(9);
     return 0;
@@ -688,14 +660,18 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = getenv("SPI_CG_NOGRAPH") == nullptr;
-  if (use_graph) {
-    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) use_graph = false;
+  if (use_graph && cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    use_graph = false;
+    cudaGetLastError();
   }
   if (use_graph) {
-    long long before = c->launches;
-    int st = iteration();
-    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
-    if (st != 0) return st;
+    const long long before = c->launches;
+    const int st = iteration();
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (st != 0) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
     if (e != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
       graph = nullptr;
@@ -704,10 +680,7 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
     }
     c->launches = before;  // counted per replay below
   }
-  const long long per_iter_launches = [&]() {
-    long long k = 13 + (lo + 63) / 64 + 1;
-    return k;
-  }();
+  const long long per_iter_launches = 14 + bp_kernel_count(lo);
   int done = 0;
   for (int iter = 1; iter <= maxit; ++iter) {
     if (use_graph) {
@@ -730,9 +703,96 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   if (niter_out) *niter_out = done;
-  SPI_CUDA(cudaMemcpyAsync(vol_out, bckn, vb, cudaMemcpyDeviceToHost, c->stream));
+  // BCKN -> float volume (staged in the float projection buffer)
+  if (sizeof(T) == sizeof(float)) {
+    SPI_CUDA(cudaMemcpyAsync(vol_out, bckn, nnn * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    std::vector<T> tmp(nnn);
+    SPI_CUDA(cudaMemcpyAsync(tmp.data(), bckn, vb, cudaMemcpyDeviceToHost, c->stream));
+    SPI_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < nnn; ++i) vol_out[i] = (float)tmp[i];
+  }
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
+}
+
+}  // namespace spi
+
+using namespace spi;
+
+extern "C" {
+
+int spi_ctx_set_cg_precision(spi_ctx* c, int fp64) {
+  if (!c) return fail(kInvalid, "NULL context");
+  c->cg_fp64 = fp64 ? 1 : 0;
+  return 0;
+}
+
+int spi_cg_project(spi_ctx* c, const float* vol, int n, float ri, const float* angles, int nang, float* projs,
+                   int on_device) {
+  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_project: bad arguments");
+  if (n < 8) return fail(kInvalid, "spi_cg_project: n = %d too small", n);
+  SPI_CUDA(cudaSetDevice(c->device));
+  CgProblem pb;
+  SPI_TRY(cg_setup(c, n, ri, pb));
+  std::vector<CgDM> dms;
+  dms_from_angles(angles, nang, dms);
+  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
+  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
+  const float* dv = vol;
+  float* dp = projs;
+  if (!on_device) {
+    SPI_TRY(c->cg_buf[4].ensure(vb));
+    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
+    SPI_CUDA(cudaMemcpyAsync(c->cg_buf[4].p, vol, vb, cudaMemcpyHostToDevice, c->stream));
+    dv = c->cg_buf[4].as<float>();
+    dp = c->cg_buf[5].as<float>();
+  }
+  SPI_TRY(launch_project<float>(c, pb, dv, c->cg_buf[3].as<CgDM>(), nang, dp));
+  if (!on_device && pbytes) SPI_CUDA(cudaMemcpyAsync(projs, dp, pbytes, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_cg_backproject(spi_ctx* c, const float* projs, int n, float ri, const float* angles, int nang, float* vol,
+                       int on_device) {
+  if (!c || !vol || !projs || (nang > 0 && !angles)) return fail(kInvalid, "spi_cg_backproject: bad arguments");
+  if (n < 8) return fail(kInvalid, "spi_cg_backproject: n = %d too small", n);
+  SPI_CUDA(cudaSetDevice(c->device));
+  CgProblem pb;
+  SPI_TRY(cg_setup(c, n, ri, pb));
+  std::vector<CgDM> dms;
+  dms_from_angles(angles, nang, dms);
+  const size_t vb = (size_t)n * n * n * sizeof(float), pbytes = (size_t)nang * n * n * sizeof(float);
+  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
+  const float* dp = projs;
+  float* dv = vol;
+  if (!on_device) {
+    SPI_TRY(c->cg_buf[4].ensure(vb));
+    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pbytes, 4)));
+    if (pbytes) SPI_CUDA(cudaMemcpyAsync(c->cg_buf[5].p, projs, pbytes, cudaMemcpyHostToDevice, c->stream));
+    dv = c->cg_buf[4].as<float>();
+    dp = c->cg_buf[5].as<float>();
+  }
+  SPI_CUDA(cudaMemsetAsync(dv, 0, vb, c->stream));
+  SPI_TRY(launch_backproject<float>(c, pb, dv, dp, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  if (!on_device) SPI_CUDA(cudaMemcpyAsync(vol, dv, vb, cudaMemcpyDeviceToHost, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
+             int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out) {
+  if (!c || !projs || !angles || !vol_out) return fail(kInvalid, "spi_bpcg: NULL argument");
+  if (n < 8 || nang <= 0) return fail(kInvalid, "spi_bpcg: n = %d, nang = %d", n, nang);
+  if (mode < 1 || mode > 3) return fail(kInvalid, "spi_bpcg: mode %d must be 1, 2 or 3", mode);
+  SPI_CUDA(cudaSetDevice(c->device));
+  if (niter_out) *niter_out = 0;
+  if (c->cg_fp64)
+    return bpcg_run<double>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out);
+  return bpcg_run<float>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out);
 }
 
 }  // extern "C"

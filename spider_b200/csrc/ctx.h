@@ -15,6 +15,9 @@ struct spi_ctx {
   bool pending_sym0[2] = {false, false};
   bool merged = false;
   int bf16 = 0;
+  int insert_mode = 1;                // 0 = tile-privatised, 1 = direct per-tap atomics
+  int slice_order = 1;                // 1 = order slices of a chunk by plane normal
+  int cg_fp64 = 1;                    // BP CG vectors/projections in FP64 (1) or FP32 (0)
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT
   spi::KBTab kb;

@@ -168,8 +168,8 @@ static int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* 
   SPI_TRY(c->pj_runs.ensure(std::max<size_t>(1, runs.size()) * sizeof(PjRun)));
   SPI_TRY(c->pj_dm.ensure(dms.size() * sizeof(PjDM)));
   if (!runs.empty())
-    SPI_CUDA(cudaMemcpy(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice));
-  SPI_CUDA(cudaMemcpy(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice));
+    SPI_CUDA(cudaMemcpyAsync(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice, c->stream));
   *nruns_out = (int)runs.size();
   return 0;
 }

@@ -262,11 +262,14 @@ def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
 
 
 def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-         ctx: Context | None = None):
+         ctx: Context | None = None, fp64: bool = True):
     """``BP CG`` (linear interpolation).  Prompts in reference order: radius
     (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
+    ``fp64`` keeps the CG vectors and projections in FP64 (default) instead
+    of the reference's REAL.
     Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
     ctx = ctx or default_context()
+    check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, 1 if fp64 else 0))
     projs = _host_f32(projs)
     n = _nx_of(projs)
     if ri is None:

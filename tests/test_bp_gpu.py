@@ -157,3 +157,22 @@ def test_bp3f_config1_full(ctx, orc):
     g = np.arange(64) - 32
     m = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= 28 ** 2
     assert np.corrcoef(got[m], vol[m])[0, 1] > 0.98
+
+
+def test_insert_kernels_agree(ctx, orc):
+    """The tile-privatised insertion and the direct per-tap insertion add the
+    same taps; they differ only in FP32 summation order."""
+    nx, nimg = 48, 300
+    _, pr, ang = _case(nx, nimg, 61)
+    # include orientations that put the x = 0 flip line inside many tiles
+    ang[:40, 1] = 90.0
+    direct = ops.bp3f(pr, ang, ctx=ctx)
+    os.environ["SPI_INSERT"] = "tile"
+    try:
+        tile = ops.bp3f(pr, ang, ctx=ctx)
+    finally:
+        del os.environ["SPI_INSERT"]
+    ref = orc.bp3f(pr, ang, prec=1, nthreads=1)
+    assert synth.rel_l2(tile, direct) <= 2e-6
+    assert synth.rel_l2(tile, ref) <= TOL
+    assert synth.rel_l2(direct, ref) <= TOL

@@ -71,11 +71,23 @@ def test_bpcg_matches_fp64_oracle(ctx, orc, mode):
     ref32, _, _, _ = orc.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=12, mode=mode, lam=0.5, prec=0)
     e64 = synth.rel_l2(vol, ref64)
     e32 = synth.rel_l2(vol, ref32)
-    print(f"BP CG mode {mode}: rel-err vs FP64 oracle {e64:.3e}, vs FP32 oracle {e32:.3e}, iters {len(log)}")
+    d_ref = synth.rel_l2(ref32, ref64)
+    print(f"BP CG mode {mode}: rel-err vs FP64 oracle {e64:.3e} (FP32 oracle vs FP64 oracle {d_ref:.3e}), "
+          f"vs FP32 oracle {e32:.3e}, iters {len(log)}")
     assert len(log) == len(rlog64)
     assert e64 <= 1e-4
-    assert e32 <= 1e-4
-    np.testing.assert_allclose(log[:, 1], rlog64[:, 1], rtol=1e-3)
+    np.testing.assert_allclose(log[:, 1], rlog64[:, 1], rtol=1e-4)
+
+
+def test_bpcg_fp32_mode_matches_fp32_oracle(ctx, orc):
+    """With REAL vectors (the reference's storage) one iteration agrees with
+    the FP32 oracle; over many iterations both drift from the exact solution
+    at their own rates, so only the first iteration is compared."""
+    n, nang = 32, 80
+    _, pr, ang = _data(n, nang, 77, snr=1.0)
+    vol, _ = ops.bpcg(pr, ang, 13.0, errm=1e-9, maxit=1, mode=1, lam=0.5, ctx=ctx, fp64=False)
+    ref, _, _, _ = orc.bpcg(pr, ang, 13.0, errm=1e-9, maxit=1, mode=1, lam=0.5, prec=0)
+    assert synth.rel_l2(vol, ref) <= 1e-5
 
 
 def test_bpcg_duplicate_angles_and_stop(ctx, orc):
