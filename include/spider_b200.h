@@ -150,6 +150,25 @@ int spi_bp32f(spi_ctx* ctx, const float* imgs, int nx, int nang, const float* an
 int spi_pj3q(spi_ctx* ctx, const float* vol, int nx, int ny, int nz, float ri,
              const float* angles, int nang, float* proj_out, int on_device);
 
+/* PJ 3Q that allocates nothing -- no counterpart in the reference; an
+ * addition for callers that must not allocate device memory: applications
+ * whose device memory belongs to a fixed arena or caching allocator, and
+ * latency-critical pipelines that cannot take cudaMalloc/cudaFree's implicit
+ * synchronisation.  Same result as spi_pj3q (up to the order of its FP32
+ * atomic sums).  vol (float[nz*ny*nx]), angles (float[3*nang]: psi, theta,
+ * phi) and proj_out (float[nang*ny*nx]) are device pointers on the current
+ * device; work is queued on `stream` (cudaStream_t, NULL = legacy stream) and
+ * the call returns without waiting for it.  Its scratch (voxel runs and
+ * rotation matrices) is one file-scope __device__ array of 1,114,112 bytes,
+ * which every GPU that loads the library holds until exit; hence the limits
+ * ny*nz <= 65536 and nang <= 16384 per call (larger requests return 101).
+ * The first call on a device looks up that array's device address, so make
+ * it before any stream capture.  Every call shares the array and overwrites
+ * it, so calls that overlap on the GPU (different streams, or different host
+ * threads on the same device) race; serialise them. */
+int spi_pj3q_noalloc(const float* vol, int nx, int ny, int nz, float ri, const float* angles,
+                     int nang, float* proj_out, void* stream);
+
 /* Exact adjoint of spi_pj3q: scatters projections back into a volume with
  * the transposed trilinear weights (vol_out is overwritten). */
 int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, float ri,

@@ -243,3 +243,179 @@ int spi_pj3q_adjoint(spi_ctx* c, const float* projs, int nx, int ny, int nz, flo
 }
 
 }  // extern "C"
+
+// ============================================================================
+// PJ 3Q without any allocation.
+//
+// For callers that must not allocate device memory themselves or through a
+// library: applications whose device memory is owned by a fixed arena or a
+// caching allocator that must not be bypassed, and latency-critical pipelines
+// that cannot absorb the implicit device synchronisation of cudaMalloc and
+// cudaFree.  spi_pj3q keeps its voxel runs and rotation matrices in context
+// buffers from cudaMalloc; this variant keeps them in one file-scope
+// __device__ array of fixed size (kNoAllocBytes, held by every GPU that loads
+// the library until the process exits) and takes all inputs and outputs as
+// caller-owned device pointers.
+#include <mutex>
+
+namespace spi {
+
+constexpr int kNoAllocMaxLines = 65536;  // ny * nz lines of voxels along x
+constexpr int kNoAllocMaxAng = 16384;    // projections per call
+struct NoAllocScratch {
+  int2 lines[kNoAllocMaxLines];          // first/last x (1-based) of the sphere on each (y, z) line
+  PjDM dms[kNoAllocMaxAng];              // rotation matrix per projection
+};
+constexpr size_t kNoAllocBytes = sizeof(NoAllocScratch);  // 1,114,112 bytes
+
+static __device__ __align__(256) unsigned char g_pj3q_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[256] = {};
+
+// Device address of g_pj3q_scratch on the current device, looked up once per
+// device (the host-side name is only a stand-in for the symbol).
+static int noalloc_scratch(NoAllocScratch** out) {
+  int dev = -1;
+  SPI_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(kDevice, "spi_pj3q_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pj3q_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(kCuda, "spi_pj3q_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<NoAllocScratch*>(g_noalloc_addr[dev]);
+  return 0;
+}
+
+// CANG in FP64 on the device (WPRO_N's inline matrix, wpro_n.f:65-81)
+__global__ void noalloc_dm_kernel(const float* __restrict__ angles, int nang, PjDM* __restrict__ dms) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nang) return;
+  const double d2r = (double)3.14159265358979323846f / 180.0;
+  const double psi = (double)angles[3 * a] * d2r, theta = (double)angles[3 * a + 1] * d2r,
+               phi = (double)angles[3 * a + 2] * d2r;
+  const double cphi = cos(phi), sphi = sin(phi), cthe = cos(theta), sthe = sin(theta), cpsi = cos(psi),
+               spsi = sin(psi);
+  float* d = dms[a].d;
+  d[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+  d[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+  d[2] = (float)(-sthe * cpsi);
+  d[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+  d[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+  d[5] = (float)(sthe * spsi);
+  d[6] = (float)(sthe * cphi);
+  d[7] = (float)(sthe * sphi);
+  d[8] = (float)(cthe);
+}
+
+// PREPCUB's run of line (y, z): first and last x inside radius ri (x2 < x1 when empty)
+__global__ void noalloc_lines_kernel(int nx, int ny, int nz, float ri, int ldpx, int ldpy, int ldpz,
+                                     int2* __restrict__ lines) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= ny * nz) return;
+  const int i2 = l % ny + 1, i1 = l / ny + 1;
+  const float r = __fmul_rn(ri, ri);
+  const float t = (float)(i1 - ldpz);
+  const float xx = __fmul_rn(t, t);
+  const float t2 = (float)(i2 - ldpy);
+  const float yy = __fadd_rn(__fmul_rn(t2, t2), xx);
+  int first = 0, last = -1;
+  for (int i3 = 1; i3 <= nx; ++i3) {
+    const float t3 = (float)(i3 - ldpx);
+    const float rc = __fadd_rn(__fmul_rn(t3, t3), yy);
+    if (rc <= r) {
+      if (first == 0) first = i3;
+      last = i3;
+    }
+  }
+  lines[l] = make_int2(first, first ? last : -1);
+}
+
+// The WPRO_N walk of wpro_kernel, reading its runs and matrices from the
+// scratch array; one thread per (projection, line).
+__global__ void __launch_bounds__(128) noalloc_wpro_kernel(const float* __restrict__ cube, int nsam, int nrow,
+                                                           int nslice, const NoAllocScratch* __restrict__ sc,
+                                                           int nang, int ldpx, int ldpy, int ldpz,
+                                                           float* __restrict__ out) {
+  const int nlines = nrow * nslice;
+  const long long total = (long long)nlines * nang;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nlines);
+    const int l = (int)(t % nlines);
+    const int2 run = sc->lines[l];
+    if (run.y < run.x) continue;
+    const PjRun r{run.x, run.y, run.x - ldpx, l % nrow + 1 - ldpy, l / nrow + 1 - ldpz};
+    const PjDM dm = sc->dms[a];
+    float* b = out + (size_t)a * nsam * nrow;
+    const int k = r.y + ldpy;
+    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
+    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
+    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+    for (int j = r.i1; j <= r.i2; ++j) {
+      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
+        const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
+        const float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
+        const float c000 = __ldg(c0), c100 = __ldg(c0 + 1), c010 = __ldg(c0 + sy), c110 = __ldg(c0 + sy + 1);
+        const float c001 = __ldg(c0 + sz), c101 = __ldg(c0 + sz + 1), c011 = __ldg(c0 + sz + sy),
+                    c111 = __ldg(c0 + sz + sy + 1);
+        const float a1 = c000;
+        const float a2 = __fsub_rn(c100, a1);
+        const float a3 = __fsub_rn(c010, a1);
+        const float a4 = __fsub_rn(c001, a1);
+        const float a5 = __fadd_rn(__fsub_rn(-a2, c010), c110);
+        const float a61 = __fadd_rn(-c001, c101);
+        const float a6 = __fadd_rn(-a2, a61);
+        const float a7 = __fadd_rn(__fsub_rn(-a3, c001), c011);
+        const float a8 = __fadd_rn(__fsub_rn(__fsub_rn(-a5, a61), c011), c111);
+        const float inner = __fadd_rn(__fadd_rn(a4, __fmul_rn(a6, dx)), __fmul_rn(__fadd_rn(a7, __fmul_rn(a8, dx)), dy));
+        float v = __fadd_rn(a1, __fmul_rn(dz, inner));
+        v = __fadd_rn(v, __fmul_rn(a3, dy));
+        v = __fadd_rn(v, __fmul_rn(dx, __fadd_rn(a2, __fmul_rn(a5, dy))));
+        atomicAdd(b + (size_t)(k - 1) * nsam + (j - 1), v);
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[1]);
+      zb = __fadd_rn(zb, dm.d[2]);
+    }
+  }
+}
+
+}  // namespace spi
+
+extern "C" int spi_pj3q_noalloc(const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
+                                float* proj_out, void* stream) {
+  using namespace spi;
+  if (!vol || !proj_out || (nang > 0 && !angles)) return fail(kInvalid, "spi_pj3q_noalloc: NULL pointer");
+  if (nx < 4 || ny < 4 || nz < 4) return fail(kInvalid, "spi_pj3q_noalloc: volume %dx%dx%d too small", nx, ny, nz);
+  if ((long long)ny * nz > kNoAllocMaxLines)
+    return fail(kInvalid, "spi_pj3q_noalloc: ny*nz = %lld exceeds the fixed scratch limit of %d lines",
+                (long long)ny * nz, kNoAllocMaxLines);
+  if (nang < 0 || nang > kNoAllocMaxAng)
+    return fail(kInvalid, "spi_pj3q_noalloc: nang = %d exceeds the fixed scratch limit of %d projections", nang,
+                kNoAllocMaxAng);
+  if (!(ri > 0.0f)) return fail(kInvalid, "spi_pj3q_noalloc: radius %g must be positive", (double)ri);
+  NoAllocScratch* sc = nullptr;
+  SPI_TRY(noalloc_scratch(&sc));
+  if (nang == 0) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int ldpx = nx / 2 + 1, ldpy = ny / 2 + 1, ldpz = nz / 2 + 1;
+  noalloc_dm_kernel<<<(nang + 127) / 128, 128, 0, st>>>(angles, nang, sc->dms);
+  SPI_TRY(check_kernel("noalloc_dm_kernel"));
+  noalloc_lines_kernel<<<(ny * nz + 127) / 128, 128, 0, st>>>(nx, ny, nz, ri, ldpx, ldpy, ldpz, sc->lines);
+  SPI_TRY(check_kernel("noalloc_lines_kernel"));
+  SPI_CUDA(cudaMemsetAsync(proj_out, 0, (size_t)nang * nx * ny * sizeof(float), st));
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long total = (long long)ny * nz * nang;
+  const int blocks = (int)std::min<long long>((total + 127) / 128, (long long)nsm * 16);
+  noalloc_wpro_kernel<<<blocks, 128, 0, st>>>(vol, nx, ny, nz, sc, nang, ldpx, ldpy, ldpz, proj_out);
+  SPI_TRY(check_kernel("noalloc_wpro_kernel"));
+  return 0;
+}
