@@ -83,7 +83,7 @@ int spi_ctx_timing(spi_ctx* ctx, double* ms_out, long long* count_out);
  * ------------------------------------------------------------------ */
 
 /* Allocate and zero `ngrids` (1 = BP 3F, 2 = BP 32F) Fourier grids for box
- * size nx (even, 8 <= nx <= 512) and set the symmetry list (sym_angles may
+ * size nx (8 <= nx <= 512) and set the symmetry list (sym_angles may
  * be NULL when nsym <= 1).  Replaces the grid setup of BP3F (bp3f.f:160-178,
  * 386-394) and BP32F (bp32f.f:163-179, 490-500). */
 int spi_bp_open(spi_ctx* ctx, int nx, int ngrids, const float* sym_angles, int nsym);
@@ -108,6 +108,14 @@ int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
  * device memory (`imgs_on_device`). */
 int spi_bp_insert(spi_ctx* ctx, const float* imgs, int nimg, const float* angles,
                   const uint8_t* half, int imgs_on_device);
+
+/* RB 3F / RB 32F insertion: as spi_bp_insert, after rotating and shifting
+ * every image with RTSQ (rtsq.f:56-140, quadratic interpolation) by its
+ * angle-document registers 6-8: inplane = float[nimg*3] (in-plane angle in
+ * degrees, x shift, y shift), host memory.  Replaces the CALLRTSQ branch of
+ * the BP3FQ / BP32FQ image loop (bp3f.f:406-425, bp32f.f:816-848). */
+int spi_bp_insert_rb(spi_ctx* ctx, const float* imgs, int nimg, const float* angles,
+                     const float* inplane, const uint8_t* half, int imgs_on_device);
 
 /* Finish the open grids: SYMPLANE0 (bp32f.f:1051-1088), NRMW2
  * (bp3f.f:1347-1371), inverse FFT (fmrs_3.f:54-59) and WINDKB2A

@@ -54,6 +54,12 @@ def lib():
                                _u8p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
                                _f64p, _f64p, ctypes.c_int]
         L.orc_bp3f.restype = ctypes.c_int
+        L.orc_rb3f.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _u8p, ctypes.c_int,
+                               _f32p, _f32p, _f32p, ctypes.c_int]
+        L.orc_rb3f.restype = ctypes.c_int
+        L.orc_symvol.argtypes = [_f32p, _f32p, ctypes.c_int, _f32p, ctypes.c_int]
+        L.orc_rtsq.argtypes = [_f32p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_float]
         L.orc_bp_insert_only.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _f32p, _u8p, ctypes.c_int]
         L.orc_bp_insert_only.restype = ctypes.c_int
         L.orc_bp_session_open.argtypes = [ctypes.c_int]
@@ -176,6 +182,40 @@ def bp32f(imgs, angles, half, *, sym=None, prec=0, nthreads=0):
     if rc != 0:
         raise RuntimeError(f"oracle bp32f failed: {rc}")
     return tuple(vols)
+
+
+def symvol(vol, sym):
+    """SYMVOL (symvol.f:39-180): sum of the volume rotated by each symmetry."""
+    vol = _f32(vol)
+    sa = _f32(sym)
+    out = np.zeros_like(vol)
+    lib().orc_symvol(_p(vol, _f32p), _p(out, _f32p), vol.shape[0], _p(sa, _f32p), sa.shape[0])
+    return out
+
+
+def rtsq(img, theta, shx, shy):
+    """RTSQ (rtsq.f:56-140) of one image [ny, nx]: rotate by theta degrees, shift."""
+    img = _f32(img)
+    out = np.zeros_like(img)
+    lib().orc_rtsq(_p(img, _f32p), _p(out, _f32p), img.shape[1], img.shape[0], theta, shx, shy)
+    return out
+
+
+def rb3f(imgs, angles, inplane, half=None, *, prec=0, nthreads=0):
+    """RB 3F / RB 32F: RTSQ with inplane [n, 3] = (angle, sx, sy), then BP 3F (half None)
+    or BP 32F (returns three volumes)."""
+    imgs = _f32(imgs)
+    ang = _f32(angles)
+    ip = _f32(inplane)
+    nang, nx = imgs.shape[0], imgs.shape[1]
+    vols = [np.zeros((nx, nx, nx), np.float32) for _ in range(3)]
+    h = None if half is None else np.ascontiguousarray(half, dtype=np.uint8)
+    rc = lib().orc_rb3f(_p(imgs, _f32p), nx, nang, _p(ang, _f32p), _p(ip, _f32p), _p(h, _u8p), prec,
+                        _p(vols[0], _f32p), _p(vols[1], _f32p) if h is not None else None,
+                        _p(vols[2], _f32p) if h is not None else None, nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle rb3f failed: {rc}")
+    return vols[0] if h is None else tuple(vols)
 
 
 def bp32f_insert_only(imgs, angles, half, *, nthreads=0):

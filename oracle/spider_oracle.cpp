@@ -251,6 +251,71 @@ void stage_image(const float* proj, int nx, std::vector<std::complex<R>>& bi,
   }
 }
 
+// QUADRI (quadri.f:83-150): quadratic interpolation with circular closure.
+// f is FDATA(NX,NY) column-major (x fastest); x, y are 1-based.
+float quadri(float xx, float yy, int nx, int ny, const float* f) {
+  float x = xx, y = yy;
+  if (x < 1.0f) x = x + (float)((1 - ifix(x) / nx) * nx);
+  if (x > (float)nx + 0.5f) x = std::fmod(x - 1.0f, (float)nx) + 1.0f;
+  if (y < 1.0f) y = y + (float)((1 - ifix(y) / ny) * ny);
+  if (y > (float)ny + 0.5f) y = std::fmod(y - 1.0f, (float)ny) + 1.0f;
+  const int i = ifix(x), j = ifix(y);
+  const float dx0 = x - (float)i, dy0 = y - (float)j;
+  int ip1 = i + 1, im1 = i - 1, jp1 = j + 1, jm1 = j - 1;
+  if (ip1 > nx) ip1 -= nx;
+  if (im1 < 1) im1 += nx;
+  if (jp1 > ny) jp1 -= ny;
+  if (jm1 < 1) jm1 += ny;
+  auto F = [&](int a, int b) { return f[(size_t)(b - 1) * nx + (a - 1)]; };
+  const float f0 = F(i, j);
+  const float c1 = F(ip1, j) - f0;
+  const float c2 = (c1 - f0 + F(im1, j)) * 0.5f;
+  const float c3 = F(i, jp1) - f0;
+  const float c4 = (c3 - f0 + F(i, jm1)) * 0.5f;
+  const float dxb = dx0 - 1.0f, dyb = dy0 - 1.0f;
+  const float hxc = (float)(int)std::copysign(1.0f, dx0);   // HXC, HYC are REAL
+  const float hyc = (float)(int)std::copysign(1.0f, dy0);
+  int ic = (int)((float)i + hxc), jc = (int)((float)j + hyc);
+  if (ic > nx) ic -= nx; else if (ic < 1) ic += nx;
+  if (jc > ny) jc -= ny; else if (jc < 1) jc += ny;
+  const float c5 = ((F(ic, jc) - f0 - hxc * c1 - (hxc * (hxc - 1.0f)) * c2 - hyc * c3 - (hyc * (hyc - 1.0f)) * c4) *
+                    (hxc * hyc));
+  return f0 + dx0 * (c1 + dxb * c2 + dy0 * c5) + dy0 * (c3 + dyb * c4);
+}
+
+// RTSQ (rtsq.f:56-140): rotate by THETA degrees (SCLI = 1) and shift, with
+// QUADRI interpolation; cod/sid are COS/SIN(THETA*DGR_TO_RAD) in REAL.
+void rtsq(const float* in, float* out, int nx, int ny, float theta, float shxi, float shyi) {
+  const float quadpi = 3.14159265358979323846f;
+  const float dgr_to_rad = quadpi / 180.0f;
+  const float shx = std::fmod(shxi, (float)nx), shy = std::fmod(shyi, (float)ny);
+  const int iycen = ny / 2 + 1, ixcen = nx / 2 + 1;
+  float rx1 = (float)(-nx / 2), rx2 = (float)(nx / 2), ry1 = (float)(-ny / 2), ry2 = (float)(ny / 2);
+  float rxe1, rxe2, rye1, rye2;
+  if (nx % 2 == 0) { rx2 = rx2 - 1.0f; rxe1 = (float)-nx; rxe2 = (float)nx; }
+  else { rxe1 = (float)(-nx - 1); rxe2 = (float)(nx + 1); }
+  if (ny % 2 == 0) { ry2 = ry2 - 1.0f; rye1 = (float)-ny; rye2 = (float)ny; }
+  else { rye1 = (float)(-ny - 1); rye2 = (float)(ny + 1); }
+  const float cod = std::cos(theta * dgr_to_rad), sid = std::sin(theta * dgr_to_rad);
+  const float coddscli = cod / 1.0f, siddscli = sid / 1.0f;
+  const float fixcenmshx = (float)(-ixcen) - shx, fiycenmshy = (float)(-iycen) - shy;
+  for (int iy = 1; iy <= ny; ++iy) {
+    float yi = (float)iy + fiycenmshy;
+    if (yi < ry1) yi = std::min(yi + rye2, ry2);
+    if (yi > ry2) yi = std::max(yi + rye1, ry1);
+    const float ycod = yi * coddscli + (float)iycen;
+    const float ysid = -yi * siddscli + (float)ixcen;
+    for (int ix = 1; ix <= nx; ++ix) {
+      float xi = (float)ix + fixcenmshx;
+      if (xi < rx1) xi = std::min(xi + rxe2, rx2);
+      if (xi > rx2) xi = std::max(xi + rxe1, rx1);
+      const float yold = xi * siddscli + ycod;
+      const float xold = xi * coddscli + ysid;
+      out[(size_t)(iy - 1) * nx + (ix - 1)] = quadri(xold, yold, nx, ny, in);
+    }
+  }
+}
+
 // ONELINE, oneline.f:38-200 (called as ONELINE(J,N2,NX,...), bp3f.f:477:
 // callee N = 2*NX, callee N2 = NX)
 template <class R>
@@ -483,6 +548,89 @@ void finish_volume(Grid<R>& g, const KBTable& kb, float* vol) {
       }
 }
 
+// TRIQUAD (triquad.f): triquadratic interpolation on a 3x3x3 neighbourhood.
+// r, s, t are DOUBLE; the products and the 27-term sum are REAL, left to right.
+float triquad(double r, double s, double t, const float* f) {
+  const float c2 = 1.0f / 2.0f, c4 = 1.0f / 4.0f, c8 = 1.0f / 8.0f;
+  const float rs = (float)(r * s), st = (float)(s * t), rt = (float)(r * t);
+  const float rst = (float)(r * (double)st);
+  const float rsq = (float)(1.0 - r * r), ssq = (float)(1.0 - s * s), tsq = (float)(1.0 - t * t);
+  const float rm1 = (float)(1.0 - r), sm1 = (float)(1.0 - s), tm1 = (float)(1.0 - t);
+  const float rp1 = (float)(1.0 + r), sp1 = (float)(1.0 + s), tp1 = (float)(1.0 + t);
+  const float R = (float)r, S = (float)s, T = (float)t;
+  float v = (-c8) * rst * rm1 * sm1 * tm1 * f[0];
+  v = v + (c4) * st * rsq * sm1 * tm1 * f[1];
+  v = v + (c8) * rst * rp1 * sm1 * tm1 * f[2];
+  v = v + (c4) * rt * rm1 * ssq * tm1 * f[3];
+  v = v + (-c2) * T * rsq * ssq * tm1 * f[4];
+  v = v + (-c4) * rt * rp1 * ssq * tm1 * f[5];
+  v = v + (c8) * rst * rm1 * sp1 * tm1 * f[6];
+  v = v + (-c4) * st * rsq * sp1 * tm1 * f[7];
+  v = v + (-c8) * rst * rp1 * sp1 * tm1 * f[8];
+  v = v + (c4) * rs * rm1 * sm1 * tsq * f[9];
+  v = v + (-c2) * S * rsq * sm1 * tsq * f[10];
+  v = v + (-c4) * rs * rp1 * sm1 * tsq * f[11];
+  v = v + (-c2) * R * rm1 * ssq * tsq * f[12];
+  v = v + rsq * ssq * tsq * f[13];
+  v = v + (c2) * R * rp1 * ssq * tsq * f[14];
+  v = v + (-c4) * rs * rm1 * sp1 * tsq * f[15];
+  v = v + (c2) * S * rsq * sp1 * tsq * f[16];
+  v = v + (c4) * rs * rp1 * sp1 * tsq * f[17];
+  v = v + (c8) * rst * rm1 * sm1 * tp1 * f[18];
+  v = v + (-c4) * st * rsq * sm1 * tp1 * f[19];
+  v = v + (-c8) * rst * rp1 * sm1 * tp1 * f[20];
+  v = v + (-c4) * rt * rm1 * ssq * tp1 * f[21];
+  v = v + (c2) * T * rsq * ssq * tp1 * f[22];
+  v = v + (c4) * rt * rp1 * ssq * tp1 * f[23];
+  v = v + (-c8) * rst * rm1 * sp1 * tp1 * f[24];
+  v = v + (c4) * st * rsq * sp1 * tp1 * f[25];
+  v = v + (c8) * rst * rp1 * sp1 * tp1 * f[26];
+  return v;
+}
+
+// SYMVOL, SP_MP branch (symvol.f:39-180): q2 = sum over symmetries of q1
+// rotated by RM (column-major 3x3 per symmetry) with TRIQDF inside radius
+// sqrt(IRADI), q1 itself outside.  Volumes nx^3, x fastest; coordinates are
+// centred (KLX = -nx/2 .. KNX).
+void symvol(const float* q1, float* q2, int nx, const float* rm, int nsym) {
+  const int klx = -nx / 2, knx = (nx % 2 == 0) ? nx / 2 - 1 : nx / 2;
+  const int mn = std::min(std::abs(klx), std::abs(knx));
+  const int iradi = (mn - 1) * (mn - 1);
+  auto Q1 = [&](int ix, int iy, int iz) { return q1[((size_t)(iz - klx) * nx + (iy - klx)) * nx + (ix - klx)]; };
+  const size_t nv = (size_t)nx * nx * nx;
+  std::fill(q2, q2 + nv, 0.0f);
+  for (int is = 0; is < nsym; ++is) {
+    const float* R = rm + 9 * is;   // RM(i,j) = R[(i-1) + 3(j-1)]
+    const bool ident = R[0] == 1.0f && R[4] == 1.0f && R[8] == 1.0f;
+    for (int iz = klx; iz <= knx; ++iz)
+      for (int iy = klx; iy <= knx; ++iy) {
+        const double qrt0 = (double)(R[1] * (float)iy + R[2] * (float)iz);
+        const double qrt1 = (double)(R[4] * (float)iy + R[5] * (float)iz);
+        const double qrt2 = (double)(R[7] * (float)iy + R[8] * (float)iz);
+        for (int ix = klx; ix <= knx; ++ix) {
+          float& o = q2[((size_t)(iz - klx) * nx + (iy - klx)) * nx + (ix - klx)];
+          if (ident) { o = o + Q1(ix, iy, iz); continue; }
+          const int icrd = ix * ix + iy * iy + iz * iz;
+          if (icrd <= iradi) {
+            const double qr0 = qrt0 + (double)(R[0] * (float)ix);
+            const double qr1 = qrt1 + (double)(R[3] * (float)ix);
+            const double qr2 = qrt2 + (double)(R[6] * (float)ix);
+            const int iox = (int)std::floor(qr0), ioy = (int)std::floor(qr1), ioz = (int)std::floor(qr2);
+            const double dx = qr0 - iox, dy = qr1 - ioy, dz = qr2 - ioz;
+            float f[27];
+            for (int l = 0; l < 27; ++l) {
+              const int X = l % 3 - 1, Y = (l / 3) % 3 - 1, Z = l / 9 - 1;
+              f[l] = Q1(iox + X, ioy + Y, ioz + Z);
+            }
+            o = o + triquad(dx, dy, dz, f);
+          } else {
+            o = o + Q1(ix, iy, iz);
+          }
+        }
+      }
+  }
+}
+
 // BP3FQ image loop (bp3f.f:298-515) / BP32FQ (bp32f.f:433-939): every image
 // is staged and inserted row by row into grid `route[img]`, rows striped by
 // LN1 = 6 under OpenMP exactly like the reference's SP_MP build.
@@ -519,10 +667,21 @@ void grid_out(const Grid<R>& g, double* x_out, double* w_out) {
 }
 
 template <class R>
-int bp_run(const float* imgs, int nx, int nang, const float* angles, const float* symang,
+int bp_run(const float* imgs_in, int nx, int nang, const float* angles, const float* symang,
            int nsym, const uint8_t* half, int halt, float* vol_all, float* vol_1, float* vol_2,
-           double* x_out, double* w_out, int nthreads) {
-  if (nx < 8 || nx % 2 != 0) return 101;
+           double* x_out, double* w_out, int nthreads, const float* inplane = nullptr) {
+  if (nx < 8) return 101;
+  // RB 3F / RB 32F: every image first goes through RTSQ with doc registers
+  // 6-8 (in-plane angle, x shift, y shift), bp3f.f:406-425
+  std::vector<float> rot;
+  const float* imgs = imgs_in;
+  if (inplane) {
+    rot.resize((size_t)nang * nx * nx);
+    for (int a = 0; a < nang; ++a)
+      rtsq(imgs_in + (size_t)a * nx * nx, &rot[(size_t)a * nx * nx], nx, nx, inplane[3 * a], inplane[3 * a + 1],
+           inplane[3 * a + 2]);
+    imgs = rot.data();
+  }
   KBTable kb;
   fill_kb(2 * nx, kb);
   std::vector<float> dm((size_t)9 * nang), sm((size_t)9 * std::max(1, nsym));
@@ -544,16 +703,24 @@ int bp_run(const float* imgs, int nx, int nang, const float* angles, const float
     delete go;
     return 0;
   }
+  // real-space symmetrisation of each output with MAXSYM > 1 (bp3f.f:252-279,
+  // bp32f.f:280-300,352-368,390-405)
+  auto sym = [&](float* v) {
+    if (nsym <= 1 || !v) return;
+    std::vector<float> tmp(v, v + (size_t)nx * nx * nx);
+    symvol(tmp.data(), v, nx, sm.data(), nsym);
+  };
   if (!half) {
     finish_volume<R>(ge, kb, vol_all);
+    sym(vol_all);
     return 0;
   }
   // BP 32F: first sample = XE, both = XE+XO (ADDADA), second = XO
   Grid<R> both(nx);
   for (size_t q = 0; q < ge.W.size(); ++q) { both.X[q] = ge.X[q] + go->X[q]; both.W[q] = ge.W[q] + go->W[q]; }
-  if (vol_1) finish_volume<R>(ge, kb, vol_1);
-  if (vol_all) finish_volume<R>(both, kb, vol_all);
-  if (vol_2) finish_volume<R>(*go, kb, vol_2);
+  if (vol_1) { finish_volume<R>(ge, kb, vol_1); sym(vol_1); }
+  if (vol_all) { finish_volume<R>(both, kb, vol_all); sym(vol_all); }
+  if (vol_2) { finish_volume<R>(*go, kb, vol_2); sym(vol_2); }
   delete go;
   return 0;
 }
@@ -994,6 +1161,30 @@ int orc_bp3f(const float* imgs, int nx, int nang, const float* angles, const flo
   if (prec == 1)
     return bp_run<double>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
   return bp_run<float>(imgs, nx, nang, angles, symang, nsym, half, halt, vol_all, vol_1, vol_2, x_out, w_out, nthreads);
+}
+
+// RB 3F (half == NULL) / RB 32F: as orc_bp3f after RTSQ of every image with
+// inplane[3*i] = angle (deg), inplane[3*i+1] = x shift, inplane[3*i+2] = y shift
+int orc_rb3f(const float* imgs, int nx, int nang, const float* angles, const float* inplane, const uint8_t* half,
+             int prec, float* vol_all, float* vol_1, float* vol_2, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (prec == 1)
+    return bp_run<double>(imgs, nx, nang, angles, nullptr, 0, half, 0, vol_all, vol_1, vol_2, nullptr, nullptr,
+                          nthreads, inplane);
+  return bp_run<float>(imgs, nx, nang, angles, nullptr, 0, half, 0, vol_all, vol_1, vol_2, nullptr, nullptr,
+                       nthreads, inplane);
+}
+
+// SYMVOL of a volume with symmetry angle triples (psi, theta, phi)
+void orc_symvol(const float* q1, float* q2, int nx, const float* symang, int nsym) {
+  std::vector<float> sm((size_t)9 * nsym);
+  for (int s = 0; s < nsym; ++s) cang(symang[3 * s + 2], symang[3 * s + 1], symang[3 * s], &sm[9 * s]);
+  symvol(q1, q2, nx, sm.data(), nsym);
+}
+
+// RTSQ of one image (rtsq.f:56-140)
+void orc_rtsq(const float* in, float* out, int nx, int ny, float theta, float shx, float shy) {
+  rtsq(in, out, nx, ny, theta, shx, shy);
 }
 
 // A BP 32F insertion session: two FP32 grids allocated and zeroed once (as

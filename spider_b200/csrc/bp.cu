@@ -86,6 +86,81 @@ __global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ im
   }
 }
 
+// ----------------------------------------------------------------------------
+// RTSQ (rtsq.f:56-140) with QUADRI (quadri.f:83-150): in-plane rotation and
+// shift of each image before PADD2, for RB 3F / RB 32F (bp3f.f:406-425).  One
+// thread per output pixel; per image the host passes COS and SIN of
+// THETA*DGR_TO_RAD (REAL) and the shifts, so every coordinate is the Fortran's.
+struct RtsqParm {
+  float cod, sid, shx, shy;
+};
+
+__device__ __forceinline__ float quadri_dev(float xx, float yy, int nx, int ny, const float* __restrict__ f) {
+  float x = xx, y = yy;
+  if (x < 1.0f) x = __fadd_rn(x, (float)((1 - __float2int_rz(x) / nx) * nx));
+  if (x > __fadd_rn((float)nx, 0.5f)) x = __fadd_rn(fmodf(__fsub_rn(x, 1.0f), (float)nx), 1.0f);
+  if (y < 1.0f) y = __fadd_rn(y, (float)((1 - __float2int_rz(y) / ny) * ny));
+  if (y > __fadd_rn((float)ny, 0.5f)) y = __fadd_rn(fmodf(__fsub_rn(y, 1.0f), (float)ny), 1.0f);
+  const int i = __float2int_rz(x), j = __float2int_rz(y);
+  const float dx0 = __fsub_rn(x, (float)i), dy0 = __fsub_rn(y, (float)j);
+  int ip1 = i + 1, im1 = i - 1, jp1 = j + 1, jm1 = j - 1;
+  if (ip1 > nx) ip1 -= nx;
+  if (im1 < 1) im1 += nx;
+  if (jp1 > ny) jp1 -= ny;
+  if (jm1 < 1) jm1 += ny;
+#define QF(a, b) __ldg(f + (size_t)((b) - 1) * nx + ((a) - 1))
+  const float f0 = QF(i, j);
+  const float c1 = __fsub_rn(QF(ip1, j), f0);
+  const float c2 = __fmul_rn(__fadd_rn(__fsub_rn(c1, f0), QF(im1, j)), 0.5f);
+  const float c3 = __fsub_rn(QF(i, jp1), f0);
+  const float c4 = __fmul_rn(__fadd_rn(__fsub_rn(c3, f0), QF(i, jm1)), 0.5f);
+  const float dxb = __fsub_rn(dx0, 1.0f), dyb = __fsub_rn(dy0, 1.0f);
+  const float hxc = (float)(int)copysignf(1.0f, dx0);
+  const float hyc = (float)(int)copysignf(1.0f, dy0);
+  int ic = __float2int_rz(__fadd_rn((float)i, hxc)), jc = __float2int_rz(__fadd_rn((float)j, hyc));
+  if (ic > nx) ic -= nx; else if (ic < 1) ic += nx;
+  if (jc > ny) jc -= ny; else if (jc < 1) jc += ny;
+  float t = __fsub_rn(QF(ic, jc), f0);
+  t = __fsub_rn(t, __fmul_rn(hxc, c1));
+  t = __fsub_rn(t, __fmul_rn(__fmul_rn(hxc, __fsub_rn(hxc, 1.0f)), c2));
+  t = __fsub_rn(t, __fmul_rn(hyc, c3));
+  t = __fsub_rn(t, __fmul_rn(__fmul_rn(hyc, __fsub_rn(hyc, 1.0f)), c4));
+  const float c5 = __fmul_rn(t, __fmul_rn(hxc, hyc));
+#undef QF
+  const float a = __fadd_rn(__fadd_rn(c1, __fmul_rn(dxb, c2)), __fmul_rn(dy0, c5));
+  const float b = __fadd_rn(c3, __fmul_rn(dyb, c4));
+  return __fadd_rn(__fadd_rn(f0, __fmul_rn(dx0, a)), __fmul_rn(dy0, b));
+}
+
+__global__ void rtsq_kernel(const float* __restrict__ in, float* __restrict__ out, int nx, int nimg,
+                            const RtsqParm* __restrict__ prm) {
+  const size_t total = (size_t)nimg * nx * nx;
+  const int iycen = nx / 2 + 1, ixcen = nx / 2 + 1;
+  const bool even = (nx % 2) == 0;
+  const float r1 = (float)(-nx / 2);
+  const float r2 = even ? __fsub_rn((float)(nx / 2), 1.0f) : (float)(nx / 2);
+  const float re1 = even ? (float)(-nx) : (float)(-nx - 1), re2 = even ? (float)nx : (float)(nx + 1);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(q / ((size_t)nx * nx));
+    const int p = (int)(q % ((size_t)nx * nx));
+    const int ix = p % nx + 1, iy = p / nx + 1;
+    const RtsqParm m = prm[b];
+    const float shx = fmodf(m.shx, (float)nx), shy = fmodf(m.shy, (float)nx);
+    const float fixcenmshx = __fsub_rn((float)(-ixcen), shx), fiycenmshy = __fsub_rn((float)(-iycen), shy);
+    float yi = __fadd_rn((float)iy, fiycenmshy);
+    if (yi < r1) yi = fminf(__fadd_rn(yi, re2), r2);
+    if (yi > r2) yi = fmaxf(__fadd_rn(yi, re1), r1);
+    const float ycod = __fadd_rn(__fmul_rn(yi, m.cod), (float)iycen);
+    const float ysid = __fadd_rn(__fmul_rn(-yi, m.sid), (float)ixcen);
+    float xi = __fadd_rn((float)ix, fixcenmshx);
+    if (xi < r1) xi = fminf(__fadd_rn(xi, re2), r2);
+    if (xi > r2) xi = fmaxf(__fadd_rn(xi, re1), r1);
+    const float yold = __fadd_rn(__fmul_rn(xi, m.sid), ycod);
+    const float xold = __fadd_rn(__fmul_rn(xi, m.cod), ysid);
+    out[q] = quadri_dev(xold, yold, nx, nx, in + (size_t)b * nx * nx);
+  }
+}
+
 // FP32 spectrum -> BF16 spectrum (reduced-precision storage mode)
 __global__ void to_bf16_kernel(const float2* __restrict__ in, __nv_bfloat162* __restrict__ out, size_t count) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < count; q += (size_t)gridDim.x * blockDim.x)
@@ -110,9 +185,9 @@ __device__ __forceinline__ float2 load_spec(const void* spec, size_t q) {
 // and weight are bit-identical to the CPU restatement; the accumulation is an
 // FP32 vector atomic per tap.
 template <bool BF16>
-__global__ void __launch_bounds__(256) insert_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
+__global__ void __launch_bounds__(512) insert_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
                                                      int nslices, int nx, const float* __restrict__ kbtab, float fltb,
-                                                     float4* __restrict__ g0, float4* __restrict__ g1) {
+                                                     float4* __restrict__ g0, float4* __restrict__ g1, int seg_map) {
   extern __shared__ float tab[];
   for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
   __syncthreads();
@@ -123,21 +198,30 @@ __global__ void __launch_bounds__(256) insert_kernel(const void* __restrict__ sp
   const float fN = (float)N;
   const int lane = threadIdx.x & 31;
   const int warps_per_block = blockDim.x >> 5;
-  const long long nitems = (long long)nslices * N;
+  // work item = 32 consecutive pixels (one warp) of one row of one slice,
+  // slice-major: the resident warps cover about one slice at a time, so the
+  // voxels they update (one thick central plane) stay resident in L2
+  const int nseg = seg_map ? (nx + 1 + 31) >> 5 : 1;
+  const long long per_slice = (long long)N * nseg;
+  const long long nitems = (long long)nslices * per_slice;
   const size_t rowlen = (size_t)(nx + 1);
   const size_t plane = (size_t)N * rowlen;
 
   for (long long item = (long long)blockIdx.x * warps_per_block + (threadIdx.x >> 5); item < nitems;
        item += (long long)gridDim.x * warps_per_block) {
-    const int s = (int)(item / N);
-    const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
+    const int s = (int)(item / per_slice);
+    const int rem = (int)(item % per_slice);
+    const int J = rem / nseg - nx + 1;  // J = -NX+1 .. NX
+    const int I0 = (rem % nseg) << 5;
+    if (I0 * I0 + J * J >= N * N / 4) continue;   // the whole segment lies outside the disk
+    const int Iend = seg_map ? min(I0 + 32, N2 + 1) : N2 + 1;
     const SliceDesc sd = slices[s];
     float4* G = sd.grid ? g1 : g0;
     const int JP = (J >= 0) ? J : N + J;
     const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
     const float fJ = (float)J;
     const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
-    for (int I = lane; I <= N2; I += 32) {
+    for (int I = I0 + lane; I < Iend; I += 32) {
       if (!((I * I + J * J) < (N * N / 4)) || (I == 0 && J < 0)) continue;
       const float fI = (float)I;
       float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
@@ -227,6 +311,12 @@ __global__ void __launch_bounds__(256) insert_kernel(const void* __restrict__ sp
 // taps (IXN < LN2, oneline.f:118-150) always do.  Every tap's voxel and weight
 // are computed exactly as in insert_kernel.
 constexpr int kTileI = 16, kTileJ = 8, kTileCap = 7296;
+
+// shared-memory reduction without a returned value (no scoreboard wait)
+__device__ __forceinline__ void red_shared_add(float* p, float v) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
 
 template <bool BF16>
 __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
@@ -339,9 +429,9 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
               const float wg = __fmul_rn(tx[lx], tyz);
               if (wg != 0.0f) {
                 const int q = rowq + ixn + lx - 2;
-                atomicAdd(s_re + q, __fmul_rn(br, wg));
-                atomicAdd(s_im + q, __fmul_rn(bi, wg));
-                atomicAdd(s_w + q, wg);
+                red_shared_add(s_re + q, __fmul_rn(br, wg));
+                red_shared_add(s_im + q, __fmul_rn(bi, wg));
+                red_shared_add(s_w + q, wg);
               }
             }
           } else {
@@ -527,6 +617,96 @@ __global__ void windkb_out_kernel(const float* __restrict__ R, int nx, int ip, f
 }
 
 // ----------------------------------------------------------------------------
+// SYMVOL (symvol.f:39-180, SP_MP branch) with TRIQDF/TRIQUAD (symvol.f:230-252,
+// triquad.f): q2 = sum over symmetries, in order, of q1 sampled at RM^T x with
+// triquadratic interpolation inside radius sqrt(IRADI) and q1 itself outside.
+// Same DOUBLE/REAL mix and operation order as the Fortran.
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+
+__device__ float triquad_dev(double r, double s, double t, const float* f) {
+  const float c2 = 0.5f, c4 = 0.25f, c8 = 0.125f;
+  const float rs = __double2float_rn(__dmul_rn(r, s)), st = __double2float_rn(__dmul_rn(s, t));
+  const float rt = __double2float_rn(__dmul_rn(r, t));
+  const float rst = __double2float_rn(__dmul_rn(r, (double)st));
+  const float rsq = __double2float_rn(__dsub_rn(1.0, __dmul_rn(r, r)));
+  const float ssq = __double2float_rn(__dsub_rn(1.0, __dmul_rn(s, s)));
+  const float tsq = __double2float_rn(__dsub_rn(1.0, __dmul_rn(t, t)));
+  const float rm1 = __double2float_rn(__dsub_rn(1.0, r)), sm1 = __double2float_rn(__dsub_rn(1.0, s));
+  const float tm1 = __double2float_rn(__dsub_rn(1.0, t));
+  const float rp1 = __double2float_rn(__dadd_rn(1.0, r)), sp1 = __double2float_rn(__dadd_rn(1.0, s));
+  const float tp1 = __double2float_rn(__dadd_rn(1.0, t));
+  const float R = __double2float_rn(r), S = __double2float_rn(s), T = __double2float_rn(t);
+  float v = fm(fm(fm(fm(fm(-c8, rst), rm1), sm1), tm1), f[0]);
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, st), rsq), sm1), tm1), f[1]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c8, rst), rp1), sm1), tm1), f[2]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, rt), rm1), ssq), tm1), f[3]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c2, T), rsq), ssq), tm1), f[4]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, rt), rp1), ssq), tm1), f[5]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c8, rst), rm1), sp1), tm1), f[6]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, st), rsq), sp1), tm1), f[7]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c8, rst), rp1), sp1), tm1), f[8]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, rs), rm1), sm1), tsq), f[9]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c2, S), rsq), sm1), tsq), f[10]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, rs), rp1), sm1), tsq), f[11]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c2, R), rm1), ssq), tsq), f[12]));
+  v = __fadd_rn(v, fm(fm(fm(rsq, ssq), tsq), f[13]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c2, R), rp1), ssq), tsq), f[14]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, rs), rm1), sp1), tsq), f[15]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c2, S), rsq), sp1), tsq), f[16]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, rs), rp1), sp1), tsq), f[17]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c8, rst), rm1), sm1), tp1), f[18]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, st), rsq), sm1), tp1), f[19]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c8, rst), rp1), sm1), tp1), f[20]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c4, rt), rm1), ssq), tp1), f[21]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c2, T), rsq), ssq), tp1), f[22]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, rt), rp1), ssq), tp1), f[23]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(-c8, rst), rm1), sp1), tp1), f[24]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c4, st), rsq), sp1), tp1), f[25]));
+  v = __fadd_rn(v, fm(fm(fm(fm(fm(c8, rst), rp1), sp1), tp1), f[26]));
+  return v;
+}
+
+__global__ void symvol_kernel(const float* __restrict__ q1, float* __restrict__ q2, int nx,
+                              const float* __restrict__ rm, int nsym) {
+  const int klx = -nx / 2, knx = (nx % 2 == 0) ? nx / 2 - 1 : nx / 2;
+  const int mn = min(abs(klx), abs(knx));
+  const int iradi = (mn - 1) * (mn - 1);
+  const size_t nv = (size_t)nx * nx * nx;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nv; q += (size_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(q % nx) + klx;
+    const size_t t = q / nx;
+    const int iy = (int)(t % nx) + klx, iz = (int)(t / nx) + klx;
+    float o = 0.0f;
+    for (int is = 0; is < nsym; ++is) {
+      const float* R = rm + 9 * is;
+      if (R[0] == 1.0f && R[4] == 1.0f && R[8] == 1.0f) {
+        o = __fadd_rn(o, q1[q]);
+        continue;
+      }
+      const int icrd = ix * ix + iy * iy + iz * iz;
+      if (icrd <= iradi) {
+        const float fy = (float)iy, fz = (float)iz, fx = (float)ix;
+        const double qr0 = __dadd_rn((double)__fadd_rn(fm(R[1], fy), fm(R[2], fz)), (double)fm(R[0], fx));
+        const double qr1 = __dadd_rn((double)__fadd_rn(fm(R[4], fy), fm(R[5], fz)), (double)fm(R[3], fx));
+        const double qr2 = __dadd_rn((double)__fadd_rn(fm(R[7], fy), fm(R[8], fz)), (double)fm(R[6], fx));
+        const int iox = (int)floor(qr0), ioy = (int)floor(qr1), ioz = (int)floor(qr2);
+        const double dx = __dsub_rn(qr0, (double)iox), dy = __dsub_rn(qr1, (double)ioy), dz = __dsub_rn(qr2, (double)ioz);
+        float f[27];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) {
+          const int X = l % 3 - 1, Y = (l / 3) % 3 - 1, Z = l / 9 - 1;
+          f[l] = __ldg(q1 + ((size_t)(ioz + Z - klx) * nx + (ioy + Y - klx)) * nx + (iox + X - klx));
+        }
+        o = __fadd_rn(o, triquad_dev(dx, dy, dz, f));
+      } else {
+        o = __fadd_rn(o, q1[q]);
+      }
+    }
+    q2[q] = o;
+  }
+}
+
+// ----------------------------------------------------------------------------
 // BP 3F P / M helpers: float4 grid <-> (X interleaved complex, W)
 __global__ void grid_split_kernel(const float4* __restrict__ G, float2* __restrict__ X, float* __restrict__ W, size_t nvox) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
@@ -597,6 +777,8 @@ void bp_release(spi_ctx* c) {
   c->gptr[0] = c->gptr[1] = nullptr;
   c->wkb_nx = 0;
   c->imgs.release();
+  c->imgs2.release();
+  c->rtsq_prm.release();
   c->padded.release();
   c->spectra.release();
   c->spec_tmp.release();
@@ -605,6 +787,7 @@ void bp_release(spi_ctx* c) {
   c->real3.release();
   c->wkb.release();
   c->volbuf.release();
+  c->symtmp.release();
   c->hslices.release();
   if (c->plan2d) cufftDestroy(c->plan2d);
   if (c->plan3d) cufftDestroy(c->plan3d);
@@ -769,7 +952,7 @@ long long spi_ctx_device_bytes(const spi_ctx* c) { return c ? c->device_bytes() 
 
 int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsym) {
   if (!c) return fail(kInvalid, "spi_bp_open: NULL context");
-  if (nx < 8 || nx > 512 || (nx & 1)) return fail(kInvalid, "spi_bp_open: nx = %d must be even, 8..512", nx);
+  if (nx < 8 || nx > 512) return fail(kInvalid, "spi_bp_open: nx = %d must be 8..512", nx);
   if (ngrids != 1 && ngrids != 2) return fail(kInvalid, "spi_bp_open: ngrids = %d must be 1 or 2", ngrids);
   if (nsym > 1 && !sym_angles) return fail(kInvalid, "spi_bp_open: nsym = %d but no symmetry angles", nsym);
   SPI_CUDA(cudaSetDevice(c->device));
@@ -809,6 +992,14 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
     c->insert_mode = (m && strcmp(m, "tile") == 0) ? 0 : 1;
     const char* o = getenv("SPI_SLICE_ORDER");
     c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
+    const char* mp = getenv("SPI_INSERT_MAP");
+    c->insert_seg_map = (mp && strcmp(mp, "seg") == 0) ? 1 : 0;
+    // The direct insertion is limited by L2 atomic contention, not by
+    // occupancy: 4 warps per SM beat 8-24 (measured at 256^3, 4,096 images).
+    c->insert_threads = env_int("SPI_INSERT_THREADS", 128);
+    if (c->insert_threads != 64 && c->insert_threads != 128 && c->insert_threads != 256 && c->insert_threads != 512)
+      c->insert_threads = 128;
+    c->insert_blocks_per_sm = env_int("SPI_INSERT_BLOCKS_PER_SM", 1);
   }
   int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)268435456ull / ((size_t)c->n * c->n * 4)));
   c->sub = sub;
@@ -826,7 +1017,7 @@ int spi_bp_attach_grids(spi_ctx* c, void* g0, void* g1) {
 }
 
 int spi_bp_grid_bytes(int nx, long long* bytes) {
-  if (!bytes || nx < 8 || nx > 512 || (nx & 1)) return fail(kInvalid, "spi_bp_grid_bytes: nx = %d", nx);
+  if (!bytes || nx < 8 || nx > 512) return fail(kInvalid, "spi_bp_grid_bytes: nx = %d", nx);
   *bytes = (long long)(nx + 1) * (2LL * nx) * (2LL * nx) * 16;
   return 0;
 }
@@ -861,8 +1052,24 @@ static int ensure_chunk_buffers(spi_ctx* c) {
   return 0;
 }
 
+static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
+                          const uint8_t* half, int imgs_on_device);
+
 int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, const uint8_t* half,
                   int imgs_on_device) {
+  return bp_insert_impl(c, imgs, nimg, angles, nullptr, half, imgs_on_device);
+}
+
+int spi_bp_insert_rb(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
+                     const uint8_t* half, int imgs_on_device) {
+  if (nimg > 0 && !inplane) return fail(kInvalid, "spi_bp_insert_rb: in-plane parameters are required");
+  return bp_insert_impl(c, imgs, nimg, angles, inplane, half, imgs_on_device);
+}
+
+}  // extern "C"
+
+static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
+                          const uint8_t* half, int imgs_on_device) {
   if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert: no open reconstruction (spi_bp_open)");
   if (nimg < 0 || (nimg > 0 && (!imgs || !angles))) return fail(kInvalid, "spi_bp_insert: bad image arguments");
   if (c->merged) return fail(kInvalid, "spi_bp_insert: images cannot follow spi_bp_partial_add");
@@ -932,6 +1139,18 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
   const double klp = (double)(float)klp_count;
   const int ip = (n - nx) / 2 + nx % 2;
   const size_t spec_plane = (size_t)n * (nx + 1);
+  std::vector<RtsqParm> rprm;
+  if (inplane) {
+    // COS/SIN(THETA*DGR_TO_RAD) in REAL, as RTSQ computes them (rtsq.f:111-112)
+    const float dgr = 3.14159265358979323846f / 180.0f;
+    rprm.resize(nimg);
+    for (int a = 0; a < nimg; ++a) {
+      const float th = inplane[3 * a];
+      rprm[a] = RtsqParm{std::cos(th * dgr), std::sin(th * dgr), inplane[3 * a + 1], inplane[3 * a + 2]};
+    }
+    SPI_TRY(c->imgs2.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
+    SPI_TRY(c->rtsq_prm.ensure((size_t)c->chunk * sizeof(RtsqParm)));
+  }
   for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
     const int nb = std::min(c->chunk, nimg - a0);
     const float* src = imgs + (size_t)a0 * nx * nx;
@@ -940,6 +1159,17 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
       SPI_CUDA(cudaMemcpyAsync(c->imgs.p, src, (size_t)nb * nx * nx * sizeof(float), cudaMemcpyHostToDevice, c->stream));
       c->phase_end(ev);
       src = c->imgs.as<float>();
+    }
+    if (inplane) {
+      SPI_CUDA(cudaMemcpyAsync(c->rtsq_prm.p, rprm.data() + a0, (size_t)nb * sizeof(RtsqParm), cudaMemcpyHostToDevice,
+                               c->stream));
+      int ev = c->phase_begin(0);
+      rtsq_kernel<<<grid_blocks(c, (size_t)nb * nx * nx, 256), 256, 0, c->stream>>>(
+          src, c->imgs2.as<float>(), nx, nb, c->rtsq_prm.as<RtsqParm>());
+      SPI_TRY(check_kernel("rtsq_kernel"));
+      c->phase_end(ev);
+      c->count();
+      src = c->imgs2.as<float>();
     }
     for (int b0 = 0; b0 < nb; b0 += c->sub) {
       const int nvalid = std::min(c->sub, nb - b0);
@@ -969,18 +1199,22 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
     int ev_ins = c->phase_begin(2);
     if (c->insert_mode == 1) {
       const size_t smem = 5000 * sizeof(float);
+      const int threads = c->insert_threads;
       int per_sm = 1;
       if (c->bf16)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, 256, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, threads, smem);
       else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, 256, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, threads, smem);
+      if (c->insert_blocks_per_sm > 0) per_sm = std::min(per_sm, c->insert_blocks_per_sm);
       const int blocks = c->sm_count * std::max(per_sm, 1);
       if (c->bf16)
-        insert_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                             c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+        insert_kernel<true><<<blocks, threads, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                                 c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1,
+                                                                 c->insert_seg_map);
       else
-        insert_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                              c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+        insert_kernel<false><<<blocks, threads, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
+                                                                  c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1,
+                                                                  c->insert_seg_map);
     } else {
       const size_t smem = 3 * kTileCap * sizeof(float);
       static bool attr_done = false;
@@ -1011,6 +1245,8 @@ int spi_bp_insert(spi_ctx* c, const float* imgs, int nimg, const float* angles, 
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
 }
+
+extern "C" {
 
 static int apply_sym0(spi_ctx* c, int g) {
   if (!c->pending_sym0[g]) return 0;
@@ -1082,6 +1318,19 @@ static int finish_one(spi_ctx* c, int ga, int gb, float* dvol) {
   SPI_TRY(check_kernel("windkb_out_kernel"));
   c->phase_end(ev);
   c->count(2);
+  if (c->nsym > 1) {
+    // real-space symmetrisation (bp3f.f:252-279): SYMVOL(TEMP = volume) -> volume
+    const size_t vbytes = total * sizeof(float);
+    SPI_TRY(c->symtmp.ensure(vbytes + 9 * sizeof(float) * (size_t)c->nsym));
+    float* q1 = c->symtmp.as<float>();
+    float* rm = q1 + total;
+    SPI_CUDA(cudaMemcpyAsync(q1, dvol, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+    SPI_CUDA(cudaMemcpyAsync(rm, c->sym_dm.data(), 9 * sizeof(float) * (size_t)c->nsym, cudaMemcpyHostToDevice,
+                             c->stream));
+    symvol_kernel<<<grid_blocks(c, total, 256), 256, 0, c->stream>>>(q1, dvol, nx, rm, c->nsym);
+    SPI_TRY(check_kernel("symvol_kernel"));
+    c->count();
+  }
   return 0;
 }
 

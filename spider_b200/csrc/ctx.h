@@ -17,6 +17,9 @@ struct spi_ctx {
   int bf16 = 0;
   int insert_mode = 1;                // 0 = tile-privatised, 1 = direct per-tap atomics
   int slice_order = 1;                // 1 = order slices of a chunk by plane normal
+  int insert_seg_map = 0;             // 1 = warps take 32-pixel row segments, 0 = whole rows
+  int insert_threads = 256;           // threads per insert block
+  int insert_blocks_per_sm = 0;       // 0 = as many as fit
   int cg_fp64 = 1;                    // BP CG vectors/projections in FP64 (1) or FP32 (0)
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT
@@ -28,6 +31,8 @@ struct spi_ctx {
   long wkb_m = 0;                     // shell voxel count M of WINDKB2A
   spi::DevBuf kbtab;                  // float[5000]
   spi::DevBuf imgs;                   // float [chunk][nx][nx]
+  spi::DevBuf imgs2;                  // float [chunk][nx][nx] (RTSQ output)
+  spi::DevBuf rtsq_prm;               // RtsqParm [chunk]
   spi::DevBuf padded;                 // float [sub][n][n]
   spi::DevBuf spectra;                // float2 or bf16x2 [chunk][n][nx+1]
   spi::DevBuf spec_tmp;               // float2 [sub][n][nx+1] (BF16 mode FFT output)
@@ -37,6 +42,7 @@ struct spi_ctx {
   spi::DevBuf wkb;                    // float[(nx/2)^2 + 1]
   spi::DevBuf acc;                    // double[8] reduction scratch
   spi::DevBuf volbuf;                 // float [nx^3] (finish output staging)
+  spi::DevBuf symtmp;                 // float [nx^3] + symmetry matrices (SYMVOL input)
   spi::HostBuf hslices;
   cufftHandle plan2d = 0;
   int plan2d_n = 0, plan2d_batch = 0;

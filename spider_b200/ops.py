@@ -10,6 +10,7 @@ function           SPIDER operation (dispatch in vtil2.f)              reference
 ``bp3f_partial``   ``BP 3F P``      partial Fourier volume + weights   BP3F(HALT), bp3f.f:191-248
 ``bp3f_merge``     ``BP 3F M``      merge partial volumes              BP3F_MERGE, bp3f.f:531
 ``bp32f``          ``BP 32F``       (vtil2.f:316-322)                  BP32F, bp32f.f:57
+``rb3f``/``rb32f`` ``RB 3F/RB 32F`` RTSQ pre-rotation (vtil2.f:88-95)  BP3F(.TRUE.), bp3f.f:406-425
 ``pj3q``           ``PJ 3Q``        (vtil2.f:218-220)                  PJ3Q_N, pj3q_n.f:41
 ``bpcg``           ``BP CG``        (vtil2.f:324)                      BPCG, bpcg.f:70
 =================  ==================================================  =========================
@@ -35,7 +36,7 @@ try:  # torch is plumbing for device memory; optional for host use
 except Exception:  # pragma: no cover
     torch = None
 
-__all__ = ["Context", "default_context", "bp3f", "bp32f", "bp3f_partial", "bp3f_merge", "pj3q",
+__all__ = ["Context", "default_context", "bp3f", "bp32f", "rb3f", "rb32f", "bp3f_partial", "bp3f_merge", "pj3q",
            "pj3q_adjoint", "bpcg", "cg_project", "cg_backproject", "SpiderError"]
 
 
@@ -104,7 +105,9 @@ class Context:
         self._nx = nx
         self._ngrids = ngrids
 
-    def bp_insert(self, imgs, angles, half=None):
+    def bp_insert(self, imgs, angles, half=None, inplane=None):
+        """Insert images; with ``inplane`` [n, 3] = (angle, sx, sy) every image is
+        first rotated and shifted by RTSQ (RB 3F / RB 32F)."""
         ang = _host_f32(angles)
         h = None if half is None else np.ascontiguousarray(
             half.detach().cpu().numpy() if (torch is not None and isinstance(half, torch.Tensor)) else half,
@@ -115,7 +118,13 @@ class Context:
         n = int(imgs.shape[0])
         if ang.shape[0] != n:
             raise SpiderError(101, f"{n} images but {ang.shape[0]} angle triples")
-        check(self._L.spi_bp_insert(self._h, _ptr(imgs), n, _ptr(ang), _ptr(h), 1 if dev else 0))
+        if inplane is None:
+            check(self._L.spi_bp_insert(self._h, _ptr(imgs), n, _ptr(ang), _ptr(h), 1 if dev else 0))
+        else:
+            ip = _host_f32(inplane)
+            if ip.shape != (n, 3):
+                raise SpiderError(101, f"in-plane parameters must be [{n}, 3]")
+            check(self._L.spi_bp_insert_rb(self._h, _ptr(imgs), n, _ptr(ang), _ptr(ip), _ptr(h), 1 if dev else 0))
 
     def bp_finish(self, want=("all",), device: bool = False):
         nx = self._nx
@@ -190,6 +199,31 @@ def bp32f(imgs, angles, half, sym=None, *, ctx: Context | None = None, bf16: boo
         ctx.bp_close()
 
 
+def rb3f(imgs, angles, inplane, sym=None, *, ctx: Context | None = None):
+    """``RB 3F``: RTSQ by (angle, sx, sy) per image, then BP 3F."""
+    ctx = ctx or default_context()
+    nx = _nx_of(imgs)
+    ctx.bp_open(nx, 1, sym)
+    try:
+        ctx.bp_insert(imgs, angles, inplane=inplane)
+        return ctx.bp_finish(("all",))["all"]
+    finally:
+        ctx.bp_close()
+
+
+def rb32f(imgs, angles, inplane, half, sym=None, *, ctx: Context | None = None):
+    """``RB 32F``: RTSQ by (angle, sx, sy) per image, then BP 32F."""
+    ctx = ctx or default_context()
+    nx = _nx_of(imgs)
+    ctx.bp_open(nx, 2, sym)
+    try:
+        ctx.bp_insert(imgs, angles, half, inplane=inplane)
+        o = ctx.bp_finish(("all", "1", "2"))
+        return o["all"], o["1"], o["2"]
+    finally:
+        ctx.bp_close()
+
+
 def bp3f_partial(imgs, angles, sym=None, *, ctx: Context | None = None):
     """``BP 3F P``: returns (X [2nx, 2nx, nx+1, 2] re/im, W [2nx, 2nx, nx+1]) after plane-0 symmetry."""
     ctx = ctx or default_context()
@@ -202,14 +236,15 @@ def bp3f_partial(imgs, angles, sym=None, *, ctx: Context | None = None):
         ctx.bp_close()
 
 
-def bp3f_merge(partials, *, ctx: Context | None = None):
-    """``BP 3F M``: sum partial (X, W) pairs and finish -> volume [nx, nx, nx]."""
+def bp3f_merge(partials, sym=None, *, ctx: Context | None = None):
+    """``BP 3F M``: sum partial (X, W) pairs and finish -> volume [nx, nx, nx]
+    (symmetrised in real space when a symmetry list is given, bp3f.f:701-728)."""
     ctx = ctx or default_context()
     partials = list(partials)
     if not partials:
         raise SpiderError(101, "no partial volumes")
     nx = int(partials[0][1].shape[2]) - 1
-    ctx.bp_open(nx, 1)
+    ctx.bp_open(nx, 1, sym)
     try:
         for x, w in partials:
             ctx.bp_partial_add(x, w)

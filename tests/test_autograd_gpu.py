@@ -1,0 +1,52 @@
+"""Differentiable PJ 3Q: the backward (trilinear insertion) against central
+finite differences with h = 1e-3 on 64 random voxels and against the FP64
+adjoint built from the FP64 oracle's forward."""
+import numpy as np
+import pytest
+
+from spider_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_pj3q_gradient(ctx, orc):
+    import torch
+    from spider_b200 import autograd
+    rng = np.random.default_rng(11)
+    n = 24
+    ri = n / 2 - 2
+    vol = synth.blob_phantom(n, 6, sigma=(1.5, 3.0), radius=6, rng=rng)
+    ang = synth.so3_angles(12, rng)
+    w = rng.standard_normal((12, n, n)).astype(np.float32)
+    v = torch.from_numpy(vol).cuda().requires_grad_(True)
+    loss = (autograd.pj3q(v, ang, ri, ctx=ctx) * torch.from_numpy(w).cuda()).sum()
+    loss.backward()
+    grad = v.grad.detach().cpu().numpy()
+    g = np.arange(n) - n // 2
+    inside = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= (ri - 1) ** 2
+    cand = np.argwhere(inside)
+    picks = cand[rng.choice(len(cand), 64, replace=False)]
+    h = 1e-3
+    w64 = w.astype(np.float64)
+    for z, y, x in picks:
+        # FP64 adjoint: the projection of the unit volume at this voxel, dotted with w
+        e = np.zeros((n, n, n), np.float32)
+        e[z, y, x] = 1.0
+        exact = float((orc.pj3q(e, ang, ri, prec=1).astype(np.float64) * w64).sum())
+        assert abs(grad[z, y, x] - exact) <= 1e-5 * max(1.0, abs(exact))
+        # central finite difference of the FP64 forward with h = 1e-3
+        vp = vol.astype(np.float64).copy()
+        vp[z, y, x] += h
+        vm = vol.astype(np.float64).copy()
+        vm[z, y, x] -= h
+        lp = (orc.pj3q(vp.astype(np.float32), ang, ri, prec=1).astype(np.float64) * w64).sum()
+        lm = (orc.pj3q(vm.astype(np.float32), ang, ri, prec=1).astype(np.float64) * w64).sum()
+        fd = (lp - lm) / (2 * h)
+        assert abs(grad[z, y, x] - fd) <= 2e-2 * max(1.0, abs(fd))
+
+
+def test_pj3q_autograd_no_cpu_path(ctx):
+    import torch
+    from spider_b200 import autograd, ops
+    with pytest.raises(ops.SpiderError):
+        autograd.pj3q(torch.zeros(8, 8, 8), np.zeros((1, 3), np.float32), 2.0, ctx=ctx)

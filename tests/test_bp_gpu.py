@@ -131,7 +131,7 @@ def test_bp_errors(ctx):
         ops.bp3f(np.zeros((3, 16, 18), np.float32), np.zeros((3, 3), np.float32), ctx=ctx)
     assert ei.value.code == 101
     with pytest.raises(ops.SpiderError) as ei:
-        ctx.bp_open(15, 1)
+        ctx.bp_open(7, 1)
     assert ei.value.code == 101
     with pytest.raises(ops.SpiderError):
         ctx.bp_open(16, 3)
@@ -166,13 +166,35 @@ def test_insert_kernels_agree(ctx, orc):
     _, pr, ang = _case(nx, nimg, 61)
     # include orientations that put the x = 0 flip line inside many tiles
     ang[:40, 1] = 90.0
-    direct = ops.bp3f(pr, ang, ctx=ctx)
-    os.environ["SPI_INSERT"] = "tile"
-    try:
-        tile = ops.bp3f(pr, ang, ctx=ctx)
-    finally:
-        del os.environ["SPI_INSERT"]
+    out = {}
+    for mode in ("direct", "tile"):
+        os.environ["SPI_INSERT"] = mode
+        try:
+            out[mode] = ops.bp3f(pr, ang, ctx=ctx)
+        finally:
+            del os.environ["SPI_INSERT"]
     ref = orc.bp3f(pr, ang, prec=1, nthreads=1)
-    assert synth.rel_l2(tile, direct) <= 2e-6
-    assert synth.rel_l2(tile, ref) <= TOL
-    assert synth.rel_l2(direct, ref) <= TOL
+    for mode, v in out.items():
+        assert synth.rel_l2(v, out["direct"]) <= 2e-6, mode
+        assert synth.rel_l2(v, ref) <= TOL, mode
+
+
+def test_rb3f_rb32f_match_oracle(ctx, orc):
+    """RB 3F / RB 32F: images shifted by up to 3 px and rotated in plane are
+    aligned by RTSQ (doc registers 6-8) before insertion."""
+    nx, nimg = 32, 200
+    vol, pr, ang = _case(nx, nimg, 71)
+    rng = np.random.default_rng(72)
+    inplane = np.stack([rng.uniform(-180, 180, nimg), rng.uniform(-3, 3, nimg), rng.uniform(-3, 3, nimg)],
+                       1).astype(np.float32)
+    got = ops.rb3f(pr, ang, inplane, ctx=ctx)
+    ref = orc.rb3f(pr, ang, inplane, prec=0, nthreads=1)
+    assert synth.rel_l2(got, ref) <= TOL
+    half = synth.half_mask(nimg, rng)
+    g = ops.rb32f(pr, ang, inplane, half, ctx=ctx)
+    r = orc.rb3f(pr, ang, inplane, half, prec=0, nthreads=1)
+    for a, b in zip(g, r):
+        assert synth.rel_l2(a, b) <= TOL
+    # zero in-plane parameters reproduce BP 3F exactly up to summation order
+    z = ops.rb3f(pr, ang, np.zeros((nimg, 3), np.float32), ctx=ctx)
+    assert synth.rel_l2(z, ops.bp3f(pr, ang, ctx=ctx)) <= 2e-6

@@ -69,4 +69,4 @@ def test_errors_without_device():
     gb = ctypes.c_longlong()
     assert L.spi_bp_grid_bytes(256, ctypes.byref(gb)) == 0
     assert gb.value == 257 * 512 * 512 * 16
-    assert L.spi_bp_grid_bytes(255, ctypes.byref(gb)) == 101
+    assert L.spi_bp_grid_bytes(6, ctypes.byref(gb)) == 101

@@ -107,3 +107,19 @@ def test_stage_image_matches_numpy():
     ky, kx = np.meshgrid(np.arange(n), np.arange(nx + 1), indexing="ij")
     f *= np.where((kx + ky) % 2 == 0, 1.0, -1.0)
     np.testing.assert_allclose(bi, f, atol=1e-4)
+
+
+def test_rtsq_shift_and_rotation():
+    """RTSQ (rtsq.f:56-140): a (sx, sy) shift moves content by (+sx, +sy); a
+    zero transform is the identity; 90 degrees maps the x axis onto y."""
+    nx = 32
+    g = np.arange(nx) - nx // 2
+    img = np.exp(-((g[None, :] - 3) ** 2 + (g[:, None] + 2) ** 2) / 8.0).astype(np.float32)
+    assert np.array_equal(oracle.rtsq(img, 0.0, 0.0, 0.0), img)
+    out = oracle.rtsq(img, 0.0, 2.0, -1.0)
+    np.testing.assert_allclose(out, np.roll(np.roll(img, 2, axis=1), -1, axis=0), atol=1e-6)
+    r = oracle.rtsq(img, 90.0, 0.0, 0.0)
+    p0 = np.unravel_index(np.argmax(img), img.shape)
+    p1 = np.unravel_index(np.argmax(r), r.shape)
+    # centre (16, 16): offset (dy, dx) = (-2, 3) -> (-3, -2) under a 90 degree turn
+    assert (p1[0] - 16, p1[1] - 16) == (-(p0[1] - 16), (p0[0] - 16))
