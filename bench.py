@@ -46,6 +46,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample time")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cg", action="store_true", help="skip the BP CG s/iter measurement")
+    p.add_argument("--cg-n", type=int, default=128)
+    p.add_argument("--cg-nang", type=int, default=10000)
+    p.add_argument("--cg-iters", type=int, default=6)
     return p.parse_args()
 
 
@@ -66,9 +70,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def insert_kernel_name():
+    """The insertion kernel the library launches (SPI_INSERT selects another)."""
+    return {"direct": "insert_kernel", "tile": "insert_tile_kernel"}.get(os.environ.get("SPI_INSERT", ""),
+                                                                         "insert_xlane_kernel")
+
+
 def traffic_per_image():
     """DRAM bytes per image of the insert kernel, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "insert_kernel_traffic.txt")
+    path = os.path.join(ROOT, "profiles", f"{insert_kernel_name()}_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -179,14 +189,96 @@ def cpu_baseline(nx, seconds, imgs_host, angles, half):
     t0 = time.perf_counter()
     sess.insert(imgs_host[:4], angles[:4], half[:4], nthreads=nthreads)
     per = (time.perf_counter() - t0) / 4
-    n = int(max(4, min(len(imgs_host), seconds / max(per, 1e-6))))
-    t0 = time.perf_counter()
-    sess.insert(imgs_host[:n], angles[:n], half[:n], nthreads=nthreads)
-    dt = time.perf_counter() - t0
+    want = int(max(4, seconds / max(per, 1e-6)))
+    n, dt = 0, 0.0
+    while n < want:            # the pool of distinct images is reused in passes
+        k = min(len(imgs_host), want - n)
+        t0 = time.perf_counter()
+        sess.insert(imgs_host[:k], angles[:k], half[:k], nthreads=nthreads)
+        dt += time.perf_counter() - t0
+        n += k
     sess.close()
     return {"value": n / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{n} images at {nx}^3 (BP 32F per-image work: PADD2 + FFT + ONELINE, FP32, "
                       f"the reference's OpenMP row striping), {dt:.1f} s"}
+
+
+def cg_measure(args, ctx, stream, rank, world):
+    """BP CG seconds per iteration (configuration: 128^3, 10,000 images of a
+    50-blob phantom at SNR 0.3, lambda 1e-3, linear interpolation).
+
+    Each variant runs the solver twice, with 1 and with 1 + K iterations, and
+    the difference of the two device-timed calls over K is the cost of one
+    iteration (setup, image upload and the initial back-projection cancel).
+    Variants: FP64 CG vectors with each iteration replayed as a CUDA graph
+    (the default), the same without the graph, and FP32 vectors (the
+    reference's REAL storage).  rel_err_fp32_vs_fp64 compares the FP32-vector
+    volume with the FP64-vector one after 1 + K iterations."""
+    import torch
+    from spider_b200 import ops, synth
+    n, nang, K = args.cg_n, args.cg_nang, args.cg_iters
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(1003 + 7919 * rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1003 + rank)
+    vol = make_phantom_gpu(n, 50, (2.0, 8.0), (0.5, 1.0), rng, dev)
+    ang = synth.so3_angles(nang, rng)
+    projs = make_chunk(ctx, vol, ang, 0.3, gen).cpu().numpy()
+    del vol
+    ri = float(n // 2 - 3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(iters, fp64):
+        e0.record(stream)
+        v, log = ops.bpcg(projs, ang, ri, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64=fp64)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, v, log
+
+    out = {}
+    vols = {}
+    for name, fp64, graph in (("fp64_graph", True, True), ("fp64_plain", True, False), ("fp32_graph", False, True)):
+        if not graph:
+            os.environ["SPI_CG_NOGRAPH"] = "1"
+        try:
+            timed(1, fp64)                       # warm-up (plans, buffers)
+            t1, _, _ = timed(1, fp64)
+            tk, v, log = timed(1 + K, fp64)
+        finally:
+            os.environ.pop("SPI_CG_NOGRAPH", None)
+        out[name] = (tk - t1) / K
+        vols[name] = v
+    rel = float(np.linalg.norm((vols["fp32_graph"] - vols["fp64_graph"]).ravel()) /
+                max(np.linalg.norm(vols["fp64_graph"].ravel()), 1e-30))
+    res = {"metric": "BP CG s/iter", "unit": "s/iter", "value": out["fp64_graph"],
+           "plain_gpu_s_per_iter": out["fp64_plain"], "fp32_vectors_s_per_iter": out["fp32_graph"],
+           "rel_err_fp32_vs_fp64": rel,
+           "config": {"n": n, "images": nang, "lambda": 1e-3, "mode": 1, "iterations_timed": K,
+                      "phantom": "50 Gaussian blobs, sigma 2-8, SNR 0.3, uniform SO(3)"}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res["cpu_baseline"] = cg_cpu_baseline(projs, ang, ri, n)
+    return res
+
+
+def cg_cpu_baseline(projs, ang, ri, n, sample=500):
+    """The oracle's FP32 BP CG (the reference's loop structure, OpenMP over
+    voxel runs) on a 500-image subset: one iteration's cost from the difference
+    of a 1- and a 2-iteration solve, extrapolated linearly to all images
+    (both operators are linear in the image count)."""
+    import oracle
+    nthreads = os.cpu_count() or 1
+    p, a = projs[:sample], ang[:sample]
+    t0 = time.perf_counter()
+    oracle.bpcg(p, a, ri, errm=0.0, chim=0.0, maxit=1, mode=1, lam=1e-3, prec=0, nthreads=nthreads)
+    t1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.bpcg(p, a, ri, errm=0.0, chim=0.0, maxit=2, mode=1, lam=1e-3, prec=0, nthreads=nthreads)
+    t2 = time.perf_counter() - t0
+    per = max(t2 - t1, 1e-9) * len(projs) / sample
+    return {"value": per, "unit": "s/iter", "cores": nthreads, "kind": "port",
+            "sample": f"{sample} of {len(projs)} images at {n}^3, 1 iteration, extrapolated linearly "
+                      f"({t1:.1f} s + {t2:.1f} s of CPU solves)"}
 
 
 def run_reference(args):
@@ -334,15 +426,17 @@ def run_ours(args):
         dms.append(_cang_host(a))
     taps = roofline.mean_taps(nx, np.array(dms), tab, fltb)
     bytes_per_img = roofline.BYTES_PER_TAP * taps + roofline.spectrum_bytes(nx, args.bf16)
-    per_launch_s = insert_ms / n_insert / 1e3
-    achieved = bytes_per_img * chunk / per_launch_s / 1e9
+    # one insert launch per FFT sub-batch: achieved = all images' algorithmic
+    # bytes over the summed launch durations (CUDA events around each launch)
+    achieved = bytes_per_img * chunk * args.steps / (insert_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
     tpi = traffic_per_image()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (tpi * chunk) if tpi else None,
-            "kernel": "insert_kernel", "peak_kind": peak_kind,
+            "kernel": insert_kernel_name(), "peak_kind": peak_kind,
             "algorithmic_bytes_per_image": bytes_per_img, "taps_per_image": taps,
-            "launch_ms": insert_ms / n_insert}
+            "launch_ms": insert_ms / n_insert, "launches": n_insert,
+            "images_per_launch": chunk * args.steps / n_insert}
 
     # ---- e2e through the C ABI with host buffers (pinned), H2D/D2H inside
     e2e = None
@@ -383,6 +477,10 @@ def run_ours(args):
                        "to three host volumes; device-timed on the library stream"}
     ctx.bp_close()
 
+    cg = None
+    if not args.no_cg and world == 1:
+        cg = cg_measure(args, ctx, stream, rank, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         hc = chunks[0][:256].cpu().numpy()
@@ -406,6 +504,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "finish_ms": finish_ms,
             "finish_phase_ms": finish_phase_ms,
+            "bpcg": cg,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

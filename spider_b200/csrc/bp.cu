@@ -300,6 +300,99 @@ __global__ void __launch_bounds__(512) insert_kernel(const void* __restrict__ sp
 }
 
 // ----------------------------------------------------------------------------
+// Insert, lanes over the x taps.  A warp takes one row J of one slice and walks
+// it six pixels at a time: lanes 5g..5g+4 share pixel I0+g and lane 5g+LX owns
+// the x tap LX, so for each (LY, LZ) pair the five vector atomics of a pixel
+// land on 80 contiguous bytes of one grid row (the x axis is the fastest) and
+// the L2 receives one or two line requests per pixel instead of five scattered
+// ones.  A lane whose tap falls below x = 0 (IXN < LN2) adds the reflected
+// point instead (oneline.f:118-150), so every lane issues exactly one atomic
+// per (LY, LZ).  Every voxel and weight is computed as in insert_kernel.
+template <bool BF16>
+__global__ void __launch_bounds__(512) insert_xlane_kernel(const void* __restrict__ spec,
+                                                           const SliceDesc* __restrict__ slices, int nslices, int nx,
+                                                           const float* __restrict__ kbtab, float fltb,
+                                                           float4* __restrict__ g0, float4* __restrict__ g1) {
+  extern __shared__ float tab[];
+  for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
+  __syncthreads();
+
+  const int N = 2 * nx, N2 = nx, LN2 = 2;
+  const int NN4 = N * N / 4;
+  const float fN = (float)N;
+  const int lane = threadIdx.x & 31;
+  const int g = lane / 5;           // pixel of the group of six (g = 6: idle lanes 30, 31)
+  const int lx = lane - 5 * g;      // x tap 0..4
+  const int warps_per_block = blockDim.x >> 5;
+  const long long nitems = (long long)nslices * N;
+  const size_t rowlen = (size_t)(nx + 1);
+  const size_t plane = (size_t)N * rowlen;
+
+  for (long long item = (long long)blockIdx.x * warps_per_block + (threadIdx.x >> 5); item < nitems;
+       item += (long long)gridDim.x * warps_per_block) {
+    const int s = (int)(item / N);
+    const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
+    const SliceDesc sd = slices[s];
+    float4* G = sd.grid ? g1 : g0;
+    const int JP = (J >= 0) ? J : N + J;
+    const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
+    const float fJ = (float)J;
+    const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
+    for (int I0 = 0; I0 <= N2 && I0 * I0 + J * J < NN4; I0 += 6) {
+      const int I = I0 + g;
+      if (g == 6 || I > N2 || !((I * I + J * J) < NN4) || (I == 0 && J < 0)) continue;
+      const float fI = (float)I;
+      float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
+      float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
+      float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
+      const float2 sp = load_spec<BF16>(spec, specrow + I);
+      float br = sp.x, bi = -sp.y;   // SPIDER forward sign = conjugate of the cuFFT R2C output
+      if (xnew < 0.0f) {
+        xnew = -xnew; ynew = -ynew; znew = -znew;
+        bi = -bi;
+      }
+      const int ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
+      const int iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
+      const int izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
+      if (!(ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+            izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1)))
+        continue;
+      float tz[5], ty[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        tz[l] = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(znew, (float)(izn + l - 2))), fltb))];
+        ty[l] = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(ynew, (float)(iyn + l - 2))), fltb))];
+      }
+      const int ixp = ixn + lx - 2;
+      const float tx = tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(xnew, (float)ixp)), fltb))];
+      if (tx == 0.0f) continue;
+      // main tap at (ixp, iyp, izp), or for ixp < 0 the reflected point
+      // (-ixp, -iyp, -izp) with the conjugate value
+      const bool refl = ixp < 0;
+      const float bis = refl ? -bi : bi;
+      const int ixa = refl ? -ixp : ixp;
+#pragma unroll
+      for (int lz = 0; lz < 5; ++lz) {
+        if (tz[lz] == 0.0f) continue;
+        const int izp = izn + lz - 2;
+        const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
+#pragma unroll
+        for (int ly = 0; ly < 5; ++ly) {
+          const float tyz = __fmul_rn(ty[ly], tz[lz]);
+          if (tyz == 0.0f) continue;
+          const int iyp = iyn + ly - 2;
+          const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
+          const float wg = __fmul_rn(tx, tyz);
+          if (wg != 0.0f)
+            atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
+                      make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
+        }
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
 // Insert, tile-privatised form.  A CTA takes a 16 (I) x 8 (J) tile of pixels
 // of one slice; 256 threads = 2 per pixel, splitting the z taps (LZ = -2..0
 // and 1..2).  The tile's taps land in a thin slab whose bounding box (at most
@@ -819,8 +912,9 @@ static int env_int(const char* name, int dflt) {
 
 using namespace spi;
 
-int spi_ctx::phase_begin(int phase) {
+int spi_ctx::phase_begin(int phase, cudaStream_t s) {
   if (!timing) return -1;
+  if (!s) s = stream;
   cudaEvent_t a, b;
   if (ev_pool.size() >= 2) {
     a = ev_pool.back(); ev_pool.pop_back();
@@ -829,14 +923,14 @@ int spi_ctx::phase_begin(int phase) {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
   }
-  cudaEventRecord(a, stream);
-  ev_pending.push_back(PhaseEv{a, b, phase});
+  cudaEventRecord(a, s);
+  ev_pending.push_back(PhaseEv{a, b, phase, s});
   return (int)ev_pending.size() - 1;
 }
 
 void spi_ctx::phase_end(int slot) {
   if (slot < 0) return;
-  cudaEventRecord(ev_pending[slot].b, stream);
+  cudaEventRecord(ev_pending[slot].b, ev_pending[slot].s);
 }
 
 void spi_ctx::phase_collect() {
@@ -898,12 +992,20 @@ int spi_ctx_create(int device, spi_ctx** out) {
     delete c;
     return fail(kCuda, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
+  e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return fail(kCuda, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
   int st = c->acc.ensure(64);
   if (st) {
+    cudaStreamDestroy(c->stream2);
     cudaStreamDestroy(c->stream);
     delete c;
     return st;
   }
+  c->pipeline = env_int("SPI_PIPELINE", 1) ? 1 : 0;
   *out = c;
   return 0;
 }
@@ -920,6 +1022,12 @@ int spi_ctx_destroy(spi_ctx* c) {
   c->hbuf.release();
   c->phase_collect();
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  for (auto e : c->ev_ready) cudaEventDestroy(e);
+  for (auto e : c->ev_done) cudaEventDestroy(e);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  cudaStreamSynchronize(c->stream2);
+  cudaStreamDestroy(c->stream2);
   cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -989,17 +1097,24 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   chunk = env_int("SPI_BP_CHUNK", chunk);
   {
     const char* m = getenv("SPI_INSERT");
-    c->insert_mode = (m && strcmp(m, "tile") == 0) ? 0 : 1;
+    c->insert_mode = (m && strcmp(m, "tile") == 0) ? 0 : (m && strcmp(m, "direct") == 0) ? 1 : 2;
     const char* o = getenv("SPI_SLICE_ORDER");
     c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
     const char* mp = getenv("SPI_INSERT_MAP");
     c->insert_seg_map = (mp && strcmp(mp, "seg") == 0) ? 1 : 0;
-    // The direct insertion is limited by L2 atomic contention, not by
-    // occupancy: 4 warps per SM beat 8-24 (measured at 256^3, 4,096 images).
-    c->insert_threads = env_int("SPI_INSERT_THREADS", 128);
+    // The insertion is limited by L2 atomics, not by occupancy.  Measured on
+    // 4,096 images: the x-lane kernel is best at 24 warps/SM for 128^3 and 16
+    // for 64^3 and 256^3; the direct kernel at 24 warps/SM for 64^3, 8 for
+    // 128^3-192^3 and 4 for 256^3.
+    int def_threads = 256, def_bps = (nx > 96 && nx <= 160) ? 3 : 2;
+    if (c->insert_mode == 1) {
+      def_threads = nx <= 96 ? 256 : 128;
+      def_bps = nx <= 96 ? 3 : nx <= 224 ? 2 : 1;
+    }
+    c->insert_threads = env_int("SPI_INSERT_THREADS", def_threads);
     if (c->insert_threads != 64 && c->insert_threads != 128 && c->insert_threads != 256 && c->insert_threads != 512)
-      c->insert_threads = 128;
-    c->insert_blocks_per_sm = env_int("SPI_INSERT_BLOCKS_PER_SM", 1);
+      c->insert_threads = def_threads;
+    c->insert_blocks_per_sm = env_int("SPI_INSERT_BLOCKS_PER_SM", def_bps);
   }
   int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)268435456ull / ((size_t)c->n * c->n * 4)));
   c->sub = sub;
@@ -1068,6 +1183,84 @@ int spi_bp_insert_rb(spi_ctx* c, const float* imgs, int nimg, const float* angle
 
 }  // extern "C"
 
+// Launch the configured insertion kernel over `nslices` slice descriptors
+// (on the library stream), persistent: sm_count x blocks-per-SM CTAs.
+template <typename K>
+static int insert_blocks(spi_ctx* c, K kernel, int threads, size_t smem, int cap) {
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (cap > 0) per_sm = std::min(per_sm, cap);
+  return c->sm_count * std::max(per_sm, 1);
+}
+
+static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g1) {
+  const void* spec = c->spectra.p;
+  const int nx = c->nx;
+  const float* tab = c->kbtab.as<float>();
+  const float fltb = c->kb.fltb;
+  float4* g0 = c->gptr[0];
+  int ev_ins = c->phase_begin(2);
+  if (c->insert_mode == 1 || c->insert_mode == 2) {
+    const size_t smem = 5000 * sizeof(float);
+    const int threads = c->insert_threads;
+    if (c->insert_mode == 1) {
+      if (c->bf16)
+        insert_kernel<true><<<insert_blocks(c, insert_kernel<true>, threads, smem, c->insert_blocks_per_sm), threads,
+                              smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, c->insert_seg_map);
+      else
+        insert_kernel<false><<<insert_blocks(c, insert_kernel<false>, threads, smem, c->insert_blocks_per_sm),
+                               threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1,
+                                                           c->insert_seg_map);
+    } else {
+      if (c->bf16)
+        insert_xlane_kernel<true><<<insert_blocks(c, insert_xlane_kernel<true>, threads, smem,
+                                                  c->insert_blocks_per_sm),
+                                    threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1);
+      else
+        insert_xlane_kernel<false><<<insert_blocks(c, insert_xlane_kernel<false>, threads, smem,
+                                                   c->insert_blocks_per_sm),
+                                     threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1);
+    }
+  } else {
+    const size_t smem = 3 * kTileCap * sizeof(float);
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(insert_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(insert_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_done = true;
+    }
+    if (c->bf16)
+      insert_tile_kernel<true><<<insert_blocks(c, insert_tile_kernel<true>, 256, smem, 0), 256, smem, c->stream>>>(
+          spec, sl, nslices, nx, tab, fltb, g0, g1);
+    else
+      insert_tile_kernel<false><<<insert_blocks(c, insert_tile_kernel<false>, 256, smem, 0), 256, smem, c->stream>>>(
+          spec, sl, nslices, nx, tab, fltb, g0, g1);
+  }
+  SPI_TRY(check_kernel("insert_kernel"));
+  c->phase_end(ev_ins);
+  c->count();
+  return 0;
+}
+
+// Events of the staging/insertion pipeline, one pair per FFT sub-batch slot.
+static int ensure_pipeline_events(spi_ctx* c, int nsubs) {
+  if (!c->ev_fork) {
+    SPI_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    SPI_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  }
+  while ((int)c->ev_ready.size() < nsubs) {
+    cudaEvent_t r, d;
+    SPI_CUDA(cudaEventCreateWithFlags(&r, cudaEventDisableTiming));
+    if (cudaEventCreateWithFlags(&d, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventDestroy(r);
+      return fail(kCuda, "cudaEventCreate failed");
+    }
+    c->ev_ready.push_back(r);
+    c->ev_done.push_back(d);
+  }
+  return 0;
+}
+
 static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
                           const uint8_t* half, int imgs_on_device) {
   if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert: no open reconstruction (spi_bp_open)");
@@ -1098,13 +1291,15 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   for (int a = 0; a < nimg; ++a)
     for (int s = 0; s < nsym; ++s) hs[(size_t)a * nsym + s].img = a % c->chunk;
   if (c->slice_order) {
-    // Within each chunk, order slices by the normal of their central plane
-    // (boustrophedon over rings of the polar angle) so that the slices in
-    // flight together touch overlapping voxels and their atomics hit in L2.
-    // The order only changes the FP32 summation order.
-    for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
-      const int nb = std::min(c->chunk, nimg - a0);
-      SliceDesc* base = hs + (size_t)a0 * nsym;
+    // Within each FFT sub-batch (one insertion launch), order slices by the
+    // normal of their central plane (boustrophedon over rings of the polar
+    // angle) so that the slices in flight together touch overlapping voxels
+    // and their atomics hit in L2.  The order only changes the FP32
+    // summation order.
+    for (int a0 = 0; a0 < nimg; a0 += c->chunk)
+      for (int b0 = a0; b0 < std::min(nimg, a0 + c->chunk); b0 += c->sub) {
+      const int nb = std::min(c->sub, std::min(nimg, a0 + c->chunk) - b0);
+      SliceDesc* base = hs + (size_t)b0 * nsym;
       const int m = nb * nsym;
       const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
       std::vector<std::pair<double, int>> key(m);
@@ -1151,95 +1346,80 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
     SPI_TRY(c->imgs2.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
     SPI_TRY(c->rtsq_prm.ensure((size_t)c->chunk * sizeof(RtsqParm)));
   }
+  // Two-stream pipeline.  The staging stream copies, rotates (RTSQ), pads and
+  // transforms FFT sub-batch b (images b0 .. b0+sub-1 of the chunk) and
+  // records ev_ready[b]; the library stream waits for it and launches the
+  // insertion of that sub-batch, then records ev_done[b], which the staging of
+  // the same sub-batch slot in the next chunk waits for before it overwrites
+  // the spectra.  Transforms and copies thus run under the (L2-atomic bound)
+  // insertion of the previous sub-batch.
+  const int nsubs = (c->chunk + c->sub - 1) / c->sub;
+  SPI_TRY(ensure_pipeline_events(c, nsubs));
+  cudaStream_t st = c->pipeline ? c->stream2 : c->stream;
+  SPI_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+  SPI_CUDA(cudaStreamWaitEvent(st, c->ev_fork, 0));
+  SPI_CUFFT(cufftSetStream(c->plan2d, st));
+  std::vector<char> done_valid(nsubs, 0);
+  float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
   for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
     const int nb = std::min(c->chunk, nimg - a0);
-    const float* src = imgs + (size_t)a0 * nx * nx;
-    if (!imgs_on_device) {
-      int ev = c->phase_begin(7);
-      SPI_CUDA(cudaMemcpyAsync(c->imgs.p, src, (size_t)nb * nx * nx * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-      c->phase_end(ev);
-      src = c->imgs.as<float>();
-    }
-    if (inplane) {
+    if (inplane)
       SPI_CUDA(cudaMemcpyAsync(c->rtsq_prm.p, rprm.data() + a0, (size_t)nb * sizeof(RtsqParm), cudaMemcpyHostToDevice,
-                               c->stream));
-      int ev = c->phase_begin(0);
-      rtsq_kernel<<<grid_blocks(c, (size_t)nb * nx * nx, 256), 256, 0, c->stream>>>(
-          src, c->imgs2.as<float>(), nx, nb, c->rtsq_prm.as<RtsqParm>());
-      SPI_TRY(check_kernel("rtsq_kernel"));
-      c->phase_end(ev);
-      c->count();
-      src = c->imgs2.as<float>();
-    }
-    for (int b0 = 0; b0 < nb; b0 += c->sub) {
+                               st));
+    // staging of every sub-batch of the chunk (staging stream)
+    for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
       const int nvalid = std::min(c->sub, nb - b0);
-      int ev = c->phase_begin(0);
-      stage_kernel<<<c->sub, 256, 0, c->stream>>>(src + (size_t)b0 * nx * nx, nx, n, ip, nvalid, klp,
-                                                 c->padded.as<float>());
+      if (done_valid[bi]) SPI_CUDA(cudaStreamWaitEvent(st, c->ev_done[bi], 0));
+      const float* src = imgs + ((size_t)a0 + b0) * nx * nx;
+      if (!imgs_on_device) {
+        int ev = c->phase_begin(7, st);
+        SPI_CUDA(cudaMemcpyAsync(c->imgs.as<float>() + (size_t)b0 * nx * nx, src,
+                                 (size_t)nvalid * nx * nx * sizeof(float), cudaMemcpyHostToDevice, st));
+        c->phase_end(ev);
+        src = c->imgs.as<float>() + (size_t)b0 * nx * nx;
+      }
+      if (inplane) {
+        int ev = c->phase_begin(0, st);
+        float* dst = c->imgs2.as<float>() + (size_t)b0 * nx * nx;
+        rtsq_kernel<<<grid_blocks(c, (size_t)nvalid * nx * nx, 256), 256, 0, st>>>(
+            src, dst, nx, nvalid, c->rtsq_prm.as<RtsqParm>() + b0);
+        SPI_TRY(check_kernel("rtsq_kernel"));
+        c->phase_end(ev);
+        c->count();
+        src = dst;
+      }
+      int ev = c->phase_begin(0, st);
+      stage_kernel<<<c->sub, 256, 0, st>>>(src, nx, n, ip, nvalid, klp, c->padded.as<float>());
       SPI_TRY(check_kernel("stage_kernel"));
       c->phase_end(ev);
       c->count();
       float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + (size_t)b0 * spec_plane;
-      ev = c->phase_begin(1);
+      ev = c->phase_begin(1, st);
       SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
       c->phase_end(ev);
       if (c->bf16) {
         const size_t cnt = (size_t)nvalid * spec_plane;
-        to_bf16_kernel<<<grid_blocks(c, cnt, 256), 256, 0, c->stream>>>(
+        to_bf16_kernel<<<grid_blocks(c, cnt, 256), 256, 0, st>>>(
             fout, reinterpret_cast<__nv_bfloat162*>(c->spectra.p) + (size_t)b0 * spec_plane, cnt);
         SPI_TRY(check_kernel("to_bf16_kernel"));
         c->count();
       }
+      SPI_CUDA(cudaEventRecord(c->ev_ready[bi], st));
     }
-    const void* spec = c->spectra.p;
+    // insertion of each sub-batch once its spectra are ready (library stream)
     SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
                              cudaMemcpyHostToDevice, c->stream));
-    const int nslices = nb * nsym;
-    float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
-    int ev_ins = c->phase_begin(2);
-    if (c->insert_mode == 1) {
-      const size_t smem = 5000 * sizeof(float);
-      const int threads = c->insert_threads;
-      int per_sm = 1;
-      if (c->bf16)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<true>, threads, smem);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_kernel<false>, threads, smem);
-      if (c->insert_blocks_per_sm > 0) per_sm = std::min(per_sm, c->insert_blocks_per_sm);
-      const int blocks = c->sm_count * std::max(per_sm, 1);
-      if (c->bf16)
-        insert_kernel<true><<<blocks, threads, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                                 c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1,
-                                                                 c->insert_seg_map);
-      else
-        insert_kernel<false><<<blocks, threads, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                                  c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1,
-                                                                  c->insert_seg_map);
-    } else {
-      const size_t smem = 3 * kTileCap * sizeof(float);
-      static bool attr_done = false;
-      if (!attr_done) {
-        cudaFuncSetAttribute(insert_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(insert_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_done = true;
-      }
-      int per_sm = 1;
-      if (c->bf16)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_tile_kernel<true>, 256, smem);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_tile_kernel<false>, 256, smem);
-      const int blocks = c->sm_count * std::max(per_sm, 1);
-      if (c->bf16)
-        insert_tile_kernel<true><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                                  c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
-      else
-        insert_tile_kernel<false><<<blocks, 256, smem, c->stream>>>(spec, c->slices.as<SliceDesc>(), nslices, nx,
-                                                                   c->kbtab.as<float>(), c->kb.fltb, c->gptr[0], g1);
+    for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
+      const int nvalid = std::min(c->sub, nb - b0);
+      SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_ready[bi], 0));
+      SPI_TRY(launch_insert(c, c->slices.as<SliceDesc>() + (size_t)b0 * nsym, nvalid * nsym, g1));
+      SPI_CUDA(cudaEventRecord(c->ev_done[bi], c->stream));
+      done_valid[bi] = 1;
     }
-    SPI_TRY(check_kernel("insert_kernel"));
-    c->phase_end(ev_ins);
-    c->count();
   }
+  // join: the library stream also waits for anything left on the staging stream
+  SPI_CUDA(cudaEventRecord(c->ev_join, st));
+  SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   c->pending_sym0[0] = true;
   if (c->ngrids == 2) c->pending_sym0[1] = true;
   SPI_CUDA(cudaStreamSynchronize(c->stream));

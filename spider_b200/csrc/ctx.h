@@ -6,7 +6,8 @@
 struct spi_ctx {
   int device = 0;
   int sm_count = 148;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // library stream: every call is ordered on it
+  cudaStream_t stream2 = nullptr;     // staging stream of the insertion pipeline
   long long launches = 0;
 
   // ---- Fourier gridding back-projection state ----
@@ -15,11 +16,14 @@ struct spi_ctx {
   bool pending_sym0[2] = {false, false};
   bool merged = false;
   int bf16 = 0;
-  int insert_mode = 1;                // 0 = tile-privatised, 1 = direct per-tap atomics
+  int insert_mode = 2;                // 0 = tile-privatised, 1 = direct per-tap atomics, 2 = x-tap lanes
   int slice_order = 1;                // 1 = order slices of a chunk by plane normal
   int insert_seg_map = 0;             // 1 = warps take 32-pixel row segments, 0 = whole rows
   int insert_threads = 256;           // threads per insert block
   int insert_blocks_per_sm = 0;       // 0 = as many as fit
+  int pipeline = 1;                   // 1 = stage/FFT on stream2 under the insertion
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
   int cg_fp64 = 1;                    // BP CG vectors/projections in FP64 (1) or FP32 (0)
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT
@@ -56,12 +60,12 @@ struct spi_ctx {
 
   // per-phase event timing
   bool timing = false;
-  struct PhaseEv { cudaEvent_t a, b; int phase; };
+  struct PhaseEv { cudaEvent_t a, b; int phase; cudaStream_t s; };
   std::vector<PhaseEv> ev_pending;
   std::vector<cudaEvent_t> ev_pool;
   double phase_ms[8] = {0};
   long long phase_n[8] = {0};
-  int phase_begin(int phase);   // returns slot or -1
+  int phase_begin(int phase, cudaStream_t s = nullptr);   // returns slot or -1; s = nullptr: stream
   void phase_end(int slot);
   void phase_collect();         // synchronises on recorded events
 

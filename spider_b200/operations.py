@@ -26,11 +26,17 @@ operation    answers (reference prompt order)
 ``BP CG``    image template, file numbers, radius, angles doc, L/F,
              reconstructed volume, 'error limit, chi^2 limit',
              'iteration limit, mode', lambda                   (bpcg.f:120-244)
+``BP CG 3``  image template, file numbers, radius, angles doc, L/F,
+             reconstructed volume, first sample volume, second sample volume,
+             limits, iteration limit & mode, lambda            (bpcg.f:139-244)
+``BP CG 3L`` as BP CG 3, with the file numbers of the first and of the second
+             sample after the image file numbers               (bpcg.f:143-152)
 ===========  =====================================================================
 
-The reference shuffles the BP 32F half sets with RANDOM_NUMBER
-(bp32f.f:543-553); here the first sample receives NANG/2 images chosen by a
-seeded permutation (``seed``), which keeps the half sizes of the reference.
+The reference shuffles the BP 32F and BP CG 3 half sets with RANDOM_NUMBER
+(bp32f.f:543-553, bpcg.f:1593-1632); here the first sample receives NANG/2
+images chosen by a seeded permutation (``seed``), which keeps the half sizes
+of the reference.
 """
 from __future__ import annotations
 
@@ -158,8 +164,13 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
                 sio.write_image(sio.expand_template(tmpl, i + 1 if conseq else k), proj[i], angles=ang[i])
         print(f"  PJ 3Q FINISHED FOR: {len(numbers):7d}   PROJECTIONS -----", file=results)
         return {"proj": proj}
-    if op == "BP CG":
+    if op in ("BP CG", "BP CG 3", "BP CG 3L"):
         numbers = sio.parse_numbers(a[1])
+        a = list(a)
+        lists = None
+        if op == "BP CG 3L":   # the two sample lists follow the image numbers
+            lists = (sio.parse_numbers(a[2]), sio.parse_numbers(a[3]))
+            del a[2:4]
         imgs = sio.read_images(a[0], numbers, ext)
         n = imgs.shape[1]
         print(f"  NUMBER OF IMAGES:{len(numbers):8d}", file=results)
@@ -167,13 +178,39 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
         ang = _angles(_name(a[3], ext), numbers)
         if a[4].strip().upper().startswith("F"):
             raise ops.SpiderError(101, "BP CG FBS interpolation is not built; use L")
-        errm, chim = (float(v) for v in a[6].replace(",", " ").split()[:2])
-        maxit, mode = (int(float(v)) for v in a[7].replace(",", " ").split()[:2])
-        lam = float(a[8])
-        vol, log = ops.bpcg(imgs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx)
-        print("  USING LINEAR INTERPOLATION", file=results)
-        for it, err, chi in log:   # bpcg.f:1213-1216
-            print(f"  ITERATION: {int(it):3d}  DIFFERENCE:{err:12.4E}  CHISQ:{chi:12.4E}", file=results)
+        k = 6 if op == "BP CG" else 8   # index of the 'error limit, chi^2 limit' answer
+        errm, chim = (float(v) for v in a[k].replace(",", " ").split()[:2])
+        maxit, mode = (int(float(v)) for v in a[k + 1].replace(",", " ").split()[:2])
+        lam = float(a[k + 2])
+
+        def _log(lg):
+            print("  USING LINEAR INTERPOLATION", file=results)
+            for it, err, chi in lg:   # bpcg.f:1213-1216
+                print(f"  ITERATION: {int(it):3d}  DIFFERENCE:{err:12.4E}  CHISQ:{chi:12.4E}", file=results)
+
+        if op == "BP CG":
+            vol, log = ops.bpcg(imgs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx)
+            _log(log)
+            sio.write_image(_name(a[5], ext), vol)
+            return {"vol": vol, "log": log}
+        if lists is None:
+            half = _half_sets(len(numbers), seed)
+            print(f"  Random lists: {int(half.sum())} {len(numbers) - int(half.sum())}", file=results)
+        else:
+            pos = {k2: i for i, k2 in enumerate(numbers)}
+            missing = [k2 for k2 in lists[0] + lists[1] if k2 not in pos]
+            if missing:
+                raise ops.SpiderError(102, f"SAMPLE LIST IMAGE {missing[0]} NOT IN THE IMAGE LIST")
+            sel = lists[0] + lists[1]
+            half = np.zeros(len(sel), np.uint8)
+            half[: len(lists[0])] = 1
+            imgs = imgs[[pos[k2] for k2 in sel]]
+            ang = ang[[pos[k2] for k2 in sel]]
+        vol, v1, v2, logs = ops.bpcg3(imgs, ang, half, ri, errm, chim, maxit, mode, lam, ctx=ctx)
+        for lg in logs:
+            _log(lg)
         sio.write_image(_name(a[5], ext), vol)
-        return {"vol": vol, "log": log}
+        sio.write_image(_name(a[6], ext), v1)
+        sio.write_image(_name(a[7], ext), v2)
+        return {"vol": vol, "vol1": v1, "vol2": v2, "logs": logs, "half": half}
     raise ops.SpiderError(101, f"operation {op!r} is not provided by this library")

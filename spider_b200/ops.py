@@ -319,6 +319,24 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     return vol, logv[: niter.value].copy()
 
 
+def bpcg3(projs, angles, half_mask, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
+          ctx: Context | None = None, fp64: bool = True):
+    """``BP CG 3``: the overall solution and one for each of two sample sets,
+    as three independent CG solves (bpcg.f:139-160,300-400).  ``half_mask[i]``
+    = 1 puts image i in the first sample (the reference draws the two lists
+    with MAKETWOLISTS, bpcg.f:1593-1632, or reads them for ``BP CG 3L``).
+    Returns (vol, vol1, vol2, (log, log1, log2))."""
+    projs = _host_f32(projs)
+    ang = _host_f32(angles)
+    m = np.asarray(half_mask).astype(bool).reshape(-1)
+    if m.shape[0] != projs.shape[0]:
+        raise SpiderError(101, "half mask length differs from the number of images")
+    v, lg = bpcg(projs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
+    v1, lg1 = bpcg(projs[m], ang[m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
+    v2, lg2 = bpcg(projs[~m], ang[~m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
+    return v, v1, v2, (lg, lg1, lg2)
+
+
 def cg_project(vol, angles, ri, *, ctx: Context | None = None):
     """PRJCQ_N (the BP CG projector A) of vol [n,n,n] -> [nang, n, n]."""
     ctx = ctx or default_context()

@@ -166,17 +166,21 @@ def test_insert_kernels_agree(ctx, orc):
     _, pr, ang = _case(nx, nimg, 61)
     # include orientations that put the x = 0 flip line inside many tiles
     ang[:40, 1] = 90.0
-    out = {}
-    for mode in ("direct", "tile"):
+    out, grids = {}, {}
+    for mode in ("direct", "tile", "xlane"):
         os.environ["SPI_INSERT"] = mode
         try:
             out[mode] = ops.bp3f(pr, ang, ctx=ctx)
+            grids[mode] = ops.bp3f_partial(pr, ang, ctx=ctx)
         finally:
             del os.environ["SPI_INSERT"]
     ref = orc.bp3f(pr, ang, prec=1, nthreads=1)
     for mode, v in out.items():
         assert synth.rel_l2(v, out["direct"]) <= 2e-6, mode
         assert synth.rel_l2(v, ref) <= TOL, mode
+        # the gridded X and W themselves: same taps, only the summation order differs
+        for a, b in zip(grids[mode], grids["direct"]):
+            assert synth.rel_l2(a, b) <= 1e-6, mode
 
 
 def test_rb3f_rb32f_match_oracle(ctx, orc):

@@ -99,3 +99,34 @@ def test_pj3q_and_partial_merge_procedures(ctx, orc, tmp_path):
     merged, _ = sio.read_image(tmp_path / "merged.spi")
     full, _ = sio.read_image(tmp_path / "full.spi")
     assert synth.rel_l2(merged, full) <= 1e-5
+
+
+def test_bpcg3_procedures(ctx, orc, tmp_path):
+    """BP CG 3 (random sample lists) and BP CG 3L (given lists): three
+    independent CG solutions, each checked against the FP64 oracle."""
+    t = str(tmp_path)
+    rng = np.random.default_rng(9)
+    vol = synth.blob_phantom(32, 6, sigma=(2, 4), radius=10, rng=rng)
+    sio.write_doc(tmp_path / "cgang.spi", synth.so3_angles(24, rng).tolist())
+    doc = sio.read_doc(tmp_path / "cgang.spi")
+    ang = np.array([doc[k][:3] for k in range(1, 25)], np.float32)
+    prj = orc.pj3q(vol, ang, 14.0)
+    sio.write_stack(tmp_path / "cg.spi", prj)
+    kw = dict(errm=1e-6, chim=0.0, maxit=4, mode=1, lam=0.5, prec=1)
+    tail = ["1.0E-6, 0.0", "4,1", "0.5"]
+    out = io.StringIO()
+    r = operations.run("BP CG 3", [f"{t}/cg@***", "1-24", "14", f"{t}/cgang", "L", f"{t}/v", f"{t}/v1",
+                                   f"{t}/v2"] + tail, ctx=ctx, results=out, seed=3)
+    half = r["half"].astype(bool)
+    assert half.sum() == 12
+    for name, sel in (("v", np.ones(24, bool)), ("v1", half), ("v2", ~half)):
+        got, _ = sio.read_image(tmp_path / f"{name}.spi")
+        ref = orc.bpcg(prj[sel], ang[sel], 14.0, **kw)[0]
+        assert synth.rel_l2(got, ref) <= 1e-4, name
+    assert "Random lists" in out.getvalue()
+    operations.run("BP CG 3L", [f"{t}/cg@***", "1-24", "1-10", "11-24", "14", f"{t}/cgang", "L", f"{t}/w",
+                                f"{t}/w1", f"{t}/w2"] + tail, ctx=ctx, results=io.StringIO())
+    for name, sel in (("w1", slice(0, 10)), ("w2", slice(10, 24))):
+        got, _ = sio.read_image(tmp_path / f"{name}.spi")
+        ref = orc.bpcg(prj[sel], ang[sel], 14.0, **kw)[0]
+        assert synth.rel_l2(got, ref) <= 1e-4, name
