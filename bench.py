@@ -70,15 +70,9 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def insert_kernel_name():
-    """The insertion kernel the library launches (SPI_INSERT selects another)."""
-    return {"direct": "insert_kernel", "tile": "insert_tile_kernel"}.get(os.environ.get("SPI_INSERT", ""),
-                                                                         "insert_xlane_kernel")
-
-
-def traffic_per_image():
+def traffic_per_image(kernel):
     """DRAM bytes per image of the insert kernel, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"{insert_kernel_name()}_traffic.txt")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -238,7 +232,8 @@ def cg_measure(args, ctx, stream, rank, world):
 
     out = {}
     vols = {}
-    for name, fp64, graph in (("fp64_graph", True, True), ("fp64_plain", True, False), ("fp32_graph", False, True)):
+    for name, fp64, graph in (("fp64_graph", True, True), ("fp64_plain", True, False), ("fp32_graph", False, True),
+                              ("mixed_graph", "mixed", True)):
         if not graph:
             os.environ["SPI_CG_NOGRAPH"] = "1"
         try:
@@ -249,11 +244,17 @@ def cg_measure(args, ctx, stream, rank, world):
             os.environ.pop("SPI_CG_NOGRAPH", None)
         out[name] = (tk - t1) / K
         vols[name] = v
-    rel = float(np.linalg.norm((vols["fp32_graph"] - vols["fp64_graph"]).ravel()) /
-                max(np.linalg.norm(vols["fp64_graph"].ravel()), 1e-30))
-    res = {"metric": "BP CG s/iter", "unit": "s/iter", "value": out["fp64_graph"],
+    def rel(name):
+        return float(np.linalg.norm((vols[name] - vols["fp64_graph"]).ravel()) /
+                     max(np.linalg.norm(vols["fp64_graph"].ravel()), 1e-30))
+    # headline: the fastest form within 1e-4 of the FP64 iteration
+    ok = [k for k in ("mixed_graph", "fp32_graph") if rel(k) <= 1e-4] + ["fp64_graph"]
+    best = min(ok, key=lambda k: out[k])
+    res = {"metric": "BP CG s/iter", "unit": "s/iter", "value": out[best], "form": best,
+           "fp64_s_per_iter": out["fp64_graph"],
            "plain_gpu_s_per_iter": out["fp64_plain"], "fp32_vectors_s_per_iter": out["fp32_graph"],
-           "rel_err_fp32_vs_fp64": rel,
+           "mixed_s_per_iter": out["mixed_graph"],
+           "rel_err_fp32_vs_fp64": rel("fp32_graph"), "rel_err_mixed_vs_fp64": rel("mixed_graph"),
            "config": {"n": n, "images": nang, "lambda": 1e-3, "mode": 1, "iterations_timed": K,
                       "phantom": "50 Gaussian blobs, sigma 2-8, SNR 0.3, uniform SO(3)"}}
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -362,6 +363,7 @@ def run_ours(args):
         ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                         ctypes.c_void_p(grids[1].data_ptr())))
     ctx.bp_open(nx, 2, bf16=args.bf16)
+    launch_cfg = ctx.bp_autotune()          # kernel variant and launch shape, timed on this GPU
 
     def barrier():
         if world > 1:
@@ -430,10 +432,10 @@ def run_ours(args):
     # bytes over the summed launch durations (CUDA events around each launch)
     achieved = bytes_per_img * chunk * args.steps / (insert_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    tpi = traffic_per_image()
+    tpi = traffic_per_image(launch_cfg["kernel"])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": (tpi * chunk) if tpi else None,
-            "kernel": insert_kernel_name(), "peak_kind": peak_kind,
+            "traffic": (tpi * chunk * args.steps / n_insert) if tpi else None,
+            "kernel": launch_cfg["kernel"], "launch": launch_cfg, "peak_kind": peak_kind,
             "algorithmic_bytes_per_image": bytes_per_img, "taps_per_image": taps,
             "launch_ms": insert_ms / n_insert, "launches": n_insert,
             "images_per_launch": chunk * args.steps / n_insert}
@@ -442,12 +444,21 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         host_chunks = [c.cpu().pin_memory() for c in chunks]
+        L.spi_ctx_set_timing(ctx.handle, 0)   # per-phase events are not part of the e2e path
         ctx.bp_close()
         if world > 1:
             ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                             ctypes.c_void_p(grids[1].data_ptr())))
         hvol = [torch.empty((nx, nx, nx), dtype=torch.float32).pin_memory() for _ in range(3)]
         ctx.bp_open(nx, 2, bf16=args.bf16)
+        ctx.bp_autotune()                   # cached choice
+        for i in range(min(args.warmup, 1)):  # first host-image call (events, buffers)
+            ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
+                                      angles[i].ctypes.data_as(ctypes.c_void_p),
+                                      halves[i].ctypes.data_as(ctypes.c_void_p), 0))
+        ctx.bp_close()
+        ctx.bp_open(nx, 2, bf16=args.bf16)
+        ctx.bp_autotune()
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)

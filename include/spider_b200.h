@@ -101,6 +101,21 @@ int spi_bp_grid_bytes(int nx, long long* bytes);
 /* Spectrum storage for subsequent inserts: 0 = FP32 (default), 1 = BF16. */
 int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
 
+/* Autotune the insertion launch of the open reconstruction (no counterpart
+ * in the reference, whose insertion is a fixed OpenMP loop): times the
+ * kernel variants and launch shapes on one sub-batch of synthetic slices,
+ * keeps the fastest and zeroes the grids again.  Call it right after
+ * spi_bp_open (and spi_bp_set_spectrum_precision); it fails with 101 once
+ * images have been inserted.  The choice is cached per (device, nx, number of
+ * grids, spectrum precision, symmetry count) for the process; force = 1
+ * measures again. */
+int spi_bp_autotune(spi_ctx* ctx, int force);
+
+/* The insertion launch in use: kernel (0 tile, 1 direct, 2 five x-tap lanes,
+ * 3 four lanes over the nonzero window), threads per CTA, CTAs per SM, and
+ * the autotuner's time of one sample launch in ms (0 when not tuned). */
+int spi_bp_get_launch(const spi_ctx* ctx, int* kernel, int* threads, int* blocks_per_sm, float* tuned_ms);
+
 /* Insert `nimg` images (float[nimg*nx*nx]) with their angles
  * (float[nimg*3], host) and optional half mask (uint8[nimg], host; NULL
  * routes every image to grid 0).  Replaces the body of the BP3FQ image loop
@@ -195,11 +210,13 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
              float* vol_out, float* log_out, int* niter_out);
 
 /* Storage and accumulation type of the BP CG vectors and projections:
- * fp64 = 1 (default) keeps CB, BCKP, BCKE, BCKN and the projections in
+ * mode = 1 (default) keeps CB, BCKP, BCKE, BCKN and the projections in
  * FP64 (the reference keeps them in REAL; its FP32 CG drifts from the exact
- * iteration by more than 1e-2 at small LAMBDA); fp64 = 0 uses FP32 as the
- * reference does.  Scalars (DELSQ, AKDEN, P, Q) are FP64 in both. */
-int spi_ctx_set_cg_precision(spi_ctx* ctx, int fp64);
+ * iteration by more than 1e-2 at small LAMBDA); mode = 0 uses FP32 as the
+ * reference does; mode = 2 is mode 1 with each projection (PRJCQ_N)
+ * accumulated in FP32 shared memory before it is stored in FP64.  Scalars
+ * (DELSQ, AKDEN, P, Q) and dot products are FP64 in all modes. */
+int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
 
 /* One application of the BP CG operators on device arrays, for the
  * differentiable wrapper and adjointness checks.  spi_cg_project: PRJCQ_N

@@ -32,6 +32,9 @@ SIGNATURES = [
     ("spi_bp_attach_grids", ctypes.c_int, [_vp, _vp, _vp]),
     ("spi_bp_grid_bytes", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
     ("spi_bp_set_spectrum_precision", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("spi_bp_autotune", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("spi_bp_get_launch", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
     ("spi_bp_insert", ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
     ("spi_bp_insert_rb", ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]),
     ("spi_bp_finish", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),

@@ -11,6 +11,10 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <cmath>
 #include <cstring>
 
@@ -308,11 +312,18 @@ __global__ void __launch_bounds__(512) insert_kernel(const void* __restrict__ sp
 // ones.  A lane whose tap falls below x = 0 (IXN < LN2) adds the reflected
 // point instead (oneline.f:118-150), so every lane issues exactly one atomic
 // per (LY, LZ).  Every voxel and weight is computed as in insert_kernel.
+//
+// Rows are handed out in slice-major order by a work counter (one atomic per
+// row and warp) rather than by a fixed grid stride: the warps then stay on
+// neighbouring rows of the same few slices for the whole launch, and the
+// voxels they update stay resident in L2 (with a fixed stride fast and slow
+// warps drift apart and the set of slices in flight grows with the launch).
 template <bool BF16>
 __global__ void __launch_bounds__(512) insert_xlane_kernel(const void* __restrict__ spec,
                                                            const SliceDesc* __restrict__ slices, int nslices, int nx,
                                                            const float* __restrict__ kbtab, float fltb,
-                                                           float4* __restrict__ g0, float4* __restrict__ g1) {
+                                                           float4* __restrict__ g0, float4* __restrict__ g1,
+                                                           unsigned long long* __restrict__ work) {
   extern __shared__ float tab[];
   for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
   __syncthreads();
@@ -323,13 +334,15 @@ __global__ void __launch_bounds__(512) insert_xlane_kernel(const void* __restric
   const int lane = threadIdx.x & 31;
   const int g = lane / 5;           // pixel of the group of six (g = 6: idle lanes 30, 31)
   const int lx = lane - 5 * g;      // x tap 0..4
-  const int warps_per_block = blockDim.x >> 5;
   const long long nitems = (long long)nslices * N;
   const size_t rowlen = (size_t)(nx + 1);
   const size_t plane = (size_t)N * rowlen;
 
-  for (long long item = (long long)blockIdx.x * warps_per_block + (threadIdx.x >> 5); item < nitems;
-       item += (long long)gridDim.x * warps_per_block) {
+  for (;;) {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(work, 1ull);
+    const long long item = (long long)__shfl_sync(0xffffffffu, it, 0);
+    if (item >= nitems) break;
     const int s = (int)(item / N);
     const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
     const SliceDesc sd = slices[s];
@@ -390,6 +403,134 @@ __global__ void __launch_bounds__(512) insert_xlane_kernel(const void* __restric
       }
     }
   }
+}
+
+// ----------------------------------------------------------------------------
+// Insert, four lanes per pixel over the nonzero taps.  The generalised
+// Kaiser-Bessel table is zero from distance ~1.8 on (0.9 of the two-voxel
+// half width), so along each axis the tap at offset -2 is nonzero only when
+// the coordinate lies more than 0.2 below its nearest voxel and the tap at +2
+// only when it lies more than 0.2 above: at most four of the five taps are
+// nonzero, in the window [-2, 1] or [-1, 2].  A warp takes one row J of one
+// slice, eight pixels at a time; lanes 4g..4g+3 share pixel I0+g, lane 4g+q
+// owns x tap XS+q of the window, and each lane loops over the 4 x 4 (Y, Z)
+// window.  Window starts are read from the same table lookups the taps use
+// (offset -2 nonzero => window [-2, 1]); the host verifies that the table is
+// zero beyond distance 2, which makes the window exact.  Compared with five
+// lanes over all 5 x 5 (Y, Z) taps this issues 2 instead of 4.2 atomic
+// instructions per pixel and uses every lane.  Each voxel and weight (and
+// the reflected points of oneline.f:118-150) is computed as in insert_kernel;
+// taps outside the window have zero weight, which the reference skips too.
+__device__ __forceinline__ float kb_tap(const float* tab, float v, int k, float fltb) {
+  return tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb))];
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__ spec,
+                                                        const SliceDesc* __restrict__ slices, int nslices, int nx,
+                                                        const float* __restrict__ kbtab, float fltb,
+                                                        float4* __restrict__ g0, float4* __restrict__ g1,
+                                                        unsigned long long* __restrict__ work) {
+  extern __shared__ float tab[];
+  for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
+  __syncthreads();
+
+  const int N = 2 * nx, N2 = nx, LN2 = 2;
+  const int NN4 = N * N / 4;
+  const float fN = (float)N;
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2;          // pixel of the group of eight
+  const int q = lane & 3;           // x tap of the window
+  const int gl = lane & ~3;         // first lane of the group
+  const long long nitems = (long long)nslices * N;
+  const size_t rowlen = (size_t)(nx + 1);
+  const size_t plane = (size_t)N * rowlen;
+
+  for (;;) {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(work, 1ull);
+    const long long item = (long long)__shfl_sync(0xffffffffu, it, 0);
+    if (item >= nitems) break;
+    const int s = (int)(item / N);
+    const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
+    const SliceDesc sd = slices[s];
+    float4* G = sd.grid ? g1 : g0;
+    const int JP = (J >= 0) ? J : N + J;
+    const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
+    const float fJ = (float)J;
+    const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
+    for (int I0 = 0; I0 <= N2 && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+      const int I = I0 + g;
+      bool ok = I <= N2 && (I * I + J * J) < NN4 && !(I == 0 && J < 0);
+      const float fI = (float)I;
+      float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
+      float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
+      float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
+      float br = 0.0f, bi = 0.0f;
+      if (ok) {
+        const float2 sp = load_spec<BF16>(spec, specrow + I);
+        br = sp.x;
+        bi = -sp.y;   // SPIDER forward sign = conjugate of the cuFFT R2C output
+      }
+      if (xnew < 0.0f) {
+        xnew = -xnew; ynew = -ynew; znew = -znew;
+        bi = -bi;
+      }
+      const int ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
+      const int iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
+      const int izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
+      ok = ok && ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+           izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1);
+      if (!ok) { xnew = ynew = znew = 0.0f; }   // keeps the lookups below in range; no taps follow
+      const int ix0 = ok ? ixn : 0, iy0 = ok ? iyn : 0, iz0 = ok ? izn : 0;
+      const int xs = kb_tap(tab, xnew, ix0 - 2, fltb) != 0.0f ? ix0 - 2 : ix0 - 1;
+      const int ys = kb_tap(tab, ynew, iy0 - 2, fltb) != 0.0f ? iy0 - 2 : iy0 - 1;
+      const int zs = kb_tap(tab, znew, iz0 - 2, fltb) != 0.0f ? iz0 - 2 : iz0 - 1;
+      const float tx = kb_tap(tab, xnew, xs + q, fltb);
+      const float tyq = kb_tap(tab, ynew, ys + q, fltb);
+      const float tzq = kb_tap(tab, znew, zs + q, fltb);
+      float ty[4], tz[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        ty[l] = __shfl_sync(0xffffffffu, tyq, gl + l);
+        tz[l] = __shfl_sync(0xffffffffu, tzq, gl + l);
+      }
+      if (!ok || tx == 0.0f) continue;
+      // main tap at (ixp, iyp, izp), or for ixp < 0 the reflected point
+      // (-ixp, -iyp, -izp) with the conjugate value
+      const int ixp = xs + q;
+      const bool refl = ixp < 0;
+      const float bis = refl ? -bi : bi;
+      const int ixa = refl ? -ixp : ixp;
+#pragma unroll
+      for (int lz = 0; lz < 4; ++lz) {
+        if (tz[lz] == 0.0f) continue;
+        const int izp = zs + lz;
+        const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
+#pragma unroll
+        for (int ly = 0; ly < 4; ++ly) {
+          const float tyz = __fmul_rn(ty[ly], tz[lz]);
+          if (tyz == 0.0f) continue;
+          const int iyp = ys + ly;
+          const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
+          const float wg = __fmul_rn(tx, tyz);
+          if (wg != 0.0f)
+            atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
+                      make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
+        }
+      }
+    }
+  }
+}
+
+// True when the table is zero for every distance >= 2 (index nint(2*fltb)
+// and above, less one for rounding), the condition under which at most four
+// consecutive taps of the five are nonzero (insert_x4_kernel).
+static bool kb_window4_ok(const KBTab& kb) {
+  const int i0 = std::max(0, (int)std::floor(2.0 * kb.fltb) - 1);
+  for (int i = i0; i < 5000; ++i)
+    if (kb.tab[i] != 0.0f) return false;
+  return true;
 }
 
 // ----------------------------------------------------------------------------
@@ -876,6 +1017,7 @@ void bp_release(spi_ctx* c) {
   c->spectra.release();
   c->spec_tmp.release();
   c->slices.release();
+  c->workctr.release();
   c->cplx.release();
   c->real3.release();
   c->wkb.release();
@@ -950,6 +1092,7 @@ void spi_ctx::phase_collect() {
 long long spi_ctx::device_bytes() const {
   long long t = 0;
   const DevBuf* bufs[] = {&grid[0], &grid[1], &kbtab, &imgs, &padded, &spectra, &spec_tmp, &slices, &cplx, &real3,
+                          &workctr,
                           &wkb, &acc, &volbuf, &pj_vol, &pj_out, &pj_runs, &pj_dm};
   for (auto b : bufs) t += (long long)b->bytes;
   for (auto& b : cg_buf) t += (long long)b.bytes;
@@ -1073,6 +1216,7 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   c->nx = nx;
   c->n = 2 * nx;
   c->ngrids = ngrids;
+  c->inserted = false;
   c->nsym = nsym > 1 ? nsym : 1;
   c->sym_dm.assign((size_t)9 * c->nsym, 0.0f);
   if (nsym > 1)
@@ -1091,13 +1235,15 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
     }
     SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
   }
-  // chunk sizes: spectra of one chunk <= ~4.3 GB FP32, FFT sub-batch <= ~256 MB padded
+  // chunk sizes: spectra of one chunk <= ~4.3 GB FP32
   const size_t spec_per_img = (size_t)c->n * (nx + 1) * sizeof(float2);
   int chunk = (int)std::min<size_t>(8192, std::max<size_t>(64, (size_t)4400000000ull / spec_per_img));
   chunk = env_int("SPI_BP_CHUNK", chunk);
   {
     const char* m = getenv("SPI_INSERT");
-    c->insert_mode = (m && strcmp(m, "tile") == 0) ? 0 : (m && strcmp(m, "direct") == 0) ? 1 : 2;
+    const int def_mode = kb_window4_ok(c->kb) ? 3 : 2;
+    c->insert_mode = !m ? def_mode : strcmp(m, "tile") == 0 ? 0 : strcmp(m, "direct") == 0 ? 1
+                   : strcmp(m, "xlane") == 0 ? 2 : def_mode;
     const char* o = getenv("SPI_SLICE_ORDER");
     c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
     const char* mp = getenv("SPI_INSERT_MAP");
@@ -1116,8 +1262,13 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
       c->insert_threads = def_threads;
     c->insert_blocks_per_sm = env_int("SPI_INSERT_BLOCKS_PER_SM", def_bps);
   }
-  int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)268435456ull / ((size_t)c->n * c->n * 4)));
+  // FFT sub-batch (and insert launch): padded images <= 1 GB.  Larger batches
+  // transform faster and, with the dynamic row counter, launch size no longer
+  // costs insertion speed (measured at 256^3: 1,024 and 4,096 alike).
+  int sub = (int)std::min<size_t>((size_t)chunk, std::max<size_t>(8, (size_t)1073741824ull / ((size_t)c->n * c->n * 4)));
+  sub = std::max(1, std::min(chunk, env_int("SPI_BP_SUB", sub)));
   c->sub = sub;
+  c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
   c->chunk = ((chunk + sub - 1) / sub) * sub;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
@@ -1200,7 +1351,7 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
   const float fltb = c->kb.fltb;
   float4* g0 = c->gptr[0];
   int ev_ins = c->phase_begin(2);
-  if (c->insert_mode == 1 || c->insert_mode == 2) {
+  if (c->insert_mode >= 1) {
     const size_t smem = 5000 * sizeof(float);
     const int threads = c->insert_threads;
     if (c->insert_mode == 1) {
@@ -1211,23 +1362,39 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
         insert_kernel<false><<<insert_blocks(c, insert_kernel<false>, threads, smem, c->insert_blocks_per_sm),
                                threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1,
                                                            c->insert_seg_map);
+    } else if (c->insert_mode == 3) {
+      SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
+      auto* work = c->workctr.as<unsigned long long>();
+      SPI_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), c->stream));
+      if (c->bf16)
+        insert_x4_kernel<true><<<insert_blocks(c, insert_x4_kernel<true>, threads, smem, c->insert_blocks_per_sm),
+                                 threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
+      else
+        insert_x4_kernel<false><<<insert_blocks(c, insert_x4_kernel<false>, threads, smem, c->insert_blocks_per_sm),
+                                  threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
     } else {
+      // row counter of this launch (launches on the library stream are serialised)
+      SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
+      auto* work = c->workctr.as<unsigned long long>();
+      SPI_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), c->stream));
       if (c->bf16)
         insert_xlane_kernel<true><<<insert_blocks(c, insert_xlane_kernel<true>, threads, smem,
                                                   c->insert_blocks_per_sm),
-                                    threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1);
+                                    threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
       else
         insert_xlane_kernel<false><<<insert_blocks(c, insert_xlane_kernel<false>, threads, smem,
                                                    c->insert_blocks_per_sm),
-                                     threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1);
+                                     threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
     }
   } else {
     const size_t smem = 3 * kTileCap * sizeof(float);
-    static bool attr_done = false;
-    if (!attr_done) {
+    // the attribute is per device; set once per device (several threads may race here harmlessly)
+    static std::atomic<unsigned long long> attr_done{0};
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_done.load() & bit)) {
       cudaFuncSetAttribute(insert_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(insert_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_done = true;
+      attr_done.fetch_or(bit);
     }
     if (c->bf16)
       insert_tile_kernel<true><<<insert_blocks(c, insert_tile_kernel<true>, 256, smem, 0), 256, smem, c->stream>>>(
@@ -1269,6 +1436,7 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   if (nimg == 0) return 0;
   SPI_CUDA(cudaSetDevice(c->device));
   SPI_TRY(ensure_chunk_buffers(c));
+  c->inserted = true;
   const int nx = c->nx, n = c->n, nsym = c->nsym;
   // slice descriptors for the whole call (host, pinned)
   const size_t nsl = (size_t)nimg * nsym;
@@ -1297,8 +1465,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
     // and their atomics hit in L2.  The order only changes the FP32
     // summation order.
     for (int a0 = 0; a0 < nimg; a0 += c->chunk)
-      for (int b0 = a0; b0 < std::min(nimg, a0 + c->chunk); b0 += c->sub) {
-      const int nb = std::min(c->sub, std::min(nimg, a0 + c->chunk) - b0);
+      for (int b0 = a0; b0 < std::min(nimg, a0 + c->chunk); b0 += c->sort_group) {
+      const int nb = std::min(c->sort_group, std::min(nimg, a0 + c->chunk) - b0);
       SliceDesc* base = hs + (size_t)b0 * nsym;
       const int m = nb * nsym;
       const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
@@ -1346,87 +1514,222 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
     SPI_TRY(c->imgs2.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
     SPI_TRY(c->rtsq_prm.ensure((size_t)c->chunk * sizeof(RtsqParm)));
   }
-  // Two-stream pipeline.  The staging stream copies, rotates (RTSQ), pads and
-  // transforms FFT sub-batch b (images b0 .. b0+sub-1 of the chunk) and
-  // records ev_ready[b]; the library stream waits for it and launches the
-  // insertion of that sub-batch, then records ev_done[b], which the staging of
-  // the same sub-batch slot in the next chunk waits for before it overwrites
-  // the spectra.  Transforms and copies thus run under the (L2-atomic bound)
-  // insertion of the previous sub-batch.
+  // Copy pipeline.  With host images, the copy stream uploads the chunk in
+  // pieces of `up` images (<= ~64 MB) and records ev_ready per piece; the
+  // library stream waits for each piece, rotates (RTSQ) and pads it, then
+  // transforms and inserts the FFT sub-batch and records ev_done for it once
+  // its images have been padded; the upload into the same sub-batch slot in
+  // the next chunk waits for that.  Uploads thus run under the transforms and
+  // the insertion, and only the first piece of a call is exposed.  (Running
+  // the transforms beside the insertion gains nothing: both are bound by the
+  // memory system, measured.)
   const int nsubs = (c->chunk + c->sub - 1) / c->sub;
-  SPI_TRY(ensure_pipeline_events(c, nsubs));
-  cudaStream_t st = c->pipeline ? c->stream2 : c->stream;
-  SPI_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-  SPI_CUDA(cudaStreamWaitEvent(st, c->ev_fork, 0));
-  SPI_CUFFT(cufftSetStream(c->plan2d, st));
+  const bool copy_pipe = !imgs_on_device && c->pipeline;
+  const int up = imgs_on_device ? c->sub
+                                : std::max(1, std::min(c->sub, (int)((64ull << 20) / ((size_t)nx * nx * sizeof(float)))));
+  const int ppsub = (c->sub + up - 1) / up;
+  SPI_TRY(ensure_pipeline_events(c, nsubs * ppsub));
+  cudaStream_t cs = copy_pipe ? c->stream2 : c->stream;
+  if (copy_pipe) {
+    SPI_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+    SPI_CUDA(cudaStreamWaitEvent(cs, c->ev_fork, 0));
+  }
+  SPI_CUFFT(cufftSetStream(c->plan2d, c->stream));
   std::vector<char> done_valid(nsubs, 0);
   float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
   for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
     const int nb = std::min(c->chunk, nimg - a0);
     if (inplane)
       SPI_CUDA(cudaMemcpyAsync(c->rtsq_prm.p, rprm.data() + a0, (size_t)nb * sizeof(RtsqParm), cudaMemcpyHostToDevice,
-                               st));
-    // staging of every sub-batch of the chunk (staging stream)
+                               c->stream));
+    SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
+                             cudaMemcpyHostToDevice, c->stream));
+    if (!imgs_on_device) {   // uploads of the whole chunk, ahead of the compute
+      for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
+        const int nvalid = std::min(c->sub, nb - b0);
+        if (done_valid[bi]) SPI_CUDA(cudaStreamWaitEvent(cs, c->ev_done[bi], 0));
+        for (int p0 = b0, pi = 0; p0 < b0 + nvalid; p0 += up, ++pi) {
+          const int np = std::min(up, b0 + nvalid - p0);
+          // (no timing events on the copy stream: recording them there was
+          // measured to serialise the uploads with the compute)
+          int ev = copy_pipe ? -1 : c->phase_begin(7, cs);
+          SPI_CUDA(cudaMemcpyAsync(c->imgs.as<float>() + (size_t)p0 * nx * nx, imgs + ((size_t)a0 + p0) * nx * nx,
+                                   (size_t)np * nx * nx * sizeof(float), cudaMemcpyHostToDevice, cs));
+          c->phase_end(ev);
+          SPI_CUDA(cudaEventRecord(c->ev_ready[(size_t)bi * ppsub + pi], cs));
+        }
+      }
+    }
     for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
       const int nvalid = std::min(c->sub, nb - b0);
-      if (done_valid[bi]) SPI_CUDA(cudaStreamWaitEvent(st, c->ev_done[bi], 0));
-      const float* src = imgs + ((size_t)a0 + b0) * nx * nx;
-      if (!imgs_on_device) {
-        int ev = c->phase_begin(7, st);
-        SPI_CUDA(cudaMemcpyAsync(c->imgs.as<float>() + (size_t)b0 * nx * nx, src,
-                                 (size_t)nvalid * nx * nx * sizeof(float), cudaMemcpyHostToDevice, st));
-        c->phase_end(ev);
-        src = c->imgs.as<float>() + (size_t)b0 * nx * nx;
-      }
-      if (inplane) {
-        int ev = c->phase_begin(0, st);
-        float* dst = c->imgs2.as<float>() + (size_t)b0 * nx * nx;
-        rtsq_kernel<<<grid_blocks(c, (size_t)nvalid * nx * nx, 256), 256, 0, st>>>(
-            src, dst, nx, nvalid, c->rtsq_prm.as<RtsqParm>() + b0);
-        SPI_TRY(check_kernel("rtsq_kernel"));
+      for (int p0 = b0, pi = 0; p0 < b0 + nvalid; p0 += up, ++pi) {
+        const int np = std::min(up, b0 + nvalid - p0);
+        const bool last = p0 + up >= b0 + nvalid;
+        const float* src;
+        if (!imgs_on_device) {
+          if (copy_pipe) SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_ready[(size_t)bi * ppsub + pi], 0));
+          src = c->imgs.as<float>() + (size_t)p0 * nx * nx;
+        } else {
+          src = imgs + ((size_t)a0 + p0) * nx * nx;
+        }
+        if (inplane) {
+          int ev = c->phase_begin(0);
+          float* dst = c->imgs2.as<float>() + (size_t)p0 * nx * nx;
+          rtsq_kernel<<<grid_blocks(c, (size_t)np * nx * nx, 256), 256, 0, c->stream>>>(
+              src, dst, nx, np, c->rtsq_prm.as<RtsqParm>() + p0);
+          SPI_TRY(check_kernel("rtsq_kernel"));
+          c->phase_end(ev);
+          c->count();
+          src = dst;
+        }
+        // the last piece also zero-pads the unused tail of the FFT batch
+        const int blocks = last ? c->sub - (p0 - b0) : np;
+        int ev = c->phase_begin(0);
+        stage_kernel<<<blocks, 256, 0, c->stream>>>(src, nx, n, ip, np, klp,
+                                                    c->padded.as<float>() + (size_t)(p0 - b0) * n * n);
+        SPI_TRY(check_kernel("stage_kernel"));
         c->phase_end(ev);
         c->count();
-        src = dst;
       }
-      int ev = c->phase_begin(0, st);
-      stage_kernel<<<c->sub, 256, 0, st>>>(src, nx, n, ip, nvalid, klp, c->padded.as<float>());
-      SPI_TRY(check_kernel("stage_kernel"));
-      c->phase_end(ev);
-      c->count();
+      SPI_CUDA(cudaEventRecord(c->ev_done[bi], c->stream));   // the uploaded images are consumed
+      done_valid[bi] = 1;
       float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + (size_t)b0 * spec_plane;
-      ev = c->phase_begin(1, st);
+      int ev = c->phase_begin(1);
       SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
       c->phase_end(ev);
       if (c->bf16) {
         const size_t cnt = (size_t)nvalid * spec_plane;
-        to_bf16_kernel<<<grid_blocks(c, cnt, 256), 256, 0, st>>>(
+        to_bf16_kernel<<<grid_blocks(c, cnt, 256), 256, 0, c->stream>>>(
             fout, reinterpret_cast<__nv_bfloat162*>(c->spectra.p) + (size_t)b0 * spec_plane, cnt);
         SPI_TRY(check_kernel("to_bf16_kernel"));
         c->count();
       }
-      SPI_CUDA(cudaEventRecord(c->ev_ready[bi], st));
-    }
-    // insertion of each sub-batch once its spectra are ready (library stream)
-    SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
-                             cudaMemcpyHostToDevice, c->stream));
-    for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
-      const int nvalid = std::min(c->sub, nb - b0);
-      SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_ready[bi], 0));
       SPI_TRY(launch_insert(c, c->slices.as<SliceDesc>() + (size_t)b0 * nsym, nvalid * nsym, g1));
-      SPI_CUDA(cudaEventRecord(c->ev_done[bi], c->stream));
-      done_valid[bi] = 1;
     }
   }
-  // join: the library stream also waits for anything left on the staging stream
-  SPI_CUDA(cudaEventRecord(c->ev_join, st));
-  SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  if (copy_pipe) {   // join
+    SPI_CUDA(cudaEventRecord(c->ev_join, cs));
+    SPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  }
   c->pending_sym0[0] = true;
   if (c->ngrids == 2) c->pending_sym0[1] = true;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
+// ----------------------------------------------------------------------------
+// Autotuner of the insertion launch.  For the open reconstruction it times
+// each candidate (kernel variant x threads per CTA x CTAs per SM) on one
+// sub-batch of synthetic slices (orientations on a spiral over the sphere,
+// zero spectra: the cost of a launch does not depend on the values), keeps
+// the fastest, and zeroes the grids again.  Results are cached per (device,
+// nx, grids, spectrum precision, symmetry count) for the process.
+struct TuneVal {
+  int mode, threads, bps;
+  float ms;
+};
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int, int>, TuneVal> g_tune;
+
+static int bp_autotune_impl(spi_ctx* c, int force) {
+  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_autotune: no open reconstruction (spi_bp_open)");
+  if (c->inserted || c->merged)
+    return fail(kInvalid, "spi_bp_autotune: call it right after spi_bp_open, before any image is inserted");
+  SPI_CUDA(cudaSetDevice(c->device));
+  const auto key = std::make_tuple(c->device, c->nx, c->ngrids, c->bf16, c->nsym);
+  if (!force) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      c->insert_mode = it->second.mode;
+      c->insert_threads = it->second.threads;
+      c->insert_blocks_per_sm = it->second.bps;
+      c->tuned_ms = it->second.ms;
+      return 0;
+    }
+  }
+  SPI_TRY(ensure_chunk_buffers(c));
+  const int nx = c->nx, nsym = c->nsym;
+  const int sample = std::min(c->sub, 512);
+  const size_t nsl = (size_t)sample * nsym;
+  SPI_TRY(c->hslices.ensure(nsl * sizeof(SliceDesc)));
+  SliceDesc* hs = c->hslices.as<SliceDesc>();
+  for (int a = 0; a < sample; ++a) {
+    const double th = std::acos(1.0 - 2.0 * (a + 0.5) / sample) * 180.0 / M_PI;
+    const float phi = (float)std::fmod(a * 137.50776405, 360.0), psi = (float)std::fmod(a * 222.4922359, 360.0);
+    float dm[9];
+    cang(phi, (float)th, psi, dm);
+    for (int sy = 0; sy < nsym; ++sy) {
+      float dms[9];
+      if (nsym > 1) matmul33(&c->sym_dm[9 * sy], dm, dms);
+      else memcpy(dms, dm, sizeof(dms));
+      SliceDesc& d = hs[(size_t)a * nsym + sy];
+      memcpy(d.dm, dms, 6 * sizeof(float));
+      d.img = a;
+      d.grid = (c->ngrids == 2) ? (a & 1) : 0;
+    }
+  }
+  SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs, nsl * sizeof(SliceDesc), cudaMemcpyHostToDevice, c->stream));
+  const size_t plane = (size_t)c->n * (nx + 1);
+  SPI_CUDA(cudaMemsetAsync(c->spectra.p, 0, (size_t)sample * plane * (c->bf16 ? 4 : 8), c->stream));
+  float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
+  const int modes[2] = {kb_window4_ok(c->kb) ? 3 : 2, 2};
+  const int shapes[5][2] = {{256, 2}, {256, 3}, {512, 2}, {128, 4}, {512, 1}};
+  cudaEvent_t e0, e1;
+  SPI_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(kCuda, "cudaEventCreate failed");
+  }
+  const bool timing = c->timing;
+  c->timing = false;
+  TuneVal best{c->insert_mode, c->insert_threads, c->insert_blocks_per_sm, 1e30f};
+  int st = 0;
+  for (int mi = 0; mi < 2 && !st; ++mi) {
+    if (mi == 1 && modes[0] == modes[1]) break;
+    for (auto& sh : shapes) {
+      c->insert_mode = modes[mi];
+      c->insert_threads = sh[0];
+      c->insert_blocks_per_sm = sh[1];
+      if ((st = launch_insert(c, c->slices.as<SliceDesc>(), (int)nsl, g1))) break;   // warm-up
+      cudaEventRecord(e0, c->stream);
+      for (int r = 0; r < 2 && !st; ++r) st = launch_insert(c, c->slices.as<SliceDesc>(), (int)nsl, g1);
+      cudaEventRecord(e1, c->stream);
+      if (st || (st = (cudaEventSynchronize(e1) == cudaSuccess) ? 0 : kCuda)) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms *= 0.5f;
+      if (ms < best.ms) best = TuneVal{modes[mi], sh[0], sh[1], ms};
+    }
+  }
+  c->timing = timing;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->insert_mode = best.mode;
+  c->insert_threads = best.threads;
+  c->insert_blocks_per_sm = best.bps;
+  c->tuned_ms = best.ms;
+  if (st) return st;
+  const size_t gbytes = grid_voxels(c) * sizeof(float4);
+  for (int g = 0; g < c->ngrids; ++g) SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  return 0;
+}
+
 extern "C" {
+
+int spi_bp_autotune(spi_ctx* c, int force) { return bp_autotune_impl(c, force); }
+
+int spi_bp_get_launch(const spi_ctx* c, int* kernel, int* threads, int* blocks_per_sm, float* tuned_ms) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (kernel) *kernel = c->insert_mode;
+  if (threads) *threads = c->insert_threads;
+  if (blocks_per_sm) *blocks_per_sm = c->insert_blocks_per_sm;
+  if (tuned_ms) *tuned_ms = c->tuned_ms;
+  return 0;
+}
 
 static int apply_sym0(spi_ctx* c, int g) {
   if (!c->pending_sym0[g]) return 0;

@@ -13,8 +13,10 @@
 //         same float operations.  One thread per voxel sums the projections
 //         in image order, the order of the reference's image loop, so the
 //         back-projection is bit-identical to the CPU form.
-// CG scalars (DELSQ, AKDEN, P, Q) are FP64 device scalars; vectors are FP32.
+// CG scalars (DELSQ, AKDEN, P, Q) are FP64 device scalars; the vectors and
+// projections are FP64 by default and FP32 (the reference's REAL) on request.
 // One CG iteration is a fixed kernel sequence captured once as a CUDA graph.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -157,14 +159,17 @@ __global__ void __launch_bounds__(256) bckpj_kernel(T* __restrict__ cube, const 
 
 // ---------------------------------------------------------------------------
 // A: PRJCQ_N splat, one CTA per projection, image privatised in shared memory.
-template <class T>
+// T is the type of the volume and projections, A that of the shared-memory
+// accumulator (A = float with T = double: FP32 native shared atomics, a third
+// of the shared memory, FP64 everywhere else).
+template <class T, class A>
 __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                          int nruns, const CgDM* __restrict__ dms, int n, int ldp,
                                                          T* __restrict__ projs) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* img = reinterpret_cast<T*>(smraw);
+  A* img = reinterpret_cast<A*>(smraw);
   const int k = blockIdx.x;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (T)0;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (A)0;
   __syncthreads();
   const CgDM dm = dms[k];
   for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
@@ -180,11 +185,11 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ c
       const T dx1m = rsub((T)1, dx);
       const T dy1m = rsub(cv, dy);
       if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        T* p = img + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, rmul(dx1m, dy1m));
-        atomicAdd(p + 1, rmul(dx, dy1m));
-        atomicAdd(p + n, rmul(dx1m, dy));
-        atomicAdd(p + n + 1, rmul(dx, dy));
+        A* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, (A)rmul(dx1m, dy1m));
+        atomicAdd(p + 1, (A)rmul(dx, dy1m));
+        atomicAdd(p + n, (A)rmul(dx1m, dy));
+        atomicAdd(p + n + 1, (A)rmul(dx, dy));
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
@@ -192,7 +197,108 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ c
   }
   __syncthreads();
   T* out = projs + (size_t)k * n * n;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = img[i];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = (T)img[i];
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision operators (precision mode 2).  Projections live only as
+// the reference's PROJT four-term table (bpcg.f:732-742) in FP32, one float4
+// {B1, B2, B3, B4} per pixel column I: B1 = P(I), B2 = P(I+N) - P(I),
+// B3 = P(I+1) - P(I), B4 = P(I+N+1) - P(I+1) - B2 (1-based, with the HIANG
+// weight LB applied to the four pixels first), so A^T reads one 16-byte
+// vector per (voxel, image) instead of four scattered values.  They are made
+// per chunk of images and consumed by the back-projection right away.
+__device__ __forceinline__ float4 projt_terms(const float* P, int I, int n, float w) {
+  if (I < 1 || I > n * n - n - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
+  float p00 = P[I - 1], p01 = P[I + n - 1], p10 = P[I], p11 = P[I + n];
+  if (w > 1.0f) {
+    p00 = __fmul_rn(p00, w); p01 = __fmul_rn(p01, w); p10 = __fmul_rn(p10, w); p11 = __fmul_rn(p11, w);
+  }
+  const float b2 = __fsub_rn(p01, p00);
+  return make_float4(p00, b2, __fsub_rn(p10, p00), __fsub_rn(__fsub_rn(p11, p10), b2));
+}
+
+// PROJT of input images [nimg][n*n] (weight 1)
+__global__ void projt_images_kernel(const float* __restrict__ imgs, int n, int nimg, float4* __restrict__ projt) {
+  const long long total = (long long)nimg * n * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t / ((long long)n * n));
+    const int I = (int)(t % ((long long)n * n)) + 1;
+    projt[t] = projt_terms(imgs + (size_t)k * n * n, I, n, 1.0f);
+  }
+}
+
+// PRJCQ_N of projections kbase .. kbase+gridDim.x-1 into FP32 shared memory,
+// written out as PROJT with the HIANG weights lb[k].
+template <class T>
+__global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
+                                                          int nruns, const CgDM* __restrict__ dms,
+                                                          const int* __restrict__ lb, int kbase, int n, int ldp,
+                                                          float4* __restrict__ projt) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* img = reinterpret_cast<float*>(smraw);
+  const int k = kbase + blockIdx.x;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = 0.0f;
+  __syncthreads();
+  const CgDM dm = dms[k];
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
+    const CgRun r = runs[ri];
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
+    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    for (int j = r.l1; j <= r.l2; ++j) {
+      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
+      const T cv = cube[(size_t)j - 1];
+      const T dx = (T)__fsub_rn(xb, (float)iqx);
+      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+      const T dx1m = rsub((T)1, dx);
+      const T dy1m = rsub(cv, dy);
+      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+        float* p = img + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, (float)rmul(dx1m, dy1m));
+        atomicAdd(p + 1, (float)rmul(dx, dy1m));
+        atomicAdd(p + n, (float)rmul(dx1m, dy));
+        atomicAdd(p + n + 1, (float)rmul(dx, dy));
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[3]);
+    }
+  }
+  __syncthreads();
+  const float w = lb ? (float)lb[k] : 1.0f;
+  float4* out = projt + (size_t)blockIdx.x * n * n;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = projt_terms(img, i + 1, n, w);
+}
+
+// BCKPJ_LIN from PROJT tables of images [k0, k1) (table of image k at
+// projt + (k - kbase) * n * n), accumulating in T.
+template <class T>
+__global__ void __launch_bounds__(256) bckpj_projt_kernel(T* __restrict__ cube, const CgRun* __restrict__ runs,
+                                                          const int* __restrict__ vox_run, const int* __restrict__ vox_off,
+                                                          long long nvox, const float4* __restrict__ projt,
+                                                          const CgDM* __restrict__ dms, int kbase, int k0, int k1, int n,
+                                                          int ldp) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const CgRun r = runs[vox_run[v]];
+    const int jt = vox_off[v];
+    const size_t lin = (size_t)r.l1 - 1 + jt;
+    T c = cube[lin];
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp), fj = (float)jt;
+    for (int k = k0; k < k1; ++k) {
+      const CgDM dm = dms[k];
+      const float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+      const float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+      const float xbb = __fadd_rn(xb, __fmul_rn(fj, dm.d[0]));
+      const float ybb = __fadd_rn(yb, __fmul_rn(fj, dm.d[3]));
+      const int iqx = __float2int_rz(xbb), iqy = __float2int_rz(ybb);
+      const int I = (iqy - 1) * n + iqx;  // PROJT column, 1-based
+      float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (I >= 1 && I <= n * n - n - 1) b = __ldg(projt + (size_t)(k - kbase) * n * n + (I - 1));
+      const T dy = (T)__fsub_rn(ybb, (float)iqy), dx = (T)__fsub_rn(xbb, (float)iqx);
+      c = radd(radd(radd(c, (T)b.x), rmul(dy, (T)b.y)), rmul(dx, radd((T)b.z, rmul(dy, (T)b.w))));
+    }
+    cube[lin] = c;
+  }
 }
 
 // Same splat with global atomics, for images that exceed shared memory.
@@ -431,17 +537,26 @@ static int blocks_for(const spi_ctx* c, long long work, int threads) {
 template <class T>
 static int launch_project(spi_ctx* c, const CgProblem& pb, const T* cube, const CgDM* dms, int nang, T* projs) {
   const int n = pb.n;
-  const size_t smem = (size_t)n * n * sizeof(T);
+  // FP32 shared-memory accumulation of FP64 projections in the mixed mode
+  const bool acc32 = sizeof(T) == 8 && c->cg_fp64 == 2;
+  const size_t smem = (size_t)n * n * (acc32 ? sizeof(float) : sizeof(T));
   if (nang <= 0) return 0;
   const size_t smem_cap = 200 * 1024;
   if (smem <= smem_cap) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      cudaFuncSetAttribute(prjcq_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
-      attr_set = true;
+    // the attribute is per device; set once per device (several threads may race here harmlessly)
+    static std::atomic<unsigned long long> attr_set{0};
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_set.load() & bit)) {
+      cudaFuncSetAttribute(prjcq_smem_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+      cudaFuncSetAttribute(prjcq_smem_kernel<T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+      attr_set.fetch_or(bit);
     }
-    prjcq_smem_kernel<T><<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
-                                                          n, pb.ldp, projs);
+    if (acc32)
+      prjcq_smem_kernel<T, float><<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(),
+                                                                  (int)pb.runs.size(), dms, n, pb.ldp, projs);
+    else
+      prjcq_smem_kernel<T, T><<<nang, 512, smem, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(),
+                                                              dms, n, pb.ldp, projs);
     SPI_TRY(check_kernel("prjcq_smem_kernel"));
   } else {
     SPI_CUDA(cudaMemsetAsync(projs, 0, (size_t)nang * n * n * sizeof(T), c->stream));
@@ -471,7 +586,54 @@ static int launch_backproject(spi_ctx* c, const CgProblem& pb, T* cube, const T*
   return 0;
 }
 
-static int bp_kernel_count(int nang) { return (nang + 63) / 64; }
+
+// images per PROJT chunk of the mixed mode: tables of <= ~1 GB
+static int projt_chunk(int n, int nang) {
+  const long long per = (long long)n * n * (long long)sizeof(float4);
+  return (int)std::max<long long>(64, std::min<long long>(nang, (1ll << 30) / per));
+}
+
+// the mixed mode needs the FP32 projection in shared memory
+static bool mixed_fits(int n) { return (size_t)n * n * sizeof(float) <= 200 * 1024; }
+
+// A^T from PROJT tables of images [k0, k1), 64 images per launch
+template <class T>
+static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, const float4* projt, const CgDM* dms,
+                                    int kbase, int k0, int k1) {
+  for (int a = k0; a < k1; a += 64) {
+    const int b = std::min(k1, a + 64);
+    bckpj_projt_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
+        cube, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(), pb.nvox, projt, dms, kbase, a,
+        b, pb.n, pb.ldp);
+    SPI_TRY(check_kernel("bckpj_projt_kernel"));
+    c->count();
+  }
+  return 0;
+}
+
+// A then A^T (BCKE += A^T A BCKP) chunk by chunk through PROJT tables
+template <class T>
+static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* out, const CgDM* dms, const int* lb,
+                               int nang, float4* projt) {
+  const int n = pb.n;
+  const int K = projt_chunk(n, nang);
+  const size_t smem = (size_t)n * n * sizeof(float);
+  static std::atomic<unsigned long long> attr_set{0};
+  const unsigned long long bit = 1ull << (c->device & 63);
+  if (!(attr_set.load() & bit)) {
+    cudaFuncSetAttribute(prjcq_projt_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set.fetch_or(bit);
+  }
+  for (int k0 = 0; k0 < nang; k0 += K) {
+    const int kc = std::min(K, nang - k0);
+    prjcq_projt_kernel<T><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, lb,
+                                                         k0, n, pb.ldp, projt);
+    SPI_TRY(check_kernel("prjcq_projt_kernel"));
+    c->count();
+    SPI_TRY(launch_backproject_projt<T>(c, pb, out, projt, dms, k0, k0, k0 + kc));
+  }
+  return 0;
+}
 
 static void dms_from_angles(const float* angles, int nang, std::vector<CgDM>& out) {
   out.resize((size_t)std::max(nang, 1));
@@ -546,17 +708,27 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   const size_t nnn = (size_t)n * n * n;
   const size_t vb = nnn * sizeof(T);
   const size_t pcount = (size_t)nang * n * n;
-  // buffers: [3] dms, [4] CB, [5] projections (T) + float staging, [6] BCKN|BCKP|BCKE, [7] scalars + lb
+  // mixed mode (FP64 vectors, FP32 PROJT tables made per chunk of images)
+  const bool mixed = sizeof(T) == 8 && c->cg_fp64 == 2 && mixed_fits(n);
+  const int K = projt_chunk(n, nang);
+  // buffers: [3] dms, [4] CB, [5] projections (T) + float staging (mixed: float images + PROJT chunk),
+  // [6] BCKN|BCKP|BCKE, [7] scalars + lb
   std::vector<CgDM> dms;
   dms_from_angles(angles, nang, dms);
   SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
   SPI_TRY(c->cg_buf[4].ensure(vb));
-  SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
+  if (mixed)
+    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float) + (size_t)K * n * n * sizeof(float4) + 16));
+  else
+    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
   SPI_TRY(c->cg_buf[6].ensure(3 * vb));
   SPI_TRY(c->cg_buf[7].ensure(sizeof(CgScal) + 64 + (size_t)nang * sizeof(int)));
   T* cb = c->cg_buf[4].as<T>();
   T* pj = c->cg_buf[5].as<T>();
-  float* pj32 = (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
+  float* pj32 = mixed ? c->cg_buf[5].as<float>()
+                      : (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
+  float4* projt = mixed ? reinterpret_cast<float4*>(c->cg_buf[5].as<char>() + ((pcount * sizeof(float) + 15) & ~size_t(15)))
+                        : nullptr;
   T* bckn = c->cg_buf[6].as<T>();
   T* bckp = bckn + nnn;
   T* bcke = bckp + nnn;
@@ -570,13 +742,24 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   astasq_kernel<<<nang, 256, 0, c->stream>>>(pj32, n, ri * ri, acc);
   SPI_TRY(check_kernel("astasq_kernel"));
   c->count();
-  if (sizeof(T) != sizeof(float)) {
-    widen_kernel<T><<<blocks_for(c, (long long)pcount, 256), 256, 0, c->stream>>>(pj32, pj, pcount);
-    SPI_TRY(check_kernel("widen_kernel"));
-    c->count();
-  }
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
-  SPI_TRY(launch_backproject<T>(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  if (mixed) {
+    for (int k0 = 0; k0 < nang; k0 += K) {
+      const int kc = std::min(K, nang - k0);
+      projt_images_kernel<<<blocks_for(c, (long long)kc * n * n, 256), 256, 0, c->stream>>>(pj32 + (size_t)k0 * n * n,
+                                                                                            n, kc, projt);
+      SPI_TRY(check_kernel("projt_images_kernel"));
+      c->count();
+      SPI_TRY(launch_backproject_projt<T>(c, pb, cb, projt, c->cg_buf[3].as<CgDM>(), k0, k0, k0 + kc));
+    }
+  } else {
+    if (sizeof(T) != sizeof(float)) {
+      widen_kernel<T><<<blocks_for(c, (long long)pcount, 256), 256, 0, c->stream>>>(pj32, pj, pcount);
+      SPI_TRY(check_kernel("widen_kernel"));
+      c->count();
+    }
+    SPI_TRY(launch_backproject<T>(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+  }
   double hacc[3];
   SPI_CUDA(cudaMemcpyAsync(hacc, acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -642,8 +825,12 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
-    SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
-    SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
+    if (mixed) {
+      SPI_TRY(launch_normal_projt<T>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo, projt));
+    } else {
+      SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
+      SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
+    }
     zero_outside_kernel<T><<<nnn_b, 256, 0, c->stream>>>(bckp, n, pb.ldp, r2);
     for (int axis = 0; axis < 3; ++axis)
       fixedge_axis_kernel<T><<<(n * n + 127) / 128, 128, 0, c->stream>>>(bckp, n, axis, mode);
@@ -664,9 +851,11 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     use_graph = false;
     cudaGetLastError();
   }
+  long long per_iter_launches = 0;
   if (use_graph) {
     const long long before = c->launches;
     const int st = iteration();
+    per_iter_launches = c->launches - before;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (st != 0) {
       if (graph) cudaGraphDestroy(graph);
@@ -680,7 +869,6 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     }
     c->launches = before;  // counted per replay below
   }
-  const long long per_iter_launches = 14 + bp_kernel_count(lo);
   int done = 0;
   for (int iter = 1; iter <= maxit; ++iter) {
     if (use_graph) {
@@ -722,9 +910,10 @@ using namespace spi;
 
 extern "C" {
 
-int spi_ctx_set_cg_precision(spi_ctx* c, int fp64) {
+int spi_ctx_set_cg_precision(spi_ctx* c, int mode) {
   if (!c) return fail(kInvalid, "NULL context");
-  c->cg_fp64 = fp64 ? 1 : 0;
+  if (mode < 0 || mode > 2) return fail(kInvalid, "spi_ctx_set_cg_precision: mode %d must be 0, 1 or 2", mode);
+  c->cg_fp64 = mode;
   return 0;
 }
 

@@ -15,18 +15,22 @@ struct spi_ctx {
   std::vector<float> sym_dm;          // 9 * nsym (column-major 3x3 each)
   bool pending_sym0[2] = {false, false};
   bool merged = false;
+  bool inserted = false;              // images went into the open grids
+  float tuned_ms = 0.0f;              // autotuner: time of the chosen launch on its sample
   int bf16 = 0;
-  int insert_mode = 2;                // 0 = tile-privatised, 1 = direct per-tap atomics, 2 = x-tap lanes
+  int insert_mode = 3;                // 0 = tile-privatised, 1 = direct per-tap atomics, 2 = five x-tap lanes,
+                                      // 3 = four lanes over the nonzero tap window
   int slice_order = 1;                // 1 = order slices of a chunk by plane normal
   int insert_seg_map = 0;             // 1 = warps take 32-pixel row segments, 0 = whole rows
   int insert_threads = 256;           // threads per insert block
   int insert_blocks_per_sm = 0;       // 0 = as many as fit
-  int pipeline = 1;                   // 1 = stage/FFT on stream2 under the insertion
+  int pipeline = 1;                   // 1 = host-image uploads on stream2 under the compute
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
   int cg_fp64 = 1;                    // BP CG vectors/projections in FP64 (1) or FP32 (0)
   int chunk = 0;                      // images per persistent insert launch
-  int sub = 0;                        // images per batched 2D FFT
+  int sub = 0;                        // images per batched 2D FFT (and per insert launch)
+  int sort_group = 0;                 // images per slice-ordering group (divides into sub)
   spi::KBTab kb;
   spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
   float4* gptr[2] = {nullptr, nullptr};      // grids in use (owned or attached)
@@ -41,6 +45,7 @@ struct spi_ctx {
   spi::DevBuf spectra;                // float2 or bf16x2 [chunk][n][nx+1]
   spi::DevBuf spec_tmp;               // float2 [sub][n][nx+1] (BF16 mode FFT output)
   spi::DevBuf slices;                 // SliceDesc [chunk * nsym]
+  spi::DevBuf workctr;                // u64 row counter of the running insert launch
   spi::DevBuf cplx;                   // float2 [n][n][nx+1] (inverse FFT input)
   spi::DevBuf real3;                  // float [n][n][n]
   spi::DevBuf wkb;                    // float[(nx/2)^2 + 1]

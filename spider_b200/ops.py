@@ -105,6 +105,20 @@ class Context:
         self._nx = nx
         self._ngrids = ngrids
 
+    KERNELS = {0: "insert_tile_kernel", 1: "insert_kernel", 2: "insert_xlane_kernel", 3: "insert_x4_kernel"}
+
+    def bp_autotune(self, force: bool = False) -> dict:
+        """Pick the insertion kernel and launch shape for the open
+        reconstruction by timing them (call right after bp_open)."""
+        check(self._L.spi_bp_autotune(self._h, 1 if force else 0))
+        return self.bp_launch()
+
+    def bp_launch(self) -> dict:
+        k, t, b, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        check(self._L.spi_bp_get_launch(self._h, ctypes.byref(k), ctypes.byref(t), ctypes.byref(b), ctypes.byref(ms)))
+        return {"kernel": self.KERNELS.get(k.value, str(k.value)), "threads": t.value, "blocks_per_sm": b.value,
+                "tuned_ms": ms.value}
+
     def bp_insert(self, imgs, angles, half=None, inplane=None):
         """Insert images; with ``inplane`` [n, 3] = (angle, sx, sy) every image is
         first rotated and shifted by RTSQ (RB 3F / RB 32F)."""
@@ -197,6 +211,41 @@ def bp32f(imgs, angles, half, sym=None, *, ctx: Context | None = None, bf16: boo
         return o["all"], o["1"], o["2"]
     finally:
         ctx.bp_close()
+
+
+def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, concurrent: bool = True,
+                     device_out: bool = False):
+    """``BP 32F`` of several classes of one image stream: ``classes`` is a list
+    of (images [n_k, nx_k, nx_k], angles [n_k, 3], half mask [n_k]) with any
+    box sizes.  Each class has its own context (grids, FFT plans, streams);
+    with ``concurrent`` the classes are inserted from one host thread each,
+    so that their launches share the GPU.  Returns a list of (vol, vol1, vol2)."""
+    import concurrent.futures as cf
+    ctxs = [Context(device) for _ in classes]
+    try:
+        for c, (imgs, _, _) in zip(ctxs, classes):
+            c.bp_open(_nx_of(imgs), 2, sym, bf16=bf16)
+
+        def insert(k):
+            imgs, ang, half = classes[k]
+            ctxs[k].bp_insert(imgs, ang, half)
+
+        if concurrent and len(classes) > 1:
+            with cf.ThreadPoolExecutor(max_workers=len(classes)) as ex:
+                for f in [ex.submit(insert, k) for k in range(len(classes))]:
+                    f.result()
+        else:
+            for k in range(len(classes)):
+                insert(k)
+        out = []
+        for c in ctxs:
+            o = c.bp_finish(("all", "1", "2"), device=device_out)
+            out.append((o["all"], o["1"], o["2"]))
+            c.bp_close()
+        return out
+    finally:
+        for c in ctxs:
+            c.close()
 
 
 def rb3f(imgs, angles, inplane, sym=None, *, ctx: Context | None = None):
@@ -297,14 +346,16 @@ def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
 
 
 def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-         ctx: Context | None = None, fp64: bool = True):
+         ctx: Context | None = None, fp64=True):
     """``BP CG`` (linear interpolation).  Prompts in reference order: radius
     (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
-    ``fp64`` keeps the CG vectors and projections in FP64 (default) instead
-    of the reference's REAL.
+    ``fp64``: True keeps the CG vectors and projections in FP64 (default),
+    False uses the reference's REAL, "mixed" keeps FP64 vectors and
+    accumulates each projection in FP32 shared memory.
     Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
     ctx = ctx or default_context()
-    check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, 1 if fp64 else 0))
+    prec = 2 if fp64 == "mixed" else (1 if fp64 else 0)
+    check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))
     projs = _host_f32(projs)
     n = _nx_of(projs)
     if ri is None:

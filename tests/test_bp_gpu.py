@@ -167,7 +167,7 @@ def test_insert_kernels_agree(ctx, orc):
     # include orientations that put the x = 0 flip line inside many tiles
     ang[:40, 1] = 90.0
     out, grids = {}, {}
-    for mode in ("direct", "tile", "xlane"):
+    for mode in ("direct", "tile", "xlane", "x4"):
         os.environ["SPI_INSERT"] = mode
         try:
             out[mode] = ops.bp3f(pr, ang, ctx=ctx)
@@ -202,3 +202,50 @@ def test_rb3f_rb32f_match_oracle(ctx, orc):
     # zero in-plane parameters reproduce BP 3F exactly up to summation order
     z = ops.rb3f(pr, ang, np.zeros((nimg, 3), np.float32), ctx=ctx)
     assert synth.rel_l2(z, ops.bp3f(pr, ang, ctx=ctx)) <= 2e-6
+
+
+@pytest.mark.parametrize("concurrent", [True, False])
+def test_bp32f_multiclass(orc, concurrent):
+    """Several classes of different box sizes (one odd) reconstructed from one
+    image stream, concurrently from one host thread per class or in turn."""
+    classes, refs = [], []
+    for k, (nx, nimg) in enumerate(((24, 120), (32, 200), (41, 150))):
+        _, pr, ang = _case(nx, nimg, 90 + k, noise=0.5)
+        half = synth.half_mask(nimg, np.random.default_rng(95 + k))
+        classes.append((pr, ang, half))
+        refs.append(orc.bp32f(pr, ang, half, prec=0, nthreads=1))
+    out = ops.bp32f_multiclass(classes, concurrent=concurrent)
+    for got, ref in zip(out, refs):
+        for a, b in zip(got, ref):
+            assert a.shape == b.shape
+            assert synth.rel_l2(a, b) <= TOL
+
+
+def test_bp_autotune(ctx, orc):
+    """The autotuner picks a launch, leaves the grids empty, and the
+    reconstruction after it still matches the oracle; it refuses to run once
+    images are in the grids; a second open of the same shape reuses the
+    cached choice."""
+    nx, nimg = 48, 200
+    _, pr, ang = _case(nx, nimg, 77)
+    half = synth.half_mask(nimg, np.random.default_rng(78))
+    ctx.bp_open(nx, 2)
+    try:
+        cfg = ctx.bp_autotune()
+        assert cfg["kernel"] in ("insert_x4_kernel", "insert_xlane_kernel")
+        assert cfg["threads"] in (128, 256, 512) and cfg["blocks_per_sm"] >= 1 and cfg["tuned_ms"] > 0
+        ctx.bp_insert(pr, ang, half)
+        with pytest.raises(ops.SpiderError) as e:
+            ctx.bp_autotune()
+        assert e.value.code == 101
+        o = ctx.bp_finish(("all", "1", "2"))
+    finally:
+        ctx.bp_close()
+    ref = orc.bp32f(pr, ang, half, prec=0, nthreads=1)
+    for a, b in zip((o["all"], o["1"], o["2"]), ref):
+        assert synth.rel_l2(a, b) <= TOL
+    ctx.bp_open(nx, 2)
+    try:
+        assert ctx.bp_autotune() == cfg        # cached
+    finally:
+        ctx.bp_close()

@@ -110,3 +110,18 @@ def test_bpcg_radius_too_large(ctx):
     with pytest.raises(ops.SpiderError) as ei:
         ops.bpcg(pr, ang, 7.0, mode=1, ctx=ctx)
     assert ei.value.code == 102
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_bpcg_mixed_precision_matches_fp64_oracle(ctx, orc, n):
+    """FP64 vectors with each projection accumulated in FP32 shared memory
+    stays within the 1e-4 bar of the FP64 oracle."""
+    nang = 160
+    _, pr, ang = _data(n, nang, 40 + n, snr=1.0)
+    ri = float(n // 2 - 3)
+    vol, log = ops.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=10, mode=1, lam=0.5, ctx=ctx, fp64="mixed")
+    ref64, rlog64, _, _ = orc.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=10, mode=1, lam=0.5, prec=1)
+    e64 = synth.rel_l2(vol, ref64)
+    print(f"BP CG mixed n={n}: rel-err vs FP64 oracle {e64:.3e}")
+    assert len(log) == len(rlog64)
+    assert e64 <= 1e-4

@@ -70,3 +70,17 @@ def test_errors_without_device():
     assert L.spi_bp_grid_bytes(256, ctypes.byref(gb)) == 0
     assert gb.value == 257 * 512 * 512 * 16
     assert L.spi_bp_grid_bytes(6, ctypes.byref(gb)) == 101
+
+
+@pytest.mark.parametrize("n2", [16, 128, 512])
+def test_kb_table_window_of_four(n2):
+    """The generalised Kaiser-Bessel table is zero for every distance >= 2
+    (in fact from ~1.8 on), so of the five ONELINE taps along an axis at most
+    four consecutive ones are nonzero; the four-lane insertion kernel relies
+    on it (and the library falls back to five lanes otherwise)."""
+    from spider_b200 import roofline
+    tab, fltb = roofline.kb_table(n2)
+    tab = np.asarray(tab)
+    assert np.all(tab[int(np.floor(2.0 * fltb)) - 1:] == 0.0)
+    first_zero = int(np.argmax(tab == 0.0))
+    assert 1.7 < first_zero / fltb < 1.9
