@@ -444,19 +444,21 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         host_chunks = [c.cpu().pin_memory() for c in chunks]
-        L.spi_ctx_set_timing(ctx.handle, 0)   # per-phase events are not part of the e2e path
-        ctx.bp_close()
-        if world > 1:
+        # per-phase timing events on the library stream were measured to
+        # serialise the uploads with the compute; the e2e path runs without them
+        L.spi_ctx_set_timing(ctx.handle, 0)
+        if world > 1:   # caller-owned grids are attached to a closed context
+            ctx.bp_close()
             ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                             ctypes.c_void_p(grids[1].data_ptr())))
         hvol = [torch.empty((nx, nx, nx), dtype=torch.float32).pin_memory() for _ in range(3)]
+        # reopening at the same size zeroes the grids and keeps every buffer
         ctx.bp_open(nx, 2, bf16=args.bf16)
         ctx.bp_autotune()                   # cached choice
-        for i in range(min(args.warmup, 1)):  # first host-image call (events, buffers)
+        for i in range(min(args.warmup, 1)):  # first host-image call (copy-stream events)
             ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
                                       angles[i].ctypes.data_as(ctypes.c_void_p),
                                       halves[i].ctypes.data_as(ctypes.c_void_p), 0))
-        ctx.bp_close()
         ctx.bp_open(nx, 2, bf16=args.bf16)
         ctx.bp_autotune()
         barrier()

@@ -70,7 +70,10 @@ void* spi_ctx_stream(const spi_ctx* ctx);
  * every phase of the back-projection is bracketed by events and its device
  * milliseconds accumulated; spi_ctx_timing copies SPI_NPHASE totals and
  * resets them.  Phases: 0 stage (PADD2), 1 2D FFT, 2 insert (ONELINE),
- * 3 SYMPLANE0, 4 NRMW2, 5 3D FFT, 6 WINDKB2A, 7 host-to-device copies. */
+ * 3 SYMPLANE0, 4 NRMW2, 5 3D FFT, 6 WINDKB2A, 7 host-to-device copies
+ * (only when they are not overlapped).  The events cost the overlap of
+ * host-image uploads with the compute (measured: uploads then run serially),
+ * so leave timing off outside diagnostics. */
 #define SPI_NPHASE 8
 int spi_ctx_set_timing(spi_ctx* ctx, int on);
 int spi_ctx_timing(spi_ctx* ctx, double* ms_out, long long* count_out);

@@ -158,6 +158,60 @@ __global__ void __launch_bounds__(256) bckpj_kernel(T* __restrict__ cube, const 
 }
 
 // ---------------------------------------------------------------------------
+// PRJCQ_N splat of one voxel run into an image in shared memory.  Positions
+// follow the reference's sequential walk XB = XB + DM(1), YB = YB + DM(4)
+// (prjcq.f:64-80), so every sample lands where the reference puts it.  Along
+// a run the 2 x 2 target cell moves by at most one pixel per voxel (|DM(1)|,
+// |DM(4)| <= 1), so the four pixel sums of the current cell are kept in
+// registers; pixels the next cell shares move with it and only the others
+// are added to shared memory.  Every weight goes to the same pixel as in the
+// reference; only the grouping of the sums differs.
+template <class T, class A>
+__device__ __forceinline__ void splat_run(A* img, const T* __restrict__ cube, const CgRun& r, const CgDM& dm, int n,
+                                          int ldp) {
+  const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
+  float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+  float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+  int cx = -4, cy = -4;                 // cached cell (none)
+  A a00 = 0, a10 = 0, a01 = 0, a11 = 0; // sums at (cx,cy), (cx+1,cy), (cx,cy+1), (cx+1,cy+1)
+  auto flush_to = [&](int qx, int qy) {
+    A n00 = 0, n10 = 0, n01 = 0, n11 = 0;
+    auto move = [&](A v, int ox, int oy) {
+      const int ex = ox - qx, ey = oy - qy;
+      if (ex == 0 && ey == 0) n00 += v;
+      else if (ex == 1 && ey == 0) n10 += v;
+      else if (ex == 0 && ey == 1) n01 += v;
+      else if (ex == 1 && ey == 1) n11 += v;
+      else if (v != (A)0) atomicAdd(img + (oy - 1) * n + (ox - 1), v);
+    };
+    move(a00, cx, cy);
+    move(a10, cx + 1, cy);
+    move(a01, cx, cy + 1);
+    move(a11, cx + 1, cy + 1);
+    a00 = n00; a10 = n10; a01 = n01; a11 = n11;
+    cx = qx; cy = qy;
+  };
+  for (int j = r.l1; j <= r.l2; ++j) {
+    const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
+    if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+      const T cv = cube[(size_t)j - 1];
+      const T dx = (T)__fsub_rn(xb, (float)iqx);
+      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+      const T dx1m = rsub((T)1, dx);
+      const T dy1m = rsub(cv, dy);
+      if (iqx != cx || iqy != cy) flush_to(iqx, iqy);
+      a00 += (A)rmul(dx1m, dy1m);
+      a10 += (A)rmul(dx, dy1m);
+      a01 += (A)rmul(dx1m, dy);
+      a11 += (A)rmul(dx, dy);
+    }
+    xb = __fadd_rn(xb, dm.d[0]);
+    yb = __fadd_rn(yb, dm.d[3]);
+  }
+  flush_to(-4, -4);
+}
+
+// ---------------------------------------------------------------------------
 // A: PRJCQ_N splat, one CTA per projection, image privatised in shared memory.
 // T is the type of the volume and projections, A that of the shared-memory
 // accumulator (A = float with T = double: FP32 native shared atomics, a third
@@ -172,29 +226,7 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ c
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (A)0;
   __syncthreads();
   const CgDM dm = dms[k];
-  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
-    const CgRun r = runs[ri];
-    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
-    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
-    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
-    for (int j = r.l1; j <= r.l2; ++j) {
-      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
-      const T cv = cube[(size_t)j - 1];
-      const T dx = (T)__fsub_rn(xb, (float)iqx);
-      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
-      const T dx1m = rsub((T)1, dx);
-      const T dy1m = rsub(cv, dy);
-      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        A* p = img + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, (A)rmul(dx1m, dy1m));
-        atomicAdd(p + 1, (A)rmul(dx, dy1m));
-        atomicAdd(p + n, (A)rmul(dx1m, dy));
-        atomicAdd(p + n + 1, (A)rmul(dx, dy));
-      }
-      xb = __fadd_rn(xb, dm.d[0]);
-      yb = __fadd_rn(yb, dm.d[3]);
-    }
-  }
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) splat_run<T, A>(img, cube, runs[ri], dm, n, ldp);
   __syncthreads();
   T* out = projs + (size_t)k * n * n;
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = (T)img[i];
@@ -241,29 +273,7 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = 0.0f;
   __syncthreads();
   const CgDM dm = dms[k];
-  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
-    const CgRun r = runs[ri];
-    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
-    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
-    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
-    for (int j = r.l1; j <= r.l2; ++j) {
-      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
-      const T cv = cube[(size_t)j - 1];
-      const T dx = (T)__fsub_rn(xb, (float)iqx);
-      const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
-      const T dx1m = rsub((T)1, dx);
-      const T dy1m = rsub(cv, dy);
-      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        float* p = img + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, (float)rmul(dx1m, dy1m));
-        atomicAdd(p + 1, (float)rmul(dx, dy1m));
-        atomicAdd(p + n, (float)rmul(dx1m, dy));
-        atomicAdd(p + n + 1, (float)rmul(dx, dy));
-      }
-      xb = __fadd_rn(xb, dm.d[0]);
-      yb = __fadd_rn(yb, dm.d[3]);
-    }
-  }
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) splat_run<T, float>(img, cube, runs[ri], dm, n, ldp);
   __syncthreads();
   const float w = lb ? (float)lb[k] : 1.0f;
   float4* out = projt + (size_t)blockIdx.x * n * n;
