@@ -260,20 +260,68 @@ __global__ void projt_images_kernel(const float* __restrict__ imgs, int n, int n
   }
 }
 
-// PRJCQ_N of projections kbase .. kbase+gridDim.x-1 into FP32 shared memory,
-// written out as PROJT with the HIANG weights lb[k].
+// max |x| over the sphere voxels, as the bit pattern of a non-negative
+// double (which orders like the unsigned integer), for the fixed-point scale
+template <class T>
+__global__ void absmax_kernel(const T* __restrict__ x, const CgRun* __restrict__ runs, const int* __restrict__ vr,
+                              const int* __restrict__ vo, long long nvox, unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs((double)x[(size_t)runs[vr[v]].l1 - 1 + vo[v]]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// PRJCQ_N of projections kbase .. kbase+gridDim.x-1, accumulated in 32-bit
+// fixed point in shared memory (native integer atomics, exact and order
+// independent), written out as PROJT with the HIANG weights lb[k].  Scale:
+// every voxel whose projection can reach a pixel lies in a 2 x 2 x (2 RI)
+// prism, whose lattice points number at most the volume of the prism grown
+// by the half-diagonal of a unit cube, pi (sqrt 2 + sqrt 3 / 2)^2 (2 RI +
+// sqrt 3) = `mcap`; each adds at most max|x| (bilinear weights <= 1), so
+// with q = round(w * 0.95 * 2^31 / (mcap * max|x|)) no pixel sum can leave
+// the int32 range.  One step of the grid is then ~1e-6 max|x|.
 template <class T>
 __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                           int nruns, const CgDM* __restrict__ dms,
                                                           const int* __restrict__ lb, int kbase, int n, int ldp,
-                                                          float4* __restrict__ projt) {
+                                                          const unsigned long long* __restrict__ maxabs_bits,
+                                                          float mcap, float4* __restrict__ projt) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  float* img = reinterpret_cast<float*>(smraw);
+  int* acc = reinterpret_cast<int*>(smraw);
+  float* img = reinterpret_cast<float*>(smraw);   // reuses the accumulator once it is converted
   const int k = kbase + blockIdx.x;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = 0.0f;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) acc[i] = 0;
+  const double maxabs = __longlong_as_double((long long)*maxabs_bits);
+  const double scale = maxabs > 0.0 ? 0.95 * 2147483648.0 / ((double)mcap * maxabs) : 0.0;
   __syncthreads();
   const CgDM dm = dms[k];
-  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) splat_run<T, float>(img, cube, runs[ri], dm, n, ldp);
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
+    const CgRun r = runs[ri];
+    const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
+    float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
+    float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    for (int j = r.l1; j <= r.l2; ++j) {
+      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
+      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+        const T cv = cube[(size_t)j - 1];
+        const T dx = (T)__fsub_rn(xb, (float)iqx);
+        const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+        const T dx1m = rsub((T)1, dx);
+        const T dy1m = rsub(cv, dy);
+        int* p = acc + (iqy - 1) * n + (iqx - 1);
+        atomicAdd(p, __double2int_rn((double)rmul(dx1m, dy1m) * scale));
+        atomicAdd(p + 1, __double2int_rn((double)rmul(dx, dy1m) * scale));
+        atomicAdd(p + n, __double2int_rn((double)rmul(dx1m, dy) * scale));
+        atomicAdd(p + n + 1, __double2int_rn((double)rmul(dx, dy) * scale));
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[3]);
+    }
+  }
+  __syncthreads();
+  const double inv = scale > 0.0 ? 1.0 / scale : 0.0;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (float)((double)acc[i] * inv);
   __syncthreads();
   const float w = lb ? (float)lb[k] : 1.0f;
   float4* out = projt + (size_t)blockIdx.x * n * n;
@@ -624,10 +672,18 @@ static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, co
 // A then A^T (BCKE += A^T A BCKP) chunk by chunk through PROJT tables
 template <class T>
 static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* out, const CgDM* dms, const int* lb,
-                               int nang, float4* projt) {
+                               int nang, float4* projt, unsigned long long* maxabs) {
   const int n = pb.n;
   const int K = projt_chunk(n, nang);
   const size_t smem = (size_t)n * n * sizeof(float);
+  // fixed-point scale of the projector: max |x| over the sphere
+  SPI_CUDA(cudaMemsetAsync(maxabs, 0, sizeof(unsigned long long), c->stream));
+  absmax_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(),
+                                                                      c->cg_buf[2].as<int>(), pb.nvox, maxabs);
+  SPI_TRY(check_kernel("absmax_kernel"));
+  c->count();
+  const float mcap = (float)(M_PI * std::pow(std::sqrt(2.0) + std::sqrt(3.0) / 2.0, 2.0) *
+                             (2.0 * pb.ri + std::sqrt(3.0)));
   static std::atomic<unsigned long long> attr_set{0};
   const unsigned long long bit = 1ull << (c->device & 63);
   if (!(attr_set.load() & bit)) {
@@ -637,7 +693,7 @@ static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* o
   for (int k0 = 0; k0 < nang; k0 += K) {
     const int kc = std::min(K, nang - k0);
     prjcq_projt_kernel<T><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, lb,
-                                                         k0, n, pb.ldp, projt);
+                                                         k0, n, pb.ldp, maxabs, mcap, projt);
     SPI_TRY(check_kernel("prjcq_projt_kernel"));
     c->count();
     SPI_TRY(launch_backproject_projt<T>(c, pb, out, projt, dms, k0, k0, k0 + kc));
@@ -836,7 +892,8 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
     if (mixed) {
-      SPI_TRY(launch_normal_projt<T>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo, projt));
+      SPI_TRY(launch_normal_projt<T>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo, projt,
+                                     reinterpret_cast<unsigned long long*>(acc + 7)));
     } else {
       SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
       SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));

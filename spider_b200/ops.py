@@ -214,7 +214,7 @@ def bp32f(imgs, angles, half, sym=None, *, ctx: Context | None = None, bf16: boo
 
 
 def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, concurrent: bool = True,
-                     device_out: bool = False):
+                     device_out: bool = False, autotune: bool = False):
     """``BP 32F`` of several classes of one image stream: ``classes`` is a list
     of (images [n_k, nx_k, nx_k], angles [n_k, 3], half mask [n_k]) with any
     box sizes.  Each class has its own context (grids, FFT plans, streams);
@@ -225,6 +225,8 @@ def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, 
     try:
         for c, (imgs, _, _) in zip(ctxs, classes):
             c.bp_open(_nx_of(imgs), 2, sym, bf16=bf16)
+            if autotune:            # launch shape per box size (cached per process)
+                c.bp_autotune()
 
         def insert(k):
             imgs, ang, half = classes[k]
