@@ -213,12 +213,17 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
              float* vol_out, float* log_out, int* niter_out);
 
 /* Storage and accumulation type of the BP CG vectors and projections:
- * mode = 1 (default) keeps CB, BCKP, BCKE, BCKN and the projections in
- * FP64 (the reference keeps them in REAL; its FP32 CG drifts from the exact
- * iteration by more than 1e-2 at small LAMBDA); mode = 0 uses FP32 as the
- * reference does; mode = 2 is mode 1 with each projection (PRJCQ_N)
- * accumulated in FP32 shared memory before it is stored in FP64.  Scalars
- * (DELSQ, AKDEN, P, Q) and dot products are FP64 in all modes. */
+ * mode = 1 keeps CB, BCKP, BCKE, BCKN and the projections in FP64 (the
+ * reference keeps them in REAL; its FP32 CG drifts from the exact iteration
+ * by more than 1e-2 at small LAMBDA); mode = 0 uses FP32 as the reference
+ * does.  Modes 2 and 3 keep the vectors in FP64, accumulate each projection
+ * (PRJCQ_N) in fixed point in shared memory with integer atomics and hand it
+ * to BCKPJ_LIN as the PROJT four-term table, made per chunk of images:
+ * mode = 2 (default) with a 47-bit grid (~1e-11 of max|x|) and FP64 tables,
+ * n*n*8 bytes of shared memory (n <= 160); mode = 3 with a 31-bit grid and
+ * FP32 tables, n*n*4 bytes (n <= 226), faster and ~1e-7 per projection.
+ * Above those sizes they use mode 1.  Scalars (DELSQ, AKDEN, P, Q) and dot
+ * products are FP64 in all modes. */
 int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
 
 /* One application of the BP CG operators on device arrays, for the

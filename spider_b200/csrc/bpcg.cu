@@ -233,30 +233,60 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ c
 }
 
 // ---------------------------------------------------------------------------
-// Mixed-precision operators (precision mode 2).  Projections live only as
-// the reference's PROJT four-term table (bpcg.f:732-742) in FP32, one float4
+// Mixed-precision operators (precision modes 2 and 3).  Projections live only
+// as the reference's PROJT four-term table (bpcg.f:732-742), one entry
 // {B1, B2, B3, B4} per pixel column I: B1 = P(I), B2 = P(I+N) - P(I),
 // B3 = P(I+1) - P(I), B4 = P(I+N+1) - P(I+1) - B2 (1-based, with the HIANG
-// weight LB applied to the four pixels first), so A^T reads one 16-byte
-// vector per (voxel, image) instead of four scattered values.  They are made
-// per chunk of images and consumed by the back-projection right away.
-__device__ __forceinline__ float4 projt_terms(const float* P, int I, int n, float w) {
-  if (I < 1 || I > n * n - n - 1) return make_float4(0.f, 0.f, 0.f, 0.f);
-  float p00 = P[I - 1], p01 = P[I + n - 1], p10 = P[I], p11 = P[I + n];
-  if (w > 1.0f) {
-    p00 = __fmul_rn(p00, w); p01 = __fmul_rn(p01, w); p10 = __fmul_rn(p10, w); p11 = __fmul_rn(p11, w);
+// weight LB applied to the four pixels first), so A^T reads one vector per
+// (voxel, image) instead of four scattered values.  The terms are formed in
+// FP64 and stored in FP64 (mode 2, WIDE) or rounded once to FP32 (mode 3).
+// Tables are made per chunk of images and consumed right away.
+template <bool WIDE> struct ProjtEntry;
+template <> struct ProjtEntry<false> { float4 v; };
+template <> struct ProjtEntry<true> { double2 a, b; };
+
+template <bool WIDE>
+__device__ __forceinline__ void projt_store(ProjtEntry<WIDE>* out, double b1, double b2, double b3, double b4);
+template <>
+__device__ __forceinline__ void projt_store<false>(ProjtEntry<false>* out, double b1, double b2, double b3, double b4) {
+  out->v = make_float4((float)b1, (float)b2, (float)b3, (float)b4);
+}
+template <>
+__device__ __forceinline__ void projt_store<true>(ProjtEntry<true>* out, double b1, double b2, double b3, double b4) {
+  out->a = make_double2(b1, b2);
+  out->b = make_double2(b3, b4);
+}
+__device__ __forceinline__ void projt_load(const ProjtEntry<false>* p, double& b1, double& b2, double& b3, double& b4) {
+  const float4 v = __ldg(&p->v);
+  b1 = v.x; b2 = v.y; b3 = v.z; b4 = v.w;
+}
+__device__ __forceinline__ void projt_load(const ProjtEntry<true>* p, double& b1, double& b2, double& b3, double& b4) {
+  const double2 a = __ldg(&p->a), b = __ldg(&p->b);
+  b1 = a.x; b2 = a.y; b3 = b.x; b4 = b.y;
+}
+
+// the four terms at column I from pixel values val(i) (0-based) and weight w
+template <bool WIDE, class V>
+__device__ __forceinline__ void projt_make(ProjtEntry<WIDE>* out, V val, int I, int n, double w) {
+  if (I < 1 || I > n * n - n - 1) {
+    projt_store<WIDE>(out, 0.0, 0.0, 0.0, 0.0);
+    return;
   }
-  const float b2 = __fsub_rn(p01, p00);
-  return make_float4(p00, b2, __fsub_rn(p10, p00), __fsub_rn(__fsub_rn(p11, p10), b2));
+  double p00 = val(I - 1), p01 = val(I + n - 1), p10 = val(I), p11 = val(I + n);
+  if (w > 1.0) { p00 *= w; p01 *= w; p10 *= w; p11 *= w; }
+  const double b2 = p01 - p00;
+  projt_store<WIDE>(out, p00, b2, p10 - p00, (p11 - p10) - b2);
 }
 
 // PROJT of input images [nimg][n*n] (weight 1)
-__global__ void projt_images_kernel(const float* __restrict__ imgs, int n, int nimg, float4* __restrict__ projt) {
+template <bool WIDE>
+__global__ void projt_images_kernel(const float* __restrict__ imgs, int n, int nimg, ProjtEntry<WIDE>* __restrict__ projt) {
   const long long total = (long long)nimg * n * n;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(t / ((long long)n * n));
     const int I = (int)(t % ((long long)n * n)) + 1;
-    projt[t] = projt_terms(imgs + (size_t)k * n * n, I, n, 1.0f);
+    const float* P = imgs + (size_t)k * n * n;
+    projt_make<WIDE>(projt + t, [P](int i) { return (double)P[i]; }, I, n, 1.0);
   }
 }
 
@@ -272,30 +302,46 @@ __global__ void absmax_kernel(const T* __restrict__ x, const CgRun* __restrict__
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
-// PRJCQ_N of projections kbase .. kbase+gridDim.x-1, accumulated in 32-bit
-// fixed point in shared memory (native integer atomics, exact and order
-// independent), written out as PROJT with the HIANG weights lb[k].  Scale:
-// every voxel whose projection can reach a pixel lies in a 2 x 2 x (2 RI)
-// prism, whose lattice points number at most the volume of the prism grown
-// by the half-diagonal of a unit cube, pi (sqrt 2 + sqrt 3 / 2)^2 (2 RI +
-// sqrt 3) = `mcap`; each adds at most max|x| (bilinear weights <= 1), so
-// with q = round(w * 0.95 * 2^31 / (mcap * max|x|)) no pixel sum can leave
-// the int32 range.  One step of the grid is then ~1e-6 max|x|.
-template <class T>
+// PRJCQ_N of projections kbase .. kbase+gridDim.x-1, accumulated in fixed
+// point in shared memory with native 32-bit integer atomics (exact and order
+// independent), written out as PROJT with the HIANG weights lb[k].
+//
+// Scale: every voxel whose projection can reach a pixel lies in a 2 x 2 x
+// (2 RI) prism, whose lattice points number at most the volume of the prism
+// grown by the half-diagonal of a unit cube, pi (sqrt 2 + sqrt 3 / 2)^2
+// (2 RI + sqrt 3) = `mcap`; each adds at most max|x| (bilinear weights
+// <= 1).  Mode 3 rounds each contribution to q = w * 0.95 * 2^31 / (mcap *
+// max|x|) in one int32 word per pixel (a step of ~1e-6 max|x|).  Mode 2
+// (WIDE) rounds to a 2^16 finer grid, q = w * 0.95 * 2^47 / (mcap * max|x|)
+// in 64 bits, and adds q >> 16 and q & 0xffff into two int32 words per
+// pixel: the high sum stays within 0.95 * 2^31 + mcap, the low one within
+// mcap * 65535, and the pixel is hi * 65536 + lo exactly (a step of ~1e-11
+// max|x|).
+template <class T, bool WIDE>
 __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                           int nruns, const CgDM* __restrict__ dms,
                                                           const int* __restrict__ lb, int kbase, int n, int ldp,
                                                           const unsigned long long* __restrict__ maxabs_bits,
-                                                          float mcap, float4* __restrict__ projt) {
+                                                          float mcap, ProjtEntry<WIDE>* __restrict__ projt) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  int* acc = reinterpret_cast<int*>(smraw);
-  float* img = reinterpret_cast<float*>(smraw);   // reuses the accumulator once it is converted
+  int* hi = reinterpret_cast<int*>(smraw);
+  int* lo = hi + n * n;   // WIDE only
   const int k = kbase + blockIdx.x;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) acc[i] = 0;
+  for (int i = threadIdx.x; i < n * n * (WIDE ? 2 : 1); i += blockDim.x) hi[i] = 0;
   const double maxabs = __longlong_as_double((long long)*maxabs_bits);
-  const double scale = maxabs > 0.0 ? 0.95 * 2147483648.0 / ((double)mcap * maxabs) : 0.0;
+  const double full = WIDE ? 0.95 * 140737488355328.0 : 0.95 * 2147483648.0;   // 2^47 or 2^31
+  const double scale = maxabs > 0.0 ? full / ((double)mcap * maxabs) : 0.0;
   __syncthreads();
   const CgDM dm = dms[k];
+  auto add = [&](int* p, double w) {
+    if (WIDE) {
+      const long long q = __double2ll_rn(w * scale);
+      atomicAdd(p, (int)(q >> 16));
+      atomicAdd(p + n * n, (int)(q & 0xffff));
+    } else {
+      atomicAdd(p, __double2int_rn(w * scale));
+    }
+  };
   for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
     const CgRun r = runs[ri];
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
@@ -309,11 +355,11 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
         const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
         const T dx1m = rsub((T)1, dx);
         const T dy1m = rsub(cv, dy);
-        int* p = acc + (iqy - 1) * n + (iqx - 1);
-        atomicAdd(p, __double2int_rn((double)rmul(dx1m, dy1m) * scale));
-        atomicAdd(p + 1, __double2int_rn((double)rmul(dx, dy1m) * scale));
-        atomicAdd(p + n, __double2int_rn((double)rmul(dx1m, dy) * scale));
-        atomicAdd(p + n + 1, __double2int_rn((double)rmul(dx, dy) * scale));
+        int* p = hi + (iqy - 1) * n + (iqx - 1);
+        add(p, (double)rmul(dx1m, dy1m));
+        add(p + 1, (double)rmul(dx, dy1m));
+        add(p + n, (double)rmul(dx1m, dy));
+        add(p + n + 1, (double)rmul(dx, dy));
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
@@ -321,19 +367,20 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
   }
   __syncthreads();
   const double inv = scale > 0.0 ? 1.0 / scale : 0.0;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) img[i] = (float)((double)acc[i] * inv);
-  __syncthreads();
-  const float w = lb ? (float)lb[k] : 1.0f;
-  float4* out = projt + (size_t)blockIdx.x * n * n;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) out[i] = projt_terms(img, i + 1, n, w);
+  const double w = lb ? (double)lb[k] : 1.0;
+  ProjtEntry<WIDE>* out = projt + (size_t)blockIdx.x * n * n;
+  auto val = [&](int i) {
+    return WIDE ? ((double)hi[i] * 65536.0 + (double)lo[i]) * inv : (double)hi[i] * inv;
+  };
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
 }
 
 // BCKPJ_LIN from PROJT tables of images [k0, k1) (table of image k at
 // projt + (k - kbase) * n * n), accumulating in T.
-template <class T>
+template <class T, bool WIDE>
 __global__ void __launch_bounds__(256) bckpj_projt_kernel(T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                           const int* __restrict__ vox_run, const int* __restrict__ vox_off,
-                                                          long long nvox, const float4* __restrict__ projt,
+                                                          long long nvox, const ProjtEntry<WIDE>* __restrict__ projt,
                                                           const CgDM* __restrict__ dms, int kbase, int k0, int k1, int n,
                                                           int ldp) {
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
@@ -350,10 +397,10 @@ __global__ void __launch_bounds__(256) bckpj_projt_kernel(T* __restrict__ cube, 
       const float ybb = __fadd_rn(yb, __fmul_rn(fj, dm.d[3]));
       const int iqx = __float2int_rz(xbb), iqy = __float2int_rz(ybb);
       const int I = (iqy - 1) * n + iqx;  // PROJT column, 1-based
-      float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (I >= 1 && I <= n * n - n - 1) b = __ldg(projt + (size_t)(k - kbase) * n * n + (I - 1));
+      double b1 = 0.0, b2 = 0.0, b3 = 0.0, b4 = 0.0;
+      if (I >= 1 && I <= n * n - n - 1) projt_load(projt + (size_t)(k - kbase) * n * n + (I - 1), b1, b2, b3, b4);
       const T dy = (T)__fsub_rn(ybb, (float)iqy), dx = (T)__fsub_rn(xbb, (float)iqx);
-      c = radd(radd(radd(c, (T)b.x), rmul(dy, (T)b.y)), rmul(dx, radd((T)b.z, rmul(dy, (T)b.w))));
+      c = radd(radd(radd(c, (T)b1), rmul(dy, (T)b2)), rmul(dx, radd((T)b3, rmul(dy, (T)b4))));
     }
     cube[lin] = c;
   }
@@ -645,22 +692,22 @@ static int launch_backproject(spi_ctx* c, const CgProblem& pb, T* cube, const T*
 }
 
 
-// images per PROJT chunk of the mixed mode: tables of <= ~1 GB
-static int projt_chunk(int n, int nang) {
-  const long long per = (long long)n * n * (long long)sizeof(float4);
+// images per PROJT chunk of the mixed modes: tables of <= ~1 GB
+static int projt_chunk(int n, int nang, size_t entry) {
+  const long long per = (long long)n * n * (long long)entry;
   return (int)std::max<long long>(64, std::min<long long>(nang, (1ll << 30) / per));
 }
 
-// the mixed mode needs the FP32 projection in shared memory
-static bool mixed_fits(int n) { return (size_t)n * n * sizeof(float) <= 200 * 1024; }
+// the mixed modes keep the fixed-point projection in shared memory
+static bool mixed_fits(int n, bool wide) { return (size_t)n * n * (wide ? 8 : 4) <= 200 * 1024; }
 
 // A^T from PROJT tables of images [k0, k1), 64 images per launch
-template <class T>
-static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, const float4* projt, const CgDM* dms,
-                                    int kbase, int k0, int k1) {
+template <class T, bool WIDE>
+static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, const ProjtEntry<WIDE>* projt,
+                                    const CgDM* dms, int kbase, int k0, int k1) {
   for (int a = k0; a < k1; a += 64) {
     const int b = std::min(k1, a + 64);
-    bckpj_projt_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
+    bckpj_projt_kernel<T, WIDE><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(
         cube, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(), c->cg_buf[2].as<int>(), pb.nvox, projt, dms, kbase, a,
         b, pb.n, pb.ldp);
     SPI_TRY(check_kernel("bckpj_projt_kernel"));
@@ -670,12 +717,12 @@ static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, co
 }
 
 // A then A^T (BCKE += A^T A BCKP) chunk by chunk through PROJT tables
-template <class T>
+template <class T, bool WIDE>
 static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* out, const CgDM* dms, const int* lb,
-                               int nang, float4* projt, unsigned long long* maxabs) {
+                               int nang, ProjtEntry<WIDE>* projt, unsigned long long* maxabs) {
   const int n = pb.n;
-  const int K = projt_chunk(n, nang);
-  const size_t smem = (size_t)n * n * sizeof(float);
+  const int K = projt_chunk(n, nang, sizeof(ProjtEntry<WIDE>));
+  const size_t smem = (size_t)n * n * (WIDE ? 8 : 4);
   // fixed-point scale of the projector: max |x| over the sphere
   SPI_CUDA(cudaMemsetAsync(maxabs, 0, sizeof(unsigned long long), c->stream));
   absmax_kernel<T><<<blocks_for(c, pb.nvox, 256), 256, 0, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), c->cg_buf[1].as<int>(),
@@ -687,16 +734,33 @@ static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* o
   static std::atomic<unsigned long long> attr_set{0};
   const unsigned long long bit = 1ull << (c->device & 63);
   if (!(attr_set.load() & bit)) {
-    cudaFuncSetAttribute(prjcq_projt_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(prjcq_projt_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set.fetch_or(bit);
   }
   for (int k0 = 0; k0 < nang; k0 += K) {
     const int kc = std::min(K, nang - k0);
-    prjcq_projt_kernel<T><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, lb,
-                                                         k0, n, pb.ldp, maxabs, mcap, projt);
+    prjcq_projt_kernel<T, WIDE><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
+                                                               lb, k0, n, pb.ldp, maxabs, mcap, projt);
     SPI_TRY(check_kernel("prjcq_projt_kernel"));
     c->count();
-    SPI_TRY(launch_backproject_projt<T>(c, pb, out, projt, dms, k0, k0, k0 + kc));
+    SPI_TRY((launch_backproject_projt<T, WIDE>(c, pb, out, projt, dms, k0, k0, k0 + kc)));
+  }
+  return 0;
+}
+
+// setup A^T of the input images through PROJT tables
+template <class T, bool WIDE>
+static int backproject_images_projt(spi_ctx* c, const CgProblem& pb, T* cb, const float* imgs, const CgDM* dms,
+                                    int nang, ProjtEntry<WIDE>* projt) {
+  const int n = pb.n;
+  const int K = projt_chunk(n, nang, sizeof(ProjtEntry<WIDE>));
+  for (int k0 = 0; k0 < nang; k0 += K) {
+    const int kc = std::min(K, nang - k0);
+    projt_images_kernel<WIDE><<<blocks_for(c, (long long)kc * n * n, 256), 256, 0, c->stream>>>(
+        imgs + (size_t)k0 * n * n, n, kc, projt);
+    SPI_TRY(check_kernel("projt_images_kernel"));
+    c->count();
+    SPI_TRY((launch_backproject_projt<T, WIDE>(c, pb, cb, projt, dms, k0, k0, k0 + kc)));
   }
   return 0;
 }
@@ -775,8 +839,10 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   const size_t vb = nnn * sizeof(T);
   const size_t pcount = (size_t)nang * n * n;
   // mixed mode (FP64 vectors, FP32 PROJT tables made per chunk of images)
-  const bool mixed = sizeof(T) == 8 && c->cg_fp64 == 2 && mixed_fits(n);
-  const int K = projt_chunk(n, nang);
+  const bool wide = c->cg_fp64 == 2;
+  const bool mixed = sizeof(T) == 8 && (c->cg_fp64 == 2 || c->cg_fp64 == 3) && mixed_fits(n, wide);
+  const size_t pentry = wide ? sizeof(ProjtEntry<true>) : sizeof(ProjtEntry<false>);
+  const int K = projt_chunk(n, nang, pentry);
   // buffers: [3] dms, [4] CB, [5] projections (T) + float staging (mixed: float images + PROJT chunk),
   // [6] BCKN|BCKP|BCKE, [7] scalars + lb
   std::vector<CgDM> dms;
@@ -784,7 +850,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
   SPI_TRY(c->cg_buf[4].ensure(vb));
   if (mixed)
-    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float) + (size_t)K * n * n * sizeof(float4) + 16));
+    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float) + (size_t)K * n * n * pentry + 32));
   else
     SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
   SPI_TRY(c->cg_buf[6].ensure(3 * vb));
@@ -793,8 +859,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   T* pj = c->cg_buf[5].as<T>();
   float* pj32 = mixed ? c->cg_buf[5].as<float>()
                       : (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
-  float4* projt = mixed ? reinterpret_cast<float4*>(c->cg_buf[5].as<char>() + ((pcount * sizeof(float) + 15) & ~size_t(15)))
-                        : nullptr;
+  void* projt = mixed ? (void*)(c->cg_buf[5].as<char>() + ((pcount * sizeof(float) + 31) & ~size_t(31))) : nullptr;
   T* bckn = c->cg_buf[6].as<T>();
   T* bckp = bckn + nnn;
   T* bcke = bckp + nnn;
@@ -810,14 +875,12 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   c->count();
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
   if (mixed) {
-    for (int k0 = 0; k0 < nang; k0 += K) {
-      const int kc = std::min(K, nang - k0);
-      projt_images_kernel<<<blocks_for(c, (long long)kc * n * n, 256), 256, 0, c->stream>>>(pj32 + (size_t)k0 * n * n,
-                                                                                            n, kc, projt);
-      SPI_TRY(check_kernel("projt_images_kernel"));
-      c->count();
-      SPI_TRY(launch_backproject_projt<T>(c, pb, cb, projt, c->cg_buf[3].as<CgDM>(), k0, k0, k0 + kc));
-    }
+    if (wide)
+      SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
+                                                static_cast<ProjtEntry<true>*>(projt))));
+    else
+      SPI_TRY((backproject_images_projt<T, false>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
+                                                 static_cast<ProjtEntry<false>*>(projt))));
   } else {
     if (sizeof(T) != sizeof(float)) {
       widen_kernel<T><<<blocks_for(c, (long long)pcount, 256), 256, 0, c->stream>>>(pj32, pj, pcount);
@@ -892,8 +955,13 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
     if (mixed) {
-      SPI_TRY(launch_normal_projt<T>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo, projt,
-                                     reinterpret_cast<unsigned long long*>(acc + 7)));
+      auto* mx = reinterpret_cast<unsigned long long*>(acc + 7);
+      if (wide)
+        SPI_TRY((launch_normal_projt<T, true>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+                                              static_cast<ProjtEntry<true>*>(projt), mx)));
+      else
+        SPI_TRY((launch_normal_projt<T, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+                                               static_cast<ProjtEntry<false>*>(projt), mx)));
     } else {
       SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
       SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
@@ -979,7 +1047,7 @@ extern "C" {
 
 int spi_ctx_set_cg_precision(spi_ctx* c, int mode) {
   if (!c) return fail(kInvalid, "NULL context");
-  if (mode < 0 || mode > 2) return fail(kInvalid, "spi_ctx_set_cg_precision: mode %d must be 0, 1 or 2", mode);
+  if (mode < 0 || mode > 3) return fail(kInvalid, "spi_ctx_set_cg_precision: mode %d must be 0 .. 3", mode);
   c->cg_fp64 = mode;
   return 0;
 }

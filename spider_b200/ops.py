@@ -348,15 +348,21 @@ def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
 
 
 def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-         ctx: Context | None = None, fp64=True):
+         ctx: Context | None = None, fp64="mixed"):
     """``BP CG`` (linear interpolation).  Prompts in reference order: radius
     (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
-    ``fp64``: True keeps the CG vectors and projections in FP64 (default),
-    False uses the reference's REAL, "mixed" keeps FP64 vectors and
-    accumulates each projection in FP32 shared memory.
+    ``fp64``: "mixed" (default) keeps the CG vectors in FP64 and the
+    projections in 47-bit fixed point / FP64 tables, "fast" in 31-bit fixed
+    point / FP32 tables, True keeps everything in FP64, False uses the
+    reference's REAL.
     Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
     ctx = ctx or default_context()
-    prec = 2 if fp64 == "mixed" else (1 if fp64 else 0)
+    if isinstance(fp64, str):
+        if fp64 not in ("mixed", "fast"):
+            raise SpiderError(101, f"unknown BP CG precision {fp64!r}")
+        prec = 2 if fp64 == "mixed" else 3
+    else:
+        prec = 1 if fp64 else 0
     check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))
     projs = _host_f32(projs)
     n = _nx_of(projs)
@@ -373,7 +379,7 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
 
 
 def bpcg3(projs, angles, half_mask, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-          ctx: Context | None = None, fp64: bool = True):
+          ctx: Context | None = None, fp64="mixed"):
     """``BP CG 3``: the overall solution and one for each of two sample sets,
     as three independent CG solves (bpcg.f:139-160,300-400).  ``half_mask[i]``
     = 1 puts image i in the first sample (the reference draws the two lists

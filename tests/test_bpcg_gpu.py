@@ -61,18 +61,19 @@ def test_cg_operator_pair_adjoint(ctx):
     assert abs(lhs - rhs) <= 1e-4 * max(abs(lhs), abs(rhs))
 
 
+@pytest.mark.parametrize("prec", ["mixed", True])
 @pytest.mark.parametrize("mode", [1, 2, 3])
-def test_bpcg_matches_fp64_oracle(ctx, orc, mode):
+def test_bpcg_matches_fp64_oracle(ctx, orc, mode, prec):
     n, nang = 32, 120
     _, pr, ang = _data(n, nang, 10 + mode, snr=1.0)
     ri = float(n // 2 - 2 - mode)
-    vol, log = ops.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=12, mode=mode, lam=0.5, ctx=ctx)
+    vol, log = ops.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=12, mode=mode, lam=0.5, ctx=ctx, fp64=prec)
     ref64, rlog64, neff, _ = orc.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=12, mode=mode, lam=0.5, prec=1)
     ref32, _, _, _ = orc.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=12, mode=mode, lam=0.5, prec=0)
     e64 = synth.rel_l2(vol, ref64)
     e32 = synth.rel_l2(vol, ref32)
     d_ref = synth.rel_l2(ref32, ref64)
-    print(f"BP CG mode {mode}: rel-err vs FP64 oracle {e64:.3e} (FP32 oracle vs FP64 oracle {d_ref:.3e}), "
+    print(f"BP CG mode {mode} prec {prec}: rel-err vs FP64 oracle {e64:.3e} (FP32 oracle vs FP64 oracle {d_ref:.3e}), "
           f"vs FP32 oracle {e32:.3e}, iters {len(log)}")
     assert len(log) == len(rlog64)
     assert e64 <= 1e-4
@@ -113,15 +114,16 @@ def test_bpcg_radius_too_large(ctx):
 
 
 @pytest.mark.parametrize("n", [32, 64])
-def test_bpcg_mixed_precision_matches_fp64_oracle(ctx, orc, n):
-    """FP64 vectors with each projection accumulated in FP32 shared memory
-    stays within the 1e-4 bar of the FP64 oracle."""
+def test_bpcg_fast_precision_matches_fp64_oracle(ctx, orc, n):
+    """Precision mode 3 (31-bit fixed-point projections, FP32 PROJT tables)
+    stays within the 1e-4 bar of the FP64 oracle on a well-conditioned case
+    (it is not the default: on ill-conditioned ones it can exceed it)."""
     nang = 160
     _, pr, ang = _data(n, nang, 40 + n, snr=1.0)
     ri = float(n // 2 - 3)
-    vol, log = ops.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=10, mode=1, lam=0.5, ctx=ctx, fp64="mixed")
+    vol, log = ops.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=10, mode=1, lam=0.5, ctx=ctx, fp64="fast")
     ref64, rlog64, _, _ = orc.bpcg(pr, ang, ri, errm=1e-7, chim=0.0, maxit=10, mode=1, lam=0.5, prec=1)
     e64 = synth.rel_l2(vol, ref64)
-    print(f"BP CG mixed n={n}: rel-err vs FP64 oracle {e64:.3e}")
+    print(f"BP CG fast n={n}: rel-err vs FP64 oracle {e64:.3e}")
     assert len(log) == len(rlog64)
     assert e64 <= 1e-4
