@@ -249,3 +249,31 @@ def test_bp_autotune(ctx, orc):
         assert ctx.bp_autotune() == cfg        # cached
     finally:
         ctx.bp_close()
+
+
+def test_bp3f_max_box_linearity(ctx):
+    """At the largest box (nx = 512: a 1024^3 padded grid of 8.6 GB) the
+    reconstruction is linear in the images for fixed angles (X is, W depends
+    only on the angles, and WINDKB2A's shell mean is linear): a size-
+    independent check where the oracle would take too long."""
+    nx, nimg = 512, 6
+    rng = np.random.default_rng(512)
+    a = rng.standard_normal((nimg, nx, nx)).astype(np.float32)
+    b = rng.standard_normal((nimg, nx, nx)).astype(np.float32)
+    ang = synth.so3_angles(nimg, rng)
+    va = ops.bp3f(a, ang, ctx=ctx)
+    vb = ops.bp3f(b, ang, ctx=ctx)
+    vab = ops.bp3f(a + 2.0 * b, ang, ctx=ctx)
+    assert va.shape == (nx, nx, nx)
+    assert np.isfinite(vab).all()
+    assert synth.rel_l2(vab, va + 2.0 * vb) <= 1e-5
+
+
+def test_bp_insert_zero_images_is_noop(ctx):
+    ctx.bp_open(32, 2)
+    try:
+        ctx.bp_insert(np.zeros((0, 32, 32), np.float32), np.zeros((0, 3), np.float32), np.zeros(0, np.uint8))
+        o = ctx.bp_finish(("all", "1", "2"))
+    finally:
+        ctx.bp_close()
+    assert all(np.all(v == 0) for v in o.values())

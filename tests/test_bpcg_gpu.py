@@ -6,6 +6,8 @@ its atomic splats.  The CG itself keeps its scalars (DELSQ, AKDEN, P, Q) in
 FP64, so the solution is compared with the FP64 oracle at rel-err <= 1e-4
 (the BP CG bar) and with the FP32 oracle at the same bound.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -127,3 +129,35 @@ def test_bpcg_fast_precision_matches_fp64_oracle(ctx, orc, n):
     print(f"BP CG fast n={n}: rel-err vs FP64 oracle {e64:.3e}")
     assert len(log) == len(rlog64)
     assert e64 <= 1e-4
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fast"])
+def test_bpcg_cluster_projector_matches_single_cta(ctx, prec):
+    """The projector split over a 2- or 4-CTA cluster (distributed shared
+    memory) sums the same fixed-point integers as the one-CTA kernel."""
+    n, nang = 32, 60
+    _, pr, ang = _data(n, nang, 51, snr=1.0)
+    out = {}
+    for cl in ("1", "2", "4"):
+        os.environ["SPI_CG_CLUSTER"] = cl
+        try:
+            out[cl], _ = ops.bpcg(pr, ang, 12.0, errm=1e-9, chim=0.0, maxit=4, mode=1, lam=0.5, ctx=ctx, fp64=prec)
+        finally:
+            del os.environ["SPI_CG_CLUSTER"]
+    for cl in ("2", "4"):
+        assert synth.rel_l2(out[cl], out["1"]) <= 1e-10, cl
+
+
+def test_bpcg_mixed_large_box_uses_cluster(ctx):
+    """n = 176 does not fit one CTA in the default mode (176^2 x 8 bytes):
+    the cluster projector runs and agrees with full FP64."""
+    n, nang = 176, 24
+    rng = np.random.default_rng(61)
+    vol = synth.blob_phantom(n, 6, sigma=(3.0, 6.0), radius=0.3 * n, rng=rng)
+    ang = synth.so3_angles(nang, rng)
+    pr = ops.pj3q(vol, ang, ctx=ctx)
+    ri = float(n // 2 - 3)
+    v2, log2 = ops.bpcg(pr, ang, ri, errm=1e-9, chim=0.0, maxit=3, mode=1, lam=0.5, ctx=ctx, fp64="mixed")
+    v1, log1 = ops.bpcg(pr, ang, ri, errm=1e-9, chim=0.0, maxit=3, mode=1, lam=0.5, ctx=ctx, fp64=True)
+    assert len(log2) == len(log1)
+    assert synth.rel_l2(v2, v1) <= 1e-7
