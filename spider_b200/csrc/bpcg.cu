@@ -17,7 +17,6 @@
 // projections are FP64 by default and FP32 (the reference's REAL) on request.
 // One CG iteration is a fixed kernel sequence captured once as a CUDA graph.
 #include <atomic>
-#include <cooperative_groups.h>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -376,82 +375,88 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
 }
 
-// The same projector for images too large for one CTA's shared memory: a
-// cluster of C CTAs per projection, CTA r holding rows [r R, (r+1) R) of the
-// fixed-point image (R = ceil(n / C)).  The CTAs split the voxel runs; every
-// splat goes to the CTA that owns the pixel's row through distributed shared
-// memory (integer atomics on the cluster window), and the PROJT epilogue reads
-// the neighbouring row of the next CTA the same way.  Integer sums do not
-// depend on the order, so the tables equal those of prjcq_projt_kernel.
+// The same projector for images too large for one CTA's shared memory: C
+// CTAs per projection, CTA b owning the pixel rows [b R, b R + R) (R =
+// ceil(n / C)) and accumulating rows [b R, b R + R + 2) of the fixed-point
+// image, the two extra rows being what its PROJT entries read beyond the
+// band (I + N, and I + 1 wrapping to the next row at the last column).  Every
+// CTA walks all runs with the reference's sequential XB/YB steps and splats
+// only into its rows, so all atomics stay in its own shared memory; the
+// voxels of other bands cost four instructions each.  Integer sums make the
+// tables identical to those of the one-CTA kernel.  (A 2-4 CTA cluster
+// adding into one another's bands through distributed shared memory was
+// measured 3-8x slower at n = 256.)
 template <class T, bool WIDE>
-__global__ void __launch_bounds__(512) prjcq_projt_cluster_kernel(
+__global__ void __launch_bounds__(512) prjcq_projt_band_kernel(
     const T* __restrict__ cube, const CgRun* __restrict__ runs, int nruns, const CgDM* __restrict__ dms,
-    const int* __restrict__ lb, int kbase, int n, int ldp, const unsigned long long* __restrict__ maxabs_bits,
+    const int* __restrict__ lb, int kbase, int n, int ldp, int C, const unsigned long long* __restrict__ maxabs_bits,
     float mcap, ProjtEntry<WIDE>* __restrict__ projt) {
-  namespace cg = cooperative_groups;
-  cg::cluster_group cluster = cg::this_cluster();
-  const int C = (int)cluster.num_blocks();
-  const int rank = (int)cluster.block_rank();
-  const int R = (n + C - 1) / C;                 // rows per CTA
-  const int band = R * n;                        // words per CTA and array
+  const int R = (n + C - 1) / C;
+  const int proj = blockIdx.x / C, b = blockIdx.x % C;
+  const int r0 = b * R;
+  const int r1 = min(n, r0 + R);             // owned rows [r0, r1)
+  const int h1 = min(n, r0 + R + 2);         // accumulated rows [r0, h1)
+  const int words = (R + 2) * n;             // per array
   extern __shared__ __align__(16) unsigned char smraw[];
-  int* hi = reinterpret_cast<int*>(smraw);       // lo = hi + band (WIDE)
-  const int proj = blockIdx.x / C;
+  int* hi = reinterpret_cast<int*>(smraw);   // lo = hi + words (WIDE)
   const int k = kbase + proj;
-  for (int i = threadIdx.x; i < band * (WIDE ? 2 : 1); i += blockDim.x) hi[i] = 0;
+  for (int i = threadIdx.x; i < words * (WIDE ? 2 : 1); i += blockDim.x) hi[i] = 0;
   const double maxabs = __longlong_as_double((long long)*maxabs_bits);
   const double full = WIDE ? 0.95 * 140737488355328.0 : 0.95 * 2147483648.0;   // 2^47 or 2^31
   const double scale = maxabs > 0.0 ? full / ((double)mcap * maxabs) : 0.0;
-  cluster.sync();   // every band is zero before any CTA adds to it
-  auto word = [&](int pix) -> int* {             // pixel (0-based) -> its high word in the owner's band
-    const int row = pix / n, owner = row / R;
-    return cluster.map_shared_rank(hi, owner) + (pix - owner * band);
-  };
-  auto add = [&](int pix, double w) {
-    int* p = word(pix);
+  __syncthreads();
+  auto add = [&](int local, double w) {
     if (WIDE) {
       const long long q = __double2ll_rn(w * scale);
-      atomicAdd(p, (int)(q >> 16));
-      atomicAdd(p + band, (int)(q & 0xffff));
+      atomicAdd(hi + local, (int)(q >> 16));
+      atomicAdd(hi + words + local, (int)(q & 0xffff));
     } else {
-      atomicAdd(p, __double2int_rn(w * scale));
+      atomicAdd(hi + local, __double2int_rn(w * scale));
     }
   };
   const CgDM dm = dms[k];
-  for (int ri = rank * blockDim.x + threadIdx.x; ri < nruns; ri += C * blockDim.x) {
+  for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
     const CgRun r = runs[ri];
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
     float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
     float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
     for (int j = r.l1; j <= r.l2; ++j) {
-      const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
-      if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        const T cv = cube[(size_t)j - 1];
-        const T dx = (T)__fsub_rn(xb, (float)iqx);
-        const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
-        const T dx1m = rsub((T)1, dx);
-        const T dy1m = rsub(cv, dy);
-        const int p0 = (iqy - 1) * n + (iqx - 1);
-        add(p0, (double)rmul(dx1m, dy1m));
-        add(p0 + 1, (double)rmul(dx, dy1m));
-        add(p0 + n, (double)rmul(dx1m, dy));
-        add(p0 + n + 1, (double)rmul(dx, dy));
+      const int iqy = __float2int_rz(yb);
+      // rows iqy-1 and iqy (0-based) of the splat; skip unless one is accumulated here
+      if (iqy >= r0 && iqy - 1 < h1) {
+        const int iqx = __float2int_rz(xb);
+        if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
+          const T cv = cube[(size_t)j - 1];
+          const T dx = (T)__fsub_rn(xb, (float)iqx);
+          const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
+          const T dx1m = rsub((T)1, dx);
+          const T dy1m = rsub(cv, dy);
+          const int ya = iqy - 1, yb1 = iqy;   // pixel rows, 0-based
+          if (ya >= r0 && ya < h1) {
+            const int l = (ya - r0) * n + (iqx - 1);
+            add(l, (double)rmul(dx1m, dy1m));
+            add(l + 1, (double)rmul(dx, dy1m));
+          }
+          if (yb1 >= r0 && yb1 < h1) {
+            const int l = (yb1 - r0) * n + (iqx - 1);
+            add(l, (double)rmul(dx1m, dy));
+            add(l + 1, (double)rmul(dx, dy));
+          }
+        }
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
     }
   }
-  cluster.sync();   // all splats have landed
+  __syncthreads();
   const double inv = scale > 0.0 ? 1.0 / scale : 0.0;
   const double w = lb ? (double)lb[k] : 1.0;
   ProjtEntry<WIDE>* out = projt + (size_t)proj * n * n;
   auto val = [&](int pix) {
-    const int* p = word(pix);
-    return WIDE ? ((double)p[0] * 65536.0 + (double)p[band]) * inv : (double)p[0] * inv;
+    const int l = pix - r0 * n;
+    return WIDE ? ((double)hi[l] * 65536.0 + (double)hi[words + l]) * inv : (double)hi[l] * inv;
   };
-  const int first = rank * band, last = min(n * n, first + band);
-  for (int i = first + threadIdx.x; i < last; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
-  cluster.sync();   // neighbours have finished reading this band
+  for (int i = r0 * n + threadIdx.x; i < r1 * n; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
 }
 
 // BCKPJ_LIN from PROJT tables of images [k0, k1) (table of image k at
@@ -778,23 +783,24 @@ static int projt_chunk(int n, int nang, size_t entry) {
 }
 
 // The mixed modes keep the fixed-point projection in shared memory, split
-// over a cluster of C CTAs (1, 2, 4 or 8) when one CTA's 200 KB do not hold
-// it; 0 when no cluster size does.  SPI_CG_CLUSTER forces a (fitting) size.
-static size_t cluster_band_bytes(int n, int C, bool wide) {
-  return (size_t)((n + C - 1) / C) * n * (wide ? 8 : 4);
+// into C row bands (1, 2, 4 or 8 CTAs per projection) when one CTA's 200 KB
+// do not hold it; 0 when no split does.  SPI_CG_BANDS forces a (fitting) C.
+static size_t band_bytes(int n, int C, bool wide) {
+  if (C == 1) return (size_t)n * n * (wide ? 8 : 4);
+  return (size_t)((n + C - 1) / C + 2) * n * (wide ? 8 : 4);
 }
-static int mixed_cluster(int n, bool wide) {
+static int mixed_bands(int n, bool wide) {
   const size_t cap = 200 * 1024;
   int C = 1;
-  while (C <= 8 && cluster_band_bytes(n, C, wide) > cap) C *= 2;
+  while (C <= 8 && band_bytes(n, C, wide) > cap) C *= 2;
   if (C > 8) return 0;
-  if (const char* e = getenv("SPI_CG_CLUSTER")) {
+  if (const char* e = getenv("SPI_CG_BANDS")) {
     const int f = atoi(e);
-    if ((f == 1 || f == 2 || f == 4 || f == 8) && f >= C) C = f;
+    if ((f == 1 || f == 2 || f == 4 || f == 8) && f >= C && f <= n / 2) C = f;
   }
   return C;
 }
-static bool mixed_fits(int n, bool wide) { return mixed_cluster(n, wide) > 0; }
+static bool mixed_fits(int n, bool wide) { return mixed_bands(n, wide) > 0; }
 
 // A^T from PROJT tables of images [k0, k1), 64 images per launch
 template <class T, bool WIDE>
@@ -830,33 +836,19 @@ static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* o
   const unsigned long long bit = 1ull << (c->device & 63);
   if (!(attr_set.load() & bit)) {
     cudaFuncSetAttribute(prjcq_projt_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(prjcq_projt_cluster_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(prjcq_projt_band_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set.fetch_or(bit);
   }
-  const int C = mixed_cluster(n, WIDE);
+  const int C = mixed_bands(n, WIDE);
   if (C < 1) return fail(kInvalid, "BP CG: n = %d too large for the mixed precision modes", n);
   for (int k0 = 0; k0 < nang; k0 += K) {
     const int kc = std::min(K, nang - k0);
-    if (C == 1) {
+    if (C == 1)
       prjcq_projt_kernel<T, WIDE><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
                                                                  lb, k0, n, pb.ldp, maxabs, mcap, projt);
-    } else {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3((unsigned)(kc * C), 1, 1);
-      cfg.blockDim = dim3(512, 1, 1);
-      cfg.dynamicSmemBytes = cluster_band_bytes(n, C, WIDE);
-      cfg.stream = c->stream;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = (unsigned)C;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      SPI_CUDA(cudaLaunchKernelEx(&cfg, prjcq_projt_cluster_kernel<T, WIDE>, x, (const CgRun*)c->cg_buf[0].as<CgRun>(),
-                                  (int)pb.runs.size(), dms, lb, k0, n, pb.ldp, (const unsigned long long*)maxabs, mcap,
-                                  projt));
-    }
+    else
+      prjcq_projt_band_kernel<T, WIDE><<<kc * C, 512, band_bytes(n, C, WIDE), c->stream>>>(
+          x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, lb, k0, n, pb.ldp, C, maxabs, mcap, projt);
     SPI_TRY(check_kernel("prjcq_projt_kernel"));
     c->count();
     SPI_TRY((launch_backproject_projt<T, WIDE>(c, pb, out, projt, dms, k0, k0, k0 + kc)));

@@ -132,25 +132,25 @@ def test_bpcg_fast_precision_matches_fp64_oracle(ctx, orc, n):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fast"])
-def test_bpcg_cluster_projector_matches_single_cta(ctx, prec):
-    """The projector split over a 2- or 4-CTA cluster (distributed shared
-    memory) sums the same fixed-point integers as the one-CTA kernel."""
+def test_bpcg_band_projector_matches_single_cta(ctx, prec):
+    """The projector split into 2, 4 or 8 row bands (one CTA each) sums the
+    same fixed-point integers as the one-CTA kernel."""
     n, nang = 32, 60
     _, pr, ang = _data(n, nang, 51, snr=1.0)
     out = {}
-    for cl in ("1", "2", "4"):
-        os.environ["SPI_CG_CLUSTER"] = cl
+    for cl in ("1", "2", "4", "8"):
+        os.environ["SPI_CG_BANDS"] = cl
         try:
             out[cl], _ = ops.bpcg(pr, ang, 12.0, errm=1e-9, chim=0.0, maxit=4, mode=1, lam=0.5, ctx=ctx, fp64=prec)
         finally:
-            del os.environ["SPI_CG_CLUSTER"]
-    for cl in ("2", "4"):
+            del os.environ["SPI_CG_BANDS"]
+    for cl in ("2", "4", "8"):
         assert synth.rel_l2(out[cl], out["1"]) <= 1e-10, cl
 
 
-def test_bpcg_mixed_large_box_uses_cluster(ctx):
+def test_bpcg_mixed_large_box_uses_bands(ctx):
     """n = 176 does not fit one CTA in the default mode (176^2 x 8 bytes):
-    the cluster projector runs and agrees with full FP64."""
+    the row-band projector runs and agrees with full FP64."""
     n, nang = 176, 24
     rng = np.random.default_rng(61)
     vol = synth.blob_phantom(n, 6, sigma=(3.0, 6.0), radius=0.3 * n, rng=rng)
