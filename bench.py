@@ -261,9 +261,41 @@ def cg_measure(args, ctx, stream, rank, world):
            "rel_err_fast_vs_fp64": rel("fast_graph"),
            "config": {"n": n, "images": nang, "lambda": 1e-3, "mode": 1, "iterations_timed": K,
                       "phantom": "50 Gaussian blobs, sigma 2-8, SNR 0.3, uniform SO(3)"}}
+    res["differentiable_cg"] = autograd_cg_measure(ctx, projs, ang, ri, K)
     if rank == 0 and world == 1 and not args.no_cpu:
         res["cpu_baseline"] = cg_cpu_baseline(projs, ang, ri, n)
     return res
+
+
+def autograd_cg_measure(ctx, projs, ang, ri, K, lam=1e-3):
+    """The differentiable reconstruction of configuration 3: CG on
+    (A^T A + lam I) x = A^T b with A = PJ 3Q through the capturable operator
+    pair (spider_b200.autograd.NormalCG), one iteration replayed as a CUDA
+    graph against the same iteration launched op by op; seconds per
+    iteration from the difference of a 1- and a (1+K)-iteration solve."""
+    import torch
+    from spider_b200 import autograd
+    n = projs.shape[1]
+    plan = autograd.PJ3QPlan((n, n, n), ang, ri, ctx=ctx)
+    b = torch.from_numpy(projs).cuda()
+    rhs = plan.adjoint(b)
+    out = {}
+    for name, graph in (("graph_s_per_iter", True), ("plain_s_per_iter", False)):
+        times = []
+        for iters in (1, 1 + K):
+            solver = autograd.NormalCG(plan, lam, iters, graph=graph)
+            solver.solve(rhs)                   # warm-up (and graph capture)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            solver.solve(rhs)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        out[name] = (times[1] - times[0]) / K
+    plan.close()
+    out["operator"] = "PJ 3Q and its exact adjoint (trilinear), FP32, FP64 dot products"
+    return out
 
 
 def cg_cpu_baseline(projs, ang, ri, n, sample=500):

@@ -200,6 +200,22 @@ int spi_pj3q_noalloc(const float* vol, int nx, int ny, int nz, float ri, const f
 int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, float ri,
                      const float* angles, int nang, float* vol_out, int on_device);
 
+/* PJ 3Q plan (no counterpart in the reference, whose PJ 3Q is one call):
+ * the voxel runs (PREPCUB, prepcub.f:54-109) and rotation matrices for one
+ * volume shape, radius and angle list (host float[nang*3]), uploaded once.
+ * spi_pj3q_plan_forward / _adjoint then only launch kernels on `stream`
+ * (a cudaStream_t; NULL = the default stream) with device buffers: they
+ * allocate nothing and do not synchronise, so they can be captured in a
+ * CUDA graph.  The forward equals spi_pj3q, the adjoint spi_pj3q_adjoint;
+ * both overwrite their output.  A plan keeps a pointer to its context for
+ * launch counting and must be destroyed before it. */
+typedef struct spi_pj3q_plan spi_pj3q_plan;
+int spi_pj3q_plan_create(spi_ctx* ctx, int nx, int ny, int nz, float ri, const float* angles, int nang,
+                         spi_pj3q_plan** out);
+int spi_pj3q_plan_forward(const spi_pj3q_plan* plan, const float* vol, float* proj_out, void* stream);
+int spi_pj3q_plan_adjoint(const spi_pj3q_plan* plan, const float* projs, float* vol_out, void* stream);
+int spi_pj3q_plan_destroy(spi_pj3q_plan* plan);
+
 /* ------------------------------------------------------------------ *
  * BP CG, linear interpolation (BPCG, bpcg.f:70 -> BPCG_2 bpcg.f:425,
  * HIANG hiang.f:40, BPCG_3_LIN bpcg.f:818).  projs = float[nang*n*n];

@@ -50,6 +50,11 @@ SIGNATURES = [
                                         _vp, ctypes.c_int, _vp, _vp]),
     ("spi_pj3q_adjoint", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                         _vp, ctypes.c_int, _vp, ctypes.c_int]),
+    ("spi_pj3q_plan_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp,
+                                            ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("spi_pj3q_plan_forward", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("spi_pj3q_plan_adjoint", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("spi_pj3q_plan_destroy", ctypes.c_int, [_vp]),
     ("spi_bpcg", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_float, ctypes.c_float,
                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp]),
     ("spi_ctx_set_cg_precision", ctypes.c_int, [_vp, ctypes.c_int]),

@@ -39,3 +39,139 @@ def pj3q(vol: torch.Tensor, angles, ri: float | None = None, ctx: ops.Context | 
         ri = float(min(vol.shape) // 2 - 2)
     ang = np.ascontiguousarray(angles, dtype=np.float32)
     return PJ3Q.apply(vol, ang, float(ri), ctx or ops.default_context(vol.device.index or 0))
+
+
+# ---------------------------------------------------------------------------
+# Capturable operator pair and a differentiable CG reconstruction on it.
+class PJ3QPlan:
+    """PJ 3Q (forward) and its exact adjoint for one volume shape, radius and
+    angle list, with the voxel runs and rotations uploaded once
+    (``spi_pj3q_plan_*``).  Both launch on torch's current CUDA stream,
+    allocate nothing in the library and do not synchronise, so they can be
+    captured in a CUDA graph."""
+
+    def __init__(self, shape, angles, ri: float | None = None, ctx: ops.Context | None = None, device: int = 0):
+        import ctypes
+        nz, ny, nx = (int(v) for v in shape)
+        self.shape = (nz, ny, nx)
+        self.ri = float(min(shape) // 2 - 2) if ri is None else float(ri)
+        self.angles = np.ascontiguousarray(angles, dtype=np.float32)
+        self.nang = int(self.angles.shape[0])
+        self.ctx = ctx or ops.default_context(device)
+        self.device = torch.device("cuda", self.ctx.device)
+        self._L = self.ctx._L
+        h = ctypes.c_void_p()
+        ops.check(self._L.spi_pj3q_plan_create(self.ctx.handle, nx, ny, nz, self.ri,
+                                               self.angles.ctypes.data_as(ctypes.c_void_p), self.nang,
+                                               ctypes.byref(h)))
+        self._h = h
+
+    def _stream(self):
+        import ctypes
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def forward(self, vol: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        import ctypes
+        if out is None:
+            out = torch.empty((self.nang,) + self.shape[1:], dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_pj3q_plan_forward(self._h, ctypes.c_void_p(vol.data_ptr()),
+                                                ctypes.c_void_p(out.data_ptr()), self._stream()))
+        return out
+
+    def adjoint(self, proj: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        import ctypes
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_pj3q_plan_adjoint(self._h, ctypes.c_void_p(proj.data_ptr()),
+                                                ctypes.c_void_p(out.data_ptr()), self._stream()))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h:
+            self._L.spi_pj3q_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NormalCG:
+    """Conjugate gradients on (A^T A + lam I) x = rhs with A = PJ 3Q, in
+    fixed device buffers; with ``graph`` one iteration is captured once as a
+    CUDA graph and replayed.  Dot products and step lengths are FP64."""
+
+    def __init__(self, plan: PJ3QPlan, lam: float, iters: int, graph: bool = True):
+        self.plan, self.lam, self.iters, self.graph = plan, float(lam), int(iters), graph
+        z = lambda shape: torch.zeros(shape, dtype=torch.float32, device=plan.device)  # noqa: E731
+        self.x, self.r, self.p, self.ap = (z(plan.shape) for _ in range(4))
+        self.q = z((plan.nang,) + plan.shape[1:])
+        self.rs = torch.zeros((), dtype=torch.float64, device=plan.device)
+        self._g = None
+
+    def _iteration(self):
+        self.plan.forward(self.p, out=self.q)
+        self.plan.adjoint(self.q, out=self.ap)
+        self.ap.add_(self.p, alpha=self.lam)
+        pap = (self.p.double() * self.ap.double()).sum()
+        alpha = torch.where(pap > 0, self.rs / pap, torch.zeros_like(pap)).float()
+        self.x.add_(alpha * self.p)
+        self.r.sub_(alpha * self.ap)
+        rs_new = (self.r.double() * self.r.double()).sum()
+        beta = torch.where(self.rs > 0, rs_new / self.rs, torch.zeros_like(rs_new)).float()
+        self.p.mul_(beta).add_(self.r)
+        self.rs.copy_(rs_new)
+
+    def solve(self, rhs: torch.Tensor) -> torch.Tensor:
+        self.x.zero_()
+        self.r.copy_(rhs)
+        self.p.copy_(rhs)
+        self.rs.copy_((rhs.double() * rhs.double()).sum())
+        if not self.graph:
+            for _ in range(self.iters):
+                self._iteration()
+            return self.x.clone()
+        if self._g is None:
+            # warm up on a side stream (as CUDA-graph capture requires), then capture one iteration
+            s = torch.cuda.Stream(self.plan.device)
+            s.wait_stream(torch.cuda.current_stream(self.plan.device))
+            saved = [t.clone() for t in (self.x, self.r, self.p, self.rs)]
+            with torch.cuda.stream(s):
+                self._iteration()
+            torch.cuda.current_stream(self.plan.device).wait_stream(s)
+            for t, v in zip((self.x, self.r, self.p, self.rs), saved):
+                t.copy_(v)
+            self._g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self._g):
+                self._iteration()
+            for t, v in zip((self.x, self.r, self.p, self.rs), saved):   # the capture did not run it
+                t.copy_(v)
+        for _ in range(self.iters):
+            self._g.replay()
+        return self.x.clone()
+
+
+class _CGReconstruct(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, b: torch.Tensor, solver: NormalCG):
+        fctx.solver = solver
+        return solver.solve(solver.plan.adjoint(b.detach().contiguous().float()))
+
+    @staticmethod
+    def backward(fctx, gx: torch.Tensor):
+        # x = M^-1 A^T b with M = A^T A + lam I symmetric: dL/db = A M^-1 dL/dx
+        s = fctx.solver
+        y = s.solve(gx.detach().contiguous().float())
+        return s.plan.forward(y), None
+
+
+def cg_reconstruct(projs: torch.Tensor, solver: NormalCG) -> torch.Tensor:
+    """Regularised least-squares reconstruction x = (A^T A + lam I)^-1 A^T b
+    from CUDA projections b [nang, ny, nx] by ``solver``'s CG iterations,
+    differentiable in b: the backward is a second CG solve (implicit
+    differentiation, no stored iterates)."""
+    if not projs.is_cuda:
+        raise ops.SpiderError(101, "cg_reconstruct needs CUDA projections (there is no CPU path)")
+    return _CGReconstruct.apply(projs, solver)

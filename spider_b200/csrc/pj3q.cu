@@ -242,6 +242,88 @@ int spi_pj3q_adjoint(spi_ctx* c, const float* projs, int nx, int ny, int nz, flo
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// PJ 3Q plans: the voxel runs (PREPCUB) and rotation matrices of one volume
+// shape, radius and angle list, uploaded once; forward and adjoint are then
+// pure launches on a caller stream (no allocation, no host synchronisation),
+// so an iterative solver can capture them in a CUDA graph.
+}  // extern "C"
+
+struct spi_pj3q_plan {
+  spi_ctx* ctx = nullptr;
+  int device = 0, nx = 0, ny = 0, nz = 0, nang = 0, nruns = 0, blocks = 0;
+  float ri = 0.0f;
+  PjRun* runs = nullptr;
+  PjDM* dms = nullptr;
+};
+
+extern "C" {
+
+int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang,
+                         spi_pj3q_plan** out) {
+  if (!out) return fail(kInvalid, "spi_pj3q_plan_create: out is NULL");
+  *out = nullptr;
+  if (nang <= 0) return fail(kInvalid, "spi_pj3q_plan_create: nang = %d", nang);
+  int nruns = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));   // runs and matrices into the context's buffers
+  auto* p = new spi_pj3q_plan();
+  p->ctx = c;
+  p->device = c->device;
+  p->nx = nx; p->ny = ny; p->nz = nz; p->nang = nang; p->nruns = nruns; p->ri = ri;
+  const long long total = (long long)nruns * nang;
+  p->blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
+  cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
+  if (e == cudaSuccess) e = cudaMalloc(&p->dms, (size_t)nang * sizeof(PjDM));
+  if (e == cudaSuccess && nruns)
+    e = cudaMemcpyAsync(p->runs, c->pj_runs.p, (size_t)nruns * sizeof(PjRun), cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(p->dms, c->pj_dm.p, (size_t)nang * sizeof(PjDM), cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    cudaFree(p->runs);
+    cudaFree(p->dms);
+    delete p;
+    return fail(kCuda, "spi_pj3q_plan_create: %s", cudaGetErrorString(e));
+  }
+  *out = p;
+  return 0;
+}
+
+int spi_pj3q_plan_forward(const spi_pj3q_plan* p, const float* vol, float* proj_out, void* stream) {
+  if (!p || !vol || !proj_out) return fail(kInvalid, "spi_pj3q_plan_forward: NULL argument");
+  auto st = static_cast<cudaStream_t>(stream);
+  SPI_CUDA(cudaMemsetAsync(proj_out, 0, (size_t)p->nang * p->nx * p->ny * sizeof(float), st));
+  if (p->blocks > 0) {
+    wpro_kernel<<<p->blocks, 128, 0, st>>>(vol, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
+                                           p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, proj_out);
+    SPI_TRY(check_kernel("wpro_kernel"));
+    p->ctx->count();
+  }
+  return 0;
+}
+
+int spi_pj3q_plan_adjoint(const spi_pj3q_plan* p, const float* projs, float* vol_out, void* stream) {
+  if (!p || !projs || !vol_out) return fail(kInvalid, "spi_pj3q_plan_adjoint: NULL argument");
+  auto st = static_cast<cudaStream_t>(stream);
+  SPI_CUDA(cudaMemsetAsync(vol_out, 0, (size_t)p->nx * p->ny * p->nz * sizeof(float), st));
+  if (p->blocks > 0) {
+    wpro_adjoint_kernel<<<p->blocks, 128, 0, st>>>(projs, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
+                                                   p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, vol_out);
+    SPI_TRY(check_kernel("wpro_adjoint_kernel"));
+    p->ctx->count();
+  }
+  return 0;
+}
+
+int spi_pj3q_plan_destroy(spi_pj3q_plan* p) {
+  if (!p) return 0;
+  cudaSetDevice(p->device);
+  cudaFree(p->runs);
+  cudaFree(p->dms);
+  delete p;
+  return 0;
+}
+
 }  // extern "C"
 
 // ============================================================================
