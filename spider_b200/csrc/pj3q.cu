@@ -56,6 +56,14 @@ __device__ __forceinline__ float run_start(const PjRun& r, float a, float b, flo
                    (float)ldp);
 }
 
+// a[o] for a run-time corner index o, by selects (no local memory)
+__device__ __forceinline__ float sel8(const float (&a)[8], int o) {
+  float v = a[0];
+#pragma unroll
+  for (int i = 1; i < 8; ++i) v = (o == i) ? a[i] : v;
+  return v;
+}
+
 __global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cube, int nsam, int nrow, int nslice,
                                                    const PjRun* __restrict__ runs, int nruns,
                                                    const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
@@ -105,11 +113,17 @@ __global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cub
 
 // Transpose of wpro_kernel: every sample spreads its projection value into
 // the 8 neighbouring voxels with the trilinear weights of the same position.
+// Along a run the 2 x 2 x 2 cell moves by at most one voxel per axis and
+// step (each row of the rotation has unit length), so the eight sums of the
+// current cell are kept in registers; when the cell moves, the corners the
+// next cell shares move with it and only the others go to memory as atomic
+// adds (about half the atomics; each weight still goes to the same voxel).
 __global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restrict__ proj, int nsam, int nrow, int nslice,
                                                            const PjRun* __restrict__ runs, int nruns,
                                                            const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
                                                            int ldpz, float* __restrict__ cube) {
   const long long total = (long long)nruns * nang;
+  const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int a = (int)(t / nruns);
     const PjRun r = runs[t % nruns];
@@ -119,7 +133,29 @@ __global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restri
     float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
     float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
     float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
-    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+    int cx = -8, cy = -8, cz = -8;   // cached cell (none); corner o = i + 2 j + 4 l at (cx+i, cy+j, cz+l)
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    auto move_to = [&](int qx, int qy, int qz) {
+      const int dx = qx - cx, dy = qy - cy, dz = qz - cz;
+      float nw[8];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {   // old corner o lands in new corner (i-dx, j-dy, l-dz) or is flushed
+        const int i = o & 1, j = (o >> 1) & 1, l = o >> 2;
+        const int ni = i - dx, nj = j - dy, nl = l - dz;
+        const bool keep = (unsigned)ni < 2u && (unsigned)nj < 2u && (unsigned)nl < 2u;
+        if (!keep && acc[o] != 0.0f)
+          atomicAdd(cube + (size_t)(cz + l - 1) * sz + (size_t)(cy + j - 1) * sy + (cx + i - 1), acc[o]);
+      }
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {   // new corner o takes old corner (i+dx, j+dy, l+dz) when it exists
+        const int oi = (o & 1) + dx, oj = ((o >> 1) & 1) + dy, ol = (o >> 2) + dz;
+        const bool has = (unsigned)oi < 2u && (unsigned)oj < 2u && (unsigned)ol < 2u;
+        nw[o] = has ? sel8(acc, oi + 2 * oj + 4 * ol) : 0.0f;
+      }
+#pragma unroll
+      for (int o = 0; o < 8; ++o) acc[o] = nw[o];
+      cx = qx; cy = qy; cz = qz;
+    };
     for (int j = r.i1; j <= r.i2; ++j) {
       const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
       if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
@@ -127,21 +163,22 @@ __global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restri
         if (p != 0.0f) {
           const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
           const float ex = 1.0f - dx, ey = 1.0f - dy, ez = 1.0f - dz;
-          float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
-          atomicAdd(c0, p * ex * ey * ez);
-          atomicAdd(c0 + 1, p * dx * ey * ez);
-          atomicAdd(c0 + sy, p * ex * dy * ez);
-          atomicAdd(c0 + sy + 1, p * dx * dy * ez);
-          atomicAdd(c0 + sz, p * ex * ey * dz);
-          atomicAdd(c0 + sz + 1, p * dx * ey * dz);
-          atomicAdd(c0 + sz + sy, p * ex * dy * dz);
-          atomicAdd(c0 + sz + sy + 1, p * dx * dy * dz);
+          if (iox != cx || ioy != cy || ioz != cz) move_to(iox, ioy, ioz);
+          acc[0] += p * ex * ey * ez;
+          acc[1] += p * dx * ey * ez;
+          acc[2] += p * ex * dy * ez;
+          acc[3] += p * dx * dy * ez;
+          acc[4] += p * ex * ey * dz;
+          acc[5] += p * dx * ey * dz;
+          acc[6] += p * ex * dy * dz;
+          acc[7] += p * dx * dy * dz;
         }
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[1]);
       zb = __fadd_rn(zb, dm.d[2]);
     }
+    move_to(-8, -8, -8);   // flush
   }
 }
 
@@ -438,14 +475,31 @@ __global__ void __launch_bounds__(128) noalloc_wpro_kernel(const float* __restri
     float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
     float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
     const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+    // the eight corner values of the current cell; a step moves the cell by
+    // at most one voxel per axis, so the corners it shares are not reloaded
+    int cx = -8, cy = -8, cz = -8;
+    float cv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // corner o = i + 2 j + 4 l
     for (int j = r.i1; j <= r.i2; ++j) {
       const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
       if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
         const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
-        const float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
-        const float c000 = __ldg(c0), c100 = __ldg(c0 + 1), c010 = __ldg(c0 + sy), c110 = __ldg(c0 + sy + 1);
-        const float c001 = __ldg(c0 + sz), c101 = __ldg(c0 + sz + 1), c011 = __ldg(c0 + sz + sy),
-                    c111 = __ldg(c0 + sz + sy + 1);
+        if (iox != cx || ioy != cy || ioz != cz) {
+          const int mx = iox - cx, my = ioy - cy, mz = ioz - cz;
+          const float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
+          float nv[8];
+#pragma unroll
+          for (int o = 0; o < 8; ++o) {
+            const int i = o & 1, jj = (o >> 1) & 1, l = o >> 2;
+            const int oi = i + mx, oj = jj + my, ol = l + mz;
+            const bool has = (unsigned)oi < 2u && (unsigned)oj < 2u && (unsigned)ol < 2u;
+            nv[o] = has ? sel8(cv, oi + 2 * oj + 4 * ol) : __ldg(c0 + l * sz + jj * sy + i);
+          }
+#pragma unroll
+          for (int o = 0; o < 8; ++o) cv[o] = nv[o];
+          cx = iox; cy = ioy; cz = ioz;
+        }
+        const float c000 = cv[0], c100 = cv[1], c010 = cv[2], c110 = cv[3];
+        const float c001 = cv[4], c101 = cv[5], c011 = cv[6], c111 = cv[7];
         const float a1 = c000;
         const float a2 = __fsub_rn(c100, a1);
         const float a3 = __fsub_rn(c010, a1);

@@ -2,6 +2,7 @@
 
     python -m spider_b200.probe insert --nx 192 --nimg 64 [--reps 3] [--bf16]
     python -m spider_b200.probe pj3q --nx 128 --nang 64
+    python -m spider_b200.probe normalcg --nx 128 --nang 512 --iters 2
     python -m spider_b200.probe bpcg --n 64 --nang 512 --iters 2 [--prec fp64|mixed|fp32]
 
 Each run launches the kernel a few times on random data so that a profiler
@@ -17,7 +18,7 @@ import numpy as np
 
 def main(argv=None) -> int:
     p = argparse.ArgumentParser()
-    p.add_argument("what", choices=["insert", "pj3q", "bpcg"])
+    p.add_argument("what", choices=["insert", "pj3q", "bpcg", "normalcg"])
     p.add_argument("--nx", type=int, default=192)
     p.add_argument("--n", type=int, default=64)
     p.add_argument("--nimg", type=int, default=64)
@@ -42,6 +43,13 @@ def main(argv=None) -> int:
         vol = torch.randn(a.nx, a.nx, a.nx, device="cuda")
         for _ in range(a.reps):
             ops.pj3q(vol, synth.so3_angles(a.nang, rng), ctx=ctx)
+    elif a.what == "normalcg":
+        from . import autograd
+        plan = autograd.PJ3QPlan((a.nx, a.nx, a.nx), synth.so3_angles(a.nang, rng), ctx=ctx)
+        b = torch.randn(a.nang, a.nx, a.nx, device="cuda")
+        for _ in range(a.reps):
+            autograd.NormalCG(plan, 1e-3, a.iters, graph=False).solve(plan.adjoint(b))
+        plan.close()
     else:
         projs = rng.standard_normal((a.nang, a.n, a.n)).astype(np.float32)
         prec = {"fp64": True, "mixed": "mixed", "fp32": False}[a.prec]
