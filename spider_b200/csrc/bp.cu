@@ -50,6 +50,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // One CTA per image; images beyond `nvalid` are written as zeros.
 __global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
                                                     int nvalid, double klp, float* __restrict__ padded) {
+  // blockIdx.y splits the padded image's rows over gridDim.y CTAs (each
+  // computes the image's border mean itself) when few images fill a launch
   const int b = blockIdx.x;
   float* out = padded + (size_t)b * n * n;
   __shared__ double red[8];
@@ -78,7 +80,9 @@ __global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ im
     __syncthreads();
   }
   const double qs = valid ? qs_sh : 0.0;
-  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+  const int q0 = (int)(((long long)n * n * blockIdx.y) / gridDim.y);
+  const int q1 = (int)(((long long)n * n * (blockIdx.y + 1)) / gridDim.y);
+  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
     int x = q % n, y = q / n;
     int i = x + nx - ip;
     if (i >= n) i -= n;
@@ -1584,9 +1588,10 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
         }
         // the last piece also zero-pads the unused tail of the FFT batch
         const int blocks = last ? c->sub - (p0 - b0) : np;
+        const int parts = std::max(1, std::min(8, (4 * c->sm_count + blocks - 1) / std::max(blocks, 1)));
         int ev = c->phase_begin(0);
-        stage_kernel<<<blocks, 256, 0, c->stream>>>(src, nx, n, ip, np, klp,
-                                                    c->padded.as<float>() + (size_t)(p0 - b0) * n * n);
+        stage_kernel<<<dim3(blocks, parts), 256, 0, c->stream>>>(src, nx, n, ip, np, klp,
+                                                                 c->padded.as<float>() + (size_t)(p0 - b0) * n * n);
         SPI_TRY(check_kernel("stage_kernel"));
         c->phase_end(ev);
         c->count();
