@@ -235,11 +235,12 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
  * does.  Modes 2 and 3 keep the vectors in FP64, accumulate each projection
  * (PRJCQ_N) in fixed point in shared memory with integer atomics and hand it
  * to BCKPJ_LIN as the PROJT four-term table, made per chunk of images:
- * mode = 2 (default) with a 47-bit grid (~1e-11 of max|x|) and FP64 tables,
- * n*n*8 bytes of shared memory (n <= 160); mode = 3 with a 31-bit grid and
- * FP32 tables, n*n*4 bytes (n <= 226), faster and ~1e-7 per projection.
- * Above those sizes they use mode 1.  Scalars (DELSQ, AKDEN, P, Q) and dot
- * products are FP64 in all modes. */
+ * mode = 2 (default) with a 47-bit grid (~1e-11 of max|x|) and FP32 tables;
+ * mode = 4 the same with FP64 tables; mode = 3 with a 31-bit grid and FP32
+ * tables (fastest, ~1e-7 per projection, not for ill-conditioned problems).
+ * Images beyond one CTA's shared memory (n*n*8 bytes for modes 2/4, n*n*4
+ * for mode 3) are split into row bands, up to 8.  Scalars (DELSQ, AKDEN, P,
+ * Q) and dot products are FP64 in all modes. */
 int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
 
 /* One application of the BP CG operators on device arrays, for the

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(512) prjcq_smem_kernel(const T* __restrict__ c
 // B3 = P(I+1) - P(I), B4 = P(I+N+1) - P(I+1) - B2 (1-based, with the HIANG
 // weight LB applied to the four pixels first), so A^T reads one vector per
 // (voxel, image) instead of four scattered values.  The terms are formed in
-// FP64 and stored in FP64 (mode 2, WIDE) or rounded once to FP32 (mode 3).
+// FP64 and stored in FP64 (mode 4) or rounded once to FP32 (modes 2, 3).
 // Tables are made per chunk of images and consumed right away.
 template <bool WIDE> struct ProjtEntry;
 template <> struct ProjtEntry<false> { float4 v; };
@@ -311,18 +311,18 @@ __global__ void absmax_kernel(const T* __restrict__ x, const CgRun* __restrict__
 // grown by the half-diagonal of a unit cube, pi (sqrt 2 + sqrt 3 / 2)^2
 // (2 RI + sqrt 3) = `mcap`; each adds at most max|x| (bilinear weights
 // <= 1).  Mode 3 rounds each contribution to q = w * 0.95 * 2^31 / (mcap *
-// max|x|) in one int32 word per pixel (a step of ~1e-6 max|x|).  Mode 2
-// (WIDE) rounds to a 2^16 finer grid, q = w * 0.95 * 2^47 / (mcap * max|x|)
+// max|x|) in one int32 word per pixel (a step of ~1e-6 max|x|).  Modes 2
+// and 4 (WIDE) round to a 2^16 finer grid, q = w * 0.95 * 2^47 / (mcap * max|x|)
 // in 64 bits, and adds q >> 16 and q & 0xffff into two int32 words per
 // pixel: the high sum stays within 0.95 * 2^31 + mcap, the low one within
 // mcap * 65535, and the pixel is hi * 65536 + lo exactly (a step of ~1e-11
 // max|x|).
-template <class T, bool WIDE>
+template <class T, bool WIDE, bool WT>
 __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                           int nruns, const CgDM* __restrict__ dms,
                                                           const int* __restrict__ lb, int kbase, int n, int ldp,
                                                           const unsigned long long* __restrict__ maxabs_bits,
-                                                          float mcap, ProjtEntry<WIDE>* __restrict__ projt) {
+                                                          float mcap, ProjtEntry<WT>* __restrict__ projt) {
   extern __shared__ __align__(16) unsigned char smraw[];
   int* hi = reinterpret_cast<int*>(smraw);
   int* lo = hi + n * n;   // WIDE only
@@ -368,11 +368,11 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
   __syncthreads();
   const double inv = scale > 0.0 ? 1.0 / scale : 0.0;
   const double w = lb ? (double)lb[k] : 1.0;
-  ProjtEntry<WIDE>* out = projt + (size_t)blockIdx.x * n * n;
+  ProjtEntry<WT>* out = projt + (size_t)blockIdx.x * n * n;
   auto val = [&](int i) {
     return WIDE ? ((double)hi[i] * 65536.0 + (double)lo[i]) * inv : (double)hi[i] * inv;
   };
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) projt_make<WT>(out + i, val, i + 1, n, w);
 }
 
 // The same projector for images too large for one CTA's shared memory: C
@@ -386,11 +386,11 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
 // tables identical to those of the one-CTA kernel.  (A 2-4 CTA cluster
 // adding into one another's bands through distributed shared memory was
 // measured 3-8x slower at n = 256.)
-template <class T, bool WIDE>
+template <class T, bool WIDE, bool WT>
 __global__ void __launch_bounds__(512) prjcq_projt_band_kernel(
     const T* __restrict__ cube, const CgRun* __restrict__ runs, int nruns, const CgDM* __restrict__ dms,
     const int* __restrict__ lb, int kbase, int n, int ldp, int C, const unsigned long long* __restrict__ maxabs_bits,
-    float mcap, ProjtEntry<WIDE>* __restrict__ projt) {
+    float mcap, ProjtEntry<WT>* __restrict__ projt) {
   const int R = (n + C - 1) / C;
   const int proj = blockIdx.x / C, b = blockIdx.x % C;
   const int r0 = b * R;
@@ -451,12 +451,12 @@ __global__ void __launch_bounds__(512) prjcq_projt_band_kernel(
   __syncthreads();
   const double inv = scale > 0.0 ? 1.0 / scale : 0.0;
   const double w = lb ? (double)lb[k] : 1.0;
-  ProjtEntry<WIDE>* out = projt + (size_t)proj * n * n;
+  ProjtEntry<WT>* out = projt + (size_t)proj * n * n;
   auto val = [&](int pix) {
     const int l = pix - r0 * n;
     return WIDE ? ((double)hi[l] * 65536.0 + (double)hi[words + l]) * inv : (double)hi[l] * inv;
   };
-  for (int i = r0 * n + threadIdx.x; i < r1 * n; i += blockDim.x) projt_make<WIDE>(out + i, val, i + 1, n, w);
+  for (int i = r0 * n + threadIdx.x; i < r1 * n; i += blockDim.x) projt_make<WT>(out + i, val, i + 1, n, w);
 }
 
 // BCKPJ_LIN from PROJT tables of images [k0, k1) (table of image k at
@@ -818,11 +818,11 @@ static int launch_backproject_projt(spi_ctx* c, const CgProblem& pb, T* cube, co
 }
 
 // A then A^T (BCKE += A^T A BCKP) chunk by chunk through PROJT tables
-template <class T, bool WIDE>
+template <class T, bool WIDE, bool WT>
 static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* out, const CgDM* dms, const int* lb,
-                               int nang, ProjtEntry<WIDE>* projt, unsigned long long* maxabs) {
+                               int nang, ProjtEntry<WT>* projt, unsigned long long* maxabs) {
   const int n = pb.n;
-  const int K = projt_chunk(n, nang, sizeof(ProjtEntry<WIDE>));
+  const int K = projt_chunk(n, nang, sizeof(ProjtEntry<WT>));
   const size_t smem = (size_t)n * n * (WIDE ? 8 : 4);
   // fixed-point scale of the projector: max |x| over the sphere
   SPI_CUDA(cudaMemsetAsync(maxabs, 0, sizeof(unsigned long long), c->stream));
@@ -835,8 +835,8 @@ static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* o
   static std::atomic<unsigned long long> attr_set{0};
   const unsigned long long bit = 1ull << (c->device & 63);
   if (!(attr_set.load() & bit)) {
-    cudaFuncSetAttribute(prjcq_projt_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(prjcq_projt_band_kernel<T, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(prjcq_projt_kernel<T, WIDE, WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(prjcq_projt_band_kernel<T, WIDE, WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set.fetch_or(bit);
   }
   const int C = mixed_bands(n, WIDE);
@@ -844,14 +844,14 @@ static int launch_normal_projt(spi_ctx* c, const CgProblem& pb, const T* x, T* o
   for (int k0 = 0; k0 < nang; k0 += K) {
     const int kc = std::min(K, nang - k0);
     if (C == 1)
-      prjcq_projt_kernel<T, WIDE><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
+      prjcq_projt_kernel<T, WIDE, WT><<<kc, 512, smem, c->stream>>>(x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms,
                                                                  lb, k0, n, pb.ldp, maxabs, mcap, projt);
     else
-      prjcq_projt_band_kernel<T, WIDE><<<kc * C, 512, band_bytes(n, C, WIDE), c->stream>>>(
+      prjcq_projt_band_kernel<T, WIDE, WT><<<kc * C, 512, band_bytes(n, C, WIDE), c->stream>>>(
           x, c->cg_buf[0].as<CgRun>(), (int)pb.runs.size(), dms, lb, k0, n, pb.ldp, C, maxabs, mcap, projt);
     SPI_TRY(check_kernel("prjcq_projt_kernel"));
     c->count();
-    SPI_TRY((launch_backproject_projt<T, WIDE>(c, pb, out, projt, dms, k0, k0, k0 + kc)));
+    SPI_TRY((launch_backproject_projt<T, WT>(c, pb, out, projt, dms, k0, k0, k0 + kc)));
   }
   return 0;
 }
@@ -947,9 +947,12 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   const size_t vb = nnn * sizeof(T);
   const size_t pcount = (size_t)nang * n * n;
   // mixed mode (FP64 vectors, FP32 PROJT tables made per chunk of images)
-  const bool wide = c->cg_fp64 == 2;
-  const bool mixed = sizeof(T) == 8 && (c->cg_fp64 == 2 || c->cg_fp64 == 3) && mixed_fits(n, wide);
-  const size_t pentry = wide ? sizeof(ProjtEntry<true>) : sizeof(ProjtEntry<false>);
+  // modes 2 and 4: 47-bit fixed-point projections; mode 4 also keeps FP64
+  // PROJT tables (mode 2 FP32 tables, mode 3 31-bit and FP32 tables)
+  const bool wide = c->cg_fp64 == 2 || c->cg_fp64 == 4;
+  const bool mixed = sizeof(T) == 8 && c->cg_fp64 >= 2 && mixed_fits(n, wide);
+  const bool wtab = c->cg_fp64 == 4;
+  const size_t pentry = wtab ? sizeof(ProjtEntry<true>) : sizeof(ProjtEntry<false>);
   const int K = projt_chunk(n, nang, pentry);
   // buffers: [3] dms, [4] CB, [5] projections (T) + float staging (mixed: float images + PROJT chunk),
   // [6] BCKN|BCKP|BCKE, [7] scalars + lb
@@ -983,7 +986,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   c->count();
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
   if (mixed) {
-    if (wide)
+    if (wtab)
       SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
                                                 static_cast<ProjtEntry<true>*>(projt))));
     else
@@ -1064,12 +1067,15 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     c->count(3);
     if (mixed) {
       auto* mx = reinterpret_cast<unsigned long long*>(acc + 7);
-      if (wide)
-        SPI_TRY((launch_normal_projt<T, true>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
-                                              static_cast<ProjtEntry<true>*>(projt), mx)));
+      if (wide && wtab)
+        SPI_TRY((launch_normal_projt<T, true, true>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+                                                    static_cast<ProjtEntry<true>*>(projt), mx)));
+      else if (wide)
+        SPI_TRY((launch_normal_projt<T, true, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+                                                     static_cast<ProjtEntry<false>*>(projt), mx)));
       else
-        SPI_TRY((launch_normal_projt<T, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
-                                               static_cast<ProjtEntry<false>*>(projt), mx)));
+        SPI_TRY((launch_normal_projt<T, false, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+                                                      static_cast<ProjtEntry<false>*>(projt), mx)));
     } else {
       SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
       SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
@@ -1155,7 +1161,7 @@ extern "C" {
 
 int spi_ctx_set_cg_precision(spi_ctx* c, int mode) {
   if (!c) return fail(kInvalid, "NULL context");
-  if (mode < 0 || mode > 3) return fail(kInvalid, "spi_ctx_set_cg_precision: mode %d must be 0 .. 3", mode);
+  if (mode < 0 || mode > 4) return fail(kInvalid, "spi_ctx_set_cg_precision: mode %d must be 0 .. 4", mode);
   c->cg_fp64 = mode;
   return 0;
 }

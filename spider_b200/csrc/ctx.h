@@ -27,7 +27,7 @@ struct spi_ctx {
   int pipeline = 1;                   // 1 = host-image uploads on stream2 under the compute
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
-  int cg_fp64 = 2;                    // BP CG precision: 0 FP32, 1 FP64, 2 FP64 vectors + fixed-point/FP32 projections
+  int cg_fp64 = 2;                    // BP CG precision: 0 FP32, 1 FP64, 2-4 FP64 vectors + fixed-point projections
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT (and per insert launch)
   int sort_group = 0;                 // images per slice-ordering group (divides into sub)

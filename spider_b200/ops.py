@@ -352,15 +352,16 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     """``BP CG`` (linear interpolation).  Prompts in reference order: radius
     (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
     ``fp64``: "mixed" (default) keeps the CG vectors in FP64 and the
-    projections in 47-bit fixed point / FP64 tables, "fast" in 31-bit fixed
-    point / FP32 tables, True keeps everything in FP64, False uses the
-    reference's REAL.
+    projections in 47-bit fixed point with FP32 PROJT tables, "mixed64" the
+    same with FP64 tables, "fast" 31-bit fixed point, True keeps everything
+    in FP64, False uses the reference's REAL.
     Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
     ctx = ctx or default_context()
     if isinstance(fp64, str):
-        if fp64 not in ("mixed", "fast"):
+        modes = {"mixed": 2, "fast": 3, "mixed64": 4}
+        if fp64 not in modes:
             raise SpiderError(101, f"unknown BP CG precision {fp64!r}")
-        prec = 2 if fp64 == "mixed" else 3
+        prec = modes[fp64]
     else:
         prec = 1 if fp64 else 0
     check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))

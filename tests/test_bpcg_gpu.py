@@ -63,7 +63,7 @@ def test_cg_operator_pair_adjoint(ctx):
     assert abs(lhs - rhs) <= 1e-4 * max(abs(lhs), abs(rhs))
 
 
-@pytest.mark.parametrize("prec", ["mixed", True])
+@pytest.mark.parametrize("prec", ["mixed", "mixed64", True])
 @pytest.mark.parametrize("mode", [1, 2, 3])
 def test_bpcg_matches_fp64_oracle(ctx, orc, mode, prec):
     n, nang = 32, 120
@@ -131,7 +131,7 @@ def test_bpcg_fast_precision_matches_fp64_oracle(ctx, orc, n):
     assert e64 <= 1e-4
 
 
-@pytest.mark.parametrize("prec", ["mixed", "fast"])
+@pytest.mark.parametrize("prec", ["mixed", "mixed64", "fast"])
 def test_bpcg_band_projector_matches_single_cta(ctx, prec):
     """The projector split into 2, 4 or 8 row bands (one CTA each) sums the
     same fixed-point integers as the one-CTA kernel."""
