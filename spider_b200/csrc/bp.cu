@@ -547,7 +547,9 @@ static bool kb_window4_ok(const KBTab& kb) {
 // taps per image).  Tiles whose pixels straddle the x = 0 flip (two separate
 // clusters) or whose box would not fit use direct global atomics; reflected
 // taps (IXN < LN2, oneline.f:118-150) always do.  Every tap's voxel and weight
-// are computed exactly as in insert_kernel.
+// are computed exactly as in insert_kernel.  With FX the box holds int32
+// fixed point (scaled per tile by the largest spectrum value) and the
+// shared adds are native integer atomics instead of float ones.
 constexpr int kTileI = 16, kTileJ = 8, kTileCap = 7296;
 
 // shared-memory reduction without a returned value (no scoreboard wait)
@@ -556,7 +558,7 @@ __device__ __forceinline__ void red_shared_add(float* p, float v) {
   asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
 
-template <bool BF16>
+template <bool BF16, bool FX>
 __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restrict__ spec, const SliceDesc* __restrict__ slices,
                                                              int nslices, int nx, const float* __restrict__ tab, float fltb,
                                                              float4* __restrict__ g0, float4* __restrict__ g1) {
@@ -564,7 +566,11 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
   float* s_re = sm;
   float* s_im = sm + kTileCap;
   float* s_w = sm + 2 * kTileCap;
+  int* f_re = reinterpret_cast<int*>(s_re);   // FX: the same words as int32 fixed point
+  int* f_im = reinterpret_cast<int*>(s_im);
+  int* f_w = reinterpret_cast<int*>(s_w);
   __shared__ int s_box[8];   // xmin,ymin,zmin,-xmax,-ymax,-zmax, flipped-any, unflipped-any
+  __shared__ unsigned s_vmax; // FX: max |Re|, |Im| of the tile's spectrum values (float bits)
 
   const int N = 2 * nx, N2 = nx, LN2 = 2;
   const float fN = (float)N;
@@ -618,7 +624,9 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
     }
     // tile bounding box of the main taps
     if (t < 8) s_box[t] = (t < 6) ? 0x7fffffff : 0;
+    if (FX && t == 0) s_vmax = 0u;
     __syncthreads();
+    if (FX && ok) atomicMax(&s_vmax, __float_as_uint(fmaxf(fabsf(br), fabsf(bi))));
     if (ok && half == 0) {
       atomicMin(&s_box[0], ixn);
       atomicMin(&s_box[1], iyn);
@@ -637,8 +645,18 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
     __syncthreads();      // every thread has read the box before it is reused
     if (!any) continue;   // uniform: no valid pixel in this tile
     const int bsize = priv ? bx * by * bz : 0;
+    // FX scales: a voxel receives from at most 64 pixels of one tile (the
+    // table is zero beyond 1.8 voxels, so a voxel's support in the slice
+    // plane is at most the largest cross-section of a 3.6-voxel cube, ~22
+    // pixels), each adding a weight <= 1 times a value <= vmax
+    const float vmax = FX ? __uint_as_float(s_vmax) : 0.0f;
+    const float sc_v = (FX && vmax > 0.0f) ? 0.95f * 2147483648.0f / (64.0f * vmax) : 0.0f;
+    const float sc_w = 0.95f * 2147483648.0f / 64.0f;
     if (priv) {
-      for (int q = t; q < bsize; q += blockDim.x) { s_re[q] = 0.f; s_im[q] = 0.f; s_w[q] = 0.f; }
+      for (int q = t; q < bsize; q += blockDim.x) {
+        if (FX) { f_re[q] = 0; f_im[q] = 0; f_w[q] = 0; }
+        else { s_re[q] = 0.f; s_im[q] = 0.f; s_w[q] = 0.f; }
+      }
       __syncthreads();
     }
     if (ok) {
@@ -667,9 +685,15 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
               const float wg = __fmul_rn(tx[lx], tyz);
               if (wg != 0.0f) {
                 const int q = rowq + ixn + lx - 2;
-                red_shared_add(s_re + q, __fmul_rn(br, wg));
-                red_shared_add(s_im + q, __fmul_rn(bi, wg));
-                red_shared_add(s_w + q, wg);
+                if (FX) {
+                  atomicAdd(f_re + q, __float2int_rn(__fmul_rn(br, wg) * sc_v));
+                  atomicAdd(f_im + q, __float2int_rn(__fmul_rn(bi, wg) * sc_v));
+                  atomicAdd(f_w + q, __float2int_rn(wg * sc_w));
+                } else {
+                  red_shared_add(s_re + q, __fmul_rn(br, wg));
+                  red_shared_add(s_im + q, __fmul_rn(bi, wg));
+                  red_shared_add(s_w + q, wg);
+                }
               }
             }
           } else {
@@ -713,15 +737,25 @@ __global__ void __launch_bounds__(256, 2) insert_tile_kernel(const void* __restr
     }
     if (priv) {
       __syncthreads();
+      const float inv_v = sc_v > 0.0f ? 1.0f / sc_v : 0.0f, inv_w = 1.0f / sc_w;
       for (int q = t; q < bsize; q += blockDim.x) {
-        const float w = s_w[q];
-        if (w != 0.0f) {
+        float4 v;
+        bool any;
+        if (FX) {
+          const int qr = f_re[q], qi = f_im[q], qw = f_w[q];
+          any = (qr | qi | qw) != 0;
+          v = make_float4((float)qr * inv_v, (float)qi * inv_v, (float)qw * inv_w, 0.0f);
+        } else {
+          v = make_float4(s_re[q], s_im[q], s_w[q], 0.0f);
+          any = v.z != 0.0f;
+        }
+        if (any) {
           const int ix = q % bx;
           const int r = q / bx;
           const int iyp = by0 + r % by, izp = bz0 + r / by;
           const int iza = (izp >= 0) ? izp : N + izp;
           const int iya = (iyp >= 0) ? iyp : N + iyp;
-          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + (bx0 + ix), make_float4(s_re[q], s_im[q], w, 0.0f));
+          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + (bx0 + ix), v);
         }
       }
     }
@@ -1247,7 +1281,7 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
     const char* m = getenv("SPI_INSERT");
     const int def_mode = kb_window4_ok(c->kb) ? 3 : 2;
     c->insert_mode = !m ? def_mode : strcmp(m, "tile") == 0 ? 0 : strcmp(m, "direct") == 0 ? 1
-                   : strcmp(m, "xlane") == 0 ? 2 : def_mode;
+                   : strcmp(m, "xlane") == 0 ? 2 : strcmp(m, "tilefx") == 0 ? 4 : def_mode;
     const char* o = getenv("SPI_SLICE_ORDER");
     c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
     const char* mp = getenv("SPI_INSERT_MAP");
@@ -1355,7 +1389,7 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
   const float fltb = c->kb.fltb;
   float4* g0 = c->gptr[0];
   int ev_ins = c->phase_begin(2);
-  if (c->insert_mode >= 1) {
+  if (c->insert_mode >= 1 && c->insert_mode <= 3) {
     const size_t smem = 5000 * sizeof(float);
     const int threads = c->insert_threads;
     if (c->insert_mode == 1) {
@@ -1392,20 +1426,26 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
     }
   } else {
     const size_t smem = 3 * kTileCap * sizeof(float);
+    const bool fx = c->insert_mode == 4;
     // the attribute is per device; set once per device (several threads may race here harmlessly)
     static std::atomic<unsigned long long> attr_done{0};
     const unsigned long long bit = 1ull << (c->device & 63);
     if (!(attr_done.load() & bit)) {
-      cudaFuncSetAttribute(insert_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(insert_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(insert_tile_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(insert_tile_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(insert_tile_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(insert_tile_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       attr_done.fetch_or(bit);
     }
-    if (c->bf16)
-      insert_tile_kernel<true><<<insert_blocks(c, insert_tile_kernel<true>, 256, smem, 0), 256, smem, c->stream>>>(
-          spec, sl, nslices, nx, tab, fltb, g0, g1);
-    else
-      insert_tile_kernel<false><<<insert_blocks(c, insert_tile_kernel<false>, 256, smem, 0), 256, smem, c->stream>>>(
-          spec, sl, nslices, nx, tab, fltb, g0, g1);
+#define SPI_TILE(B, F)                                                                                    \
+  insert_tile_kernel<B, F><<<insert_blocks(c, insert_tile_kernel<B, F>, 256, smem, 0), 256, smem, c->stream>>>( \
+      spec, sl, nslices, nx, tab, fltb, g0, g1)
+    if (c->bf16) {
+      if (fx) SPI_TILE(true, true); else SPI_TILE(true, false);
+    } else {
+      if (fx) SPI_TILE(false, true); else SPI_TILE(false, false);
+    }
+#undef SPI_TILE
   }
   SPI_TRY(check_kernel("insert_kernel"));
   c->phase_end(ev_ins);

@@ -167,7 +167,7 @@ def test_insert_kernels_agree(ctx, orc):
     # include orientations that put the x = 0 flip line inside many tiles
     ang[:40, 1] = 90.0
     out, grids = {}, {}
-    for mode in ("direct", "tile", "xlane", "x4"):
+    for mode in ("direct", "tile", "xlane", "x4", "tilefx"):
         os.environ["SPI_INSERT"] = mode
         try:
             out[mode] = ops.bp3f(pr, ang, ctx=ctx)
