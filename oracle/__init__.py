@@ -75,6 +75,11 @@ def lib():
                                ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                _f32p, _f32p, _i32p, _i32p, _f64p, ctypes.c_int]
         L.orc_bpcg.restype = ctypes.c_int
+        L.orc_bpcg_fbs.argtypes = L.orc_bpcg.argtypes
+        L.orc_bpcg_fbs.restype = ctypes.c_int
+        L.orc_fbs2.argtypes = [_f32p, ctypes.c_int, _f32p, ctypes.c_int, ctypes.c_int, _f64p]
+        L.orc_fbs3.argtypes = [_f32p, ctypes.c_int, _f32p, ctypes.c_int, _f64p]
+        L.orc_prjcq_fbs3.argtypes = [_f32p, ctypes.c_int, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
         L.orc_prjcq.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
         L.orc_bckpj.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
         L.orc_hiang.argtypes = [_f32p, ctypes.c_int, _f32p, _i32p, _f32p]
@@ -268,8 +273,8 @@ def prepcub_count(nx, ny, nz, ri):
     return lib().orc_prepcub_count(nx, ny, nz, ri)
 
 
-def bpcg(projs, angles, ri, *, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, prec=0, nthreads=0):
-    """BP CG (linear): returns (vol [n,n,n], log [niter,3], nang_eff, stats[4])."""
+def bpcg(projs, angles, ri, *, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, prec=0, nthreads=0, fbs=False):
+    """BP CG (linear, or FBS with ``fbs``): returns (vol [n,n,n], log [niter,3], nang_eff, stats[4])."""
     projs = _f32(projs)
     ang = _f32(angles)
     nang, n = projs.shape[0], projs.shape[1]
@@ -278,9 +283,10 @@ def bpcg(projs, angles, ri, *, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0
     niter = ctypes.c_int(0)
     neff = ctypes.c_int(0)
     stats = np.zeros(4, np.float64)
-    rc = lib().orc_bpcg(_p(projs, _f32p), n, nang, _p(ang, _f32p), ri, errm, chim, maxit, mode, lam,
-                        prec, _p(vol, _f32p), _p(logv, _f32p), ctypes.byref(niter), ctypes.byref(neff),
-                        stats.ctypes.data_as(_f64p), nthreads)
+    fn = lib().orc_bpcg_fbs if fbs else lib().orc_bpcg
+    rc = fn(_p(projs, _f32p), n, nang, _p(ang, _f32p), ri, errm, chim, maxit, mode, lam,
+            prec, _p(vol, _f32p), _p(logv, _f32p), ctypes.byref(niter), ctypes.byref(neff),
+            stats.ctypes.data_as(_f64p), nthreads)
     if rc != 0:
         raise RuntimeError(f"oracle bpcg failed: {rc}")
     return vol, logv[: niter.value].copy(), neff.value, stats
@@ -325,3 +331,31 @@ def fixedge(p, ri, mode):
 
 def prepcub_s_count(n, ri):
     return lib().orc_prepcub_s_count(n, ri)
+
+
+def fbs2(img, xy, prec=1):
+    """FBS2_PREP + FBS2 (fbs2.f) of an n x n image at points xy [m, 2] (1-based X, Y)."""
+    img = _f32(img)
+    xy = _f32(xy)
+    out = np.zeros(xy.shape[0], np.float64)
+    lib().orc_fbs2(_p(img, _f32p), img.shape[0], _p(xy, _f32p), xy.shape[0], prec, out.ctypes.data_as(_f64p))
+    return out
+
+
+def fbs3(vol, xyz):
+    """FBS3_PREP + FBS3 (fbs3.f, FP64) of an n^3 volume at points xyz [m, 3] (1-based)."""
+    vol = _f32(vol)
+    xyz = _f32(xyz)
+    out = np.zeros(xyz.shape[0], np.float64)
+    lib().orc_fbs3(_p(vol, _f32p), vol.shape[0], _p(xyz, _f32p), xyz.shape[0], out.ctypes.data_as(_f64p))
+    return out
+
+
+def prjcq_fbs3(vol, angles, prec=1):
+    """PRJCQ_FBS3 (prjcq.f:97-167) of vol for each (psi, theta, phi): [nang, n, n]."""
+    vol = _f32(vol)
+    ang = _f32(angles)
+    n = vol.shape[0]
+    out = np.zeros((ang.shape[0], n, n), np.float32)
+    lib().orc_prjcq_fbs3(_p(vol, _f32p), n, _p(ang, _f32p), ang.shape[0], prec, _p(out, _f32p))
+    return out

@@ -1012,10 +1012,253 @@ void regularize(R* bcke, const R* p, int n, R anoise, const std::vector<RunS>& r
 // BPCG (bpcg.f:70-411) -> BPCG_2 (bpcg.f:425-814) -> HIANG -> BPCG_3_LIN
 // (bpcg.f:818-1238), linear interpolation, non-MPI.  `logv` receives
 // (iteration, err, chi2) triples.  Returns IRTFLG-style status.
+// ------------------------------------------- BP CG, FBS interpolation -----
+// SPIDER real FFTs as FMRS calls them with SPIDER_SIGN and SPIDER_SCALE
+// (fmrs.f:76-132, fftw3.f:376-450): forward = r2c with the imaginary parts
+// negated, no scale; inverse = imaginary parts negated, c2r, times 1/N.  The
+// half spectrum is [..][n/2+1] (x fastest).  c2r semantics: complex
+// transforms along the other axes, then a real transform along x that uses
+// only the real parts of the x = 0 and x = n/2 bins (what FFTW's c2r does
+// with them; the derivative spectra of FBS2_PREP / FBS3_PREP are not
+// Hermitian in those planes, so the reference's output there is whatever
+// its c2r makes of it, and both this restatement and the GPU take this form).
+void spider_fwd(const double* f, int n, int dims, std::vector<cd>& F) {
+  const int h = n / 2 + 1;
+  const long planes = dims == 3 ? n : 1;
+  F.assign((size_t)planes * n * h, cd(0, 0));
+  FFT1 fx(n, -1);
+  std::vector<cd> line(n), out(n);
+  for (long k = 0; k < planes; ++k)
+    for (int j = 0; j < n; ++j) {
+      for (int i = 0; i < n; ++i) line[i] = cd(f[((size_t)k * n + j) * n + i], 0.0);
+      fx.exec(line.data(), 1, out.data());
+      for (int i = 0; i < h; ++i) F[((size_t)k * n + j) * h + i] = out[i];
+    }
+  for (long k = 0; k < planes; ++k)   // along y
+    for (int i = 0; i < h; ++i) {
+      for (int j = 0; j < n; ++j) line[j] = F[((size_t)k * n + j) * h + i];
+      fx.exec(line.data(), 1, out.data());
+      for (int j = 0; j < n; ++j) F[((size_t)k * n + j) * h + i] = out[j];
+    }
+  if (dims == 3)
+    for (int j = 0; j < n; ++j)   // along z
+      for (int i = 0; i < h; ++i) {
+        for (int k = 0; k < n; ++k) line[k] = F[((size_t)k * n + j) * h + i];
+        fx.exec(line.data(), 1, out.data());
+        for (int k = 0; k < n; ++k) F[((size_t)k * n + j) * h + i] = out[k];
+      }
+  for (auto& v : F) v = std::conj(v);   // SPIDER sign
+}
+
+void spider_inv(std::vector<cd> G, int n, int dims, double* f) {
+  const int h = n / 2 + 1;
+  const long planes = dims == 3 ? n : 1;
+  for (auto& v : G) v = std::conj(v);   // SPIDER sign
+  FFT1 fb(n, +1);
+  std::vector<cd> line(n), out(n);
+  for (long k = 0; k < planes; ++k)
+    for (int i = 0; i < h; ++i) {
+      for (int j = 0; j < n; ++j) line[j] = G[((size_t)k * n + j) * h + i];
+      fb.exec(line.data(), 1, out.data());
+      for (int j = 0; j < n; ++j) G[((size_t)k * n + j) * h + i] = out[j];
+    }
+  if (dims == 3)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < h; ++i) {
+        for (int k = 0; k < n; ++k) line[k] = G[((size_t)k * n + j) * h + i];
+        fb.exec(line.data(), 1, out.data());
+        for (int k = 0; k < n; ++k) G[((size_t)k * n + j) * h + i] = out[k];
+      }
+  const double scale = 1.0 / (dims == 3 ? (double)n * n * n : (double)n * n);
+  for (long k = 0; k < planes; ++k)
+    for (int j = 0; j < n; ++j) {
+      const cd* g = &G[((size_t)k * n + j) * h];
+      line[0] = cd(g[0].real(), 0.0);
+      for (int i = 1; i < h; ++i) {
+        line[i] = g[i];
+        if (n - i != i) line[n - i] = std::conj(g[i]);
+      }
+      if (n % 2 == 0) line[n / 2] = cd(g[n / 2].real(), 0.0);
+      fb.exec(line.data(), 1, out.data());
+      for (int i = 0; i < n; ++i) f[((size_t)k * n + j) * n + i] = out[i].real() * scale;
+    }
+}
+
+// -i*w*v in the interleaved form of FBS2_PREP / FBS3_PREP: (re, im) -> (im w, -re w)
+static inline cd mul_mi(cd v, double w) { return cd(v.imag() * w, -v.real() * w); }
+
+// FBS2_PREP (fbs2.f:182-247): x, y and xy derivatives of an n x n image
+// through the 2D FFT.  WY(n/2) keeps the value (n/2) 2 pi / n here (FBS3_PREP
+// zeroes its Nyquist frequencies, FBS2_PREP does not).
+template <class R>
+void fbs2_prep(const R* img, int n, std::vector<R>& x1, std::vector<R>& y1, std::vector<R>& xy2) {
+  const int h = n / 2 + 1;
+  std::vector<double> f((size_t)n * n);
+  for (size_t i = 0; i < f.size(); ++i) f[i] = (double)img[i];
+  std::vector<cd> F;
+  spider_fwd(f.data(), n, 2, F);
+  const float a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / NX in REAL
+  std::vector<cd> X((size_t)n * h), Y((size_t)n * h), XY((size_t)n * h);
+  for (int j = 0; j < n; ++j) {
+    const double wy = (double)((float)(j <= n / 2 ? j : j - n) * a4);
+    for (int i = 0; i < h; ++i) {
+      const double wx = (double)((float)i * a4);
+      const size_t q = (size_t)j * h + i;
+      X[q] = mul_mi(F[q], wx);
+      Y[q] = mul_mi(F[q], wy);
+      XY[q] = mul_mi(X[q], wy);
+    }
+  }
+  std::vector<double> o((size_t)n * n);
+  auto out = [&](std::vector<cd>& G, std::vector<R>& dst) {
+    spider_inv(G, n, 2, o.data());
+    dst.resize(o.size());
+    for (size_t i = 0; i < o.size(); ++i) dst[i] = (R)o[i];
+  };
+  out(X, x1);
+  out(Y, y1);
+  out(XY, xy2);
+}
+
+// FBS3_PREP (fbs3.f:294-407): the seven derivatives of an n^3 volume.  The
+// XZ2 real part takes X1's real part (fbs3.f:371: X1(2*K+1) where the
+// pattern of the other lines has X1(2*K+2)); kept as the reference has it.
+template <class R>
+void fbs3_prep(const R* vol, int n, std::vector<R>* d /* x1 y1 z1 xy2 xz2 yz2 xyz */) {
+  const int h = n / 2 + 1;
+  std::vector<double> f((size_t)n * n * n);
+  for (size_t i = 0; i < f.size(); ++i) f[i] = (double)vol[i];
+  std::vector<cd> F;
+  spider_fwd(f.data(), n, 3, F);
+  const float a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / N in REAL
+  auto wsig = [&](int j) -> double {   // WY / WZ with the Nyquist entry zeroed
+    if (n % 2 == 0 && j == n / 2) return 0.0;
+    return (double)((float)(j <= n / 2 ? j : j - n) * a4);
+  };
+  std::vector<std::vector<cd>> D(7, std::vector<cd>(F.size()));
+  for (int l = 0; l < n; ++l)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < h; ++i) {
+        const size_t q = ((size_t)l * n + j) * h + i;
+        const double wx = (double)((float)i * a4), wy = wsig(j), wz = wsig(l);
+        const cd x1 = mul_mi(F[q], wx), y1 = mul_mi(F[q], wy), xy2 = mul_mi(x1, wy);
+        D[0][q] = x1;
+        D[1][q] = y1;
+        D[2][q] = mul_mi(F[q], wz);
+        D[3][q] = xy2;
+        D[4][q] = cd(x1.real() * wz, -x1.real() * wz);   // fbs3.f:371-372 as written
+        D[5][q] = mul_mi(y1, wz);
+        D[6][q] = mul_mi(xy2, wz);
+      }
+  std::vector<double> o((size_t)n * n * n);
+  for (int m = 0; m < 7; ++m) {
+    spider_inv(D[m], n, 3, o.data());
+    d[m].resize(o.size());
+    for (size_t i = 0; i < o.size(); ++i) d[m][i] = (R)o[i];
+  }
+}
+
+// one cubic along x (fbs2.f / fbs3.f): F(DX) from values and x derivatives at 0, 1
+template <class R>
+static inline R cub(R f0, R d0, R f1, R d1, R dx, R dx2, R dx3) {
+  R a2 = (R)3 * (f1 - f0) - (R)2 * d0 - d1;
+  R a3 = (R)2 * (-f1 + f0) + d0 + d1;
+  return f0 + d0 * dx + a2 * dx2 + a3 * dx3;
+}
+
+static inline int fmodulo(int a, int m) { int r = a % m; return r < 0 ? r + m : r; }
+
+// FBS2 (fbs2.f:94-180) with CHKBOUND: bicubic from values and derivatives,
+// indices wrapped (MODULO).  Arrays are [n][n] (x fastest), 0-based.
+template <class R>
+R fbs2(float x, float y, int n, const R* f, const R* x1, const R* y1, const R* xy2) {
+  const int i = (int)std::floor(x), j = (int)std::floor(y);
+  const R dx = (R)(x - (float)i), dy = (R)(y - (float)j);
+  const R dx2 = dx * dx, dx3 = dx * dx * dx;
+  const int i2 = fmodulo(i - 1, n), j2 = fmodulo(j - 1, n), i3 = fmodulo(i, n), j3 = fmodulo(j, n);
+  auto at = [&](const R* a, int ii, int jj) { return a[(size_t)jj * n + ii]; };
+  const R adx = cub<R>(at(f, i2, j2), at(x1, i2, j2), at(f, i3, j2), at(x1, i3, j2), dx, dx2, dx3);
+  const R bdx = cub<R>(at(f, i2, j3), at(x1, i2, j3), at(f, i3, j3), at(x1, i3, j3), dx, dx2, dx3);
+  const R dadx = cub<R>(at(y1, i2, j2), at(xy2, i2, j2), at(y1, i3, j2), at(xy2, i3, j2), dx, dx2, dx3);
+  const R dbdx = cub<R>(at(y1, i2, j3), at(xy2, i2, j3), at(y1, i3, j3), at(xy2, i3, j3), dx, dx2, dx3);
+  const R a2 = (R)3 * (bdx - adx) - (R)2 * dadx - dbdx;
+  const R a3 = (R)2 * (adx - bdx) + dadx + dbdx;
+  return adx + dadx * dy + a2 * (dy * dy) + a3 * (dy * dy * dy);
+}
+
+// FBS3 (fbs3.f:60-290): tricubic from the volume and its seven derivatives,
+// indices wrapped.  d = {x1, y1, z1, xy2, xz2, yz2, xyz}, each [n][n][n].
+template <class R>
+R fbs3(float x, float y, float z, int n, const R* f1, const std::vector<R>* d) {
+  const int i = (int)std::floor(x), j = (int)std::floor(y), l = (int)std::floor(z);
+  const int i2 = fmodulo(i - 1, n), j2 = fmodulo(j - 1, n), l2 = fmodulo(l - 1, n);
+  const int i3 = (i2 + 1) % n, j3 = (j2 + 1) % n, l3 = (l2 + 1) % n;
+  const R dx = (R)(x - (float)i), dy = (R)(y - (float)j), dz = (R)(z - (float)l);
+  const R dx2 = dx * dx, dx3 = dx * dx * dx, dy2 = dy * dy, dy3 = dy * dy * dy;
+  auto at = [&](const R* a, int ii, int jj, int ll) { return a[((size_t)ll * n + jj) * n + ii]; };
+  const R *X1 = d[0].data(), *Y1 = d[1].data(), *Z1 = d[2].data(), *XY2 = d[3].data(), *XZ2 = d[4].data(),
+          *YZ2 = d[5].data(), *XYZ = d[6].data();
+  // value and z-derivative on plane L: bicubic in (x, y) of (F, X1, Y1, XY2) and (Z1, XZ2, YZ2, XYZ)
+  auto plane = [&](const R* f, const R* fx, const R* fy, const R* fxy, int ll) {
+    const R adx = cub<R>(at(f, i2, j2, ll), at(fx, i2, j2, ll), at(f, i3, j2, ll), at(fx, i3, j2, ll), dx, dx2, dx3);
+    const R bdx = cub<R>(at(f, i2, j3, ll), at(fx, i2, j3, ll), at(f, i3, j3, ll), at(fx, i3, j3, ll), dx, dx2, dx3);
+    const R dadx = cub<R>(at(fy, i2, j2, ll), at(fxy, i2, j2, ll), at(fy, i3, j2, ll), at(fxy, i3, j2, ll), dx, dx2, dx3);
+    const R dbdx = cub<R>(at(fy, i2, j3, ll), at(fxy, i2, j3, ll), at(fy, i3, j3, ll), at(fxy, i3, j3, ll), dx, dx2, dx3);
+    const R a2 = (R)3 * (bdx - adx) - (R)2 * dadx - dbdx;
+    const R a3 = (R)2 * (adx - bdx) + dadx + dbdx;
+    return adx + dadx * dy + a2 * dy2 + a3 * dy3;
+  };
+  const R c0 = plane(f1, X1, Y1, XY2, l2), dc0 = plane(Z1, XZ2, YZ2, XYZ, l2);
+  const R c1 = plane(f1, X1, Y1, XY2, l3), dc1 = plane(Z1, XZ2, YZ2, XYZ, l3);
+  const R a2 = (R)3 * (c1 - c0) - (R)2 * dc0 - dc1;
+  const R a3 = (R)2 * (c0 - c1) + dc0 + dc1;
+  return c0 + dc0 * dz + a2 * (dz * dz) + a3 * (dz * dz * dz);
+}
+
+// PRJCQ_FBS3 (prjcq.f:97-167): every line (J, K) of the cube, sample I
+// walked with XB += DM(1), YB += DM(2), ZB += DM(3); pixel (I, J) sums over K.
+template <class R>
+void prjcq_fbs3(const R* cube, const float* dm, R* prj, int n, const std::vector<R>* d) {
+  std::fill(prj, prj + (size_t)n * n, (R)0);
+  const int h = n / 2;
+  for (int k = 1; k <= n; ++k)
+    for (int j = 1; j <= n; ++j) {
+      // -N/2*DM(1) + (J-N/2-1)*DM(4) + (K-N/2-1)*DM(7) + N/2+1, left to right in REAL
+      float xb = -((float)h * dm[0]) + (float)(j - h - 1) * dm[3] + (float)(k - h - 1) * dm[6] + (float)h + 1.0f;
+      float yb = -((float)h * dm[1]) + (float)(j - h - 1) * dm[4] + (float)(k - h - 1) * dm[7] + (float)h + 1.0f;
+      float zb = -((float)h * dm[2]) + (float)(j - h - 1) * dm[5] + (float)(k - h - 1) * dm[8] + (float)h + 1.0f;
+      for (int i = 1; i <= n; ++i) {
+        const int iox = ifix(xb), ioy = ifix(yb), ioz = ifix(zb);
+        if (iox >= 1 && iox < n && ioy >= 1 && ioy < n && ioz >= 1 && ioz < n)
+          prj[(size_t)(j - 1) * n + (i - 1)] += fbs3<R>(xb, yb, zb, n, cube, d);
+        xb = xb + dm[0];
+        yb = yb + dm[1];
+        zb = zb + dm[2];
+      }
+    }
+}
+
+// BCKPJ_FBS (bckpj.f:123-164): voxel gather along the runs, sequential XB += DM(1), YB += DM(4).
+template <class R>
+void bckpj_fbs(R* cube, const float* dm, const R* proj, const R* x1, const R* y1, const R* xy2, int n,
+               const std::vector<RunS>& runs, int ldp, int ldpnm, int nthreads) {
+  #pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (long r = 0; r < (long)runs.size(); ++r) {
+    const RunS& rn = runs[r];
+    float xb = ((float)(rn.x - ldp) * dm[0] + (float)(rn.y - ldp) * dm[1] + (float)(rn.z - ldp) * dm[2]) + (float)ldpnm;
+    float yb = ((float)(rn.x - ldp) * dm[3] + (float)(rn.y - ldp) * dm[4] + (float)(rn.z - ldp) * dm[5]) + (float)ldpnm;
+    for (int j = rn.l1; j <= rn.l2; ++j) {
+      cube[j - 1] = cube[j - 1] + fbs2<R>(xb, yb, n, proj, x1, y1, xy2);
+      xb = xb + dm[0];
+      yb = yb + dm[3];
+    }
+  }
+}
+
 template <class R>
 int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
              int maxit, int mode, float anoise, float* vol, float* logv, int* niter, int* nang_eff,
-             double* stats, int nthreads) {
+             double* stats, int nthreads, bool fbs = false) {
   const int ldp = n / 2 + 1, ldpnm = ldp;
   std::vector<RunS> runs;
   prepcub_s(n, ri, ldp, runs);
@@ -1044,8 +1287,15 @@ int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri,
       }
     }
     for (int i = 0; i < n * n; ++i) proj[i] = (R)x[i];
-    make_projt<R>(proj.data(), n, projt);
-    bckpj_lin<R>(cb.data(), &dm[9 * k], projt.data(), n, runs, ldp, ldpnm, nthreads);
+    if (fbs) {   // bpcg.f:713-731
+      std::vector<R> dx1, dy1, dxy2;
+      fbs2_prep<R>(proj.data(), n, dx1, dy1, dxy2);
+      bckpj_fbs<R>(cb.data(), &dm[9 * k], proj.data(), dx1.data(), dy1.data(), dxy2.data(), n, runs, ldp, ldpnm,
+                   nthreads);
+    } else {
+      make_projt<R>(proj.data(), n, projt);
+      bckpj_lin<R>(cb.data(), &dm[9 * k], projt.data(), n, runs, ldp, ldpnm, nthreads);
+    }
   }
   d_aba = d_aba / d_klp;
   R bnorm = 0;
@@ -1063,9 +1313,10 @@ int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri,
   int lo = hiang(ang, nang, dm, lb);
   if (nang_eff) *nang_eff = lo;
   float di = (float)(n / 2);
-  if ((mode == 1 && (ri + 1.0f + 1.0f) > di) || (mode == 2 && (ri + 2.0f + 1.0f) > di) ||
-      (mode == 3 && (ri + 3.0f + 1.0f) > di))
-    return 102;  // 'RADIUS TOO LARGE', bpcg.f:272-277
+  const float extra = fbs ? 0.0f : 1.0f;   // FBS: RI + MODE > DI (bpcg.f:269-276), linear: RI + MODE + 1
+  if ((mode == 1 && (ri + 1.0f + extra) > di) || (mode == 2 && (ri + 2.0f + extra) > di) ||
+      (mode == 3 && (ri + 3.0f + extra) > di))
+    return 102;  // 'RADIUS TOO LARGE', bpcg.f:272-290
   // BPCG_3_LIN
   std::vector<R> bckn(nnn, (R)0), bckp(nnn, (R)0), bcke(nnn, (R)0);
   R q = 0;
@@ -1081,7 +1332,23 @@ int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri,
     q = (R)-1 / delsq;
     std::fill(bcke.begin(), bcke.end(), (R)0);
     int numth = nthreads > 0 ? nthreads : 1;
-    for (int k0 = 0; k0 < lo; k0 += numth) {
+    if (fbs) {   // BPCG_3_FBS (bpcg.f:1760-1822): derivatives of BCKP, full-cube projections, FBS2 back-projection
+      std::vector<R> d3[7];
+      fbs3_prep<R>(bckp.data(), n, d3);
+      std::vector<std::vector<R>> projs_k(lo, std::vector<R>((size_t)n * n));
+      #pragma omp parallel for num_threads(numth) schedule(dynamic, 1)
+      for (int k = 0; k < lo; ++k) prjcq_fbs3<R>(bckp.data(), &dm[9 * k], projs_k[k].data(), n, d3);
+      for (int k = 0; k < lo; ++k) {
+        std::vector<R>& pj = projs_k[k];
+        if (lb[k] > 1)
+          for (auto& v : pj) v = v * (R)lb[k];
+        std::vector<R> dx1, dy1, dxy2;
+        fbs2_prep<R>(pj.data(), n, dx1, dy1, dxy2);
+        bckpj_fbs<R>(bcke.data(), &dm[9 * k], pj.data(), dx1.data(), dy1.data(), dxy2.data(), n, runs, ldp, ldpnm,
+                     nthreads);
+      }
+    }
+    for (int k0 = 0; k0 < (fbs ? 0 : lo); k0 += numth) {
       int lnum = std::min(numth, lo - k0);
       std::vector<std::vector<R>> projs_k(lnum, std::vector<R>((size_t)n * n, (R)0));
       #pragma omp parallel for num_threads(numth) schedule(static)
@@ -1263,6 +1530,60 @@ int orc_bpcg(const float* projs, int n, int nang, const float* angles, float ri,
   if (prec == 1)
     return bpcg_run<double>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff, stats, nthreads);
   return bpcg_run<float>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff, stats, nthreads);
+}
+
+// BP CG with FBS interpolation (the 'F' answer, BPCG_3_FBS)
+int orc_bpcg_fbs(const float* projs, int n, int nang, const float* angles, float ri, float errm, float chim,
+                 int maxit, int mode, float lambda, int prec, float* vol, float* logv, int* niter, int* nang_eff,
+                 double* stats, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (prec == 1)
+    return bpcg_run<double>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff,
+                            stats, nthreads, true);
+  return bpcg_run<float>(projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol, logv, niter, nang_eff,
+                         stats, nthreads, true);
+}
+
+// FBS2_PREP + FBS2 at the given points of one n x n image (prec 1: FP64)
+void orc_fbs2(const float* img, int n, const float* xy, int npts, int prec, double* out) {
+  if (prec == 1) {
+    std::vector<double> f(img, img + (size_t)n * n), a, b, c;
+    fbs2_prep<double>(f.data(), n, a, b, c);
+    for (int p = 0; p < npts; ++p) out[p] = fbs2<double>(xy[2 * p], xy[2 * p + 1], n, f.data(), a.data(), b.data(), c.data());
+  } else {
+    std::vector<float> f(img, img + (size_t)n * n), a, b, c;
+    fbs2_prep<float>(f.data(), n, a, b, c);
+    for (int p = 0; p < npts; ++p) out[p] = fbs2<float>(xy[2 * p], xy[2 * p + 1], n, f.data(), a.data(), b.data(), c.data());
+  }
+}
+
+// FBS3_PREP + FBS3 at the given points of one n^3 volume (FP64)
+void orc_fbs3(const float* vol, int n, const float* xyz, int npts, double* out) {
+  std::vector<double> f(vol, vol + (size_t)n * n * n);
+  std::vector<double> d[7];
+  fbs3_prep<double>(f.data(), n, d);
+  for (int p = 0; p < npts; ++p) out[p] = fbs3<double>(xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], n, f.data(), d);
+}
+
+// PRJCQ_FBS3 of vol for each (psi, theta, phi) (prec 1: FP64)
+void orc_prjcq_fbs3(const float* vol, int n, const float* angles, int nang, int prec, float* proj_out) {
+  std::vector<double> f(vol, vol + (size_t)n * n * n);
+  std::vector<double> d[7];
+  fbs3_prep<double>(f.data(), n, d);
+  std::vector<float> ff(vol, vol + (size_t)n * n * n);
+  std::vector<float> d32[7];
+  if (prec != 1) fbs3_prep<float>(ff.data(), n, d32);
+  for (int k = 0; k < nang; ++k) {
+    float dm[9];
+    cang(angles[3 * k + 2], angles[3 * k + 1], angles[3 * k + 0], dm);
+    if (prec == 1) {
+      std::vector<double> p((size_t)n * n);
+      prjcq_fbs3<double>(f.data(), dm, p.data(), n, d);
+      for (size_t i = 0; i < p.size(); ++i) proj_out[(size_t)k * n * n + i] = (float)p[i];
+    } else {
+      prjcq_fbs3<float>(ff.data(), dm, proj_out + (size_t)k * n * n, n, d32);
+    }
+  }
 }
 
 // Single operator applications, for adjointness and parity tests.
