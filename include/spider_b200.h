@@ -243,6 +243,18 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
  * Q) and dot products are FP64 in all modes. */
 int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
 
+/* Interpolation of BP CG's operators, the 'L' / 'F' answer of BP CG
+ * (bpcg.f:177-180): fbs = 0 (default) PRJCQ_N / BCKPJ_LIN, linear;
+ * fbs = 1 BPCG_3_FBS (bpcg.f:1760-1822): the projector PRJCQ_FBS3
+ * (prjcq.f:97-167) samples the tricubic FBS3 interpolant of the direction
+ * along every line of the full cube, the back-projector BCKPJ_FBS
+ * (bckpj.f:123-164) the bicubic FBS2 interpolant of each projection; both
+ * interpolants come from FFT derivatives (FBS2_PREP fbs2.f:182-247,
+ * FBS3_PREP fbs3.f:294-407), computed in FP64.  With FBS the radius limit is
+ * RI + MODE <= N/2 (linear: RI + MODE + 1), N is limited to 512, precision
+ * mode 0 keeps FP32 vectors and every other mode FP64. */
+int spi_ctx_set_cg_interpolation(spi_ctx* ctx, int fbs);
+
 /* One application of the BP CG operators on device arrays, for the
  * differentiable wrapper and adjointness checks.  spi_cg_project: PRJCQ_N
  * (prjcq.f:48-82) of vol into projs (overwritten).  spi_cg_backproject:

@@ -16,6 +16,7 @@
 // CG scalars (DELSQ, AKDEN, P, Q) are FP64 device scalars; the vectors and
 // projections are FP64 by default and FP32 (the reference's REAL) on request.
 // One CG iteration is a fixed kernel sequence captured once as a CUDA graph.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -90,6 +91,8 @@ __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+
+#include "bpcg_fbs.cuh"
 
 // ---------------------------------------------------------------------------
 // ASTASQ (bpcg.f:1244-1274): FP64 sums per image; counts are host constants.
@@ -680,6 +683,7 @@ __global__ void widen_kernel(const float* __restrict__ in, T* __restrict__ out, 
 
 void cg_release(spi_ctx* c) {
   for (auto& b : c->cg_buf) b.release();
+  for (auto& b : c->cg_fbs) b.release();
 }
 
 // Device-side problem description shared by the entry points
@@ -885,7 +889,9 @@ static void dms_from_angles(const float* angles, int nang, std::vector<CgDM>& ou
 // HIANG (hiang.f:40-112).  ang[3*i] = phi, [3*i+1] = theta, [3*i+2] = psi.
 // Duplicates (after the fold and the 0.01 degree truncation of phi) merge into
 // their first occurrence, exactly as the reference's pairwise scan does.
-static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std::vector<int>& lb) {
+// dm9 (FBS only) receives all nine DM entries per merged angle.
+static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std::vector<int>& lb,
+                 std::vector<float>* dm9 = nullptr) {
   for (int i = 0; i < nang; ++i) {
     if (ang[3 * i + 1] >= 90.0f) {
       ang[3 * i + 1] = 180.0f - ang[3 * i + 1];
@@ -933,8 +939,172 @@ static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std:
     d[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
     d[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
     d[5] = (float)(sthe * spsi);
+    if (dm9) {
+      if (o == 0) dm9->assign((size_t)9 * lo, 0.0f);
+      float* e = dm9->data() + (size_t)9 * o;
+      memcpy(e, d, 6 * sizeof(float));
+      e[6] = (float)(sthe * cphi);
+      e[7] = (float)(sthe * sphi);
+      e[8] = (float)(cthe);
+    }
   }
   return lo;
+}
+
+// ---------------------------------------------------------------------------
+// FBS operators: cuFFT plans and scratch for one BP CG solve.  Projections are
+// processed in chunks of K (the 2D plans' batch).
+struct FbsState {
+  int n = 0, K = 0;
+  float a4 = 0.0f;
+  cufftHandle p3f = 0, p3i = 0, p2f = 0, p2i = 0;
+  double* dbl3 = nullptr;   // [n^3] FFT input
+  double2* F3 = nullptr;    // [n][n][h] forward spectrum
+  double2* W3 = nullptr;    // [7][n][n][h] derivative spectra
+  double* D3 = nullptr;     // [7][n^3] derivatives
+  void* V = nullptr;        // T [n^3][8] interleaved FBS3 table
+  double* dbl2 = nullptr;   // [K][n][n]
+  double2* F2 = nullptr;    // [K][n][h]
+  double2* W2 = nullptr;    // [3][K][n][h]
+  double* D2 = nullptr;     // [3][K][n][n]
+  void* P2 = nullptr;       // T [K][n*n][4] interleaved FBS2 tables
+  void* pt = nullptr;       // T [K][n][n] projections of the iteration
+  int2* segs = nullptr;     // {run, first offset} per BCKPJ_FBS segment
+  long long nseg = 0;
+  float* dm9 = nullptr;     // 9 floats per merged angle
+  FbsState() = default;
+  FbsState(const FbsState&) = delete;
+  FbsState& operator=(const FbsState&) = delete;
+  ~FbsState() {
+    if (p3f) cufftDestroy(p3f);
+    if (p3i) cufftDestroy(p3i);
+    if (p2f) cufftDestroy(p2f);
+    if (p2i) cufftDestroy(p2i);
+  }
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+template <class T>
+static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
+  const int n = pb.n, h = n / 2 + 1;
+  const size_t nn = (size_t)n * n, nnn = nn * n, s3 = nn * h, s2 = (size_t)n * h;
+  fs.n = n;
+  fs.a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / N in REAL
+  // chunk: about 1 GiB of 2D scratch, at most 16384 projections
+  const size_t per_img = nn * 8 + s2 * 16 * 4 + nn * 8 * 3 + nn * 4 * sizeof(T) + nn * sizeof(T);
+  fs.K = (int)std::max<size_t>(1, std::min<size_t>({(size_t)nang, (size_t)16384, (size_t(1) << 30) / per_img}));
+  if (const char* e = getenv("SPI_FBS_CHUNK")) {   // smaller chunks (tests of the chunk loop)
+    const int k = atoi(e);
+    if (k > 0 && k < fs.K) fs.K = k;
+  }
+  const size_t K = (size_t)fs.K;
+  std::vector<int2> segs;
+  for (size_t r = 0; r < pb.runs.size(); ++r) {
+    const int len = pb.runs[r].l2 - pb.runs[r].l1 + 1;
+    for (int o = 0; o < len; o += kFbsSeg) segs.push_back(make_int2((int)r, o));
+  }
+  fs.nseg = (long long)segs.size();
+  const size_t b3[5] = {align256(nnn * 8), align256(s3 * 16), align256(7 * s3 * 16), align256(7 * nnn * 8),
+                        align256(nnn * 8 * sizeof(T))};
+  const size_t b2[6] = {align256(K * nn * 8), align256(K * s2 * 16), align256(3 * K * s2 * 16),
+                        align256(3 * K * nn * 8), align256(K * nn * 4 * sizeof(T)), align256(K * nn * sizeof(T))};
+  size_t t3 = 0, t2 = 0;
+  for (size_t b : b3) t3 += b;
+  for (size_t b : b2) t2 += b;
+  SPI_TRY(c->cg_fbs[0].ensure(t3));
+  SPI_TRY(c->cg_fbs[1].ensure(t2));
+  SPI_TRY(c->cg_fbs[2].ensure(std::max<size_t>(1, segs.size()) * sizeof(int2)));
+  SPI_TRY(c->cg_fbs[3].ensure((size_t)9 * std::max(nang, 1) * sizeof(float)));
+  char* p = c->cg_fbs[0].as<char>();
+  fs.dbl3 = reinterpret_cast<double*>(p); p += b3[0];
+  fs.F3 = reinterpret_cast<double2*>(p); p += b3[1];
+  fs.W3 = reinterpret_cast<double2*>(p); p += b3[2];
+  fs.D3 = reinterpret_cast<double*>(p); p += b3[3];
+  fs.V = p;
+  p = c->cg_fbs[1].as<char>();
+  fs.dbl2 = reinterpret_cast<double*>(p); p += b2[0];
+  fs.F2 = reinterpret_cast<double2*>(p); p += b2[1];
+  fs.W2 = reinterpret_cast<double2*>(p); p += b2[2];
+  fs.D2 = reinterpret_cast<double*>(p); p += b2[3];
+  fs.P2 = p; p += b2[4];
+  fs.pt = p;
+  fs.segs = c->cg_fbs[2].as<int2>();
+  fs.dm9 = c->cg_fbs[3].as<float>();
+  if (!segs.empty())
+    SPI_CUDA(cudaMemcpyAsync(fs.segs, segs.data(), segs.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  int d3[3] = {n, n, n}, d2[2] = {n, n};
+  SPI_CUFFT(cufftPlan3d(&fs.p3f, n, n, n, CUFFT_D2Z));
+  SPI_CUFFT(cufftPlanMany(&fs.p3i, 3, d3, nullptr, 1, (int)s3, nullptr, 1, (int)nnn, CUFFT_Z2D, 7));
+  SPI_CUFFT(cufftPlanMany(&fs.p2f, 2, d2, nullptr, 1, (int)nn, nullptr, 1, (int)s2, CUFFT_D2Z, fs.K));
+  SPI_CUFFT(cufftPlanMany(&fs.p2i, 2, d2, nullptr, 1, (int)s2, nullptr, 1, (int)nn, CUFFT_Z2D, 3 * fs.K));
+  for (cufftHandle hnd : {fs.p3f, fs.p3i, fs.p2f, fs.p2i}) SPI_CUFFT(cufftSetStream(hnd, c->stream));
+  return 0;
+}
+
+// FBS2_PREP of kc images src[kc][n][n] (S = float images or T projections) into P2
+template <class S, class T>
+static int fbs2_prepare(spi_ctx* c, FbsState& fs, const S* src, int kc, T* P2) {
+  const int n = fs.n;
+  const size_t nn = (size_t)n * n, count = (size_t)kc * nn, padded = (size_t)fs.K * nn;
+  fbs_to_double_kernel<S, T><<<blocks_for(c, (long long)padded, 256), 256, 0, c->stream>>>(src, fs.dbl2, count, padded);
+  SPI_TRY(check_kernel("fbs_to_double_kernel"));
+  SPI_CUFFT(cufftExecD2Z(fs.p2f, fs.dbl2, reinterpret_cast<cufftDoubleComplex*>(fs.F2)));
+  const size_t spec = (size_t)fs.K * n * (n / 2 + 1);
+  fbs2_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(fs.F2, fs.W2, n, fs.K, fs.a4,
+                                                                              1.0 / ((double)n * n));
+  SPI_TRY(check_kernel("fbs2_spec_kernel"));
+  SPI_CUFFT(cufftExecZ2D(fs.p2i, reinterpret_cast<cufftDoubleComplex*>(fs.W2), fs.D2));
+  fbs2_pack_kernel<S, T><<<blocks_for(c, (long long)count, 256), 256, 0, c->stream>>>(src, fs.D2, P2, count, padded);
+  SPI_TRY(check_kernel("fbs2_pack_kernel"));
+  c->count(3);
+  return 0;
+}
+
+// FBS3_PREP of the cube into the interleaved table fs.V
+template <class T>
+static int fbs3_prepare(spi_ctx* c, FbsState& fs, const T* cube) {
+  const int n = fs.n;
+  const size_t nnn = (size_t)n * n * n;
+  fbs_to_double_kernel<T, T><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.dbl3, nnn, nnn);
+  SPI_TRY(check_kernel("fbs_to_double_kernel"));
+  SPI_CUFFT(cufftExecD2Z(fs.p3f, fs.dbl3, reinterpret_cast<cufftDoubleComplex*>(fs.F3)));
+  const size_t spec = (size_t)n * n * (n / 2 + 1);
+  fbs3_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(fs.F3, fs.W3, n, fs.a4,
+                                                                              1.0 / ((double)n * n * n));
+  SPI_TRY(check_kernel("fbs3_spec_kernel"));
+  SPI_CUFFT(cufftExecZ2D(fs.p3i, reinterpret_cast<cufftDoubleComplex*>(fs.W3), fs.D3));
+  fbs3_pack_kernel<T><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.D3, static_cast<T*>(fs.V), nnn);
+  SPI_TRY(check_kernel("fbs3_pack_kernel"));
+  c->count(3);
+  return 0;
+}
+
+// PRJCQ_FBS3 of fs.V for merged angles [k0, k0 + kc) into fs.pt, scaled by LB
+template <class T>
+static int fbs_project(spi_ctx* c, FbsState& fs, const int* dlb, int k0, int kc) {
+  const int n = fs.n;
+  const int threads = (n + 31) / 32 * 32;
+  const size_t smem = (size_t)threads * (kFbsIC + 1) * sizeof(T);
+  if (smem > 48 * 1024)
+    SPI_CUDA(cudaFuncSetAttribute(prjcq_fbs3_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  prjcq_fbs3_kernel<T><<<dim3(n, kc), threads, smem, c->stream>>>(static_cast<const T*>(fs.V), fs.dm9, dlb, k0, n,
+                                                                  static_cast<T*>(fs.pt));
+  SPI_TRY(check_kernel("prjcq_fbs3_kernel"));
+  c->count();
+  return 0;
+}
+
+// BCKPJ_FBS of kc prepared tables P2 (angles dms[0..kc)) summed into cube
+template <class T>
+static int fbs_backproject(spi_ctx* c, const CgProblem& pb, FbsState& fs, T* cube, const T* P2, const CgDM* dms,
+                           int kc) {
+  if (fs.nseg == 0 || kc <= 0) return 0;
+  bckpj_fbs_kernel<T><<<blocks_for(c, fs.nseg, 256), 256, 0, c->stream>>>(
+      cube, c->cg_buf[0].as<CgRun>(), fs.segs, fs.nseg, P2, dms, kc, pb.n, pb.ldp);
+  SPI_TRY(check_kernel("bckpj_fbs_kernel"));
+  c->count();
+  return 0;
 }
 
 // BPCG_2 + HIANG + BPCG_3_LIN with vectors and projections stored as T
@@ -949,8 +1119,11 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   // mixed mode (FP64 vectors, FP32 PROJT tables made per chunk of images)
   // modes 2 and 4: 47-bit fixed-point projections; mode 4 also keeps FP64
   // PROJT tables (mode 2 FP32 tables, mode 3 31-bit and FP32 tables)
+  // FBS interpolation keeps T for the vectors and projections (FP64 in modes 1-4)
+  const bool fbs = c->cg_interp == 1;
+  if (fbs && n > 512) return fail(kInvalid, "BP CG FBS: n = %d above 512", n);
   const bool wide = c->cg_fp64 == 2 || c->cg_fp64 == 4;
-  const bool mixed = sizeof(T) == 8 && c->cg_fp64 >= 2 && mixed_fits(n, wide);
+  const bool mixed = !fbs && sizeof(T) == 8 && c->cg_fp64 >= 2 && mixed_fits(n, wide);
   const bool wtab = c->cg_fp64 == 4;
   const size_t pentry = wtab ? sizeof(ProjtEntry<true>) : sizeof(ProjtEntry<false>);
   const int K = projt_chunk(n, nang, pentry);
@@ -960,7 +1133,9 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   dms_from_angles(angles, nang, dms);
   SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
   SPI_TRY(c->cg_buf[4].ensure(vb));
-  if (mixed)
+  if (fbs)
+    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float)));
+  else if (mixed)
     SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float) + (size_t)K * n * n * pentry + 32));
   else
     SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
@@ -968,7 +1143,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   SPI_TRY(c->cg_buf[7].ensure(sizeof(CgScal) + 64 + (size_t)nang * sizeof(int)));
   T* cb = c->cg_buf[4].as<T>();
   T* pj = c->cg_buf[5].as<T>();
-  float* pj32 = mixed ? c->cg_buf[5].as<float>()
+  float* pj32 = (mixed || fbs) ? c->cg_buf[5].as<float>()
                       : (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
   void* projt = mixed ? (void*)(c->cg_buf[5].as<char>() + ((pcount * sizeof(float) + 31) & ~size_t(31))) : nullptr;
   T* bckn = c->cg_buf[6].as<T>();
@@ -985,7 +1160,15 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   SPI_TRY(check_kernel("astasq_kernel"));
   c->count();
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
-  if (mixed) {
+  FbsState fs;
+  if (fbs) {   // bpcg.f:713-731: FBS2_PREP and BCKPJ_FBS of every image, in order
+    SPI_TRY(fbs_setup<T>(c, pb, nang, fs));
+    for (int k0 = 0; k0 < nang; k0 += fs.K) {
+      const int kc = std::min(fs.K, nang - k0);
+      SPI_TRY((fbs2_prepare<float, T>(c, fs, pj32 + (size_t)k0 * n * n, kc, static_cast<T*>(fs.P2))));
+      SPI_TRY(fbs_backproject<T>(c, pb, fs, cb, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
+    }
+  } else if (mixed) {
     if (wtab)
       SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
                                                 static_cast<ProjtEntry<true>*>(projt))));
@@ -1036,11 +1219,16 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     ang[3 * k + 2] = angles[3 * k];
   }
   std::vector<int> lb;
-  const int lo = hiang(ang, nang, dms, lb);
+  std::vector<float> dm9;
+  const int lo = hiang(ang, nang, dms, lb, fbs ? &dm9 : nullptr);
   const float di = (float)(n / 2);
-  if ((mode == 1 && (ri + 1.0f + 1.0f) > di) || (mode == 2 && (ri + 2.0f + 1.0f) > di) ||
-      (mode == 3 && (ri + 3.0f + 1.0f) > di))
+  // bpcg.f:269-290: FBS needs RI + MODE <= N/2, linear RI + MODE + 1 <= N/2
+  const float extra = fbs ? 0.0f : 1.0f;
+  if ((mode == 1 && (ri + 1.0f + extra) > di) || (mode == 2 && (ri + 2.0f + extra) > di) ||
+      (mode == 3 && (ri + 3.0f + extra) > di))
     return fail(kMissing, "RADIUS TOO LARGE (%d)", (int)ri);
+  if (fbs)
+    SPI_CUDA(cudaMemcpyAsync(fs.dm9, dm9.data(), dm9.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), (size_t)lo * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(dlb, lb.data(), (size_t)lo * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   // ---- BPCG_3_LIN
@@ -1065,7 +1253,15 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
-    if (mixed) {
+    if (fbs) {   // BPCG_3_FBS (bpcg.f:1760-1822)
+      SPI_TRY(fbs3_prepare<T>(c, fs, bckp));
+      for (int k0 = 0; k0 < lo; k0 += fs.K) {
+        const int kc = std::min(fs.K, lo - k0);
+        SPI_TRY(fbs_project<T>(c, fs, dlb, k0, kc));
+        SPI_TRY((fbs2_prepare<T, T>(c, fs, static_cast<const T*>(fs.pt), kc, static_cast<T*>(fs.P2))));
+        SPI_TRY(fbs_backproject<T>(c, pb, fs, bcke, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
+      }
+    } else if (mixed) {
       auto* mx = reinterpret_cast<unsigned long long*>(acc + 7);
       if (wide && wtab)
         SPI_TRY((launch_normal_projt<T, true, true>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
@@ -1095,7 +1291,8 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   // capture one iteration as a CUDA graph, then replay it
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  bool use_graph = getenv("SPI_CG_NOGRAPH") == nullptr;
+  // the FBS iteration runs cuFFT plans and is launched directly
+  bool use_graph = !fbs && getenv("SPI_CG_NOGRAPH") == nullptr;
   if (use_graph && cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     use_graph = false;
     cudaGetLastError();
@@ -1158,6 +1355,13 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
 using namespace spi;
 
 extern "C" {
+
+int spi_ctx_set_cg_interpolation(spi_ctx* c, int fbs) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (fbs != 0 && fbs != 1) return fail(kInvalid, "spi_ctx_set_cg_interpolation: %d must be 0 (linear) or 1 (FBS)", fbs);
+  c->cg_interp = fbs;
+  return 0;
+}
 
 int spi_ctx_set_cg_precision(spi_ctx* c, int mode) {
   if (!c) return fail(kInvalid, "NULL context");

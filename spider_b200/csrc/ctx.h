@@ -28,6 +28,7 @@ struct spi_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
   int cg_fp64 = 2;                    // BP CG precision: 0 FP32, 1 FP64, 2-4 FP64 vectors + fixed-point projections
+  int cg_interp = 0;                  // BP CG interpolation: 0 linear, 1 FBS
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT (and per insert launch)
   int sort_group = 0;                 // images per slice-ordering group (divides into sub)
@@ -61,6 +62,7 @@ struct spi_ctx {
   // ---- PJ 3Q / BP CG scratch ----
   spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
   spi::DevBuf cg_buf[8];
+  spi::DevBuf cg_fbs[4];              // FBS: 3D scratch + table, 2D chunk scratch, segments, DM(1..9)
   spi::HostBuf hbuf;
 
   // per-phase event timing

@@ -176,20 +176,20 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
         print(f"  NUMBER OF IMAGES:{len(numbers):8d}", file=results)
         ri = float(a[2]) if a[2].strip() else float(n // 2 - 2)
         ang = _angles(_name(a[3], ext), numbers)
-        if a[4].strip().upper().startswith("F"):
-            raise ops.SpiderError(101, "BP CG FBS interpolation is not built; use L")
+        fbs = a[4].strip().upper().startswith("F")   # FBS_WANTED = (ANSW(1:1) == 'F'), bpcg.f:177-180
+        interp = "fbs" if fbs else "linear"
         k = 6 if op == "BP CG" else 8   # index of the 'error limit, chi^2 limit' answer
         errm, chim = (float(v) for v in a[k].replace(",", " ").split()[:2])
         maxit, mode = (int(float(v)) for v in a[k + 1].replace(",", " ").split()[:2])
         lam = float(a[k + 2])
 
         def _log(lg):
-            print("  USING LINEAR INTERPOLATION", file=results)
+            print("  USING FBS INTERPOLATION" if fbs else "  USING LINEAR INTERPOLATION", file=results)
             for it, err, chi in lg:   # bpcg.f:1213-1216
                 print(f"  ITERATION: {int(it):3d}  DIFFERENCE:{err:12.4E}  CHISQ:{chi:12.4E}", file=results)
 
         if op == "BP CG":
-            vol, log = ops.bpcg(imgs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx)
+            vol, log = ops.bpcg(imgs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx, interp=interp)
             _log(log)
             sio.write_image(_name(a[5], ext), vol)
             return {"vol": vol, "log": log}
@@ -206,7 +206,7 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
             half[: len(lists[0])] = 1
             imgs = imgs[[pos[k2] for k2 in sel]]
             ang = ang[[pos[k2] for k2 in sel]]
-        vol, v1, v2, logs = ops.bpcg3(imgs, ang, half, ri, errm, chim, maxit, mode, lam, ctx=ctx)
+        vol, v1, v2, logs = ops.bpcg3(imgs, ang, half, ri, errm, chim, maxit, mode, lam, ctx=ctx, interp=interp)
         for lg in logs:
             _log(lg)
         sio.write_image(_name(a[5], ext), vol)

@@ -348,9 +348,12 @@ def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
 
 
 def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-         ctx: Context | None = None, fp64="mixed"):
-    """``BP CG`` (linear interpolation).  Prompts in reference order: radius
-    (default n/2-2), error & chi^2 limits, iteration limit & mode, lambda.
+         ctx: Context | None = None, fp64="mixed", interp="linear"):
+    """``BP CG``.  Prompts in reference order: radius (default n/2-2),
+    error & chi^2 limits, iteration limit & mode, lambda.
+    ``interp``: "linear" (the 'L' answer) or "fbs" (the 'F' answer: FBS
+    interpolation through FFT derivatives, BPCG_3_FBS); with "fbs",
+    ``fp64=False`` keeps FP32 vectors and every other setting FP64.
     ``fp64``: "mixed" (default) keeps the CG vectors in FP64 and the
     projections in 47-bit fixed point with FP32 PROJT tables, "mixed64" the
     same with FP64 tables, "fast" 31-bit fixed point, True keeps everything
@@ -365,6 +368,10 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     else:
         prec = 1 if fp64 else 0
     check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))
+    interps = {"linear": 0, "l": 0, "fbs": 1, "f": 1}
+    if str(interp).lower() not in interps:
+        raise SpiderError(101, f"unknown BP CG interpolation {interp!r}")
+    check(ctx._L.spi_ctx_set_cg_interpolation(ctx.handle, interps[str(interp).lower()]))
     projs = _host_f32(projs)
     n = _nx_of(projs)
     if ri is None:
@@ -380,7 +387,7 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
 
 
 def bpcg3(projs, angles, half_mask, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
-          ctx: Context | None = None, fp64="mixed"):
+          ctx: Context | None = None, fp64="mixed", interp="linear"):
     """``BP CG 3``: the overall solution and one for each of two sample sets,
     as three independent CG solves (bpcg.f:139-160,300-400).  ``half_mask[i]``
     = 1 puts image i in the first sample (the reference draws the two lists
@@ -391,9 +398,9 @@ def bpcg3(projs, angles, half_mask, ri=None, errm=5e-5, chim=0.0, maxit=20, mode
     m = np.asarray(half_mask).astype(bool).reshape(-1)
     if m.shape[0] != projs.shape[0]:
         raise SpiderError(101, "half mask length differs from the number of images")
-    v, lg = bpcg(projs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
-    v1, lg1 = bpcg(projs[m], ang[m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
-    v2, lg2 = bpcg(projs[~m], ang[~m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64)
+    v, lg = bpcg(projs, ang, ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64, interp=interp)
+    v1, lg1 = bpcg(projs[m], ang[m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64, interp=interp)
+    v2, lg2 = bpcg(projs[~m], ang[~m], ri, errm, chim, maxit, mode, lam, ctx=ctx, fp64=fp64, interp=interp)
     return v, v1, v2, (lg, lg1, lg2)
 
 

@@ -4,6 +4,7 @@
     python -m spider_b200.probe pj3q --nx 128 --nang 64
     python -m spider_b200.probe normalcg --nx 128 --nang 512 --iters 2
     python -m spider_b200.probe bpcg --n 64 --nang 512 --iters 2 [--prec fp64|mixed|mixed64|fast|fp32]
+                                 [--interp linear|fbs]
 
 Each run launches the kernel a few times on random data so that a profiler
 can skip the first launch (`-s 1`) and capture one steady-state launch.
@@ -27,6 +28,7 @@ def main(argv=None) -> int:
     p.add_argument("--iters", type=int, default=2)
     p.add_argument("--bf16", action="store_true")
     p.add_argument("--prec", choices=["fp64", "mixed", "mixed64", "fast", "fp32"], default="fp64")
+    p.add_argument("--interp", choices=["linear", "fbs"], default="linear")
     a = p.parse_args(argv)
     import torch
 
@@ -54,7 +56,7 @@ def main(argv=None) -> int:
         projs = rng.standard_normal((a.nang, a.n, a.n)).astype(np.float32)
         prec = {"fp64": True, "fp32": False}.get(a.prec, a.prec)
         ops.bpcg(projs, synth.so3_angles(a.nang, rng), a.n / 2 - 3, errm=0.0, maxit=a.iters, mode=1,
-                 lam=1e-3, ctx=ctx, fp64=prec)
+                 lam=1e-3, ctx=ctx, fp64=prec, interp=a.interp)
     torch.cuda.synchronize()
     print(f"ok {a.what}: {ctx.launches} kernel launches")
     ctx.close()

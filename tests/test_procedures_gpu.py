@@ -76,6 +76,23 @@ def test_testbpcg_procedure(ctx, orc, tmp_path):
     print(f"  BP CG    Range: {vol.min():12.5E}...{vol.max():12.5E}")
 
 
+def test_bpcg_fbs_procedure(ctx, orc, tmp_path):
+    """testbpcg.tst with the 'F' answer: FBS interpolation (BPCG_3_FBS)."""
+    img = _setup(tmp_path)
+    out = io.StringIO()
+    t = str(tmp_path)
+    operations.run("BP CG", [f"{t}/jnk***", "1-12", "35", f"{t}/savangbprp", "F", f"{t}/jnkbpcg_fbs",
+                             "1.0E5, 0.0", "25,1", "2000"], ctx=ctx, results=out)
+    vol, _ = sio.read_image(tmp_path / "jnkbpcg_fbs.spi")
+    ref, rlog, _, _ = orc.bpcg(np.stack([img] * 12), ANGLES, 35.0, errm=1.0e5, chim=0.0, maxit=25, mode=1,
+                               lam=2000.0, prec=1, fbs=True)
+    assert synth.rel_l2(vol, ref) <= 1e-4
+    assert "USING FBS INTERPOLATION" in out.getvalue()
+    lines = [ln for ln in out.getvalue().splitlines() if "ITERATION" in ln]
+    assert len(lines) == len(rlog)
+    print(f"  BP CG F  Range: {vol.min():12.5E}...{vol.max():12.5E}")
+
+
 def test_pj3q_and_partial_merge_procedures(ctx, orc, tmp_path):
     t = str(tmp_path)
     rng = np.random.default_rng(5)
