@@ -255,6 +255,14 @@ int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
  * mode 0 keeps FP32 vectors and every other mode FP64. */
 int spi_ctx_set_cg_interpolation(spi_ctx* ctx, int fbs);
 
+/* In-plane rotation of spi_bp_insert_rb (RB 3F / RB 32F), SPIDER's FBS mode
+ * (`MD` with `FBS ON`, setmode.f:399-409, read by bp3f.f:412-424):
+ * fbs = 0 (default) RTSQ (rtsq.f:56-140, quadratic QUADRI); fbs = 1 RTSF
+ * (rtsf.f:109-205, SCLI = 1): FBS2_PREP of each image (FFT derivatives,
+ * FP64 transforms) and bicubic FBS2 with wrapped indices at every rotated
+ * and shifted source position. */
+int spi_ctx_set_rb_interpolation(spi_ctx* ctx, int fbs);
+
 /* One application of the BP CG operators on device arrays, for the
  * differentiable wrapper and adjointness checks.  spi_cg_project: PRJCQ_N
  * (prjcq.f:48-82) of vol into projs (overwritten).  spi_cg_backproject:

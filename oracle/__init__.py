@@ -55,9 +55,11 @@ def lib():
                                _f64p, _f64p, ctypes.c_int]
         L.orc_bp3f.restype = ctypes.c_int
         L.orc_rb3f.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _u8p, ctypes.c_int,
-                               _f32p, _f32p, _f32p, ctypes.c_int]
+                               _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int]
         L.orc_rb3f.restype = ctypes.c_int
         L.orc_symvol.argtypes = [_f32p, _f32p, ctypes.c_int, _f32p, ctypes.c_int]
+        L.orc_rtsf.argtypes = [_f32p, _f32p, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        L.orc_rtsf.restype = None
         L.orc_rtsq.argtypes = [_f32p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                ctypes.c_float]
         L.orc_bp_insert_only.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _f32p, _u8p, ctypes.c_int]
@@ -206,9 +208,17 @@ def rtsq(img, theta, shx, shy):
     return out
 
 
-def rb3f(imgs, angles, inplane, half=None, *, prec=0, nthreads=0):
-    """RB 3F / RB 32F: RTSQ with inplane [n, 3] = (angle, sx, sy), then BP 3F (half None)
-    or BP 32F (returns three volumes)."""
+def rtsf(img, theta, shx, shy):
+    """RTSF (rtsf.f:109-205, SCLI = 1) of one square image: FBS rotate and shift."""
+    img = _f32(img)
+    out = np.zeros_like(img)
+    lib().orc_rtsf(_p(img, _f32p), _p(out, _f32p), img.shape[1], theta, shx, shy)
+    return out
+
+
+def rb3f(imgs, angles, inplane, half=None, *, prec=0, nthreads=0, fbs=False):
+    """RB 3F / RB 32F: RTSQ (RTSF with ``fbs``, SPIDER's FBS mode) with inplane
+    [n, 3] = (angle, sx, sy), then BP 3F (half None) or BP 32F (returns three volumes)."""
     imgs = _f32(imgs)
     ang = _f32(angles)
     ip = _f32(inplane)
@@ -217,7 +227,7 @@ def rb3f(imgs, angles, inplane, half=None, *, prec=0, nthreads=0):
     h = None if half is None else np.ascontiguousarray(half, dtype=np.uint8)
     rc = lib().orc_rb3f(_p(imgs, _f32p), nx, nang, _p(ang, _f32p), _p(ip, _f32p), _p(h, _u8p), prec,
                         _p(vols[0], _f32p), _p(vols[1], _f32p) if h is not None else None,
-                        _p(vols[2], _f32p) if h is not None else None, nthreads)
+                        _p(vols[2], _f32p) if h is not None else None, nthreads, 1 if fbs else 0)
     if rc != 0:
         raise RuntimeError(f"oracle rb3f failed: {rc}")
     return vols[0] if h is None else tuple(vols)

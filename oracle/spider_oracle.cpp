@@ -648,6 +648,13 @@ void insert_images(std::vector<Grid<R>*>& grids, const float* imgs, int nx, int 
       float dms[9];
       if (nsym > 1) matmul33(sm9 + 9 * is, dm9 + 9 * a, dms);
       else std::memcpy(dms, dm9 + 9 * a, sizeof(dms));
+      // The reference's schedule (bp3f.f:397-398, 469-471): rows J of one
+      // group, LN1 = 6 apart, run in parallel.  It is not race-free: a group
+      // with J = 0 or 3 (mod 6) holds rows J and -J, which write the same
+      // Friedel-mirrored voxels, and oblique rows 6 apart can share taps, so
+      // with more than one thread updates are lost (rel-l2 ~1e-4 at 128^3,
+      // varying run to run).  Parity checks run it with one thread; the
+      // threaded form serves as the timed CPU baseline.
       const int ln1 = 6;
       for (int jt = 1; jt <= ln1; ++jt) {
         #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
@@ -666,20 +673,29 @@ void grid_out(const Grid<R>& g, double* x_out, double* w_out) {
   }
 }
 
+void rtsf(const float* in, float* out, int nx, float thetat, float shxi, float shyi);
+
 template <class R>
 int bp_run(const float* imgs_in, int nx, int nang, const float* angles, const float* symang,
            int nsym, const uint8_t* half, int halt, float* vol_all, float* vol_1, float* vol_2,
-           double* x_out, double* w_out, int nthreads, const float* inplane = nullptr) {
+           double* x_out, double* w_out, int nthreads, const float* inplane = nullptr, bool use_rtsf = false) {
   if (nx < 8) return 101;
-  // RB 3F / RB 32F: every image first goes through RTSQ with doc registers
-  // 6-8 (in-plane angle, x shift, y shift), bp3f.f:406-425
+  // RB 3F / RB 32F: every image first goes through RTSQ (RTSF with SPIDER's
+  // FBS mode on) with doc registers 6-8 (in-plane angle, x shift, y shift),
+  // bp3f.f:406-425
   std::vector<float> rot;
   const float* imgs = imgs_in;
   if (inplane) {
     rot.resize((size_t)nang * nx * nx);
-    for (int a = 0; a < nang; ++a)
-      rtsq(imgs_in + (size_t)a * nx * nx, &rot[(size_t)a * nx * nx], nx, nx, inplane[3 * a], inplane[3 * a + 1],
-           inplane[3 * a + 2]);
+    #pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static) if (use_rtsf)
+    for (int a = 0; a < nang; ++a) {
+      if (use_rtsf)
+        rtsf(imgs_in + (size_t)a * nx * nx, &rot[(size_t)a * nx * nx], nx, inplane[3 * a], inplane[3 * a + 1],
+             inplane[3 * a + 2]);
+      else
+        rtsq(imgs_in + (size_t)a * nx * nx, &rot[(size_t)a * nx * nx], nx, nx, inplane[3 * a], inplane[3 * a + 1],
+             inplane[3 * a + 2]);
+    }
     imgs = rot.data();
   }
   KBTable kb;
@@ -1215,6 +1231,46 @@ R fbs3(float x, float y, float z, int n, const R* f1, const std::vector<R>* d) {
   return c0 + dc0 * dz + a2 * (dz * dz) + a3 * (dz * dz * dz);
 }
 
+// Fortran MODULO for REAL: A - FLOOR(A/P)*P, here as fmod with the sign of P
+static inline float fmodulo_real(float a, float p) {
+  float r = std::fmod(a, p);
+  if (r != 0.0f && ((r < 0.0f) != (p < 0.0f))) r += p;
+  return r;
+}
+
+// RTSF (rtsf.f:109-205), the SCLI = 1 branch that RB 3F / RB 32F take
+// (bp3f.f:414-417 passes SCLI = 1.0): FBS2_PREP of the image, then FBS2 with
+// wrapped indices at the rotated and shifted source position of every output
+// pixel.  REAL arithmetic, left to right; THETA = THETAT * PI / 180.
+void rtsf(const float* in, float* out, int nx, float thetat, float shxi, float shyi) {
+  const int ny = nx;
+  std::vector<float> x1, y1, xy2;
+  fbs2_prep<float>(in, nx, x1, y1, xy2);
+  const float pi = 3.14159265358979323846f;
+  const float theta = thetat * pi / 180.0f;
+  const float costh = std::cos(theta), sinth = std::sin(theta);
+  const int cx = nx / 2 + 1, cy = ny / 2 + 1;
+  const float shx = fmodulo_real(shxi, (float)nx), shy = fmodulo_real(shyi, (float)ny);
+  const float fy0 = -shy - (float)cy, fy1 = -shy + (float)ny - (float)cy, fy2 = -shy - (float)ny - (float)cy;
+  const float fx0 = -shx - (float)cx, fx1 = -shx + (float)nx - (float)cx, fx2 = -shx - (float)nx - (float)cx;
+  const float shypny = shy + (float)ny, shxpnx = shx + (float)nx;
+  for (int iy = 1; iy <= ny; ++iy) {
+    float fy = (float)iy + fy0;
+    if ((float)(iy - 1) < shy) fy = (float)iy + fy1;
+    if ((float)(iy - 1) >= shypny) fy = (float)iy + fy2;
+    const float ycod = costh * fy + (float)cy;
+    const float ysid = -sinth * fy + (float)cx;
+    for (int ix = 1; ix <= nx; ++ix) {
+      float fx = (float)ix + fx0;
+      if ((float)(ix - 1) < shx) fx = (float)ix + fx1;
+      if ((float)(ix - 1) >= shxpnx) fx = (float)ix + fx2;
+      const float xold = costh * fx + ysid;
+      const float yold = sinth * fx + ycod;
+      out[(size_t)(iy - 1) * nx + (ix - 1)] = fbs2<float>(xold, yold, nx, in, x1.data(), y1.data(), xy2.data());
+    }
+  }
+}
+
 // PRJCQ_FBS3 (prjcq.f:97-167): every line (J, K) of the cube, sample I
 // walked with XB += DM(1), YB += DM(2), ZB += DM(3); pixel (I, J) sums over K.
 template <class R>
@@ -1433,13 +1489,18 @@ int orc_bp3f(const float* imgs, int nx, int nang, const float* angles, const flo
 // RB 3F (half == NULL) / RB 32F: as orc_bp3f after RTSQ of every image with
 // inplane[3*i] = angle (deg), inplane[3*i+1] = x shift, inplane[3*i+2] = y shift
 int orc_rb3f(const float* imgs, int nx, int nang, const float* angles, const float* inplane, const uint8_t* half,
-             int prec, float* vol_all, float* vol_1, float* vol_2, int nthreads) {
+             int prec, float* vol_all, float* vol_1, float* vol_2, int nthreads, int fbs) {
   if (nthreads <= 0) nthreads = omp_get_max_threads();
   if (prec == 1)
     return bp_run<double>(imgs, nx, nang, angles, nullptr, 0, half, 0, vol_all, vol_1, vol_2, nullptr, nullptr,
-                          nthreads, inplane);
+                          nthreads, inplane, fbs != 0);
   return bp_run<float>(imgs, nx, nang, angles, nullptr, 0, half, 0, vol_all, vol_1, vol_2, nullptr, nullptr,
-                       nthreads, inplane);
+                       nthreads, inplane, fbs != 0);
+}
+
+// RTSF of one square image (rtsf.f:109-205, SCLI = 1)
+void orc_rtsf(const float* in, float* out, int nx, float theta, float shx, float shy) {
+  rtsf(in, out, nx, theta, shx, shy);
 }
 
 // SYMVOL of a volume with symmetry angle triples (psi, theta, phi)

@@ -59,6 +59,7 @@ SIGNATURES = [
                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp]),
     ("spi_ctx_set_cg_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_ctx_set_cg_interpolation", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("spi_ctx_set_rb_interpolation", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_cg_project", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, _vp, ctypes.c_int, _vp,
                                       ctypes.c_int]),
     ("spi_cg_backproject", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, _vp, ctypes.c_int, _vp,

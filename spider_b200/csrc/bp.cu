@@ -1051,6 +1051,7 @@ void bp_release(spi_ctx* c) {
   c->imgs.release();
   c->imgs2.release();
   c->rtsq_prm.release();
+  rtsf_release(c);
   c->padded.release();
   c->spectra.release();
   c->spec_tmp.release();
@@ -1547,6 +1548,7 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   const int ip = (n - nx) / 2 + nx % 2;
   const size_t spec_plane = (size_t)n * (nx + 1);
   std::vector<RtsqParm> rprm;
+  const bool rtsf = inplane && c->rb_fbs;
   if (inplane) {
     // COS/SIN(THETA*DGR_TO_RAD) in REAL, as RTSQ computes them (rtsq.f:111-112)
     const float dgr = 3.14159265358979323846f / 180.0f;
@@ -1554,6 +1556,17 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
     for (int a = 0; a < nimg; ++a) {
       const float th = inplane[3 * a];
       rprm[a] = RtsqParm{std::cos(th * dgr), std::sin(th * dgr), inplane[3 * a + 1], inplane[3 * a + 2]};
+      if (rtsf) {
+        // RTSF: THETA = THETAT * PI / 180, COS/SIN in REAL; SHX, SHY = MODULO(SH, NX)
+        // (rtsf.f:158-168), Fortran MODULO as fmod with the sign of NX
+        const float theta = th * 3.14159265358979323846f / 180.0f;
+        auto modulo = [&](float v) {
+          float r = std::fmod(v, (float)nx);
+          if (r != 0.0f && r < 0.0f) r += (float)nx;
+          return r;
+        };
+        rprm[a] = RtsqParm{std::cos(theta), std::sin(theta), modulo(inplane[3 * a + 1]), modulo(inplane[3 * a + 2])};
+      }
     }
     SPI_TRY(c->imgs2.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
     SPI_TRY(c->rtsq_prm.ensure((size_t)c->chunk * sizeof(RtsqParm)));
@@ -1619,11 +1632,16 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
         if (inplane) {
           int ev = c->phase_begin(0);
           float* dst = c->imgs2.as<float>() + (size_t)p0 * nx * nx;
-          rtsq_kernel<<<grid_blocks(c, (size_t)np * nx * nx, 256), 256, 0, c->stream>>>(
-              src, dst, nx, np, c->rtsq_prm.as<RtsqParm>() + p0);
-          SPI_TRY(check_kernel("rtsq_kernel"));
+          if (rtsf) {
+            static_assert(sizeof(RtsqParm) == sizeof(float4), "RTSF reads the parameters as float4");
+            SPI_TRY(rtsf_images(c, src, dst, nx, np, reinterpret_cast<const float4*>(c->rtsq_prm.as<RtsqParm>() + p0)));
+          } else {
+            rtsq_kernel<<<grid_blocks(c, (size_t)np * nx * nx, 256), 256, 0, c->stream>>>(
+                src, dst, nx, np, c->rtsq_prm.as<RtsqParm>() + p0);
+            SPI_TRY(check_kernel("rtsq_kernel"));
+            c->count();
+          }
           c->phase_end(ev);
-          c->count();
           src = dst;
         }
         // the last piece also zero-pads the unused tail of the FFT batch

@@ -952,21 +952,131 @@ static int hiang(std::vector<float>& ang, int nang, std::vector<CgDM>& dms, std:
 }
 
 // ---------------------------------------------------------------------------
+// FBS2_PREP for batches of K images: cuFFT plans and FP64 scratch.
+struct Fbs2Work {
+  int n = 0, K = 0;
+  float a4 = 0.0f;          // A4 = PI2 / N in REAL
+  cufftHandle fwd = 0, inv = 0;
+  double* dbl = nullptr;    // [K][n][n] FFT input
+  double2* F = nullptr;     // [K][n][h]
+  double2* W = nullptr;     // [3][K][n][h]
+  double* D = nullptr;      // [3][K][n][n]
+  void destroy() {
+    if (fwd) cufftDestroy(fwd);
+    if (inv) cufftDestroy(inv);
+    fwd = inv = 0;
+  }
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// bytes of the scratch of K images (the four arrays, each 256-byte aligned)
+static size_t fbs2_work_bytes(int n, size_t K) {
+  const size_t nn = (size_t)n * n, s2 = (size_t)n * (n / 2 + 1);
+  return align256(K * nn * 8) + align256(K * s2 * 16) + align256(3 * K * s2 * 16) + align256(3 * K * nn * 8);
+}
+
+// carve the scratch from p and (with `plans`) create the plans on stream s
+static int fbs2_work_init(Fbs2Work& w, int n, int K, char* p, cudaStream_t s, bool plans = true) {
+  const size_t nn = (size_t)n * n, s2 = (size_t)n * (n / 2 + 1);
+  w.n = n;
+  w.K = K;
+  w.a4 = 6.28318530717958647692f / (float)n;
+  w.dbl = reinterpret_cast<double*>(p); p += align256((size_t)K * nn * 8);
+  w.F = reinterpret_cast<double2*>(p); p += align256((size_t)K * s2 * 16);
+  w.W = reinterpret_cast<double2*>(p); p += align256(3 * (size_t)K * s2 * 16);
+  w.D = reinterpret_cast<double*>(p);
+  if (!plans) return 0;
+  int d2[2] = {n, n};
+  SPI_CUFFT(cufftPlanMany(&w.fwd, 2, d2, nullptr, 1, (int)nn, nullptr, 1, (int)s2, CUFFT_D2Z, K));
+  SPI_CUFFT(cufftPlanMany(&w.inv, 2, d2, nullptr, 1, (int)s2, nullptr, 1, (int)nn, CUFFT_Z2D, 3 * K));
+  SPI_CUFFT(cufftSetStream(w.fwd, s));
+  SPI_CUFFT(cufftSetStream(w.inv, s));
+  return 0;
+}
+
+// FBS2_PREP of kc <= K images src[kc][n][n] (S = float images or T
+// projections) into the interleaved tables P2[kc][n*n][4]
+template <class S, class T>
+static int fbs2_prepare(spi_ctx* c, const Fbs2Work& w, const S* src, int kc, T* P2) {
+  const int n = w.n;
+  const size_t nn = (size_t)n * n, count = (size_t)kc * nn, padded = (size_t)w.K * nn;
+  fbs_to_double_kernel<S, T><<<blocks_for(c, (long long)padded, 256), 256, 0, c->stream>>>(src, w.dbl, count, padded);
+  SPI_TRY(check_kernel("fbs_to_double_kernel"));
+  SPI_CUFFT(cufftExecD2Z(w.fwd, w.dbl, reinterpret_cast<cufftDoubleComplex*>(w.F)));
+  const size_t spec = (size_t)w.K * n * (n / 2 + 1);
+  fbs2_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(w.F, w.W, n, w.K, w.a4,
+                                                                              1.0 / ((double)n * n));
+  SPI_TRY(check_kernel("fbs2_spec_kernel"));
+  SPI_CUFFT(cufftExecZ2D(w.inv, reinterpret_cast<cufftDoubleComplex*>(w.W), w.D));
+  fbs2_pack_kernel<S, T><<<blocks_for(c, (long long)count, 256), 256, 0, c->stream>>>(src, w.D, P2, count, padded);
+  SPI_TRY(check_kernel("fbs2_pack_kernel"));
+  c->count(3);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// RTSF of nimg device images src -> dst (RB 3F / RB 32F in FBS mode).  The
+// plans and scratch (batches of up to K images, about 256 MB) stay with the
+// context for the next call of the same size.
+void rtsf_release(spi_ctx* c) {
+  if (c->rtsf_plan[0]) cufftDestroy(c->rtsf_plan[0]);
+  if (c->rtsf_plan[1]) cufftDestroy(c->rtsf_plan[1]);
+  c->rtsf_plan[0] = c->rtsf_plan[1] = 0;
+  c->rtsf_n = c->rtsf_k = 0;
+  c->rtsf_buf.release();
+}
+
+int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm) {
+  if (nimg <= 0) return 0;
+  const size_t nn = (size_t)nx * nx;
+  const size_t per = fbs2_work_bytes(nx, 1) + nn * 4 * sizeof(float);
+  const int K = (int)std::max<size_t>(1, std::min<size_t>(1024, (size_t(256) << 20) / per));
+  Fbs2Work w;
+  if (c->rtsf_n != nx || c->rtsf_k != K) {
+    rtsf_release(c);
+    SPI_TRY(c->rtsf_buf.ensure(fbs2_work_bytes(nx, K) + align256((size_t)K * nn * 4 * sizeof(float))));
+    const int st = fbs2_work_init(w, nx, K, c->rtsf_buf.as<char>(), c->stream);
+    if (st != 0) {
+      w.destroy();
+      return st;
+    }
+    c->rtsf_plan[0] = w.fwd;
+    c->rtsf_plan[1] = w.inv;
+    c->rtsf_n = nx;
+    c->rtsf_k = K;
+  } else {
+    SPI_TRY(fbs2_work_init(w, nx, K, c->rtsf_buf.as<char>(), c->stream, false));
+    w.fwd = c->rtsf_plan[0];
+    w.inv = c->rtsf_plan[1];
+    SPI_CUFFT(cufftSetStream(w.fwd, c->stream));
+    SPI_CUFFT(cufftSetStream(w.inv, c->stream));
+  }
+  float* P2 = reinterpret_cast<float*>(c->rtsf_buf.as<char>() + fbs2_work_bytes(nx, K));
+  for (int b0 = 0; b0 < nimg; b0 += K) {
+    const int kb = std::min(K, nimg - b0);
+    SPI_TRY((fbs2_prepare<float, float>(c, w, src + (size_t)b0 * nn, kb, P2)));
+    rtsf_kernel<<<blocks_for(c, (long long)kb * nn, 256), 256, 0, c->stream>>>(P2, dst + (size_t)b0 * nn, nx, kb,
+                                                                             prm + b0);
+    SPI_TRY(check_kernel("rtsf_kernel"));
+    c->count();
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // FBS operators: cuFFT plans and scratch for one BP CG solve.  Projections are
 // processed in chunks of K (the 2D plans' batch).
 struct FbsState {
   int n = 0, K = 0;
   float a4 = 0.0f;
-  cufftHandle p3f = 0, p3i = 0, p2f = 0, p2i = 0;
+  cufftHandle p3f = 0, p3i = 0;
+  Fbs2Work w2;              // FBS2_PREP of K images
   double* dbl3 = nullptr;   // [n^3] FFT input
   double2* F3 = nullptr;    // [n][n][h] forward spectrum
   double2* W3 = nullptr;    // [7][n][n][h] derivative spectra
   double* D3 = nullptr;     // [7][n^3] derivatives
   void* V = nullptr;        // T [n^3][8] interleaved FBS3 table
-  double* dbl2 = nullptr;   // [K][n][n]
-  double2* F2 = nullptr;    // [K][n][h]
-  double2* W2 = nullptr;    // [3][K][n][h]
-  double* D2 = nullptr;     // [3][K][n][n]
   void* P2 = nullptr;       // T [K][n*n][4] interleaved FBS2 tables
   void* pt = nullptr;       // T [K][n][n] projections of the iteration
   int2* segs = nullptr;     // {run, first offset} per BCKPJ_FBS segment
@@ -978,21 +1088,18 @@ struct FbsState {
   ~FbsState() {
     if (p3f) cufftDestroy(p3f);
     if (p3i) cufftDestroy(p3i);
-    if (p2f) cufftDestroy(p2f);
-    if (p2i) cufftDestroy(p2i);
+    w2.destroy();
   }
 };
-
-static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 template <class T>
 static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
   const int n = pb.n, h = n / 2 + 1;
-  const size_t nn = (size_t)n * n, nnn = nn * n, s3 = nn * h, s2 = (size_t)n * h;
+  const size_t nn = (size_t)n * n, nnn = nn * n, s3 = nn * h;
   fs.n = n;
   fs.a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / N in REAL
   // chunk: about 1 GiB of 2D scratch, at most 16384 projections
-  const size_t per_img = nn * 8 + s2 * 16 * 4 + nn * 8 * 3 + nn * 4 * sizeof(T) + nn * sizeof(T);
+  const size_t per_img = fbs2_work_bytes(n, 1) + nn * 4 * sizeof(T) + nn * sizeof(T);
   fs.K = (int)std::max<size_t>(1, std::min<size_t>({(size_t)nang, (size_t)16384, (size_t(1) << 30) / per_img}));
   if (const char* e = getenv("SPI_FBS_CHUNK")) {   // smaller chunks (tests of the chunk loop)
     const int k = atoi(e);
@@ -1007,8 +1114,8 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
   fs.nseg = (long long)segs.size();
   const size_t b3[5] = {align256(nnn * 8), align256(s3 * 16), align256(7 * s3 * 16), align256(7 * nnn * 8),
                         align256(nnn * 8 * sizeof(T))};
-  const size_t b2[6] = {align256(K * nn * 8), align256(K * s2 * 16), align256(3 * K * s2 * 16),
-                        align256(3 * K * nn * 8), align256(K * nn * 4 * sizeof(T)), align256(K * nn * sizeof(T))};
+  const size_t w2b = fbs2_work_bytes(n, K);
+  const size_t b2[3] = {w2b, align256(K * nn * 4 * sizeof(T)), align256(K * nn * sizeof(T))};
   size_t t3 = 0, t2 = 0;
   for (size_t b : b3) t3 += b;
   for (size_t b : b2) t2 += b;
@@ -1023,41 +1130,19 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
   fs.D3 = reinterpret_cast<double*>(p); p += b3[3];
   fs.V = p;
   p = c->cg_fbs[1].as<char>();
-  fs.dbl2 = reinterpret_cast<double*>(p); p += b2[0];
-  fs.F2 = reinterpret_cast<double2*>(p); p += b2[1];
-  fs.W2 = reinterpret_cast<double2*>(p); p += b2[2];
-  fs.D2 = reinterpret_cast<double*>(p); p += b2[3];
-  fs.P2 = p; p += b2[4];
+  SPI_TRY(fbs2_work_init(fs.w2, n, fs.K, p, c->stream));
+  p += b2[0];
+  fs.P2 = p; p += b2[1];
   fs.pt = p;
   fs.segs = c->cg_fbs[2].as<int2>();
   fs.dm9 = c->cg_fbs[3].as<float>();
   if (!segs.empty())
     SPI_CUDA(cudaMemcpyAsync(fs.segs, segs.data(), segs.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
-  int d3[3] = {n, n, n}, d2[2] = {n, n};
+  int d3[3] = {n, n, n};
   SPI_CUFFT(cufftPlan3d(&fs.p3f, n, n, n, CUFFT_D2Z));
   SPI_CUFFT(cufftPlanMany(&fs.p3i, 3, d3, nullptr, 1, (int)s3, nullptr, 1, (int)nnn, CUFFT_Z2D, 7));
-  SPI_CUFFT(cufftPlanMany(&fs.p2f, 2, d2, nullptr, 1, (int)nn, nullptr, 1, (int)s2, CUFFT_D2Z, fs.K));
-  SPI_CUFFT(cufftPlanMany(&fs.p2i, 2, d2, nullptr, 1, (int)s2, nullptr, 1, (int)nn, CUFFT_Z2D, 3 * fs.K));
-  for (cufftHandle hnd : {fs.p3f, fs.p3i, fs.p2f, fs.p2i}) SPI_CUFFT(cufftSetStream(hnd, c->stream));
-  return 0;
-}
-
-// FBS2_PREP of kc images src[kc][n][n] (S = float images or T projections) into P2
-template <class S, class T>
-static int fbs2_prepare(spi_ctx* c, FbsState& fs, const S* src, int kc, T* P2) {
-  const int n = fs.n;
-  const size_t nn = (size_t)n * n, count = (size_t)kc * nn, padded = (size_t)fs.K * nn;
-  fbs_to_double_kernel<S, T><<<blocks_for(c, (long long)padded, 256), 256, 0, c->stream>>>(src, fs.dbl2, count, padded);
-  SPI_TRY(check_kernel("fbs_to_double_kernel"));
-  SPI_CUFFT(cufftExecD2Z(fs.p2f, fs.dbl2, reinterpret_cast<cufftDoubleComplex*>(fs.F2)));
-  const size_t spec = (size_t)fs.K * n * (n / 2 + 1);
-  fbs2_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(fs.F2, fs.W2, n, fs.K, fs.a4,
-                                                                              1.0 / ((double)n * n));
-  SPI_TRY(check_kernel("fbs2_spec_kernel"));
-  SPI_CUFFT(cufftExecZ2D(fs.p2i, reinterpret_cast<cufftDoubleComplex*>(fs.W2), fs.D2));
-  fbs2_pack_kernel<S, T><<<blocks_for(c, (long long)count, 256), 256, 0, c->stream>>>(src, fs.D2, P2, count, padded);
-  SPI_TRY(check_kernel("fbs2_pack_kernel"));
-  c->count(3);
+  SPI_CUFFT(cufftSetStream(fs.p3f, c->stream));
+  SPI_CUFFT(cufftSetStream(fs.p3i, c->stream));
   return 0;
 }
 
@@ -1165,7 +1250,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     SPI_TRY(fbs_setup<T>(c, pb, nang, fs));
     for (int k0 = 0; k0 < nang; k0 += fs.K) {
       const int kc = std::min(fs.K, nang - k0);
-      SPI_TRY((fbs2_prepare<float, T>(c, fs, pj32 + (size_t)k0 * n * n, kc, static_cast<T*>(fs.P2))));
+      SPI_TRY((fbs2_prepare<float, T>(c, fs.w2, pj32 + (size_t)k0 * n * n, kc, static_cast<T*>(fs.P2))));
       SPI_TRY(fbs_backproject<T>(c, pb, fs, cb, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
     }
   } else if (mixed) {
@@ -1258,7 +1343,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
       for (int k0 = 0; k0 < lo; k0 += fs.K) {
         const int kc = std::min(fs.K, lo - k0);
         SPI_TRY(fbs_project<T>(c, fs, dlb, k0, kc));
-        SPI_TRY((fbs2_prepare<T, T>(c, fs, static_cast<const T*>(fs.pt), kc, static_cast<T*>(fs.P2))));
+        SPI_TRY((fbs2_prepare<T, T>(c, fs.w2, static_cast<const T*>(fs.pt), kc, static_cast<T*>(fs.P2))));
         SPI_TRY(fbs_backproject<T>(c, pb, fs, bcke, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
       }
     } else if (mixed) {
@@ -1355,6 +1440,13 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
 using namespace spi;
 
 extern "C" {
+
+int spi_ctx_set_rb_interpolation(spi_ctx* c, int fbs) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (fbs != 0 && fbs != 1) return fail(kInvalid, "spi_ctx_set_rb_interpolation: %d must be 0 (RTSQ) or 1 (RTSF)", fbs);
+  c->rb_fbs = fbs;
+  return 0;
+}
 
 int spi_ctx_set_cg_interpolation(spi_ctx* c, int fbs) {
   if (!c) return fail(kInvalid, "NULL context");

@@ -322,3 +322,33 @@ __global__ void fbs3_pack_kernel(const T* __restrict__ cube, const double* __res
     o[7] = (T)D[6 * nnn + q];
   }
 }
+
+// ---------------------------------------------------------------------------
+// RTSF (rtsf.f:109-205), the SCLI = 1 branch that RB 3F / RB 32F take with
+// SPIDER's FBS mode on (bp3f.f:412-417): output pixel (IX, IY) is FBS2 (with
+// wrapped indices) of the image at its rotated and shifted source position.
+// prm[b] = {COS(THETA), SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)} in REAL,
+// computed by the host; P2 = [nimg][nx*nx][4] FBS2 tables of the images.
+__global__ void rtsf_kernel(const float* __restrict__ P2, float* __restrict__ out, int nx, int nimg,
+                            const float4* __restrict__ prm) {
+  const size_t nn = (size_t)nx * nx, total = (size_t)nimg * nn;
+  const float fn = (float)nx, fc = (float)(nx / 2 + 1);   // CX = CY = NX/2 + 1
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(q / nn);
+    const int p = (int)(q % nn);
+    const int ix = p % nx + 1, iy = p / nx + 1;
+    const float4 m = prm[b];
+    // FY = IY + FY0, replaced by IY + FY1 / IY + FY2 across the shifted edge
+    float fy = __fadd_rn((float)iy, __fsub_rn(-m.w, fc));
+    if ((float)(iy - 1) < m.w) fy = __fadd_rn((float)iy, __fsub_rn(__fadd_rn(-m.w, fn), fc));
+    if ((float)(iy - 1) >= __fadd_rn(m.w, fn)) fy = __fadd_rn((float)iy, __fsub_rn(__fsub_rn(-m.w, fn), fc));
+    float fx = __fadd_rn((float)ix, __fsub_rn(-m.z, fc));
+    if ((float)(ix - 1) < m.z) fx = __fadd_rn((float)ix, __fsub_rn(__fadd_rn(-m.z, fn), fc));
+    if ((float)(ix - 1) >= __fadd_rn(m.z, fn)) fx = __fadd_rn((float)ix, __fsub_rn(__fsub_rn(-m.z, fn), fc));
+    const float ycod = __fadd_rn(__fmul_rn(m.x, fy), fc);
+    const float ysid = __fadd_rn(__fmul_rn(-m.y, fy), fc);
+    const float xold = __fadd_rn(__fmul_rn(m.x, fx), ysid);
+    const float yold = __fadd_rn(__fmul_rn(m.y, fx), ycod);
+    out[q] = fbs2_eval<float>(xold, yold, nx, P2 + (size_t)b * nn * 4);
+  }
+}

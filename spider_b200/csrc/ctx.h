@@ -29,6 +29,10 @@ struct spi_ctx {
   std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
   int cg_fp64 = 2;                    // BP CG precision: 0 FP32, 1 FP64, 2-4 FP64 vectors + fixed-point projections
   int cg_interp = 0;                  // BP CG interpolation: 0 linear, 1 FBS
+  int rb_fbs = 0;                     // RB 3F / RB 32F rotate with RTSF (FBS) instead of RTSQ
+  cufftHandle rtsf_plan[2] = {0, 0};  // RTSF: batched 2D D2Z / Z2D of FBS2_PREP
+  int rtsf_n = 0, rtsf_k = 0;         // image size and batch of those plans
+  spi::DevBuf rtsf_buf;               // RTSF scratch: FP64 FFT arrays + FBS2 tables
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT (and per insert launch)
   int sort_group = 0;                 // images per slice-ordering group (divides into sub)
@@ -85,5 +89,9 @@ namespace spi {
 void bp_release(spi_ctx* c);
 void pj_release(spi_ctx* c);
 void cg_release(spi_ctx* c);
+void rtsf_release(spi_ctx* c);
+// RTSF (rtsf.f:109-205, SCLI = 1) of nimg device images; prm[b] = {COS(THETA),
+// SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)}; runs on the context stream.
+int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm);
 int check_kernel(const char* what);
 }  // namespace spi

@@ -31,6 +31,9 @@ operation    answers (reference prompt order)
              limits, iteration limit & mode, lambda            (bpcg.f:139-244)
 ``BP CG 3L`` as BP CG 3, with the file numbers of the first and of the second
              sample after the image file numbers               (bpcg.f:143-152)
+``MD``       the mode: 'FBS ON' / 'USE FBS' / 'FBS' makes RB 3F and RB 32F
+             rotate with RTSF, 'FBS OFF' / 'NO FBS' with RTSQ  (setmode.f:399-409);
+             other modes are not provided
 ===========  =====================================================================
 
 The reference shuffles the BP 32F and BP CG 3 half sets with RANDOM_NUMBER
@@ -128,6 +131,17 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
         sio.write_image(_name(a[5], ext), v1)
         sio.write_image(_name(a[6], ext), v2)
         return {"vol": v_all, "vol1": v1, "vol2": v2, "half": half}
+    if op == "MD":
+        mode = " ".join(a[0].upper().split()) if a else ""
+        if mode in ("FBS ON", "USE FBS", "FBS"):
+            ctx.set_fbs(True)
+            print("  USING FBS INTERPOLATION", file=results)
+        elif mode in ("FBS OFF", "NO FBS"):
+            ctx.set_fbs(False)
+            print("  NOT USING FBS INTERPOLATION", file=results)
+        else:
+            raise ops.SpiderError(101, f"MD mode {mode!r} is not provided by this library")
+        return {"fbs": ctx.fbs}
     if op == "BP 3F M":
         numbers = sio.parse_numbers(a[1])
         parts = []

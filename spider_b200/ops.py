@@ -72,6 +72,12 @@ class Context:
         self._h = h
         self.device = device
         self._L = L
+        self.fbs = False
+
+    def set_fbs(self, on: bool):
+        """SPIDER's ``MD`` FBS mode: RB 3F / RB 32F rotate with RTSF (on) or RTSQ."""
+        check(self._L.spi_ctx_set_rb_interpolation(self._h, 1 if on else 0))
+        self.fbs = bool(on)
 
     @property
     def handle(self):
@@ -250,9 +256,17 @@ def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, 
             c.close()
 
 
-def rb3f(imgs, angles, inplane, sym=None, *, ctx: Context | None = None):
-    """``RB 3F``: RTSQ by (angle, sx, sy) per image, then BP 3F."""
+def _rb_mode(ctx, fbs):
+    """fbs None keeps the context's mode (SPIDER's ``MD`` FBS setting)."""
+    if fbs is not None:
+        ctx.set_fbs(bool(fbs))
+
+
+def rb3f(imgs, angles, inplane, sym=None, *, ctx: Context | None = None, fbs=None):
+    """``RB 3F``: RTSQ (RTSF with ``fbs`` or the context's FBS mode) by
+    (angle, sx, sy) per image, then BP 3F."""
     ctx = ctx or default_context()
+    _rb_mode(ctx, fbs)
     nx = _nx_of(imgs)
     ctx.bp_open(nx, 1, sym)
     try:
@@ -262,9 +276,11 @@ def rb3f(imgs, angles, inplane, sym=None, *, ctx: Context | None = None):
         ctx.bp_close()
 
 
-def rb32f(imgs, angles, inplane, half, sym=None, *, ctx: Context | None = None):
-    """``RB 32F``: RTSQ by (angle, sx, sy) per image, then BP 32F."""
+def rb32f(imgs, angles, inplane, half, sym=None, *, ctx: Context | None = None, fbs=None):
+    """``RB 32F``: RTSQ (RTSF with ``fbs`` or the context's FBS mode) by
+    (angle, sx, sy) per image, then BP 32F."""
     ctx = ctx or default_context()
+    _rb_mode(ctx, fbs)
     nx = _nx_of(imgs)
     ctx.bp_open(nx, 2, sym)
     try:

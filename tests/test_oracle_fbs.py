@@ -50,3 +50,57 @@ def test_bpcg_fbs_runs_fp32_and_fp64_agree():
     assert synth.rel_l2(v32, v64) < 1e-4
     # a different interpolation, the same problem: close to the linear solution, not equal
     assert 1e-6 < synth.rel_l2(v64, vl) < 0.5
+
+
+def test_rtsf_identity_and_integer_shifts():
+    """RTSF (rtsf.f:109-205) with no rotation reproduces integer shifts exactly
+    (circularly), since FBS2 at grid points returns the pixel itself."""
+    rng = np.random.default_rng(3)
+    img = rng.standard_normal((24, 24)).astype(np.float32)
+    assert np.array_equal(oracle.rtsf(img, 0.0, 0.0, 0.0), img)
+    assert np.array_equal(oracle.rtsf(img, 0.0, 3.0, 0.0), np.roll(img, 3, axis=1))
+    assert np.array_equal(oracle.rtsf(img, 0.0, 0.0, -5.0), np.roll(img, -5, axis=0))
+    assert np.array_equal(oracle.rtsf(img, 0.0, 27.0, 0.0), np.roll(img, 3, axis=1))   # MODULO(SHX, NX)
+
+
+def test_rtsf_rotates_band_limited_image():
+    """A band-limited image rotated by RTSF matches the analytic rotation
+    (about the centre NX/2+1) to the accuracy of the cubic interpolation; a
+    quarter turn is a transposition up to float rounding of COS(90)."""
+    n = 32
+    y, x = np.mgrid[1:n + 1, 1:n + 1].astype(np.float64)
+    c = n // 2 + 1
+
+    def f(xx, yy):
+        return np.cos(2 * np.pi * (2 * xx + 1 * yy) / n + 0.4) + 0.5 * np.sin(2 * np.pi * (xx - 3 * yy) / n)
+
+    img = f(x, y).astype(np.float32)
+    for th in (17.0, -63.0):
+        t = np.deg2rad(th)
+        # RTSF reads the source at XOLD = cos*FX - sin*FY + CX, YOLD = sin*FX + cos*FY + CY
+        xs = np.cos(t) * (x - c) - np.sin(t) * (y - c) + c
+        ys = np.sin(t) * (x - c) + np.cos(t) * (y - c) + c
+        ref = f(xs, ys)
+        got = oracle.rtsf(img, th, 0.0, 0.0)
+        assert np.abs(got - ref).max() < 2e-3, th
+    q = oracle.rtsf(img, 90.0, 0.0, 0.0)
+    xs = -(y - c) + c
+    ys = (x - c) + c
+    assert np.abs(q - f(xs, ys)).max() < 1e-4
+
+
+def test_rb3f_fbs_mode_uses_rtsf():
+    """RB 3F in FBS mode equals BP 3F of the RTSF-rotated images."""
+    from spider_b200 import synth
+    rng = np.random.default_rng(4)
+    n, nimg = 24, 12
+    imgs = rng.standard_normal((nimg, n, n)).astype(np.float32)
+    ang = synth.so3_angles(nimg, rng)
+    inplane = np.stack([rng.uniform(-180, 180, nimg), rng.uniform(-3, 3, nimg), rng.uniform(-3, 3, nimg)], 1)
+    inplane = inplane.astype(np.float32)
+    rot = np.stack([oracle.rtsf(imgs[i], *inplane[i]) for i in range(nimg)])
+    a = oracle.rb3f(imgs, ang, inplane, fbs=True, nthreads=1)
+    b = oracle.bp3f(rot, ang, nthreads=1)
+    assert np.array_equal(a, b)
+    c = oracle.rb3f(imgs, ang, inplane, nthreads=1)
+    assert not np.array_equal(a, c)
