@@ -1137,7 +1137,7 @@ void fbs2_prep(const R* img, int n, std::vector<R>& x1, std::vector<R>& y1, std:
 }
 
 // FBS3_PREP (fbs3.f:294-407): the seven derivatives of an n^3 volume.  The
-// XZ2 real part takes X1's real part (fbs3.f:371: X1(2*K+1) where the
+// XZ2 real part takes X1's real part (fbs3.f:379: X1(2*K+1) where the
 // pattern of the other lines has X1(2*K+2)); kept as the reference has it.
 template <class R>
 void fbs3_prep(const R* vol, int n, std::vector<R>* d /* x1 y1 z1 xy2 xz2 yz2 xyz */) {
@@ -1162,7 +1162,7 @@ void fbs3_prep(const R* vol, int n, std::vector<R>* d /* x1 y1 z1 xy2 xz2 yz2 xy
         D[1][q] = y1;
         D[2][q] = mul_mi(F[q], wz);
         D[3][q] = xy2;
-        D[4][q] = cd(x1.real() * wz, -x1.real() * wz);   // fbs3.f:371-372 as written
+        D[4][q] = cd(x1.real() * wz, -x1.real() * wz);   // fbs3.f:379-380 as written
         D[5][q] = mul_mi(y1, wz);
         D[6][q] = mul_mi(xy2, wz);
       }

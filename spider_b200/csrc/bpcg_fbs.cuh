@@ -255,7 +255,7 @@ __global__ void fbs2_spec_kernel(const double2* __restrict__ F, double2* __restr
 // FBS3_PREP spectra.  F = [n][n][h]; W = [7][n][n][h] = {X1, Y1, Z1, XY2, XZ2,
 // YZ2, XYZ}, prepared for the inverse as in fbs2_spec_kernel.  WY and WZ are
 // zero at the Nyquist index (fbs3.f:330-345); XZ2 takes X1's real part for
-// both components (fbs3.f:371-372), as the reference has it.
+// both components (fbs3.f:379-380), as the reference has it.
 __global__ void fbs3_spec_kernel(const double2* __restrict__ F, double2* __restrict__ W, int n, float a4,
                                  double scale) {
   const int h = n / 2 + 1;
