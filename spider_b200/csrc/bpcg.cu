@@ -1170,11 +1170,21 @@ template <class T>
 static int fbs_project(spi_ctx* c, FbsState& fs, const int* dlb, int k0, int kc) {
   const int n = fs.n;
   const int threads = (n + 31) / 32 * 32;
-  const size_t smem = (size_t)threads * (kFbsIC + 1) * sizeof(T);
-  if (smem > 48 * 1024)
-    SPI_CUDA(cudaFuncSetAttribute(prjcq_fbs3_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  prjcq_fbs3_kernel<T><<<dim3(n, kc), threads, smem, c->stream>>>(static_cast<const T*>(fs.V), fs.dm9, dlb, k0, n,
-                                                                  static_cast<T*>(fs.pt));
+  // samples per line between two row reductions: the shared tile is also L1
+  // that the gathers would use (SPI_FBS_IC = 8, 16 or 32 overrides)
+  int ic = kFbsIC;
+  if (const char* e = getenv("SPI_FBS_IC")) ic = atoi(e);
+  auto launch = [&](auto kern, int icv) -> int {
+    const size_t smem = (size_t)threads * (icv + 1) * sizeof(T);
+    if (smem > 48 * 1024)
+      SPI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<dim3(n, kc), threads, smem, c->stream>>>(static_cast<const T*>(fs.V), fs.dm9, dlb, k0, n,
+                                                    static_cast<T*>(fs.pt));
+    return 0;
+  };
+  if (ic == 8) SPI_TRY(launch(prjcq_fbs3_kernel<T, 8>, 8));
+  else if (ic == 32) SPI_TRY(launch(prjcq_fbs3_kernel<T, 32>, 32));
+  else SPI_TRY(launch(prjcq_fbs3_kernel<T, 16>, 16));
   SPI_TRY(check_kernel("prjcq_fbs3_kernel"));
   c->count();
   return 0;

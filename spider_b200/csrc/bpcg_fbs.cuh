@@ -24,7 +24,7 @@
 // round-to-nearest arithmetic without contraction.
 #pragma once
 
-constexpr int kFbsIC = 32;   // I samples per line between two row reductions (PRJCQ_FBS3)
+constexpr int kFbsIC = 16;   // I samples per line between two row reductions (PRJCQ_FBS3)
 constexpr int kFbsSeg = 8;   // run voxels per thread (BCKPJ_FBS)
 
 template <class T> struct FbsQuad { T a, b, c, d; };
@@ -33,10 +33,12 @@ __device__ __forceinline__ FbsQuad<float> fbs_ldq(const float* p) {
   const float4 v = __ldg(reinterpret_cast<const float4*>(p));
   return {v.x, v.y, v.z, v.w};
 }
+// one 256-bit read-only load (sm_100); every FP64 quad starts on a 32-byte
+// boundary (tables are 256-byte aligned, quads 32 bytes apart)
 __device__ __forceinline__ FbsQuad<double> fbs_ldq(const double* p) {
-  const double2 u = __ldg(reinterpret_cast<const double2*>(p));
-  const double2 w = __ldg(reinterpret_cast<const double2*>(p) + 1);
-  return {u.x, u.y, w.x, w.y};
+  FbsQuad<double> q;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(q.a), "=d"(q.b), "=d"(q.c), "=d"(q.d) : "l"(p));
+  return q;
 }
 
 // One cubic from values and derivatives at 0 and 1 (fbs2.f:150-170):
@@ -104,15 +106,15 @@ __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, 
 
 // ---------------------------------------------------------------------------
 // PRJCQ_FBS3: CTA (row J, projection k); thread t walks line K = t+1 of the
-// cube along I.  The samples of kFbsIC consecutive I go to shared memory and
+// cube along I.  The samples of IC consecutive I go to shared memory and
 // the pixel (I, J) sums them over K in order, as the reference's loop nest
 // does; then the HIANG multiplicity LB scales the pixel (bpcg.f:1790-1796).
-template <class T>
+template <class T, int IC>
 __global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V, const float* __restrict__ dm9,
                                                          const int* __restrict__ lb, int k0, int n,
                                                          T* __restrict__ projs) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* tile = reinterpret_cast<T*>(smraw);   // [blockDim.x][kFbsIC + 1]
+  T* tile = reinterpret_cast<T*>(smraw);   // [blockDim.x][IC + 1]
   const int k = blockIdx.y;
   const int j = blockIdx.x + 1;
   const int kk = threadIdx.x + 1;
@@ -130,15 +132,15 @@ __global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V
   const float d0 = dm[0], d1 = dm[1], d2 = dm[2];
   const int w = lb ? lb[k0 + k] : 1;
   T* out = projs + (size_t)k * n * n + (size_t)(j - 1) * n;
-  for (int i0 = 1; i0 <= n; i0 += kFbsIC) {
-    const int m = min(kFbsIC, n - i0 + 1);
+  for (int i0 = 1; i0 <= n; i0 += IC) {
+    const int m = min(IC, n - i0 + 1);
     if (live) {
       for (int ii = 0; ii < m; ++ii) {
         T s = (T)0;
         const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
         if (iox >= 1 && iox < n && ioy >= 1 && ioy < n && ioz >= 1 && ioz < n)
           s = fbs3_eval<T>(xb, yb, zb, iox, ioy, ioz, n, V);
-        tile[threadIdx.x * (kFbsIC + 1) + ii] = s;
+        tile[threadIdx.x * (IC + 1) + ii] = s;
         xb = __fadd_rn(xb, d0);
         yb = __fadd_rn(yb, d1);
         zb = __fadd_rn(zb, d2);
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V
     __syncthreads();
     if ((int)threadIdx.x < m) {
       T acc = (T)0;
-      for (int t = 0; t < n; ++t) acc = radd(acc, tile[t * (kFbsIC + 1) + threadIdx.x]);
+      for (int t = 0; t < n; ++t) acc = radd(acc, tile[t * (IC + 1) + threadIdx.x]);
       if (w > 1) acc = rmul(acc, (T)w);
       out[i0 - 1 + threadIdx.x] = acc;
     }
