@@ -251,8 +251,10 @@ int spi_ctx_set_cg_precision(spi_ctx* ctx, int mode);
  * (bckpj.f:123-164) the bicubic FBS2 interpolant of each projection; both
  * interpolants come from FFT derivatives (FBS2_PREP fbs2.f:182-247,
  * FBS3_PREP fbs3.f:294-407), computed in FP64.  With FBS the radius limit is
- * RI + MODE <= N/2 (linear: RI + MODE + 1), N is limited to 512, precision
- * mode 0 keeps FP32 vectors and every other mode FP64. */
+ * RI + MODE <= N/2 (linear: RI + MODE + 1) and N is limited to 512.
+ * Precision (spi_ctx_set_cg_precision): modes 1 and 4 are FP64 throughout,
+ * modes 2 and 3 keep FP64 vectors and arithmetic with FP32 interpolation
+ * tables (half the gathered bytes), mode 0 is FP32. */
 int spi_ctx_set_cg_interpolation(spi_ctx* ctx, int fbs);
 
 /* In-plane rotation of spi_bp_insert_rb (RB 3F / RB 32F), SPIDER's FBS mode

@@ -995,13 +995,14 @@ static int fbs2_work_init(Fbs2Work& w, int n, int K, char* p, cudaStream_t s, bo
   return 0;
 }
 
-// FBS2_PREP of kc <= K images src[kc][n][n] (S = float images or T
-// projections) into the interleaved tables P2[kc][n*n][4]
-template <class S, class T>
-static int fbs2_prepare(spi_ctx* c, const Fbs2Work& w, const S* src, int kc, T* P2) {
+// FBS2_PREP of kc <= K images src[kc][n][n] (S = float images or the
+// vector type's projections) into the interleaved tables P2[kc][n*n][4] of
+// type TT
+template <class S, class TT>
+static int fbs2_prepare(spi_ctx* c, const Fbs2Work& w, const S* src, int kc, TT* P2) {
   const int n = w.n;
   const size_t nn = (size_t)n * n, count = (size_t)kc * nn, padded = (size_t)w.K * nn;
-  fbs_to_double_kernel<S, T><<<blocks_for(c, (long long)padded, 256), 256, 0, c->stream>>>(src, w.dbl, count, padded);
+  fbs_to_double_kernel<S, S><<<blocks_for(c, (long long)padded, 256), 256, 0, c->stream>>>(src, w.dbl, count, padded);
   SPI_TRY(check_kernel("fbs_to_double_kernel"));
   SPI_CUFFT(cufftExecD2Z(w.fwd, w.dbl, reinterpret_cast<cufftDoubleComplex*>(w.F)));
   const size_t spec = (size_t)w.K * n * (n / 2 + 1);
@@ -1009,7 +1010,7 @@ static int fbs2_prepare(spi_ctx* c, const Fbs2Work& w, const S* src, int kc, T* 
                                                                               1.0 / ((double)n * n));
   SPI_TRY(check_kernel("fbs2_spec_kernel"));
   SPI_CUFFT(cufftExecZ2D(w.inv, reinterpret_cast<cufftDoubleComplex*>(w.W), w.D));
-  fbs2_pack_kernel<S, T><<<blocks_for(c, (long long)count, 256), 256, 0, c->stream>>>(src, w.D, P2, count, padded);
+  fbs2_pack_kernel<S, TT><<<blocks_for(c, (long long)count, 256), 256, 0, c->stream>>>(src, w.D, P2, count, padded);
   SPI_TRY(check_kernel("fbs2_pack_kernel"));
   c->count(3);
   return 0;
@@ -1082,6 +1083,7 @@ struct FbsState {
   int2* segs = nullptr;     // {run, first offset} per BCKPJ_FBS segment
   long long nseg = 0;
   float* dm9 = nullptr;     // 9 floats per merged angle
+  size_t tsz = 8;           // bytes per table value (FP32 tables in precision modes 2 and 3)
   FbsState() = default;
   FbsState(const FbsState&) = delete;
   FbsState& operator=(const FbsState&) = delete;
@@ -1093,13 +1095,14 @@ struct FbsState {
 };
 
 template <class T>
-static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
+static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, size_t tsz) {
   const int n = pb.n, h = n / 2 + 1;
   const size_t nn = (size_t)n * n, nnn = nn * n, s3 = nn * h;
   fs.n = n;
+  fs.tsz = tsz;
   fs.a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / N in REAL
   // chunk: about 1 GiB of 2D scratch, at most 16384 projections
-  const size_t per_img = fbs2_work_bytes(n, 1) + nn * 4 * sizeof(T) + nn * sizeof(T);
+  const size_t per_img = fbs2_work_bytes(n, 1) + nn * 4 * tsz + nn * sizeof(T);
   fs.K = (int)std::max<size_t>(1, std::min<size_t>({(size_t)nang, (size_t)16384, (size_t(1) << 30) / per_img}));
   if (const char* e = getenv("SPI_FBS_CHUNK")) {   // smaller chunks (tests of the chunk loop)
     const int k = atoi(e);
@@ -1113,9 +1116,9 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
   }
   fs.nseg = (long long)segs.size();
   const size_t b3[5] = {align256(nnn * 8), align256(s3 * 16), align256(7 * s3 * 16), align256(7 * nnn * 8),
-                        align256(nnn * 8 * sizeof(T))};
+                        align256(nnn * 8 * tsz)};
   const size_t w2b = fbs2_work_bytes(n, K);
-  const size_t b2[3] = {w2b, align256(K * nn * 4 * sizeof(T)), align256(K * nn * sizeof(T))};
+  const size_t b2[3] = {w2b, align256(K * nn * 4 * tsz), align256(K * nn * sizeof(T))};
   size_t t3 = 0, t2 = 0;
   for (size_t b : b3) t3 += b;
   for (size_t b : b2) t2 += b;
@@ -1146,8 +1149,8 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs) {
   return 0;
 }
 
-// FBS3_PREP of the cube into the interleaved table fs.V
-template <class T>
+// FBS3_PREP of the cube into the interleaved table fs.V (type TT)
+template <class T, class TT>
 static int fbs3_prepare(spi_ctx* c, FbsState& fs, const T* cube) {
   const int n = fs.n;
   const size_t nnn = (size_t)n * n * n;
@@ -1159,46 +1162,73 @@ static int fbs3_prepare(spi_ctx* c, FbsState& fs, const T* cube) {
                                                                               1.0 / ((double)n * n * n));
   SPI_TRY(check_kernel("fbs3_spec_kernel"));
   SPI_CUFFT(cufftExecZ2D(fs.p3i, reinterpret_cast<cufftDoubleComplex*>(fs.W3), fs.D3));
-  fbs3_pack_kernel<T><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.D3, static_cast<T*>(fs.V), nnn);
+  fbs3_pack_kernel<T, TT><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.D3,
+                                                                                    static_cast<TT*>(fs.V), nnn);
   SPI_TRY(check_kernel("fbs3_pack_kernel"));
   c->count(3);
   return 0;
 }
 
 // PRJCQ_FBS3 of fs.V for merged angles [k0, k0 + kc) into fs.pt, scaled by LB
-template <class T>
+template <class T, class TT>
 static int fbs_project(spi_ctx* c, FbsState& fs, const int* dlb, int k0, int kc) {
   const int n = fs.n;
   const int threads = (n + 31) / 32 * 32;
-  // samples per line between two row reductions: the shared tile is also L1
-  // that the gathers would use (SPI_FBS_IC = 8, 16 or 32 overrides)
-  int ic = kFbsIC;
-  if (const char* e = getenv("SPI_FBS_IC")) ic = atoi(e);
-  auto launch = [&](auto kern, int icv) -> int {
-    const size_t smem = (size_t)threads * (icv + 1) * sizeof(T);
+  const size_t smem = (size_t)threads * (kFbsIC + 1) * sizeof(T);
+  auto launch = [&](auto kern) -> int {
     if (smem > 48 * 1024)
       SPI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<dim3(n, kc), threads, smem, c->stream>>>(static_cast<const T*>(fs.V), fs.dm9, dlb, k0, n,
+    kern<<<dim3(n, kc), threads, smem, c->stream>>>(static_cast<const TT*>(fs.V), fs.dm9, dlb, k0, n,
                                                     static_cast<T*>(fs.pt));
     return 0;
   };
-  if (ic == 8) SPI_TRY(launch(prjcq_fbs3_kernel<T, 8>, 8));
-  else if (ic == 32) SPI_TRY(launch(prjcq_fbs3_kernel<T, 32>, 32));
-  else SPI_TRY(launch(prjcq_fbs3_kernel<T, 16>, 16));
+  // a 256-thread bound lets the FP64 form keep its registers (n <= 256)
+  if (threads <= 256) SPI_TRY(launch(prjcq_fbs3_kernel<T, TT, 256>));
+  else SPI_TRY(launch(prjcq_fbs3_kernel<T, TT, 512>));
   SPI_TRY(check_kernel("prjcq_fbs3_kernel"));
   c->count();
   return 0;
 }
 
 // BCKPJ_FBS of kc prepared tables P2 (angles dms[0..kc)) summed into cube
-template <class T>
-static int fbs_backproject(spi_ctx* c, const CgProblem& pb, FbsState& fs, T* cube, const T* P2, const CgDM* dms,
+template <class T, class TT>
+static int fbs_backproject(spi_ctx* c, const CgProblem& pb, FbsState& fs, T* cube, const TT* P2, const CgDM* dms,
                            int kc) {
   if (fs.nseg == 0 || kc <= 0) return 0;
-  bckpj_fbs_kernel<T><<<blocks_for(c, fs.nseg, 256), 256, 0, c->stream>>>(
+  bckpj_fbs_kernel<T, TT><<<blocks_for(c, fs.nseg, 256), 256, 0, c->stream>>>(
       cube, c->cg_buf[0].as<CgRun>(), fs.segs, fs.nseg, P2, dms, kc, pb.n, pb.ldp);
   SPI_TRY(check_kernel("bckpj_fbs_kernel"));
   c->count();
+  return 0;
+}
+
+// CB = A^T b with FBS (bpcg.f:713-731): FBS2_PREP and BCKPJ_FBS of every
+// image, in order, chunk by chunk
+template <class T, class TT>
+static int fbs_backproject_images(spi_ctx* c, const CgProblem& pb, FbsState& fs, T* cb, const float* imgs, int nang,
+                                  const CgDM* dms) {
+  const size_t nn = (size_t)pb.n * pb.n;
+  for (int k0 = 0; k0 < nang; k0 += fs.K) {
+    const int kc = std::min(fs.K, nang - k0);
+    SPI_TRY((fbs2_prepare<float, TT>(c, fs.w2, imgs + (size_t)k0 * nn, kc, static_cast<TT*>(fs.P2))));
+    SPI_TRY((fbs_backproject<T, TT>(c, pb, fs, cb, static_cast<const TT*>(fs.P2), dms + k0, kc)));
+  }
+  return 0;
+}
+
+// BCKE += A^T A BCKP with FBS (BPCG_3_FBS, bpcg.f:1760-1822): FBS3_PREP of
+// the direction, then per chunk of merged angles PRJCQ_FBS3 (scaled by LB),
+// FBS2_PREP of the projections and BCKPJ_FBS
+template <class T, class TT>
+static int fbs_normal(spi_ctx* c, const CgProblem& pb, FbsState& fs, const T* bckp, T* bcke, const int* dlb, int lo,
+                      const CgDM* dms) {
+  SPI_TRY((fbs3_prepare<T, TT>(c, fs, bckp)));
+  for (int k0 = 0; k0 < lo; k0 += fs.K) {
+    const int kc = std::min(fs.K, lo - k0);
+    SPI_TRY((fbs_project<T, TT>(c, fs, dlb, k0, kc)));
+    SPI_TRY((fbs2_prepare<T, TT>(c, fs.w2, static_cast<const T*>(fs.pt), kc, static_cast<TT*>(fs.P2))));
+    SPI_TRY((fbs_backproject<T, TT>(c, pb, fs, bcke, static_cast<const TT*>(fs.P2), dms + k0, kc)));
+  }
   return 0;
 }
 
@@ -1256,13 +1286,15 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   c->count();
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
   FbsState fs;
-  if (fbs) {   // bpcg.f:713-731: FBS2_PREP and BCKPJ_FBS of every image, in order
-    SPI_TRY(fbs_setup<T>(c, pb, nang, fs));
-    for (int k0 = 0; k0 < nang; k0 += fs.K) {
-      const int kc = std::min(fs.K, nang - k0);
-      SPI_TRY((fbs2_prepare<float, T>(c, fs.w2, pj32 + (size_t)k0 * n * n, kc, static_cast<T*>(fs.P2))));
-      SPI_TRY(fbs_backproject<T>(c, pb, fs, cb, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
-    }
+  // FBS interpolation tables: FP32 in precision modes 2 and 3 (FP64 vectors
+  // and arithmetic), the vector type otherwise
+  const bool fbs32 = fbs && sizeof(T) == 8 && (c->cg_fp64 == 2 || c->cg_fp64 == 3);
+  if (fbs) {
+    SPI_TRY(fbs_setup<T>(c, pb, nang, fs, fbs32 ? sizeof(float) : sizeof(T)));
+    if (fbs32)
+      SPI_TRY((fbs_backproject_images<T, float>(c, pb, fs, cb, pj32, nang, c->cg_buf[3].as<CgDM>())));
+    else
+      SPI_TRY((fbs_backproject_images<T, T>(c, pb, fs, cb, pj32, nang, c->cg_buf[3].as<CgDM>())));
   } else if (mixed) {
     if (wtab)
       SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
@@ -1348,14 +1380,10 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
-    if (fbs) {   // BPCG_3_FBS (bpcg.f:1760-1822)
-      SPI_TRY(fbs3_prepare<T>(c, fs, bckp));
-      for (int k0 = 0; k0 < lo; k0 += fs.K) {
-        const int kc = std::min(fs.K, lo - k0);
-        SPI_TRY(fbs_project<T>(c, fs, dlb, k0, kc));
-        SPI_TRY((fbs2_prepare<T, T>(c, fs.w2, static_cast<const T*>(fs.pt), kc, static_cast<T*>(fs.P2))));
-        SPI_TRY(fbs_backproject<T>(c, pb, fs, bcke, static_cast<const T*>(fs.P2), c->cg_buf[3].as<CgDM>() + k0, kc));
-      }
+    if (fbs32) {
+      SPI_TRY((fbs_normal<T, float>(c, pb, fs, bckp, bcke, dlb, lo, c->cg_buf[3].as<CgDM>())));
+    } else if (fbs) {
+      SPI_TRY((fbs_normal<T, T>(c, pb, fs, bckp, bcke, dlb, lo, c->cg_buf[3].as<CgDM>())));
     } else if (mixed) {
       auto* mx = reinterpret_cast<unsigned long long*>(acc + 7);
       if (wide && wtab)

@@ -24,7 +24,9 @@
 // round-to-nearest arithmetic without contraction.
 #pragma once
 
-constexpr int kFbsIC = 16;   // I samples per line between two row reductions (PRJCQ_FBS3)
+// I samples per line between two row reductions (PRJCQ_FBS3): the shared
+// tile takes L1 from the gathers, and 16 measured as fast as 8 and faster than 32
+constexpr int kFbsIC = 16;
 constexpr int kFbsSeg = 8;   // run voxels per thread (BCKPJ_FBS)
 
 template <class T> struct FbsQuad { T a, b, c, d; };
@@ -39,6 +41,13 @@ __device__ __forceinline__ FbsQuad<double> fbs_ldq(const double* p) {
   FbsQuad<double> q;
   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(q.a), "=d"(q.b), "=d"(q.c), "=d"(q.d) : "l"(p));
   return q;
+}
+
+// a table quad (type TT) widened to the arithmetic type T
+template <class T, class TT>
+__device__ __forceinline__ FbsQuad<T> fbs_ld(const TT* p) {
+  const FbsQuad<TT> q = fbs_ldq(p);
+  return {(T)q.a, (T)q.b, (T)q.c, (T)q.d};
 }
 
 // One cubic from values and derivatives at 0 and 1 (fbs2.f:150-170):
@@ -66,27 +75,29 @@ __device__ __forceinline__ int fbs_mod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
-// FBS2 with CHKBOUND (indices wrapped): P = [n*n][4] {P, X1, Y1, XY2}.
-// Every index is reduced modulo n, so any position reads inside the table.
-template <class T>
-__device__ __forceinline__ T fbs2_eval(float x, float y, int n, const T* __restrict__ P) {
+// FBS2 with CHKBOUND (indices wrapped): P = [n*n][4] {P, X1, Y1, XY2} of
+// type TT, arithmetic in T.  Every index is reduced modulo n, so any
+// position reads inside the table.
+template <class T, class TT>
+__device__ __forceinline__ T fbs2_eval(float x, float y, int n, const TT* __restrict__ P) {
   const int i = __float2int_rd(x), j = __float2int_rd(y);
   const T dx = (T)__fsub_rn(x, (float)i), dy = (T)__fsub_rn(y, (float)j);
   const T dx2 = rmul(dx, dx), dx3 = rmul(dx2, dx), dy2 = rmul(dy, dy), dy3 = rmul(dy2, dy);
   const int i2 = fbs_mod(i - 1, n), j2 = fbs_mod(j - 1, n), i3 = fbs_mod(i, n), j3 = fbs_mod(j, n);
-  const FbsQuad<T> q00 = fbs_ldq(P + ((size_t)j2 * n + i2) * 4);
-  const FbsQuad<T> q10 = fbs_ldq(P + ((size_t)j2 * n + i3) * 4);
-  const FbsQuad<T> q01 = fbs_ldq(P + ((size_t)j3 * n + i2) * 4);
-  const FbsQuad<T> q11 = fbs_ldq(P + ((size_t)j3 * n + i3) * 4);
+  const FbsQuad<T> q00 = fbs_ld<T>(P + ((size_t)j2 * n + i2) * 4);
+  const FbsQuad<T> q10 = fbs_ld<T>(P + ((size_t)j2 * n + i3) * 4);
+  const FbsQuad<T> q01 = fbs_ld<T>(P + ((size_t)j3 * n + i2) * 4);
+  const FbsQuad<T> q11 = fbs_ld<T>(P + ((size_t)j3 * n + i3) * 4);
   return fbs_bicubic(q00, q10, q01, q11, dx, dx2, dx3, dy, dy2, dy3);
 }
 
 // FBS3 at (x, y, z) with i = IFIX(x), j = IFIX(y), l = IFIX(z) all in
 // [1, n-1] (the PRJCQ_FBS3 bounds check): the corners are (i-1, i) etc.,
-// 0-based, with no wrap.  V = [n^3][8] {F, X1, Y1, XY2, Z1, XZ2, YZ2, XYZ}.
-template <class T>
+// 0-based, with no wrap.  V = [n^3][8] {F, X1, Y1, XY2, Z1, XZ2, YZ2, XYZ}
+// of type TT, arithmetic in T.
+template <class T, class TT>
 __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, int l, int n,
-                                       const T* __restrict__ V) {
+                                       const TT* __restrict__ V) {
   const T dx = (T)__fsub_rn(x, (float)i), dy = (T)__fsub_rn(y, (float)j), dz = (T)__fsub_rn(z, (float)l);
   const T dx2 = rmul(dx, dx), dx3 = rmul(dx2, dx), dy2 = rmul(dy, dy), dy3 = rmul(dy2, dy);
   const T dz2 = rmul(dz, dz), dz3 = rmul(dz2, dz);
@@ -95,11 +106,12 @@ __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, 
   T c[2], dc[2];
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
-    const T* b = V + v0 + p * sz;
+    const TT* b = V + v0 + p * sz;
     // value plane: F, X1, Y1, XY2; z-derivative plane: Z1, XZ2, YZ2, XYZ
-    c[p] = fbs_bicubic(fbs_ldq(b), fbs_ldq(b + 8), fbs_ldq(b + sy), fbs_ldq(b + sy + 8), dx, dx2, dx3, dy, dy2, dy3);
-    dc[p] = fbs_bicubic(fbs_ldq(b + 4), fbs_ldq(b + 12), fbs_ldq(b + sy + 4), fbs_ldq(b + sy + 12), dx, dx2, dx3,
-                        dy, dy2, dy3);
+    c[p] = fbs_bicubic(fbs_ld<T>(b), fbs_ld<T>(b + 8), fbs_ld<T>(b + sy), fbs_ld<T>(b + sy + 8), dx, dx2, dx3, dy,
+                       dy2, dy3);
+    dc[p] = fbs_bicubic(fbs_ld<T>(b + 4), fbs_ld<T>(b + 12), fbs_ld<T>(b + sy + 4), fbs_ld<T>(b + sy + 12), dx, dx2,
+                        dx3, dy, dy2, dy3);
   }
   return fbs_cub(c[0], dc[0], c[1], dc[1], dz, dz2, dz3);
 }
@@ -109,11 +121,12 @@ __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, 
 // cube along I.  The samples of IC consecutive I go to shared memory and
 // the pixel (I, J) sums them over K in order, as the reference's loop nest
 // does; then the HIANG multiplicity LB scales the pixel (bpcg.f:1790-1796).
-template <class T, int IC>
-__global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V, const float* __restrict__ dm9,
+template <class T, class TT, int MAXT>
+__global__ void __launch_bounds__(MAXT) prjcq_fbs3_kernel(const TT* __restrict__ V, const float* __restrict__ dm9,
                                                          const int* __restrict__ lb, int k0, int n,
                                                          T* __restrict__ projs) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int IC = kFbsIC;
   T* tile = reinterpret_cast<T*>(smraw);   // [blockDim.x][IC + 1]
   const int k = blockIdx.y;
   const int j = blockIdx.x + 1;
@@ -139,7 +152,7 @@ __global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V
         T s = (T)0;
         const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
         if (iox >= 1 && iox < n && ioy >= 1 && ioy < n && ioz >= 1 && ioz < n)
-          s = fbs3_eval<T>(xb, yb, zb, iox, ioy, ioz, n, V);
+          s = fbs3_eval<T, TT>(xb, yb, zb, iox, ioy, ioz, n, V);
         tile[threadIdx.x * (IC + 1) + ii] = s;
         xb = __fadd_rn(xb, d0);
         yb = __fadd_rn(yb, d1);
@@ -162,10 +175,10 @@ __global__ void __launch_bounds__(512) prjcq_fbs3_kernel(const T* __restrict__ V
 // projection, in order, the thread repeats the run's sequential walk up to
 // its segment, then adds FBS2 at each of its voxels.  segs[s] = {run, first
 // offset within the run}.
-template <class T>
+template <class T, class TT>
 __global__ void __launch_bounds__(256) bckpj_fbs_kernel(T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                         const int2* __restrict__ segs, long long nseg,
-                                                        const T* __restrict__ P2, const CgDM* __restrict__ dms,
+                                                        const TT* __restrict__ P2, const CgDM* __restrict__ dms,
                                                         int kc, int n, int ldp) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x) {
     const int2 sg = segs[s];
@@ -185,10 +198,10 @@ __global__ void __launch_bounds__(256) bckpj_fbs_kernel(T* __restrict__ cube, co
         xb = __fadd_rn(xb, dm.d[0]);
         yb = __fadd_rn(yb, dm.d[3]);
       }
-      const T* P = P2 + (size_t)k * n * n * 4;
+      const TT* P = P2 + (size_t)k * n * n * 4;
 #pragma unroll
       for (int t = 0; t < kFbsSeg; ++t) {
-        if (t < len) c[t] = radd(c[t], fbs2_eval<T>(xb, yb, n, P));
+        if (t < len) c[t] = radd(c[t], fbs2_eval<T, TT>(xb, yb, n, P));
         xb = __fadd_rn(xb, dm.d[0]);
         yb = __fadd_rn(yb, dm.d[3]);
       }
@@ -307,21 +320,21 @@ __global__ void fbs2_pack_kernel(const S* __restrict__ src, const double* __rest
   }
 }
 
-// V[v] = {F, X1, Y1, XY2, Z1, XZ2, YZ2, XYZ}; D = [7][n^3] in the order
-// X1, Y1, Z1, XY2, XZ2, YZ2, XYZ
-template <class T>
-__global__ void fbs3_pack_kernel(const T* __restrict__ cube, const double* __restrict__ D, T* __restrict__ V,
+// V[v] = {F, X1, Y1, XY2, Z1, XZ2, YZ2, XYZ} of type TT; D = [7][n^3] in the
+// order X1, Y1, Z1, XY2, XZ2, YZ2, XYZ
+template <class T, class TT>
+__global__ void fbs3_pack_kernel(const T* __restrict__ cube, const double* __restrict__ D, TT* __restrict__ V,
                                  size_t nnn) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nnn; q += (size_t)gridDim.x * blockDim.x) {
-    T* o = V + q * 8;
-    o[0] = cube[q];
-    o[1] = (T)D[q];
-    o[2] = (T)D[nnn + q];
-    o[3] = (T)D[3 * nnn + q];
-    o[4] = (T)D[2 * nnn + q];
-    o[5] = (T)D[4 * nnn + q];
-    o[6] = (T)D[5 * nnn + q];
-    o[7] = (T)D[6 * nnn + q];
+    TT* o = V + q * 8;
+    o[0] = (TT)cube[q];
+    o[1] = (TT)D[q];
+    o[2] = (TT)D[nnn + q];
+    o[3] = (TT)D[3 * nnn + q];
+    o[4] = (TT)D[2 * nnn + q];
+    o[5] = (TT)D[4 * nnn + q];
+    o[6] = (TT)D[5 * nnn + q];
+    o[7] = (TT)D[6 * nnn + q];
   }
 }
 
@@ -351,6 +364,6 @@ __global__ void rtsf_kernel(const float* __restrict__ P2, float* __restrict__ ou
     const float ysid = __fadd_rn(__fmul_rn(-m.y, fy), fc);
     const float xold = __fadd_rn(__fmul_rn(m.x, fx), ysid);
     const float yold = __fadd_rn(__fmul_rn(m.y, fx), ycod);
-    out[q] = fbs2_eval<float>(xold, yold, nx, P2 + (size_t)b * nn * 4);
+    out[q] = fbs2_eval<float, float>(xold, yold, nx, P2 + (size_t)b * nn * 4);
   }
 }

@@ -368,8 +368,9 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     """``BP CG``.  Prompts in reference order: radius (default n/2-2),
     error & chi^2 limits, iteration limit & mode, lambda.
     ``interp``: "linear" (the 'L' answer) or "fbs" (the 'F' answer: FBS
-    interpolation through FFT derivatives, BPCG_3_FBS); with "fbs",
-    ``fp64=False`` keeps FP32 vectors and every other setting FP64.
+    interpolation through FFT derivatives, BPCG_3_FBS); with "fbs", True
+    and "mixed64" are FP64 throughout, "mixed" and "fast" keep FP64 vectors
+    and arithmetic with FP32 interpolation tables, False is FP32.
     ``fp64``: "mixed" (default) keeps the CG vectors in FP64 and the
     projections in 47-bit fixed point with FP32 PROJT tables, "mixed64" the
     same with FP64 tables, "fast" 31-bit fixed point, True keeps everything
