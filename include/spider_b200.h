@@ -176,6 +176,15 @@ int spi_bp32f(spi_ctx* ctx, const float* imgs, int nx, int nang, const float* an
 int spi_pj3q(spi_ctx* ctx, const float* vol, int nx, int ny, int nz, float ri,
              const float* angles, int nang, float* proj_out, int on_device);
 
+/* PJ 3F: PJ 3Q with FBS interpolation (PJ3Q_N(.TRUE.), vtil2.f:222-228;
+ * writpro_n.f:154-205 -> FBS3_PREP fbs3.f:294-407 -> WPRO_FBS wpro_fbs.f):
+ * the voxel runs of PJ 3Q, each sample the tricubic FBS3 interpolant (FFT
+ * derivatives, wrapped indices) instead of the trilinear one.  Same
+ * arguments as spi_pj3q; cubic volumes only (nx = ny = nz <= 1024); FP32
+ * tables and arithmetic (the reference's REAL), FP64 transforms. */
+int spi_pj3f(spi_ctx* ctx, const float* vol, int nx, int ny, int nz, float ri,
+             const float* angles, int nang, float* proj_out, int on_device);
+
 /* PJ 3Q that allocates nothing -- no counterpart in the reference; an
  * addition for callers that must not allocate device memory: applications
  * whose device memory belongs to a fixed arena or caching allocator, and

@@ -69,6 +69,9 @@ def lib():
         L.orc_bp_session_free.argtypes = [ctypes.c_void_p]
         L.orc_bp_session_insert.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int, _f32p, _u8p, ctypes.c_int]
         L.orc_bp_session_insert.restype = ctypes.c_int
+        L.orc_pj3f.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _f32p, ctypes.c_int, ctypes.c_int, _f32p,
+                               ctypes.c_int]
+        L.orc_pj3f.restype = None
         L.orc_pj3q.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                _f32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int]
         L.orc_prepcub_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
@@ -264,6 +267,21 @@ class BpSession:
 
     def __del__(self):
         self.close()
+
+
+def pj3f(vol, angles, ri=None, *, prec=0, nthreads=0):
+    """PJ 3F (PJ 3Q with FBS interpolation): cubic vol [n, n, n] -> projections [nang, n, n]."""
+    vol = _f32(vol)
+    n = vol.shape[0]
+    if vol.shape != (n, n, n):
+        raise ValueError("PJ 3F: cubic volume expected")
+    if ri is None:
+        ri = float(n // 2 - 2)
+    ang = _f32(angles)
+    nang = ang.shape[0]
+    out = np.zeros((nang, n, n), np.float32)
+    lib().orc_pj3f(_p(vol, _f32p), n, ri, _p(ang, _f32p), nang, prec, _p(out, _f32p), nthreads)
+    return out
 
 
 def pj3q(vol, angles, ri=None, *, prec=0, nthreads=0):

@@ -1294,6 +1294,46 @@ void prjcq_fbs3(const R* cube, const float* dm, R* prj, int n, const std::vector
     }
 }
 
+// WPRO_FBS (wpro_fbs.f:1-150): PJ 3F, WPRO_N's walk along the PREPCUB runs
+// with an FBS3 sample (wrapped indices) per voxel; the bounds test, when the
+// sphere does not fit, admits IFIX in 1..N (wpro_fbs.f:138-144).
+template <class R>
+void wpro_fbs(R* b, int n, const R* cube, const std::vector<R>* d, const std::vector<RunC>& runs, float phi,
+              float theta, float psi, float ri, int ldp) {
+  const double d2r = QUADPI_F / 180.0;
+  double cphi = std::cos((double)phi * d2r), sphi = std::sin((double)phi * d2r);
+  double cthe = std::cos((double)theta * d2r), sthe = std::sin((double)theta * d2r);
+  double cpsi = std::cos((double)psi * d2r), spsi = std::sin((double)psi * d2r);
+  float dm[9];
+  dm[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
+  dm[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
+  dm[2] = (float)(-sthe * cpsi);
+  dm[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
+  dm[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
+  dm[5] = (float)(sthe * spsi);
+  dm[6] = (float)(sthe * cphi);
+  dm[7] = (float)(sthe * sphi);
+  dm[8] = (float)(cthe);
+  std::fill(b, b + (size_t)n * n, (R)0);
+  const bool nocheck = (2.0f * (ri + 1.0f) + 1.0f) <= (float)n;
+  for (const RunC& rn : runs) {
+    const int k = rn.y + ldp;
+    float xb = (float)rn.x * dm[0] + (float)rn.y * dm[3] + (float)rn.z * dm[6] + (float)ldp;
+    float yb = (float)rn.x * dm[1] + (float)rn.y * dm[4] + (float)rn.z * dm[7] + (float)ldp;
+    float zb = (float)rn.x * dm[2] + (float)rn.y * dm[5] + (float)rn.z * dm[8] + (float)ldp;
+    for (int j = rn.i1; j <= rn.i2; ++j) {
+      const int iox = ifix(xb), ioy = ifix(yb), ioz = ifix(zb);
+      if (nocheck || (iox > 0 && iox <= n && ioy > 0 && ioy <= n && ioz > 0 && ioz <= n)) {
+        R& o = b[(size_t)(k - 1) * n + (j - 1)];
+        o = o + fbs3<R>(xb, yb, zb, n, cube, d);
+      }
+      xb = xb + dm[0];
+      yb = yb + dm[1];
+      zb = zb + dm[2];
+    }
+  }
+}
+
 // BCKPJ_FBS (bckpj.f:123-164): voxel gather along the runs, sequential XB += DM(1), YB += DM(4).
 template <class R>
 void bckpj_fbs(R* cube, const float* dm, const R* proj, const R* x1, const R* y1, const R* xy2, int n,
@@ -1575,6 +1615,31 @@ void orc_pj3q(const float* vol, int nx, int ny, int nz, float ri, const float* a
       wpro_n<float>(out, nx, ny, nz, vol, runs, angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], ri, ldpx, ldpy, ldpz);
     }
   }
+}
+
+// PJ 3F: PJ 3Q with FBS interpolation (PJ3Q_N(.TRUE.), vtil2.f:222-228,
+// writpro_n.f:154-205): FBS3_PREP of the cubic volume, then WPRO_FBS per angle
+void orc_pj3f(const float* vol, int n, float ri, const float* angles, int nang, int prec, float* proj_out,
+              int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  const int ldp = n / 2 + 1;
+  std::vector<RunC> runs;
+  prepcub(n, n, n, ri, ldp, ldp, ldp, runs);
+  auto go = [&](auto zero) {
+    using R = decltype(zero);
+    std::vector<R> cube((size_t)n * n * n);
+    for (size_t i = 0; i < cube.size(); ++i) cube[i] = (R)vol[i];
+    std::vector<R> d[7];
+    fbs3_prep<R>(cube.data(), n, d);
+    #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (int a = 0; a < nang; ++a) {
+      std::vector<R> b((size_t)n * n);
+      wpro_fbs<R>(b.data(), n, cube.data(), d, runs, angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], ri, ldp);
+      float* out = proj_out + (size_t)a * n * n;
+      for (size_t i = 0; i < b.size(); ++i) out[i] = (float)b[i];
+    }
+  };
+  if (prec == 1) go(0.0); else go(0.0f);
 }
 
 // Number of voxel runs PREPCUB produces (for tests of the run lists)

@@ -46,6 +46,8 @@ SIGNATURES = [
                                  _vp, _vp, _vp]),
     ("spi_pj3q", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                 _vp, ctypes.c_int, _vp, ctypes.c_int]),
+    ("spi_pj3f", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                _vp, ctypes.c_int, _vp, ctypes.c_int]),
     ("spi_pj3q_noalloc", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                         _vp, ctypes.c_int, _vp, _vp]),
     ("spi_pj3q_adjoint", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,

@@ -1066,18 +1066,70 @@ int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, cons
 }
 
 // ---------------------------------------------------------------------------
+// FBS3_PREP of one n^3 volume: cuFFT plans and FP64 scratch.
+struct Fbs3Work {
+  int n = 0;
+  float a4 = 0.0f;          // A4 = PI2 / N in REAL
+  cufftHandle fwd = 0, inv = 0;
+  double* dbl = nullptr;    // [n^3] FFT input
+  double2* F = nullptr;     // [n][n][h] forward spectrum
+  double2* W = nullptr;     // [7][n][n][h] derivative spectra
+  double* D = nullptr;      // [7][n^3] derivatives
+  void destroy() {
+    if (fwd) cufftDestroy(fwd);
+    if (inv) cufftDestroy(inv);
+    fwd = inv = 0;
+  }
+};
+
+static size_t fbs3_work_bytes(int n) {
+  const size_t nnn = (size_t)n * n * n, s3 = (size_t)n * n * (n / 2 + 1);
+  return align256(nnn * 8) + align256(s3 * 16) + align256(7 * s3 * 16) + align256(7 * nnn * 8);
+}
+
+static int fbs3_work_init(Fbs3Work& w, int n, char* p, cudaStream_t s) {
+  const size_t nnn = (size_t)n * n * n, s3 = (size_t)n * n * (n / 2 + 1);
+  w.n = n;
+  w.a4 = 6.28318530717958647692f / (float)n;
+  w.dbl = reinterpret_cast<double*>(p); p += align256(nnn * 8);
+  w.F = reinterpret_cast<double2*>(p); p += align256(s3 * 16);
+  w.W = reinterpret_cast<double2*>(p); p += align256(7 * s3 * 16);
+  w.D = reinterpret_cast<double*>(p);
+  int d3[3] = {n, n, n};
+  SPI_CUFFT(cufftPlan3d(&w.fwd, n, n, n, CUFFT_D2Z));
+  SPI_CUFFT(cufftPlanMany(&w.inv, 3, d3, nullptr, 1, (int)s3, nullptr, 1, (int)nnn, CUFFT_Z2D, 7));
+  SPI_CUFFT(cufftSetStream(w.fwd, s));
+  SPI_CUFFT(cufftSetStream(w.inv, s));
+  return 0;
+}
+
+// FBS3_PREP of the cube into the interleaved table V[n^3][8] of type TT
+template <class T, class TT>
+static int fbs3_prepare(spi_ctx* c, const Fbs3Work& w, const T* cube, TT* V) {
+  const int n = w.n;
+  const size_t nnn = (size_t)n * n * n;
+  fbs_to_double_kernel<T, T><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, w.dbl, nnn, nnn);
+  SPI_TRY(check_kernel("fbs_to_double_kernel"));
+  SPI_CUFFT(cufftExecD2Z(w.fwd, w.dbl, reinterpret_cast<cufftDoubleComplex*>(w.F)));
+  const size_t spec = (size_t)n * n * (n / 2 + 1);
+  fbs3_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(w.F, w.W, n, w.a4,
+                                                                              1.0 / ((double)n * n * n));
+  SPI_TRY(check_kernel("fbs3_spec_kernel"));
+  SPI_CUFFT(cufftExecZ2D(w.inv, reinterpret_cast<cufftDoubleComplex*>(w.W), w.D));
+  fbs3_pack_kernel<T, TT><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, w.D, V, nnn);
+  SPI_TRY(check_kernel("fbs3_pack_kernel"));
+  c->count(3);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // FBS operators: cuFFT plans and scratch for one BP CG solve.  Projections are
 // processed in chunks of K (the 2D plans' batch).
 struct FbsState {
   int n = 0, K = 0;
-  float a4 = 0.0f;
-  cufftHandle p3f = 0, p3i = 0;
   Fbs2Work w2;              // FBS2_PREP of K images
-  double* dbl3 = nullptr;   // [n^3] FFT input
-  double2* F3 = nullptr;    // [n][n][h] forward spectrum
-  double2* W3 = nullptr;    // [7][n][n][h] derivative spectra
-  double* D3 = nullptr;     // [7][n^3] derivatives
-  void* V = nullptr;        // T [n^3][8] interleaved FBS3 table
+  Fbs3Work w3;              // FBS3_PREP of the direction
+  void* V = nullptr;        // TT [n^3][8] interleaved FBS3 table
   void* P2 = nullptr;       // T [K][n*n][4] interleaved FBS2 tables
   void* pt = nullptr;       // T [K][n][n] projections of the iteration
   int2* segs = nullptr;     // {run, first offset} per BCKPJ_FBS segment
@@ -1088,19 +1140,17 @@ struct FbsState {
   FbsState(const FbsState&) = delete;
   FbsState& operator=(const FbsState&) = delete;
   ~FbsState() {
-    if (p3f) cufftDestroy(p3f);
-    if (p3i) cufftDestroy(p3i);
     w2.destroy();
+    w3.destroy();
   }
 };
 
 template <class T>
 static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, size_t tsz) {
-  const int n = pb.n, h = n / 2 + 1;
-  const size_t nn = (size_t)n * n, nnn = nn * n, s3 = nn * h;
+  const int n = pb.n;
+  const size_t nn = (size_t)n * n, nnn = nn * n;
   fs.n = n;
   fs.tsz = tsz;
-  fs.a4 = 6.28318530717958647692f / (float)n;   // A4 = PI2 / N in REAL
   // chunk: about 1 GiB of 2D scratch, at most 16384 projections
   const size_t per_img = fbs2_work_bytes(n, 1) + nn * 4 * tsz + nn * sizeof(T);
   fs.K = (int)std::max<size_t>(1, std::min<size_t>({(size_t)nang, (size_t)16384, (size_t(1) << 30) / per_img}));
@@ -1115,8 +1165,7 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, si
     for (int o = 0; o < len; o += kFbsSeg) segs.push_back(make_int2((int)r, o));
   }
   fs.nseg = (long long)segs.size();
-  const size_t b3[5] = {align256(nnn * 8), align256(s3 * 16), align256(7 * s3 * 16), align256(7 * nnn * 8),
-                        align256(nnn * 8 * tsz)};
+  const size_t b3[2] = {fbs3_work_bytes(n), align256(nnn * 8 * tsz)};
   const size_t w2b = fbs2_work_bytes(n, K);
   const size_t b2[3] = {w2b, align256(K * nn * 4 * tsz), align256(K * nn * sizeof(T))};
   size_t t3 = 0, t2 = 0;
@@ -1127,11 +1176,8 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, si
   SPI_TRY(c->cg_fbs[2].ensure(std::max<size_t>(1, segs.size()) * sizeof(int2)));
   SPI_TRY(c->cg_fbs[3].ensure((size_t)9 * std::max(nang, 1) * sizeof(float)));
   char* p = c->cg_fbs[0].as<char>();
-  fs.dbl3 = reinterpret_cast<double*>(p); p += b3[0];
-  fs.F3 = reinterpret_cast<double2*>(p); p += b3[1];
-  fs.W3 = reinterpret_cast<double2*>(p); p += b3[2];
-  fs.D3 = reinterpret_cast<double*>(p); p += b3[3];
-  fs.V = p;
+  SPI_TRY(fbs3_work_init(fs.w3, n, p, c->stream));
+  fs.V = p + b3[0];
   p = c->cg_fbs[1].as<char>();
   SPI_TRY(fbs2_work_init(fs.w2, n, fs.K, p, c->stream));
   p += b2[0];
@@ -1141,31 +1187,6 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, si
   fs.dm9 = c->cg_fbs[3].as<float>();
   if (!segs.empty())
     SPI_CUDA(cudaMemcpyAsync(fs.segs, segs.data(), segs.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
-  int d3[3] = {n, n, n};
-  SPI_CUFFT(cufftPlan3d(&fs.p3f, n, n, n, CUFFT_D2Z));
-  SPI_CUFFT(cufftPlanMany(&fs.p3i, 3, d3, nullptr, 1, (int)s3, nullptr, 1, (int)nnn, CUFFT_Z2D, 7));
-  SPI_CUFFT(cufftSetStream(fs.p3f, c->stream));
-  SPI_CUFFT(cufftSetStream(fs.p3i, c->stream));
-  return 0;
-}
-
-// FBS3_PREP of the cube into the interleaved table fs.V (type TT)
-template <class T, class TT>
-static int fbs3_prepare(spi_ctx* c, FbsState& fs, const T* cube) {
-  const int n = fs.n;
-  const size_t nnn = (size_t)n * n * n;
-  fbs_to_double_kernel<T, T><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.dbl3, nnn, nnn);
-  SPI_TRY(check_kernel("fbs_to_double_kernel"));
-  SPI_CUFFT(cufftExecD2Z(fs.p3f, fs.dbl3, reinterpret_cast<cufftDoubleComplex*>(fs.F3)));
-  const size_t spec = (size_t)n * n * (n / 2 + 1);
-  fbs3_spec_kernel<<<blocks_for(c, (long long)spec, 256), 256, 0, c->stream>>>(fs.F3, fs.W3, n, fs.a4,
-                                                                              1.0 / ((double)n * n * n));
-  SPI_TRY(check_kernel("fbs3_spec_kernel"));
-  SPI_CUFFT(cufftExecZ2D(fs.p3i, reinterpret_cast<cufftDoubleComplex*>(fs.W3), fs.D3));
-  fbs3_pack_kernel<T, TT><<<blocks_for(c, (long long)nnn, 256), 256, 0, c->stream>>>(cube, fs.D3,
-                                                                                    static_cast<TT*>(fs.V), nnn);
-  SPI_TRY(check_kernel("fbs3_pack_kernel"));
-  c->count(3);
   return 0;
 }
 
@@ -1222,7 +1243,7 @@ static int fbs_backproject_images(spi_ctx* c, const CgProblem& pb, FbsState& fs,
 template <class T, class TT>
 static int fbs_normal(spi_ctx* c, const CgProblem& pb, FbsState& fs, const T* bckp, T* bcke, const int* dlb, int lo,
                       const CgDM* dms) {
-  SPI_TRY((fbs3_prepare<T, TT>(c, fs, bckp)));
+  SPI_TRY((fbs3_prepare<T, TT>(c, fs.w3, bckp, static_cast<TT*>(fs.V))));
   for (int k0 = 0; k0 < lo; k0 += fs.K) {
     const int kc = std::min(fs.K, lo - k0);
     SPI_TRY((fbs_project<T, TT>(c, fs, dlb, k0, kc)));
@@ -1478,6 +1499,59 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
 using namespace spi;
 
 extern "C" {
+
+int spi_pj3f(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
+             float* proj_out, int on_device) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (nx != ny || nx != nz) return fail(kInvalid, "PJ 3F: cubic volumes only (%dx%dx%d)", nx, ny, nz);
+  if (nx > 1024) return fail(kInvalid, "PJ 3F: n = %d above 1024", nx);
+  int nruns = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));
+  if (!vol || !proj_out) return fail(kInvalid, "PJ 3F: NULL buffer");
+  const int n = nx;
+  const size_t nnn = (size_t)n * n * n, vbytes = nnn * sizeof(float);
+  const size_t pbytes = (size_t)nang * n * n * sizeof(float);
+  const float* dvol = vol;
+  float* dout = proj_out;
+  if (!on_device) {
+    SPI_TRY(c->pj_vol.ensure(vbytes));
+    SPI_TRY(c->pj_out.ensure(std::max<size_t>(pbytes, 4)));
+    SPI_CUDA(cudaMemcpyAsync(c->pj_vol.p, vol, vbytes, cudaMemcpyHostToDevice, c->stream));
+    dvol = c->pj_vol.as<float>();
+    dout = c->pj_out.as<float>();
+  }
+  if (nang == 0) return 0;
+  // FBS3_PREP of the volume (writpro_n.f:154-185), REAL tables
+  const size_t wb = fbs3_work_bytes(n);
+  SPI_TRY(c->pj_fbs.ensure(wb + align256(nnn * 8 * sizeof(float))));
+  Fbs3Work w;
+  int st = fbs3_work_init(w, n, c->pj_fbs.as<char>(), c->stream);
+  float* V = reinterpret_cast<float*>(c->pj_fbs.as<char>() + wb);
+  if (st == 0) st = fbs3_prepare<float, float>(c, w, dvol, V);
+  if (st == 0) {
+    const cudaError_t e = cudaMemsetAsync(dout, 0, pbytes, c->stream);
+    if (e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
+  }
+  if (st == 0) {
+    const long long total = (long long)nruns * nang;
+    const int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
+    const int nocheck = (2.0f * (ri + 1.0f) + 1.0f) <= (float)n;
+    if (blocks > 0) {
+      wpro_fbs_kernel<float, float><<<blocks, 128, 0, c->stream>>>(V, n, c->pj_runs.as<PjRun>(), nruns,
+                                                                   c->pj_dm.as<PjDM>(), nang, n / 2 + 1, nocheck, dout);
+      st = check_kernel("wpro_fbs_kernel");
+      c->count();
+    }
+  }
+  if (st == 0 && !on_device) {
+    const cudaError_t e = cudaMemcpyAsync(proj_out, dout, pbytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
+  }
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  w.destroy();
+  if (st == 0 && e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
+  return st;
+}
 
 int spi_ctx_set_rb_interpolation(spi_ctx* c, int fbs) {
   if (!c) return fail(kInvalid, "NULL context");

@@ -116,6 +116,67 @@ __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, 
   return fbs_cub(c[0], dc[0], c[1], dc[1], dz, dz2, dz3);
 }
 
+// FBS3 at any position with wrapped indices (FBS3 as WPRO_FBS calls it,
+// fbs3.f:60-290): i = FLOOR(x), corners MODULO(i-1, n) and the next one
+// modulo n, and likewise for y and z.
+template <class T, class TT>
+__device__ __forceinline__ T fbs3_eval_wrap(float x, float y, float z, int n, const TT* __restrict__ V) {
+  const int i = __float2int_rd(x), j = __float2int_rd(y), l = __float2int_rd(z);
+  const int i2 = fbs_mod(i - 1, n), j2 = fbs_mod(j - 1, n), l2 = fbs_mod(l - 1, n);
+  const int i3 = (i2 + 1) % n, j3 = (j2 + 1) % n, l3 = (l2 + 1) % n;
+  const T dx = (T)__fsub_rn(x, (float)i), dy = (T)__fsub_rn(y, (float)j), dz = (T)__fsub_rn(z, (float)l);
+  const T dx2 = rmul(dx, dx), dx3 = rmul(dx2, dx), dy2 = rmul(dy, dy), dy3 = rmul(dy2, dy);
+  const T dz2 = rmul(dz, dz), dz3 = rmul(dz2, dz);
+  auto at = [&](int ii, int jj, int ll) { return V + (((size_t)ll * n + jj) * n + ii) * 8; };
+  T c[2], dc[2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int ll = p ? l3 : l2;
+    const TT *q00 = at(i2, j2, ll), *q10 = at(i3, j2, ll), *q01 = at(i2, j3, ll), *q11 = at(i3, j3, ll);
+    c[p] = fbs_bicubic(fbs_ld<T>(q00), fbs_ld<T>(q10), fbs_ld<T>(q01), fbs_ld<T>(q11), dx, dx2, dx3, dy, dy2, dy3);
+    dc[p] = fbs_bicubic(fbs_ld<T>(q00 + 4), fbs_ld<T>(q10 + 4), fbs_ld<T>(q01 + 4), fbs_ld<T>(q11 + 4), dx, dx2,
+                        dx3, dy, dy2, dy3);
+  }
+  return fbs_cub(c[0], dc[0], c[1], dc[1], dz, dz2, dz3);
+}
+
+// ---------------------------------------------------------------------------
+// WPRO_FBS (wpro_fbs.f:1-150), PJ 3F: one thread per (projection, run) walks
+// the run as WPRO_N does (XB = XB + DM(1), ...); every sample is FBS3 with
+// wrapped indices; the runs of one output row K = Y + LDP meet in a pixel
+// through atomics.  nocheck: the sphere fits (2(RI+1)+1 <= N); otherwise
+// samples whose IFIX lies outside 1..N are skipped (wpro_fbs.f:138-144).
+template <class T, class TT>
+__global__ void __launch_bounds__(128) wpro_fbs_kernel(const TT* __restrict__ V, int n, const PjRun* __restrict__ runs,
+                                                       int nruns, const PjDM* __restrict__ dms, int nang, int ldp,
+                                                       int nocheck, float* __restrict__ out) {
+  const long long total = (long long)nruns * nang;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nruns);
+    const PjRun r = runs[t % nruns];
+    const PjDM dm = dms[a];
+    float* b = out + (size_t)a * n * n;
+    const int k = r.y + ldp;
+    // IPCUBE(3)*DM(a) + IPCUBE(4)*DM(b) + IPCUBE(5)*DM(c) + LDP, left to right
+    auto start = [&](float da, float db, float dc) {
+      return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn((float)r.x, da), __fmul_rn((float)r.y, db)),
+                                 __fmul_rn((float)r.z, dc)),
+                       (float)ldp);
+    };
+    float xb = start(dm.d[0], dm.d[3], dm.d[6]);
+    float yb = start(dm.d[1], dm.d[4], dm.d[7]);
+    float zb = start(dm.d[2], dm.d[5], dm.d[8]);
+    for (int j = r.i1; j <= r.i2; ++j) {
+      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+      if (nocheck || (iox > 0 && iox <= n && ioy > 0 && ioy <= n && ioz > 0 && ioz <= n))
+        atomicAdd(b + (size_t)(k - 1) * n + (j - 1), (float)fbs3_eval_wrap<T, TT>(xb, yb, zb, n, V));
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[1]);
+      zb = __fadd_rn(zb, dm.d[2]);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // PRJCQ_FBS3: CTA (row J, projection k); thread t walks line K = t+1 of the
 // cube along I.  The samples of IC consecutive I go to shared memory and

@@ -65,6 +65,7 @@ struct spi_ctx {
 
   // ---- PJ 3Q / BP CG scratch ----
   spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
+  spi::DevBuf pj_fbs;                 // PJ 3F: FBS3_PREP scratch + the FBS3 table
   spi::DevBuf cg_buf[8];
   spi::DevBuf cg_fbs[4];              // FBS: 3D scratch + table, 2D chunk scratch, segments, DM(1..9)
   spi::HostBuf hbuf;
@@ -90,6 +91,19 @@ void bp_release(spi_ctx* c);
 void pj_release(spi_ctx* c);
 void cg_release(spi_ctx* c);
 void rtsf_release(spi_ctx* c);
+
+// PJ 3Q / PJ 3F voxel runs (PREPCUB, prepcub.f:54-109) and rotations
+struct PjRun {
+  int i1, i2;     // first/last x (1-based) of the run
+  int x, y, z;    // centred coordinates of the first voxel
+};
+struct PjDM {
+  float d[9];
+};
+// Validates the arguments, builds the runs of the sphere of radius ri and
+// the DM of every angle (psi, theta, phi) and uploads them to pj_runs / pj_dm
+// on the context stream.
+int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out);
 // RTSF (rtsf.f:109-205, SCLI = 1) of nimg device images; prm[b] = {COS(THETA),
 // SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)}; runs on the context stream.
 int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm);

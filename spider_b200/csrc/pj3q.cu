@@ -16,15 +16,6 @@
 
 namespace spi {
 
-struct PjRun {
-  int i1, i2;     // first/last x (1-based) of the run
-  int x, y, z;    // centred coordinates of the first voxel
-};
-
-struct PjDM {
-  float d[9];
-};
-
 static void prepcub(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<PjRun>& runs) {
   const float r = ri * ri;
   runs.clear();
@@ -187,10 +178,10 @@ void pj_release(spi_ctx* c) {
   c->pj_out.release();
   c->pj_runs.release();
   c->pj_dm.release();
+  c->pj_fbs.release();
 }
 
-static int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang,
-                     int* nruns_out) {
+int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out) {
   if (!c) return fail(kInvalid, "NULL context");
   if (nx < 4 || ny < 4 || nz < 4) return fail(kInvalid, "PJ 3Q: volume %dx%dx%d too small", nx, ny, nz);
   if (nang < 0 || (nang > 0 && !angles)) return fail(kInvalid, "PJ 3Q: bad angle list");

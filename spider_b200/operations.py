@@ -23,6 +23,7 @@ operation    answers (reference prompt order)
                                                                (bp3f.f:563-648)
 ``PJ 3Q``    input volume, 'radius[, Y]' (consecutive numbers), angle numbers,
              angles doc, output projection template            (pj3q_n.f:73-160)
+``PJ 3F``    as PJ 3Q, with FBS interpolation (cubic volumes)  (vtil2.f:222-228)
 ``BP CG``    image template, file numbers, radius, angles doc, L/F,
              reconstructed volume, 'error limit, chi^2 limit',
              'iteration limit, mode', lambda                   (bpcg.f:120-244)
@@ -157,7 +158,7 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
         vol = ops.bp3f_merge(parts, sym, ctx=ctx)
         sio.write_image(_name(a[3], ext), vol)
         return {"vol": vol}
-    if op == "PJ 3Q":
+    if op in ("PJ 3Q", "PJ 3F"):
         vol, _ = sio.read_image(_name(a[0], ext))
         if vol.ndim == 2:
             vol = vol[None]
@@ -169,14 +170,14 @@ def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=
         conseq = len(parts) > 1 and "Y" in parts[1].upper()
         numbers = sio.parse_numbers(a[2])
         ang = _angles(_name(a[3], ext), numbers)
-        proj = ops.pj3q(vol, ang, ri, ctx=ctx)
+        proj = (ops.pj3f if op == "PJ 3F" else ops.pj3q)(vol, ang, ri, ctx=ctx)
         tmpl = _name(a[4], ext)
         if "@" in tmpl:
             sio.write_stack(tmpl.split("@", 1)[0], proj, angles=ang)
         else:
             for i, k in enumerate(numbers):
                 sio.write_image(sio.expand_template(tmpl, i + 1 if conseq else k), proj[i], angles=ang[i])
-        print(f"  PJ 3Q FINISHED FOR: {len(numbers):7d}   PROJECTIONS -----", file=results)
+        print(f"  {op} FINISHED FOR: {len(numbers):7d}   PROJECTIONS -----", file=results)
         return {"proj": proj}
     if op in ("BP CG", "BP CG 3", "BP CG 3L"):
         numbers = sio.parse_numbers(a[1])

@@ -344,6 +344,25 @@ def pj3q(vol, angles, ri=None, *, ctx: Context | None = None):
     return out
 
 
+def pj3f(vol, angles, ri=None, *, ctx: Context | None = None):
+    """``PJ 3F``: FBS (tricubic, FFT-derivative) projections [nang, n, n] of a
+    cubic vol [n, n, n]; host arrays or CUDA tensors, as :func:`pj3q`."""
+    ctx = ctx or default_context()
+    nx, ny, nz = _vol_shape(vol)
+    if ri is None:
+        ri = float(min(nx, ny, nz) // 2 - 2)  # pj3q_n.f:82
+    ang = _host_f32(angles)
+    nang = ang.shape[0]
+    dev = _is_dev(vol)
+    if dev:
+        out = torch.empty((nang, ny, nx), dtype=torch.float32, device=vol.device)
+    else:
+        vol = _host_f32(vol)
+        out = np.zeros((nang, ny, nx), np.float32)
+    check(ctx._L.spi_pj3f(ctx.handle, _ptr(vol), nx, ny, nz, float(ri), _ptr(ang), nang, _ptr(out), 1 if dev else 0))
+    return out
+
+
 def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
     """Exact adjoint of :func:`pj3q`: volume [nz, ny, nx] from projections [nang, ny, nx]."""
     ctx = ctx or default_context()
