@@ -10,7 +10,12 @@ Layout (SPIDER's image_doc and docfile formats):
   PSI3/THETA3/PHI3/LANGLE at 101-104 (written by PJ 3Q, writpro_n.f:244-249).
 * A simple image/volume is the header followed by NY*NZ records.  A stack is
   an overall header (ISTACK > 0, MAXIM = highest image number) followed, for
-  each image, by its own header (IMGNUM) and its data.
+  each image, by its own header (IMGNUM) and its data.  An indexed stack has
+  ISTACK = -MAXINDX and, after the overall header, INDXREC = ceil(MAXINDX/NX)
+  records of raw int32 entries: entry k is the 1-based storage slot of image
+  number k (0 = absent), and slot s starts at record
+  LABREC + INDXREC + (s-1)*(LABREC + NY*NZ) (lunsethdr.f:215-240,505-530,
+  2140-2200).
 * Files are native little-endian float32; byte-swapped files are recognised
   by the plausibility of their header words.
 * Document files: lines ``key nregs v1 v2 ...``; a ';' in column 2 marks a
@@ -133,21 +138,40 @@ def write_image(path, arr, *, angles=None):
 
 
 def read_stack(path, numbers=None):
-    """Stack file -> (array [n, ny, nx], list of image numbers, per-image headers)."""
+    """Stack or indexed stack file -> (array [n, ny, nx], list of image
+    numbers, per-image headers).  numbers None: every image (1..MAXIM; for
+    an indexed stack every number present in the index)."""
     h, order = read_header(path)
     nx, ny, nz, labbyt = _geom(h)
     istack, maxim = int(h[23]), int(h[25])
-    if istack <= 0:
-        raise ValueError(f"{path}: not a (non-indexed) stack")
+    if istack == 0:
+        raise ValueError(f"{path}: not a stack")
     per = labbyt + nx * ny * nz * 4
+    index = None
+    base = labbyt
+    if istack < 0:   # indexed stack: MAXINDX = -ISTACK, then the index records
+        maxindx = -istack
+        indxrec = -(-maxindx // nx)
+        with open(path, "rb") as f:
+            f.seek(labbyt)
+            index = np.frombuffer(f.read(indxrec * nx * 4), dtype=order + "i4")[:maxindx].astype(np.int64)
+        base = labbyt + indxrec * nx * 4
+        if numbers is None:
+            numbers = [int(k) + 1 for k in np.nonzero(index > 0)[0]]
     nums = list(range(1, maxim + 1)) if numbers is None else list(numbers)
     out = np.zeros((len(nums), ny, nx) if nz == 1 else (len(nums), nz, ny, nx), np.float32)
     heads = []
     with open(path, "rb") as f:
         for i, k in enumerate(nums):
-            if k < 1 or k > maxim:
-                raise ValueError(f"{path}: image {k} not in stack (MAXIM {maxim})")
-            f.seek(labbyt + (k - 1) * per)
+            if index is not None:
+                if k < 1 or k > len(index) or index[k - 1] <= 0:
+                    raise ValueError(f"{path}: image {k} not in the indexed stack")
+                slot = int(index[k - 1])
+            else:
+                if k < 1 or k > maxim:
+                    raise ValueError(f"{path}: image {k} not in stack (MAXIM {maxim})")
+                slot = k
+            f.seek(base + (slot - 1) * per)
             ih = np.frombuffer(f.read(labbyt), dtype=order + "f4").astype(np.float32)
             d = np.frombuffer(f.read(nx * ny * nz * 4), dtype=order + "f4").astype(np.float32)
             out[i] = d.reshape(out.shape[1:])
@@ -155,16 +179,33 @@ def read_stack(path, numbers=None):
     return out, nums, heads
 
 
-def write_stack(path, arr, *, angles=None):
-    """Write images [n, ny, nx] as a stack (numbers 1..n); optional angles [n, 3]."""
+def write_stack(path, arr, *, angles=None, numbers=None, maxindx=None):
+    """Write images [n, ny, nx] as a stack (numbers 1..n); optional angles [n, 3].
+    With ``numbers`` (and ``maxindx`` >= max(numbers)) an indexed stack is
+    written instead: image i gets number numbers[i] and storage slot i+1."""
     a = np.ascontiguousarray(arr, dtype="<f4")
     n, ny, nx = a.shape
     iform = 1
+    nums = list(range(1, n + 1)) if numbers is None else [int(k) for k in numbers]
     with open(path, "wb") as f:
-        f.write(_make_header(nx, ny, 1, iform, istack=2, maxim=n).astype("<f4").tobytes())
+        if numbers is None:
+            f.write(_make_header(nx, ny, 1, iform, istack=2, maxim=n).astype("<f4").tobytes())
+        else:
+            maxindx = int(maxindx if maxindx is not None else max(nums))
+            if len(nums) != n or min(nums) < 1 or max(nums) > maxindx or len(set(nums)) != n:
+                raise ValueError("indexed stack: numbers must be distinct, in 1..maxindx")
+            h = _make_header(nx, ny, 1, iform, istack=0, maxim=max(nums))
+            h[23] = -maxindx            # ISTACK = -MAXINDX
+            h[27] = n                   # LASTINDX: highest storage slot in use
+            f.write(h.astype("<f4").tobytes())
+            indxrec = -(-maxindx // nx)
+            index = np.zeros(indxrec * nx, "<i4")
+            for slot, k in enumerate(nums, start=1):
+                index[k - 1] = slot
+            f.write(index.tobytes())
         for i in range(n):
             ang = None if angles is None else angles[i]
-            f.write(_make_header(nx, ny, 1, iform, istack=0, imgnum=i + 1, data=a[i],
+            f.write(_make_header(nx, ny, 1, iform, istack=0, imgnum=nums[i], data=a[i],
                                  angles=ang).astype("<f4").tobytes())
             f.write(a[i].tobytes())
 

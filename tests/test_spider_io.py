@@ -73,3 +73,29 @@ def test_numbers_and_templates():
     assert sio.add_extension("stk@***") == "stk.spi@***"
     with pytest.raises(ValueError):
         sio.read_header(__file__)
+
+
+def test_indexed_stack(tmp_path):
+    """Indexed stacks (ISTACK = -MAXINDX, lunsethdr.f:505-530, 2140-2200):
+    image numbers map to storage slots through the int32 index records."""
+    rng = np.random.default_rng(5)
+    imgs = rng.standard_normal((3, 7, 10)).astype(np.float32)
+    p = tmp_path / "ix.spi"
+    sio.write_stack(p, imgs, numbers=[15, 2, 9], maxindx=17)   # NX = 10: two index records
+    h, _ = sio.read_header(p)
+    assert int(h[23]) == -17
+    got, nums, heads = sio.read_stack(p, [2, 9, 15])
+    assert nums == [2, 9, 15]
+    assert np.array_equal(got, imgs[[1, 2, 0]])
+    assert [int(x[26]) for x in heads] == [2, 9, 15]          # IMGNUM of each stored image
+    every, nums, _ = sio.read_stack(p)                         # every number in the index
+    assert nums == [2, 9, 15] and np.array_equal(every, imgs[[1, 2, 0]])
+    with pytest.raises(ValueError):
+        sio.read_stack(p, [3])
+    # the same file byte-swapped (every word is 4 bytes) reads the same
+    q = tmp_path / "ix_swapped.spi"
+    q.write_bytes(np.frombuffer(p.read_bytes(), "<u4").byteswap().tobytes())
+    got2, _, _ = sio.read_stack(q, [9])
+    assert np.array_equal(got2[0], imgs[2])
+    # and through a template
+    assert np.array_equal(sio.read_images(str(tmp_path / "ix@***"), [15, 2]), imgs[[0, 1]])
