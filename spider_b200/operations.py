@@ -37,6 +37,11 @@ operation    answers (reference prompt order)
              other modes are not provided
 ===========  =====================================================================
 
+The back-projection operations read their images chunk by chunk
+(``sio.stream_images``): the next chunk is read from disk into a second
+pinned buffer while the GPU inserts the current one, instead of one REDVOL
+per image between insertions (bp3f.f:401-430).
+
 The reference shuffles the BP 32F and BP CG 3 half sets with RANDOM_NUMBER
 (bp32f.f:543-553, bpcg.f:1593-1632); here the first sample receives NANG/2
 images chosen by a seeded permutation (``seed``), which keeps the half sizes
@@ -94,40 +99,68 @@ def _half_sets(n, seed):
     return half
 
 
-def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=None):
-    """Run one SPIDER operation; returns a dict of the arrays it wrote."""
+def _pinned_pair(chunk, ny, nx):
+    """Two float32 [chunk, ny, nx] host buffers, page-locked when CUDA is there."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return [torch.empty((chunk, ny, nx), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    except Exception:
+        pass
+    return None
+
+
+def _stream_insert(ctx, src, ang, half, inplane, chunk):
+    """Insert every image of src, chunk by chunk, reading ahead on a thread."""
+    ny, nx = src.shape
+    chunk = max(1, min(len(src), chunk or max(1, (256 << 20) // (4 * nx * ny))))
+    for start, imgs in sio.stream_images(src, chunk, _pinned_pair(chunk, ny, nx)):
+        sl = slice(start, start + len(imgs))
+        ctx.bp_insert(imgs, ang[sl], None if half is None else half[sl],
+                      inplane=None if inplane is None else inplane[sl])
+
+
+def run(op: str, answers, *, ext: str = "spi", ctx=None, seed: int = 0, results=None, chunk=None):
+    """Run one SPIDER operation; returns a dict of the arrays it wrote.
+    ``chunk``: images per insertion call of the back-projection operations
+    (default: about 256 MB of images)."""
     results = results or sys.stdout
     op = " ".join(op.upper().split())
     a = [str(x) for x in answers]
     ctx = ctx or ops.default_context()
     if op in ("BP 3F", "BP 32F", "RB 3F", "RB 32F", "BP 3F P"):
         numbers = sio.parse_numbers(a[1])
-        imgs = sio.read_images(a[0], numbers, ext)
-        if imgs.shape[1] != imgs.shape[2]:
-            raise ops.SpiderError(101, "ONLY WORKS ON SQUARE IMAGES")
+        src = sio.ImageSource(a[0], numbers, ext)
+        ny, nx = src.shape
+        if ny != nx:
+            raise ops.SpiderError(101, "ONLY WORKS ON SQUARE IMAGES")   # bp3f.f:135-138
         print(f"  NUMBER OF IMAGES: {len(numbers):7d}", file=results)
         ang = _angles(_name(a[2], ext), numbers)
         sym = _symmetries(a[3] if a[3].strip() == "*" else _name(a[3], ext))
         inplane = _inplane(_name(a[2], ext), numbers) if op.startswith("RB") else None
+        half = _half_sets(len(numbers), seed) if op in ("BP 32F", "RB 32F") else None
+        ctx.bp_open(nx, 1 if half is None else 2, sym)
+        try:
+            _stream_insert(ctx, src, ang, half, inplane, chunk)
+            if op == "BP 3F P":
+                x, w = ctx.bp_partial_out(0)
+            elif half is None:
+                vol = ctx.bp_finish(("all",))["all"]
+            else:
+                o = ctx.bp_finish(("all", "1", "2"))
+                v_all, v1, v2 = o["all"], o["1"], o["2"]
+        finally:
+            ctx.bp_close()
         if op == "BP 3F P":
-            x, w = ops.bp3f_partial(imgs, ang, sym, ctx=ctx)
-            nx = imgs.shape[1]
             xv = x.reshape(2 * nx, 2 * nx, 2 * (nx + 1))
             out = _name(a[4], ext)
             sio.write_image(out, xv)
             base, e = os.path.splitext(out)
             sio.write_image(f"{base}_W{e}", w)
             return {"x": x, "w": w}
-        if op in ("BP 3F", "RB 3F"):
-            vol = ops.rb3f(imgs, ang, inplane, sym, ctx=ctx) if inplane is not None else \
-                ops.bp3f(imgs, ang, sym, ctx=ctx)
+        if half is None:
             sio.write_image(_name(a[4], ext), vol)
             return {"vol": vol}
-        half = _half_sets(len(numbers), seed)
-        if inplane is not None:
-            v_all, v1, v2 = ops.rb32f(imgs, ang, inplane, half, sym, ctx=ctx)
-        else:
-            v_all, v1, v2 = ops.bp32f(imgs, ang, half, sym, ctx=ctx)
         sio.write_image(_name(a[4], ext), v_all)
         sio.write_image(_name(a[5], ext), v1)
         sio.write_image(_name(a[6], ext), v2)

@@ -286,3 +286,103 @@ def read_images(template: str, numbers, ext: str = "spi"):
         return imgs
     arrs = [read_image(expand_template(t, k))[0] for k in numbers]
     return np.stack(arrs).astype(np.float32)
+
+
+# ----------------------------------------------------------------- streaming
+class ImageSource:
+    """The images named by a template and file numbers ('jnk***' files or a
+    'stk@***' stack / indexed stack), read by position without loading them
+    all: ``shape`` = (ny, nx); ``read_into(start, out)`` fills out[:count]
+    with images numbers[start:start+count]."""
+
+    def __init__(self, template: str, numbers, ext: str = "spi"):
+        self.numbers = list(numbers)
+        if not self.numbers:
+            raise ValueError("no images")
+        t = add_extension(template, ext)
+        self.stack = "@" in t
+        if self.stack:
+            self.path = t.split("@", 1)[0]
+            h, self.order = read_header(self.path)
+            nx, ny, nz, labbyt = _geom(h)
+            if nz != 1:
+                raise ValueError(f"{self.path}: stack of volumes, images expected")
+            istack = int(h[23])
+            if istack == 0:
+                raise ValueError(f"{self.path}: not a stack")
+            self._per = labbyt + nx * ny * 4
+            self._labbyt = labbyt
+            self._base = labbyt
+            self._slot = {}
+            if istack < 0:
+                maxindx = -istack
+                indxrec = -(-maxindx // nx)
+                with open(self.path, "rb") as f:
+                    f.seek(labbyt)
+                    index = np.frombuffer(f.read(indxrec * nx * 4), dtype=self.order + "i4")[:maxindx]
+                self._base = labbyt + indxrec * nx * 4
+                for k in self.numbers:
+                    if k < 1 or k > len(index) or index[k - 1] <= 0:
+                        raise ValueError(f"{self.path}: image {k} not in the indexed stack")
+                    self._slot[k] = int(index[k - 1])
+            else:
+                maxim = int(h[25])
+                for k in self.numbers:
+                    if k < 1 or k > maxim:
+                        raise ValueError(f"{self.path}: image {k} not in stack (MAXIM {maxim})")
+                    self._slot[k] = k
+        else:
+            self.template = t
+            h, _ = read_header(expand_template(t, self.numbers[0]))
+            nx, ny, _, _ = _geom(h)
+        self.shape = (ny, nx)
+
+    def __len__(self):
+        return len(self.numbers)
+
+    def read_into(self, start: int, out: np.ndarray) -> int:
+        """Read up to len(out) images from position start into out; returns the count."""
+        ny, nx = self.shape
+        count = min(len(out), len(self.numbers) - start)
+        if not self.stack:
+            for i in range(count):
+                img, _ = read_image(expand_template(self.template, self.numbers[start + i]))
+                if img.shape != (ny, nx):
+                    raise ValueError(f"image {self.numbers[start + i]}: size {img.shape} differs from {(ny, nx)}")
+                out[i] = img
+            return count
+        with open(self.path, "rb", buffering=0) as f:
+            for i in range(count):
+                f.seek(self._base + (self._slot[self.numbers[start + i]] - 1) * self._per + self._labbyt)
+                dst = out[i]
+                if f.readinto(memoryview(dst).cast("B")) != nx * ny * 4:
+                    raise ValueError(f"{self.path}: truncated data")
+                if self.order == ">":
+                    dst.byteswap(inplace=True)
+        return count
+
+
+def stream_images(src: "ImageSource", chunk: int, buffers=None):
+    """Yield (start, images[count, ny, nx]) chunk by chunk.  The next chunk is
+    read on a background thread while the caller works on the current one, so
+    reading overlaps the caller's compute (for example a GPU insertion called
+    through ctypes, which releases the GIL).  A yielded array is valid until
+    the generator is resumed twice; ``buffers`` may pass two preallocated
+    float32 arrays [chunk, ny, nx] (pinned host memory, for instance)."""
+    from concurrent.futures import ThreadPoolExecutor
+    ny, nx = src.shape
+    n = len(src)
+    chunk = max(1, min(int(chunk), n))
+    if buffers is None:
+        buffers = [np.empty((chunk, ny, nx), np.float32) for _ in range(2)]
+    with ThreadPoolExecutor(max_workers=1) as pool:
+        pending = pool.submit(src.read_into, 0, buffers[0][:chunk])
+        start, i = 0, 0
+        while start < n:
+            count = pending.result()
+            cur = buffers[i % 2]
+            nxt = start + count
+            if nxt < n:
+                pending = pool.submit(src.read_into, nxt, buffers[(i + 1) % 2][:chunk])
+            yield start, cur[:count]
+            start, i = nxt, i + 1

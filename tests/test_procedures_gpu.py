@@ -93,6 +93,44 @@ def test_bpcg_fbs_procedure(ctx, orc, tmp_path):
     print(f"  BP CG F  Range: {vol.min():12.5E}...{vol.max():12.5E}")
 
 
+@pytest.mark.parametrize("indexed", [False, True])
+def test_streamed_bp32f_and_rb32f_procedures(ctx, tmp_path, indexed):
+    """BP 32F / RB 32F read their stack in chunks (next chunk read while the
+    current one is inserted); the volumes equal the one-call array operation
+    up to the order of the atomic sums."""
+    rng = np.random.default_rng(8)
+    n, nx = 150, 32
+    vol = synth.blob_phantom(nx, 8, sigma=(1.5, 4.0), radius=10, rng=rng)
+    ang = synth.so3_angles(n, rng)
+    import oracle
+    pr = oracle.pj3q(vol, ang)
+    inplane = np.stack([rng.uniform(-20, 20, n), rng.uniform(-2, 2, n), rng.uniform(-2, 2, n)], 1)
+    t = str(tmp_path)
+    if indexed:   # numbers 200, 199, ... stored in slots 1, 2, ...
+        sio.write_stack(tmp_path / "stk.spi", pr[::-1], numbers=list(range(51, 201)), maxindx=250)
+        numbers = list(range(51, 201))
+        keys = numbers
+    else:
+        sio.write_stack(tmp_path / "stk.spi", pr)
+        numbers = list(range(1, n + 1))
+        keys = numbers
+    order = pr[::-1] if indexed else pr
+    sio.write_doc(tmp_path / "ang.spi", [list(ang[i]) + [0, 0] + list(inplane[i]) for i in range(n)], keys=keys)
+    doc = sio.read_doc(tmp_path / "ang.spi")
+    ang_d = np.array([doc[k][:3] for k in keys], np.float32)
+    ip_d = np.array([doc[k][5:8] for k in keys], np.float32)
+    spec = f"{numbers[0]}-{numbers[-1]}"
+    for op, extra in (("BP 32F", []), ("RB 32F", ["*"])):
+        r = operations.run(op, [f"{t}/stk@***", spec, f"{t}/ang", "*", f"{t}/v", f"{t}/v1", f"{t}/v2"] + extra,
+                           ctx=ctx, results=io.StringIO(), chunk=40)
+        if op == "BP 32F":
+            ref = ops.bp32f(order, ang_d, r["half"], ctx=ctx)
+        else:
+            ref = ops.rb32f(order, ang_d, ip_d, r["half"], ctx=ctx)
+        for got, want in zip((r["vol"], r["vol1"], r["vol2"]), ref):
+            assert synth.rel_l2(got, want) <= 1e-6, op
+
+
 def test_pj3q_and_partial_merge_procedures(ctx, orc, tmp_path):
     t = str(tmp_path)
     rng = np.random.default_rng(5)

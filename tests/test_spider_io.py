@@ -99,3 +99,30 @@ def test_indexed_stack(tmp_path):
     assert np.array_equal(got2[0], imgs[2])
     # and through a template
     assert np.array_equal(sio.read_images(str(tmp_path / "ix@***"), [15, 2]), imgs[[0, 1]])
+
+
+@pytest.mark.parametrize("kind", ["files", "stack", "indexed"])
+@pytest.mark.parametrize("chunk", [1, 4, 7, 100])
+def test_stream_images(tmp_path, kind, chunk):
+    """stream_images yields the images in file-number order, chunk by chunk,
+    from image files, a stack or an indexed stack (read ahead on a thread)."""
+    rng = np.random.default_rng(11)
+    imgs = rng.standard_normal((10, 6, 6)).astype(np.float32)
+    if kind == "files":
+        for i in range(10):
+            sio.write_image(tmp_path / f"im{i + 1:03d}.spi", imgs[i])
+        tmpl, numbers, want = str(tmp_path / "im***"), [3, 1, 10, 4], imgs[[2, 0, 9, 3]]
+    elif kind == "stack":
+        sio.write_stack(tmp_path / "st.spi", imgs)
+        tmpl, numbers, want = str(tmp_path / "st@***"), list(range(10, 0, -1)), imgs[::-1]
+    else:
+        sio.write_stack(tmp_path / "ix.spi", imgs, numbers=[20 - i for i in range(10)], maxindx=25)
+        tmpl, numbers, want = str(tmp_path / "ix@***"), [11, 20, 15], imgs[[9, 0, 5]]
+    src = sio.ImageSource(tmpl, numbers)
+    assert src.shape == (6, 6) and len(src) == len(numbers)
+    got, starts = [], []
+    for start, c in sio.stream_images(src, chunk):
+        starts.append(start)
+        got.append(c.copy())
+    assert np.array_equal(np.concatenate(got), want)
+    assert starts == list(range(0, len(numbers), min(chunk, len(numbers))))
