@@ -1134,6 +1134,7 @@ struct FbsState {
   void* pt = nullptr;       // T [K][n][n] projections of the iteration
   int2* segs = nullptr;     // {run, first offset} per BCKPJ_FBS segment
   long long nseg = 0;
+  int seg = kFbsSeg;        // voxels per BCKPJ_FBS segment
   float* dm9 = nullptr;     // 9 floats per merged angle
   size_t tsz = 8;           // bytes per table value (FP32 tables in precision modes 2 and 3)
   FbsState() = default;
@@ -1159,10 +1160,14 @@ static int fbs_setup(spi_ctx* c, const CgProblem& pb, int nang, FbsState& fs, si
     if (k > 0 && k < fs.K) fs.K = k;
   }
   const size_t K = (size_t)fs.K;
+  if (const char* e = getenv("SPI_FBS_SEG")) {   // 2, 4 or 8 voxels per back-projector thread
+    const int v = atoi(e);
+    if (v == 2 || v == 4 || v == 8) fs.seg = v;
+  }
   std::vector<int2> segs;
   for (size_t r = 0; r < pb.runs.size(); ++r) {
     const int len = pb.runs[r].l2 - pb.runs[r].l1 + 1;
-    for (int o = 0; o < len; o += kFbsSeg) segs.push_back(make_int2((int)r, o));
+    for (int o = 0; o < len; o += fs.seg) segs.push_back(make_int2((int)r, o));
   }
   fs.nseg = (long long)segs.size();
   const size_t b3[2] = {fbs3_work_bytes(n), align256(nnn * 8 * tsz)};
@@ -1216,8 +1221,13 @@ template <class T, class TT>
 static int fbs_backproject(spi_ctx* c, const CgProblem& pb, FbsState& fs, T* cube, const TT* P2, const CgDM* dms,
                            int kc) {
   if (fs.nseg == 0 || kc <= 0) return 0;
-  bckpj_fbs_kernel<T, TT><<<blocks_for(c, fs.nseg, 256), 256, 0, c->stream>>>(
-      cube, c->cg_buf[0].as<CgRun>(), fs.segs, fs.nseg, P2, dms, kc, pb.n, pb.ldp);
+  auto launch = [&](auto kern) {
+    kern<<<blocks_for(c, fs.nseg, 256), 256, 0, c->stream>>>(cube, c->cg_buf[0].as<CgRun>(), fs.segs, fs.nseg, P2,
+                                                             dms, kc, pb.n, pb.ldp);
+  };
+  if (fs.seg == 2) launch(bckpj_fbs_kernel<T, TT, 2>);
+  else if (fs.seg == 8) launch(bckpj_fbs_kernel<T, TT, 8>);
+  else launch(bckpj_fbs_kernel<T, TT, 4>);
   SPI_TRY(check_kernel("bckpj_fbs_kernel"));
   c->count();
   return 0;

@@ -27,7 +27,9 @@
 // I samples per line between two row reductions (PRJCQ_FBS3): the shared
 // tile takes L1 from the gathers, and 16 measured as fast as 8 and faster than 32
 constexpr int kFbsIC = 16;
-constexpr int kFbsSeg = 8;   // run voxels per thread (BCKPJ_FBS)
+// run voxels per BCKPJ_FBS thread: 4 measured fastest over 128^3 and 256^3
+// (2 is 4% faster at 128^3 and 8% slower at 256^3; 8 and 16 are slower)
+constexpr int kFbsSeg = 4;
 
 template <class T> struct FbsQuad { T a, b, c, d; };
 
@@ -232,11 +234,11 @@ __global__ void __launch_bounds__(MAXT) prjcq_fbs3_kernel(const TT* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// BCKPJ_FBS: thread per segment of up to kFbsSeg voxels of a run.  For each
+// BCKPJ_FBS: thread per segment of up to SEG voxels of a run.  For each
 // projection, in order, the thread repeats the run's sequential walk up to
 // its segment, then adds FBS2 at each of its voxels.  segs[s] = {run, first
 // offset within the run}.
-template <class T, class TT>
+template <class T, class TT, int SEG>
 __global__ void __launch_bounds__(256) bckpj_fbs_kernel(T* __restrict__ cube, const CgRun* __restrict__ runs,
                                                         const int2* __restrict__ segs, long long nseg,
                                                         const TT* __restrict__ P2, const CgDM* __restrict__ dms,
@@ -245,11 +247,11 @@ __global__ void __launch_bounds__(256) bckpj_fbs_kernel(T* __restrict__ cube, co
     const int2 sg = segs[s];
     const CgRun r = runs[sg.x];
     const int o0 = sg.y;
-    const int len = min(kFbsSeg, r.l2 - r.l1 + 1 - o0);
+    const int len = min(SEG, r.l2 - r.l1 + 1 - o0);
     const size_t lin = (size_t)r.l1 - 1 + o0;
-    T c[kFbsSeg];
+    T c[SEG];
 #pragma unroll
-    for (int t = 0; t < kFbsSeg; ++t) c[t] = t < len ? cube[lin + t] : (T)0;
+    for (int t = 0; t < SEG; ++t) c[t] = t < len ? cube[lin + t] : (T)0;
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
     for (int k = 0; k < kc; ++k) {
       const CgDM dm = dms[k];
@@ -261,14 +263,14 @@ __global__ void __launch_bounds__(256) bckpj_fbs_kernel(T* __restrict__ cube, co
       }
       const TT* P = P2 + (size_t)k * n * n * 4;
 #pragma unroll
-      for (int t = 0; t < kFbsSeg; ++t) {
+      for (int t = 0; t < SEG; ++t) {
         if (t < len) c[t] = radd(c[t], fbs2_eval<T, TT>(xb, yb, n, P));
         xb = __fadd_rn(xb, dm.d[0]);
         yb = __fadd_rn(yb, dm.d[3]);
       }
     }
 #pragma unroll
-    for (int t = 0; t < kFbsSeg; ++t)
+    for (int t = 0; t < SEG; ++t)
       if (t < len) cube[lin + t] = c[t];
   }
 }
