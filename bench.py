@@ -508,6 +508,7 @@ def run_ours(args):
                                       halves[i].ctypes.data_as(ctypes.c_void_p), 0))
         if world > 1:
             import torch.distributed as dist
+            torch.cuda.synchronize()   # the last insertions run on the library stream
             for g in grids:
                 dist.all_reduce(g)
             torch.cuda.synchronize()

@@ -123,7 +123,8 @@ int spi_bp_get_launch(const spi_ctx* ctx, int* kernel, int* threads, int* blocks
  * (float[nimg*3], host) and optional half mask (uint8[nimg], host; NULL
  * routes every image to grid 0).  Replaces the body of the BP3FQ image loop
  * (bp3f.f:403-493) and of BP32FQ's (bp32f.f:809-913).  Images may be host or
- * device memory (`imgs_on_device`). */
+ * device memory (`imgs_on_device`); the call returns when the images are in
+ * the grids. */
 int spi_bp_insert(spi_ctx* ctx, const float* imgs, int nimg, const float* angles,
                   const uint8_t* half, int imgs_on_device);
 
