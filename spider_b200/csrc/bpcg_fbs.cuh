@@ -45,6 +45,25 @@ __device__ __forceinline__ FbsQuad<double> fbs_ldq(const double* p) {
   return q;
 }
 
+// one voxel of an FBS3 table: its value quad {F, X1, Y1, XY2} and its
+// z-derivative quad {Z1, XZ2, YZ2, XYZ}.  An FP32 voxel is one 32-byte
+// sector, read by one 256-bit load; an FP64 voxel by two.
+template <class T>
+__device__ __forceinline__ void fbs_ldvox(const float* p, FbsQuad<T>& val, FbsQuad<T>& der) {
+  float a[8];
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+      : "l"(p));
+  val = {(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  der = {(T)a[4], (T)a[5], (T)a[6], (T)a[7]};
+}
+template <class T>
+__device__ __forceinline__ void fbs_ldvox(const double* p, FbsQuad<T>& val, FbsQuad<T>& der) {
+  const FbsQuad<double> u = fbs_ldq(p), w = fbs_ldq(p + 4);
+  val = {(T)u.a, (T)u.b, (T)u.c, (T)u.d};
+  der = {(T)w.a, (T)w.b, (T)w.c, (T)w.d};
+}
+
 // a table quad (type TT) widened to the arithmetic type T
 template <class T, class TT>
 __device__ __forceinline__ FbsQuad<T> fbs_ld(const TT* p) {
@@ -110,10 +129,13 @@ __device__ __forceinline__ T fbs3_eval(float x, float y, float z, int i, int j, 
   for (int p = 0; p < 2; ++p) {
     const TT* b = V + v0 + p * sz;
     // value plane: F, X1, Y1, XY2; z-derivative plane: Z1, XZ2, YZ2, XYZ
-    c[p] = fbs_bicubic(fbs_ld<T>(b), fbs_ld<T>(b + 8), fbs_ld<T>(b + sy), fbs_ld<T>(b + sy + 8), dx, dx2, dx3, dy,
-                       dy2, dy3);
-    dc[p] = fbs_bicubic(fbs_ld<T>(b + 4), fbs_ld<T>(b + 12), fbs_ld<T>(b + sy + 4), fbs_ld<T>(b + sy + 12), dx, dx2,
-                        dx3, dy, dy2, dy3);
+    FbsQuad<T> v00, v10, v01, v11, d00, d10, d01, d11;
+    fbs_ldvox<T>(b, v00, d00);
+    fbs_ldvox<T>(b + 8, v10, d10);
+    fbs_ldvox<T>(b + sy, v01, d01);
+    fbs_ldvox<T>(b + sy + 8, v11, d11);
+    c[p] = fbs_bicubic(v00, v10, v01, v11, dx, dx2, dx3, dy, dy2, dy3);
+    dc[p] = fbs_bicubic(d00, d10, d01, d11, dx, dx2, dx3, dy, dy2, dy3);
   }
   return fbs_cub(c[0], dc[0], c[1], dc[1], dz, dz2, dz3);
 }
@@ -134,10 +156,13 @@ __device__ __forceinline__ T fbs3_eval_wrap(float x, float y, float z, int n, co
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     const int ll = p ? l3 : l2;
-    const TT *q00 = at(i2, j2, ll), *q10 = at(i3, j2, ll), *q01 = at(i2, j3, ll), *q11 = at(i3, j3, ll);
-    c[p] = fbs_bicubic(fbs_ld<T>(q00), fbs_ld<T>(q10), fbs_ld<T>(q01), fbs_ld<T>(q11), dx, dx2, dx3, dy, dy2, dy3);
-    dc[p] = fbs_bicubic(fbs_ld<T>(q00 + 4), fbs_ld<T>(q10 + 4), fbs_ld<T>(q01 + 4), fbs_ld<T>(q11 + 4), dx, dx2,
-                        dx3, dy, dy2, dy3);
+    FbsQuad<T> v00, v10, v01, v11, d00, d10, d01, d11;
+    fbs_ldvox<T>(at(i2, j2, ll), v00, d00);
+    fbs_ldvox<T>(at(i3, j2, ll), v10, d10);
+    fbs_ldvox<T>(at(i2, j3, ll), v01, d01);
+    fbs_ldvox<T>(at(i3, j3, ll), v11, d11);
+    c[p] = fbs_bicubic(v00, v10, v01, v11, dx, dx2, dx3, dy, dy2, dy3);
+    dc[p] = fbs_bicubic(d00, d10, d01, d11, dx, dx2, dx3, dy, dy2, dy3);
   }
   return fbs_cub(c[0], dc[0], c[1], dc[1], dz, dz2, dz3);
 }
