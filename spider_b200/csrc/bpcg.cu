@@ -350,10 +350,12 @@ __global__ void __launch_bounds__(512) prjcq_projt_kernel(const T* __restrict__ 
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
     float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
     float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    T cnext = cube[(size_t)r.l1 - 1];   // the next voxel's value, loaded one step ahead
     for (int j = r.l1; j <= r.l2; ++j) {
+      const T cv = cnext;
+      if (j < r.l2) cnext = cube[(size_t)j];
       const int iqx = __float2int_rz(xb), iqy = __float2int_rz(yb);
       if (iqx >= 1 && iqx < n && iqy >= 1 && iqy < n) {
-        const T cv = cube[(size_t)j - 1];
         const T dx = (T)__fsub_rn(xb, (float)iqx);
         const T dy = rmul((T)__fsub_rn(yb, (float)iqy), cv);
         const T dx1m = rsub((T)1, dx);
