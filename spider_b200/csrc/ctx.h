@@ -66,6 +66,7 @@ struct spi_ctx {
   // ---- PJ 3Q / BP CG scratch ----
   spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
   spi::DevBuf pj_fbs;                 // PJ 3F: FBS3_PREP scratch + the FBS3 table
+  spi::DevBuf pj_v4;                  // PJ 3Q: the volume as float4 quads of x/y neighbours
   spi::DevBuf cg_buf[8];
   spi::DevBuf cg_fbs[4];              // FBS: 3D scratch + table, 2D chunk scratch, segments, DM(1..9)
   spi::HostBuf hbuf;

@@ -9,7 +9,8 @@ from spider_b200 import ops, synth
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64), (40, 36, 33)])
+# (200, 192, 188): above 6M voxels, the unpacked-volume kernel; the others use x/y-neighbour quads
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64), (40, 36, 33), (200, 192, 188)])
 def test_pj3q_matches_oracle(ctx, orc, shape):
     nz, ny, nx = shape
     rng = np.random.default_rng(sum(shape))
