@@ -81,8 +81,10 @@ def test_cg_reconstruct_dense_fp64_and_gradients(ctx, orc):
     x = autograd.cg_reconstruct(bt, solver)
     assert synth.rel_l2(x.detach().cpu().numpy().ravel(), x_ref) <= 1e-4
     plain = autograd.cg_reconstruct(bt.detach(), autograd.NormalCG(plan, lam, iters, graph=False))
-    # the adjoint scatters with FP32 atomics, so two runs differ in summation order
-    assert synth.rel_l2(plain.cpu().numpy(), x.detach().cpu().numpy()) <= 1e-5
+    # the projector and the adjoint sum with FP32 atomics, so two runs differ
+    # in summation order, and 80 iterations at lambda 0.2 amplify it (measured
+    # 3e-6 .. 1.4e-5 between runs): held to the same bar as the solution
+    assert synth.rel_l2(plain.cpu().numpy(), x.detach().cpu().numpy()) <= 1e-4
     loss = (x.double() * torch.tensor(w, device="cuda")).sum()
     loss.backward()
     grad = bt.grad.detach().cpu().numpy().ravel()
