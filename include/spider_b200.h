@@ -218,9 +218,10 @@ int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, f
  * allocate nothing and do not synchronise, so they can be captured in a
  * CUDA graph.  The forward equals spi_pj3q, the adjoint spi_pj3q_adjoint;
  * both overwrite their output.  Besides the runs and matrices a plan for a
- * volume of up to 6M voxels holds a 16-byte-per-voxel copy of it in
- * x/y-neighbour quads, refreshed by every forward call.  A plan keeps a
- * pointer to its context for launch counting and must be destroyed before it. */
+ * volume of up to 6M voxels holds two 16-byte-per-voxel buffers: the volume
+ * in x/y-neighbour quads (refreshed by every forward call) and the adjoint's
+ * quad accumulator.  A plan keeps a pointer to its context for launch
+ * counting and must be destroyed before it. */
 typedef struct spi_pj3q_plan spi_pj3q_plan;
 int spi_pj3q_plan_create(spi_ctx* ctx, int nx, int ny, int nz, float ri, const float* angles, int nang,
                          spi_pj3q_plan** out);

@@ -241,6 +241,85 @@ __global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restri
   }
 }
 
+// The adjoint into x/y-neighbour quads: a sample's eight trilinear weights
+// are two float4 adds (planes z and z+1) to the quad of its cell, whose
+// origin is the cell's lowest corner; the two quads of the current cell stay
+// in registers while the walk stays in it.  Every weight is the one
+// wpro_adjoint_kernel adds to the same voxel; pj_unfold4_kernel then sums
+// the four quads that hold a voxel.  Two 16-byte vector atomics per cell
+// instead of about 3.6 scalar L2 requests per sample (measured at 128^3,
+// where the adjoint is bound by L2 throughput).
+__global__ void __launch_bounds__(128) wpro_adjoint4_kernel(const float* __restrict__ proj, int nsam, int nrow,
+                                                            int nslice, const PjRun* __restrict__ runs, int nruns,
+                                                            const PjDM* __restrict__ dms, int nang, int ldpx,
+                                                            int ldpy, int ldpz, float4* __restrict__ q4) {
+  const long long total = (long long)nruns * nang;
+  const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t / nruns);
+    const PjRun r = runs[t % nruns];
+    const PjDM dm = dms[a];
+    const float* b = proj + (size_t)a * nsam * nrow;
+    const int k = r.y + ldpy;
+    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
+    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
+    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    int cx = 0, cy = 0, cz = 0;   // cached cell (1-based lowest corner; 0 = none)
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+    auto flush = [&]() {
+      if (cx > 0) {
+        float4* p0 = q4 + (size_t)(cz - 1) * sz + (size_t)(cy - 1) * sy + (cx - 1);
+        atomicAdd(p0, a0);
+        atomicAdd(p0 + sz, a1);
+      }
+    };
+    for (int j = r.i1; j <= r.i2; ++j) {
+      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
+        const float p = __ldg(b + (size_t)(k - 1) * nsam + (j - 1));
+        if (p != 0.0f) {
+          const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
+          const float ex = 1.0f - dx, ey = 1.0f - dy, ez = 1.0f - dz;
+          if (iox != cx || ioy != cy || ioz != cz) {
+            flush();
+            cx = iox; cy = ioy; cz = ioz;
+            a0 = make_float4(0.f, 0.f, 0.f, 0.f);
+            a1 = a0;
+          }
+          a0.x += p * ex * ey * ez;
+          a0.y += p * dx * ey * ez;
+          a0.z += p * ex * dy * ez;
+          a0.w += p * dx * dy * ez;
+          a1.x += p * ex * ey * dz;
+          a1.y += p * dx * ey * dz;
+          a1.z += p * ex * dy * dz;
+          a1.w += p * dx * dy * dz;
+        }
+      }
+      xb = __fadd_rn(xb, dm.d[0]);
+      yb = __fadd_rn(yb, dm.d[1]);
+      zb = __fadd_rn(zb, dm.d[2]);
+    }
+    flush();
+  }
+}
+
+// voxel (x, y, z) = its share of the quads with origins (x, y), (x-1, y),
+// (x, y-1) and (x-1, y-1) in plane z
+__global__ void pj_unfold4_kernel(const float4* __restrict__ q4, int nsam, int nrow, int nslice,
+                                  float* __restrict__ cube) {
+  const size_t total = (size_t)nsam * nrow * nslice;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(q % nsam);
+    const int y = (int)((q / nsam) % nrow);
+    float v = q4[q].x;
+    if (x > 0) v += q4[q - 1].y;
+    if (y > 0) v += q4[q - nsam].z;
+    if (x > 0 && y > 0) v += q4[q - nsam - 1].w;
+    cube[q] = v;
+  }
+}
+
 void pj_release(spi_ctx* c) {
   c->pj_vol.release();
   c->pj_out.release();
@@ -337,15 +416,29 @@ int spi_pj3q_adjoint(spi_ctx* c, const float* projs, int nx, int ny, int nz, flo
     dp = c->pj_out.as<float>();
     dvol = c->pj_vol.as<float>();
   }
-  SPI_CUDA(cudaMemsetAsync(dvol, 0, vbytes, c->stream));
   const long long total = (long long)nruns * nang;
   int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
-  if (blocks > 0) {
-    wpro_adjoint_kernel<<<blocks, 128, 0, c->stream>>>(dp, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
-                                                       c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1,
-                                                       dvol);
-    SPI_TRY(check_kernel("wpro_adjoint_kernel"));
-    c->count();
+  const size_t nvox = (size_t)nx * ny * nz;
+  if (blocks > 0 && nvox * sizeof(float4) <= kQuadMaxBytes) {
+    SPI_TRY(c->pj_v4.ensure(nvox * sizeof(float4)));
+    SPI_CUDA(cudaMemsetAsync(c->pj_v4.p, 0, nvox * sizeof(float4), c->stream));
+    wpro_adjoint4_kernel<<<blocks, 128, 0, c->stream>>>(dp, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
+                                                        c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1,
+                                                        nz / 2 + 1, c->pj_v4.as<float4>());
+    SPI_TRY(check_kernel("wpro_adjoint4_kernel"));
+    pj_unfold4_kernel<<<(int)std::min<size_t>((nvox + 255) / 256, (size_t)c->sm_count * 16), 256, 0, c->stream>>>(
+        c->pj_v4.as<float4>(), nx, ny, nz, dvol);
+    SPI_TRY(check_kernel("pj_unfold4_kernel"));
+    c->count(2);
+  } else {
+    SPI_CUDA(cudaMemsetAsync(dvol, 0, vbytes, c->stream));
+    if (blocks > 0) {
+      wpro_adjoint_kernel<<<blocks, 128, 0, c->stream>>>(dp, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
+                                                         c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1,
+                                                         nz / 2 + 1, dvol);
+      SPI_TRY(check_kernel("wpro_adjoint_kernel"));
+      c->count();
+    }
   }
   if (!on_device) SPI_CUDA(cudaMemcpyAsync(vol_out, dvol, vbytes, cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -366,6 +459,7 @@ struct spi_pj3q_plan {
   PjRun* runs = nullptr;
   PjDM* dms = nullptr;
   float4* v4 = nullptr;   // quad-packed volume of the forward projection
+  float4* q4 = nullptr;   // quad accumulator of the adjoint
 };
 
 extern "C" {
@@ -385,8 +479,10 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   p->blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
   cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
   if (e == cudaSuccess) e = cudaMalloc(&p->dms, (size_t)nang * sizeof(PjDM));
-  if (e == cudaSuccess && (size_t)nx * ny * nz * sizeof(float4) <= kQuadMaxBytes)
+  if (e == cudaSuccess && (size_t)nx * ny * nz * sizeof(float4) <= kQuadMaxBytes) {
     e = cudaMalloc(&p->v4, (size_t)nx * ny * nz * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&p->q4, (size_t)nx * ny * nz * sizeof(float4));
+  }
   if (e == cudaSuccess && nruns)
     e = cudaMemcpyAsync(p->runs, c->pj_runs.p, (size_t)nruns * sizeof(PjRun), cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess)
@@ -396,6 +492,7 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
     cudaFree(p->runs);
     cudaFree(p->dms);
     cudaFree(p->v4);
+    cudaFree(p->q4);
     delete p;
     return fail(kCuda, "spi_pj3q_plan_create: %s", cudaGetErrorString(e));
   }
@@ -428,7 +525,19 @@ int spi_pj3q_plan_forward(const spi_pj3q_plan* p, const float* vol, float* proj_
 int spi_pj3q_plan_adjoint(const spi_pj3q_plan* p, const float* projs, float* vol_out, void* stream) {
   if (!p || !projs || !vol_out) return fail(kInvalid, "spi_pj3q_plan_adjoint: NULL argument");
   auto st = static_cast<cudaStream_t>(stream);
-  SPI_CUDA(cudaMemsetAsync(vol_out, 0, (size_t)p->nx * p->ny * p->nz * sizeof(float), st));
+  const size_t nvox = (size_t)p->nx * p->ny * p->nz;
+  if (p->q4 && p->blocks > 0) {
+    SPI_CUDA(cudaMemsetAsync(p->q4, 0, nvox * sizeof(float4), st));
+    wpro_adjoint4_kernel<<<p->blocks, 128, 0, st>>>(projs, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
+                                                    p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, p->q4);
+    SPI_TRY(check_kernel("wpro_adjoint4_kernel"));
+    pj_unfold4_kernel<<<(int)std::min<size_t>((nvox + 255) / 256, (size_t)p->ctx->sm_count * 16), 256, 0, st>>>(
+        p->q4, p->nx, p->ny, p->nz, vol_out);
+    SPI_TRY(check_kernel("pj_unfold4_kernel"));
+    p->ctx->count(2);
+    return 0;
+  }
+  SPI_CUDA(cudaMemsetAsync(vol_out, 0, nvox * sizeof(float), st));
   if (p->blocks > 0) {
     wpro_adjoint_kernel<<<p->blocks, 128, 0, st>>>(projs, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
                                                    p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, vol_out);
@@ -444,6 +553,7 @@ int spi_pj3q_plan_destroy(spi_pj3q_plan* p) {
   cudaFree(p->runs);
   cudaFree(p->dms);
   cudaFree(p->v4);
+  cudaFree(p->q4);
   delete p;
   return 0;
 }
