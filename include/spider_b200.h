@@ -241,6 +241,26 @@ int spi_bpcg(spi_ctx* ctx, const float* projs, int n, int nang, const float* ang
              float ri, float errm, float chim, int maxit, int mode, float lambda,
              float* vol_out, float* log_out, int* niter_out);
 
+/* BP CG across several processes, one GPU each: the reference's MPI form
+ * (bpcg.f:522-672, 855-1080).  This rank holds images [first, first+count)
+ * of the nang angles (projs = float[count*n*n]; angles = all nang triples);
+ * HIANG runs on every rank over all angles and each rank applies the normal
+ * operator to its SETPART block of the merged list.  `allreduce` is called
+ * with the same sequence on every rank and must sum the device array `data`
+ * (count values, FP64 when fp64 = 1, else FP32) over the ranks in place,
+ * ordered on `stream` (a cudaStream_t: the library's stream; the sum must be
+ * there when work queued on it after the call runs) and return 0: once for
+ * CB and once for the three ASTASQ sums, then once per iteration for BCKE
+ * (the n^3 all-reduce per iteration); the rest of the iteration is
+ * replicated, so every rank returns the same volume and log.  With world = 1
+ * and no callback this is spi_bpcg on images [first, first+count).  Sharded
+ * runs launch each iteration op by op (no CUDA graph). */
+typedef int (*spi_allreduce_fn)(void* data, long long count, int fp64, void* stream, void* user);
+int spi_bpcg_shard(spi_ctx* ctx, const float* projs, int first, int count, int n, int nang,
+                   const float* angles, float ri, float errm, float chim, int maxit, int mode,
+                   float lambda, int rank, int world, spi_allreduce_fn allreduce, void* user,
+                   float* vol_out, float* log_out, int* niter_out);
+
 /* Storage and accumulation type of the BP CG vectors and projections:
  * mode = 1 keeps CB, BCKP, BCKE, BCKN and the projections in FP64 (the
  * reference keeps them in REAL; its FP32 CG drifts from the exact iteration

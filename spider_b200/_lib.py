@@ -16,6 +16,9 @@ _c_u8_p = ctypes.POINTER(ctypes.c_uint8)
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
 
+# spi_allreduce_fn: int (*)(void* data, long long count, int fp64, void* stream, void* user)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, _vp, ctypes.c_longlong, ctypes.c_int, _vp, _vp)
+
 # (name, restype, argtypes) of every exported symbol
 SIGNATURES = [
     ("spi_version", ctypes.c_int, []),
@@ -59,6 +62,10 @@ SIGNATURES = [
     ("spi_pj3q_plan_destroy", ctypes.c_int, [_vp]),
     ("spi_bpcg", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_float, ctypes.c_float,
                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp]),
+    ("spi_bpcg_shard", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_int, ctypes.c_int, ALLREDUCE_FN, _vp, _vp, _vp,
+                                      _vp]),
     ("spi_ctx_set_cg_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_ctx_set_cg_interpolation", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_ctx_set_rb_interpolation", ctypes.c_int, [_vp, ctypes.c_int]),

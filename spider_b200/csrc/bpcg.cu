@@ -1253,11 +1253,11 @@ static int fbs_backproject_images(spi_ctx* c, const CgProblem& pb, FbsState& fs,
 // the direction, then per chunk of merged angles PRJCQ_FBS3 (scaled by LB),
 // FBS2_PREP of the projections and BCKPJ_FBS
 template <class T, class TT>
-static int fbs_normal(spi_ctx* c, const CgProblem& pb, FbsState& fs, const T* bckp, T* bcke, const int* dlb, int lo,
-                      const CgDM* dms) {
+static int fbs_normal(spi_ctx* c, const CgProblem& pb, FbsState& fs, const T* bckp, T* bcke, const int* dlb, int kb,
+                      int ke, const CgDM* dms) {
   SPI_TRY((fbs3_prepare<T, TT>(c, fs.w3, bckp, static_cast<TT*>(fs.V))));
-  for (int k0 = 0; k0 < lo; k0 += fs.K) {
-    const int kc = std::min(fs.K, lo - k0);
+  for (int k0 = kb; k0 < ke; k0 += fs.K) {
+    const int kc = std::min(fs.K, ke - k0);
     SPI_TRY((fbs_project<T, TT>(c, fs, dlb, k0, kc)));
     SPI_TRY((fbs2_prepare<T, TT>(c, fs.w2, static_cast<const T*>(fs.pt), kc, static_cast<TT*>(fs.P2))));
     SPI_TRY((fbs_backproject<T, TT>(c, pb, fs, bcke, static_cast<const TT*>(fs.P2), dms + k0, kc)));
@@ -1265,15 +1265,35 @@ static int fbs_normal(spi_ctx* c, const CgProblem& pb, FbsState& fs, const T* bc
   return 0;
 }
 
-// BPCG_2 + HIANG + BPCG_3_LIN with vectors and projections stored as T
+// One rank's share of a BP CG solve over several processes (the reference's
+// MPI form, bpcg.f:522-672, 855-1080): its images are [first, first+count) of
+// the angle list, its merged angles the SETPART block of HIANG's list, and
+// `reduce` sums a device array over the ranks in place (ALLREDUCE_MPI).
+struct CgShard {
+  int first = 0, count = 0;
+  int rank = 0, world = 1;
+  spi_allreduce_fn reduce = nullptr;
+  void* user = nullptr;
+  int sum(spi_ctx* c, void* data, long long n, bool fp64) const {
+    if (!reduce) return 0;
+    const int st = reduce(data, n, fp64 ? 1 : 0, c->stream, user);
+    if (st != 0) return fail(kInvalid, "BP CG: the all-reduce callback returned %d", st);
+    return 0;
+  }
+};
+
+// BPCG_2 + HIANG + BPCG_3_LIN with vectors and projections stored as T;
+// nang angles in all, this rank's images `projs` = sh.count of them.
 template <class T>
 static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float* angles, float ri, float errm,
-                    float chim, int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out) {
+                    float chim, int maxit, int mode, float lambda, float* vol_out, float* log_out, int* niter_out,
+                    const CgShard& sh) {
   CgProblem pb;
   SPI_TRY(cg_setup(c, n, ri, pb));
   const size_t nnn = (size_t)n * n * n;
   const size_t vb = nnn * sizeof(T);
-  const size_t pcount = (size_t)nang * n * n;
+  const int nimg = sh.count;
+  const size_t pcount = (size_t)nimg * n * n;
   // mixed mode (FP64 vectors, FP32 PROJT tables made per chunk of images)
   // modes 2 and 4: 47-bit fixed-point projections; mode 4 also keeps FP64
   // PROJT tables (mode 2 FP32 tables, mode 3 31-bit and FP32 tables)
@@ -1284,25 +1304,45 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   const bool mixed = !fbs && sizeof(T) == 8 && c->cg_fp64 >= 2 && mixed_fits(n, wide);
   const bool wtab = c->cg_fp64 == 4;
   const size_t pentry = wtab ? sizeof(ProjtEntry<true>) : sizeof(ProjtEntry<false>);
-  const int K = projt_chunk(n, nang, pentry);
+  // ---- HIANG (hiang.f:40-112) over all the angles, and this rank's block of
+  // the merged list.  ang[3*i] = phi, [3*i+1] = theta, [3*i+2] = psi.
+  std::vector<float> ang((size_t)3 * nang);
+  for (int k = 0; k < nang; ++k) {
+    ang[3 * k] = angles[3 * k + 2];
+    ang[3 * k + 1] = angles[3 * k + 1];
+    ang[3 * k + 2] = angles[3 * k];
+  }
+  std::vector<CgDM> mdms;
+  std::vector<int> lb;
+  std::vector<float> dm9;
+  const int lo = hiang(ang, nang, mdms, lb, fbs ? &dm9 : nullptr);
+  // SETPART (setpart.f:4-29): blocks of lo / world, the first lo % world ranks one more
+  const int kq = lo / sh.world, kr = lo % sh.world;
+  const int kb = sh.rank * kq + std::min(sh.rank, kr);
+  const int kc_all = kq + (sh.rank < kr ? 1 : 0);
+  const int ke = kb + kc_all;
+  const int K = projt_chunk(n, std::max(nimg, kc_all), pentry);
+  const int pj_rows = std::max(nimg, kc_all);   // projections of the images, then of the merged block
   // buffers: [3] dms, [4] CB, [5] projections (T) + float staging (mixed: float images + PROJT chunk),
   // [6] BCKN|BCKP|BCKE, [7] scalars + lb
   std::vector<CgDM> dms;
-  dms_from_angles(angles, nang, dms);
-  SPI_TRY(c->cg_buf[3].ensure(dms.size() * sizeof(CgDM)));
+  dms_from_angles(angles + 3 * (size_t)sh.first, nimg, dms);
+  SPI_TRY(c->cg_buf[3].ensure(std::max(dms.size(), mdms.size()) * sizeof(CgDM)));
   SPI_TRY(c->cg_buf[4].ensure(vb));
   if (fbs)
-    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float)));
+    SPI_TRY(c->cg_buf[5].ensure(std::max<size_t>(pcount, 1) * sizeof(float)));
   else if (mixed)
     SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(float) + (size_t)K * n * n * pentry + 32));
   else
-    SPI_TRY(c->cg_buf[5].ensure(pcount * sizeof(T) + (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0)));
+    SPI_TRY(c->cg_buf[5].ensure((size_t)pj_rows * n * n * sizeof(T) +
+                                (sizeof(T) != sizeof(float) ? pcount * sizeof(float) : 0) + 4));
   SPI_TRY(c->cg_buf[6].ensure(3 * vb));
   SPI_TRY(c->cg_buf[7].ensure(sizeof(CgScal) + 64 + (size_t)nang * sizeof(int)));
   T* cb = c->cg_buf[4].as<T>();
   T* pj = c->cg_buf[5].as<T>();
   float* pj32 = (mixed || fbs) ? c->cg_buf[5].as<float>()
-                      : (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + pcount) : reinterpret_cast<float*>(pj);
+                      : (sizeof(T) != sizeof(float)) ? reinterpret_cast<float*>(pj + (size_t)pj_rows * n * n)
+                                                     : reinterpret_cast<float*>(pj);
   void* projt = mixed ? (void*)(c->cg_buf[5].as<char>() + ((pcount * sizeof(float) + 31) & ~size_t(31))) : nullptr;
   T* bckn = c->cg_buf[6].as<T>();
   T* bckp = bckn + nnn;
@@ -1311,38 +1351,43 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal));
   int* dlb = reinterpret_cast<int*>(reinterpret_cast<char*>(c->cg_buf[7].p) + sizeof(CgScal) + 64);
   SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), dms.size() * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
-  SPI_CUDA(cudaMemcpyAsync(pj32, projs, pcount * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if (pcount) SPI_CUDA(cudaMemcpyAsync(pj32, projs, pcount * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   // ---- BPCG_2: statistics, CB = A^T b, background correction
   SPI_CUDA(cudaMemsetAsync(acc, 0, 64, c->stream));
-  astasq_kernel<<<nang, 256, 0, c->stream>>>(pj32, n, ri * ri, acc);
-  SPI_TRY(check_kernel("astasq_kernel"));
-  c->count();
+  if (nimg > 0) {
+    astasq_kernel<<<nimg, 256, 0, c->stream>>>(pj32, n, ri * ri, acc);
+    SPI_TRY(check_kernel("astasq_kernel"));
+    c->count();
+  }
   SPI_CUDA(cudaMemsetAsync(cb, 0, vb, c->stream));
   FbsState fs;
   // FBS interpolation tables: FP32 in precision modes 2 and 3 (FP64 vectors
   // and arithmetic), the vector type otherwise
   const bool fbs32 = fbs && sizeof(T) == 8 && (c->cg_fp64 == 2 || c->cg_fp64 == 3);
   if (fbs) {
-    SPI_TRY(fbs_setup<T>(c, pb, nang, fs, fbs32 ? sizeof(float) : sizeof(T)));
+    SPI_TRY(fbs_setup<T>(c, pb, std::max(std::max(nimg, lo), 1), fs, fbs32 ? sizeof(float) : sizeof(T)));
     if (fbs32)
-      SPI_TRY((fbs_backproject_images<T, float>(c, pb, fs, cb, pj32, nang, c->cg_buf[3].as<CgDM>())));
+      SPI_TRY((fbs_backproject_images<T, float>(c, pb, fs, cb, pj32, nimg, c->cg_buf[3].as<CgDM>())));
     else
-      SPI_TRY((fbs_backproject_images<T, T>(c, pb, fs, cb, pj32, nang, c->cg_buf[3].as<CgDM>())));
+      SPI_TRY((fbs_backproject_images<T, T>(c, pb, fs, cb, pj32, nimg, c->cg_buf[3].as<CgDM>())));
   } else if (mixed) {
     if (wtab)
-      SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
+      SPI_TRY((backproject_images_projt<T, true>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nimg,
                                                 static_cast<ProjtEntry<true>*>(projt))));
     else
-      SPI_TRY((backproject_images_projt<T, false>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nang,
+      SPI_TRY((backproject_images_projt<T, false>(c, pb, cb, pj32, c->cg_buf[3].as<CgDM>(), nimg,
                                                  static_cast<ProjtEntry<false>*>(projt))));
   } else {
-    if (sizeof(T) != sizeof(float)) {
+    if (sizeof(T) != sizeof(float) && pcount) {
       widen_kernel<T><<<blocks_for(c, (long long)pcount, 256), 256, 0, c->stream>>>(pj32, pj, pcount);
       SPI_TRY(check_kernel("widen_kernel"));
       c->count();
     }
-    SPI_TRY(launch_backproject<T>(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nang));
+    SPI_TRY(launch_backproject<T>(c, pb, cb, pj, c->cg_buf[3].as<CgDM>(), nullptr, nimg));
   }
+  // the ranks' CB and ASTASQ sums (bpcg.f:653-663)
+  SPI_TRY(sh.sum(c, cb, (long long)nnn, sizeof(T) == 8));
+  SPI_TRY(sh.sum(c, acc, 3, true));
   double hacc[3];
   SPI_CUDA(cudaMemcpyAsync(hacc, acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -1371,16 +1416,6 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   SPI_CUDA(cudaMemcpyAsync(&bnorm, acc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   const double chi2 = d_ssq - d_aba * (2 * d_sus - d_aba * kls);
-  // ---- HIANG
-  std::vector<float> ang((size_t)3 * nang);
-  for (int k = 0; k < nang; ++k) {
-    ang[3 * k] = angles[3 * k + 2];
-    ang[3 * k + 1] = angles[3 * k + 1];
-    ang[3 * k + 2] = angles[3 * k];
-  }
-  std::vector<int> lb;
-  std::vector<float> dm9;
-  const int lo = hiang(ang, nang, dms, lb, fbs ? &dm9 : nullptr);
   const float di = (float)(n / 2);
   // bpcg.f:269-290: FBS needs RI + MODE <= N/2, linear RI + MODE + 1 <= N/2
   const float extra = fbs ? 0.0f : 1.0f;
@@ -1389,7 +1424,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     return fail(kMissing, "RADIUS TOO LARGE (%d)", (int)ri);
   if (fbs)
     SPI_CUDA(cudaMemcpyAsync(fs.dm9, dm9.data(), dm9.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, dms.data(), (size_t)lo * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
+  SPI_CUDA(cudaMemcpyAsync(c->cg_buf[3].p, mdms.data(), (size_t)lo * sizeof(CgDM), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(dlb, lb.data(), (size_t)lo * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   // ---- BPCG_3_LIN
   SPI_CUDA(cudaMemsetAsync(bckn, 0, 2 * vb, c->stream));  // BCKN, BCKP
@@ -1413,25 +1448,31 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
     scal_after_dir_kernel<<<1, 32, 0, c->stream>>>(sc);
     SPI_CUDA(cudaMemsetAsync(bcke, 0, vb, c->stream));
     c->count(3);
+    // this rank's merged angles [kb, ke) (all of them on one rank)
+    const CgDM* mdm = c->cg_buf[3].as<CgDM>() + kb;
+    const int* mlb = dlb + kb;
+    const int mc = ke - kb;
     if (fbs32) {
-      SPI_TRY((fbs_normal<T, float>(c, pb, fs, bckp, bcke, dlb, lo, c->cg_buf[3].as<CgDM>())));
+      SPI_TRY((fbs_normal<T, float>(c, pb, fs, bckp, bcke, dlb, kb, ke, c->cg_buf[3].as<CgDM>())));
     } else if (fbs) {
-      SPI_TRY((fbs_normal<T, T>(c, pb, fs, bckp, bcke, dlb, lo, c->cg_buf[3].as<CgDM>())));
+      SPI_TRY((fbs_normal<T, T>(c, pb, fs, bckp, bcke, dlb, kb, ke, c->cg_buf[3].as<CgDM>())));
     } else if (mixed) {
       auto* mx = reinterpret_cast<unsigned long long*>(acc + 7);
       if (wide && wtab)
-        SPI_TRY((launch_normal_projt<T, true, true>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+        SPI_TRY((launch_normal_projt<T, true, true>(c, pb, bckp, bcke, mdm, mlb, mc,
                                                     static_cast<ProjtEntry<true>*>(projt), mx)));
       else if (wide)
-        SPI_TRY((launch_normal_projt<T, true, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+        SPI_TRY((launch_normal_projt<T, true, false>(c, pb, bckp, bcke, mdm, mlb, mc,
                                                      static_cast<ProjtEntry<false>*>(projt), mx)));
       else
-        SPI_TRY((launch_normal_projt<T, false, false>(c, pb, bckp, bcke, c->cg_buf[3].as<CgDM>(), dlb, lo,
+        SPI_TRY((launch_normal_projt<T, false, false>(c, pb, bckp, bcke, mdm, mlb, mc,
                                                       static_cast<ProjtEntry<false>*>(projt), mx)));
     } else {
-      SPI_TRY(launch_project<T>(c, pb, bckp, c->cg_buf[3].as<CgDM>(), lo, pj));
-      SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, c->cg_buf[3].as<CgDM>(), dlb, lo));
+      SPI_TRY(launch_project<T>(c, pb, bckp, mdm, mc, pj));
+      SPI_TRY(launch_backproject<T>(c, pb, bcke, pj, mdm, mlb, mc));
     }
+    // the ranks' BCKE (bpcg.f:1031-1032)
+    SPI_TRY(sh.sum(c, bcke, (long long)nnn, sizeof(T) == 8));
     zero_outside_kernel<T><<<nnn_b, 256, 0, c->stream>>>(bckp, n, pb.ldp, r2);
     for (int axis = 0; axis < 3; ++axis)
       fixedge_axis_kernel<T><<<(n * n + 127) / 128, 128, 0, c->stream>>>(bckp, n, axis, mode);
@@ -1448,7 +1489,7 @@ static int bpcg_run(spi_ctx* c, const float* projs, int n, int nang, const float
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   // the FBS iteration runs cuFFT plans and is launched directly
-  bool use_graph = !fbs && getenv("SPI_CG_NOGRAPH") == nullptr;
+  bool use_graph = !fbs && !sh.reduce && getenv("SPI_CG_NOGRAPH") == nullptr;
   if (use_graph && cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     use_graph = false;
     cudaGetLastError();
@@ -1648,9 +1689,39 @@ int spi_bpcg(spi_ctx* c, const float* projs, int n, int nang, const float* angle
   if (mode < 1 || mode > 3) return fail(kInvalid, "spi_bpcg: mode %d must be 1, 2 or 3", mode);
   SPI_CUDA(cudaSetDevice(c->device));
   if (niter_out) *niter_out = 0;
+  CgShard sh;   // one process: every image and merged angle, nothing to sum
+  sh.count = nang;
   if (c->cg_fp64)
-    return bpcg_run<double>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out);
-  return bpcg_run<float>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out);
+    return bpcg_run<double>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out,
+                            niter_out, sh);
+  return bpcg_run<float>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out,
+                         sh);
+}
+
+int spi_bpcg_shard(spi_ctx* c, const float* projs, int first, int count, int n, int nang, const float* angles,
+                   float ri, float errm, float chim, int maxit, int mode, float lambda, int rank, int world,
+                   spi_allreduce_fn allreduce, void* user, float* vol_out, float* log_out, int* niter_out) {
+  if (!c || !angles || !vol_out || (count > 0 && !projs)) return fail(kInvalid, "spi_bpcg_shard: NULL argument");
+  if (n < 8 || nang <= 0) return fail(kInvalid, "spi_bpcg_shard: n = %d, nang = %d", n, nang);
+  if (first < 0 || count < 0 || first + count > nang)
+    return fail(kInvalid, "spi_bpcg_shard: images [%d, %d) outside the %d angles", first, first + count, nang);
+  if (world < 1 || rank < 0 || rank >= world) return fail(kInvalid, "spi_bpcg_shard: rank %d of %d", rank, world);
+  if (world > 1 && !allreduce) return fail(kInvalid, "spi_bpcg_shard: %d ranks need an all-reduce callback", world);
+  if (mode < 1 || mode > 3) return fail(kInvalid, "spi_bpcg_shard: mode %d must be 1, 2 or 3", mode);
+  SPI_CUDA(cudaSetDevice(c->device));
+  if (niter_out) *niter_out = 0;
+  CgShard sh;
+  sh.first = first;
+  sh.count = count;
+  sh.rank = rank;
+  sh.world = world;
+  sh.reduce = allreduce;
+  sh.user = user;
+  if (c->cg_fp64)
+    return bpcg_run<double>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out,
+                            niter_out, sh);
+  return bpcg_run<float>(c, projs, n, nang, angles, ri, errm, chim, maxit, mode, lambda, vol_out, log_out, niter_out,
+                         sh);
 }
 
 }  // extern "C"

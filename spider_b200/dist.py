@@ -62,3 +62,25 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
     finally:
         ctx.bp_close()
         _lib.check(L.spi_bp_attach_grids(ctx.handle, None, None))
+
+
+def sharded_bpcg(ctx, projs, angles, rank: int, world: int, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1,
+                 lam=2000.0, group=None, fp64="mixed", interp="linear"):
+    """BP CG over all ranks (bpcg.f:522-672, 855-1080): each rank passes the
+    full image set (or its own SETPART block with the same length as the
+    full set's block), back-projects its block, and works on its block of
+    HIANG's merged angles; CB, the image statistics and, every iteration,
+    BCKE are summed with torch.distributed (NCCL on GPUs).  Every rank
+    returns the same (volume, log)."""
+    import torch.distributed as tdist
+
+    from . import ops
+    nang = int(angles.shape[0])
+    start, count = shard(nang, rank, world)
+    block = projs[start:start + count] if int(projs.shape[0]) == nang else projs
+
+    def sum_inplace(t):
+        tdist.all_reduce(t, op=tdist.ReduceOp.SUM, group=group)
+
+    return ops.bpcg_shard(block, start, angles, ri, errm, chim, maxit, mode, lam, rank=rank, world=world,
+                          sum_inplace=sum_inplace if world > 1 else None, ctx=ctx, fp64=fp64, interp=interp)

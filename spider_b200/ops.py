@@ -382,6 +382,22 @@ def pj3q_adjoint(projs, angles, shape, ri=None, *, ctx: Context | None = None):
     return out
 
 
+def _set_cg_modes(ctx, fp64, interp):
+    """BP CG precision mode and interpolation of the context (see bpcg)."""
+    if isinstance(fp64, str):
+        modes = {"mixed": 2, "fast": 3, "mixed64": 4}
+        if fp64 not in modes:
+            raise SpiderError(101, f"unknown BP CG precision {fp64!r}")
+        prec = modes[fp64]
+    else:
+        prec = 1 if fp64 else 0
+    check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))
+    interps = {"linear": 0, "l": 0, "fbs": 1, "f": 1}
+    if str(interp).lower() not in interps:
+        raise SpiderError(101, f"unknown BP CG interpolation {interp!r}")
+    check(ctx._L.spi_ctx_set_cg_interpolation(ctx.handle, interps[str(interp).lower()]))
+
+
 def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
          ctx: Context | None = None, fp64="mixed", interp="linear"):
     """``BP CG``.  Prompts in reference order: radius (default n/2-2),
@@ -396,18 +412,7 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     in FP64, False uses the reference's REAL.
     Returns (volume [n,n,n], log [niter, 3] of (iteration, difference, chisq))."""
     ctx = ctx or default_context()
-    if isinstance(fp64, str):
-        modes = {"mixed": 2, "fast": 3, "mixed64": 4}
-        if fp64 not in modes:
-            raise SpiderError(101, f"unknown BP CG precision {fp64!r}")
-        prec = modes[fp64]
-    else:
-        prec = 1 if fp64 else 0
-    check(ctx._L.spi_ctx_set_cg_precision(ctx.handle, prec))
-    interps = {"linear": 0, "l": 0, "fbs": 1, "f": 1}
-    if str(interp).lower() not in interps:
-        raise SpiderError(101, f"unknown BP CG interpolation {interp!r}")
-    check(ctx._L.spi_ctx_set_cg_interpolation(ctx.handle, interps[str(interp).lower()]))
+    _set_cg_modes(ctx, fp64, interp)
     projs = _host_f32(projs)
     n = _nx_of(projs)
     if ri is None:
@@ -419,6 +424,58 @@ def bpcg(projs, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000
     check(ctx._L.spi_bpcg(ctx.handle, _ptr(projs), n, projs.shape[0], _ptr(ang), float(ri), float(errm),
                           float(chim), int(maxit), int(mode), float(lam), _ptr(vol), _ptr(logv),
                           ctypes.cast(ctypes.byref(niter), ctypes.c_void_p)))
+    return vol, logv[: niter.value].copy()
+
+
+class _DeviceArray:
+    """A device array the library passes to an all-reduce callback, as a
+    zero-copy torch tensor through __cuda_array_interface__."""
+
+    def __init__(self, ptr, count, fp64):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8" if fp64 else "<f4",
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+def allreduce_callback(sum_inplace):
+    """Wrap ``sum_inplace(tensor)`` (sums a CUDA tensor over the ranks in
+    place, e.g. ``torch.distributed.all_reduce``) as the library's
+    spi_allreduce_fn.  The library's stream is synchronised before the call
+    and the device after it, so the sum is complete when the callback returns."""
+    def cb(ptr, count, fp64, stream, user):
+        try:
+            t = torch.as_tensor(_DeviceArray(ptr, count, fp64), device="cuda")
+            torch.cuda.ExternalStream(stream, device=t.device).synchronize()
+            sum_inplace(t)
+            torch.cuda.synchronize(t.device)
+            return 0
+        except Exception:   # reported by the library as a failed all-reduce
+            return 1
+    return _lib.ALLREDUCE_FN(cb)
+
+
+def bpcg_shard(projs, first, angles, ri=None, errm=5e-5, chim=0.0, maxit=20, mode=1, lam=2000.0, *,
+               rank=0, world=1, sum_inplace=None, ctx: Context | None = None, fp64="mixed", interp="linear"):
+    """One rank's BP CG over several processes (the reference's MPI form):
+    ``projs`` are images first .. first+len(projs)-1 of the full ``angles``
+    list; ``sum_inplace(tensor)`` sums a CUDA tensor over the ranks in place
+    (CB, the image statistics, then BCKE every iteration).  Every rank returns
+    the same (volume, log)."""
+    ctx = ctx or default_context()
+    _set_cg_modes(ctx, fp64, interp)
+    projs = _host_f32(projs)
+    ang = _host_f32(angles)
+    count = int(projs.shape[0])
+    n = int(projs.shape[-1])
+    if ri is None:
+        ri = float(n // 2 - 2)  # bpcg.f:161
+    vol = np.zeros((n, n, n), np.float32)
+    logv = np.zeros((max(maxit, 1), 3), np.float32)
+    niter = ctypes.c_int(0)
+    cb = allreduce_callback(sum_inplace) if sum_inplace is not None else ctypes.cast(None, _lib.ALLREDUCE_FN)
+    check(ctx._L.spi_bpcg_shard(ctx.handle, _ptr(projs) if count else None, int(first), count, n, ang.shape[0],
+                                _ptr(ang), float(ri), float(errm), float(chim), int(maxit), int(mode), float(lam),
+                                int(rank), int(world), cb, None, _ptr(vol), _ptr(logv),
+                                ctypes.cast(ctypes.byref(niter), ctypes.c_void_p)))
     return vol, logv[: niter.value].copy()
 
 
