@@ -226,9 +226,10 @@ def cg_measure(args, ctx, stream, rank, world):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def timed(iters, fp64):
+    def timed(iters, fp64, interp="linear"):
         e0.record(stream)
-        v, log = ops.bpcg(projs, ang, ri, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64=fp64)
+        v, log = ops.bpcg(projs, ang, ri, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64=fp64,
+                          interp=interp)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3, v, log
@@ -264,6 +265,11 @@ def cg_measure(args, ctx, stream, rank, world):
            "config": {"n": n, "images": nang, "lambda": 1e-3, "mode": 1, "iterations_timed": K,
                       "phantom": "50 Gaussian blobs, sigma 2-8, SNR 0.3, uniform SO(3)"}}
     res["differentiable_cg"] = autograd_cg_measure(ctx, projs, ang, ri, K)
+    # the 'F' answer (FBS interpolation), default precision mode: informational
+    timed(1, "mixed", "fbs")
+    t1, _, _ = timed(1, "mixed", "fbs")
+    tk, _, _ = timed(1 + K, "mixed", "fbs")
+    res["fbs_s_per_iter"] = (tk - t1) / K
     if rank == 0 and world == 1 and not args.no_cpu:
         res["cpu_baseline"] = cg_cpu_baseline(projs, ang, ri, n)
     return res
