@@ -220,8 +220,9 @@ int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, f
  * both overwrite their output.  Besides the runs and matrices a plan for a
  * volume of up to 6M voxels holds two 16-byte-per-voxel buffers: the volume
  * in x/y-neighbour quads (refreshed by every forward call) and the adjoint's
- * quad accumulator.  A plan keeps a pointer to its context for launch
- * counting and must be destroyed before it. */
+ * quad accumulator, so forward calls of one plan must not overlap on the
+ * GPU, nor adjoint calls (a forward and an adjoint may).  A plan keeps a
+ * pointer to its context for launch counting and must be destroyed before it. */
 typedef struct spi_pj3q_plan spi_pj3q_plan;
 int spi_pj3q_plan_create(spi_ctx* ctx, int nx, int ny, int nz, float ri, const float* angles, int nang,
                          spi_pj3q_plan** out);
