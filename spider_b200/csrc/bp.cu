@@ -1132,7 +1132,7 @@ long long spi_ctx::device_bytes() const {
   long long t = 0;
   const DevBuf* bufs[] = {&grid[0], &grid[1], &kbtab, &imgs, &padded, &spectra, &spec_tmp, &slices, &cplx, &real3,
                           &workctr,
-                          &wkb, &acc, &volbuf, &pj_vol, &pj_out, &pj_runs, &pj_dm};
+                          &wkb, &acc, &volbuf, &pj_vol, &pj_out, &pj_runs, &pj_dm, &pj_rows, &pj_v4, &pj_fbs};
   for (auto b : bufs) t += (long long)b->bytes;
   for (auto& b : cg_buf) t += (long long)b.bytes;
   return t;

@@ -67,6 +67,7 @@ struct spi_ctx {
   spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
   spi::DevBuf pj_fbs;                 // PJ 3F: FBS3_PREP scratch + the FBS3 table
   spi::DevBuf pj_v4;                  // PJ 3Q: the volume as float4 quads of x/y neighbours
+  spi::DevBuf pj_rows;                // PJ 3Q forward: runs in (y, |z|) order, then the row tasks
   spi::DevBuf cg_buf[8];
   spi::DevBuf cg_fbs[4];              // FBS: 3D scratch + table, 2D chunk scratch, segments, DM(1..9)
   spi::HostBuf hbuf;
@@ -104,7 +105,12 @@ struct PjDM {
 // Validates the arguments, builds the runs of the sphere of radius ri and
 // the DM of every angle (psi, theta, phi) and uploads them to pj_runs / pj_dm
 // on the context stream.
-int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out);
+// Also uploads to pj_rows the runs in (y, |z|) order followed by the row
+// tasks of the warp forward projection (int4 {first run, runs, x1, x2}: up to
+// 32 runs of one row y and the union of their x ranges); *ntasks_out gets
+// their number.
+int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out,
+              int* ntasks_out = nullptr);
 // RTSF (rtsf.f:109-205, SCLI = 1) of nimg device images; prm[b] = {COS(THETA),
 // SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)}; runs on the context stream.
 int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm);

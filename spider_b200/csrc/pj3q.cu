@@ -3,12 +3,15 @@
 //
 // PREPCUB (prepcub.f:54-109) turns the sphere of radius RI into runs of
 // voxels along x.  WPRO_N walks each run accumulating the sample position
-// with XB = XB + DM(1) (sequential float additions), so one thread owns one
-// (projection, run) pair and walks it in the same order: every sample
-// position and every trilinear weight is bit-identical to the CPU form.
-// Runs are ordered (z, y); consecutive threads of a warp hold consecutive y
-// and therefore write different output rows K = y + LDPY.
+// with XB = XB + DM(1) (sequential float additions), so one GPU thread owns
+// one (projection, run) pair and walks it in the same order: every sample
+// position and every trilinear weight is bit-identical to the CPU form.  The
+// forward projection gives a warp up to 32 runs of one output row and sums
+// their samples at each x before one atomic add (wpro_warp_kernel); the
+// adjoint walks the runs in PREPCUB's (z, y) order, one per thread.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/spider_b200.h"
@@ -55,6 +58,97 @@ __device__ __forceinline__ float sel8(const float (&a)[8], int o) {
   return v;
 }
 
+// One WPRO_N sample at (xb, yb, zb): the trilinear value when IFIX of every
+// coordinate lies in 1..n-1 (wpro_n.f:93-98), else 0 (the reference adds
+// nothing).  FORM (PjForm) selects the plain volume (eight floats), quads
+// (two 16-byte loads) or cells (one 32-byte load); all give the same bits.
+template <int FORM>
+__device__ __forceinline__ float wpro_sample(const float* __restrict__ cube, const float4* __restrict__ v4, int nsam,
+                                             int nrow, int nslice, float xb, float yb, float zb) {
+  const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+  if (!(iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice)) return 0.0f;
+  const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
+  const size_t o = (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
+  const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
+  float c000, c100, c010, c110, c001, c101, c011, c111;
+  if (FORM == 2) {
+    float a[8];
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+        : "l"(v4 + 2 * o));
+    c000 = a[0]; c100 = a[1]; c010 = a[2]; c110 = a[3];
+    c001 = a[4]; c101 = a[5]; c011 = a[6]; c111 = a[7];
+  } else if (FORM == 1) {
+    const float4 q0 = __ldg(v4 + o), q1 = __ldg(v4 + o + sz);
+    c000 = q0.x; c100 = q0.y; c010 = q0.z; c110 = q0.w;
+    c001 = q1.x; c101 = q1.y; c011 = q1.z; c111 = q1.w;
+  } else {
+    const float* c0 = cube + o;
+    c000 = __ldg(c0); c100 = __ldg(c0 + 1); c010 = __ldg(c0 + sy); c110 = __ldg(c0 + sy + 1);
+    c001 = __ldg(c0 + sz); c101 = __ldg(c0 + sz + 1); c011 = __ldg(c0 + sz + sy); c111 = __ldg(c0 + sz + sy + 1);
+  }
+  // A1..A8 exactly as wpro_n.f:103-114
+  const float a1 = c000;
+  const float a2 = __fsub_rn(c100, a1);
+  const float a3 = __fsub_rn(c010, a1);
+  const float a4 = __fsub_rn(c001, a1);
+  const float a5 = __fadd_rn(__fsub_rn(-a2, c010), c110);
+  const float a61 = __fadd_rn(-c001, c101);
+  const float a6 = __fadd_rn(-a2, a61);
+  const float a7 = __fadd_rn(__fsub_rn(-a3, c001), c011);
+  const float a8 = __fadd_rn(__fsub_rn(__fsub_rn(-a5, a61), c011), c111);
+  // A1 + DZ*(A4 + A6*DX + (A7 + A8*DX)*DY) + A3*DY + DX*(A2 + A5*DY)
+  const float inner = __fadd_rn(__fadd_rn(a4, __fmul_rn(a6, dx)), __fmul_rn(__fadd_rn(a7, __fmul_rn(a8, dx)), dy));
+  float v = __fadd_rn(a1, __fmul_rn(dz, inner));
+  v = __fadd_rn(v, __fmul_rn(a3, dy));
+  return __fadd_rn(v, __fmul_rn(dx, __fadd_rn(a2, __fmul_rn(a5, dy))));
+}
+
+// Forward projection by row tasks: a warp takes up to 32 runs of one output
+// row K = y + LDPY (tasks = int4 {first run, runs, x1, x2}, runs in order of
+// |z| so their x ranges nest) and walks them in step over x = x1..x2, every
+// lane its own run with the reference's sequential XB = XB + DM(1) while x
+// lies in its range.  The lanes' samples at one x all belong to pixel (x, K),
+// so the warp sums them with shuffles and one lane adds the sum: one L2
+// atomic per 32 samples instead of one per sample (at 128^3 the L2
+// reductions fall from 64M to 2.4M per 64 projections).  Reads the packed
+// volume (FORM: quads or cells); sample values are the bits of wpro_kernel's,
+// only the order of the sum over z differs.
+template <int FORM>
+__global__ void __launch_bounds__(128) wpro_warp_kernel(const float4* __restrict__ v4, int nsam, int nrow, int nslice,
+                                                        const PjRun* __restrict__ runs,
+                                                        const int4* __restrict__ tasks, int ntasks,
+                                                        const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
+                                                        int ldpz, float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const long long nwork = (long long)ntasks * nang;
+  const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < nwork; w += stride) {
+    const int a = (int)(w / ntasks);
+    const int4 tk = tasks[w % ntasks];
+    const bool live = lane < tk.y;
+    const PjRun r = runs[tk.x + (live ? lane : 0)];
+    const int i1 = live ? r.i1 : 1, i2 = live ? r.i2 : 0;
+    const PjDM dm = dms[a];
+    float* row = out + (size_t)a * nsam * nrow + (size_t)(r.y + ldpy - 1) * nsam;
+    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
+    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
+    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    for (int j = tk.z; j <= tk.w; ++j) {
+      float v = 0.0f;
+      if (j >= i1 && j <= i2) {
+        v = wpro_sample<FORM>(nullptr, v4, nsam, nrow, nslice, xb, yb, zb);
+        xb = __fadd_rn(xb, dm.d[0]);
+        yb = __fadd_rn(yb, dm.d[1]);
+        zb = __fadd_rn(zb, dm.d[2]);
+      }
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+      if (lane == 0 && v != 0.0f) atomicAdd(row + (j - 1), v);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cube, int nsam, int nrow, int nslice,
                                                    const PjRun* __restrict__ runs, int nruns,
                                                    const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
@@ -64,37 +158,13 @@ __global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cub
     const int a = (int)(t / nruns);
     const PjRun r = runs[t % nruns];
     const PjDM dm = dms[a];
-    float* b = out + (size_t)a * nsam * nrow;
-    const int k = r.y + ldpy;
+    float* b = out + (size_t)a * nsam * nrow + (size_t)(r.y + ldpy - 1) * nsam;
     float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
     float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
     float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
-    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
     for (int j = r.i1; j <= r.i2; ++j) {
-      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
-      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
-        const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
-        const float* c0 = cube + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
-        const float c000 = __ldg(c0), c100 = __ldg(c0 + 1), c010 = __ldg(c0 + sy), c110 = __ldg(c0 + sy + 1);
-        const float c001 = __ldg(c0 + sz), c101 = __ldg(c0 + sz + 1), c011 = __ldg(c0 + sz + sy),
-                    c111 = __ldg(c0 + sz + sy + 1);
-        // A1..A8 exactly as wpro_n.f:103-114
-        const float a1 = c000;
-        const float a2 = __fsub_rn(c100, a1);
-        const float a3 = __fsub_rn(c010, a1);
-        const float a4 = __fsub_rn(c001, a1);
-        const float a5 = __fadd_rn(__fsub_rn(-a2, c010), c110);
-        const float a61 = __fadd_rn(-c001, c101);
-        const float a6 = __fadd_rn(-a2, a61);
-        const float a7 = __fadd_rn(__fsub_rn(-a3, c001), c011);
-        const float a8 = __fadd_rn(__fsub_rn(__fsub_rn(-a5, a61), c011), c111);
-        // A1 + DZ*(A4 + A6*DX + (A7 + A8*DX)*DY) + A3*DY + DX*(A2 + A5*DY)
-        const float inner = __fadd_rn(__fadd_rn(a4, __fmul_rn(a6, dx)), __fmul_rn(__fadd_rn(a7, __fmul_rn(a8, dx)), dy));
-        float v = __fadd_rn(a1, __fmul_rn(dz, inner));
-        v = __fadd_rn(v, __fmul_rn(a3, dy));
-        v = __fadd_rn(v, __fmul_rn(dx, __fadd_rn(a2, __fmul_rn(a5, dy))));
-        atomicAdd(b + (size_t)(k - 1) * nsam + (j - 1), v);
-      }
+      const float v = wpro_sample<0>(cube, nullptr, nsam, nrow, nslice, xb, yb, zb);
+      if (v != 0.0f) atomicAdd(b + (j - 1), v);
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[1]);
       zb = __fadd_rn(zb, dm.d[2]);
@@ -102,13 +172,34 @@ __global__ void __launch_bounds__(128) wpro_kernel(const float* __restrict__ cub
   }
 }
 
-// The volume as quads {f(x,y,z), f(x+1,y,z), f(x,y+1,z), f(x+1,y+1,z)}
-// (0 past the last x or y), so a trilinear sample reads two 16-byte quads
-// (planes z and z+1) instead of eight scattered floats: 1.2-1.3x faster at
-// 128^3, where the 32 MB of quads stay in L2; at 256^3 (268 MB of quads
-// against 67 MB of volume) no faster, so volumes above kQuadMaxBytes of
-// quads use wpro_kernel.
+// Packed volumes for the forward projection.  Quads {f(x,y,z), f(x+1,y,z),
+// f(x,y+1,z), f(x+1,y+1,z)} (16 bytes per voxel, 0 past the last x or y):
+// a trilinear sample reads two quads (planes z and z+1) instead of eight
+// scattered floats.  Cells (32 bytes per voxel: the quads of planes z and
+// z+1 side by side, 0 past the last z): one 256-bit load per sample.
+// Measured with plans of 2,000 (128^3) and 500 (256^3) projections, against
+// one thread per run on the plain volume (97k and 8.7k projections/s):
+// wpro_warp_kernel on cells 189k at 128^3 (67 MB, inside L2) but 11.0k at
+// 256^3 (537 MB); on quads 153k and 13.1k.  So cells while they take at most
+// kCellMaxBytes, quads up to quad_fwd_max(), then the plain volume.  The
+// adjoint's quad accumulator (wpro_adjoint4_kernel) is used up to
+// kQuadMaxBytes, where it stays in L2.
 constexpr size_t kQuadMaxBytes = size_t(96) << 20;
+constexpr size_t kCellMaxBytes = size_t(96) << 20;
+// 8 GB of packed volume (quads of volumes up to about 800^3); SPI_PJ_QUADMAX
+// (MiB) overrides, 0 keeps every forward projection on the plain volume.
+static size_t quad_fwd_max() {
+  const char* e = getenv("SPI_PJ_QUADMAX");
+  return e ? (size_t)std::max(0LL, atoll(e)) << 20 : size_t(8) << 30;
+}
+enum PjForm { kPjPlain = 0, kPjQuads = 1, kPjCells = 2 };
+static int pj_fwd_form(size_t nvox) {
+  const size_t cap = quad_fwd_max();
+  if (nvox * 32 <= std::min(cap, kCellMaxBytes)) return kPjCells;
+  return nvox * 16 <= cap ? kPjQuads : kPjPlain;
+}
+static size_t pj_packed_bytes(int form, size_t nvox) { return form == kPjCells ? nvox * 32 : form == kPjQuads ? nvox * 16 : 0; }
+
 __global__ void pj_pack4_kernel(const float* __restrict__ cube, int nsam, int nrow, int nslice,
                                 float4* __restrict__ v4) {
   const size_t total = (size_t)nsam * nrow * nslice;
@@ -121,52 +212,25 @@ __global__ void pj_pack4_kernel(const float* __restrict__ cube, int nsam, int nr
   }
 }
 
-// wpro_kernel on the quad-packed volume: the same runs, walk, bounds and
-// A1..A8 arithmetic, so every projection value is the same bits.
-__global__ void __launch_bounds__(128) wpro4_kernel(const float4* __restrict__ v4, int nsam, int nrow, int nslice,
-                                                    const PjRun* __restrict__ runs, int nruns,
-                                                    const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
-                                                    int ldpz, float* __restrict__ out) {
-  const long long total = (long long)nruns * nang;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(t / nruns);
-    const PjRun r = runs[t % nruns];
-    const PjDM dm = dms[a];
-    float* b = out + (size_t)a * nsam * nrow;
-    const int k = r.y + ldpy;
-    float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
-    float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
-    float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
-    const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
-    for (int j = r.i1; j <= r.i2; ++j) {
-      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
-      if (iox >= 1 && iox < nsam && ioy >= 1 && ioy < nrow && ioz >= 1 && ioz < nslice) {
-        const float dx = __fsub_rn(xb, (float)iox), dy = __fsub_rn(yb, (float)ioy), dz = __fsub_rn(zb, (float)ioz);
-        const float4* c0 = v4 + (size_t)(ioz - 1) * sz + (size_t)(ioy - 1) * sy + (iox - 1);
-        const float4 q0 = __ldg(c0), q1 = __ldg(c0 + sz);
-        const float c000 = q0.x, c100 = q0.y, c010 = q0.z, c110 = q0.w;
-        const float c001 = q1.x, c101 = q1.y, c011 = q1.z, c111 = q1.w;
-        // A1..A8 exactly as wpro_n.f:103-114
-        const float a1 = c000;
-        const float a2 = __fsub_rn(c100, a1);
-        const float a3 = __fsub_rn(c010, a1);
-        const float a4 = __fsub_rn(c001, a1);
-        const float a5 = __fadd_rn(__fsub_rn(-a2, c010), c110);
-        const float a61 = __fadd_rn(-c001, c101);
-        const float a6 = __fadd_rn(-a2, a61);
-        const float a7 = __fadd_rn(__fsub_rn(-a3, c001), c011);
-        const float a8 = __fadd_rn(__fsub_rn(__fsub_rn(-a5, a61), c011), c111);
-        // A1 + DZ*(A4 + A6*DX + (A7 + A8*DX)*DY) + A3*DY + DX*(A2 + A5*DY)
-        const float inner = __fadd_rn(__fadd_rn(a4, __fmul_rn(a6, dx)), __fmul_rn(__fadd_rn(a7, __fmul_rn(a8, dx)), dy));
-        float v = __fadd_rn(a1, __fmul_rn(dz, inner));
-        v = __fadd_rn(v, __fmul_rn(a3, dy));
-        v = __fadd_rn(v, __fmul_rn(dx, __fadd_rn(a2, __fmul_rn(a5, dy))));
-        atomicAdd(b + (size_t)(k - 1) * nsam + (j - 1), v);
-      }
-      xb = __fadd_rn(xb, dm.d[0]);
-      yb = __fadd_rn(yb, dm.d[1]);
-      zb = __fadd_rn(zb, dm.d[2]);
+// cell of voxel q: v8[2q] = quad of plane z, v8[2q + 1] = quad of plane z + 1
+__global__ void pj_pack_cells_kernel(const float* __restrict__ cube, int nsam, int nrow, int nslice,
+                                     float4* __restrict__ v8) {
+  const size_t total = (size_t)nsam * nrow * nslice, sz = (size_t)nsam * nrow;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(q % nsam);
+    const int y = (int)((q / nsam) % nrow);
+    const int z = (int)(q / sz);
+    const bool bx = x + 1 < nsam, by = y + 1 < nrow;
+    float4 lo = make_float4(__ldg(cube + q), bx ? __ldg(cube + q + 1) : 0.0f, by ? __ldg(cube + q + nsam) : 0.0f,
+                            (bx && by) ? __ldg(cube + q + nsam + 1) : 0.0f);
+    float4 hi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (z + 1 < nslice) {
+      const float* c1 = cube + q + sz;
+      hi = make_float4(__ldg(c1), bx ? __ldg(c1 + 1) : 0.0f, by ? __ldg(c1 + nsam) : 0.0f,
+                       (bx && by) ? __ldg(c1 + nsam + 1) : 0.0f);
     }
+    v8[2 * q] = lo;
+    v8[2 * q + 1] = hi;
   }
 }
 
@@ -327,9 +391,37 @@ void pj_release(spi_ctx* c) {
   c->pj_dm.release();
   c->pj_fbs.release();
   c->pj_v4.release();
+  c->pj_rows.release();
 }
 
-int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out) {
+// The runs of every row y in order of |z| (ties: -z first), cut into tasks of
+// at most 32 runs: rows[0..nruns) are the runs, then ntasks int4 tasks.
+static void row_tasks(const std::vector<PjRun>& runs, std::vector<PjRun>& rowruns, std::vector<int4>& tasks) {
+  std::vector<int> order(runs.size());
+  for (size_t i = 0; i < runs.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
+    const PjRun &a = runs[p], &b = runs[q];
+    if (a.y != b.y) return a.y < b.y;
+    return std::abs(a.z) < std::abs(b.z);
+  });
+  rowruns.clear();
+  tasks.clear();
+  for (int i : order) rowruns.push_back(runs[i]);
+  for (size_t i = 0; i < rowruns.size();) {
+    size_t e = i + 1;
+    while (e < rowruns.size() && e - i < 32 && rowruns[e].y == rowruns[i].y) ++e;
+    int j1 = rowruns[i].i1, j2 = rowruns[i].i2;
+    for (size_t q = i; q < e; ++q) {
+      j1 = std::min(j1, rowruns[q].i1);
+      j2 = std::max(j2, rowruns[q].i2);
+    }
+    tasks.push_back(make_int4((int)i, (int)(e - i), j1, j2));
+    i = e;
+  }
+}
+
+int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out,
+              int* ntasks_out) {
   if (!c) return fail(kInvalid, "NULL context");
   if (nx < 4 || ny < 4 || nz < 4) return fail(kInvalid, "PJ 3Q: volume %dx%dx%d too small", nx, ny, nz);
   if (nang < 0 || (nang > 0 && !angles)) return fail(kInvalid, "PJ 3Q: bad angle list");
@@ -346,7 +438,62 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
   if (!runs.empty())
     SPI_CUDA(cudaMemcpyAsync(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice, c->stream));
+  std::vector<PjRun> rowruns;
+  std::vector<int4> tasks;
+  row_tasks(runs, rowruns, tasks);
+  const size_t rbytes = rowruns.size() * sizeof(PjRun), toff = (rbytes + 15) & ~size_t(15);
+  SPI_TRY(c->pj_rows.ensure(toff + std::max<size_t>(1, tasks.size()) * sizeof(int4)));
+  if (!rowruns.empty()) {
+    SPI_CUDA(cudaMemcpyAsync(c->pj_rows.p, rowruns.data(), rbytes, cudaMemcpyHostToDevice, c->stream));
+    SPI_CUDA(cudaMemcpyAsync(static_cast<char*>(c->pj_rows.p) + toff, tasks.data(), tasks.size() * sizeof(int4),
+                             cudaMemcpyHostToDevice, c->stream));
+  }
   *nruns_out = (int)runs.size();
+  if (ntasks_out) *ntasks_out = (int)tasks.size();
+  return 0;
+}
+
+// row-task view of pj_rows
+static const int4* pj_tasks_of(void* rows, int nruns) {
+  const size_t toff = ((size_t)nruns * sizeof(PjRun) + 15) & ~size_t(15);
+  return reinterpret_cast<const int4*>(static_cast<const char*>(rows) + toff);
+}
+
+// Forward projection of vol (device, nx*ny*nz) into the zeroed out, in the
+// given PjForm: packs the volume into packed (quads or cells), then the warp
+// row-task kernel; the plain form runs one thread per run on vol.
+static int pj_forward(spi_ctx* c, cudaStream_t st, const float* vol, int form, float4* packed, int nx, int ny, int nz,
+                      const PjRun* runs, int nruns, const void* rows, int ntasks, const PjDM* dms, int nang,
+                      float* out) {
+  if (nruns == 0 || nang == 0) return 0;
+  const size_t nvox = (size_t)nx * ny * nz;
+  const int ldpx = nx / 2 + 1, ldpy = ny / 2 + 1, ldpz = nz / 2 + 1;
+  if (form == kPjPlain) {
+    const long long total = (long long)nruns * nang;
+    const int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
+    wpro_kernel<<<blocks, 128, 0, st>>>(vol, nx, ny, nz, runs, nruns, dms, nang, ldpx, ldpy, ldpz, out);
+    SPI_TRY(check_kernel("wpro_kernel"));
+    c->count();
+    return 0;
+  }
+  const int pblocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)c->sm_count * 16);
+  if (form == kPjCells)
+    pj_pack_cells_kernel<<<pblocks, 256, 0, st>>>(vol, nx, ny, nz, packed);
+  else
+    pj_pack4_kernel<<<pblocks, 256, 0, st>>>(vol, nx, ny, nz, packed);
+  SPI_TRY(check_kernel("pj_pack_kernel"));
+  const long long warps = (long long)ntasks * nang;
+  const int blocks = (int)std::min<long long>((warps + 3) / 4, (long long)c->sm_count * 16);
+  const PjRun* rr = static_cast<const PjRun*>(rows);
+  const int4* tk = pj_tasks_of(const_cast<void*>(rows), nruns);
+  if (form == kPjCells)
+    wpro_warp_kernel<kPjCells><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx, ldpy, ldpz,
+                                                       out);
+  else
+    wpro_warp_kernel<kPjQuads><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx, ldpy, ldpz,
+                                                       out);
+  SPI_TRY(check_kernel("wpro_warp_kernel"));
+  c->count(2);
   return 0;
 }
 
@@ -358,8 +505,8 @@ extern "C" {
 
 int spi_pj3q(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
              float* proj_out, int on_device) {
-  int nruns = 0;
-  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));
+  int nruns = 0, ntasks = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks));
   if (!vol || !proj_out) return fail(kInvalid, "PJ 3Q: NULL buffer");
   const size_t vbytes = (size_t)nx * ny * nz * sizeof(float);
   const size_t pbytes = (size_t)nang * nx * ny * sizeof(float);
@@ -374,27 +521,15 @@ int spi_pj3q(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
   }
   if (nang == 0) return 0;
   SPI_CUDA(cudaMemsetAsync(dout, 0, pbytes, c->stream));
-  const long long total = (long long)nruns * nang;
-  int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
-  if (blocks > 0) {
-    const size_t nvox = (size_t)nx * ny * nz;
-    if (nvox * sizeof(float4) <= kQuadMaxBytes) {
-      SPI_TRY(c->pj_v4.ensure(nvox * sizeof(float4)));
-      pj_pack4_kernel<<<(int)std::min<size_t>((nvox + 255) / 256, (size_t)c->sm_count * 16), 256, 0, c->stream>>>(
-          dvol, nx, ny, nz, c->pj_v4.as<float4>());
-      SPI_TRY(check_kernel("pj_pack4_kernel"));
-      wpro4_kernel<<<blocks, 128, 0, c->stream>>>(c->pj_v4.as<float4>(), nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
-                                                  c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1,
-                                                  dout);
-      SPI_TRY(check_kernel("wpro4_kernel"));
-      c->count(2);
-    } else {
-      wpro_kernel<<<blocks, 128, 0, c->stream>>>(dvol, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns,
-                                                 c->pj_dm.as<PjDM>(), nang, nx / 2 + 1, ny / 2 + 1, nz / 2 + 1, dout);
-      SPI_TRY(check_kernel("wpro_kernel"));
-      c->count();
-    }
+  const size_t nvox = (size_t)nx * ny * nz;
+  const int form = pj_fwd_form(nvox);
+  float4* packed = nullptr;
+  if (nruns > 0 && form != kPjPlain) {
+    SPI_TRY(c->pj_v4.ensure(pj_packed_bytes(form, nvox)));
+    packed = c->pj_v4.as<float4>();
   }
+  SPI_TRY(pj_forward(c, c->stream, dvol, form, packed, nx, ny, nz, c->pj_runs.as<PjRun>(), nruns, c->pj_rows.p, ntasks,
+                     c->pj_dm.as<PjDM>(), nang, dout));
   if (!on_device) SPI_CUDA(cudaMemcpyAsync(proj_out, dout, pbytes, cudaMemcpyDeviceToHost, c->stream));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
@@ -454,11 +589,12 @@ int spi_pj3q_adjoint(spi_ctx* c, const float* projs, int nx, int ny, int nz, flo
 
 struct spi_pj3q_plan {
   spi_ctx* ctx = nullptr;
-  int device = 0, nx = 0, ny = 0, nz = 0, nang = 0, nruns = 0, blocks = 0;
+  int device = 0, nx = 0, ny = 0, nz = 0, nang = 0, nruns = 0, ntasks = 0, blocks = 0, form = 0;
   float ri = 0.0f;
   PjRun* runs = nullptr;
+  void* rows = nullptr;   // runs in (y, |z|) order, then the row tasks (forward)
   PjDM* dms = nullptr;
-  float4* v4 = nullptr;   // quad-packed volume of the forward projection
+  float4* v4 = nullptr;   // packed volume of the forward projection (quads or cells, by form)
   float4* q4 = nullptr;   // quad accumulator of the adjoint
 };
 
@@ -469,27 +605,32 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   if (!out) return fail(kInvalid, "spi_pj3q_plan_create: out is NULL");
   *out = nullptr;
   if (nang <= 0) return fail(kInvalid, "spi_pj3q_plan_create: nang = %d", nang);
-  int nruns = 0;
-  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));   // runs and matrices into the context's buffers
+  int nruns = 0, ntasks = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks));   // runs and matrices into the context's buffers
   auto* p = new spi_pj3q_plan();
   p->ctx = c;
   p->device = c->device;
-  p->nx = nx; p->ny = ny; p->nz = nz; p->nang = nang; p->nruns = nruns; p->ri = ri;
+  p->nx = nx; p->ny = ny; p->nz = nz; p->nang = nang; p->nruns = nruns; p->ntasks = ntasks; p->ri = ri;
+  const size_t rows_bytes = (((size_t)nruns * sizeof(PjRun) + 15) & ~size_t(15)) + std::max(1, ntasks) * sizeof(int4);
   const long long total = (long long)nruns * nang;
   p->blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
   cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
   if (e == cudaSuccess) e = cudaMalloc(&p->dms, (size_t)nang * sizeof(PjDM));
-  if (e == cudaSuccess && (size_t)nx * ny * nz * sizeof(float4) <= kQuadMaxBytes) {
-    e = cudaMalloc(&p->v4, (size_t)nx * ny * nz * sizeof(float4));
-    if (e == cudaSuccess) e = cudaMalloc(&p->q4, (size_t)nx * ny * nz * sizeof(float4));
-  }
+  if (e == cudaSuccess) e = cudaMalloc(&p->rows, rows_bytes);
+  const size_t nvox = (size_t)nx * ny * nz;
+  p->form = nruns ? pj_fwd_form(nvox) : kPjPlain;
+  if (e == cudaSuccess && p->form != kPjPlain) e = cudaMalloc(&p->v4, pj_packed_bytes(p->form, nvox));
+  if (e == cudaSuccess && nvox * sizeof(float4) <= kQuadMaxBytes) e = cudaMalloc(&p->q4, nvox * sizeof(float4));
   if (e == cudaSuccess && nruns)
     e = cudaMemcpyAsync(p->runs, c->pj_runs.p, (size_t)nruns * sizeof(PjRun), cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(p->dms, c->pj_dm.p, (size_t)nang * sizeof(PjDM), cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess && nruns)
+    e = cudaMemcpyAsync(p->rows, c->pj_rows.p, rows_bytes, cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     cudaFree(p->runs);
+    cudaFree(p->rows);
     cudaFree(p->dms);
     cudaFree(p->v4);
     cudaFree(p->q4);
@@ -504,22 +645,8 @@ int spi_pj3q_plan_forward(const spi_pj3q_plan* p, const float* vol, float* proj_
   if (!p || !vol || !proj_out) return fail(kInvalid, "spi_pj3q_plan_forward: NULL argument");
   auto st = static_cast<cudaStream_t>(stream);
   SPI_CUDA(cudaMemsetAsync(proj_out, 0, (size_t)p->nang * p->nx * p->ny * sizeof(float), st));
-  if (p->blocks > 0 && p->v4) {
-    const size_t nvox = (size_t)p->nx * p->ny * p->nz;
-    pj_pack4_kernel<<<(int)std::min<size_t>((nvox + 255) / 256, (size_t)p->ctx->sm_count * 16), 256, 0, st>>>(
-        vol, p->nx, p->ny, p->nz, p->v4);
-    SPI_TRY(check_kernel("pj_pack4_kernel"));
-    wpro4_kernel<<<p->blocks, 128, 0, st>>>(p->v4, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
-                                            p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, proj_out);
-    SPI_TRY(check_kernel("wpro4_kernel"));
-    p->ctx->count(2);
-  } else if (p->blocks > 0) {
-    wpro_kernel<<<p->blocks, 128, 0, st>>>(vol, p->nx, p->ny, p->nz, p->runs, p->nruns, p->dms, p->nang,
-                                           p->nx / 2 + 1, p->ny / 2 + 1, p->nz / 2 + 1, proj_out);
-    SPI_TRY(check_kernel("wpro_kernel"));
-    p->ctx->count();
-  }
-  return 0;
+  return pj_forward(p->ctx, st, vol, p->form, p->v4, p->nx, p->ny, p->nz, p->runs, p->nruns, p->rows, p->ntasks, p->dms,
+                    p->nang, proj_out);
 }
 
 int spi_pj3q_plan_adjoint(const spi_pj3q_plan* p, const float* projs, float* vol_out, void* stream) {
@@ -551,6 +678,7 @@ int spi_pj3q_plan_destroy(spi_pj3q_plan* p) {
   if (!p) return 0;
   cudaSetDevice(p->device);
   cudaFree(p->runs);
+  cudaFree(p->rows);
   cudaFree(p->dms);
   cudaFree(p->v4);
   cudaFree(p->q4);

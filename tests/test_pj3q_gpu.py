@@ -9,9 +9,15 @@ from spider_b200 import ops, synth
 pytestmark = pytest.mark.gpu
 
 
-# (200, 192, 188): above 6M voxels, the unpacked-volume kernel; the others use x/y-neighbour quads
+# packed: the warp row-task kernel on the packed volume, 32-byte cells up to
+# 96 MB of cells (3M voxels) and 16-byte quads above, so (200, 192, 188)
+# takes quads and the others cells; plain: SPI_PJ_QUADMAX=0, one thread per
+# run on the volume
+@pytest.mark.parametrize("form", ["packed", "plain"])
 @pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64), (40, 36, 33), (200, 192, 188)])
-def test_pj3q_matches_oracle(ctx, orc, shape):
+def test_pj3q_matches_oracle(ctx, orc, shape, form, monkeypatch):
+    if form == "plain":
+        monkeypatch.setenv("SPI_PJ_QUADMAX", "0")
     nz, ny, nx = shape
     rng = np.random.default_rng(sum(shape))
     vol = synth.blob_phantom(max(shape), 10, sigma=(1.5, 4), radius=0.3 * min(shape), rng=rng)[:nz, :ny, :nx].copy()
@@ -20,7 +26,7 @@ def test_pj3q_matches_oracle(ctx, orc, shape):
     ref = orc.pj3q(vol, ang, prec=0)
     ref64 = orc.pj3q(vol, ang, prec=1)
     e = synth.rel_l2(got, ref)
-    print(f"PJ 3Q {shape}: rel-L2 vs FP32 oracle {e:.3e}, vs FP64 {synth.rel_l2(got, ref64):.3e}")
+    print(f"PJ 3Q {shape} {form}: rel-L2 vs FP32 oracle {e:.3e}, vs FP64 {synth.rel_l2(got, ref64):.3e}")
     assert e <= 1e-5
 
 
@@ -54,3 +60,22 @@ def test_pj3q_device_tensors(ctx, orc):
     ang = synth.so3_angles(10, rng)
     got = ops.pj3q(torch.from_numpy(vol).cuda(), ang, ctx=ctx).cpu().numpy()
     assert synth.rel_l2(got, orc.pj3q(vol, ang)) <= 1e-5
+
+
+@pytest.mark.parametrize("quadmax", [None, "0"])
+def test_pj3q_plan_forward_forms(ctx, orc, quadmax, monkeypatch):
+    """A plan on the packed volume (the default; cells at this size) and one
+    on the plain volume both reproduce the oracle, for a ragged shape with
+    several row tasks per row."""
+    import torch
+    from spider_b200 import autograd
+    if quadmax is not None:
+        monkeypatch.setenv("SPI_PJ_QUADMAX", quadmax)
+    rng = np.random.default_rng(11)
+    shape = (72, 80, 76)
+    vol = synth.blob_phantom(80, 12, sigma=(1.5, 4), radius=24, rng=rng)[:72, :80, :76].copy()
+    ang = synth.so3_angles(24, rng)
+    plan = autograd.PJ3QPlan(shape, ang, ctx=ctx)
+    got = plan.forward(torch.from_numpy(vol).cuda()).cpu().numpy()
+    plan.close()
+    assert synth.rel_l2(got, orc.pj3q(vol, ang, prec=0)) <= 1e-5
