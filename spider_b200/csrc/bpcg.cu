@@ -1089,7 +1089,7 @@ static size_t fbs3_work_bytes(int n) {
   return align256(nnn * 8) + align256(s3 * 16) + align256(7 * s3 * 16) + align256(7 * nnn * 8);
 }
 
-static int fbs3_work_init(Fbs3Work& w, int n, char* p, cudaStream_t s) {
+static int fbs3_work_init(Fbs3Work& w, int n, char* p, cudaStream_t s, bool plans = true) {
   const size_t nnn = (size_t)n * n * n, s3 = (size_t)n * n * (n / 2 + 1);
   w.n = n;
   w.a4 = 6.28318530717958647692f / (float)n;
@@ -1097,6 +1097,7 @@ static int fbs3_work_init(Fbs3Work& w, int n, char* p, cudaStream_t s) {
   w.F = reinterpret_cast<double2*>(p); p += align256(s3 * 16);
   w.W = reinterpret_cast<double2*>(p); p += align256(7 * s3 * 16);
   w.D = reinterpret_cast<double*>(p);
+  if (!plans) return 0;
   int d3[3] = {n, n, n};
   SPI_CUFFT(cufftPlan3d(&w.fwd, n, n, n, CUFFT_D2Z));
   SPI_CUFFT(cufftPlanMany(&w.inv, 3, d3, nullptr, 1, (int)s3, nullptr, 1, (int)nnn, CUFFT_Z2D, 7));
@@ -1558,8 +1559,8 @@ int spi_pj3f(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
   if (!c) return fail(kInvalid, "NULL context");
   if (nx != ny || nx != nz) return fail(kInvalid, "PJ 3F: cubic volumes only (%dx%dx%d)", nx, ny, nz);
   if (nx > 1024) return fail(kInvalid, "PJ 3F: n = %d above 1024", nx);
-  int nruns = 0;
-  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns));
+  int nruns = 0, ntasks = 0;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks));
   if (!vol || !proj_out) return fail(kInvalid, "PJ 3F: NULL buffer");
   const int n = nx;
   const size_t nnn = (size_t)n * n * n, vbytes = nnn * sizeof(float);
@@ -1577,8 +1578,29 @@ int spi_pj3f(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
   // FBS3_PREP of the volume (writpro_n.f:154-185), REAL tables
   const size_t wb = fbs3_work_bytes(n);
   SPI_TRY(c->pj_fbs.ensure(wb + align256(nnn * 8 * sizeof(float))));
+  // the FBS3_PREP plans stay with the context for the next call of this n
   Fbs3Work w;
-  int st = fbs3_work_init(w, n, c->pj_fbs.as<char>(), c->stream);
+  int st = 0;
+  if (c->pjf_n != n) {
+    if (c->pjf_plan[0]) cufftDestroy(c->pjf_plan[0]);
+    if (c->pjf_plan[1]) cufftDestroy(c->pjf_plan[1]);
+    c->pjf_plan[0] = c->pjf_plan[1] = 0;
+    c->pjf_n = 0;
+    st = fbs3_work_init(w, n, c->pj_fbs.as<char>(), c->stream);
+    if (st != 0) {
+      w.destroy();
+      return st;
+    }
+    c->pjf_plan[0] = w.fwd;
+    c->pjf_plan[1] = w.inv;
+    c->pjf_n = n;
+  } else {
+    SPI_TRY(fbs3_work_init(w, n, c->pj_fbs.as<char>(), c->stream, false));
+    w.fwd = c->pjf_plan[0];
+    w.inv = c->pjf_plan[1];
+    SPI_CUFFT(cufftSetStream(w.fwd, c->stream));
+    SPI_CUFFT(cufftSetStream(w.inv, c->stream));
+  }
   float* V = reinterpret_cast<float*>(c->pj_fbs.as<char>() + wb);
   if (st == 0) st = fbs3_prepare<float, float>(c, w, dvol, V);
   if (st == 0) {
@@ -1586,13 +1608,15 @@ int spi_pj3f(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
     if (e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
   }
   if (st == 0) {
-    const long long total = (long long)nruns * nang;
-    const int blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
     const int nocheck = (2.0f * (ri + 1.0f) + 1.0f) <= (float)n;
-    if (blocks > 0) {
-      wpro_fbs_kernel<float, float><<<blocks, 128, 0, c->stream>>>(V, n, c->pj_runs.as<PjRun>(), nruns,
-                                                                   c->pj_dm.as<PjDM>(), nang, n / 2 + 1, nocheck, dout);
-      st = check_kernel("wpro_fbs_kernel");
+    if (ntasks > 0) {
+      const size_t toff = pj_tasks_offset(nruns);
+      const long long warps = (long long)ntasks * nang;
+      const int blocks = (int)std::min<long long>((warps + 3) / 4, (long long)c->sm_count * 16);
+      wpro_fbs_warp_kernel<float, float><<<blocks, 128, 0, c->stream>>>(
+          V, n, c->pj_rows.as<PjRun>(), reinterpret_cast<const int4*>(c->pj_rows.as<char>() + toff), ntasks,
+          c->pj_dm.as<PjDM>(), nang, n / 2 + 1, nocheck, dout);
+      st = check_kernel("wpro_fbs_warp_kernel");
       c->count();
     }
   }
@@ -1601,7 +1625,6 @@ int spi_pj3f(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
     if (e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
   }
   const cudaError_t e = cudaStreamSynchronize(c->stream);
-  w.destroy();
   if (st == 0 && e != cudaSuccess) st = fail(kCuda, "PJ 3F: %s", cudaGetErrorString(e));
   return st;
 }

@@ -168,23 +168,32 @@ __device__ __forceinline__ T fbs3_eval_wrap(float x, float y, float z, int n, co
 }
 
 // ---------------------------------------------------------------------------
-// WPRO_FBS (wpro_fbs.f:1-150), PJ 3F: one thread per (projection, run) walks
-// the run as WPRO_N does (XB = XB + DM(1), ...); every sample is FBS3 with
-// wrapped indices; the runs of one output row K = Y + LDP meet in a pixel
-// through atomics.  nocheck: the sphere fits (2(RI+1)+1 <= N); otherwise
-// samples whose IFIX lies outside 1..N are skipped (wpro_fbs.f:138-144).
+// WPRO_FBS (wpro_fbs.f:1-150), PJ 3F, by row tasks as PJ 3Q's
+// wpro_warp_kernel: a warp walks up to 32 runs of one output row K = Y + LDP
+// (tasks int4 {first run, runs, x1, x2} over the runs in (y, |z|) order) in
+// step over x, each lane its run as WPRO_N does (XB = XB + DM(1), ...), every
+// sample FBS3 with wrapped indices, and one lane adds the warp's sum of the
+// pixel's samples (1.06x the speed of one thread per run with an atomic per
+// sample at 128^3, 1.56x at 256^3).  nocheck: the sphere fits
+// (2(RI+1)+1 <= N); otherwise samples whose IFIX lies outside 1..N are
+// skipped (wpro_fbs.f:138-144).
 template <class T, class TT>
-__global__ void __launch_bounds__(128) wpro_fbs_kernel(const TT* __restrict__ V, int n, const PjRun* __restrict__ runs,
-                                                       int nruns, const PjDM* __restrict__ dms, int nang, int ldp,
-                                                       int nocheck, float* __restrict__ out) {
-  const long long total = (long long)nruns * nang;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(t / nruns);
-    const PjRun r = runs[t % nruns];
+__global__ void __launch_bounds__(128) wpro_fbs_warp_kernel(const TT* __restrict__ V, int n,
+                                                            const PjRun* __restrict__ runs,
+                                                            const int4* __restrict__ tasks, int ntasks,
+                                                            const PjDM* __restrict__ dms, int nang, int ldp,
+                                                            int nocheck, float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const long long nwork = (long long)ntasks * nang;
+  const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long wk = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; wk < nwork; wk += stride) {
+    const int a = (int)(wk / ntasks);
+    const int4 tk = tasks[wk % ntasks];
+    const bool live = lane < tk.y;
+    const PjRun r = runs[tk.x + (live ? lane : 0)];
+    const int i1 = live ? r.i1 : 1, i2 = live ? r.i2 : 0;
     const PjDM dm = dms[a];
-    float* b = out + (size_t)a * n * n;
-    const int k = r.y + ldp;
-    // IPCUBE(3)*DM(a) + IPCUBE(4)*DM(b) + IPCUBE(5)*DM(c) + LDP, left to right
+    float* row = out + (size_t)a * n * n + (size_t)(r.y + ldp - 1) * n;
     auto start = [&](float da, float db, float dc) {
       return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn((float)r.x, da), __fmul_rn((float)r.y, db)),
                                  __fmul_rn((float)r.z, dc)),
@@ -193,13 +202,19 @@ __global__ void __launch_bounds__(128) wpro_fbs_kernel(const TT* __restrict__ V,
     float xb = start(dm.d[0], dm.d[3], dm.d[6]);
     float yb = start(dm.d[1], dm.d[4], dm.d[7]);
     float zb = start(dm.d[2], dm.d[5], dm.d[8]);
-    for (int j = r.i1; j <= r.i2; ++j) {
-      const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
-      if (nocheck || (iox > 0 && iox <= n && ioy > 0 && ioy <= n && ioz > 0 && ioz <= n))
-        atomicAdd(b + (size_t)(k - 1) * n + (j - 1), (float)fbs3_eval_wrap<T, TT>(xb, yb, zb, n, V));
-      xb = __fadd_rn(xb, dm.d[0]);
-      yb = __fadd_rn(yb, dm.d[1]);
-      zb = __fadd_rn(zb, dm.d[2]);
+    for (int j = tk.z; j <= tk.w; ++j) {
+      float v = 0.0f;
+      if (j >= i1 && j <= i2) {
+        const int iox = __float2int_rz(xb), ioy = __float2int_rz(yb), ioz = __float2int_rz(zb);
+        if (nocheck || (iox > 0 && iox <= n && ioy > 0 && ioy <= n && ioz > 0 && ioz <= n))
+          v = (float)fbs3_eval_wrap<T, TT>(xb, yb, zb, n, V);
+        xb = __fadd_rn(xb, dm.d[0]);
+        yb = __fadd_rn(yb, dm.d[1]);
+        zb = __fadd_rn(zb, dm.d[2]);
+      }
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+      if (lane == 0 && v != 0.0f) atomicAdd(row + (j - 1), v);
     }
   }
 }

@@ -66,6 +66,8 @@ struct spi_ctx {
   // ---- PJ 3Q / BP CG scratch ----
   spi::DevBuf pj_vol, pj_out, pj_runs, pj_dm;
   spi::DevBuf pj_fbs;                 // PJ 3F: FBS3_PREP scratch + the FBS3 table
+  cufftHandle pjf_plan[2] = {0, 0};   // PJ 3F: FBS3_PREP's 3D D2Z and 7-batch Z2D
+  int pjf_n = 0;                      // cube size of those plans
   spi::DevBuf pj_v4;                  // PJ 3Q: the volume as float4 quads of x/y neighbours
   spi::DevBuf pj_rows;                // PJ 3Q forward: runs in (y, |z|) order, then the row tasks
   spi::DevBuf cg_buf[8];
@@ -102,6 +104,8 @@ struct PjRun {
 struct PjDM {
   float d[9];
 };
+// byte offset of the row tasks in pj_rows, after nruns runs (16-byte aligned)
+inline size_t pj_tasks_offset(int nruns) { return ((size_t)nruns * sizeof(PjRun) + 15) & ~size_t(15); }
 // Validates the arguments, builds the runs of the sphere of radius ri and
 // the DM of every angle (psi, theta, phi) and uploads them to pj_runs / pj_dm
 // on the context stream.

@@ -19,27 +19,34 @@
 
 namespace spi {
 
+// PREPCUB's runs, in its (z, y) order.  The reference tests every voxel of
+// a line, t3*t3 + yy <= r in REAL; with t3 = i - LDPX that value only grows
+// with |t3| (m*m is exact below 2^24 and rounding is monotone), so the voxels
+// that pass are the interval |i - LDPX| <= m of the largest m that passes:
+// found from the square root and settled by the same float test, O(1) per
+// line instead of O(nsam).
 static void prepcub(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<PjRun>& runs) {
   const float r = ri * ri;
   runs.clear();
+  auto pass = [&](int m, float yy) {
+    const float t3 = (float)m;
+    return t3 * t3 + yy <= r;
+  };
   for (int i1 = 1; i1 <= nslice; ++i1) {
-    float t = (float)(i1 - ldpz);
-    float xx = t * t;
+    const float t = (float)(i1 - ldpz);
+    const float xx = t * t;
     for (int i2 = 1; i2 <= nrow; ++i2) {
-      float t2 = (float)(i2 - ldpy);
-      float yy = t2 * t2 + xx;
-      bool first = true;
-      for (int i3 = 1; i3 <= nsam; ++i3) {
-        float t3 = (float)(i3 - ldpx);
-        float rc = t3 * t3 + yy;
-        if (first) {
-          if (rc > r) continue;
-          first = false;
-          runs.push_back(PjRun{i3, i3, i3 - ldpx, i2 - ldpy, i1 - ldpz});
-        } else if (rc <= r) {
-          runs.back().i2 = i3;
-        }
-      }
+      const float t2 = (float)(i2 - ldpy);
+      const float yy = t2 * t2 + xx;
+      // largest |t3| that still passes, capped by the line's extent
+      const int mmax = std::max(ldpx - 1, nsam - ldpx);
+      int m = (int)std::sqrt(std::max(0.0, (double)r - (double)yy));
+      m = std::min(m, mmax);
+      while (m < mmax && pass(m + 1, yy)) ++m;
+      while (m >= 0 && !pass(m, yy)) --m;
+      if (m < 0) continue;
+      const int a = std::max(1, ldpx - m), b = std::min(nsam, ldpx + m);
+      if (a <= b) runs.push_back(PjRun{a, b, a - ldpx, i2 - ldpy, i1 - ldpz});
     }
   }
 }
@@ -392,6 +399,10 @@ void pj_release(spi_ctx* c) {
   c->pj_fbs.release();
   c->pj_v4.release();
   c->pj_rows.release();
+  if (c->pjf_plan[0]) cufftDestroy(c->pjf_plan[0]);
+  if (c->pjf_plan[1]) cufftDestroy(c->pjf_plan[1]);
+  c->pjf_plan[0] = c->pjf_plan[1] = 0;
+  c->pjf_n = 0;
 }
 
 // The runs of every row y in order of |z| (ties: -z first), cut into tasks of
@@ -441,7 +452,7 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
   std::vector<PjRun> rowruns;
   std::vector<int4> tasks;
   row_tasks(runs, rowruns, tasks);
-  const size_t rbytes = rowruns.size() * sizeof(PjRun), toff = (rbytes + 15) & ~size_t(15);
+  const size_t rbytes = rowruns.size() * sizeof(PjRun), toff = pj_tasks_offset((int)rowruns.size());
   SPI_TRY(c->pj_rows.ensure(toff + std::max<size_t>(1, tasks.size()) * sizeof(int4)));
   if (!rowruns.empty()) {
     SPI_CUDA(cudaMemcpyAsync(c->pj_rows.p, rowruns.data(), rbytes, cudaMemcpyHostToDevice, c->stream));
@@ -454,9 +465,8 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
 }
 
 // row-task view of pj_rows
-static const int4* pj_tasks_of(void* rows, int nruns) {
-  const size_t toff = ((size_t)nruns * sizeof(PjRun) + 15) & ~size_t(15);
-  return reinterpret_cast<const int4*>(static_cast<const char*>(rows) + toff);
+static const int4* pj_tasks_of(const void* rows, int nruns) {
+  return reinterpret_cast<const int4*>(static_cast<const char*>(rows) + pj_tasks_offset(nruns));
 }
 
 // Forward projection of vol (device, nx*ny*nz) into the zeroed out, in the
@@ -485,7 +495,7 @@ static int pj_forward(spi_ctx* c, cudaStream_t st, const float* vol, int form, f
   const long long warps = (long long)ntasks * nang;
   const int blocks = (int)std::min<long long>((warps + 3) / 4, (long long)c->sm_count * 16);
   const PjRun* rr = static_cast<const PjRun*>(rows);
-  const int4* tk = pj_tasks_of(const_cast<void*>(rows), nruns);
+  const int4* tk = pj_tasks_of(rows, nruns);
   if (form == kPjCells)
     wpro_warp_kernel<kPjCells><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx, ldpy, ldpz,
                                                        out);
@@ -611,7 +621,7 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   p->ctx = c;
   p->device = c->device;
   p->nx = nx; p->ny = ny; p->nz = nz; p->nang = nang; p->nruns = nruns; p->ntasks = ntasks; p->ri = ri;
-  const size_t rows_bytes = (((size_t)nruns * sizeof(PjRun) + 15) & ~size_t(15)) + std::max(1, ntasks) * sizeof(int4);
+  const size_t rows_bytes = pj_tasks_offset(nruns) + std::max(1, ntasks) * sizeof(int4);
   const long long total = (long long)nruns * nang;
   p->blocks = (int)std::min<long long>((total + 127) / 128, (long long)c->sm_count * 16);
   cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
