@@ -16,39 +16,16 @@
 
 #include "../../include/spider_b200.h"
 #include "ctx.h"
+#include "pj_runs.h"
 
 namespace spi {
 
-// PREPCUB's runs, in its (z, y) order.  The reference tests every voxel of
-// a line, t3*t3 + yy <= r in REAL; with t3 = i - LDPX that value only grows
-// with |t3| (m*m is exact below 2^24 and rounding is monotone), so the voxels
-// that pass are the interval |i - LDPX| <= m of the largest m that passes:
-// found from the square root and settled by the same float test, O(1) per
-// line instead of O(nsam).
+// PREPCUB's runs, in its (z, y) order
 static void prepcub(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<PjRun>& runs) {
-  const float r = ri * ri;
   runs.clear();
-  auto pass = [&](int m, float yy) {
-    const float t3 = (float)m;
-    return t3 * t3 + yy <= r;
-  };
-  for (int i1 = 1; i1 <= nslice; ++i1) {
-    const float t = (float)(i1 - ldpz);
-    const float xx = t * t;
-    for (int i2 = 1; i2 <= nrow; ++i2) {
-      const float t2 = (float)(i2 - ldpy);
-      const float yy = t2 * t2 + xx;
-      // largest |t3| that still passes, capped by the line's extent
-      const int mmax = std::max(ldpx - 1, nsam - ldpx);
-      int m = (int)std::sqrt(std::max(0.0, (double)r - (double)yy));
-      m = std::min(m, mmax);
-      while (m < mmax && pass(m + 1, yy)) ++m;
-      while (m >= 0 && !pass(m, yy)) --m;
-      if (m < 0) continue;
-      const int a = std::max(1, ldpx - m), b = std::min(nsam, ldpx + m);
-      if (a <= b) runs.push_back(PjRun{a, b, a - ldpx, i2 - ldpy, i1 - ldpz});
-    }
-  }
+  prepcub_lines(nsam, nrow, nslice, ri, ldpx, ldpy, ldpz, [&](int a, int b, int y, int z) {
+    runs.push_back(PjRun{a, b, a - ldpx, y - ldpy, z - ldpz});
+  });
 }
 
 // Start position of a run: IPCUBE(3)*DM(1) + IPCUBE(4)*DM(4) + IPCUBE(5)*DM(7) + LDPX

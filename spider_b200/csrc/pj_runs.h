@@ -1,0 +1,44 @@
+// PREPCUB (prepcub.f:54-109) run finding for PJ 3Q / PJ 3F, host only and
+// free of CUDA so a CPU test can compile it.
+//
+// The reference tests every voxel of an x line, t3*t3 + yy <= r in REAL,
+// and makes the voxels that pass one run.  With t3 = i - LDPX that value
+// only grows with |t3| (m*m is exact below 2^24 and rounding is monotone),
+// so the voxels that pass are the interval |i - LDPX| <= m of the largest m
+// that passes: found here from the square root and settled by the same float
+// test, O(1) per line instead of O(nsam).
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+
+namespace spi {
+
+// emit(first x, last x, y index, z index) for every line that holds a run,
+// 1-based, in PREPCUB's order (z outer, y inner)
+template <class Emit>
+inline void prepcub_lines(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, Emit emit) {
+  const float r = ri * ri;
+  auto pass = [&](int m, float yy) {
+    const float t3 = (float)m;
+    return t3 * t3 + yy <= r;
+  };
+  const int mmax = std::max(ldpx - 1, nsam - ldpx);   // largest |t3| on the line
+  for (int i1 = 1; i1 <= nslice; ++i1) {
+    const float t = (float)(i1 - ldpz);
+    const float xx = t * t;
+    for (int i2 = 1; i2 <= nrow; ++i2) {
+      const float t2 = (float)(i2 - ldpy);
+      const float yy = t2 * t2 + xx;
+      int m = (int)std::sqrt(std::max(0.0, (double)r - (double)yy));
+      m = std::min(m, mmax);
+      while (m < mmax && pass(m + 1, yy)) ++m;
+      while (m >= 0 && !pass(m, yy)) --m;
+      if (m < 0) continue;
+      const int a = std::max(1, ldpx - m), b = std::min(nsam, ldpx + m);
+      if (a <= b) emit(a, b, i2, i1);
+    }
+  }
+}
+
+}  // namespace spi

@@ -1,0 +1,63 @@
+// Compares spider_b200/csrc/pj_runs.h (PREPCUB run finding by interval) with
+// a voxel-by-voxel restatement of PREPCUB (prepcub.f:54-109): every voxel of
+// every x line tested with t3*t3 + yy <= r in REAL, the first that passes
+// opening the run and every later one that passes extending it.  Prints the
+// number of cases and mismatches; exit status 1 on any mismatch.
+#include <cstdio>
+#include <vector>
+
+#include "../spider_b200/csrc/pj_runs.h"
+
+struct Run { int i1, i2, y, z; };
+
+static void by_voxel(int nsam, int nrow, int nslice, float ri, int ldpx, int ldpy, int ldpz, std::vector<Run>& out) {
+  const float r = ri * ri;
+  for (int i1 = 1; i1 <= nslice; ++i1) {
+    const float t = (float)(i1 - ldpz);
+    const float xx = t * t;
+    for (int i2 = 1; i2 <= nrow; ++i2) {
+      const float t2 = (float)(i2 - ldpy);
+      const float yy = t2 * t2 + xx;
+      bool first = true;
+      for (int i3 = 1; i3 <= nsam; ++i3) {
+        const float t3 = (float)(i3 - ldpx);
+        const float rc = t3 * t3 + yy;
+        if (first) {
+          if (rc > r) continue;
+          first = false;
+          out.push_back(Run{i3, i3, i2, i1});
+        } else if (rc <= r) {
+          out.back().i2 = i3;
+        }
+      }
+    }
+  }
+}
+
+int main() {
+  const int shapes[][3] = {{4, 4, 4},     {5, 7, 6},       {32, 32, 32},   {33, 31, 30},
+                           {40, 36, 33},  {64, 64, 64},    {75, 75, 75},   {128, 128, 128},
+                           {129, 64, 17}, {200, 192, 188}, {256, 256, 256}};
+  const float radii[] = {0.5f, 1.0f, 1.5f, 3.0f, 5.0f, 14.0f, 16.0f, 30.9999f, 31.0f,
+                         62.0f, 63.0f, 64.0f, 94.0f, 126.0f, 127.0f, 200.0f, 1000.0f};
+  long long cases = 0, bad = 0;
+  for (const auto& sh : shapes)
+    for (float ri : radii)
+      for (int shift = -1; shift <= 1; ++shift) {   // centres off the middle voxel too
+        const int nx = sh[0], ny = sh[1], nz = sh[2];
+        const int lx = nx / 2 + 1 + shift, ly = ny / 2 + 1, lz = nz / 2 + 1 - shift;
+        std::vector<Run> a, b;
+        by_voxel(nx, ny, nz, ri, lx, ly, lz, a);
+        spi::prepcub_lines(nx, ny, nz, ri, lx, ly, lz, [&](int i1, int i2, int y, int z) { b.push_back(Run{i1, i2, y, z}); });
+        ++cases;
+        bool same = a.size() == b.size();
+        for (size_t i = 0; same && i < a.size(); ++i)
+          same = a[i].i1 == b[i].i1 && a[i].i2 == b[i].i2 && a[i].y == b[i].y && a[i].z == b[i].z;
+        if (!same) {
+          ++bad;
+          std::printf("mismatch %dx%dx%d ri=%g shift=%d: %zu vs %zu runs\n", nx, ny, nz, ri, shift, a.size(), b.size());
+        }
+      }
+  std::printf("%lld cases, %lld mismatches\n", cases, bad);
+  return bad != 0;
+}
