@@ -420,11 +420,16 @@ __global__ void __launch_bounds__(512) prjcq_projt_band_kernel(
     }
   };
   const CgDM dm = dms[k];
+  const float ystep = dm.d[3];
   for (int ri = threadIdx.x; ri < nruns; ri += blockDim.x) {
     const CgRun r = runs[ri];
     const float fx = (float)(r.x - ldp), fy = (float)(r.y - ldp), fz = (float)(r.z - ldp);
     float xb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[0]), __fmul_rn(fy, dm.d[1])), __fmul_rn(fz, dm.d[2])), (float)ldp);
     float yb = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, dm.d[3]), __fmul_rn(fy, dm.d[4])), __fmul_rn(fz, dm.d[5])), (float)ldp);
+    // A run whose rows all miss the band is skipped: its YB is linear in the
+    // step up to the walk's rounding (well under the 2-row margin).
+    const float ye = yb + (float)(r.l2 - r.l1) * ystep;
+    if (fmaxf(yb, ye) + 2.0f < (float)r0 || fminf(yb, ye) - 2.0f > (float)(h1 + 1)) continue;
     for (int j = r.l1; j <= r.l2; ++j) {
       const int iqy = __float2int_rz(yb);
       // rows iqy-1 and iqy (0-based) of the splat; skip unless one is accumulated here
@@ -448,6 +453,10 @@ __global__ void __launch_bounds__(512) prjcq_projt_band_kernel(
             add(l + 1, (double)rmul(dx, dy));
           }
         }
+      } else if ((ystep > 0.0f && iqy > h1) || (ystep < 0.0f && iqy < r0)) {
+        // past the band: adding DM(4) of one sign moves YB (and its
+        // truncation) one way only, so no later voxel of the run reaches it
+        break;
       }
       xb = __fadd_rn(xb, dm.d[0]);
       yb = __fadd_rn(yb, dm.d[3]);
