@@ -79,3 +79,23 @@ def test_pj3q_plan_forward_forms(ctx, orc, quadmax, monkeypatch):
     got = plan.forward(torch.from_numpy(vol).cuda()).cpu().numpy()
     plan.close()
     assert synth.rel_l2(got, orc.pj3q(vol, ang, prec=0)) <= 1e-5
+
+
+def test_pj3q_adjoint_slabs(ctx, monkeypatch):
+    """At 168^3 the quad accumulator (76 MB) is filled in two z slabs; the
+    result equals the scalar-atomic adjoint (SPI_PJ_QUADMAX=0) up to the
+    order of the float sums, and <A x, y> = <x, A^T y> holds."""
+    rng = np.random.default_rng(13)
+    n = 168
+    ang = synth.so3_angles(12, rng)
+    y = rng.standard_normal((12, n, n)).astype(np.float32)
+    x = rng.standard_normal((n, n, n)).astype(np.float32)
+    slabs = ops.pj3q_adjoint(y, ang, (n, n, n), ctx=ctx)
+    monkeypatch.setenv("SPI_PJ_QUADMAX", "0")
+    plain = ops.pj3q_adjoint(y, ang, (n, n, n), ctx=ctx)
+    monkeypatch.delenv("SPI_PJ_QUADMAX")
+    assert synth.rel_l2(slabs, plain) <= 1e-6
+    ax = ops.pj3q(x, ang, ctx=ctx)
+    lhs = float(np.dot(ax.ravel().astype(np.float64), y.ravel()))
+    rhs = float(np.dot(x.ravel().astype(np.float64), slabs.ravel()))
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs))
