@@ -217,12 +217,14 @@ int spi_pj3q_adjoint(spi_ctx* ctx, const float* projs, int nx, int ny, int nz, f
  * (a cudaStream_t; NULL = the default stream) with device buffers: they
  * allocate nothing and do not synchronise, so they can be captured in a
  * CUDA graph.  The forward equals spi_pj3q, the adjoint spi_pj3q_adjoint;
- * both overwrite their output.  Besides the runs and matrices a plan for a
- * volume of up to 6M voxels holds two 16-byte-per-voxel buffers: the volume
- * in x/y-neighbour quads (refreshed by every forward call) and the adjoint's
- * quad accumulator, so forward calls of one plan must not overlap on the
- * GPU, nor adjoint calls (a forward and an adjoint may).  A plan keeps a
- * pointer to its context for launch counting and must be destroyed before it. */
+ * both overwrite their output.  Besides the runs and matrices a plan holds
+ * two buffers: the packed volume of the forward projection (32 bytes per
+ * voxel up to 3M voxels, 16 above; refreshed by every forward call) and the
+ * adjoint's quad accumulator (16 bytes per voxel), each while it takes at
+ * most 8 GB (environment SPI_PJ_QUADMAX, in MiB, lowers that cap), so forward
+ * calls of one plan must not overlap on the GPU, nor adjoint calls (a forward
+ * and an adjoint may).  A plan keeps a pointer to its context for launch
+ * counting and must be destroyed before it. */
 typedef struct spi_pj3q_plan spi_pj3q_plan;
 int spi_pj3q_plan_create(spi_ctx* ctx, int nx, int ny, int nz, float ri, const float* angles, int nang,
                          spi_pj3q_plan** out);
