@@ -109,12 +109,12 @@ inline size_t pj_tasks_offset(int nruns) { return ((size_t)nruns * sizeof(PjRun)
 // Validates the arguments, builds the runs of the sphere of radius ri and
 // the DM of every angle (psi, theta, phi) and uploads them to pj_runs / pj_dm
 // on the context stream.
-// Also uploads to pj_rows the runs in (y, |z|) order followed by the row
-// tasks of the warp forward projection (int4 {first run, runs, x1, x2}: up to
-// 32 runs of one row y and the union of their x ranges); *ntasks_out gets
-// their number.
+// Also uploads to pj_rows the runs in (y, |z|) order (z_order: (y, z))
+// followed by the row tasks of the warp forward projection (int4 {first run,
+// runs, x1, x2}: up to 32 runs of one row y and the union of their x
+// ranges); *ntasks_out gets their number.
 int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out,
-              int* ntasks_out = nullptr);
+              int* ntasks_out = nullptr, bool z_order = false);
 // RTSF (rtsf.f:109-205, SCLI = 1) of nimg device images; prm[b] = {COS(THETA),
 // SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)}; runs on the context stream.
 int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm);

@@ -97,13 +97,17 @@ __device__ __forceinline__ float wpro_sample(const float* __restrict__ cube, con
 // atomic per 32 samples instead of one per sample (at 128^3 the L2
 // reductions fall from 64M to 2.4M per 64 projections).  Reads the packed
 // volume (FORM: quads or cells); sample values are the bits of wpro_kernel's,
-// only the order of the sum over z differs.
-template <int FORM>
+// only the order of the sum over z differs.  SLAB: only samples whose IOZ
+// lies in zlo <= IOZ < zhi are taken, so a packed volume larger than L2 is
+// read slab by slab (the row tasks then hold consecutive z); a run whose ZB
+// misses the slab sits out, a lane stops at the slab's far side (ZB moves one
+// way along a run), and the warp leaves the task once all lanes have.
+template <int FORM, bool SLAB>
 __global__ void __launch_bounds__(128) wpro_warp_kernel(const float4* __restrict__ v4, int nsam, int nrow, int nslice,
                                                         const PjRun* __restrict__ runs,
                                                         const int4* __restrict__ tasks, int ntasks,
                                                         const PjDM* __restrict__ dms, int nang, int ldpx, int ldpy,
-                                                        int ldpz, float* __restrict__ out) {
+                                                        int ldpz, int zlo, int zhi, float* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const long long nwork = (long long)ntasks * nang;
   const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -112,23 +116,44 @@ __global__ void __launch_bounds__(128) wpro_warp_kernel(const float4* __restrict
     const int4 tk = tasks[w % ntasks];
     const bool live = lane < tk.y;
     const PjRun r = runs[tk.x + (live ? lane : 0)];
-    const int i1 = live ? r.i1 : 1, i2 = live ? r.i2 : 0;
+    int i1 = live ? r.i1 : 1, i2 = live ? r.i2 : 0;
     const PjDM dm = dms[a];
     float* row = out + (size_t)a * nsam * nrow + (size_t)(r.y + ldpy - 1) * nsam;
     float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
     float yb = run_start(r, dm.d[1], dm.d[4], dm.d[7], ldpy);
     float zb = run_start(r, dm.d[2], dm.d[5], dm.d[8], ldpz);
+    if (SLAB) {
+      // a run whose ZB (linear along it; 2-voxel margin for the walk's
+      // rounding) misses the slab takes no part in this pass
+      const float ze = zb + (float)(i2 - i1) * dm.d[2];
+      if (fmaxf(zb, ze) + 2.0f < (float)zlo || fminf(zb, ze) - 2.0f > (float)zhi) i2 = i1 - 1;
+      if (!__any_sync(0xffffffffu, i2 >= i1)) continue;
+    }
     for (int j = tk.z; j <= tk.w; ++j) {
       float v = 0.0f;
       if (j >= i1 && j <= i2) {
-        v = wpro_sample<FORM>(nullptr, v4, nsam, nrow, nslice, xb, yb, zb);
+        if (SLAB) {
+          const int ioz = __float2int_rz(zb);
+          if ((dm.d[2] > 0.0f && ioz >= zhi) || (dm.d[2] < 0.0f && ioz < zlo)) {
+            i2 = j - 1;   // past the slab: ZB moves one way along the run
+          } else if (ioz >= zlo && ioz < zhi) {
+            v = wpro_sample<FORM>(nullptr, v4, nsam, nrow, nslice, xb, yb, zb);
+          }
+        } else {
+          v = wpro_sample<FORM>(nullptr, v4, nsam, nrow, nslice, xb, yb, zb);
+        }
         xb = __fadd_rn(xb, dm.d[0]);
         yb = __fadd_rn(yb, dm.d[1]);
         zb = __fadd_rn(zb, dm.d[2]);
       }
+      // SLAB: every lane has finished its run or passed the slab after this step
+      const bool finished = SLAB && __all_sync(0xffffffffu, j >= i2);
+      if (!SLAB || __any_sync(0xffffffffu, v != 0.0f)) {
 #pragma unroll
-      for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
-      if (lane == 0 && v != 0.0f) atomicAdd(row + (j - 1), v);
+        for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+        if (lane == 0 && v != 0.0f) atomicAdd(row + (j - 1), v);
+      }
+      if (finished) break;
     }
   }
 }
@@ -176,6 +201,16 @@ constexpr size_t kSlabBytes = size_t(64) << 20;
 static size_t quad_fwd_max() {
   const char* e = getenv("SPI_PJ_QUADMAX");
   return e ? (size_t)std::max(0LL, atoll(e)) << 20 : size_t(8) << 30;
+}
+// z slabs of the forward projection for a packed volume of `bytes`: one pass
+// up to twice kCellMaxBytes, above that slabs of at most kCellMaxBytes whose
+// quads stay in L2 (wpro_warp_kernel<FORM, true>).  Plans at 256^3 (268 MB
+// of quads, 3 slabs), 500 projections: 15.0k against 13.4k projections/s in
+// one pass (64 MB slabs 14.4k, 32 MB 11.0k; cells in 96 MB slabs 12.5k); at
+// 192^3 (113 MB of quads) two slabs were 9% slower than one pass.
+static int fwd_slabs(size_t bytes) {
+  if (bytes <= 2 * kCellMaxBytes) return 1;
+  return (int)((bytes + kCellMaxBytes - 1) / kCellMaxBytes);
 }
 enum PjForm { kPjPlain = 0, kPjQuads = 1, kPjCells = 2 };
 static int pj_fwd_form(size_t nvox) {
@@ -396,13 +431,14 @@ void pj_release(spi_ctx* c) {
 
 // The runs of every row y in order of |z| (ties: -z first), cut into tasks of
 // at most 32 runs: rows[0..nruns) are the runs, then ntasks int4 tasks.
-static void row_tasks(const std::vector<PjRun>& runs, std::vector<PjRun>& rowruns, std::vector<int4>& tasks) {
+static void row_tasks(const std::vector<PjRun>& runs, std::vector<PjRun>& rowruns, std::vector<int4>& tasks,
+                      bool z_order) {
   std::vector<int> order(runs.size());
   for (size_t i = 0; i < runs.size(); ++i) order[i] = (int)i;
   std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
     const PjRun &a = runs[p], &b = runs[q];
     if (a.y != b.y) return a.y < b.y;
-    return std::abs(a.z) < std::abs(b.z);
+    return z_order ? a.z < b.z : std::abs(a.z) < std::abs(b.z);
   });
   rowruns.clear();
   tasks.clear();
@@ -421,7 +457,7 @@ static void row_tasks(const std::vector<PjRun>& runs, std::vector<PjRun>& rowrun
 }
 
 int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out,
-              int* ntasks_out) {
+              int* ntasks_out, bool z_order) {
   if (!c) return fail(kInvalid, "NULL context");
   if (nx < 4 || ny < 4 || nz < 4) return fail(kInvalid, "PJ 3Q: volume %dx%dx%d too small", nx, ny, nz);
   if (nang < 0 || (nang > 0 && !angles)) return fail(kInvalid, "PJ 3Q: bad angle list");
@@ -440,7 +476,7 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
   SPI_CUDA(cudaMemcpyAsync(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice, c->stream));
   std::vector<PjRun> rowruns;
   std::vector<int4> tasks;
-  row_tasks(runs, rowruns, tasks);
+  row_tasks(runs, rowruns, tasks, z_order);
   const size_t rbytes = rowruns.size() * sizeof(PjRun), toff = pj_tasks_offset((int)rowruns.size());
   SPI_TRY(c->pj_rows.ensure(toff + std::max<size_t>(1, tasks.size()) * sizeof(int4)));
   if (!rowruns.empty()) {
@@ -485,14 +521,32 @@ static int pj_forward(spi_ctx* c, cudaStream_t st, const float* vol, int form, f
   const int blocks = (int)std::min<long long>((warps + 3) / 4, (long long)c->sm_count * 16);
   const PjRun* rr = static_cast<const PjRun*>(rows);
   const int4* tk = pj_tasks_of(rows, nruns);
-  if (form == kPjCells)
-    wpro_warp_kernel<kPjCells><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx, ldpy, ldpz,
-                                                       out);
-  else
-    wpro_warp_kernel<kPjQuads><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx, ldpy, ldpz,
-                                                       out);
-  SPI_TRY(check_kernel("wpro_warp_kernel"));
-  c->count(2);
+  const int S = fwd_slabs(pj_packed_bytes(form, nvox));
+  if (S == 1) {
+    if (form == kPjCells)
+      wpro_warp_kernel<kPjCells, false><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx,
+                                                                ldpy, ldpz, 1, nz, out);
+    else
+      wpro_warp_kernel<kPjQuads, false><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx,
+                                                                ldpy, ldpz, 1, nz, out);
+    SPI_TRY(check_kernel("wpro_warp_kernel"));
+    c->count(2);
+    return 0;
+  }
+  // cells have IOZ = 1 .. nz-1; S slabs of T planes each
+  const int T = (nz - 1 + S - 1) / S;
+  for (int zlo = 1; zlo < nz; zlo += T) {
+    const int zhi = std::min(nz, zlo + T);
+    if (form == kPjCells)
+      wpro_warp_kernel<kPjCells, true><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx,
+                                                               ldpy, ldpz, zlo, zhi, out);
+    else
+      wpro_warp_kernel<kPjQuads, true><<<blocks, 128, 0, st>>>(packed, nx, ny, nz, rr, tk, ntasks, dms, nang, ldpx,
+                                                               ldpy, ldpz, zlo, zhi, out);
+    SPI_TRY(check_kernel("wpro_warp_kernel"));
+    c->count();
+  }
+  c->count();
   return 0;
 }
 
@@ -545,7 +599,9 @@ extern "C" {
 int spi_pj3q(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, const float* angles, int nang,
              float* proj_out, int on_device) {
   int nruns = 0, ntasks = 0;
-  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks));
+  const int form = pj_fwd_form((size_t)nx * ny * nz);
+  const bool slabbed = form != kPjPlain && fwd_slabs(pj_packed_bytes(form, (size_t)nx * ny * nz)) > 1;
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks, slabbed));
   if (!vol || !proj_out) return fail(kInvalid, "PJ 3Q: NULL buffer");
   const size_t vbytes = (size_t)nx * ny * nz * sizeof(float);
   const size_t pbytes = (size_t)nang * nx * ny * sizeof(float);
@@ -561,7 +617,6 @@ int spi_pj3q(spi_ctx* c, const float* vol, int nx, int ny, int nz, float ri, con
   if (nang == 0) return 0;
   SPI_CUDA(cudaMemsetAsync(dout, 0, pbytes, c->stream));
   const size_t nvox = (size_t)nx * ny * nz;
-  const int form = pj_fwd_form(nvox);
   float4* packed = nullptr;
   if (nruns > 0 && form != kPjPlain) {
     SPI_TRY(c->pj_v4.ensure(pj_packed_bytes(form, nvox)));
@@ -629,7 +684,11 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   *out = nullptr;
   if (nang <= 0) return fail(kInvalid, "spi_pj3q_plan_create: nang = %d", nang);
   int nruns = 0, ntasks = 0;
-  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks));   // runs and matrices into the context's buffers
+  const size_t nvox = (size_t)nx * ny * nz;
+  const int form = pj_fwd_form(nvox);
+  const bool slabbed = form != kPjPlain && fwd_slabs(pj_packed_bytes(form, nvox)) > 1;
+  // runs, row tasks and matrices into the context's buffers
+  SPI_TRY(pj_common(c, nx, ny, nz, ri, angles, nang, &nruns, &ntasks, slabbed));
   auto* p = new spi_pj3q_plan();
   p->ctx = c;
   p->device = c->device;
@@ -638,8 +697,7 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
   if (e == cudaSuccess) e = cudaMalloc(&p->dms, (size_t)nang * sizeof(PjDM));
   if (e == cudaSuccess) e = cudaMalloc(&p->rows, rows_bytes);
-  const size_t nvox = (size_t)nx * ny * nz;
-  p->form = nruns ? pj_fwd_form(nvox) : kPjPlain;
+  p->form = nruns ? form : kPjPlain;
   if (e == cudaSuccess && p->form != kPjPlain) e = cudaMalloc(&p->v4, pj_packed_bytes(p->form, nvox));
   if (e == cudaSuccess && nruns && nvox * sizeof(float4) <= quad_fwd_max()) e = cudaMalloc(&p->q4, nvox * sizeof(float4));
   if (e == cudaSuccess && nruns)
