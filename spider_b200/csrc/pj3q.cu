@@ -429,32 +429,6 @@ void pj_release(spi_ctx* c) {
   c->pjf_n = 0;
 }
 
-// The runs of every row y in order of |z| (ties: -z first), cut into tasks of
-// at most 32 runs: rows[0..nruns) are the runs, then ntasks int4 tasks.
-static void row_tasks(const std::vector<PjRun>& runs, std::vector<PjRun>& rowruns, std::vector<int4>& tasks,
-                      bool z_order) {
-  std::vector<int> order(runs.size());
-  for (size_t i = 0; i < runs.size(); ++i) order[i] = (int)i;
-  std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
-    const PjRun &a = runs[p], &b = runs[q];
-    if (a.y != b.y) return a.y < b.y;
-    return z_order ? a.z < b.z : std::abs(a.z) < std::abs(b.z);
-  });
-  rowruns.clear();
-  tasks.clear();
-  for (int i : order) rowruns.push_back(runs[i]);
-  for (size_t i = 0; i < rowruns.size();) {
-    size_t e = i + 1;
-    while (e < rowruns.size() && e - i < 32 && rowruns[e].y == rowruns[i].y) ++e;
-    int j1 = rowruns[i].i1, j2 = rowruns[i].i2;
-    for (size_t q = i; q < e; ++q) {
-      j1 = std::min(j1, rowruns[q].i1);
-      j2 = std::max(j2, rowruns[q].i2);
-    }
-    tasks.push_back(make_int4((int)i, (int)(e - i), j1, j2));
-    i = e;
-  }
-}
 
 int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles, int nang, int* nruns_out,
               int* ntasks_out, bool z_order) {
@@ -475,8 +449,9 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
     SPI_CUDA(cudaMemcpyAsync(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice, c->stream));
   std::vector<PjRun> rowruns;
-  std::vector<int4> tasks;
-  row_tasks(runs, rowruns, tasks, z_order);
+  std::vector<std::array<int, 4>> tasks;
+  row_tasks(runs, z_order, rowruns, tasks);
+  static_assert(sizeof(std::array<int, 4>) == sizeof(int4), "row tasks are uploaded as int4");
   const size_t rbytes = rowruns.size() * sizeof(PjRun), toff = pj_tasks_offset((int)rowruns.size());
   SPI_TRY(c->pj_rows.ensure(toff + std::max<size_t>(1, tasks.size()) * sizeof(int4)));
   if (!rowruns.empty()) {

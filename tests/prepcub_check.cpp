@@ -1,9 +1,17 @@
 // Compares spider_b200/csrc/pj_runs.h (PREPCUB run finding by interval) with
 // a voxel-by-voxel restatement of PREPCUB (prepcub.f:54-109): every voxel of
 // every x line tested with t3*t3 + yy <= r in REAL, the first that passes
-// opening the run and every later one that passes extending it.  Prints the
-// number of cases and mismatches; exit status 1 on any mismatch.
+// opening the run and every later one that passes extending it.  Then checks
+// the row tasks built from those runs, in both orders: the reordered runs
+// are a permutation of the runs, grouped by row in the requested order, and
+// the tasks tile them with at most 32 runs of one row each and the union of
+// their x ranges.  Prints the number of cases and mismatches; exit status 1
+// on any mismatch.
+#include <algorithm>
+#include <array>
 #include <cstdio>
+#include <cstdlib>
+#include <tuple>
 #include <vector>
 
 #include "../spider_b200/csrc/pj_runs.h"
@@ -34,6 +42,40 @@ static void by_voxel(int nsam, int nrow, int nslice, float ri, int ldpx, int ldp
   }
 }
 
+static bool tasks_ok(const std::vector<Run>& runs, bool z_order) {
+  std::vector<Run> rr;
+  std::vector<std::array<int, 4>> tasks;
+  spi::row_tasks(runs, z_order, rr, tasks);
+  if (rr.size() != runs.size()) return false;
+  auto key = [](const Run& r) { return std::make_tuple(r.y, r.z, r.i1, r.i2); };
+  std::vector<std::tuple<int, int, int, int>> a, b;
+  for (const Run& r : runs) a.push_back(key(r));
+  for (const Run& r : rr) b.push_back(key(r));
+  std::sort(a.begin(), a.end());
+  std::sort(b.begin(), b.end());
+  if (a != b) return false;
+  for (size_t i = 1; i < rr.size(); ++i) {
+    if (rr[i].y < rr[i - 1].y) return false;
+    if (rr[i].y == rr[i - 1].y) {
+      const int p = z_order ? rr[i - 1].z : std::abs(rr[i - 1].z), q = z_order ? rr[i].z : std::abs(rr[i].z);
+      if (q < p) return false;
+    }
+  }
+  size_t next = 0;
+  for (const auto& t : tasks) {
+    if ((size_t)t[0] != next || t[1] < 1 || t[1] > 32) return false;
+    int x1 = rr[t[0]].i1, x2 = rr[t[0]].i2;
+    for (int q = t[0]; q < t[0] + t[1]; ++q) {
+      if (rr[q].y != rr[t[0]].y) return false;
+      x1 = std::min(x1, rr[q].i1);
+      x2 = std::max(x2, rr[q].i2);
+    }
+    if (x1 != t[2] || x2 != t[3]) return false;
+    next += t[1];
+  }
+  return next == rr.size();
+}
+
 int main() {
   const int shapes[][3] = {{4, 4, 4},     {5, 7, 6},       {32, 32, 32},   {33, 31, 30},
                            {40, 36, 33},  {64, 64, 64},    {75, 75, 75},   {128, 128, 128},
@@ -57,6 +99,11 @@ int main() {
           ++bad;
           std::printf("mismatch %dx%dx%d ri=%g shift=%d: %zu vs %zu runs\n", nx, ny, nz, ri, shift, a.size(), b.size());
         }
+        for (bool zo : {false, true})
+          if (!tasks_ok(b, zo)) {
+            ++bad;
+            std::printf("bad row tasks %dx%dx%d ri=%g shift=%d z_order=%d\n", nx, ny, nz, ri, shift, (int)zo);
+          }
       }
   std::printf("%lld cases, %lld mismatches\n", cases, bad);
   return bad != 0;

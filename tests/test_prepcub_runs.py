@@ -1,7 +1,8 @@
 """PREPCUB run finding (prepcub.f:54-109) as the library does it, by one
 interval per x line, against the reference's voxel-by-voxel test: the same
-runs over shapes, radii and centres (tests/prepcub_check.cpp, built with the
-host C++ compiler)."""
+runs over shapes, radii and centres; and the row tasks of the warp forward
+projections built from them, in both orders (tests/prepcub_check.cpp, built
+with the host C++ compiler)."""
 import os
 import shutil
 import subprocess
