@@ -190,16 +190,24 @@ int spi_pj3f(spi_ctx* ctx, const float* vol, int nx, int ny, int nz, float ri,
  * addition for callers that must not allocate device memory: applications
  * whose device memory belongs to a fixed arena or caching allocator, and
  * latency-critical pipelines that cannot take cudaMalloc/cudaFree's implicit
- * synchronisation.  Same result as spi_pj3q (up to the order of its FP32
- * atomic sums).  vol (float[nz*ny*nx]), angles (float[3*nang]: psi, theta,
+ * synchronisation.  Same operator as spi_pj3q: its rotation matrices are
+ * built on the device with the host's FP64 operation order (they differ only
+ * where the device's and host's cos/sin differ in a last bit that also moves
+ * the single-precision rounding), and its sums differ in the order of the
+ * FP32 atomic additions.  vol (float[nz*ny*nx]), angles (float[3*nang]: psi, theta,
  * phi) and proj_out (float[nang*ny*nx]) are device pointers on the current
  * device; work is queued on `stream` (cudaStream_t, NULL = legacy stream) and
  * the call returns without waiting for it.  Its scratch (voxel runs and
  * rotation matrices) is one file-scope __device__ array of 1,114,112 bytes,
  * which every GPU that loads the library holds until exit; hence the limits
  * ny*nz <= 65536 and nang <= 16384 per call (larger requests return 101).
- * The first call on a device looks up that array's device address, so make
- * it before any stream capture.  Every call shares the array and overwrites
+ * Each call looks up that array's device address, which allocates nothing.
+ * Under lazy module loading (CUDA_MODULE_LOADING=LAZY, the CUDA default) the
+ * first call on a device may be what loads the library's device code, and
+ * with it the array: that load is the driver's one implicit allocation, so
+ * make the first call before any stream capture and before the caller's
+ * memory budget is fixed (or set CUDA_MODULE_LOADING=EAGER, which loads it
+ * with the context).  Every call shares the array and overwrites
  * it, so calls that overlap on the GPU (different streams, or different host
  * threads on the same device) race; serialise them. */
 int spi_pj3q_noalloc(const float* vol, int nx, int ny, int nz, float ri, const float* angles,

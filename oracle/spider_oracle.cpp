@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <climits>
 #include <complex>
 #include <cstdint>
 #include <cstring>
@@ -318,8 +319,13 @@ void rtsq(const float* in, float* out, int nx, int ny, float theta, float shxi, 
 
 // ONELINE, oneline.f:38-200 (called as ONELINE(J,N2,NX,...), bp3f.f:477:
 // callee N = 2*NX, callee N2 = NX)
+//
+// zlo/zhi: only taps whose signed z index (izp for the main taps, -izp for
+// the reflected ones; -NX < z < NX) lies in [zlo, zhi) are applied -- the
+// owner-computes schedule of insert_images_owned.  The defaults apply all.
 template <class R>
-void oneline(int J, Grid<R>& g, const std::complex<R>* bi, const float* dm, const KBTable& kb) {
+void oneline(int J, Grid<R>& g, const std::complex<R>* bi, const float* dm, const KBTable& kb,
+             int zlo = INT_MIN, int zhi = INT_MAX) {
   const int N = g.n, N2 = g.nx, LN2 = kb.ln2;
   const int JP = (J >= 0) ? J : N + J;
   const float fltb = kb.fltb;
@@ -341,10 +347,14 @@ void oneline(int J, Grid<R>& g, const std::complex<R>* bi, const float* dm, cons
     if (!(ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
           izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1)))
       continue;
+    // none of this pixel's taps lands in the owned z range
+    if (!(izn + LN2 >= zlo && izn - LN2 < zhi) && !(ixn < LN2 && -izn + LN2 >= zlo && -izn - LN2 < zhi))
+      continue;
     if (ixn >= 0) {
       int lb = -std::min(ixn, LN2);
       for (int lz = -LN2; lz <= LN2; ++lz) {
         int izp = izn + lz;
+        if (izp < zlo || izp >= zhi) continue;
         int iza = (izp >= 0) ? izp : N + izp;
         float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
         if (tz == 0.0f) continue;
@@ -367,6 +377,7 @@ void oneline(int J, Grid<R>& g, const std::complex<R>* bi, const float* dm, cons
     if (ixn < LN2) {  // reflected points, oneline.f:118-150
       for (int lz = -LN2; lz <= LN2; ++lz) {
         int izp = izn + lz;
+        if (-izp < zlo || -izp >= zhi) continue;
         int izt = (izp > 0) ? N - izp : -izp;
         float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
         if (tz == 0.0f) continue;
@@ -653,12 +664,70 @@ void insert_images(std::vector<Grid<R>*>& grids, const float* imgs, int nx, int 
       // with J = 0 or 3 (mod 6) holds rows J and -J, which write the same
       // Friedel-mirrored voxels, and oblique rows 6 apart can share taps, so
       // with more than one thread updates are lost (rel-l2 ~1e-4 at 128^3,
-      // varying run to run).  Parity checks run it with one thread; the
-      // threaded form serves as the timed CPU baseline.
+      // varying run to run).  The checker runs it with one thread or uses
+      // insert_images_owned; the threaded form is the timed CPU baseline.
       const int ln1 = 6;
       for (int jt = 1; jt <= ln1; ++jt) {
         #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
         for (int J = -nx + jt; J <= nx; J += ln1) oneline<R>(J, g, bi.data(), dms, kb);
+      }
+    }
+  }
+}
+
+// Race-free parallel form of the same image loop (owner computes).  Thread t
+// of T owns a contiguous range of signed z planes, balanced by the expected
+// tap density of central sections (proportional to NX - |z|), and walks every
+// image, symmetry and row in the serial order, applying only the taps that
+// land in its planes.  Each voxel therefore receives exactly the additions of
+// the one-thread loop, in the same order: the grids are bit-identical to the
+// serial result for any thread count.  Images are staged (PADD2 + FFT) in
+// parallel batches first.
+template <class R>
+void insert_images_owned(std::vector<Grid<R>*>& grids, const float* imgs, int nx, int nang,
+                         const float* dm9, const float* sm9, int nsym, const uint8_t* route,
+                         const KBTable& kb, int nthreads) {
+  const int n = 2 * nx;
+  FFT1 fx(n, -1), fy(n, -1);
+  const int T = std::max(1, nthreads);
+  // z ranges: signed z runs over [-nx+1, nx-1]
+  std::vector<int> zb(T + 1);
+  {
+    double tot = 0.0;
+    for (int z = -nx + 1; z <= nx - 1; ++z) tot += (double)(nx - std::abs(z));
+    double acc = 0.0;
+    int t = 1;
+    zb[0] = -nx + 1;
+    for (int z = -nx + 1; z <= nx - 1 && t < T; ++z) {
+      acc += (double)(nx - std::abs(z));
+      while (t < T && acc >= tot * t / T) zb[t++] = z + 1;
+    }
+    while (t < T) zb[t++] = nx;
+    zb[T] = nx;
+  }
+  const size_t spec = (size_t)(nx + 1) * n;
+  const int batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)nang,
+                                                               ((size_t)512 << 20) / (spec * sizeof(std::complex<R>))));
+  std::vector<std::vector<std::complex<R>>> bis(batch);
+  const int ln1 = 6;
+  for (int a0 = 0; a0 < nang; a0 += batch) {
+    const int nb = std::min(batch, nang - a0);
+    #pragma omp parallel for num_threads(T) schedule(dynamic, 1)
+    for (int b = 0; b < nb; ++b) stage_image<R>(imgs + (size_t)(a0 + b) * nx * nx, nx, bis[b], fx, fy, 1);
+    #pragma omp parallel num_threads(T)
+    {
+      const int t = omp_get_thread_num();
+      const int zlo = zb[t], zhi = zb[t + 1];
+      for (int b = 0; b < nb; ++b) {
+        const int a = a0 + b;
+        Grid<R>& g = *grids[route ? route[a] : 0];
+        for (int is = 0; is < std::max(1, nsym); ++is) {
+          float dms[9];
+          if (nsym > 1) matmul33(sm9 + 9 * is, dm9 + 9 * a, dms);
+          else std::memcpy(dms, dm9 + 9 * a, sizeof(dms));
+          for (int jt = 1; jt <= ln1; ++jt)
+            for (int J = -nx + jt; J <= nx; J += ln1) oneline<R>(J, g, bis[b].data(), dms, kb, zlo, zhi);
+        }
       }
     }
   }
@@ -687,7 +756,7 @@ int bp_run(const float* imgs_in, int nx, int nang, const float* angles, const fl
   const float* imgs = imgs_in;
   if (inplane) {
     rot.resize((size_t)nang * nx * nx);
-    #pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static) if (use_rtsf)
+    #pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static)
     for (int a = 0; a < nang; ++a) {
       if (use_rtsf)
         rtsf(imgs_in + (size_t)a * nx * nx, &rot[(size_t)a * nx * nx], nx, inplane[3 * a], inplane[3 * a + 1],
@@ -711,7 +780,13 @@ int bp_run(const float* imgs_in, int nx, int nang, const float* angles, const fl
   if (half) { go = new Grid<R>(nx); grids.push_back(go); }
   std::vector<uint8_t> route;
   if (half) { route.resize(nang); for (int a = 0; a < nang; ++a) route[a] = half[a] ? 0 : 1; }
-  insert_images<R>(grids, imgs, nx, nang, dm.data(), sm.data(), nsym, half ? route.data() : nullptr, kb, nthreads);
+  // the checker never uses the reference's racy row striping: one thread
+  // runs the serial loop, more threads the owner-computes schedule (same sums)
+  if (nthreads > 1)
+    insert_images_owned<R>(grids, imgs, nx, nang, dm.data(), sm.data(), nsym, half ? route.data() : nullptr, kb,
+                           nthreads);
+  else
+    insert_images<R>(grids, imgs, nx, nang, dm.data(), sm.data(), nsym, half ? route.data() : nullptr, kb, 1);
   symplane0<R>(ge);
   if (go) symplane0<R>(*go);
   if (halt) {  // BP 3F P: partial X and W after SYMPLANE0

@@ -769,8 +769,6 @@ int spi_pj3q_plan_destroy(spi_pj3q_plan* p) {
 // __device__ array of fixed size (kNoAllocBytes, held by every GPU that loads
 // the library until the process exits) and takes all inputs and outputs as
 // caller-owned device pointers.
-#include <mutex>
-
 namespace spi {
 
 constexpr int kNoAllocMaxLines = 65536;  // ny * nz lines of voxels along x
@@ -783,45 +781,44 @@ constexpr size_t kNoAllocBytes = sizeof(NoAllocScratch);  // 1,114,112 bytes
 
 static __device__ __align__(256) unsigned char g_pj3q_scratch[kNoAllocBytes];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[256] = {};
-
-// Device address of g_pj3q_scratch on the current device, looked up once per
-// device (the host-side name is only a stand-in for the symbol).
+// Device address of g_pj3q_scratch on the current device.  The host-side
+// name is only a stand-in for the symbol, so the address is looked up on
+// every call: the lookup allocates nothing, and a cached address would go
+// stale if the device's primary context were released and the module loaded
+// again at another address.
 static int noalloc_scratch(NoAllocScratch** out) {
   int dev = -1;
   SPI_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) return fail(kDevice, "spi_pj3q_noalloc: device %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_pj3q_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(kCuda, "spi_pj3q_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
-    g_noalloc_addr[dev] = p;
-  }
-  *out = static_cast<NoAllocScratch*>(g_noalloc_addr[dev]);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_pj3q_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(kCuda, "spi_pj3q_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
+  *out = static_cast<NoAllocScratch*>(p);
   return 0;
 }
 
-// CANG in FP64 on the device (WPRO_N's inline matrix, wpro_n.f:65-81)
+// CANG in FP64 on the device (WPRO_N's inline matrix, wpro_n.f:65-81), with
+// the host's operation order and every product and sum rounded on its own
+// (no fused multiply-add), as host_math.cpp evaluates it.  The matrices then
+// equal spi_pj3q's unless the device's and the host's double cos/sin differ
+// in a last bit that also changes the single-precision rounding.
 __global__ void noalloc_dm_kernel(const float* __restrict__ angles, int nang, PjDM* __restrict__ dms) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= nang) return;
   const double d2r = (double)3.14159265358979323846f / 180.0;
-  const double psi = (double)angles[3 * a] * d2r, theta = (double)angles[3 * a + 1] * d2r,
-               phi = (double)angles[3 * a + 2] * d2r;
+  const double psi = __dmul_rn((double)angles[3 * a], d2r), theta = __dmul_rn((double)angles[3 * a + 1], d2r),
+               phi = __dmul_rn((double)angles[3 * a + 2], d2r);
   const double cphi = cos(phi), sphi = sin(phi), cthe = cos(theta), sthe = sin(theta), cpsi = cos(psi),
                spsi = sin(psi);
   float* d = dms[a].d;
-  d[0] = (float)(cphi * cthe * cpsi - sphi * spsi);
-  d[1] = (float)(sphi * cthe * cpsi + cphi * spsi);
-  d[2] = (float)(-sthe * cpsi);
-  d[3] = (float)(-cphi * cthe * spsi - sphi * cpsi);
-  d[4] = (float)(-sphi * cthe * spsi + cphi * cpsi);
-  d[5] = (float)(sthe * spsi);
-  d[6] = (float)(sthe * cphi);
-  d[7] = (float)(sthe * sphi);
+  d[0] = (float)__dsub_rn(__dmul_rn(__dmul_rn(cphi, cthe), cpsi), __dmul_rn(sphi, spsi));
+  d[1] = (float)__dadd_rn(__dmul_rn(__dmul_rn(sphi, cthe), cpsi), __dmul_rn(cphi, spsi));
+  d[2] = (float)__dmul_rn(-sthe, cpsi);
+  d[3] = (float)__dsub_rn(__dmul_rn(__dmul_rn(-cphi, cthe), spsi), __dmul_rn(sphi, cpsi));
+  d[4] = (float)__dadd_rn(__dmul_rn(__dmul_rn(-sphi, cthe), spsi), __dmul_rn(cphi, cpsi));
+  d[5] = (float)__dmul_rn(sthe, spsi);
+  d[6] = (float)__dmul_rn(sthe, cphi);
+  d[7] = (float)__dmul_rn(sthe, sphi);
   d[8] = (float)(cthe);
 }
 

@@ -47,7 +47,9 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
     gb = ctypes.c_longlong()
     _lib.check(L.spi_bp_grid_bytes(nx, ctypes.byref(gb)))
     dev = device or torch.device(f"cuda:{ctx.device}")
-    grids = [torch.zeros(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
+    # spi_bp_open zeroes attached grids on the library stream; torch.empty
+    # leaves no fill pending on torch's stream that could land after it
+    grids = [torch.empty(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
     _lib.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                      ctypes.c_void_p(grids[1].data_ptr())))
     try:
@@ -55,8 +57,11 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
         start, count = shard(int(imgs.shape[0]), rank, world)
         if count:
             ctx.bp_insert(imgs[start:start + count], angles[start:start + count], half[start:start + count])
-        torch.cuda.synchronize(dev)
+        torch.cuda.synchronize(dev)     # insertions ran on the library's own stream
         allreduce_grids(grids)
+        # NCCL orders the reduce on torch's current stream only; the library
+        # stream (non-blocking) would not wait for it before SYMPLANE0/NRMW2
+        torch.cuda.synchronize(dev)
         out = ctx.bp_finish(("all", "1", "2"))
         return out["all"], out["1"], out["2"]
     finally:
