@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--cg-n", type=int, default=128)
     p.add_argument("--cg-nang", type=int, default=10000)
     p.add_argument("--cg-iters", type=int, default=6)
+    p.add_argument("--check-images", type=int, default=8192,
+                   help="images of the FP64-oracle check of the 256^3 volumes (0 = skip)")
     return p.parse_args()
 
 
@@ -200,17 +202,51 @@ def cpu_baseline(nx, seconds, imgs_host, angles, half):
                       f"the reference's OpenMP row striping), {dt:.1f} s"}
 
 
+def fp64_check(ctx, nx, chunks, angles, halves, nimg, bf16):
+    """Relative L2 of the three BP 32F volumes against the FP64 oracle
+    (owner-computes schedule on all host cores) on `nimg` of the bench's
+    images (the two resident chunks with the angles of the first two steps),
+    for the compensated accumulation the bench times and for plain FP32
+    atomics."""
+    import oracle
+    from spider_b200 import synth
+    per = [min(nimg // 2, int(c.shape[0])) for c in chunks[:2]]
+    imgs = [chunks[k][:per[k]] for k in range(2)]
+    ang = np.concatenate([angles[k][:per[k]] for k in range(2)])
+    half = np.concatenate([halves[k][:per[k]] for k in range(2)])
+    gpu = {}
+    for name, comp in (("compensated", True), ("plain", False)):
+        ctx.set_accumulation(comp)
+        ctx.bp_open(nx, 2, bf16=bf16)
+        for k in range(2):
+            ctx.bp_insert(imgs[k], angles[k][:per[k]], halves[k][:per[k]])
+        o = ctx.bp_finish(("all", "1", "2"))
+        ctx.bp_close()
+        gpu[name] = (o["all"], o["1"], o["2"])
+    ctx.set_accumulation(True)
+    host = np.concatenate([t.cpu().numpy() for t in imgs])
+    t0 = time.perf_counter()
+    ref = oracle.bp32f(host, ang, half, prec=1)
+    dt = time.perf_counter() - t0
+    out = {"images": int(host.shape[0]), "oracle_s": dt, "oracle_threads": os.cpu_count()}
+    for name, vols in gpu.items():
+        out[name] = {k: synth.rel_l2(a, b) for k, a, b in zip(("all", "first", "second"), vols, ref)}
+    out["fsc_nyquist_compensated"] = float(synth.fsc(gpu["compensated"][0], ref[0])[nx // 2])
+    return out
+
+
 def cg_measure(args, ctx, stream, rank, world):
     """BP CG seconds per iteration (configuration: 128^3, 10,000 images of a
     50-blob phantom at SNR 0.3, lambda 1e-3, linear interpolation).
 
-    Each variant runs the solver twice, with 1 and with 1 + K iterations, and
+    Each form runs the solver twice, with 1 and with 1 + K iterations, and
     the difference of the two device-timed calls over K is the cost of one
     iteration (setup, image upload and the initial back-projection cancel).
-    Variants: FP64 CG vectors with each iteration replayed as a CUDA graph
-    (the default), the same without the graph, and FP32 vectors (the
-    reference's REAL storage).  rel_err_fp32_vs_fp64 compares the FP32-vector
-    volume with the FP64-vector one after 1 + K iterations."""
+    `value` is the library's default form, FP64 CG vectors with 47-bit
+    fixed-point projections (mode 2), each iteration replayed as a CUDA graph.
+    The other forms are reported beside it.  Accuracy of every form is stated
+    against the FP64 oracle on a fixed ill-conditioned check case (32^3, 120
+    images, 12 iterations, lambda 0.5)."""
     import torch
     from spider_b200 import ops, synth
     n, nang, K = args.cg_n, args.cg_nang, args.cg_iters
@@ -226,53 +262,181 @@ def cg_measure(args, ctx, stream, rank, world):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def timed(iters, fp64, interp="linear"):
+    def timed(p, a, iters, fp64, interp="linear", r=ri):
         e0.record(stream)
-        v, log = ops.bpcg(projs, ang, ri, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64=fp64,
+        v, log = ops.bpcg(p, a, r, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64=fp64,
                           interp=interp)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3, v, log
 
-    out = {}
-    vols = {}
-    for name, fp64, graph in (("fp64_graph", True, True), ("fp64_plain", True, False), ("fp32_graph", False, True),
-                              ("mixed_graph", "mixed", True), ("fast_graph", "fast", True),
-                              ("mixed64_graph", "mixed64", True)):
+    def per_iter(p, a, fp64, k, interp="linear", r=ri):
+        timed(p, a, 1, fp64, interp, r)          # warm-up (plans, buffers)
+        t1, _, _ = timed(p, a, 1, fp64, interp, r)
+        tk, v, _ = timed(p, a, 1 + k, fp64, interp, r)
+        return (tk - t1) / k, v
+
+    out, vols = {}, {}
+    for name, fp64, graph in (("mixed_graph", "mixed", True), ("fp64_graph", True, True),
+                              ("fp64_plain", True, False), ("fp32_graph", False, True),
+                              ("fast_graph", "fast", True), ("mixed64_graph", "mixed64", True)):
         if not graph:
             os.environ["SPI_CG_NOGRAPH"] = "1"
         try:
-            timed(1, fp64)                       # warm-up (plans, buffers)
-            t1, _, _ = timed(1, fp64)
-            tk, v, log = timed(1 + K, fp64)
+            out[name], vols[name] = per_iter(projs, ang, fp64, K)
         finally:
             os.environ.pop("SPI_CG_NOGRAPH", None)
-        out[name] = (tk - t1) / K
-        vols[name] = v
+
     def rel(name):
-        return float(np.linalg.norm((vols[name] - vols["fp64_graph"]).ravel()) /
-                     max(np.linalg.norm(vols["fp64_graph"].ravel()), 1e-30))
-    # headline: the fastest form within 1e-4 of the FP64 iteration
-    ok = [k for k in ("fast_graph", "mixed_graph", "mixed64_graph", "fp32_graph") if rel(k) <= 1e-4] + ["fp64_graph"]
-    best = min(ok, key=lambda k: out[k])
-    res = {"metric": "BP CG s/iter", "unit": "s/iter", "value": out[best], "form": best,
-           "fp64_s_per_iter": out["fp64_graph"],
-           "plain_gpu_s_per_iter": out["fp64_plain"], "fp32_vectors_s_per_iter": out["fp32_graph"],
-           "mixed_s_per_iter": out["mixed_graph"], "fast_s_per_iter": out["fast_graph"],
-           "mixed64_s_per_iter": out["mixed64_graph"], "rel_err_mixed64_vs_fp64": rel("mixed64_graph"),
-           "rel_err_fp32_vs_fp64": rel("fp32_graph"), "rel_err_mixed_vs_fp64": rel("mixed_graph"),
-           "rel_err_fast_vs_fp64": rel("fast_graph"),
+        return synth.rel_l2(vols[name], vols["fp64_graph"])
+
+    # roofline of the iteration (both operators): per image, A reads each
+    # sphere voxel and read-modify-writes a projection pixel, A^T reads the
+    # pixel table and read-modify-writes the voxel, 2 x (4 + 8) bytes per
+    # sphere voxel, plus the 4 n^2 bytes of the image
+    c = n // 2 + 1
+    g = np.arange(1, n + 1) - c
+    v_sphere = int(((g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= ri * ri).sum())
+    bytes_iter = nang * (2 * 12 * v_sphere + 4 * n * n)
+    peak, peak_kind = measured_peak()
+    achieved = bytes_iter / out["mixed_graph"] / 1e9
+    res = {"metric": "BP CG s/iter", "unit": "s/iter", "value": out["mixed_graph"],
+           "form": "mixed_graph: FP64 vectors, 47-bit fixed-point projections, FP32 PROJT (mode 2, the default)",
+           "fp64_s_per_iter": out["fp64_graph"], "plain_gpu_s_per_iter": out["fp64_plain"],
+           "fp32_vectors_s_per_iter": out["fp32_graph"], "fast_s_per_iter": out["fast_graph"],
+           "mixed64_s_per_iter": out["mixed64_graph"],
+           "rel_err_vs_fp64_form": {k: rel(k) for k in ("mixed_graph", "fast_graph", "mixed64_graph", "fp32_graph")},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": peak_kind, "algorithmic_bytes_per_iter": bytes_iter,
+                        "sphere_voxels": v_sphere,
+                        "note": "per image 2 x (4 + 8) B per sphere voxel + 4 n^2 B; the operators' tables and "
+                                "volumes stay in L2, so this is an algorithmic, not a DRAM, figure"},
            "config": {"n": n, "images": nang, "lambda": 1e-3, "mode": 1, "iterations_timed": K,
                       "phantom": "50 Gaussian blobs, sigma 2-8, SNR 0.3, uniform SO(3)"}}
+    res["check_vs_fp64_oracle"] = cg_oracle_check(ctx)
+    res["n256"] = cg_256_measure(args, ctx, stream, rank)
     res["differentiable_cg"] = autograd_cg_measure(ctx, projs, ang, ri, K)
+    res["differentiable_cg_fourier"] = fourier_cg_measure(ctx, projs, ang, K)
     # the 'F' answer (FBS interpolation), default precision mode: informational
-    timed(1, "mixed", "fbs")
-    t1, _, _ = timed(1, "mixed", "fbs")
-    tk, _, _ = timed(1 + K, "mixed", "fbs")
-    res["fbs_s_per_iter"] = (tk - t1) / K
+    res["fbs_s_per_iter"], _ = per_iter(projs, ang, "mixed", K, "fbs")
     if rank == 0 and world == 1 and not args.no_cpu:
         res["cpu_baseline"] = cg_cpu_baseline(projs, ang, ri, n)
     return res
+
+
+def cg_oracle_check(ctx):
+    """Relative error of each BP CG form against the FP64 oracle on a fixed
+    ill-conditioned case: 32^3, 120 PJ 3Q projections of a 12-blob phantom at
+    SNR 1, radius 13, lambda 0.5, 12 iterations (where the reference's REAL CG
+    drifts ~4e-2 from the exact iteration)."""
+    import oracle
+    from spider_b200 import ops, synth
+    rng = np.random.default_rng(4242)
+    n, nang = 32, 120
+    vol = synth.blob_phantom(n, 12, sigma=(1.5, 4.0), radius=0.35 * n, rng=rng)
+    ang = synth.so3_angles(nang, rng)
+    pr = synth.add_noise(oracle.pj3q(vol, ang), 1.0, rng)
+    kw = dict(errm=1e-7, chim=0.0, maxit=12, mode=1, lam=0.5)
+    ref, _, _, _ = oracle.bpcg(pr, ang, 13.0, prec=1, **kw)
+    out = {}
+    for name, fp64 in (("mixed", "mixed"), ("fast", "fast"), ("mixed64", "mixed64"), ("fp64", True),
+                       ("fp32", False)):
+        v, _ = ops.bpcg(pr, ang, 13.0, ctx=ctx, fp64=fp64, **kw)
+        out[name] = synth.rel_l2(v, ref)
+    ref32, _, _, _ = oracle.bpcg(pr, ang, 13.0, prec=0, **kw)
+    out["fp32_oracle"] = synth.rel_l2(ref32, ref)
+    return out
+
+
+def cg_256_measure(args, ctx, stream, rank, nang=10000, k=2):
+    """BP CG at 256^3 (configuration 5's box) in the default form: 10,000 PJ 3Q
+    projections of a 200-blob phantom at SNR 0.05, lambda 1e-3, seconds per
+    iteration from a 1- and a (1 + k)-iteration solve."""
+    import torch
+    from spider_b200 import ops, synth
+    n = 256
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(1105 + rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1105 + rank)
+    vol = make_phantom_gpu(n, 200, (1.5, 10.0), (0.5, 1.0), rng, dev)
+    ang = synth.so3_angles(nang, rng)
+    projs = torch.cat([make_chunk(ctx, vol, ang[a:a + 2500], 0.05, gen) for a in range(0, nang, 2500)]).cpu().numpy()
+    del vol
+    ri = float(n // 2 - 3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ts = []
+    for iters in (1, 1, 1 + k):
+        e0.record(stream)
+        ops.bpcg(projs, ang, ri, errm=0.0, chim=0.0, maxit=iters, mode=1, lam=1e-3, ctx=ctx, fp64="mixed")
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    return {"s_per_iter": (ts[2] - ts[1]) / k, "images": nang, "form": "mixed_graph (mode 2)",
+            "solve_1_iter_s": ts[1], "iterations_timed": k}
+
+
+def fourier_cg_measure(ctx, projs, ang, K, lam=1e-3, check_images=1000, check_iters=3):
+    """The differentiable reconstruction on the FourierSlice pair (E = central
+    slice extraction, E^T = ONELINE's insertion without weights): CG on
+    (E^T E + lam I) x = E^T b from the staged image spectra, one iteration
+    (the fused normal operator + FP64 dot products) replayed as a CUDA graph
+    against the same iteration launched op by op.  rel_err_vs_fp64_oracle: the
+    graph-captured CG after `check_iters` iterations against an FP64 CG on
+    the oracle's pair, on the first `check_images` images."""
+    import oracle
+    import torch
+    from spider_b200 import autograd
+    n = projs.shape[1]
+    imgs = torch.from_numpy(projs).cuda()
+    plan = autograd.FourierSlicePlan(n, ang, ctx=ctx)
+    b = plan.stage(imgs)
+    rhs = plan.adjoint(b)
+    del b
+    out = {}
+    for name, graph in (("graph_s_per_iter", True), ("plain_s_per_iter", False)):
+        times = []
+        for iters in (1, 1 + K):
+            solver = autograd.NormalCG(plan, lam, iters, graph=graph)
+            solver.solve(rhs)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            solver.solve(rhs)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        out[name] = (times[1] - times[0]) / K
+    plan.close()
+    del rhs
+    # FP64 check on a subset
+    sub = autograd.FourierSlicePlan(n, ang[:check_images], ctx=ctx)
+    bs = sub.stage(imgs[:check_images].contiguous())
+    x = autograd.NormalCG(sub, lam, check_iters, graph=True).solve(sub.adjoint(bs)).cpu().numpy().astype(np.float64)
+    bh = bs.cpu().numpy().astype(np.float64)
+    sub.close()
+    bh = bh[..., 0] + 1j * bh[..., 1]
+    a = ang[:check_images]
+    t0 = time.perf_counter()
+    r = oracle.fslice_insert(bh, a)
+    xr = np.zeros_like(r)
+    p = r.copy()
+    rs = np.vdot(r, r).real
+    for _ in range(check_iters):
+        ap = oracle.fslice_insert(oracle.fslice_extract(p, a), a) + lam * p
+        alpha = rs / np.vdot(p, ap).real
+        xr += alpha * p
+        r -= alpha * ap
+        rs_new = np.vdot(r, r).real
+        p = r + (rs_new / rs) * p
+        rs = rs_new
+    xg = x[..., 0] + 1j * x[..., 1]
+    out["rel_err_vs_fp64_oracle"] = float(np.linalg.norm(xg - xr) / np.linalg.norm(xr))
+    out["check"] = f"{check_images} images, {check_iters} iterations, oracle FP64 CG {time.perf_counter() - t0:.1f} s"
+    out["operator"] = "FourierSlice (central-slice extraction) and ONELINE insertion without weights, FP32, " \
+                      "fused E^T E + lam I, FP64 dot products"
+    return out
 
 
 def autograd_cg_measure(ctx, projs, ang, ri, K, lam=1e-3):
@@ -418,8 +582,8 @@ def run_ours(args):
         ctx.bp_insert(chunks[i % 2], angles[i], halves[i])
     torch.cuda.synchronize()
     L.spi_ctx_set_timing(ctx.handle, 1)
-    ms = (ctypes.c_double * 8)()
-    cnt = (ctypes.c_longlong * 8)()
+    ms = (ctypes.c_double * 9)()
+    cnt = (ctypes.c_longlong * 9)()
     L.spi_ctx_timing(ctx.handle, ms, cnt)   # reset
     clocks = ClockSampler(local)
     barrier()
@@ -443,6 +607,7 @@ def run_ours(args):
     L.spi_ctx_timing(ctx.handle, ms, cnt)
     insert_ms = ms[2]
     n_insert = max(int(cnt[2]), 1)
+    fold_ms = ms[8]
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([t_ms], device=dev)
@@ -455,8 +620,10 @@ def run_ours(args):
     f0 = time.perf_counter()
     if world > 1:
         import torch.distributed as dist
+        ctx.bp_flush()                       # grids hold the complete sums
         for g in grids:
             dist.all_reduce(g)
+        torch.cuda.synchronize()
     outs = ctx.bp_finish(("all", "1", "2"), device=True)
     torch.cuda.synchronize()
     finish_ms = (time.perf_counter() - f0) * 1e3
@@ -514,7 +681,7 @@ def run_ours(args):
                                       halves[i].ctypes.data_as(ctypes.c_void_p), 0))
         if world > 1:
             import torch.distributed as dist
-            torch.cuda.synchronize()   # the last insertions run on the library stream
+            ctx.bp_flush()             # the last insertions and folds are done on the library stream
             for g in grids:
                 dist.all_reduce(g)
             torch.cuda.synchronize()
@@ -539,6 +706,10 @@ def run_ours(args):
     if not args.no_cg and world == 1:
         cg = cg_measure(args, ctx, stream, rank, world)
 
+    check = None
+    if rank == 0 and world == 1 and args.check_images > 0:
+        check = fp64_check(ctx, nx, chunks, angles, halves, args.check_images, args.bf16)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         hc = chunks[0][:256].cpu().numpy()
@@ -554,8 +725,12 @@ def run_ours(args):
                        "nx": nx, "images_per_step": chunk, "spectra": "bf16" if args.bf16 else "f32",
                        "phantom": "200 Gaussian blobs, sigma 1.5-10, SNR 0.05, uniform SO(3)",
                        "l2": "inputs larger than L2 (1.07 GB images + 2.16 GB grids per step)",
+                       "accumulation": "FP32 vector atomics into a partial grid, two-sum folded into "
+                                       "grid + compensation every 4,096 images",
                        "parallelism": f"dp{world}" if world > 1 else "single GPU"},
             "roofline": roof,
+            "fold_ms_per_step": fold_ms / args.steps,
+            "rel_l2_vs_fp64": check,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

@@ -71,10 +71,11 @@ void* spi_ctx_stream(const spi_ctx* ctx);
  * milliseconds accumulated; spi_ctx_timing copies SPI_NPHASE totals and
  * resets them.  Phases: 0 stage (PADD2), 1 2D FFT, 2 insert (ONELINE),
  * 3 SYMPLANE0, 4 NRMW2, 5 3D FFT, 6 WINDKB2A, 7 host-to-device copies
- * (only when they are not overlapped).  The events cost the overlap of
- * host-image uploads with the compute (measured: uploads then run serially),
- * so leave timing off outside diagnostics. */
-#define SPI_NPHASE 8
+ * (only when they are not overlapped), 8 folds of the compensated
+ * accumulation.  The events cost the overlap of host-image uploads with the
+ * compute (measured: uploads then run serially), so leave timing off
+ * outside diagnostics. */
+#define SPI_NPHASE 9
 int spi_ctx_set_timing(spi_ctx* ctx, int on);
 int spi_ctx_timing(spi_ctx* ctx, double* ms_out, long long* count_out);
 
@@ -103,6 +104,24 @@ int spi_bp_grid_bytes(int nx, long long* bytes);
 
 /* Spectrum storage for subsequent inserts: 0 = FP32 (default), 1 = BF16. */
 int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
+
+/* Grid accumulation of the next spi_bp_open (no counterpart in the
+ * reference, whose X += BTQ*W, oneline.f:107-110, is a plain REAL sum).
+ * compensated = 1 (default; environment SPI_BP_ACCUM=0 changes the default):
+ * the taps of each run of `fold_every` images (0 = the default, 4,096 or
+ * SPI_BP_FOLD) are summed with FP32 atomics into a partial grid, which is
+ * then folded into the grid by an error-free two-sum whose rounding errors
+ * are kept in a compensation grid; the compensation is added in once before
+ * SYMPLANE0.  The error of the sums then grows with the images per fold, not
+ * with all images.  Costs two more grid-sized buffers and one pass over
+ * them per fold.  compensated = 0: every tap is added straight into the
+ * grid.  Fails with 101 while a reconstruction is open. */
+int spi_bp_set_accumulation(spi_ctx* ctx, int compensated, int fold_every);
+
+/* Complete the grids of the open reconstruction: fold pending partial sums
+ * and add the compensation in, so that caller-owned grids hold the full sums
+ * (call before summing them across processes).  Synchronises the stream. */
+int spi_bp_flush(spi_ctx* ctx);
 
 /* Autotune the insertion launch of the open reconstruction (no counterpart
  * in the reference, whose insertion is a fixed OpenMP loop): times the
@@ -239,6 +258,46 @@ int spi_pj3q_plan_create(spi_ctx* ctx, int nx, int ny, int nz, float ri, const f
 int spi_pj3q_plan_forward(const spi_pj3q_plan* plan, const float* vol, float* proj_out, void* stream);
 int spi_pj3q_plan_adjoint(const spi_pj3q_plan* plan, const float* projs, float* vol_out, void* stream);
 int spi_pj3q_plan_destroy(spi_pj3q_plan* plan);
+
+/* ------------------------------------------------------------------ *
+ * FourierSlice: the central-slice operator pair on ONELINE's geometry
+ * (no counterpart in the reference, which has the insertion, ONELINE
+ * oneline.f:38-200, but no extraction with the same kernel).
+ *   forward E: grid -> slices, the exact adjoint of the insertion;
+ *   adjoint E^T: slices -> grid, ONELINE's X += BTQ*W without the weight
+ *   grid (same voxels, table weights, Hermitian flips and reflected points).
+ * A grid is float2 [2nx][2nx][nx+1] (complex, i fastest: Fortran
+ * X(0:NX,N,N)); slices are float2 [nang][2nx][nx+1] in the layout and sign of
+ * the staged spectra (spi_fslice_stage: PADD2, phase, 2D R2C; ONELINE's BI is
+ * their conjugate).  All pointers are device pointers; `stream` is a
+ * cudaStream_t (NULL = legacy stream).  forward, adjoint and normal allocate
+ * nothing and do not synchronise, so they can be captured in a CUDA graph.
+ * ------------------------------------------------------------------ */
+typedef struct spi_fslice_plan spi_fslice_plan;
+
+/* Slice geometry of nang angle triples (host float[3*nang], psi, theta, phi)
+ * for box nx (8..512): CANG per slice (cang.f:44-81) and the FILLBESSIL table
+ * (fillbessi0.f:88-125), uploaded once. */
+int spi_fslice_plan_create(spi_ctx* ctx, int nx, const float* angles, int nang, spi_fslice_plan** plan);
+/* Slices of nang device images float[nang*nx*nx]: PADD2 + ASTA_D + phase
+ * (bp3f.f:1307-1343, asta.f:61-92, bp3f.f:453-458) and the 2D transform.
+ * Its batch buffer and FFT plans are made on the first call. */
+int spi_fslice_stage(spi_fslice_plan* plan, const float* imgs, float* slices, void* stream);
+/* slices = E grid (overwritten; pixels without taps are zero). */
+int spi_fslice_forward(const spi_fslice_plan* plan, const float* grid, float* slices, void* stream);
+/* grid = E^T slices (overwritten). */
+int spi_fslice_adjoint(const spi_fslice_plan* plan, const float* slices, float* grid, void* stream);
+/* grid_out = E^T E grid_in + lam * grid_in in one pass over the taps
+ * (grid_out must not alias grid_in). */
+int spi_fslice_normal(const spi_fslice_plan* plan, const float* grid_in, float lam, float* grid_out, void* stream);
+/* Real-space volume float[nx^3] of a grid of spectrum coefficients: the grid
+ * models V(k) = sum_v X_v K(k - v), so the volume is the inverse transform of
+ * X (plane 0 replaced by its Hermitian part, phase (-1)^(i+j+k), SPIDER's
+ * inverse sign, 1/n^3) multiplied by |WKB| (WINDKB2A's table,
+ * bp32f.f:964-1005) inside radius nx/2 and zero outside.  Its buffers and
+ * FFT plan are made on the first call. */
+int spi_fslice_volume(spi_fslice_plan* plan, const float* grid, float* vol_out, void* stream);
+int spi_fslice_plan_destroy(spi_fslice_plan* plan);
 
 /* ------------------------------------------------------------------ *
  * BP CG, linear interpolation (BPCG, bpcg.f:70 -> BPCG_2 bpcg.f:425,

@@ -90,6 +90,10 @@ def lib():
         L.orc_hiang.argtypes = [_f32p, ctypes.c_int, _f32p, _i32p, _f32p]
         L.orc_hiang.restype = ctypes.c_int
         L.orc_fixedge.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, ctypes.c_int]
+        L.orc_fslice_insert.argtypes = [_f64p, ctypes.c_int, _f32p, ctypes.c_int, _f64p, ctypes.c_int]
+        L.orc_fslice_insert.restype = None
+        L.orc_fslice_extract.argtypes = [_f64p, ctypes.c_int, _f32p, ctypes.c_int, _f64p, ctypes.c_int]
+        L.orc_fslice_extract.restype = None
         L.orc_prepcub_s_count.argtypes = [ctypes.c_int, ctypes.c_float]
         L.orc_prepcub_s_count.restype = ctypes.c_int
         _lib = L
@@ -386,4 +390,28 @@ def prjcq_fbs3(vol, angles, prec=1):
     n = vol.shape[0]
     out = np.zeros((ang.shape[0], n, n), np.float32)
     lib().orc_prjcq_fbs3(_p(vol, _f32p), n, _p(ang, _f32p), ang.shape[0], prec, _p(out, _f32p))
+    return out
+
+
+def fslice_extract(grid, angles, *, nthreads=0):
+    """FourierSlice forward in FP64: complex grid [2nx, 2nx, nx+1] -> slices
+    [nang, 2nx, nx+1] (the adjoint of ONELINE's insertion without weights)."""
+    X = np.ascontiguousarray(grid, dtype=np.complex128)
+    n, nx = X.shape[0], X.shape[2] - 1
+    ang = _f32(angles)
+    out = np.zeros((ang.shape[0], n, nx + 1), np.complex128)
+    lib().orc_fslice_extract(X.ctypes.data_as(_f64p), nx, _p(ang, _f32p), ang.shape[0], out.ctypes.data_as(_f64p),
+                             nthreads)
+    return out
+
+
+def fslice_insert(slices, angles, *, nthreads=0):
+    """FourierSlice adjoint in FP64: slices [nang, 2nx, nx+1] -> grid
+    [2nx, 2nx, nx+1] (ONELINE's insertion of X without weights)."""
+    T = np.ascontiguousarray(slices, dtype=np.complex128)
+    n, nx = T.shape[1], T.shape[2] - 1
+    ang = _f32(angles)
+    out = np.zeros((n, n, nx + 1), np.complex128)
+    lib().orc_fslice_insert(T.ctypes.data_as(_f64p), nx, _p(ang, _f32p), ang.shape[0], out.ctypes.data_as(_f64p),
+                            nthreads)
     return out

@@ -1557,7 +1557,152 @@ int bpcg_run(const float* projs, int n, int nang, const float* angles, float ri,
 }  // namespace
 
 // ============================================================ C ABI =======
+// ------------------------------------------- FourierSlice (P1 adjoint) ----
+// The central-slice pair on ONELINE's geometry with the weights W dropped
+// (no counterpart in the reference).  The slice values T are in the layout
+// and sign of the staged spectra the insertion reads (cuFFT R2C of the
+// padded, shifted image; ONELINE's BI = conj(T)).  Every tap -- voxel,
+// table weight, Hermitian flip and reflected point -- is enumerated exactly
+// as oneline() does (oneline.f:38-200), so
+//   insert:  X[v] += wg * BTQ (main taps), X[v'] += wg * conj(BTQ) (reflected),
+//            BTQ = BI, or conj(BI) for a pixel whose x < 0 was flipped;
+//   extract: the real-linear adjoint of insert,
+//            BI_adj = sum wg * X[v] + sum wg * conj(X[v']), conj'ed for a
+//            flipped pixel, and T = conj(BI_adj).
+// visit(I, flipped, q, wg, reflected) for every nonzero tap of row J whose
+// signed z index (izp for main taps, -izp for reflected ones) lies in
+// [zlo, zhi), as oneline() filters it for the owner-computes schedule.
+template <class F>
+void oneline_taps(int J, int nx, const float* dm, const KBTable& kb, F&& visit, int zlo = INT_MIN,
+                  int zhi = INT_MAX) {
+  const int N = 2 * nx, N2 = nx, LN2 = kb.ln2;
+  const float fltb = kb.fltb;
+  auto idx = [&](int i, int j, int k) { return ((size_t)k * N + j) * (nx + 1) + i; };
+  for (int I = 0; I <= N2; ++I) {
+    if (!((I * I + J * J) < (N * N / 4) && !(I == 0 && J < 0))) continue;
+    float xnew = (float)I * dm[0] + (float)J * dm[3];
+    float ynew = (float)I * dm[1] + (float)J * dm[4];
+    float znew = (float)I * dm[2] + (float)J * dm[5];
+    bool flipped = false;
+    if (xnew < 0.0f) { xnew = -xnew; ynew = -ynew; znew = -znew; flipped = true; }
+    int ixn = ifix((xnew + 0.5f) + (float)N) - N;
+    int iyn = ifix((ynew + 0.5f) + (float)N) - N;
+    int izn = ifix((znew + 0.5f) + (float)N) - N;
+    if (!(ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+          izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1)))
+      continue;
+    if (!(izn + LN2 >= zlo && izn - LN2 < zhi) && !(ixn < LN2 && -izn + LN2 >= zlo && -izn - LN2 < zhi))
+      continue;
+    if (ixn >= 0) {
+      int lb = -std::min(ixn, LN2);
+      for (int lz = -LN2; lz <= LN2; ++lz) {
+        int izp = izn + lz, iza = (izp >= 0) ? izp : N + izp;
+        if (izp < zlo || izp >= zhi) continue;
+        float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
+        if (tz == 0.0f) continue;
+        for (int ly = -LN2; ly <= LN2; ++ly) {
+          int iyp = iyn + ly, iya = (iyp >= 0) ? iyp : N + iyp;
+          float ty = kb.tab[nint_pos(std::fabs(ynew - (float)iyp) * fltb)] * tz;
+          if (ty == 0.0f) continue;
+          for (int ixp = lb + ixn; ixp <= LN2 + ixn; ++ixp) {
+            float wg = kb.tab[nint_pos(std::fabs(xnew - (float)ixp) * fltb)] * ty;
+            if (wg != 0.0f) visit(I, flipped, idx(ixp, iya, iza), wg, false);
+          }
+        }
+      }
+    }
+    if (ixn < LN2) {
+      for (int lz = -LN2; lz <= LN2; ++lz) {
+        int izp = izn + lz, izt = (izp > 0) ? N - izp : -izp;
+        if (-izp < zlo || -izp >= zhi) continue;
+        float tz = kb.tab[nint_pos(std::fabs(znew - (float)izp) * fltb)];
+        if (tz == 0.0f) continue;
+        for (int ly = -LN2; ly <= LN2; ++ly) {
+          int iyp = iyn + ly, iyt = (iyp > 0) ? N - iyp : -iyp;
+          float ty = kb.tab[nint_pos(std::fabs(ynew - (float)iyp) * fltb)] * tz;
+          if (ty == 0.0f) continue;
+          for (int ixp = ixn - LN2; ixp <= -1; ++ixp) {
+            float wg = kb.tab[nint_pos(std::fabs(xnew - (float)ixp) * fltb)] * ty;
+            if (wg != 0.0f) visit(I, flipped, idx(-ixp, iyt, izt), wg, true);
+          }
+        }
+      }
+    }
+  }
+}
+
+// T [nang][N][nx+1] -> X [N][N][nx+1], FP64, images in order, rows J = -NX+1..NX;
+// threads own contiguous ranges of signed z (every voxel's sum in that order)
+void fslice_insert(const cd* T, int nx, int nang, const float* dm9, const KBTable& kb, cd* X, int nthreads) {
+  const int N = 2 * nx;
+  const int nt = std::max(1, std::min(nthreads, 2 * nx - 1));
+  #pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num(), T_ = omp_get_num_threads();
+    const int zlo = -nx + 1 + (int)((long)(2 * nx - 1) * t / T_);
+    const int zhi = -nx + 1 + (int)((long)(2 * nx - 1) * (t + 1) / T_);
+    for (int a = 0; a < nang; ++a)
+      for (int J = -nx + 1; J <= nx; ++J) {
+        const int JP = (J >= 0) ? J : N + J;
+        const cd* row = T + ((size_t)a * N + JP) * (nx + 1);
+        oneline_taps(
+            J, nx, dm9 + 9 * a, kb,
+            [&](int I, bool flipped, size_t q, float wg, bool refl) {
+              const cd bi = std::conj(row[I]);
+              const cd btq = flipped ? std::conj(bi) : bi;
+              X[q] += (double)wg * (refl ? std::conj(btq) : btq);
+            },
+            zlo, zhi);
+      }
+  }
+}
+
+void fslice_extract(const cd* X, int nx, int nang, const float* dm9, const KBTable& kb, cd* T, int nthreads) {
+  const int N = 2 * nx;
+  #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int a = 0; a < nang; ++a) {
+    std::vector<cd> acc(nx + 1);
+    std::vector<char> flip(nx + 1);
+    for (int J = -nx + 1; J <= nx; ++J) {
+      const int JP = (J >= 0) ? J : N + J;
+      std::fill(acc.begin(), acc.end(), cd(0, 0));
+      std::fill(flip.begin(), flip.end(), 0);
+      oneline_taps(J, nx, dm9 + 9 * a, kb, [&](int I, bool flipped, size_t q, float wg, bool refl) {
+        acc[I] += (double)wg * (refl ? std::conj(X[q]) : X[q]);
+        flip[I] = flipped;
+      });
+      cd* row = T + ((size_t)a * N + JP) * (nx + 1);
+      for (int I = 0; I <= nx; ++I) {
+        const cd bi_adj = flip[I] ? std::conj(acc[I]) : acc[I];
+        row[I] = std::conj(bi_adj);
+      }
+    }
+  }
+}
+
 extern "C" {
+
+// FourierSlice pair in FP64: angles (psi, theta, phi) per slice; complex
+// arrays interleaved (re, im).
+void orc_fslice_insert(const double* T, int nx, const float* angles, int nang, double* X_out, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  KBTable kb;
+  fill_kb(2 * nx, kb);
+  std::vector<float> dm((size_t)9 * nang);
+  for (int a = 0; a < nang; ++a) cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], &dm[9 * a]);
+  const size_t nv = (size_t)(nx + 1) * 4 * nx * nx;
+  std::fill(X_out, X_out + 2 * nv, 0.0);
+  fslice_insert(reinterpret_cast<const cd*>(T), nx, nang, dm.data(), kb, reinterpret_cast<cd*>(X_out), nthreads);
+}
+
+void orc_fslice_extract(const double* X, int nx, const float* angles, int nang, double* T_out, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  KBTable kb;
+  fill_kb(2 * nx, kb);
+  std::vector<float> dm((size_t)9 * nang);
+  for (int a = 0; a < nang; ++a) cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], &dm[9 * a]);
+  fslice_extract(reinterpret_cast<const cd*>(X), nx, nang, dm.data(), kb, reinterpret_cast<cd*>(T_out), nthreads);
+}
 
 void orc_fillbessil(int n2, float* tab, float* fltb, float* alpha, float* aaaa) {
   KBTable t;

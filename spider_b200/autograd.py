@@ -98,23 +98,136 @@ class PJ3QPlan:
             pass
 
 
-class NormalCG:
-    """Conjugate gradients on (A^T A + lam I) x = rhs with A = PJ 3Q, in
-    fixed device buffers; with ``graph`` one iteration is captured once as a
-    CUDA graph and replayed.  Dot products and step lengths are FP64."""
+# ---------------------------------------------------------------------------
+# FourierSlice: the central-slice pair on ONELINE's geometry.
+class FourierSlicePlan:
+    """The FourierSlice operator pair (``spi_fslice_*``) for one box size and
+    angle list: ``forward`` extracts central slices from a Fourier grid (the
+    exact adjoint of ONELINE's insertion, oneline.f:38-200, without the weight
+    grid), ``adjoint`` inserts slices into a grid (that insertion), ``normal``
+    applies E^T E + lam I in one fused pass.  Grids are float32 tensors
+    [2nx, 2nx, nx+1, 2] (complex as (re, im) pairs), slices [nang, 2nx, nx+1, 2]
+    in the layout and sign of the staged image spectra (``stage``).  forward,
+    adjoint and normal run on torch's current stream, allocate nothing in the
+    library and do not synchronise, so they can be captured in a CUDA graph."""
 
-    def __init__(self, plan: PJ3QPlan, lam: float, iters: int, graph: bool = True):
+    def __init__(self, nx: int, angles, ctx: ops.Context | None = None, device: int = 0):
+        import ctypes
+        self.nx = int(nx)
+        self.n = 2 * self.nx
+        self.angles = np.ascontiguousarray(angles, dtype=np.float32)
+        self.nang = int(self.angles.shape[0])
+        self.ctx = ctx or ops.default_context(device)
+        self.device = torch.device("cuda", self.ctx.device)
+        self._L = self.ctx._L
+        self.shape = (self.n, self.n, self.nx + 1, 2)
+        self.range_shape = (self.nang, self.n, self.nx + 1, 2)
+        h = ctypes.c_void_p()
+        ops.check(self._L.spi_fslice_plan_create(self.ctx.handle, self.nx,
+                                                 self.angles.ctypes.data_as(ctypes.c_void_p), self.nang,
+                                                 ctypes.byref(h)))
+        self._h = h
+
+    def _stream(self):
+        import ctypes
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    @staticmethod
+    def _p(t):
+        import ctypes
+        if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+            raise ops.SpiderError(101, "FourierSlice needs contiguous float32 CUDA tensors")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def stage(self, imgs: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Slices of CUDA images [nang, nx, nx]: PADD2, phase, 2D transform."""
+        if out is None:
+            out = torch.empty(self.range_shape, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_fslice_stage(self._h, self._p(imgs), self._p(out), self._stream()))
+        return out
+
+    def forward(self, grid: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.range_shape, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_fslice_forward(self._h, self._p(grid), self._p(out), self._stream()))
+        return out
+
+    def adjoint(self, slices: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_fslice_adjoint(self._h, self._p(slices), self._p(out), self._stream()))
+        return out
+
+    def normal(self, grid: torch.Tensor, lam: float, out: torch.Tensor | None = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_fslice_normal(self._h, self._p(grid), float(lam), self._p(out), self._stream()))
+        return out
+
+    def volume(self, grid: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Real-space volume [nx, nx, nx] of a grid of spectrum coefficients."""
+        if out is None:
+            out = torch.empty((self.nx,) * 3, dtype=torch.float32, device=self.device)
+        ops.check(self._L.spi_fslice_volume(self._h, self._p(grid), self._p(out), self._stream()))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h:
+            self._L.spi_fslice_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FourierSlice(torch.autograd.Function):
+    """Differentiable central-slice extraction: forward E (grid -> slices),
+    backward the insertion E^T (ONELINE without weights), recomputing every
+    tap's voxel and weight from the plan's angles instead of storing them."""
+
+    @staticmethod
+    def forward(fctx, grid: torch.Tensor, plan: FourierSlicePlan):
+        fctx.plan = plan
+        return plan.forward(grid.detach().contiguous().float())
+
+    @staticmethod
+    def backward(fctx, grad: torch.Tensor):
+        return fctx.plan.adjoint(grad.detach().contiguous().float()), None
+
+
+def fourier_slice(grid: torch.Tensor, plan: FourierSlicePlan) -> torch.Tensor:
+    """Differentiable FourierSlice of a CUDA grid [2nx, 2nx, nx+1, 2]."""
+    if not grid.is_cuda:
+        raise ops.SpiderError(101, "fourier_slice needs a CUDA grid (there is no CPU path)")
+    return FourierSlice.apply(grid, plan)
+
+
+class NormalCG:
+    """Conjugate gradients on (A^T A + lam I) x = rhs, in fixed device
+    buffers; A is the plan's operator (PJ 3Q with PJ3QPlan, the FourierSlice
+    extraction with FourierSlicePlan, whose E^T E + lam I is one fused pass).
+    With ``graph`` one iteration is captured once as a CUDA graph and
+    replayed.  Dot products and step lengths are FP64."""
+
+    def __init__(self, plan, lam: float, iters: int, graph: bool = True):
         self.plan, self.lam, self.iters, self.graph = plan, float(lam), int(iters), graph
         z = lambda shape: torch.zeros(shape, dtype=torch.float32, device=plan.device)  # noqa: E731
         self.x, self.r, self.p, self.ap = (z(plan.shape) for _ in range(4))
-        self.q = z((plan.nang,) + plan.shape[1:])
+        self.fused = hasattr(plan, "normal")
+        self.q = None if self.fused else z((plan.nang,) + tuple(plan.shape[1:]))
         self.rs = torch.zeros((), dtype=torch.float64, device=plan.device)
         self._g = None
 
     def _iteration(self):
-        self.plan.forward(self.p, out=self.q)
-        self.plan.adjoint(self.q, out=self.ap)
-        self.ap.add_(self.p, alpha=self.lam)
+        if self.fused:
+            self.plan.normal(self.p, self.lam, out=self.ap)
+        else:
+            self.plan.forward(self.p, out=self.q)
+            self.plan.adjoint(self.q, out=self.ap)
+            self.ap.add_(self.p, alpha=self.lam)
         pap = (self.p.double() * self.ap.double()).sum()
         alpha = torch.where(pap > 0, self.rs / pap, torch.zeros_like(pap)).float()
         self.x.add_(alpha * self.p)

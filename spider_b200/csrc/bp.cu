@@ -998,6 +998,51 @@ __global__ void grid_add_kernel(float4* __restrict__ G, const float2* __restrict
   }
 }
 
+// ----------------------------------------------------------------------------
+// Compensated accumulation.  The insertion adds the taps of a run of images
+// into a partial grid P (plain FP32 vector atomics); every `fold_every`
+// images P is folded into the running grid H with an error-free two-sum
+// (Knuth: s = h + p, e = (h - (s - b)) + (p - b) with b = s - h), whose
+// rounding errors e accumulate in a compensation grid C, and P is cleared.
+// H + C then carries the sum to about twice single precision, so the error
+// of the total grows with the images per fold instead of with all images.
+// COLLAPSE (before SYMPLANE0 / NRMW2 or a partial read-out) ends the
+// accumulation: H = fl(H + C), one rounding, and C is cleared.
+__device__ __forceinline__ void two_sum(float& h, float p, float& c) {
+  const float s = __fadd_rn(h, p);
+  const float b = __fsub_rn(s, h);
+  const float e = __fadd_rn(__fsub_rn(h, __fsub_rn(s, b)), __fsub_rn(p, b));
+  h = s;
+  c = __fadd_rn(c, e);
+}
+
+template <bool COLLAPSE>
+__global__ void fold_kernel(float4* __restrict__ P, float4* __restrict__ H, float4* __restrict__ C, size_t nvox) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
+    const float4 d = P[q];
+    const bool any = d.x != 0.0f || d.y != 0.0f || d.z != 0.0f;
+    if (!COLLAPSE && !any) continue;
+    float4 c = C[q];
+    const bool has_c = c.x != 0.0f || c.y != 0.0f || c.z != 0.0f;
+    if (!any && !has_c) continue;
+    float4 h = H[q];
+    if (any) {
+      two_sum(h.x, d.x, c.x);
+      two_sum(h.y, d.y, c.y);
+      two_sum(h.z, d.z, c.z);
+      P[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    if (COLLAPSE) {
+      h.x = __fadd_rn(h.x, c.x);
+      h.y = __fadd_rn(h.y, c.y);
+      h.z = __fadd_rn(h.z, c.z);
+      c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    H[q] = h;
+    C[q] = c;
+  }
+}
+
 // ============================================================================
 // host side
 
@@ -1046,6 +1091,10 @@ void HostBuf::release() {
 
 void bp_release(spi_ctx* c) {
   for (auto& g : c->grid) g.release();
+  for (auto& g : c->part) g.release();
+  for (auto& g : c->comp) g.release();
+  c->unfolded = 0;
+  c->comp_dirty = false;
   c->gptr[0] = c->gptr[1] = nullptr;
   c->wkb_nx = 0;
   c->imgs.release();
@@ -1083,10 +1132,56 @@ static int grid_blocks(const spi_ctx* c, size_t work, int threads) {
 
 static size_t grid_voxels(const spi_ctx* c) { return (size_t)(c->nx + 1) * c->n * c->n; }
 
+// The grid the insertion adds into: the partial grid with compensated
+// accumulation, else the grid itself.
+static float4* insert_target(spi_ctx* c, int g) { return c->accum ? c->part[g].as<float4>() : c->gptr[g]; }
+
+// Fold the partial grids into the grids (two-sum, compensation kept), or with
+// `collapse` also add the compensation into the grids and clear it; a no-op
+// without compensated accumulation or pending sums.
+static int fold_grids(spi_ctx* c, bool collapse) {
+  if (!c->accum || c->ngrids == 0) return 0;
+  if (c->unfolded == 0 && !(collapse && c->comp_dirty)) return 0;
+  const size_t nvox = grid_voxels(c);
+  int ev = c->phase_begin(8);
+  for (int g = 0; g < c->ngrids; ++g) {
+    float4 *P = c->part[g].as<float4>(), *H = c->gptr[g], *C = c->comp[g].as<float4>();
+    if (collapse)
+      fold_kernel<true><<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(P, H, C, nvox);
+    else
+      fold_kernel<false><<<grid_blocks(c, nvox, 256), 256, 0, c->stream>>>(P, H, C, nvox);
+    SPI_TRY(check_kernel("fold_kernel"));
+    c->count();
+  }
+  c->phase_end(ev);
+  c->unfolded = 0;
+  c->comp_dirty = !collapse;
+  return 0;
+}
+
 static int env_int(const char* name, int dflt) {
   const char* s = getenv(name);
   if (!s || !*s) return dflt;
   return atoi(s);
+}
+
+// PADD2 + ASTA_D + phase shift (stage_kernel) of nimg device images of box
+// nx into padded[b][2nx][2nx] on stream s: the input of the batched R2C.
+int stage_images(const spi_ctx* c, cudaStream_t s, const float* imgs, int nx, int nimg, float* padded) {
+  if (nimg <= 0) return 0;
+  const int n = 2 * nx;
+  int klp_count = 0;
+  const float rr = (float)(nx / 2) * (float)(nx / 2);
+  const int nc = nx / 2 + 1;
+  for (int j = 1; j <= nx; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      const float t = (float)(j - nc), t2 = (float)(i - nc);
+      if (t * t + t2 * t2 > rr) ++klp_count;
+    }
+  const int ip = (n - nx) / 2 + nx % 2;
+  const int parts = std::max(1, std::min(8, (4 * c->sm_count + nimg - 1) / nimg));
+  stage_kernel<<<dim3(nimg, parts), 256, 0, s>>>(imgs, nx, n, ip, nimg, (double)(float)klp_count, padded);
+  return check_kernel("stage_kernel");
 }
 
 }  // namespace spi
@@ -1130,7 +1225,7 @@ void spi_ctx::phase_collect() {
 
 long long spi_ctx::device_bytes() const {
   long long t = 0;
-  const DevBuf* bufs[] = {&grid[0], &grid[1], &kbtab, &imgs, &padded, &spectra, &spec_tmp, &slices, &cplx, &real3,
+  const DevBuf* bufs[] = {&grid[0], &grid[1], &part[0], &part[1], &comp[0], &comp[1], &kbtab, &imgs, &padded, &spectra, &spec_tmp, &slices, &cplx, &real3,
                           &workctr,
                           &wkb, &acc, &volbuf, &pj_vol, &pj_out, &pj_runs, &pj_dm, &pj_rows, &pj_v4, &pj_fbs};
   for (auto b : bufs) t += (long long)b->bytes;
@@ -1188,6 +1283,7 @@ int spi_ctx_create(int device, spi_ctx** out) {
     return st;
   }
   c->pipeline = env_int("SPI_PIPELINE", 1) ? 1 : 0;
+  c->accum = env_int("SPI_BP_ACCUM", 1) ? 1 : 0;
   *out = c;
   return 0;
 }
@@ -1230,7 +1326,7 @@ int spi_ctx_timing(spi_ctx* c, double* ms_out, long long* count_out) {
   if (!c) return fail(kInvalid, "NULL context");
   SPI_CUDA(cudaSetDevice(c->device));
   c->phase_collect();
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < SPI_NPHASE; ++i) {
     if (ms_out) ms_out[i] = c->phase_ms[i];
     if (count_out) count_out[i] = c->phase_n[i];
     c->phase_ms[i] = 0.0;
@@ -1274,7 +1370,16 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
       c->gptr[g] = c->grid[g].as<float4>();
     }
     SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
+    if (c->accum) {
+      SPI_TRY(c->part[g].ensure(gbytes));
+      SPI_TRY(c->comp[g].ensure(gbytes));
+      SPI_CUDA(cudaMemsetAsync(c->part[g].p, 0, gbytes, c->stream));
+      SPI_CUDA(cudaMemsetAsync(c->comp[g].p, 0, gbytes, c->stream));
+    }
   }
+  c->unfolded = 0;
+  c->comp_dirty = false;
+  if (c->fold_every <= 0) c->fold_every = env_int("SPI_BP_FOLD", 4096);
   // chunk sizes: spectra of one chunk <= ~4.3 GB FP32
   const size_t spec_per_img = (size_t)c->n * (nx + 1) * sizeof(float2);
   int chunk = (int)std::min<size_t>(8192, std::max<size_t>(64, (size_t)4400000000ull / spec_per_img));
@@ -1334,6 +1439,23 @@ int spi_bp_set_spectrum_precision(spi_ctx* c, int bf16) {
   return 0;
 }
 
+int spi_bp_set_accumulation(spi_ctx* c, int compensated, int fold_every) {
+  if (!c) return fail(kInvalid, "NULL context");
+  if (c->ngrids) return fail(kInvalid, "spi_bp_set_accumulation: call before spi_bp_open");
+  if (fold_every < 0) return fail(kInvalid, "spi_bp_set_accumulation: fold_every = %d", fold_every);
+  c->accum = compensated ? 1 : 0;
+  c->fold_every = fold_every;
+  return 0;
+}
+
+int spi_bp_flush(spi_ctx* c) {
+  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_flush: no open reconstruction");
+  SPI_CUDA(cudaSetDevice(c->device));
+  SPI_TRY(fold_grids(c, true));
+  SPI_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 static int ensure_chunk_buffers(spi_ctx* c) {
   const int nx = c->nx, n = c->n;
   SPI_TRY(c->imgs.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
@@ -1389,7 +1511,7 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
   const int nx = c->nx;
   const float* tab = c->kbtab.as<float>();
   const float fltb = c->kb.fltb;
-  float4* g0 = c->gptr[0];
+  float4* g0 = insert_target(c, 0);
   int ev_ins = c->phase_begin(2);
   if (c->insert_mode >= 1 && c->insert_mode <= 3) {
     const size_t smem = 5000 * sizeof(float);
@@ -1594,7 +1716,7 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   }
   SPI_CUFFT(cufftSetStream(c->plan2d, c->stream));
   std::vector<char> done_valid(nsubs, 0);
-  float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
+  float4* g1 = insert_target(c, c->ngrids == 2 ? 1 : 0);
   for (int a0 = 0; a0 < nimg; a0 += c->chunk) {
     const int nb = std::min(c->chunk, nimg - a0);
     if (inplane)
@@ -1669,6 +1791,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
         c->count();
       }
       SPI_TRY(launch_insert(c, c->slices.as<SliceDesc>() + (size_t)b0 * nsym, nvalid * nsym, g1));
+      c->unfolded += nvalid;
+      if (c->unfolded >= c->fold_every) SPI_TRY(fold_grids(c, false));
     }
   }
   if (copy_pipe) {   // join
@@ -1740,7 +1864,7 @@ static int bp_autotune_impl(spi_ctx* c, int force) {
   SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs, nsl * sizeof(SliceDesc), cudaMemcpyHostToDevice, c->stream));
   const size_t plane = (size_t)c->n * (nx + 1);
   SPI_CUDA(cudaMemsetAsync(c->spectra.p, 0, (size_t)sample * plane * (c->bf16 ? 4 : 8), c->stream));
-  float4* g1 = c->ngrids == 2 ? c->gptr[1] : c->gptr[0];
+  float4* g1 = insert_target(c, c->ngrids == 2 ? 1 : 0);
   const int modes[2] = {kb_window4_ok(c->kb) ? 3 : 2, 2};
   const int shapes[5][2] = {{256, 2}, {256, 3}, {512, 2}, {128, 4}, {512, 1}};
   cudaEvent_t e0, e1;
@@ -1779,7 +1903,10 @@ static int bp_autotune_impl(spi_ctx* c, int force) {
   c->tuned_ms = best.ms;
   if (st) return st;
   const size_t gbytes = grid_voxels(c) * sizeof(float4);
-  for (int g = 0; g < c->ngrids; ++g) SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
+  for (int g = 0; g < c->ngrids; ++g) {
+    SPI_CUDA(cudaMemsetAsync(c->gptr[g], 0, gbytes, c->stream));
+    if (c->accum) SPI_CUDA(cudaMemsetAsync(c->part[g].p, 0, gbytes, c->stream));
+  }
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best;
@@ -1800,6 +1927,7 @@ int spi_bp_get_launch(const spi_ctx* c, int* kernel, int* threads, int* blocks_p
 }
 
 static int apply_sym0(spi_ctx* c, int g) {
+  SPI_TRY(fold_grids(c, true));   // the grids hold the complete sums from here on
   if (!c->pending_sym0[g]) return 0;
   const int m = c->nx - 1;
   const int work = m * m + 2 * m;

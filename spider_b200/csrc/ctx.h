@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.h"
+#include "../../include/spider_b200.h"
 
 struct spi_ctx {
   int device = 0;
@@ -38,6 +39,12 @@ struct spi_ctx {
   int sort_group = 0;                 // images per slice-ordering group (divides into sub)
   spi::KBTab kb;
   spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
+  int accum = 1;                      // 1 = compensated: insert into part[], two-sum fold into grid + comp
+  int fold_every = 0;                 // images between folds (compensated accumulation)
+  long long unfolded = 0;             // images inserted into part[] since the last fold
+  bool comp_dirty = false;            // comp[] may hold nonzero compensation terms
+  spi::DevBuf part[2];                // float4 partial sums of the images since the last fold
+  spi::DevBuf comp[2];                // float4 low-order compensation of grid[] (two-sum error terms)
   float4* gptr[2] = {nullptr, nullptr};      // grids in use (owned or attached)
   float4* ext_grid[2] = {nullptr, nullptr};  // caller-owned grids (spi_bp_attach_grids)
   int wkb_nx = 0;                     // nx the cached |WKB| table belongs to
@@ -79,8 +86,8 @@ struct spi_ctx {
   struct PhaseEv { cudaEvent_t a, b; int phase; cudaStream_t s; };
   std::vector<PhaseEv> ev_pending;
   std::vector<cudaEvent_t> ev_pool;
-  double phase_ms[8] = {0};
-  long long phase_n[8] = {0};
+  double phase_ms[SPI_NPHASE] = {0};
+  long long phase_n[SPI_NPHASE] = {0};
   int phase_begin(int phase, cudaStream_t s = nullptr);   // returns slot or -1; s = nullptr: stream
   void phase_end(int slot);
   void phase_collect();         // synchronises on recorded events
@@ -119,4 +126,7 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
 // SIN(THETA), MODULO(SHX, NX), MODULO(SHY, NX)}; runs on the context stream.
 int rtsf_images(spi_ctx* c, const float* src, float* dst, int nx, int nimg, const float4* prm);
 int check_kernel(const char* what);
+// PADD2 + ASTA_D + phase shift of nimg device images (box nx) into padded
+// [nimg][2nx][2nx] float on stream s (the staging of the back-projection)
+int stage_images(const spi_ctx* c, cudaStream_t s, const float* imgs, int nx, int nimg, float* padded);
 }  // namespace spi

@@ -57,7 +57,7 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
         start, count = shard(int(imgs.shape[0]), rank, world)
         if count:
             ctx.bp_insert(imgs[start:start + count], angles[start:start + count], half[start:start + count])
-        torch.cuda.synchronize(dev)     # insertions ran on the library's own stream
+        ctx.bp_flush()                  # grids hold the complete sums; the library stream is idle
         allreduce_grids(grids)
         # NCCL orders the reduce on torch's current stream only; the library
         # stream (non-blocking) would not wait for it before SYMPLANE0/NRMW2

@@ -174,6 +174,17 @@ class Context:
     def bp_close(self):
         check(self._L.spi_bp_close(self._h))
 
+    def set_accumulation(self, compensated: bool = True, fold_every: int = 0):
+        """Grid accumulation of the next bp_open: compensated (two-sum folds
+        of a partial grid every ``fold_every`` images, 0 = default) or plain
+        FP32 atomics into the grid."""
+        check(self._L.spi_bp_set_accumulation(self._h, 1 if compensated else 0, int(fold_every)))
+
+    def bp_flush(self):
+        """Fold pending sums and the compensation into the grids (before an
+        exchange of caller-owned grids); synchronises the library stream."""
+        check(self._L.spi_bp_flush(self._h))
+
 
 _tls = threading.local()
 

@@ -93,11 +93,53 @@ def fsc(v1: np.ndarray, v2: np.ndarray) -> np.ndarray:
     n = v1.shape[0]
     g = np.arange(n) - n // 2
     r = np.sqrt(g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2)
-    ri = np.rint(r).astype(int)
-    out = np.zeros(n // 2 + 1)
-    for s in range(n // 2 + 1):
-        m = ri == s
-        num = np.sum(f1[m] * np.conj(f2[m])).real
-        den = np.sqrt(np.sum(np.abs(f1[m]) ** 2) * np.sum(np.abs(f2[m]) ** 2))
-        out[s] = num / den if den > 0 else 1.0
+    ri = np.rint(r).astype(np.int64).ravel()
+    m = ri <= n // 2
+    ri = ri[m]
+    a, b = f1.ravel()[m], f2.ravel()[m]
+    nb = n // 2 + 1
+    num = np.bincount(ri, weights=(a * np.conj(b)).real, minlength=nb)
+    d1 = np.bincount(ri, weights=np.abs(a) ** 2, minlength=nb)
+    d2 = np.bincount(ri, weights=np.abs(b) ** 2, minlength=nb)
+    den = np.sqrt(d1 * d2)
+    out = np.ones(nb)
+    ok = den > 0
+    out[ok] = num[ok] / den[ok]
+    return out
+
+
+def projection_stack(ctx, vol: np.ndarray, angles: np.ndarray, snr: float | None = None, shifts=None,
+                     seed: int = 0, chunk: int = 4096):
+    """Noisy, shifted PJ 3Q projections as a CUDA tensor [n, ny, nx] float32.
+
+    The clean projections come from this library's PJ 3Q (``ops.pj3q``) in
+    chunks; ``shifts`` [n, 2] = (sx, sy) pixels moves each image circularly by
+    a Fourier phase (+x by +sx, the direction RTSQ shifts); ``snr`` adds white
+    Gaussian noise of variance var(image)/snr from a seeded torch generator.
+    Test and benchmark data only: the inputs of every path come from here and
+    go to the GPU path and the oracle alike.
+    """
+    import torch
+
+    from . import ops
+    dev = torch.device("cuda", ctx.device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    n = int(angles.shape[0])
+    ny, nx = int(vol.shape[1]), int(vol.shape[2])
+    out = torch.empty((n, ny, nx), dtype=torch.float32, device=dev)
+    dvol = torch.from_numpy(np.ascontiguousarray(vol, np.float32)).to(dev)
+    for a0 in range(0, n, chunk):
+        a1 = min(n, a0 + chunk)
+        pr = ops.pj3q(dvol, angles[a0:a1], ctx=ctx)
+        if shifts is not None:
+            ky = torch.fft.fftfreq(ny, device=dev, dtype=torch.float64)[:, None]
+            kx = torch.fft.fftfreq(nx, device=dev, dtype=torch.float64)[None, :]
+            sh = torch.as_tensor(np.asarray(shifts[a0:a1], np.float64), device=dev)
+            ph = torch.exp(-2j * np.pi * (kx[None] * sh[:, 0, None, None] + ky[None] * sh[:, 1, None, None]))
+            pr = torch.fft.ifft2(torch.fft.fft2(pr.double()) * ph).real.float()
+        if snr:
+            sd = torch.sqrt(pr.var(dim=(1, 2), keepdim=True) / snr)
+            pr = pr + torch.randn(pr.shape, device=dev, generator=gen) * sd
+        out[a0:a1] = pr
     return out

@@ -121,9 +121,12 @@ def test_bp32f_bf16_spectra(ctx, orc):
     g_all, _, _ = ops.bp32f(pr, ang, half, ctx=ctx, bf16=True)
     r_all, _, _ = orc.bp32f(pr, ang, half, prec=1, nthreads=1)
     e = synth.rel_l2(g_all, r_all)
-    print(f"BF16 spectra: rel-L2 vs FP64 oracle {e:.3e}")
-    assert e <= 5e-3
-    assert synth.fsc(g_all, r_all)[nx // 2] >= 0.99
+    f = synth.fsc(g_all, r_all)[nx // 2]
+    print(f"BF16 spectra: rel-L2 vs FP64 oracle {e:.3e}, FSC at Nyquist {f:.7f}")
+    # BF16 keeps 8 bits of each spectrum value: the volume moves by ~1e-4 of
+    # its norm, while every Fourier shell still correlates to >= 0.999
+    assert e <= 5e-4
+    assert f >= 0.999
 
 
 def test_bp_errors(ctx):
