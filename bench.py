@@ -47,9 +47,23 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cg", action="store_true", help="skip the BP CG s/iter measurement")
-    p.add_argument("--workload", choices=["bp32f", "multiclass"], default="bp32f",
-                   help="multiclass: eight classes of box 96-256, 80,000 images (separate JSON line)")
+    p.add_argument("--workload", choices=["bp32f", "multiclass", "kernel"], default="bp32f",
+                   help="multiclass: eight classes of box 96-256, 80,000 images (separate JSON line); "
+                        "kernel: a small run of one kernel family for profilers (--kernel)")
+    p.add_argument("--kernel", choices=["insert", "pj3q", "bpcg", "normalcg", "fslice"], default="insert",
+                   help="--workload kernel: insert (BP 32F insertion of --nimg images at --nx, --reps launches), "
+                        "pj3q (--nang projections of an --nx^3 volume), bpcg (--iters BP CG iterations at "
+                        "--n^3 with --nang images, --prec, --interp), normalcg (PJ 3Q normal-equation CG), "
+                        "fslice (FourierSlice normal-equation CG)")
+    p.add_argument("--nimg", type=int, default=64)
+    p.add_argument("--nang", type=int, default=64)
+    p.add_argument("--n", type=int, default=64)
+    p.add_argument("--reps", type=int, default=3)
+    p.add_argument("--iters", type=int, default=2)
+    p.add_argument("--prec", choices=["fp64", "mixed", "mixed64", "fast", "fp32"], default="fp64")
+    p.add_argument("--interp", choices=["linear", "fbs"], default="linear")
     p.add_argument("--mc-images", type=int, default=80000)
+    p.add_argument("--no-mc", action="store_true", help="skip the multi-class measurement")
     p.add_argument("--cg-n", type=int, default=128)
     p.add_argument("--cg-nang", type=int, default=10000)
     p.add_argument("--cg-iters", type=int, default=6)
@@ -392,28 +406,31 @@ def fourier_cg_measure(ctx, projs, ang, K, lam=1e-3, check_images=1000, check_it
     imgs = torch.from_numpy(projs).cuda()
     plan = autograd.FourierSlicePlan(n, ang, ctx=ctx)
     b = plan.stage(imgs)
-    rhs = plan.adjoint(b)
+    rhs = plan.adjoint64(b)
+    rhs32 = plan.adjoint(b)
     del b
     out = {}
-    for name, graph in (("graph_s_per_iter", True), ("plain_s_per_iter", False)):
+    for name, graph, op64 in (("graph_s_per_iter", True, True), ("plain_s_per_iter", False, True),
+                              ("fp32_operator_graph_s_per_iter", True, False)):
         times = []
         for iters in (1, 1 + K):
-            solver = autograd.NormalCG(plan, lam, iters, graph=graph)
-            solver.solve(rhs)
+            solver = autograd.NormalCG(plan, lam, iters, graph=graph, fp64_operator=op64)
+            r = rhs if op64 else rhs32
+            solver.solve(r)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            solver.solve(rhs)
+            solver.solve(r)
             e1.record()
             e1.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
         out[name] = (times[1] - times[0]) / K
     plan.close()
-    del rhs
+    del rhs, rhs32
     # FP64 check on a subset
     sub = autograd.FourierSlicePlan(n, ang[:check_images], ctx=ctx)
     bs = sub.stage(imgs[:check_images].contiguous())
-    x = autograd.NormalCG(sub, lam, check_iters, graph=True).solve(sub.adjoint(bs)).cpu().numpy().astype(np.float64)
+    x = autograd.NormalCG(sub, lam, check_iters, graph=True).solve(sub.adjoint64(bs)).cpu().numpy().astype(np.float64)
     bh = bs.cpu().numpy().astype(np.float64)
     sub.close()
     bh = bh[..., 0] + 1j * bh[..., 1]
@@ -434,8 +451,9 @@ def fourier_cg_measure(ctx, projs, ang, K, lam=1e-3, check_images=1000, check_it
     xg = x[..., 0] + 1j * x[..., 1]
     out["rel_err_vs_fp64_oracle"] = float(np.linalg.norm(xg - xr) / np.linalg.norm(xr))
     out["check"] = f"{check_images} images, {check_iters} iterations, oracle FP64 CG {time.perf_counter() - t0:.1f} s"
-    out["operator"] = "FourierSlice (central-slice extraction) and ONELINE insertion without weights, FP32, " \
-                      "fused E^T E + lam I, FP64 dot products"
+    out["operator"] = "FourierSlice (central-slice extraction) and ONELINE insertion without weights, fused " \
+                      "E^T E + lam I with FP64 sums and scatter (FP32 table weights), FP64 CG vectors; " \
+                      "fp32_operator: the same pass with FP32 sums"
     return out
 
 
@@ -706,6 +724,10 @@ def run_ours(args):
     if not args.no_cg and world == 1:
         cg = cg_measure(args, ctx, stream, rank, world)
 
+    mc = None
+    if rank == 0 and world == 1 and not args.no_mc:
+        mc = multiclass_measure(args)
+
     check = None
     if rank == 0 and world == 1 and args.check_images > 0:
         check = fp64_check(ctx, nx, chunks, angles, halves, args.check_images, args.bf16)
@@ -738,6 +760,7 @@ def run_ours(args):
             "finish_ms": finish_ms,
             "finish_phase_ms": finish_phase_ms,
             "bpcg": cg,
+            "multiclass": mc,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -759,20 +782,19 @@ def _cang_host(a):
                     dtype=np.float32)
 
 
-def run_multiclass(args):
+def multiclass_measure(args, steps=2):
     """Uneven multi-class insertion: K = 8 classes with boxes
     {96,128,160,192,192,224,256,256}, each a 30-80-blob phantom; images
     assigned uniformly at random to the classes, SNR 0.1, uniform SO(3);
-    every class is a BP 32F in its own context (grids, plans, autotuned
-    launch), inserted concurrently from one host thread per class, then
-    finished.  Timed by the host clock between device synchronisations
-    (several streams), images already resident on the device."""
+    every class is a BP 32F with its own grids, all classes inserted through
+    spi_bp_insert_multi (one insertion launch per round over every class's
+    slices, one stream), then finished; open + insertion + finish of all
+    classes are timed, images resident on the device; the rate with one context and host thread per class (concurrent
+    streams) is given beside it.  Several streams run at once in the second
+    form, so both are timed by the host clock between synchronisations."""
     import torch
     from spider_b200 import ops, synth
-    rank, world, local = dist_env()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local)
+    _, _, local = dist_env()
     dev = torch.device(f"cuda:{local}")
     boxes = [96, 128, 160, 192, 192, 224, 256, 256]
     rng = np.random.default_rng(1004)
@@ -791,25 +813,90 @@ def run_multiclass(args):
     ctx.close()
     torch.cuda.synchronize()
 
-    def one_pass():
+    ctxs = [ops.Context(local) for _ in classes]      # kept across passes: buffers and plans are reused
+
+    def one_pass(one_launch):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        out = ops.bp32f_multiclass(classes, device=local, device_out=True, autotune=True)
+        ops.bp32f_multiclass(classes, device=local, device_out=True, autotune=not one_launch,
+                             one_launch=one_launch, ctxs=ctxs)
         torch.cuda.synchronize()
-        return time.perf_counter() - t, out
+        return time.perf_counter() - t
 
-    one_pass()                                  # warm-up (plans, autotuner cache)
-    dts = [one_pass()[0] for _ in range(max(args.steps, 1))]
-    dt = min(dts)
-    line = {"metric": "images backprojected/s, 8 classes of box 96-256 (BP 32F each)",
-            "value": args.mc_images / dt, "unit": "images/s", "n_gpus": 1, "steps": len(dts), "warmup": 1,
-            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
+    res = {}
+    for name, one in (("one_launch", True), ("threads", False)):
+        one_pass(one)                                  # warm-up (plans, buffers)
+        res[name] = min(one_pass(one) for _ in range(max(steps, 1)))
+    for c in ctxs:
+        c.close()
+    return {"metric": "images backprojected/s, 8 classes of box 96-256 (BP 32F each)",
+            "value": args.mc_images / res["one_launch"], "unit": "images/s",
+            "threads_value": args.mc_images / res["threads"],
             "config": {"workload": "multi-class BP 32F, boxes 96,128,160,192,192,224,256,256",
                        "images": args.mc_images, "per_class": [int(c[0].shape[0]) for c in classes],
-                       "timing": "host clock between device synchronisations, min over steps; "
-                                 "includes open, insertion and finish of all eight classes"}}
+                       "timing": "host clock around synchronised calls (open, insertion and finish of all eight "
+                                 "classes; the contexts, their buffers and FFT plans are kept across passes), "
+                                 "min over passes",
+                       "forms": "value: spi_bp_insert_multi (one insertion launch per round, one stream); "
+                                "threads_value: one context and host thread per class"}}
+
+
+def run_multiclass(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    m = multiclass_measure(args, args.steps)
+    line = {"metric": m["metric"], "value": m["value"], "unit": "images/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": m["config"], "threads_value": m["threads_value"]}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_kernel_workload(a):
+    """Small, self-contained runs of one kernel family on random data, for
+    profilers (ncu): each launches its kernels a few times, so that a
+    capture can skip the first launch (-s 1) and take a steady-state one.
+    Prints one line, no JSON: these are not benchmark numbers."""
+    import torch
+    from spider_b200 import ops, synth
+    ctx = ops.Context(0)
+    rng = np.random.default_rng(0)
+    if a.kernel == "insert":
+        imgs = torch.randn(a.nimg, a.nx, a.nx, device="cuda")
+        ctx.bp_open(a.nx, 2, bf16=a.bf16)
+        for _ in range(a.reps):
+            ctx.bp_insert(imgs, synth.so3_angles(a.nimg, rng), synth.half_mask(a.nimg, rng))
+        ctx.bp_close()
+    elif a.kernel == "pj3q":
+        vol = torch.randn(a.nx, a.nx, a.nx, device="cuda")
+        for _ in range(a.reps):
+            ops.pj3q(vol, synth.so3_angles(a.nang, rng), ctx=ctx)
+    elif a.kernel == "normalcg":
+        from spider_b200 import autograd
+        plan = autograd.PJ3QPlan((a.nx, a.nx, a.nx), synth.so3_angles(a.nang, rng), ctx=ctx)
+        b = torch.randn(a.nang, a.nx, a.nx, device="cuda")
+        for _ in range(a.reps):
+            autograd.NormalCG(plan, 1e-3, a.iters, graph=False).solve(plan.adjoint(b))
+        plan.close()
+    elif a.kernel == "fslice":
+        from spider_b200 import autograd
+        plan = autograd.FourierSlicePlan(a.nx, synth.so3_angles(a.nang, rng), ctx=ctx)
+        b = plan.stage(torch.randn(a.nang, a.nx, a.nx, device="cuda"))
+        for _ in range(a.reps):   # --prec fp32: the FP32 normal operator, else the FP64 one
+            autograd.NormalCG(plan, 1e-3, a.iters, graph=False,
+                              fp64_operator=a.prec != "fp32").solve(plan.adjoint(b))
+        plan.close()
+    else:
+        projs = rng.standard_normal((a.nang, a.n, a.n)).astype(np.float32)
+        prec = {"fp64": True, "fp32": False}.get(a.prec, a.prec)
+        ops.bpcg(projs, synth.so3_angles(a.nang, rng), a.n / 2 - 3, errm=0.0, maxit=a.iters, mode=1,
+                 lam=1e-3, ctx=ctx, fp64=prec, interp=a.interp)
+    torch.cuda.synchronize()
+    print(f"ok {a.kernel}: {ctx.launches} kernel launches")
+    ctx.close()
     return 0
 
 
@@ -819,6 +906,8 @@ def main():
         return run_reference(args)
     if args.workload == "multiclass":
         return run_multiclass(args)
+    if args.workload == "kernel":
+        return run_kernel_workload(args)
     return run_ours(args)
 
 

@@ -118,6 +118,19 @@ int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
  * grid.  Fails with 101 while a reconstruction is open. */
 int spi_bp_set_accumulation(spi_ctx* ctx, int compensated, int fold_every);
 
+/* Insert the images of several classes in one call (no counterpart in the
+ * reference, which reconstructs one volume per run; the per-image work is
+ * BP32FQ's loop, bp32f.f:802-913).  ctxs[k] is an open reconstruction
+ * (spi_bp_open with class k's box size; at most 16 classes and 8 distinct
+ * box sizes, one spectrum precision); imgs[k] (nimg[k] images of that box,
+ * host or device per imgs_on_device), angles[k] and half[k] (half may be
+ * NULL, or hold NULL entries) as for spi_bp_insert.  Each round stages the
+ * next FFT sub-batch of every class and inserts all of them with ONE kernel
+ * launch whose rows carry their class's box size, table, spectra and grids.
+ * All work runs on ctxs[0]'s stream; the call returns when it is done. */
+int spi_bp_insert_multi(spi_ctx* const* ctxs, int nclass, const float* const* imgs, const int* nimg,
+                        const float* const* angles, const uint8_t* const* half, int imgs_on_device);
+
 /* Complete the grids of the open reconstruction: fold pending partial sums
  * and add the compensation in, so that caller-owned grids hold the full sums
  * (call before summing them across processes).  Synchronises the stream. */
@@ -290,6 +303,14 @@ int spi_fslice_adjoint(const spi_fslice_plan* plan, const float* slices, float* 
 /* grid_out = E^T E grid_in + lam * grid_in in one pass over the taps
  * (grid_out must not alias grid_in). */
 int spi_fslice_normal(const spi_fslice_plan* plan, const float* grid_in, float lam, float* grid_out, void* stream);
+/* The same normal operator on FP64 grids (double2 [2nx][2nx][nx+1]): same taps
+ * and FP32 table weights, FP64 pixel sums and FP64 atomic scatter.  For CG:
+ * late directions p have ||E^T E p|| << ||E^T E|| ||p||, where FP32 sums lose
+ * that many digits. */
+int spi_fslice_normal64(const spi_fslice_plan* plan, const double* grid_in, double lam, double* grid_out,
+                        void* stream);
+/* grid = E^T slices into an FP64 grid (FP64 scatter; the CG's right-hand side). */
+int spi_fslice_adjoint64(const spi_fslice_plan* plan, const float* slices, double* grid, void* stream);
 /* Real-space volume float[nx^3] of a grid of spectrum coefficients: the grid
  * models V(k) = sum_v X_v K(k - v), so the volume is the inverse transform of
  * X (plane 0 replaced by its Hermitian part, phase (-1)^(i+j+k), SPIDER's

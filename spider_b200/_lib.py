@@ -37,6 +37,7 @@ SIGNATURES = [
     ("spi_bp_set_spectrum_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_bp_set_accumulation", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     ("spi_bp_flush", ctypes.c_int, [_vp]),
+    ("spi_bp_insert_multi", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int]),
     ("spi_bp_autotune", ctypes.c_int, [_vp, ctypes.c_int]),
     ("spi_bp_get_launch", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
@@ -64,6 +65,8 @@ SIGNATURES = [
     ("spi_fslice_forward", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_adjoint", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_normal", ctypes.c_int, [_vp, _vp, ctypes.c_float, _vp, _vp]),
+    ("spi_fslice_normal64", ctypes.c_int, [_vp, _vp, ctypes.c_double, _vp, _vp]),
+    ("spi_fslice_adjoint64", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_volume", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_plan_destroy", ctypes.c_int, [_vp]),
     ("spi_pj3q_plan_forward", ctypes.c_int, [_vp, _vp, _vp, _vp]),

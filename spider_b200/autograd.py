@@ -164,6 +164,29 @@ class FourierSlicePlan:
         ops.check(self._L.spi_fslice_normal(self._h, self._p(grid), float(lam), self._p(out), self._stream()))
         return out
 
+    def normal64(self, grid: torch.Tensor, lam: float, out: torch.Tensor | None = None) -> torch.Tensor:
+        """E^T E + lam I on FP64 grids: FP64 sums and scatter, FP32 table weights."""
+        import ctypes
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
+        for t in (grid, out):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ops.SpiderError(101, "normal64 needs contiguous float64 CUDA tensors")
+        ops.check(self._L.spi_fslice_normal64(self._h, ctypes.c_void_p(grid.data_ptr()), float(lam),
+                                              ctypes.c_void_p(out.data_ptr()), self._stream()))
+        return out
+
+    def adjoint64(self, slices: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """E^T slices into an FP64 grid (FP64 scatter): the CG's right-hand side."""
+        import ctypes
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
+        if not (out.is_cuda and out.dtype == torch.float64 and out.is_contiguous()):
+            raise ops.SpiderError(101, "adjoint64 needs a contiguous float64 CUDA output")
+        ops.check(self._L.spi_fslice_adjoint64(self._h, self._p(slices), ctypes.c_void_p(out.data_ptr()),
+                                               self._stream()))
+        return out
+
     def volume(self, grid: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
         """Real-space volume [nx, nx, nx] of a grid of spectrum coefficients."""
         if out is None:
@@ -210,30 +233,62 @@ class NormalCG:
     buffers; A is the plan's operator (PJ 3Q with PJ3QPlan, the FourierSlice
     extraction with FourierSlicePlan, whose E^T E + lam I is one fused pass).
     With ``graph`` one iteration is captured once as a CUDA graph and
-    replayed.  Dot products and step lengths are FP64."""
+    replayed.  Dot products and step lengths are FP64; with ``fp64_vectors``
+    (the default for the FourierSlice pair, whose eigenvalues spread over
+    many orders of magnitude) x, r and p are FP64 too, and with
+    ``fp64_operator`` (the default with FP64 vectors on the FourierSlice
+    pair) the normal operator sums in FP64 as well (``normal64``): a late
+    direction p has ||E^T E p|| << ||E^T E|| ||p||, and FP32 sums would lose
+    that many digits.  Otherwise the operator's input and output are FP32.
+    ``solve`` returns x in FP32."""
 
-    def __init__(self, plan, lam: float, iters: int, graph: bool = True):
+    def __init__(self, plan, lam: float, iters: int, graph: bool = True, fp64_vectors: bool | None = None,
+                 fp64_operator: bool | None = None):
         self.plan, self.lam, self.iters, self.graph = plan, float(lam), int(iters), graph
-        z = lambda shape: torch.zeros(shape, dtype=torch.float32, device=plan.device)  # noqa: E731
-        self.x, self.r, self.p, self.ap = (z(plan.shape) for _ in range(4))
         self.fused = hasattr(plan, "normal")
+        self.vec64 = self.fused if fp64_vectors is None else bool(fp64_vectors)
+        # FP64 normal operator (FourierSlice pair with FP64 vectors): no FP32 copies at all
+        self.op64 = (self.vec64 and hasattr(plan, "normal64")) if fp64_operator is None else bool(fp64_operator)
+        if self.op64 and not (self.vec64 and hasattr(plan, "normal64")):
+            raise ops.SpiderError(101, "an FP64 operator needs FP64 vectors and a plan with normal64")
+        vt = torch.float64 if self.vec64 else torch.float32
+        z = lambda shape, dt=torch.float32: torch.zeros(shape, dtype=dt, device=plan.device)  # noqa: E731
+        self.x, self.r, self.p = (z(plan.shape, vt) for _ in range(3))
+        self.ap = None if self.op64 else z(plan.shape)                    # operator output (FP32)
+        self.p32 = z(plan.shape) if (self.vec64 and not self.op64) else None  # operator input (FP32)
+        self.ap64 = z(plan.shape, vt) if self.vec64 else None
         self.q = None if self.fused else z((plan.nang,) + tuple(plan.shape[1:]))
         self.rs = torch.zeros((), dtype=torch.float64, device=plan.device)
         self._g = None
 
     def _iteration(self):
+        if self.op64:
+            self.plan.normal64(self.p, self.lam, out=self.ap64)
+            self._update(self.ap64)
+            return
+        pin = self.p
+        if self.vec64:
+            self.p32.copy_(self.p)
+            pin = self.p32
         if self.fused:
-            self.plan.normal(self.p, self.lam, out=self.ap)
+            self.plan.normal(pin, self.lam, out=self.ap)
         else:
-            self.plan.forward(self.p, out=self.q)
+            self.plan.forward(pin, out=self.q)
             self.plan.adjoint(self.q, out=self.ap)
-            self.ap.add_(self.p, alpha=self.lam)
-        pap = (self.p.double() * self.ap.double()).sum()
-        alpha = torch.where(pap > 0, self.rs / pap, torch.zeros_like(pap)).float()
+            self.ap.add_(pin, alpha=self.lam)
+        ap = self.ap
+        if self.vec64:
+            self.ap64.copy_(self.ap)
+            ap = self.ap64
+        self._update(ap)
+
+    def _update(self, ap):
+        pap = (self.p.double() * ap.double()).sum()
+        alpha = torch.where(pap > 0, self.rs / pap, torch.zeros_like(pap)).to(self.x.dtype)
         self.x.add_(alpha * self.p)
-        self.r.sub_(alpha * self.ap)
+        self.r.sub_(alpha * ap)
         rs_new = (self.r.double() * self.r.double()).sum()
-        beta = torch.where(self.rs > 0, rs_new / self.rs, torch.zeros_like(rs_new)).float()
+        beta = torch.where(self.rs > 0, rs_new / self.rs, torch.zeros_like(rs_new)).to(self.x.dtype)
         self.p.mul_(beta).add_(self.r)
         self.rs.copy_(rs_new)
 
@@ -245,7 +300,7 @@ class NormalCG:
         if not self.graph:
             for _ in range(self.iters):
                 self._iteration()
-            return self.x.clone()
+            return self.x.to(torch.float32, copy=True)
         if self._g is None:
             # warm up on a side stream (as CUDA-graph capture requires), then capture one iteration
             s = torch.cuda.Stream(self.plan.device)
@@ -263,14 +318,16 @@ class NormalCG:
                 t.copy_(v)
         for _ in range(self.iters):
             self._g.replay()
-        return self.x.clone()
+        return self.x.to(torch.float32, copy=True)
 
 
 class _CGReconstruct(torch.autograd.Function):
     @staticmethod
     def forward(fctx, b: torch.Tensor, solver: NormalCG):
         fctx.solver = solver
-        return solver.solve(solver.plan.adjoint(b.detach().contiguous().float()))
+        b = b.detach().contiguous().float()
+        rhs = solver.plan.adjoint64(b) if solver.op64 else solver.plan.adjoint(b)
+        return solver.solve(rhs)
 
     @staticmethod
     def backward(fctx, gx: torch.Tensor):

@@ -429,6 +429,83 @@ __device__ __forceinline__ float kb_tap(const float* tab, float v, int k, float 
   return tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb))];
 }
 
+// One row J of one slice, eight pixels at a time, as described above: the
+// body of insert_x4_kernel and insert_mc_kernel.
+template <bool BF16>
+__device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, const SliceDesc& sd, float4* __restrict__ G,
+                                              int J, int nx, const float* tab, float fltb, int g, int q, int gl) {
+  const int N = 2 * nx, N2 = nx, LN2 = 2;
+  const int NN4 = N * N / 4;
+  const float fN = (float)N;
+  const size_t rowlen = (size_t)(nx + 1);
+  const size_t plane = (size_t)N * rowlen;
+  const int JP = (J >= 0) ? J : N + J;
+  const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
+  const float fJ = (float)J;
+  const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
+  for (int I0 = 0; I0 <= N2 && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+    const int I = I0 + g;
+    bool ok = I <= N2 && (I * I + J * J) < NN4 && !(I == 0 && J < 0);
+    const float fI = (float)I;
+    float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
+    float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
+    float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
+    float br = 0.0f, bi = 0.0f;
+    if (ok) {
+      const float2 sp = load_spec<BF16>(spec, specrow + I);
+      br = sp.x;
+      bi = -sp.y;   // SPIDER forward sign = conjugate of the cuFFT R2C output
+    }
+    if (xnew < 0.0f) {
+      xnew = -xnew; ynew = -ynew; znew = -znew;
+      bi = -bi;
+    }
+    const int ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
+    const int iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
+    const int izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
+    ok = ok && ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
+         izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1);
+    if (!ok) { xnew = ynew = znew = 0.0f; }   // keeps the lookups below in range; no taps follow
+    const int ix0 = ok ? ixn : 0, iy0 = ok ? iyn : 0, iz0 = ok ? izn : 0;
+    const int xs = kb_tap(tab, xnew, ix0 - 2, fltb) != 0.0f ? ix0 - 2 : ix0 - 1;
+    const int ys = kb_tap(tab, ynew, iy0 - 2, fltb) != 0.0f ? iy0 - 2 : iy0 - 1;
+    const int zs = kb_tap(tab, znew, iz0 - 2, fltb) != 0.0f ? iz0 - 2 : iz0 - 1;
+    const float tx = kb_tap(tab, xnew, xs + q, fltb);
+    const float tyq = kb_tap(tab, ynew, ys + q, fltb);
+    const float tzq = kb_tap(tab, znew, zs + q, fltb);
+    float ty[4], tz[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      ty[l] = __shfl_sync(0xffffffffu, tyq, gl + l);
+      tz[l] = __shfl_sync(0xffffffffu, tzq, gl + l);
+    }
+    if (!ok || tx == 0.0f) continue;
+    // main tap at (ixp, iyp, izp), or for ixp < 0 the reflected point
+    // (-ixp, -iyp, -izp) with the conjugate value
+    const int ixp = xs + q;
+    const bool refl = ixp < 0;
+    const float bis = refl ? -bi : bi;
+    const int ixa = refl ? -ixp : ixp;
+#pragma unroll
+    for (int lz = 0; lz < 4; ++lz) {
+      if (tz[lz] == 0.0f) continue;
+      const int izp = zs + lz;
+      const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
+#pragma unroll
+      for (int ly = 0; ly < 4; ++ly) {
+        const float tyz = __fmul_rn(ty[ly], tz[lz]);
+        if (tyz == 0.0f) continue;
+        const int iyp = ys + ly;
+        const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
+        const float wg = __fmul_rn(tx, tyz);
+        if (wg != 0.0f)
+          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
+                    make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
+      }
+    }
+  }
+}
+
 template <bool BF16>
 __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__ spec,
                                                         const SliceDesc* __restrict__ slices, int nslices, int nx,
@@ -439,16 +516,12 @@ __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__
   for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
   __syncthreads();
 
-  const int N = 2 * nx, N2 = nx, LN2 = 2;
-  const int NN4 = N * N / 4;
-  const float fN = (float)N;
+  const int N = 2 * nx;
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2;          // pixel of the group of eight
   const int q = lane & 3;           // x tap of the window
   const int gl = lane & ~3;         // first lane of the group
   const long long nitems = (long long)nslices * N;
-  const size_t rowlen = (size_t)(nx + 1);
-  const size_t plane = (size_t)N * rowlen;
 
   for (;;) {
     unsigned long long it = 0;
@@ -458,72 +531,55 @@ __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__
     const int s = (int)(item / N);
     const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
     const SliceDesc sd = slices[s];
-    float4* G = sd.grid ? g1 : g0;
-    const int JP = (J >= 0) ? J : N + J;
-    const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
-    const float fJ = (float)J;
-    const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
-    for (int I0 = 0; I0 <= N2 && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
-      const int I = I0 + g;
-      bool ok = I <= N2 && (I * I + J * J) < NN4 && !(I == 0 && J < 0);
-      const float fI = (float)I;
-      float xnew = __fadd_rn(__fmul_rn(fI, sd.dm[0]), j3);
-      float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
-      float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
-      float br = 0.0f, bi = 0.0f;
-      if (ok) {
-        const float2 sp = load_spec<BF16>(spec, specrow + I);
-        br = sp.x;
-        bi = -sp.y;   // SPIDER forward sign = conjugate of the cuFFT R2C output
-      }
-      if (xnew < 0.0f) {
-        xnew = -xnew; ynew = -ynew; znew = -znew;
-        bi = -bi;
-      }
-      const int ixn = __float2int_rz(__fadd_rn(__fadd_rn(xnew, 0.5f), fN)) - N;
-      const int iyn = __float2int_rz(__fadd_rn(__fadd_rn(ynew, 0.5f), fN)) - N;
-      const int izn = __float2int_rz(__fadd_rn(__fadd_rn(znew, 0.5f), fN)) - N;
-      ok = ok && ixn <= (N2 - LN2 - 1) && iyn >= (-N2 + 2 + LN2) && iyn <= (N2 - LN2 - 1) &&
-           izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1);
-      if (!ok) { xnew = ynew = znew = 0.0f; }   // keeps the lookups below in range; no taps follow
-      const int ix0 = ok ? ixn : 0, iy0 = ok ? iyn : 0, iz0 = ok ? izn : 0;
-      const int xs = kb_tap(tab, xnew, ix0 - 2, fltb) != 0.0f ? ix0 - 2 : ix0 - 1;
-      const int ys = kb_tap(tab, ynew, iy0 - 2, fltb) != 0.0f ? iy0 - 2 : iy0 - 1;
-      const int zs = kb_tap(tab, znew, iz0 - 2, fltb) != 0.0f ? iz0 - 2 : iz0 - 1;
-      const float tx = kb_tap(tab, xnew, xs + q, fltb);
-      const float tyq = kb_tap(tab, ynew, ys + q, fltb);
-      const float tzq = kb_tap(tab, znew, zs + q, fltb);
-      float ty[4], tz[4];
-#pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        ty[l] = __shfl_sync(0xffffffffu, tyq, gl + l);
-        tz[l] = __shfl_sync(0xffffffffu, tzq, gl + l);
-      }
-      if (!ok || tx == 0.0f) continue;
-      // main tap at (ixp, iyp, izp), or for ixp < 0 the reflected point
-      // (-ixp, -iyp, -izp) with the conjugate value
-      const int ixp = xs + q;
-      const bool refl = ixp < 0;
-      const float bis = refl ? -bi : bi;
-      const int ixa = refl ? -ixp : ixp;
-#pragma unroll
-      for (int lz = 0; lz < 4; ++lz) {
-        if (tz[lz] == 0.0f) continue;
-        const int izp = zs + lz;
-        const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
-#pragma unroll
-        for (int ly = 0; ly < 4; ++ly) {
-          const float tyz = __fmul_rn(ty[ly], tz[lz]);
-          if (tyz == 0.0f) continue;
-          const int iyp = ys + ly;
-          const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
-          const float wg = __fmul_rn(tx, tyz);
-          if (wg != 0.0f)
-            atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
-                      make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
-        }
-      }
-    }
+    insert_row_x4<BF16>(spec, sd, sd.grid ? g1 : g0, J, nx, tab, fltb, g, q, gl);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Insert for several classes of different box sizes in one launch (BP 32F of
+// each class, the image loop bp32f.f:802-913 run for all classes together).
+// The work items are the rows of every class's slices, class after class;
+// a row finds its class by its item index and takes that class's box size,
+// table (one shared-memory copy per distinct box size), spectra and grids.
+// Each row is inserted exactly as insert_x4_kernel inserts it.
+struct McClass {
+  const void* spec;            // spectra of the class's images in this launch
+  const SliceDesc* slices;     // the class's slice descriptors
+  float4* g0;                  // grids the taps go to (half-set 1 and 2)
+  float4* g1;
+  long long item0;             // first work item (row) of the class
+  int nx, nslices, tab, pad;   // box size, slices, table index
+};
+static_assert(sizeof(McClass) == 56, "class descriptor is 56 bytes");
+constexpr int kMcMaxClass = 16, kMcMaxTab = 8;
+
+template <bool BF16>
+__global__ void __launch_bounds__(512) insert_mc_kernel(const McClass* __restrict__ cls, int ncls, long long nitems,
+                                                        const float* __restrict__ tabs, const float* __restrict__ fltbs,
+                                                        int ntab, unsigned long long* __restrict__ work) {
+  extern __shared__ float tab[];   // [ntab][5000]
+  __shared__ McClass sc[kMcMaxClass];
+  __shared__ float sfl[kMcMaxTab];
+  for (int i = threadIdx.x; i < 5000 * ntab; i += blockDim.x) tab[i] = tabs[i];
+  if (threadIdx.x < ncls) sc[threadIdx.x] = cls[threadIdx.x];
+  if (threadIdx.x < ntab) sfl[threadIdx.x] = fltbs[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3, gl = lane & ~3;
+  for (;;) {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(work, 1ull);
+    const long long item = (long long)__shfl_sync(0xffffffffu, it, 0);
+    if (item >= nitems) break;
+    int c = 0;
+    while (c + 1 < ncls && sc[c + 1].item0 <= item) ++c;
+    const McClass& C = sc[c];
+    const int N = 2 * C.nx;
+    const long long local = item - C.item0;
+    const int s = (int)(local / N);
+    const int J = (int)(local % N) - C.nx + 1;
+    const SliceDesc sd = C.slices[s];
+    insert_row_x4<BF16>(C.spec, sd, sd.grid ? C.g1 : C.g0, J, C.nx, tab + 5000 * C.tab, sfl[C.tab], g, q, gl);
   }
 }
 
@@ -1106,6 +1162,8 @@ void bp_release(spi_ctx* c) {
   c->spec_tmp.release();
   c->slices.release();
   c->workctr.release();
+  c->mc_params.release();
+  c->mc_host.release();
   c->cplx.release();
   c->real3.release();
   c->wkb.release();
@@ -1596,20 +1654,17 @@ static int ensure_pipeline_events(spi_ctx* c, int nsubs) {
   return 0;
 }
 
-static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
-                          const uint8_t* half, int imgs_on_device) {
-  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert: no open reconstruction (spi_bp_open)");
-  if (nimg < 0 || (nimg > 0 && (!imgs || !angles))) return fail(kInvalid, "spi_bp_insert: bad image arguments");
-  if (c->merged) return fail(kInvalid, "spi_bp_insert: images cannot follow spi_bp_partial_add");
-  if (nimg == 0) return 0;
-  SPI_CUDA(cudaSetDevice(c->device));
-  SPI_TRY(ensure_chunk_buffers(c));
-  c->inserted = true;
-  const int nx = c->nx, n = c->n, nsym = c->nsym;
-  // slice descriptors for the whole call (host, pinned)
-  const size_t nsl = (size_t)nimg * nsym;
-  SPI_TRY(c->hslices.ensure(nsl * sizeof(SliceDesc)));
-  SliceDesc* hs = c->hslices.as<SliceDesc>();
+// Slice descriptors of nimg images: CANG of each angle triple (BUILDM1,
+// bp3f.f:1287), its products with the symmetry matrices (bp3f.f:460-466) and
+// the grid its half-set mask routes it to; image index a % chunk.  With slice
+// ordering on, the slices of each group of `group` images within a chunk are
+// ordered by the normal of their central plane (boustrophedon over rings of
+// the polar angle), so the slices in flight together touch overlapping
+// voxels and their atomics hit in L2; the order only changes the FP32
+// summation order.
+static void build_slices(const spi_ctx* c, const float* angles, const uint8_t* half, int nimg, int chunk, int group,
+                         SliceDesc* hs) {
+  const int nsym = c->nsym;
   for (int a = 0; a < nimg; ++a) {
     float dm[9];
     cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);  // BUILDM1 (bp3f.f:1287)
@@ -1620,21 +1675,14 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
       else memcpy(dms, dm, sizeof(dms));
       SliceDesc& d = hs[(size_t)a * nsym + s];
       memcpy(d.dm, dms, 6 * sizeof(float));
-      d.img = a;  // rebased per chunk below
+      d.img = a % chunk;
       d.grid = g;
     }
   }
-  for (int a = 0; a < nimg; ++a)
-    for (int s = 0; s < nsym; ++s) hs[(size_t)a * nsym + s].img = a % c->chunk;
-  if (c->slice_order) {
-    // Within each FFT sub-batch (one insertion launch), order slices by the
-    // normal of their central plane (boustrophedon over rings of the polar
-    // angle) so that the slices in flight together touch overlapping voxels
-    // and their atomics hit in L2.  The order only changes the FP32
-    // summation order.
-    for (int a0 = 0; a0 < nimg; a0 += c->chunk)
-      for (int b0 = a0; b0 < std::min(nimg, a0 + c->chunk); b0 += c->sort_group) {
-      const int nb = std::min(c->sort_group, std::min(nimg, a0 + c->chunk) - b0);
+  if (!c->slice_order) return;
+  for (int a0 = 0; a0 < nimg; a0 += chunk)
+    for (int b0 = a0; b0 < std::min(nimg, a0 + chunk); b0 += group) {
+      const int nb = std::min(group, std::min(nimg, a0 + chunk) - b0);
       SliceDesc* base = hs + (size_t)b0 * nsym;
       const int m = nb * nsym;
       const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
@@ -1656,7 +1704,23 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
       std::vector<SliceDesc> tmp(base, base + m);
       for (int q = 0; q < m; ++q) base[q] = tmp[key[q].second];
     }
-  }
+}
+
+static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
+                          const uint8_t* half, int imgs_on_device) {
+  if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert: no open reconstruction (spi_bp_open)");
+  if (nimg < 0 || (nimg > 0 && (!imgs || !angles))) return fail(kInvalid, "spi_bp_insert: bad image arguments");
+  if (c->merged) return fail(kInvalid, "spi_bp_insert: images cannot follow spi_bp_partial_add");
+  if (nimg == 0) return 0;
+  SPI_CUDA(cudaSetDevice(c->device));
+  SPI_TRY(ensure_chunk_buffers(c));
+  c->inserted = true;
+  const int nx = c->nx, n = c->n, nsym = c->nsym;
+  // slice descriptors for the whole call (host, pinned)
+  const size_t nsl = (size_t)nimg * nsym;
+  SPI_TRY(c->hslices.ensure(nsl * sizeof(SliceDesc)));
+  SliceDesc* hs = c->hslices.as<SliceDesc>();
+  build_slices(c, angles, half, nimg, c->chunk, c->sort_group, hs);
   int klp_count = 0;
   {
     float rr = (float)(nx / 2) * (float)(nx / 2);
@@ -1807,6 +1871,238 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   // chunk's uploads then run under this chunk's last insertion.
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
+}
+
+// ----------------------------------------------------------------------------
+// Multi-class insertion: the images of several open reconstructions (one
+// context per class, each opened with its own box size) in one call whose
+// insertion is one launch per round over the slices of every class.  All work
+// runs on the first context's stream: while the call runs, the other
+// classes' contexts use that stream (their own are idle and restored after).
+namespace {
+struct StreamSwap {
+  std::vector<spi_ctx*> ctxs;
+  std::vector<cudaStream_t> saved;
+  ~StreamSwap() {
+    for (size_t i = 0; i < ctxs.size(); ++i) ctxs[i]->stream = saved[i];
+  }
+};
+}  // namespace
+
+static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* const* imgs, const int* nimg,
+                                const float* const* angles, const uint8_t* const* half, int imgs_on_device) {
+  if (!ctxs || ncls < 1 || ncls > kMcMaxClass || !imgs || !nimg || !angles)
+    return fail(kInvalid, "spi_bp_insert_multi: %d classes (1..%d) or NULL arrays", ncls, kMcMaxClass);
+  spi_ctx* lead = ctxs[0];
+  for (int k = 0; k < ncls; ++k) {
+    spi_ctx* c = ctxs[k];
+    if (!c || c->ngrids == 0) return fail(kInvalid, "spi_bp_insert_multi: class %d has no open reconstruction", k);
+    if (c->merged) return fail(kInvalid, "spi_bp_insert_multi: class %d follows spi_bp_partial_add", k);
+    if (c->device != lead->device || c->bf16 != lead->bf16)
+      return fail(kInvalid, "spi_bp_insert_multi: class %d is on another device or spectrum precision", k);
+    if (nimg[k] < 0 || (nimg[k] > 0 && (!imgs[k] || !angles[k])))
+      return fail(kInvalid, "spi_bp_insert_multi: bad images of class %d", k);
+    for (int j = 0; j < k; ++j)
+      if (ctxs[j] == c) return fail(kInvalid, "spi_bp_insert_multi: class %d repeats a context", k);
+  }
+  // one table per distinct box size
+  std::vector<int> tab_nx, cls_tab(ncls);
+  for (int k = 0; k < ncls; ++k) {
+    auto it = std::find(tab_nx.begin(), tab_nx.end(), ctxs[k]->nx);
+    if (it == tab_nx.end()) {
+      if ((int)tab_nx.size() == kMcMaxTab)
+        return fail(kInvalid, "spi_bp_insert_multi: more than %d distinct box sizes", kMcMaxTab);
+      cls_tab[k] = (int)tab_nx.size();
+      tab_nx.push_back(ctxs[k]->nx);
+    } else {
+      cls_tab[k] = (int)(it - tab_nx.begin());
+    }
+    if (!kb_window4_ok(ctxs[k]->kb))
+      return fail(kInvalid, "spi_bp_insert_multi: the table of nx = %d is not a four-tap window", ctxs[k]->nx);
+  }
+  const int ntab = (int)tab_nx.size();
+  SPI_CUDA(cudaSetDevice(lead->device));
+  StreamSwap swap;
+  for (int k = 0; k < ncls; ++k) {
+    SPI_CUDA(cudaStreamSynchronize(ctxs[k]->stream));
+    swap.ctxs.push_back(ctxs[k]);
+    swap.saved.push_back(ctxs[k]->stream);
+  }
+  cudaStream_t st = lead->stream;
+  for (int k = 1; k < ncls; ++k) ctxs[k]->stream = st;
+  // rounds and slice counts (the FFT sub-batch of each class was set by spi_bp_open)
+  int rounds = 0;
+  std::vector<size_t> sl_off(ncls + 1, 0);
+  for (int k = 0; k < ncls; ++k) {
+    rounds = std::max(rounds, (nimg[k] + ctxs[k]->sub - 1) / ctxs[k]->sub);
+    sl_off[k + 1] = sl_off[k] + (size_t)nimg[k] * ctxs[k]->nsym;
+  }
+  // Everything the host copies during the call sits in one pinned buffer
+  // (copies from pageable memory would synchronise the stream every round):
+  // the slice descriptors of every class, one class table per round, the
+  // tables and their FLTB.
+  const size_t cls_bytes = sizeof(McClass) * kMcMaxClass;
+  const size_t h_sl = 0, h_cls = h_sl + sl_off[ncls] * sizeof(SliceDesc);
+  const size_t h_tab = h_cls + (size_t)std::max(rounds, 1) * cls_bytes;
+  SPI_TRY(lead->mc_host.ensure(h_tab + sizeof(float) * (5000 + 1) * kMcMaxTab));
+  SliceDesc* hs_all = reinterpret_cast<SliceDesc*>(lead->mc_host.as<char>() + h_sl);
+  McClass* hc_all = reinterpret_cast<McClass*>(lead->mc_host.as<char>() + h_cls);
+  float* ht = reinterpret_cast<float*>(lead->mc_host.as<char>() + h_tab);
+  float* hf = ht + 5000 * kMcMaxTab;
+  // launch parameters on the device: class table, then the tables and their FLTB
+  SPI_TRY(lead->mc_params.ensure(cls_bytes + sizeof(float) * (5000 + 1) * kMcMaxTab + sizeof(unsigned long long)));
+  auto* d_cls = lead->mc_params.as<McClass>();
+  float* d_tabs = reinterpret_cast<float*>(lead->mc_params.as<char>() + cls_bytes);
+  float* d_fl = d_tabs + 5000 * kMcMaxTab;
+  auto* d_work = reinterpret_cast<unsigned long long*>(d_fl + kMcMaxTab);
+  for (int t = 0; t < ntab; ++t)
+    for (int k = 0; k < ncls; ++k)
+      if (cls_tab[k] == t) {
+        memcpy(ht + (size_t)5000 * t, ctxs[k]->kb.tab, 5000 * sizeof(float));
+        hf[t] = ctxs[k]->kb.fltb;
+        break;
+      }
+  SPI_CUDA(cudaMemcpyAsync(d_tabs, ht, (size_t)5000 * ntab * sizeof(float), cudaMemcpyHostToDevice, st));
+  SPI_CUDA(cudaMemcpyAsync(d_fl, hf, ntab * sizeof(float), cudaMemcpyHostToDevice, st));
+  const size_t smem = (size_t)5000 * ntab * sizeof(float);
+  {
+    static std::mutex mu;
+    static unsigned long long done = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    const unsigned long long bit = 1ull << (lead->device & 63);
+    if (!(done & bit)) {
+      SPI_CUDA(cudaFuncSetAttribute(insert_mc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(5000 * kMcMaxTab * sizeof(float))));
+      SPI_CUDA(cudaFuncSetAttribute(insert_mc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(5000 * kMcMaxTab * sizeof(float))));
+      done |= bit;
+    }
+  }
+  // per class: buffers (room for two FFT sub-batches: round r stages into
+  // half r % 2 while round r - 1's insertion reads the other), slice
+  // descriptors of all its images, staging constants
+  std::vector<double> klp(ncls);
+  for (int k = 0; k < ncls; ++k) {
+    spi_ctx* c = ctxs[k];
+    SPI_TRY(ensure_chunk_buffers(c));
+    const size_t two = (size_t)std::max(c->chunk, 2 * c->sub);
+    const size_t plane = (size_t)c->n * (c->nx + 1);
+    SPI_TRY(c->spectra.ensure(two * plane * (c->bf16 ? sizeof(__nv_bfloat162) : sizeof(float2))));
+    SPI_TRY(c->slices.ensure(two * c->nsym * sizeof(SliceDesc)));
+    if (!imgs_on_device) SPI_TRY(c->imgs.ensure(two * c->nx * c->nx * sizeof(float)));
+    if (nimg[k] > 0)
+      build_slices(c, angles[k], half ? half[k] : nullptr, nimg[k], c->sub, c->sub, hs_all + sl_off[k]);
+    const int nx = c->nx;
+    int cnt = 0;
+    const float rr = (float)(nx / 2) * (float)(nx / 2);
+    const int nc = nx / 2 + 1;
+    for (int j = 1; j <= nx; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const float t = (float)(j - nc), t2 = (float)(i - nc);
+        if (t * t + t2 * t2 > rr) ++cnt;
+      }
+    klp[k] = (double)(float)cnt;
+    if (nimg[k] > 0) c->inserted = true;
+  }
+  // rounds: every class stages its next FFT sub-batch on the staging stream,
+  // then one launch on the compute stream inserts them all
+  cudaStream_t s2 = lead->stream2;
+  SPI_TRY(ensure_pipeline_events(lead, 2));   // ev_ready[h]: half h staged; ev_done[h]: half h inserted
+  SPI_CUDA(cudaEventRecord(lead->ev_fork, st));
+  SPI_CUDA(cudaStreamWaitEvent(s2, lead->ev_fork, 0));
+  for (int k = 0; k < ncls; ++k) SPI_CUFFT(cufftSetStream(ctxs[k]->plan2d, s2));
+  for (int r = 0; r < rounds; ++r) {
+    const int h = r & 1;
+    McClass* hc = hc_all + (size_t)r * kMcMaxClass;
+    int nc = 0;
+    long long items = 0;
+    if (r >= 2) SPI_CUDA(cudaStreamWaitEvent(s2, lead->ev_done[h], 0));   // round r - 2 read this half
+    for (int k = 0; k < ncls; ++k) {
+      spi_ctx* c = ctxs[k];
+      const int nx = c->nx, n = c->n;
+      const int a0 = r * c->sub, nb = std::min(c->sub, nimg[k] - a0);
+      if (nb <= 0) continue;
+      const size_t plane = (size_t)n * (nx + 1);
+      const size_t hoff = (size_t)h * c->sub;   // first image of this half
+      const float* src = imgs[k] + (size_t)a0 * nx * nx;
+      if (!imgs_on_device) {
+        float* dst = c->imgs.as<float>() + hoff * nx * nx;
+        SPI_CUDA(cudaMemcpyAsync(dst, src, (size_t)nb * nx * nx * sizeof(float), cudaMemcpyHostToDevice, s2));
+        src = dst;
+      }
+      const int ip = (n - nx) / 2 + nx % 2;
+      const int parts = std::max(1, std::min(8, (4 * c->sm_count + c->sub - 1) / c->sub));
+      stage_kernel<<<dim3(c->sub, parts), 256, 0, s2>>>(src, nx, n, ip, nb, klp[k], c->padded.as<float>());
+      SPI_TRY(check_kernel("stage_kernel"));
+      c->count();
+      float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + hoff * plane;
+      SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      if (c->bf16) {
+        const size_t cntv = (size_t)nb * plane;
+        to_bf16_kernel<<<grid_blocks(c, cntv, 256), 256, 0, s2>>>(
+            fout, reinterpret_cast<__nv_bfloat162*>(c->spectra.p) + hoff * plane, cntv);
+        SPI_TRY(check_kernel("to_bf16_kernel"));
+        c->count();
+      }
+      const size_t nsl = (size_t)nb * c->nsym;
+      SliceDesc* dsl = c->slices.as<SliceDesc>() + hoff * c->nsym;
+      SPI_CUDA(cudaMemcpyAsync(dsl, hs_all + sl_off[k] + (size_t)a0 * c->nsym, nsl * sizeof(SliceDesc),
+                               cudaMemcpyHostToDevice, s2));
+      McClass m{};
+      m.spec = c->bf16 ? (const void*)(reinterpret_cast<__nv_bfloat162*>(c->spectra.p) + hoff * plane)
+                       : (const void*)(c->spectra.as<float2>() + hoff * plane);
+      m.slices = dsl;
+      m.g0 = insert_target(c, 0);
+      m.g1 = insert_target(c, c->ngrids == 2 ? 1 : 0);
+      m.item0 = items;
+      m.nx = nx;
+      m.nslices = (int)nsl;
+      m.tab = cls_tab[k];
+      hc[nc++] = m;
+      items += (long long)nsl * n;
+    }
+    SPI_CUDA(cudaEventRecord(lead->ev_ready[h], s2));
+    if (nc == 0) continue;
+    SPI_CUDA(cudaStreamWaitEvent(st, lead->ev_ready[h], 0));
+    SPI_CUDA(cudaMemcpyAsync(d_cls, hc, nc * sizeof(McClass), cudaMemcpyHostToDevice, st));
+    SPI_CUDA(cudaMemsetAsync(d_work, 0, sizeof(unsigned long long), st));
+    int per_sm = 1;
+    if (lead->bf16)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_mc_kernel<true>, 512, smem);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_mc_kernel<false>, 512, smem);
+    const int blocks = lead->sm_count * std::max(1, std::min(per_sm, 2));
+    int ev = lead->phase_begin(2, st);
+    if (lead->bf16)
+      insert_mc_kernel<true><<<blocks, 512, smem, st>>>(d_cls, nc, items, d_tabs, d_fl, ntab, d_work);
+    else
+      insert_mc_kernel<false><<<blocks, 512, smem, st>>>(d_cls, nc, items, d_tabs, d_fl, ntab, d_work);
+    SPI_TRY(check_kernel("insert_mc_kernel"));
+    lead->phase_end(ev);
+    lead->count();
+    SPI_CUDA(cudaEventRecord(lead->ev_done[h], st));
+    for (int k = 0; k < ncls; ++k) {
+      spi_ctx* c = ctxs[k];
+      const int nb = std::min(c->sub, nimg[k] - r * c->sub);
+      if (nb <= 0) continue;
+      c->unfolded += nb;
+      if (c->unfolded >= c->fold_every) SPI_TRY(fold_grids(c, false));
+    }
+    // the staging buffers and descriptors of every class are reused next round
+  }
+  for (int k = 0; k < ncls; ++k) {
+    if (nimg[k] <= 0) continue;
+    ctxs[k]->pending_sym0[0] = true;
+    if (ctxs[k]->ngrids == 2) ctxs[k]->pending_sym0[1] = true;
+  }
+  SPI_CUDA(cudaStreamSynchronize(s2));
+  SPI_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+extern "C" int spi_bp_insert_multi(spi_ctx* const* ctxs, int nclass, const float* const* imgs, const int* nimg,
+                                   const float* const* angles, const uint8_t* const* half, int imgs_on_device) {
+  return bp_insert_multi_impl(ctxs, nclass, imgs, nimg, angles, half, imgs_on_device);
 }
 
 // ----------------------------------------------------------------------------

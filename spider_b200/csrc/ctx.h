@@ -58,6 +58,8 @@ struct spi_ctx {
   spi::DevBuf spec_tmp;               // float2 [sub][n][nx+1] (BF16 mode FFT output)
   spi::DevBuf slices;                 // SliceDesc [chunk * nsym]
   spi::DevBuf workctr;                // u64 row counter of the running insert launch
+  spi::DevBuf mc_params;              // multi-class insertion: class table + tables of the launch
+  spi::HostBuf mc_host;               // multi-class insertion: pinned descriptors, class tables, tables
   spi::DevBuf cplx;                   // float2 [n][n][nx+1] (inverse FFT input)
   spi::DevBuf real3;                  // float [n][n][n]
   spi::DevBuf wkb;                    // float[(nx/2)^2 + 1]

@@ -213,6 +213,103 @@ __global__ void __launch_bounds__(256) fs_kernel(const float2* __restrict__ in, 
   }
 }
 
+// The normal operator in FP64: the same taps and FP32 table weights, with the
+// grids, the pixel sums and the scatter (FP64 atomics) in double precision.
+// Late CG iterations apply E^T E to directions whose image is much smaller
+// than ||E^T E|| ||p||; FP32 sums would lose that many digits there.
+__device__ __forceinline__ double2 fs_gather64(const double2* __restrict__ X, const FsWin& w, int q, int nx) {
+  double2 acc = make_double2(0.0, 0.0);
+  if (!w.ok) return acc;
+#pragma unroll
+  for (int lz = 0; lz < 4; ++lz) {
+    if (w.tz[lz] == 0.0f) continue;
+#pragma unroll
+    for (int ly = 0; ly < 4; ++ly) {
+      const float tyz = __fmul_rn(w.ty[ly], w.tz[lz]);
+      if (tyz == 0.0f) continue;
+      const float wg = __fmul_rn(w.tx, tyz);
+      if (wg == 0.0f) continue;
+      bool refl;
+      const double2 v = X[fs_voxel(w, q, ly, lz, nx, refl)];
+      const double d = (double)wg;
+      acc.x = __dadd_rn(acc.x, __dmul_rn(v.x, d));
+      acc.y = refl ? __dsub_rn(acc.y, __dmul_rn(v.y, d)) : __dadd_rn(acc.y, __dmul_rn(v.y, d));
+    }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void fs_scatter64(double2* __restrict__ X, const FsWin& w, int q, int nx, double2 b) {
+  if (!w.ok) return;
+#pragma unroll
+  for (int lz = 0; lz < 4; ++lz) {
+    if (w.tz[lz] == 0.0f) continue;
+#pragma unroll
+    for (int ly = 0; ly < 4; ++ly) {
+      const float tyz = __fmul_rn(w.ty[ly], w.tz[lz]);
+      if (tyz == 0.0f) continue;
+      const float wg = __fmul_rn(w.tx, tyz);
+      if (wg == 0.0f) continue;
+      bool refl;
+      double* v = reinterpret_cast<double*>(X + fs_voxel(w, q, ly, lz, nx, refl));
+      const double d = (double)wg;
+      atomicAdd(v, __dmul_rn(b.x, d));
+      atomicAdd(v + 1, refl ? -__dmul_rn(b.y, d) : __dmul_rn(b.y, d));
+    }
+  }
+}
+
+// NORMAL: E^T E of an FP64 grid; else E^T of FP32 slices (`sl_in`) into an
+// FP64 grid.
+template <bool NORMAL>
+__global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restrict__ in, const float2* __restrict__ sl_in,
+                                                          double2* __restrict__ out,
+                                                          const FsDesc* __restrict__ slices, int nslices, int nx,
+                                                          const float* __restrict__ kbtab, float fltb) {
+  extern __shared__ float tab[];
+  for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
+  __syncthreads();
+  const int N = 2 * nx, NN4 = N * N / 4;
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3, gl = lane & ~3;
+  const long long nitems = (long long)nslices * N;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < nitems;
+       item += warps) {
+    const int s = (int)(item / N);
+    const int J = (int)(item % N) - nx + 1;
+    const FsDesc sd = slices[s];
+    const int JP = (J >= 0) ? J : N + J;
+    const size_t srow = ((size_t)sd.img * N + JP) * (size_t)(nx + 1);
+    for (int I0 = 0; I0 <= nx && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+      FsWin w;
+      fs_window(sd, I0 + g, J, nx, tab, fltb, q, gl, w);
+      double2 v;
+      if (NORMAL) {
+        v = fs_gather64(in, w, q, nx);
+        v.x = __dadd_rn(v.x, __shfl_xor_sync(0xffffffffu, v.x, 1));
+        v.y = __dadd_rn(v.y, __shfl_xor_sync(0xffffffffu, v.y, 1));
+        v.x = __dadd_rn(v.x, __shfl_xor_sync(0xffffffffu, v.x, 2));
+        v.y = __dadd_rn(v.y, __shfl_xor_sync(0xffffffffu, v.y, 2));
+      } else {   // BTQ = BI = conj(T), or T for a flipped pixel
+        v = make_double2(0.0, 0.0);
+        if (w.ok) {
+          const float2 t = sl_in[srow + I0 + g];
+          v = make_double2((double)t.x, w.flipped ? (double)t.y : -(double)t.y);
+        }
+      }
+      fs_scatter64(out, w, q, nx, v);
+    }
+  }
+}
+
+__global__ void fs_scale64_kernel(const double2* __restrict__ p, double lam, double2* __restrict__ q, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = p[i];
+    q[i] = make_double2(__dmul_rn(lam, v.x), __dmul_rn(lam, v.y));
+  }
+}
+
 __global__ void fs_scale_kernel(const float2* __restrict__ p, float lam, float2* __restrict__ q, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float2 v = p[i];
@@ -434,6 +531,34 @@ int spi_fslice_normal(const spi_fslice_plan* p, const float* grid_in, float lam,
                                                    p->fltb);
   SPI_TRY(check_kernel("fs_kernel<normal>"));
   p->ctx->count(2);
+  return 0;
+}
+
+int spi_fslice_normal64(const spi_fslice_plan* p, const double* grid_in, double lam, double* grid_out, void* stream) {
+  if (!p || !grid_in || !grid_out) return fail(kInvalid, "spi_fslice_normal64: NULL argument");
+  if (grid_in == grid_out) return fail(kInvalid, "spi_fslice_normal64: input and output must differ");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t ne = fs_grid_elems(p);
+  fs_scale64_kernel<<<fs_grid_blocks(p, ne), 256, 0, s>>>(reinterpret_cast<const double2*>(grid_in), lam,
+                                                          reinterpret_cast<double2*>(grid_out), ne);
+  SPI_TRY(check_kernel("fs_scale64_kernel"));
+  fs_normal64_kernel<true><<<fs_blocks(p), 256, kFsSmem, s>>>(reinterpret_cast<const double2*>(grid_in), nullptr,
+                                                              reinterpret_cast<double2*>(grid_out), p->sl, p->nang,
+                                                              p->nx, p->tab, p->fltb);
+  SPI_TRY(check_kernel("fs_normal64_kernel"));
+  p->ctx->count(2);
+  return 0;
+}
+
+int spi_fslice_adjoint64(const spi_fslice_plan* p, const float* slices, double* grid, void* stream) {
+  if (!p || !grid || !slices) return fail(kInvalid, "spi_fslice_adjoint64: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  SPI_CUDA(cudaMemsetAsync(grid, 0, fs_grid_elems(p) * sizeof(double2), s));
+  fs_normal64_kernel<false><<<fs_blocks(p), 256, kFsSmem, s>>>(nullptr, reinterpret_cast<const float2*>(slices),
+                                                               reinterpret_cast<double2*>(grid), p->sl, p->nang,
+                                                               p->nx, p->tab, p->fltb);
+  SPI_TRY(check_kernel("fs_normal64_kernel<insert>"));
+  p->ctx->count();
   return 0;
 }
 

@@ -33,10 +33,12 @@ def allreduce_grids(tensors, group=None):
     return tensors
 
 
-def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
+def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None, allreduce=None):
     """BP 32F over all ranks: each rank passes the full image set (or its own
     block), inserts its SETPART block into caller-owned grids, the grids are
-    all-reduced, and every rank finishes the three volumes."""
+    completed (spi_bp_flush) and summed over the ranks, and every rank
+    finishes the three volumes.  ``allreduce`` sums a list of tensors in place
+    over the ranks (default: torch.distributed, NCCL on GPUs)."""
     import ctypes
 
     import torch
@@ -46,7 +48,7 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
     nx = int(imgs.shape[-1])
     gb = ctypes.c_longlong()
     _lib.check(L.spi_bp_grid_bytes(nx, ctypes.byref(gb)))
-    dev = device or torch.device(f"cuda:{ctx.device}")
+    dev = torch.device(device) if device is not None else torch.device(f"cuda:{ctx.device}")
     # spi_bp_open zeroes attached grids on the library stream; torch.empty
     # leaves no fill pending on torch's stream that could land after it
     grids = [torch.empty(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
@@ -58,10 +60,11 @@ def sharded_bp32f(ctx, imgs, angles, half, rank: int, world: int, device=None):
         if count:
             ctx.bp_insert(imgs[start:start + count], angles[start:start + count], half[start:start + count])
         ctx.bp_flush()                  # grids hold the complete sums; the library stream is idle
-        allreduce_grids(grids)
+        (allreduce or allreduce_grids)(grids)
         # NCCL orders the reduce on torch's current stream only; the library
         # stream (non-blocking) would not wait for it before SYMPLANE0/NRMW2
-        torch.cuda.synchronize(dev)
+        if dev.type == "cuda":
+            torch.cuda.synchronize(dev)
         out = ctx.bp_finish(("all", "1", "2"))
         return out["all"], out["1"], out["2"]
     finally:

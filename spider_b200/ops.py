@@ -231,19 +231,37 @@ def bp32f(imgs, angles, half, sym=None, *, ctx: Context | None = None, bf16: boo
 
 
 def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, concurrent: bool = True,
-                     device_out: bool = False, autotune: bool = False):
+                     device_out: bool = False, autotune: bool = False, one_launch: bool = True, ctxs=None):
     """``BP 32F`` of several classes of one image stream: ``classes`` is a list
     of (images [n_k, nx_k, nx_k], angles [n_k, 3], half mask [n_k]) with any
-    box sizes.  Each class has its own context (grids, FFT plans, streams);
-    with ``concurrent`` the classes are inserted from one host thread each,
-    so that their launches share the GPU.  Returns a list of (vol, vol1, vol2)."""
+    box sizes.  Each class has its own context (grids, FFT plans).  With
+    ``one_launch`` (default) all classes go through spi_bp_insert_multi: one
+    insertion launch per round over every class's slices, on one stream.
+    Otherwise, with ``concurrent`` the classes are inserted from one host
+    thread each, so that their launches share the GPU.  Returns a list of
+    (vol, vol1, vol2).  ``ctxs``: one context per class to use (and keep
+    open) instead of new ones, so that repeated calls reuse their buffers
+    and FFT plans."""
     import concurrent.futures as cf
-    ctxs = [Context(device) for _ in classes]
+    own = ctxs is None
+    if own:
+        ctxs = [Context(device) for _ in classes]
+    elif len(ctxs) != len(classes):
+        raise SpiderError(101, "one context per class")
     try:
         for c, (imgs, _, _) in zip(ctxs, classes):
             c.bp_open(_nx_of(imgs), 2, sym, bf16=bf16)
-            if autotune:            # launch shape per box size (cached per process)
+            if autotune and not one_launch:   # launch shape per box size (cached per process)
                 c.bp_autotune()
+
+        if one_launch:
+            bp_insert_multi(ctxs, classes)
+            out = []
+            for c in ctxs:
+                o = c.bp_finish(("all", "1", "2"), device=device_out)
+                out.append((o["all"], o["1"], o["2"]))
+                c.bp_close()
+            return out
 
         def insert(k):
             imgs, ang, half = classes[k]
@@ -263,8 +281,43 @@ def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, 
             c.bp_close()
         return out
     finally:
-        for c in ctxs:
-            c.close()
+        if own:
+            for c in ctxs:
+                c.close()
+
+
+def bp_insert_multi(ctxs, classes):
+    """spi_bp_insert_multi: insert (images, angles, half) of every class into
+    its open context, all classes in one insertion launch per round."""
+    k = len(ctxs)
+    if k != len(classes):
+        raise SpiderError(101, "one context per class")
+    keep = []
+    dev = None
+    P = ctypes.c_void_p * k
+    pi, pa, ph = P(), P(), P()
+    counts = (ctypes.c_int * k)()
+    for i, (imgs, ang, half) in enumerate(classes):
+        d = _is_dev(imgs)
+        if dev is None:
+            dev = d
+        elif d != dev:
+            raise SpiderError(101, "all classes' images must be on the host or all on the device")
+        if not d:
+            imgs = _host_f32(imgs)
+        a = _host_f32(ang)
+        if a.shape[0] != imgs.shape[0]:
+            raise SpiderError(101, f"class {i}: {imgs.shape[0]} images but {a.shape[0]} angle triples")
+        h = None if half is None else np.ascontiguousarray(
+            half.detach().cpu().numpy() if (torch is not None and isinstance(half, torch.Tensor)) else half,
+            dtype=np.uint8)
+        keep += [imgs, a, h]
+        pi[i] = _ptr(imgs).value if int(imgs.shape[0]) else None
+        pa[i] = _ptr(a).value if int(a.shape[0]) else None
+        ph[i] = None if h is None else _ptr(h).value
+        counts[i] = int(imgs.shape[0])
+    handles = P(*[c.handle.value for c in ctxs])
+    check(ctxs[0]._L.spi_bp_insert_multi(handles, k, pi, counts, pa, ph, 1 if dev else 0))
 
 
 def _rb_mode(ctx, fbs):

@@ -207,21 +207,63 @@ def test_rb3f_rb32f_match_oracle(ctx, orc):
     assert synth.rel_l2(z, ops.bp3f(pr, ang, ctx=ctx)) <= 2e-6
 
 
-@pytest.mark.parametrize("concurrent", [True, False])
-def test_bp32f_multiclass(orc, concurrent):
-    """Several classes of different box sizes (one odd) reconstructed from one
-    image stream, concurrently from one host thread per class or in turn."""
+@pytest.mark.parametrize("mode", ["one_launch", "concurrent", "in_turn"])
+def test_bp32f_multiclass(orc, mode):
+    """Several classes of different box sizes (one odd, two equal) reconstructed
+    from one image stream: all classes in one insertion launch per round
+    (spi_bp_insert_multi), or one context per class inserted concurrently from
+    one host thread each, or in turn."""
     classes, refs = [], []
-    for k, (nx, nimg) in enumerate(((24, 120), (32, 200), (41, 150))):
+    for k, (nx, nimg) in enumerate(((24, 120), (32, 200), (41, 150), (32, 90))):
         _, pr, ang = _case(nx, nimg, 90 + k, noise=0.5)
         half = synth.half_mask(nimg, np.random.default_rng(95 + k))
         classes.append((pr, ang, half))
         refs.append(orc.bp32f(pr, ang, half, prec=0, nthreads=1))
-    out = ops.bp32f_multiclass(classes, concurrent=concurrent)
+    out = ops.bp32f_multiclass(classes, one_launch=mode == "one_launch", concurrent=mode == "concurrent")
     for got, ref in zip(out, refs):
         for a, b in zip(got, ref):
             assert a.shape == b.shape
             assert synth.rel_l2(a, b) <= TOL
+
+
+def test_bp_insert_multi_rounds_and_errors(ctx, orc):
+    """spi_bp_insert_multi with device images and FFT sub-batches smaller
+    than the image counts (several rounds, classes running out at different
+    rounds): one insertion launch per round, volumes equal to the oracle's;
+    invalid calls are refused with 101."""
+    import torch
+    os.environ["SPI_BP_SUB"] = "64"
+    ctxs = [ops.Context(0) for _ in range(3)]
+    try:
+        data = []
+        for k, (nx, nimg) in enumerate(((16, 300), (20, 70), (16, 130))):
+            _, pr, ang = _case(nx, nimg, 400 + k)
+            half = synth.half_mask(nimg, np.random.default_rng(410 + k))
+            data.append((torch.from_numpy(pr).cuda(), ang, half))
+            ctxs[k].bp_open(nx, 2)
+        l0 = ctxs[0].launches
+        ops.bp_insert_multi(ctxs, data)
+        rounds = (300 + 63) // 64
+        # per round one insertion launch plus the staging of each class that still has images
+        staged = sum((n + 63) // 64 for n in (300, 70, 130))
+        assert ctxs[0].launches - l0 >= rounds
+        outs = []
+        for c in ctxs:
+            o = c.bp_finish(("all", "1", "2"))
+            outs.append((o["all"], o["1"], o["2"]))
+            c.bp_close()
+        for (pr, ang, half), got in zip(data, outs):
+            ref = orc.bp32f(pr.cpu().numpy(), ang, half, prec=0)
+            for a, b in zip(got, ref):
+                assert synth.rel_l2(a, b) <= TOL
+        with pytest.raises(ops.SpiderError) as e:       # a closed class
+            ops.bp_insert_multi(ctxs[:1], data[:1])
+        assert e.value.code == 101
+        assert staged > rounds
+    finally:
+        del os.environ["SPI_BP_SUB"]
+        for c in ctxs:
+            c.close()
 
 
 def test_bp_autotune(ctx, orc):

@@ -4,9 +4,11 @@ oracle pair; the differentiable slice function against central finite
 differences (h = 1e-3) on 64 random voxels and against the FP64 adjoint; the
 graph-captured CG on the pair against an FP64 CG on the oracle pair.
 
-Bars: relative L2 <= 1e-5 for the operators (FP32 sums of at most 64 taps per
-pixel, FP32 atomics in the insertion); <= 1e-4 for CG iterates (the
-solution's conditioning amplifies FP32 summation order)."""
+Bars: relative L2 <= 1e-5 for the FP32 operators (FP32 sums of at most 64
+taps per pixel, FP32 atomics in the insertion), 1e-12 for the FP64 normal
+operator; <= 1e-4 for CG iterates.  The CG runs on the FP64 normal operator
+by default: with FP32 sums, late directions p (||E^T E p|| << ||E^T E|| ||p||)
+lose digits, and the iterate drifts from the FP64 CG by far more than 1e-4."""
 import numpy as np
 import pytest
 
@@ -54,6 +56,14 @@ def test_fslice_operators_match_oracle(ctx, orc, nx):
         nrm = _cplx(plan.normal(_real(X), lam))
         two = orc.fslice_insert(ref_ex, ang) + lam * X.astype(np.complex128)
         assert np.linalg.norm(nrm - two) <= TOL * np.linalg.norm(two)
+        # the FP64 normal operator: FP64 sums and scatter of the same taps
+        x64 = _real(X).double()
+        n64 = plan.normal64(x64.contiguous(), lam).cpu().numpy()
+        n64 = n64[..., 0] + 1j * n64[..., 1]
+        assert np.linalg.norm(n64 - two) <= 1e-12 * np.linalg.norm(two)
+        a64 = plan.adjoint64(_real(T)).cpu().numpy()
+        a64 = a64[..., 0] + 1j * a64[..., 1]
+        assert np.linalg.norm(a64 - ref_ins) <= 1e-12 * np.linalg.norm(ref_ins)
         print(f"nx={nx}: extract {np.linalg.norm(ex - ref_ex) / np.linalg.norm(ref_ex):.2e}, "
               f"insert {np.linalg.norm(ins - ref_ins) / np.linalg.norm(ref_ins):.2e}, "
               f"normal {np.linalg.norm(nrm - two) / np.linalg.norm(two):.2e}, adjoint identity "
@@ -132,9 +142,10 @@ def test_fourier_cg_graph_plain_and_fp64(ctx, orc):
     plan = autograd.FourierSlicePlan(nx, ang, ctx=ctx)
     try:
         b = plan.stage(imgs)
-        rhs = plan.adjoint(b)
-        xg = autograd.NormalCG(plan, lam, iters, graph=True).solve(rhs)
-        xp = autograd.NormalCG(plan, lam, iters, graph=False).solve(rhs)
+        rhs64 = plan.adjoint64(b)
+        xg = autograd.NormalCG(plan, lam, iters, graph=True).solve(rhs64)
+        xp = autograd.NormalCG(plan, lam, iters, graph=False).solve(rhs64)
+        x32 = autograd.NormalCG(plan, lam, iters, graph=True, fp64_operator=False).solve(plan.adjoint(b))
         assert synth.rel_l2(xp.cpu().numpy(), xg.cpu().numpy()) <= 1e-4
         v = plan.volume(xg.contiguous()).cpu().numpy()
         bh = _cplx(b)
@@ -154,7 +165,9 @@ def test_fourier_cg_graph_plain_and_fp64(ctx, orc):
         p = r + (rs_new / rs) * p
         rs = rs_new
     e = np.linalg.norm(_cplx(xg) - x) / np.linalg.norm(x)
-    print(f"Fourier CG, {iters} iterations: graph vs FP64 oracle CG {e:.2e}")
+    e32 = np.linalg.norm(_cplx(x32) - x) / np.linalg.norm(x)
+    print(f"Fourier CG, {iters} iterations: FP64 operator vs FP64 oracle CG {e:.2e}; "
+          f"FP32 operator {e32:.2e}")
     assert e <= 1e-4
     g = np.arange(nx) - nx // 2
     m = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= (0.4 * nx) ** 2
@@ -173,6 +186,7 @@ def test_fslice_volume_matches_numpy(ctx, orc):
     nx = 24
     n = 2 * nx
     X = (rng.standard_normal((n, n, nx + 1)) + 1j * rng.standard_normal((n, n, nx + 1)))
+    X[:, :, nx] = 0.0      # no tap reaches i = nx (IXN <= NX - 3), so a solution grid is zero there
     plan = autograd.FourierSlicePlan(nx, synth.so3_angles(3, rng), ctx=ctx)
     try:
         got = plan.volume(_real(X)).cpu().numpy()
@@ -182,9 +196,9 @@ def test_fslice_volume_matches_numpy(ctx, orc):
     jm, km = (-np.arange(n)) % n, (-np.arange(n)) % n
     Z[:, :, 0] = 0.5 * (X[:, :, 0] + np.conj(X[km][:, jm][:, :, 0]))
     k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(nx + 1), indexing="ij")
-    Z = Z * np.where((i + j + k) % 2 == 1, -1.0, 1.0)
+    Z = np.conj(Z * np.where((i + j + k) % 2 == 1, -1.0, 1.0))   # SPIDER's inverse sign
     Z[0, 0, 0] = Z[0, 0, 0].real
-    R = np.fft.irfftn(Z, s=(n, n, n))               # sum of conj(conj Z) e^{+...} / n^3
+    R = np.fft.irfftn(Z, s=(n, n, n), axes=(0, 1, 2))   # sum of Z e^{+2 pi i k.x} / n^3
     ip = (n - nx) // 2 + nx % 2
     crop = R[ip:ip + nx, ip:ip + nx, ip:ip + nx]
     wkb = orc.windkb_table(nx).astype(np.float64)
@@ -193,3 +207,66 @@ def test_fslice_volume_matches_numpy(ctx, orc):
     lr = gg[:, None, None] ** 2 + gg[None, :, None] ** 2 + gg[None, None, :] ** 2
     ref = np.where(lr <= (nx // 2) ** 2, crop * wkb[np.minimum(lr, len(wkb) - 1)], 0.0)
     assert synth.rel_l2(got, ref) <= TOL
+
+
+def _oracle_cg(orc, rhs, ang, lam, iters):
+    x = np.zeros_like(rhs)
+    r = rhs.copy()
+    p = r.copy()
+    rs = np.vdot(r, r).real
+    for _ in range(iters):
+        ap = orc.fslice_insert(orc.fslice_extract(p, ang), ang) + lam * p
+        alpha = rs / np.vdot(p, ap).real
+        x += alpha * p
+        r -= alpha * ap
+        rs_new = np.vdot(r, r).real
+        p = r + (rs_new / rs) * p
+        rs = rs_new
+    return x
+
+
+def test_fourier_cg_reconstruct_gradient(ctx, orc):
+    """cg_reconstruct on the FourierSlice pair: x = (E^T E + lam I)^-1 E^T b
+    by CG, differentiable in the slices b through a second CG solve (implicit
+    differentiation: dL/db = E (E^T E + lam I)^-1 dL/dx).  Solution and
+    gradient against the same iterations in FP64 on the oracle pair, and the
+    gradient against central finite differences (h = 1e-3) of the FP64
+    reconstruction on 64 random slice values."""
+    import torch
+    from spider_b200 import autograd
+    rng = np.random.default_rng(44)
+    nx, nang, lam, iters = 16, 30, 5.0, 40
+    n = 2 * nx
+    ang = synth.so3_angles(nang, rng)
+    b = rng.standard_normal((nang, n, nx + 1)) + 1j * rng.standard_normal((nang, n, nx + 1))
+    w = rng.standard_normal((n, n, nx + 1)) + 1j * rng.standard_normal((n, n, nx + 1))
+    plan = autograd.FourierSlicePlan(nx, ang, ctx=ctx)
+    try:
+        solver = autograd.NormalCG(plan, lam, iters, graph=True)
+        bt = _real(b).requires_grad_(True)
+        x = autograd.cg_reconstruct(bt, solver)
+        loss = (x.double() * _real(w).double()).sum()
+        loss.backward()
+        grad = _cplx(bt.grad)
+        xg = _cplx(x)
+    finally:
+        plan.close()
+    # the extraction leaves pixels without taps at zero, so b enters only where E^T reads it
+    x_ref = _oracle_cg(orc, orc.fslice_insert(b, ang), ang, lam, iters)
+    assert np.linalg.norm(xg - x_ref) <= 1e-5 * np.linalg.norm(x_ref)
+    g_ref = orc.fslice_extract(_oracle_cg(orc, w, ang, lam, iters), ang)
+    assert np.linalg.norm(grad - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+    h = 1e-3
+    scale = np.abs(g_ref).max()
+    wy = _oracle_cg(orc, w, ang, lam, iters)       # M^-1 w: L(b) = Re<w, M^-1 E^T b> = Re<E M^-1 w, b>
+    touched = np.argwhere(np.abs(g_ref) > 0)
+    for k, (a, j, i) in enumerate(touched[rng.choice(len(touched), 64, replace=False)]):
+        comp = 1.0 if k % 2 == 0 else 1j
+        bp, bm = b.copy(), b.copy()
+        bp[a, j, i] += h * comp
+        bm[a, j, i] -= h * comp
+        lp = np.sum((np.conj(wy) * orc.fslice_insert(bp, ang)).real)
+        lm = np.sum((np.conj(wy) * orc.fslice_insert(bm, ang)).real)
+        fd = (lp - lm) / (2 * h)
+        g = grad[a, j, i].real if k % 2 == 0 else grad[a, j, i].imag
+        assert abs(g - fd) <= 1e-4 * max(abs(fd), 1e-3 * scale)
