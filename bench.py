@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--interp", choices=["linear", "fbs"], default="linear")
     p.add_argument("--mc-images", type=int, default=80000)
     p.add_argument("--no-mc", action="store_true", help="skip the multi-class measurement")
+    p.add_argument("--no-config5", action="store_true",
+                   help="skip the BF16 / 8,192-image-step run and the 256^3 FourierSlice CG")
     p.add_argument("--cg-n", type=int, default=128)
     p.add_argument("--cg-nang", type=int, default=10000)
     p.add_argument("--cg-iters", type=int, default=6)
@@ -246,6 +248,72 @@ def fp64_check(ctx, nx, chunks, angles, halves, nimg, bf16):
     for name, vols in gpu.items():
         out[name] = {k: synth.rel_l2(a, b) for k, a, b in zip(("all", "first", "second"), vols, ref)}
     out["fsc_nyquist_compensated"] = float(synth.fsc(gpu["compensated"][0], ref[0])[nx // 2])
+    return out, ref
+
+
+def config5_measure(args, ctx, stream, chunks, angles, halves, ref, steps=12, cg_iters=30):
+    """Configuration 5's reduced-precision form at 256^3: BP 32F with BF16
+    spectra, 8,192-image steps (the two resident 4,096-image chunks, new
+    angles every step), `steps` steps timed on the library stream (~98k
+    images); its volumes for the FP64-checked images against the FP64 oracle;
+    and a FourierSlice CG at 256^3 on those 8,192 images, `cg_iters`
+    iterations replayed as a CUDA graph (FP64 normal operator and vectors)
+    against the same iterations launched op by op."""
+    import torch
+    from spider_b200 import autograd, synth
+    nx = int(chunks[0].shape[-1])
+    imgs = torch.cat([chunks[0], chunks[1]]).contiguous()
+    n8 = int(imgs.shape[0])
+    rng = np.random.default_rng(5005)
+    out = {"images_per_step": n8, "steps": steps, "spectra": "bf16"}
+    ctx.bp_open(nx, 2, bf16=True)
+    ctx.bp_autotune()
+    ctx.bp_insert(imgs, synth.so3_angles(n8, rng), synth.half_mask(n8, rng))   # warm-up
+    angs = [synth.so3_angles(n8, rng) for _ in range(steps)]
+    hs = [synth.half_mask(n8, rng) for _ in range(steps)]
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        ctx.bp_insert(imgs, angs[i], hs[i])
+    e1.record(stream)
+    e1.synchronize()
+    ctx.bp_close()
+    out["images_per_s"] = n8 * steps / (e0.elapsed_time(e1) / 1e3)
+    if ref is not None:
+        per = [min(args.check_images // 2, int(c.shape[0])) for c in chunks[:2]]
+        ctx.bp_open(nx, 2, bf16=True)
+        for k in range(2):
+            ctx.bp_insert(chunks[k][:per[k]], angles[k][:per[k]], halves[k][:per[k]])
+        o = ctx.bp_finish(("all", "1", "2"))
+        ctx.bp_close()
+        out["rel_l2_vs_fp64"] = {k: synth.rel_l2(a, b) for k, a, b in
+                                 zip(("all", "first", "second"), (o["all"], o["1"], o["2"]), ref)}
+        out["fsc_nyquist_vs_fp64"] = float(synth.fsc(o["all"], ref[0])[nx // 2])
+    # FourierSlice CG at 256^3
+    ang = np.concatenate([angles[0][:int(chunks[0].shape[0])], angles[1][:int(chunks[1].shape[0])]])
+    plan = autograd.FourierSlicePlan(nx, ang, ctx=ctx)
+    b = plan.stage(imgs)
+    rhs = plan.adjoint64(b)
+    del b
+    cg = {"images": n8, "iterations": cg_iters, "lambda": 1e-3}
+    for name, graph, iters in (("graph", True, cg_iters), ("plain", False, 3)):
+        s1 = autograd.NormalCG(plan, 1e-3, 1, graph=graph)
+        sk = autograd.NormalCG(plan, 1e-3, iters, graph=graph)
+        t = []
+        for sv in (s1, sk):
+            sv.solve(rhs)                          # warm-up (and graph capture)
+            e0.record()
+            sv.solve(rhs)
+            e1.record()
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1) / 1e3)
+        cg[f"{name}_s_per_iter"] = (t[1] - t[0]) / (iters - 1)
+        cg[f"{name}_solve_s"] = t[1]
+        del s1, sk
+    plan.close()
+    out["fourier_cg"] = cg
     return out
 
 
@@ -728,9 +796,13 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_mc:
         mc = multiclass_measure(args)
 
-    check = None
+    check, ref = None, None
     if rank == 0 and world == 1 and args.check_images > 0:
-        check = fp64_check(ctx, nx, chunks, angles, halves, args.check_images, args.bf16)
+        check, ref = fp64_check(ctx, nx, chunks, angles, halves, args.check_images, args.bf16)
+
+    c5 = None
+    if rank == 0 and world == 1 and not args.no_config5 and nx == 256:
+        c5 = config5_measure(args, ctx, stream, chunks, angles, halves, ref)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -761,6 +833,7 @@ def run_ours(args):
             "finish_phase_ms": finish_phase_ms,
             "bpcg": cg,
             "multiclass": mc,
+            "config5": c5,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
