@@ -92,16 +92,20 @@ def measured_peak():
 
 
 def traffic_per_image(kernel):
-    """DRAM bytes per image of the insert kernel, from the committed ncu summary."""
+    """DRAM bytes per image of the insert kernel and the build they were
+    measured on, from the committed ncu summary (None, None if absent)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_traffic.txt")
+    val, where = None, None
     try:
         with open(path) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_image"):
-                    return float(line.split("=")[1].split()[0])
+                    val = float(line.split("=")[1].split()[0])
+                elif line.startswith("measured_at"):
+                    where = line.split("=", 1)[1].strip()
     except Exception:
         pass
-    return None
+    return val, where
 
 
 class ClockSampler:
@@ -729,9 +733,10 @@ def run_ours(args):
     # bytes over the summed launch durations (CUDA events around each launch)
     achieved = bytes_per_img * chunk * args.steps / (insert_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    tpi = traffic_per_image(launch_cfg["kernel"])
+    tpi, tpi_at = traffic_per_image(launch_cfg["kernel"].split("+")[0])   # the same taps with or without prefetch
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (tpi * chunk * args.steps / n_insert) if tpi else None,
+            "traffic_source": f"ncu DRAM bytes per image x images per launch, {tpi_at}" if tpi else None,
             "kernel": launch_cfg["kernel"], "launch": launch_cfg, "peak_kind": peak_kind,
             "algorithmic_bytes_per_image": bytes_per_img, "taps_per_image": taps,
             "launch_ms": insert_ms / n_insert, "launches": n_insert,
