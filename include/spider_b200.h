@@ -109,8 +109,10 @@ int spi_bp_set_spectrum_precision(spi_ctx* ctx, int bf16);
  * reference, whose X += BTQ*W, oneline.f:107-110, is a plain REAL sum).
  * compensated = 1 (default; environment SPI_BP_ACCUM=0 changes the default):
  * the taps of each run of `fold_every` images (0 = the default, 4,096 or
- * SPI_BP_FOLD) are summed with FP32 atomics into a partial grid, which is
- * then folded into the grid by an error-free two-sum whose rounding errors
+ * SPI_BP_FOLD; a fold follows the insertion launch -- one per FFT sub-batch
+ * -- in which the count is reached) are summed with FP32 atomics into a
+ * partial grid, which is then folded into the grid by an error-free two-sum
+ * whose rounding errors
  * are kept in a compensation grid; the compensation is added in once before
  * SYMPLANE0.  The error of the sums then grows with the images per fold, not
  * with all images.  Costs two more grid-sized buffers and one pass over

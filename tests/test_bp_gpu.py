@@ -322,3 +322,39 @@ def test_bp_insert_zero_images_is_noop(ctx):
     finally:
         ctx.bp_close()
     assert all(np.all(v == 0) for v in o.values())
+
+
+def test_accumulation_modes_and_flush(ctx, orc):
+    """Compensated accumulation (default, and with a fold every 50 images)
+    and plain FP32 atomics all match the oracle; spi_bp_flush leaves the
+    grids holding the complete sums (BP 3F P after a flush equals the
+    oracle's partial grids); the mode cannot change while a reconstruction
+    is open."""
+    nx, nimg = 32, 260
+    _, pr, ang = _case(nx, nimg, 501, noise=0.5)
+    ref = orc.bp3f(pr, ang, prec=1)
+    rx, rw = orc.bp3f_partial(pr, ang, prec=1)
+    try:
+        for comp, fold in ((True, 0), (True, 50), (False, 0)):
+            ctx.set_accumulation(comp, fold)
+            got = ops.bp3f(pr, ang, ctx=ctx)
+            assert synth.rel_l2(got, ref) <= TOL, (comp, fold)
+        ctx.set_accumulation(True, 50)
+        ctx.bp_open(nx, 1)
+        try:
+            with pytest.raises(ops.SpiderError) as e:
+                ctx.set_accumulation(False)
+            assert e.value.code == 101
+            ctx.bp_insert(pr, ang)
+            ctx.bp_flush()
+            x, w = ctx.bp_partial_out(0)
+        finally:
+            ctx.bp_close()
+        gx = x[..., 0] + 1j * x[..., 1]
+        assert np.linalg.norm(gx - rx) <= TOL * np.linalg.norm(rx)
+        assert synth.rel_l2(w, rw) <= TOL
+        with pytest.raises(ops.SpiderError) as e:
+            ctx.bp_flush()                       # nothing open
+        assert e.value.code == 101
+    finally:
+        ctx.set_accumulation(True, 0)

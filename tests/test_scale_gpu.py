@@ -77,3 +77,59 @@ def test_config2_rb32f_128_20k_images(ctx, orc):
     g = np.arange(nx) - nx // 2
     m = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= (0.4 * nx) ** 2
     assert np.corrcoef(got[0][m], vol[m])[0, 1] > 0.5
+
+
+def test_config3_fourier_cg_128_10k_images(ctx, orc):
+    """Configuration 3's differentiable reconstruction on the FourierSlice
+    pair: 10,000 PJ 3Q projections of 128^2 from a 50-blob phantom at SNR
+    0.3, CG on (E^T E + 1e-3 I) x = E^T b, 50 iterations replayed as a CUDA
+    graph.  The graph-captured and the op-by-op solve agree, the volume is the
+    phantom, and on the first 2,000 images 5 iterations match an FP64 CG on
+    the oracle pair within 1e-4."""
+    from spider_b200 import autograd
+    nx, nimg, lam = 128, 10000, 1e-3
+    rng = synth.rng_for(2)
+    vol = synth.blob_phantom(nx, 50, sigma=(2.0, 8.0), amp=(0.5, 1.0), rng=rng)
+    ang = synth.so3_angles(nimg, rng)
+    imgs = synth.projection_stack(ctx, vol, ang, snr=0.3, seed=1002)
+    plan = autograd.FourierSlicePlan(nx, ang, ctx=ctx)
+    try:
+        rhs = plan.adjoint64(plan.stage(imgs))
+        xg = autograd.NormalCG(plan, lam, 50, graph=True).solve(rhs)
+        xp = autograd.NormalCG(plan, lam, 50, graph=False).solve(rhs)
+        e_gp = synth.rel_l2(xp.cpu().numpy(), xg.cpu().numpy())
+        v = plan.volume(xg.contiguous()).cpu().numpy()
+    finally:
+        plan.close()
+    g = np.arange(nx) - nx // 2
+    m = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2) <= (0.4 * nx) ** 2
+    cc = np.corrcoef(v[m], vol[m])[0, 1]
+    print(f"config 3: 50 iterations graph vs op by op {e_gp:.2e}; volume vs phantom correlation {cc:.4f}")
+    assert e_gp <= 1e-4
+    assert cc > 0.7      # noisy data (SNR 0.3) and little regularisation: a loose bar on the content
+    # FP64 check on a subset
+    nsub, its = 2000, 5
+    sub = autograd.FourierSlicePlan(nx, ang[:nsub], ctx=ctx)
+    try:
+        bs = sub.stage(imgs[:nsub].contiguous())
+        x = autograd.NormalCG(sub, lam, its, graph=True).solve(sub.adjoint64(bs)).cpu().numpy().astype(np.float64)
+        bh = bs.cpu().numpy().astype(np.float64)
+    finally:
+        sub.close()
+    bh = bh[..., 0] + 1j * bh[..., 1]
+    a = ang[:nsub]
+    r = orc.fslice_insert(bh, a)
+    xr = np.zeros_like(r)
+    p = r.copy()
+    rs = np.vdot(r, r).real
+    for _ in range(its):
+        ap = orc.fslice_insert(orc.fslice_extract(p, a), a) + lam * p
+        alpha = rs / np.vdot(p, ap).real
+        xr += alpha * p
+        r -= alpha * ap
+        rs_new = np.vdot(r, r).real
+        p = r + (rs_new / rs) * p
+        rs = rs_new
+    e = np.linalg.norm(x[..., 0] + 1j * x[..., 1] - xr) / np.linalg.norm(xr)
+    print(f"config 3 subset: {its} iterations vs FP64 oracle CG {e:.2e}")
+    assert e <= 1e-4
