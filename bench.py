@@ -733,7 +733,7 @@ def run_ours(args):
     # bytes over the summed launch durations (CUDA events around each launch)
     achieved = bytes_per_img * chunk * args.steps / (insert_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    tpi, tpi_at = traffic_per_image(launch_cfg["kernel"].split("+")[0])   # the same taps with or without prefetch
+    tpi, tpi_at = traffic_per_image(launch_cfg["kernel"])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (tpi * chunk * args.steps / n_insert) if tpi else None,
             "traffic_source": f"ncu DRAM bytes per image x images per launch, {tpi_at}" if tpi else None,

@@ -149,8 +149,7 @@ int spi_bp_flush(spi_ctx* ctx);
 int spi_bp_autotune(spi_ctx* ctx, int force);
 
 /* The insertion launch in use: kernel (0 tile, 1 direct, 2 five x-tap lanes,
- * 3 four lanes over the nonzero window, 5 the same with the next pixels'
- * spectrum values and the next row prefetched), threads per CTA, CTAs per SM, and
+ * 3 four lanes over the nonzero window), threads per CTA, CTAs per SM, and
  * the autotuner's time of one sample launch in ms (0 when not tuned). */
 int spi_bp_get_launch(const spi_ctx* ctx, int* kernel, int* threads, int* blocks_per_sm, float* tuned_ms);
 

@@ -430,10 +430,8 @@ __device__ __forceinline__ float kb_tap(const float* tab, float v, int k, float 
 }
 
 // One row J of one slice, eight pixels at a time, as described above: the
-// body of insert_x4_kernel and insert_mc_kernel.  With PF the spectrum
-// values of the next eight pixels are loaded while the current ones are
-// inserted (two more registers; the taps and their order are unchanged).
-template <bool BF16, bool PF = false>
+// body of insert_x4_kernel and insert_mc_kernel.
+template <bool BF16>
 __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, const SliceDesc& sd, float4* __restrict__ G,
                                               int J, int nx, const float* tab, float fltb, int g, int q, int gl) {
   const int N = 2 * nx, N2 = nx, LN2 = 2;
@@ -445,8 +443,6 @@ __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, con
   const size_t specrow = (size_t)sd.img * plane + (size_t)JP * rowlen;
   const float fJ = (float)J;
   const float j3 = __fmul_rn(fJ, sd.dm[3]), j4 = __fmul_rn(fJ, sd.dm[4]), j5 = __fmul_rn(fJ, sd.dm[5]);
-  float2 sp_next = make_float2(0.0f, 0.0f);
-  if (PF && g <= N2 && (g * g + J * J) < NN4 && !(g == 0 && J < 0)) sp_next = load_spec<BF16>(spec, specrow + g);
   for (int I0 = 0; I0 <= N2 && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
     const int I = I0 + g;
     bool ok = I <= N2 && (I * I + J * J) < NN4 && !(I == 0 && J < 0);
@@ -455,16 +451,7 @@ __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, con
     float ynew = __fadd_rn(__fmul_rn(fI, sd.dm[1]), j4);
     float znew = __fadd_rn(__fmul_rn(fI, sd.dm[2]), j5);
     float br = 0.0f, bi = 0.0f;
-    if (PF) {
-      const float2 sp = sp_next;
-      const int In = I + 8;
-      sp_next = make_float2(0.0f, 0.0f);
-      if (In <= N2 && (In * In + J * J) < NN4) sp_next = load_spec<BF16>(spec, specrow + In);
-      if (ok) {
-        br = sp.x;
-        bi = -sp.y;
-      }
-    } else if (ok) {
+    if (ok) {
       const float2 sp = load_spec<BF16>(spec, specrow + I);
       br = sp.x;
       bi = -sp.y;   // SPIDER forward sign = conjugate of the cuFFT R2C output
@@ -519,10 +506,7 @@ __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, con
   }
 }
 
-// PF: besides the spectrum prefetch, a warp takes its next row from the
-// counter when it starts the current one, so the atomic's round trip is
-// hidden behind the row (each warp takes one row past the end at most).
-template <bool BF16, bool PF = false>
+template <bool BF16>
 __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__ spec,
                                                         const SliceDesc* __restrict__ slices, int nslices, int nx,
                                                         const float* __restrict__ kbtab, float fltb,
@@ -539,22 +523,15 @@ __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__
   const int gl = lane & ~3;         // first lane of the group
   const long long nitems = (long long)nslices * N;
 
-  unsigned long long nxt = 0;
-  if (PF && lane == 0) nxt = atomicAdd(work, 1ull);
   for (;;) {
     unsigned long long it = 0;
-    if (PF) {
-      it = nxt;
-    } else if (lane == 0) {
-      it = atomicAdd(work, 1ull);
-    }
+    if (lane == 0) it = atomicAdd(work, 1ull);
     const long long item = (long long)__shfl_sync(0xffffffffu, it, 0);
     if (item >= nitems) break;
-    if (PF && lane == 0) nxt = atomicAdd(work, 1ull);
     const int s = (int)(item / N);
     const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
     const SliceDesc sd = slices[s];
-    insert_row_x4<BF16, PF>(spec, sd, sd.grid ? g1 : g0, J, nx, tab, fltb, g, q, gl);
+    insert_row_x4<BF16>(spec, sd, sd.grid ? g1 : g0, J, nx, tab, fltb, g, q, gl);
   }
 }
 
@@ -1469,8 +1446,7 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
     const char* m = getenv("SPI_INSERT");
     const int def_mode = kb_window4_ok(c->kb) ? 3 : 2;
     c->insert_mode = !m ? def_mode : strcmp(m, "tile") == 0 ? 0 : strcmp(m, "direct") == 0 ? 1
-                   : strcmp(m, "xlane") == 0 ? 2 : strcmp(m, "tilefx") == 0 ? 4
-                   : (strcmp(m, "x4p") == 0 && def_mode == 3) ? 5 : def_mode;
+                   : strcmp(m, "xlane") == 0 ? 2 : strcmp(m, "tilefx") == 0 ? 4 : def_mode;
     const char* o = getenv("SPI_SLICE_ORDER");
     c->slice_order = (o && strcmp(o, "input") == 0) ? 0 : 1;
     const char* mp = getenv("SPI_INSERT_MAP");
@@ -1595,7 +1571,7 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
   const float fltb = c->kb.fltb;
   float4* g0 = insert_target(c, 0);
   int ev_ins = c->phase_begin(2);
-  if ((c->insert_mode >= 1 && c->insert_mode <= 3) || c->insert_mode == 5) {
+  if (c->insert_mode >= 1 && c->insert_mode <= 3) {
     const size_t smem = 5000 * sizeof(float);
     const int threads = c->insert_threads;
     if (c->insert_mode == 1) {
@@ -1606,19 +1582,16 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
         insert_kernel<false><<<insert_blocks(c, insert_kernel<false>, threads, smem, c->insert_blocks_per_sm),
                                threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1,
                                                            c->insert_seg_map);
-    } else if (c->insert_mode == 3 || c->insert_mode == 5) {
+    } else if (c->insert_mode == 3) {
       SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
       auto* work = c->workctr.as<unsigned long long>();
       SPI_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), c->stream));
-#define SPI_X4(B, P)                                                                                         \
-  insert_x4_kernel<B, P><<<insert_blocks(c, insert_x4_kernel<B, P>, threads, smem, c->insert_blocks_per_sm), \
-                           threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work)
-      if (c->insert_mode == 5) {
-        if (c->bf16) SPI_X4(true, true); else SPI_X4(false, true);
-      } else {
-        if (c->bf16) SPI_X4(true, false); else SPI_X4(false, false);
-      }
-#undef SPI_X4
+      if (c->bf16)
+        insert_x4_kernel<true><<<insert_blocks(c, insert_x4_kernel<true>, threads, smem, c->insert_blocks_per_sm),
+                                 threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
+      else
+        insert_x4_kernel<false><<<insert_blocks(c, insert_x4_kernel<false>, threads, smem, c->insert_blocks_per_sm),
+                                  threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
     } else {
       // row counter of this launch (launches on the library stream are serialised)
       SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
@@ -2188,8 +2161,7 @@ static int bp_autotune_impl(spi_ctx* c, int force) {
   const size_t plane = (size_t)c->n * (nx + 1);
   SPI_CUDA(cudaMemsetAsync(c->spectra.p, 0, (size_t)sample * plane * (c->bf16 ? 4 : 8), c->stream));
   float4* g1 = insert_target(c, c->ngrids == 2 ? 1 : 0);
-  const bool w4 = kb_window4_ok(c->kb);
-  const int modes[3] = {w4 ? 3 : 2, w4 ? 5 : 2, 2};
+  const int modes[2] = {kb_window4_ok(c->kb) ? 3 : 2, 2};
   const int shapes[5][2] = {{256, 2}, {256, 3}, {512, 2}, {128, 4}, {512, 1}};
   cudaEvent_t e0, e1;
   SPI_CUDA(cudaEventCreate(&e0));
@@ -2201,8 +2173,8 @@ static int bp_autotune_impl(spi_ctx* c, int force) {
   c->timing = false;
   TuneVal best{c->insert_mode, c->insert_threads, c->insert_blocks_per_sm, 1e30f};
   int st = 0;
-  for (int mi = 0; mi < 3 && !st; ++mi) {
-    if (mi > 0 && modes[mi] == modes[0]) continue;
+  for (int mi = 0; mi < 2 && !st; ++mi) {
+    if (mi == 1 && modes[0] == modes[1]) break;
     for (auto& sh : shapes) {
       c->insert_mode = modes[mi];
       c->insert_threads = sh[0];

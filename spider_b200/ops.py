@@ -111,8 +111,7 @@ class Context:
         self._nx = nx
         self._ngrids = ngrids
 
-    KERNELS = {0: "insert_tile_kernel", 1: "insert_kernel", 2: "insert_xlane_kernel", 3: "insert_x4_kernel",
-               5: "insert_x4_kernel+prefetch"}
+    KERNELS = {0: "insert_tile_kernel", 1: "insert_kernel", 2: "insert_xlane_kernel", 3: "insert_x4_kernel"}
 
     def bp_autotune(self, force: bool = False) -> dict:
         """Pick the insertion kernel and launch shape for the open
