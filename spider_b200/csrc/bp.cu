@@ -428,12 +428,20 @@ __global__ void __launch_bounds__(512) insert_xlane_kernel(const void* __restric
 __device__ __forceinline__ float kb_tap(const float* tab, float v, int k, float fltb) {
   return tab[nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb))];
 }
+// The same lookup in a table cut after entry `last`, which (like every entry
+// after it) is zero: for a table kb_window4_ok accepts, the result is the
+// same as kb_tap's.
+__device__ __forceinline__ float kb_tap_cut(const float* tab, float v, int k, float fltb, int last) {
+  return tab[min(nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb)), last)];
+}
 
 // One row J of one slice, eight pixels at a time, as described above: the
 // body of insert_x4_kernel and insert_mc_kernel.
-template <bool BF16>
+template <bool BF16, int CUT = 0>
 __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, const SliceDesc& sd, float4* __restrict__ G,
                                               int J, int nx, const float* tab, float fltb, int g, int q, int gl) {
+  // CUT > 0: the table holds entries 0..CUT-1 only (see kb_tap_cut)
+  auto tap = [&](float v, int k) { return CUT ? kb_tap_cut(tab, v, k, fltb, CUT - 1) : kb_tap(tab, v, k, fltb); };
   const int N = 2 * nx, N2 = nx, LN2 = 2;
   const int NN4 = N * N / 4;
   const float fN = (float)N;
@@ -467,12 +475,12 @@ __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, con
          izn >= (-N2 + 2 + LN2) && izn <= (N2 - LN2 - 1);
     if (!ok) { xnew = ynew = znew = 0.0f; }   // keeps the lookups below in range; no taps follow
     const int ix0 = ok ? ixn : 0, iy0 = ok ? iyn : 0, iz0 = ok ? izn : 0;
-    const int xs = kb_tap(tab, xnew, ix0 - 2, fltb) != 0.0f ? ix0 - 2 : ix0 - 1;
-    const int ys = kb_tap(tab, ynew, iy0 - 2, fltb) != 0.0f ? iy0 - 2 : iy0 - 1;
-    const int zs = kb_tap(tab, znew, iz0 - 2, fltb) != 0.0f ? iz0 - 2 : iz0 - 1;
-    const float tx = kb_tap(tab, xnew, xs + q, fltb);
-    const float tyq = kb_tap(tab, ynew, ys + q, fltb);
-    const float tzq = kb_tap(tab, znew, zs + q, fltb);
+    const int xs = tap(xnew, ix0 - 2) != 0.0f ? ix0 - 2 : ix0 - 1;
+    const int ys = tap(ynew, iy0 - 2) != 0.0f ? iy0 - 2 : iy0 - 1;
+    const int zs = tap(znew, iz0 - 2) != 0.0f ? iz0 - 2 : iz0 - 1;
+    const float tx = tap(xnew, xs + q);
+    const float tyq = tap(ynew, ys + q);
+    const float tzq = tap(znew, zs + q);
     float ty[4], tz[4];
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
@@ -552,15 +560,20 @@ struct McClass {
 };
 static_assert(sizeof(McClass) == 56, "class descriptor is 56 bytes");
 constexpr int kMcMaxClass = 16, kMcMaxTab = 8;
+// Entries of a table the multi-class kernel keeps: a table kb_window4_ok
+// accepts is zero from floor(2 * FLTB) - 1 = 3331 on (FLTB = 4999/3), so
+// 3,332 entries (13 KB) hold every nonzero value and a zero to clamp to;
+// eight tables then fit two CTAs per SM.
+constexpr int kMcTab = 3332;
 
 template <bool BF16>
 __global__ void __launch_bounds__(512) insert_mc_kernel(const McClass* __restrict__ cls, int ncls, long long nitems,
                                                         const float* __restrict__ tabs, const float* __restrict__ fltbs,
                                                         int ntab, unsigned long long* __restrict__ work) {
-  extern __shared__ float tab[];   // [ntab][5000]
+  extern __shared__ float tab[];   // [ntab][kMcTab]
   __shared__ McClass sc[kMcMaxClass];
   __shared__ float sfl[kMcMaxTab];
-  for (int i = threadIdx.x; i < 5000 * ntab; i += blockDim.x) tab[i] = tabs[i];
+  for (int i = threadIdx.x; i < kMcTab * ntab; i += blockDim.x) tab[i] = tabs[(i / kMcTab) * 5000 + i % kMcTab];
   if (threadIdx.x < ncls) sc[threadIdx.x] = cls[threadIdx.x];
   if (threadIdx.x < ntab) sfl[threadIdx.x] = fltbs[threadIdx.x];
   __syncthreads();
@@ -579,7 +592,8 @@ __global__ void __launch_bounds__(512) insert_mc_kernel(const McClass* __restric
     const int s = (int)(local / N);
     const int J = (int)(local % N) - C.nx + 1;
     const SliceDesc sd = C.slices[s];
-    insert_row_x4<BF16>(C.spec, sd, sd.grid ? C.g1 : C.g0, J, C.nx, tab + 5000 * C.tab, sfl[C.tab], g, q, gl);
+    insert_row_x4<BF16, kMcTab>(C.spec, sd, sd.grid ? C.g1 : C.g0, J, C.nx, tab + kMcTab * C.tab, sfl[C.tab], g, q,
+                                gl);
   }
 }
 
@@ -1964,7 +1978,9 @@ static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* con
       }
   SPI_CUDA(cudaMemcpyAsync(d_tabs, ht, (size_t)5000 * ntab * sizeof(float), cudaMemcpyHostToDevice, st));
   SPI_CUDA(cudaMemcpyAsync(d_fl, hf, ntab * sizeof(float), cudaMemcpyHostToDevice, st));
-  const size_t smem = (size_t)5000 * ntab * sizeof(float);
+  const size_t smem = (size_t)kMcTab * ntab * sizeof(float);
+  // every table must be zero from entry kMcTab - 1 on (checked above by kb_window4_ok: zero from 3331)
+  static_assert(kMcTab >= 3332, "the cut table must keep entries 0..3331");
   {
     static std::mutex mu;
     static unsigned long long done = 0;
@@ -1972,9 +1988,9 @@ static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* con
     const unsigned long long bit = 1ull << (lead->device & 63);
     if (!(done & bit)) {
       SPI_CUDA(cudaFuncSetAttribute(insert_mc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(5000 * kMcMaxTab * sizeof(float))));
+                                    (int)(kMcTab * kMcMaxTab * sizeof(float))));
       SPI_CUDA(cudaFuncSetAttribute(insert_mc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(5000 * kMcMaxTab * sizeof(float))));
+                                    (int)(kMcTab * kMcMaxTab * sizeof(float))));
       done |= bit;
     }
   }
@@ -2071,7 +2087,7 @@ static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* con
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_mc_kernel<true>, 512, smem);
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, insert_mc_kernel<false>, 512, smem);
-    const int blocks = lead->sm_count * std::max(1, std::min(per_sm, 2));
+    const int blocks = lead->sm_count * std::max(1, std::min(per_sm, env_int("SPI_MC_BLOCKS_PER_SM", 2)));
     int ev = lead->phase_begin(2, st);
     if (lead->bf16)
       insert_mc_kernel<true><<<blocks, 512, smem, st>>>(d_cls, nc, items, d_tabs, d_fl, ntab, d_work);
