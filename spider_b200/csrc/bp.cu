@@ -47,50 +47,62 @@ __device__ __forceinline__ double warp_sum(double v) {
 // nx/2 (asta.f:61-92).  The phase BI*(-1)**(I+J+1) (bp3f.f:453-458) equals a
 // circular shift of the padded image by n/2 in both axes, so the padded
 // image is written already shifted: pixel i lands at (ip + i - nx) mod n.
-// One CTA per image; images beyond `nvalid` are written as zeros.
+// One CTA per image (blockIdx.y splits the padded rows over gridDim.y CTAs,
+// each computing the image's border mean itself, when few images fill a
+// launch).  Warps take whole rows, lanes consecutive pixels, so no index is
+// divided; each value is the same (double)pixel - mean rounded to float.
+// Images beyond `nvalid` are written as zeros.
 __global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
                                                     int nvalid, double klp, float* __restrict__ padded) {
-  // blockIdx.y splits the padded image's rows over gridDim.y CTAs (each
-  // computes the image's border mean itself) when few images fill a launch
   const int b = blockIdx.x;
   float* out = padded + (size_t)b * n * n;
   __shared__ double red[8];
   __shared__ double qs_sh;
   const bool valid = b < nvalid;
   const float* img = imgs + (size_t)b * nx * nx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   if (valid) {
     const float rr = (float)(nx / 2) * (float)(nx / 2);
     const int nc = nx / 2 + 1;
     double s = 0.0;
-    for (int p = threadIdx.x; p < nx * nx; p += blockDim.x) {
-      int i = p % nx, j = p / nx;
-      float t = (float)(j + 1 - nc);
-      float t2 = (float)(i + 1 - nc);
-      float r2 = __fadd_rn(__fmul_rn(t, t), __fmul_rn(t2, t2));
-      if (r2 > rr) s += (double)img[p];
+    for (int j = warp; j < nx; j += nwarps) {
+      const float t = (float)(j + 1 - nc);
+      const float tt = __fmul_rn(t, t);
+      const float* row = img + (size_t)j * nx;
+      for (int i = lane; i < nx; i += 32) {
+        const float t2 = (float)(i + 1 - nc);
+        if (__fadd_rn(tt, __fmul_rn(t2, t2)) > rr) s += (double)__ldg(row + i);
+      }
     }
     s = warp_sum(s);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    if (lane == 0) red[warp] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+      for (int w = 0; w < nwarps; ++w) t += red[w];
       qs_sh = t / klp;
     }
     __syncthreads();
   }
   const double qs = valid ? qs_sh : 0.0;
-  const int q0 = (int)(((long long)n * n * blockIdx.y) / gridDim.y);
-  const int q1 = (int)(((long long)n * n * (blockIdx.y + 1)) / gridDim.y);
-  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-    int x = q % n, y = q / n;
-    int i = x + nx - ip;
-    if (i >= n) i -= n;
+  const int y0 = (int)(((long long)n * blockIdx.y) / gridDim.y);
+  const int y1 = (int)(((long long)n * (blockIdx.y + 1)) / gridDim.y);
+  for (int y = y0 + warp; y < y1; y += nwarps) {
     int j = y + nx - ip;
     if (j >= n) j -= n;
-    float v = 0.0f;
-    if (valid && i < nx && j < nx) v = __double2float_rn(__dsub_rn((double)img[(size_t)j * nx + i], qs));
-    out[q] = v;
+    float* orow = out + (size_t)y * n;
+    if (!valid || j >= nx) {                        // a padding row
+      for (int x = lane; x < n; x += 32) orow[x] = 0.0f;
+      continue;
+    }
+    const float* irow = img + (size_t)j * nx;
+    int i = lane + nx - ip;                          // source column of x = lane, kept in [0, n)
+    if (i >= n) i -= n;
+    for (int x = lane; x < n; x += 32) {
+      orow[x] = (i < nx) ? __double2float_rn(__dsub_rn((double)__ldg(irow + i), qs)) : 0.0f;
+      i += 32;
+      if (i >= n) i -= n;
+    }
   }
 }
 

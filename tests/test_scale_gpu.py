@@ -164,3 +164,50 @@ def test_bp32f_256_against_fp64(ctx, orc):
         print(f"256^3 {name}: FP32 spectra {e:.2e} (FSC {f:.7f}), BF16 spectra {e16:.2e} (FSC {f16:.7f})")
         assert e <= TOL and f >= 0.999, name
         assert e16 <= 2e-3 and f16 >= 0.999, name
+
+
+def test_config3_fourier_slice_gradient_128(ctx, orc):
+    """The differentiable FourierSlice at configuration 3's box (128^3, 2,000
+    slices): the backward (the insertion E^T) against the FP64 oracle
+    insertion of the same upstream gradient, and against central finite
+    differences (h = 1e-3) of the forward on 64 random voxels (real and
+    imaginary parts), the loss summed in FP64."""
+    import torch
+    from spider_b200 import autograd
+    rng = np.random.default_rng(3003)
+    nx, nang = 128, 2000
+    n = 2 * nx
+    ang = synth.so3_angles(nang, rng)
+    X = (rng.standard_normal((n, n, nx + 1)) + 1j * rng.standard_normal((n, n, nx + 1))).astype(np.complex64)
+    G = (rng.standard_normal((nang, n, nx + 1)) + 1j * rng.standard_normal((nang, n, nx + 1))).astype(np.complex64)
+    plan = autograd.FourierSlicePlan(nx, ang, ctx=ctx)
+    try:
+        xt = torch.tensor(np.stack([X.real, X.imag], -1), device="cuda").contiguous().requires_grad_(True)
+        gt = torch.tensor(np.stack([G.real, G.imag], -1), device="cuda").contiguous()
+        (autograd.fourier_slice(xt, plan).double() * gt.double()).sum().backward()
+        gr = xt.grad.detach().cpu().numpy().astype(np.float64)
+        grad = gr[..., 0] + 1j * gr[..., 1]
+        exact = orc.fslice_insert(G.astype(np.complex128), ang)
+        e = np.linalg.norm(grad - exact) / np.linalg.norm(exact)
+        touched = np.argwhere(np.abs(exact) > 0)
+        picks = touched[rng.choice(len(touched), 64, replace=False)]
+        h = 1e-3
+        scale = np.abs(exact).max()
+        worst = 0.0
+        x0 = xt.detach()
+        for k, (a, b, c) in enumerate(picks):
+            comp = k % 2
+            xp_, xm_ = x0.clone(), x0.clone()
+            xp_[a, b, c, comp] += h
+            xm_[a, b, c, comp] -= h
+            lp = float((plan.forward(xp_).double() * gt.double()).sum())
+            lm = float((plan.forward(xm_).double() * gt.double()).sum())
+            fd = (lp - lm) / (2 * h)
+            g = grad[a, b, c].real if comp == 0 else grad[a, b, c].imag
+            worst = max(worst, abs(g - fd) / max(abs(fd), 1e-3 * scale))
+    finally:
+        plan.close()
+    print(f"config 3 gradient at 128^3: backward vs FP64 oracle insertion {e:.2e}; "
+          f"finite differences, worst relative gap {worst:.2e}")
+    assert e <= 1e-5
+    assert worst <= 1e-3
