@@ -107,6 +107,179 @@ __global__ void __launch_bounds__(256) stage_kernel(const float* __restrict__ im
 }
 
 // ----------------------------------------------------------------------------
+// Staging and the forward 2D transform for power-of-two padded sizes n, in
+// two passes (FMRS_2's R2C, fmrs_2.f:54-58, with cuFFT's sign and layout:
+// out[y'][k] = sum_y sum_x in[y][x] e^(-2 pi i (k x + y' y) / n), k = 0..n/2).
+// Only the nx rows of the padded image that hold image pixels are nonzero,
+// so the row pass transforms those rows only and the column pass never
+// stores the zero ones.
+//
+// Pass 1 (stage_rowfft_kernel, one CTA per image as stage_kernel, which it
+// replaces): the same staged values (pixel - FP64 border mean, shifted by n/2)
+// for each image row j, then a real FFT of length n as a complex FFT of
+// length h = n/2 of z[m] = in[2m] + i in[2m+1] (radix-2, in shared memory,
+// inputs loaded in bit-reversed order) split into R[k] = E[k] + W^k O[k],
+// E = (Z[k] + conj Z[h-k]) / 2, O = (Z[k] - conj Z[h-k]) / 2i, W = e^(-2 pi i/n).
+// R (h + 1 values) goes to inter[b][j][.].
+// Pass 2 (colfft_kernel): a CTA takes 16 columns k of one image, places row
+// j's values at the padded row y = (j + ip - nx) mod n (bit-reversed), zero
+// elsewhere, and runs 16 complex FFTs of length n.  Twiddles W^t, t < n/2,
+// come from a table computed in FP64 on the host.
+constexpr int kRowThreads = 64;   // threads per row FFT in pass 1
+constexpr int kColTile = 16;      // columns per CTA in pass 2
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
+// in-place radix-2 decimation-in-time stages over `len` points (input in
+// bit-reversed order) at a[0..len); threads t0..t0+nt-1 of the CTA share the
+// work; tw[t] = W_n^t with W_len^u = tw[u * (n / len)]
+__device__ __forceinline__ void fft_stages(float2* a, int len, int lg, const float2* tw, int twstep, int t0, int nt,
+                                           int tid) {
+  for (int st = 1; st <= lg; ++st) {
+    const int half = 1 << (st - 1);
+    const int tws = (len >> st) * twstep;
+    for (int bfly = tid - t0; bfly < (len >> 1); bfly += nt) {
+      const int grp = bfly >> (st - 1), k = bfly & (half - 1);
+      const int pos = (grp << st) + k;
+      const float2 w = tw[k * tws];
+      const float2 u = a[pos], v = cmulf(w, a[pos + half]);
+      a[pos] = make_float2(__fadd_rn(u.x, v.x), __fadd_rn(u.y, v.y));
+      a[pos + half] = make_float2(__fsub_rn(u.x, v.x), __fsub_rn(u.y, v.y));
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int bitrev(int v, int lg) { return (int)(__brev((unsigned)v) >> (32 - lg)); }
+
+__global__ void __launch_bounds__(256) stage_rowfft_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
+                                                           int nvalid, double klp, const float2* __restrict__ twg,
+                                                           float2* __restrict__ inter, size_t inter_stride) {
+  extern __shared__ float2 fsm[];            // tw[n/2], then 4 rows of h complex values
+  const int h = n >> 1, lgh = 31 - __clz(h);
+  float2* tw = fsm;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  const int b = blockIdx.x;
+  if (b >= nvalid) return;                   // uniform per CTA; only valid images are transformed
+  __shared__ double red[8];
+  __shared__ double qs_sh;
+  const float* img = imgs + (size_t)b * nx * nx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  {
+    const float rr = (float)(nx / 2) * (float)(nx / 2);
+    const int nc = nx / 2 + 1;
+    double s = 0.0;
+    for (int j = warp; j < nx; j += nwarps) {
+      const float t = (float)(j + 1 - nc);
+      const float tt = __fmul_rn(t, t);
+      const float* row = img + (size_t)j * nx;
+      for (int i = lane; i < nx; i += 32) {
+        const float t2 = (float)(i + 1 - nc);
+        if (__fadd_rn(tt, __fmul_rn(t2, t2)) > rr) s += (double)__ldg(row + i);
+      }
+    }
+    s = warp_sum(s);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nwarps; ++w) t += red[w];
+      qs_sh = t / klp;
+    }
+    __syncthreads();
+  }
+  const double qs = qs_sh;
+  const int groups = blockDim.x / kRowThreads, grp = threadIdx.x / kRowThreads;
+  float2* a = fsm + h + (size_t)grp * h;
+  float2* ib = inter + (size_t)b * inter_stride;
+  // image rows j0.. of this CTA part (blockIdx.y splits them when few images fill a launch)
+  const int j0 = (int)(((long long)nx * blockIdx.y) / gridDim.y), j1 = (int)(((long long)nx * (blockIdx.y + 1)) / gridDim.y);
+  const int rounds = (j1 - j0 + groups - 1) / groups;
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int j = j0 + rd * groups + grp;
+    const bool has = j < j1;
+    if (has) {
+      const float* irow = img + (size_t)j * nx;
+      for (int m = threadIdx.x - grp * kRowThreads; m < h; m += kRowThreads) {
+        float v2[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int i = 2 * m + e + nx - ip;        // padded column x = 2m + e holds pixel i when i < nx
+          if (i >= n) i -= n;
+          v2[e] = (i < nx) ? __double2float_rn(__dsub_rn((double)__ldg(irow + i), qs)) : 0.0f;
+        }
+        a[bitrev(m, lgh)] = make_float2(v2[0], v2[1]);
+      }
+    }
+    __syncthreads();
+    fft_stages(a, h, lgh, tw, 2, grp * kRowThreads, kRowThreads, threadIdx.x);
+    if (has) {
+      float2* orow = ib + (size_t)j * (h + 1);
+      for (int k = threadIdx.x - grp * kRowThreads; k <= h; k += kRowThreads) {
+        const float2 zk = a[k & (h - 1)], zc = a[(h - k) & (h - 1)];
+        // E = (zk + conj zc) / 2, O = (zk - conj zc) / (2i)
+        const float2 e = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.x, zc.x)), __fmul_rn(0.5f, __fsub_rn(zk.y, zc.y)));
+        const float2 o = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.y, zc.y)), __fmul_rn(-0.5f, __fsub_rn(zk.x, zc.x)));
+        const float2 w = (k < h) ? tw[k] : make_float2(-1.0f, 0.0f);
+        const float2 wo = cmulf(w, o);
+        orow[k] = make_float2(__fadd_rn(e.x, wo.x), __fadd_rn(e.y, wo.y));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) colfft_kernel(const float2* __restrict__ inter, size_t inter_stride, int nx,
+                                                     int n, int ip, int nvalid, const float2* __restrict__ twg,
+                                                     float2* __restrict__ out) {
+  extern __shared__ float2 fsm[];            // tw[n/2], then kColTile columns of n values, stride n + 1
+  const int h = n >> 1, lg = 31 - __clz(n);
+  const int cs = n + 1;                      // column stride: the tile's columns start in different banks
+  const int tiles = (h + 1 + kColTile - 1) / kColTile;
+  const int b = blockIdx.x / tiles, k0 = (blockIdx.x % tiles) * kColTile;
+  float2* tw = fsm;
+  float2* a = fsm + h;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  if (b >= nvalid) return;
+  const int ncol = min(kColTile, h + 1 - k0);
+  for (int q = threadIdx.x; q < kColTile * cs; q += blockDim.x) a[q] = make_float2(0.0f, 0.0f);
+  __syncthreads();
+  const float2* ib = inter + (size_t)b * inter_stride;
+  for (int q = threadIdx.x; q < nx * kColTile; q += blockDim.x) {
+    const int j = q / kColTile, c = q % kColTile;
+    if (c >= ncol) continue;
+    int y = j + ip - nx;
+    if (y < 0) y += n;
+    a[c * cs + bitrev(y, lg)] = ib[(size_t)j * (h + 1) + k0 + c];
+  }
+  __syncthreads();
+  // kColTile transforms of n points; thread t works on column t % kColTile
+  const int c = threadIdx.x % kColTile, tpc = blockDim.x / kColTile, sub = threadIdx.x / kColTile;
+  float2* col = a + (size_t)c * cs;
+  for (int st = 1; st <= lg; ++st) {
+    const int half = 1 << (st - 1);
+    const int tws = n >> st;
+    for (int bfly = sub; bfly < h; bfly += tpc) {
+      const int grp = bfly >> (st - 1), k = bfly & (half - 1);
+      const int pos = (grp << st) + k;
+      const float2 w = tw[k * tws];
+      const float2 u = col[pos], v = cmulf(w, col[pos + half]);
+      col[pos] = make_float2(__fadd_rn(u.x, v.x), __fadd_rn(u.y, v.y));
+      col[pos + half] = make_float2(__fsub_rn(u.x, v.x), __fsub_rn(u.y, v.y));
+    }
+    __syncthreads();
+  }
+  float2* ob = out + (size_t)b * n * (h + 1);
+  for (int q = threadIdx.x; q < n * kColTile; q += blockDim.x) {
+    const int y = q / kColTile, cc = q % kColTile;
+    if (cc < ncol) ob[(size_t)y * (h + 1) + k0 + cc] = a[cc * cs + y];
+  }
+}
+
+// ----------------------------------------------------------------------------
 // RTSQ (rtsq.f:56-140) with QUADRI (quadri.f:83-150): in-plane rotation and
 // shift of each image before PADD2, for RB 3F / RB 32F (bp3f.f:406-425).  One
 // thread per output pixel; per image the host passes COS and SIN of
@@ -1184,6 +1357,7 @@ void bp_release(spi_ctx* c) {
   c->rtsq_prm.release();
   rtsf_release(c);
   c->padded.release();
+  c->fft_tw.release();
   c->spectra.release();
   c->spec_tmp.release();
   c->slices.release();
@@ -1498,6 +1672,13 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   sub = std::max(1, std::min(chunk, env_int("SPI_BP_SUB", sub)));
   c->sub = sub;
   c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
+  {
+    // the own two-pass R2C is opt-in (SPI_FFT=own): measured slower than
+    // staging + cuFFT at 256^3 (2.4 against 1.4 ms per 1,024 images)
+    const char* f = getenv("SPI_FFT");
+    const bool pow2 = (c->n & (c->n - 1)) == 0 && c->n >= 16 && c->n <= 1024;
+    c->fft_own = (pow2 && f && strcmp(f, "own") == 0) ? 1 : 0;
+  }
   c->chunk = ((chunk + sub - 1) / sub) * sub;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
@@ -1540,8 +1721,32 @@ int spi_bp_flush(spi_ctx* c) {
   return 0;
 }
 
+// Twiddles of the own R2C: W_n^t = e^(-2 pi i t / n), t < n/2, computed in FP64.
+static int ensure_fft_twiddles(spi_ctx* c) {
+  const int n = c->n, h = n / 2;
+  if (c->fft_tw.p && c->fft_tw.bytes >= (size_t)h * sizeof(float2)) return 0;
+  std::vector<float2> tw(h);
+  for (int t = 0; t < h; ++t) {
+    const double a = -2.0 * M_PI * (double)t / (double)n;
+    tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  SPI_TRY(c->fft_tw.ensure((size_t)h * sizeof(float2)));
+  SPI_CUDA(cudaMemcpy(c->fft_tw.p, tw.data(), (size_t)h * sizeof(float2), cudaMemcpyHostToDevice));
+  static std::mutex mu;
+  static unsigned long long done = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  const unsigned long long bit = 1ull << (c->device & 63);
+  if (!(done & bit)) {   // the column pass holds 16 columns of up to 1,024 points
+    SPI_CUDA(cudaFuncSetAttribute(colfft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((512 + kColTile * 1025) * sizeof(float2))));
+    done |= bit;
+  }
+  return 0;
+}
+
 static int ensure_chunk_buffers(spi_ctx* c) {
   const int nx = c->nx, n = c->n;
+  if (c->fft_own) SPI_TRY(ensure_fft_twiddles(c));
   SPI_TRY(c->imgs.ensure((size_t)c->chunk * nx * nx * sizeof(float)));
   SPI_TRY(c->padded.ensure((size_t)c->sub * n * n * sizeof(float)));
   const size_t plane = (size_t)n * (nx + 1);
@@ -1857,13 +2062,24 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
           c->phase_end(ev);
           src = dst;
         }
-        // the last piece also zero-pads the unused tail of the FFT batch
-        const int blocks = last ? c->sub - (p0 - b0) : np;
-        const int parts = std::max(1, std::min(8, (4 * c->sm_count + blocks - 1) / std::max(blocks, 1)));
         int ev = c->phase_begin(0);
-        stage_kernel<<<dim3(blocks, parts), 256, 0, c->stream>>>(src, nx, n, ip, np, klp,
-                                                                 c->padded.as<float>() + (size_t)(p0 - b0) * n * n);
-        SPI_TRY(check_kernel("stage_kernel"));
+        if (c->fft_own) {
+          // pass 1 of the own R2C: staged rows transformed into padded, used as
+          // the row-spectrum buffer (n*n/2 complex slots per image)
+          const int parts = std::max(1, std::min(8, (4 * c->sm_count + np - 1) / std::max(np, 1)));
+          const size_t smem = (size_t)(n / 2) * 5 * sizeof(float2);
+          stage_rowfft_kernel<<<dim3(np, parts), 256, smem, c->stream>>>(
+              src, nx, n, ip, np, klp, c->fft_tw.as<float2>(),
+              c->padded.as<float2>() + (size_t)(p0 - b0) * n * n / 2, (size_t)n * n / 2);
+          SPI_TRY(check_kernel("stage_rowfft_kernel"));
+        } else {
+          // the last piece also zero-pads the unused tail of the FFT batch
+          const int blocks = last ? c->sub - (p0 - b0) : np;
+          const int parts = std::max(1, std::min(8, (4 * c->sm_count + blocks - 1) / std::max(blocks, 1)));
+          stage_kernel<<<dim3(blocks, parts), 256, 0, c->stream>>>(src, nx, n, ip, np, klp,
+                                                                   c->padded.as<float>() + (size_t)(p0 - b0) * n * n);
+          SPI_TRY(check_kernel("stage_kernel"));
+        }
         c->phase_end(ev);
         c->count();
       }
@@ -1871,7 +2087,16 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
       done_valid[bi] = 1;
       float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + (size_t)b0 * spec_plane;
       int ev = c->phase_begin(1);
-      SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      if (c->fft_own) {   // pass 2: the columns of the valid images
+        const int tiles = (n / 2 + 1 + kColTile - 1) / kColTile;
+        const size_t smem = ((size_t)(n / 2) + (size_t)kColTile * (n + 1)) * sizeof(float2);
+        colfft_kernel<<<nvalid * tiles, 256, smem, c->stream>>>(c->padded.as<float2>(), (size_t)n * n / 2, nx, n, ip,
+                                                                 nvalid, c->fft_tw.as<float2>(), fout);
+        SPI_TRY(check_kernel("colfft_kernel"));
+        c->count();
+      } else {
+        SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      }
       c->phase_end(ev);
       if (c->bf16) {
         const size_t cnt = (size_t)nvalid * spec_plane;

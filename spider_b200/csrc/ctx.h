@@ -69,6 +69,8 @@ struct spi_ctx {
   spi::HostBuf hslices;
   cufftHandle plan2d = 0;
   int plan2d_n = 0, plan2d_batch = 0;
+  int fft_own = 0;                    // 1 = the library's own two-pass R2C (power-of-two n), 0 = cuFFT
+  spi::DevBuf fft_tw;                 // float2 W_n^t, t < n/2 (FP64-computed twiddles of the own R2C)
   cufftHandle plan3d = 0;
   int plan3d_n = 0;
 

@@ -358,3 +358,29 @@ def test_accumulation_modes_and_flush(ctx, orc):
         assert e.value.code == 101
     finally:
         ctx.set_accumulation(True, 0)
+
+
+def test_own_r2c_matches_cufft_path(ctx, orc):
+    """The library's own two-pass R2C (SPI_FFT=own: staging fused with the row
+    transforms, then the column transforms; power-of-two padded sizes) gives
+    the volumes of the staging + cuFFT path and of the oracle, host and
+    device images, BF16 spectra too."""
+    import torch
+    for nx, nimg in ((32, 200), (64, 150)):
+        _, pr, ang = _case(nx, nimg, 600 + nx)
+        half = synth.half_mask(nimg, np.random.default_rng(601))
+        ref = orc.bp32f(pr, ang, half, prec=1)
+        base = ops.bp32f(pr, ang, half, ctx=ctx)
+        os.environ["SPI_FFT"] = "own"
+        try:
+            own = ops.bp32f(pr, ang, half, ctx=ctx)
+            own_dev = ops.bp32f(torch.from_numpy(pr).cuda(), ang, half, ctx=ctx)
+            own16 = ops.bp32f(pr, ang, half, ctx=ctx, bf16=True)
+        finally:
+            del os.environ["SPI_FFT"]
+        for a, b, c, d, r in zip(own, own_dev, base, own16, ref):
+            assert synth.rel_l2(a, r) <= TOL
+            assert synth.rel_l2(b, r) <= TOL
+            assert synth.rel_l2(a, c) <= TOL
+            assert synth.rel_l2(d, r) <= 5e-4
+
