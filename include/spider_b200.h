@@ -311,6 +311,9 @@ int spi_fslice_normal(const spi_fslice_plan* plan, const float* grid_in, float l
  * that many digits. */
 int spi_fslice_normal64(const spi_fslice_plan* plan, const double* grid_in, double lam, double* grid_out,
                         void* stream);
+/* slices = E grid on FP64 arrays (FP64 sums of the same taps; an exact
+ * reference for gradient checks of the FP32 extraction). */
+int spi_fslice_forward64(const spi_fslice_plan* plan, const double* grid, double* slices, void* stream);
 /* grid = E^T slices into an FP64 grid (FP64 scatter; the CG's right-hand side). */
 int spi_fslice_adjoint64(const spi_fslice_plan* plan, const float* slices, double* grid, void* stream);
 /* Real-space volume float[nx^3] of a grid of spectrum coefficients: the grid

@@ -67,6 +67,7 @@ SIGNATURES = [
     ("spi_fslice_normal", ctypes.c_int, [_vp, _vp, ctypes.c_float, _vp, _vp]),
     ("spi_fslice_normal64", ctypes.c_int, [_vp, _vp, ctypes.c_double, _vp, _vp]),
     ("spi_fslice_adjoint64", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("spi_fslice_forward64", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_volume", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("spi_fslice_plan_destroy", ctypes.c_int, [_vp]),
     ("spi_pj3q_plan_forward", ctypes.c_int, [_vp, _vp, _vp, _vp]),

@@ -176,6 +176,18 @@ class FourierSlicePlan:
                                               ctypes.c_void_p(out.data_ptr()), self._stream()))
         return out
 
+    def forward64(self, grid: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """E on an FP64 grid into FP64 slices (FP64 sums of the same taps)."""
+        import ctypes
+        if out is None:
+            out = torch.empty(self.range_shape, dtype=torch.float64, device=self.device)
+        for t in (grid, out):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ops.SpiderError(101, "forward64 needs contiguous float64 CUDA tensors")
+        ops.check(self._L.spi_fslice_forward64(self._h, ctypes.c_void_p(grid.data_ptr()),
+                                               ctypes.c_void_p(out.data_ptr()), self._stream()))
+        return out
+
     def adjoint64(self, slices: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
         """E^T slices into an FP64 grid (FP64 scatter): the CG's right-hand side."""
         import ctypes

@@ -303,6 +303,46 @@ __global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restr
   }
 }
 
+// Extraction E on an FP64 grid into FP64 slices (FP64 sums of the same taps):
+// an exact reference of the FP32 extraction for gradient checks.
+__global__ void __launch_bounds__(256) fs_extract64_kernel(const double2* __restrict__ in, double2* __restrict__ out,
+                                                           const FsDesc* __restrict__ slices, int nslices, int nx,
+                                                           const float* __restrict__ kbtab, float fltb) {
+  extern __shared__ float tab[];
+  for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
+  __syncthreads();
+  const int N = 2 * nx, NN4 = N * N / 4;
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3, gl = lane & ~3;
+  const long long nitems = (long long)nslices * N;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < nitems;
+       item += warps) {
+    const int s = (int)(item / N);
+    const int J = (int)(item % N) - nx + 1;
+    const FsDesc sd = slices[s];
+    const int JP = (J >= 0) ? J : N + J;
+    const size_t srow = ((size_t)sd.img * N + JP) * (size_t)(nx + 1);
+    int I0 = 0;
+    for (; I0 <= nx && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+      const int I = I0 + g;
+      FsWin w;
+      fs_window(sd, I, J, nx, tab, fltb, q, gl, w);
+      double2 v = fs_gather64(in, w, q, nx);
+      v.x = __dadd_rn(v.x, __shfl_xor_sync(0xffffffffu, v.x, 1));
+      v.y = __dadd_rn(v.y, __shfl_xor_sync(0xffffffffu, v.y, 1));
+      v.x = __dadd_rn(v.x, __shfl_xor_sync(0xffffffffu, v.x, 2));
+      v.y = __dadd_rn(v.y, __shfl_xor_sync(0xffffffffu, v.y, 2));
+      if (q == 0 && I <= nx) {
+        double2 t = make_double2(0.0, 0.0);
+        if (I * I + J * J < NN4 && !(I == 0 && J < 0)) t = w.flipped ? v : make_double2(v.x, -v.y);
+        out[srow + I] = t;
+      }
+    }
+    for (int I = I0 + lane; I <= nx; I += 32) out[srow + I] = make_double2(0.0, 0.0);
+  }
+}
+
 __global__ void fs_scale64_kernel(const double2* __restrict__ p, double lam, double2* __restrict__ q, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double2 v = p[i];
@@ -547,6 +587,17 @@ int spi_fslice_normal64(const spi_fslice_plan* p, const double* grid_in, double 
                                                               p->nx, p->tab, p->fltb);
   SPI_TRY(check_kernel("fs_normal64_kernel"));
   p->ctx->count(2);
+  return 0;
+}
+
+int spi_fslice_forward64(const spi_fslice_plan* p, const double* grid, double* slices, void* stream) {
+  if (!p || !grid || !slices) return fail(kInvalid, "spi_fslice_forward64: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  fs_extract64_kernel<<<fs_blocks(p), 256, kFsSmem, s>>>(reinterpret_cast<const double2*>(grid),
+                                                         reinterpret_cast<double2*>(slices), p->sl, p->nang, p->nx,
+                                                         p->tab, p->fltb);
+  SPI_TRY(check_kernel("fs_extract64_kernel"));
+  p->ctx->count();
   return 0;
 }
 

@@ -170,8 +170,9 @@ def test_config3_fourier_slice_gradient_128(ctx, orc):
     """The differentiable FourierSlice at configuration 3's box (128^3, 2,000
     slices): the backward (the insertion E^T) against the FP64 oracle
     insertion of the same upstream gradient, and against central finite
-    differences (h = 1e-3) of the forward on 64 random voxels (real and
-    imaginary parts), the loss summed in FP64."""
+    differences (h = 1e-3) on 64 random voxels (real and imaginary parts) of
+    the loss through the FP64 extraction (the same taps summed in FP64, so
+    the differences carry no FP32 rounding of the forward)."""
     import torch
     from spider_b200 import autograd
     rng = np.random.default_rng(3003)
@@ -194,14 +195,15 @@ def test_config3_fourier_slice_gradient_128(ctx, orc):
         h = 1e-3
         scale = np.abs(exact).max()
         worst = 0.0
-        x0 = xt.detach()
+        x0 = xt.detach().double()
+        g64 = gt.double()
         for k, (a, b, c) in enumerate(picks):
             comp = k % 2
             xp_, xm_ = x0.clone(), x0.clone()
             xp_[a, b, c, comp] += h
             xm_[a, b, c, comp] -= h
-            lp = float((plan.forward(xp_).double() * gt.double()).sum())
-            lm = float((plan.forward(xm_).double() * gt.double()).sum())
+            lp = float((plan.forward64(xp_) * g64).sum())
+            lm = float((plan.forward64(xm_) * g64).sum())
             fd = (lp - lm) / (2 * h)
             g = grad[a, b, c].real if comp == 0 else grad[a, b, c].imag
             worst = max(worst, abs(g - fd) / max(abs(fd), 1e-3 * scale))
@@ -210,4 +212,4 @@ def test_config3_fourier_slice_gradient_128(ctx, orc):
     print(f"config 3 gradient at 128^3: backward vs FP64 oracle insertion {e:.2e}; "
           f"finite differences, worst relative gap {worst:.2e}")
     assert e <= 1e-5
-    assert worst <= 1e-3
+    assert worst <= 1e-4
