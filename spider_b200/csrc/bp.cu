@@ -622,7 +622,7 @@ __device__ __forceinline__ float kb_tap_cut(const float* tab, float v, int k, fl
 
 // One row J of one slice, eight pixels at a time, as described above: the
 // body of insert_x4_kernel and insert_mc_kernel.
-template <bool BF16, int CUT = 0, bool I32 = false>
+template <bool BF16, int CUT = 0>
 __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, const SliceDesc& sd, float4* __restrict__ G,
                                               int J, int nx, const float* tab, float fltb, int g, int q, int gl) {
   // CUT > 0: the table holds entries 0..CUT-1 only (see kb_tap_cut)
@@ -679,53 +679,27 @@ __device__ __forceinline__ void insert_row_x4(const void* __restrict__ spec, con
     const bool refl = ixp < 0;
     const float bis = refl ? -bi : bi;
     const int ixa = refl ? -ixp : ixp;
-    if (I32) {
-      // the four plane and four row offsets of the window once per pixel, in
-      // 32 bits (a grid index stays below 2^30 up to nx = 512)
-      unsigned zoff[4], yoff[4];
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const int izp = zs + l, iyp = ys + l;
-        const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
+    for (int lz = 0; lz < 4; ++lz) {
+      if (tz[lz] == 0.0f) continue;
+      const int izp = zs + lz;
+      const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
+#pragma unroll
+      for (int ly = 0; ly < 4; ++ly) {
+        const float tyz = __fmul_rn(ty[ly], tz[lz]);
+        if (tyz == 0.0f) continue;
+        const int iyp = ys + ly;
         const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
-        zoff[l] = (unsigned)iza * (unsigned)(N * (nx + 1));
-        yoff[l] = (unsigned)iya * (unsigned)(nx + 1) + (unsigned)ixa;
-      }
-#pragma unroll
-      for (int lz = 0; lz < 4; ++lz) {
-        if (tz[lz] == 0.0f) continue;
-#pragma unroll
-        for (int ly = 0; ly < 4; ++ly) {
-          const float tyz = __fmul_rn(ty[ly], tz[lz]);
-          if (tyz == 0.0f) continue;
-          const float wg = __fmul_rn(tx, tyz);
-          if (wg != 0.0f)
-            atomicAdd(G + (zoff[lz] + yoff[ly]), make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
-        }
-      }
-    } else {
-#pragma unroll
-      for (int lz = 0; lz < 4; ++lz) {
-        if (tz[lz] == 0.0f) continue;
-        const int izp = zs + lz;
-        const int iza = refl ? ((izp > 0) ? N - izp : -izp) : ((izp >= 0) ? izp : N + izp);
-#pragma unroll
-        for (int ly = 0; ly < 4; ++ly) {
-          const float tyz = __fmul_rn(ty[ly], tz[lz]);
-          if (tyz == 0.0f) continue;
-          const int iyp = ys + ly;
-          const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
-          const float wg = __fmul_rn(tx, tyz);
-          if (wg != 0.0f)
-            atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
-                      make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
-        }
+        const float wg = __fmul_rn(tx, tyz);
+        if (wg != 0.0f)
+          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
+                    make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
       }
     }
   }
 }
 
-template <bool BF16, bool I32 = false>
+template <bool BF16>
 __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__ spec,
                                                         const SliceDesc* __restrict__ slices, int nslices, int nx,
                                                         const float* __restrict__ kbtab, float fltb,
@@ -750,7 +724,7 @@ __global__ void __launch_bounds__(512) insert_x4_kernel(const void* __restrict__
     const int s = (int)(item / N);
     const int J = (int)(item % N) - nx + 1;  // J = -NX+1 .. NX
     const SliceDesc sd = slices[s];
-    insert_row_x4<BF16, 0, I32>(spec, sd, sd.grid ? g1 : g0, J, nx, tab, fltb, g, q, gl);
+    insert_row_x4<BF16>(spec, sd, sd.grid ? g1 : g0, J, nx, tab, fltb, g, q, gl);
   }
 }
 
@@ -1843,16 +1817,12 @@ static int launch_insert(spi_ctx* c, const SliceDesc* sl, int nslices, float4* g
       SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
       auto* work = c->workctr.as<unsigned long long>();
       SPI_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), c->stream));
-      static const bool i32 = env_int("SPI_INSERT_I32", 0) != 0;
-#define SPI_X4(B, I)                                                                                         \
-  insert_x4_kernel<B, I><<<insert_blocks(c, insert_x4_kernel<B, I>, threads, smem, c->insert_blocks_per_sm), \
-                           threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work)
-      if (i32) {
-        if (c->bf16) SPI_X4(true, true); else SPI_X4(false, true);
-      } else {
-        if (c->bf16) SPI_X4(true, false); else SPI_X4(false, false);
-      }
-#undef SPI_X4
+      if (c->bf16)
+        insert_x4_kernel<true><<<insert_blocks(c, insert_x4_kernel<true>, threads, smem, c->insert_blocks_per_sm),
+                                 threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
+      else
+        insert_x4_kernel<false><<<insert_blocks(c, insert_x4_kernel<false>, threads, smem, c->insert_blocks_per_sm),
+                                  threads, smem, c->stream>>>(spec, sl, nslices, nx, tab, fltb, g0, g1, work);
     } else {
       // row counter of this launch (launches on the library stream are serialised)
       SPI_TRY(c->workctr.ensure(sizeof(unsigned long long)));
@@ -2606,18 +2576,22 @@ int spi_bp_finish(spi_ctx* c, float* vol_all, float* vol_1, float* vol_2, int ou
     if (vol_all) jobs[nj++] = {vol_all, 0, 1};
     if (vol_2) jobs[nj++] = {vol_2, 1, -1};
   }
+  // Host outputs: each volume gets its own staging buffer, and its copy to
+  // the host runs on the second stream while the next volume is computed.
+  if (!out_on_device) {
+    SPI_TRY(c->volbuf.ensure((size_t)std::max(nj, 1) * vbytes));
+    SPI_TRY(ensure_pipeline_events(c, 3));
+  }
   for (int t = 0; t < nj; ++t) {
-    float* dst = jobs[t].out;
-    if (!out_on_device) {
-      SPI_TRY(c->volbuf.ensure(vbytes));
-      dst = c->volbuf.as<float>();
-    }
+    float* dst = out_on_device ? jobs[t].out : c->volbuf.as<float>() + (size_t)t * (vbytes / sizeof(float));
     SPI_TRY(finish_one(c, jobs[t].ga, jobs[t].gb, dst));
     if (!out_on_device) {
-      SPI_CUDA(cudaMemcpyAsync(jobs[t].out, dst, vbytes, cudaMemcpyDeviceToHost, c->stream));
-      SPI_CUDA(cudaStreamSynchronize(c->stream));  // volbuf is reused by the next job
+      SPI_CUDA(cudaEventRecord(c->ev_ready[t], c->stream));
+      SPI_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_ready[t], 0));
+      SPI_CUDA(cudaMemcpyAsync(jobs[t].out, dst, vbytes, cudaMemcpyDeviceToHost, c->stream2));
     }
   }
+  if (!out_on_device) SPI_CUDA(cudaStreamSynchronize(c->stream2));
   SPI_CUDA(cudaStreamSynchronize(c->stream));
   return 0;
 }
