@@ -860,7 +860,7 @@ def _cang_host(a):
                     dtype=np.float32)
 
 
-def multiclass_measure(args, steps=2):
+def multiclass_measure(args, steps=4):
     """Uneven multi-class insertion: K = 8 classes with boxes
     {96,128,160,192,192,224,256,256}, each a 30-80-blob phantom; images
     assigned uniformly at random to the classes, SNR 0.1, uniform SO(3);
@@ -869,7 +869,10 @@ def multiclass_measure(args, steps=2):
     slices, one stream), then finished; open + insertion + finish of all
     classes are timed, images resident on the device; the rate with one context and host thread per class (concurrent
     streams) is given beside it.  Several streams run at once in the second
-    form, so both are timed by the host clock between synchronisations."""
+    form, so both are timed by the host clock between synchronisations.
+    Each pass opens (allocates) and closes (frees) the classes' grids and FFT
+    plans, which varies by up to a second between passes on the same box, so
+    the minimum of four passes is reported."""
     import torch
     from spider_b200 import ops, synth
     _, _, local = dist_env()
@@ -891,7 +894,7 @@ def multiclass_measure(args, steps=2):
     ctx.close()
     torch.cuda.synchronize()
 
-    ctxs = [ops.Context(local) for _ in classes]      # kept across passes: buffers and plans are reused
+    ctxs = [ops.Context(local) for _ in classes]      # kept across passes
 
     def one_pass(one_launch):
         torch.cuda.synchronize()
@@ -913,8 +916,8 @@ def multiclass_measure(args, steps=2):
             "config": {"workload": "multi-class BP 32F, boxes 96,128,160,192,192,224,256,256",
                        "images": args.mc_images, "per_class": [int(c[0].shape[0]) for c in classes],
                        "timing": "host clock around synchronised calls (open, insertion and finish of all eight "
-                                 "classes; the contexts, their buffers and FFT plans are kept across passes), "
-                                 "min over passes",
+                                 "classes; the contexts are kept across passes, and each pass opens and closes "
+                                 f"the classes' grids, buffers and FFT plans), min over {max(steps, 1)} passes",
                        "forms": "value: spi_bp_insert_multi (one insertion launch per round, one stream); "
                                 "threads_value: one context and host thread per class"}}
 

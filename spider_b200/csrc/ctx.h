@@ -22,6 +22,7 @@ struct spi_ctx {
   int insert_mode = 3;                // 0 = tile-privatised, 1 = direct per-tap atomics, 2 = five x-tap lanes,
                                       // 3 = four lanes over the nonzero tap window
   int slice_order = 1;                // 1 = order slices of a chunk by plane normal
+  int line_order = 1;                 // x4 insertion order: 0 rows, 2 columns, 1 per slice (SliceDesc::cols)
   int insert_seg_map = 0;             // 1 = warps take 32-pixel row segments, 0 = whole rows
   int insert_threads = 256;           // threads per insert block
   int insert_blocks_per_sm = 0;       // 0 = as many as fit

@@ -164,19 +164,24 @@ def test_bp3f_config1_full(ctx, orc):
 
 def test_insert_kernels_agree(ctx, orc):
     """The tile-privatised insertion and the direct per-tap insertion add the
-    same taps; they differ only in FP32 summation order."""
+    same taps; they differ only in FP32 summation order.  So do the x4
+    kernel's row-by-row, column-by-column and per-slice insertion orders."""
     nx, nimg = 48, 300
     _, pr, ang = _case(nx, nimg, 61)
     # include orientations that put the x = 0 flip line inside many tiles
     ang[:40, 1] = 90.0
     out, grids = {}, {}
-    for mode in ("direct", "tile", "xlane", "x4", "tilefx"):
-        os.environ["SPI_INSERT"] = mode
+    for mode in ("direct", "tile", "xlane", "x4", "tilefx", "x4:rows", "x4:cols"):
+        kernel, _, order = mode.partition(":")
+        os.environ["SPI_INSERT"] = kernel
+        if order:
+            os.environ["SPI_INSERT_ORDER"] = order
         try:
             out[mode] = ops.bp3f(pr, ang, ctx=ctx)
             grids[mode] = ops.bp3f_partial(pr, ang, ctx=ctx)
         finally:
             del os.environ["SPI_INSERT"]
+            os.environ.pop("SPI_INSERT_ORDER", None)
     ref = orc.bp3f(pr, ang, prec=1, nthreads=1)
     for mode, v in out.items():
         assert synth.rel_l2(v, out["direct"]) <= 2e-6, mode
@@ -207,19 +212,26 @@ def test_rb3f_rb32f_match_oracle(ctx, orc):
     assert synth.rel_l2(z, ops.bp3f(pr, ang, ctx=ctx)) <= 2e-6
 
 
-@pytest.mark.parametrize("mode", ["one_launch", "concurrent", "in_turn"])
+@pytest.mark.parametrize("mode", ["one_launch", "one_launch:cols", "concurrent", "in_turn"])
 def test_bp32f_multiclass(orc, mode):
     """Several classes of different box sizes (one odd, two equal) reconstructed
     from one image stream: all classes in one insertion launch per round
-    (spi_bp_insert_multi), or one context per class inserted concurrently from
-    one host thread each, or in turn."""
+    (spi_bp_insert_multi; also with every slice inserted column by column),
+    or one context per class inserted concurrently from one host thread
+    each, or in turn."""
     classes, refs = [], []
     for k, (nx, nimg) in enumerate(((24, 120), (32, 200), (41, 150), (32, 90))):
         _, pr, ang = _case(nx, nimg, 90 + k, noise=0.5)
         half = synth.half_mask(nimg, np.random.default_rng(95 + k))
         classes.append((pr, ang, half))
         refs.append(orc.bp32f(pr, ang, half, prec=0, nthreads=1))
-    out = ops.bp32f_multiclass(classes, one_launch=mode == "one_launch", concurrent=mode == "concurrent")
+    mode, _, order = mode.partition(":")
+    if order:
+        os.environ["SPI_INSERT_ORDER"] = order
+    try:
+        out = ops.bp32f_multiclass(classes, one_launch=mode == "one_launch", concurrent=mode == "concurrent")
+    finally:
+        os.environ.pop("SPI_INSERT_ORDER", None)
     for got, ref in zip(out, refs):
         for a, b in zip(got, ref):
             assert a.shape == b.shape
