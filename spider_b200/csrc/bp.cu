@@ -623,7 +623,10 @@ __device__ __forceinline__ float kb_tap_cut(const float* tab, float v, int k, fl
 
 // The largest m >= 0 with m * m < rem (rem > 0).
 __device__ __forceinline__ int isqrt_below(int rem) {
-  int m = (int)sqrtf((float)(rem - 1));
+  // approximate square root (no IEEE slow path); the two loops make m exact
+  float f;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(f) : "f"((float)(rem - 1)));
+  int m = (int)f;
   while (m > 0 && m * m >= rem) --m;
   while ((m + 1) * (m + 1) < rem) ++m;
   return m;

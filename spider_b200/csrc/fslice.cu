@@ -21,6 +21,7 @@
 // nonzero window of the table.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -32,7 +33,7 @@ namespace spi {
 struct FsDesc {
   float dm[6];  // DM(1:6) of the slice (CANG, cang.f:44-81)
   int img;      // slice index
-  int pad;
+  int cols;     // order of the insertion and normal kernels: 0 row by row, 1 by half columns
 };
 static_assert(sizeof(FsDesc) == 32, "slice descriptor is 32 bytes");
 
@@ -42,6 +43,44 @@ __device__ __forceinline__ int fs_nint_pos(float v) {  // Fortran NINT, v >= 0
 }
 __device__ __forceinline__ float fs_tap(const float* tab, float v, int k, float fltb) {
   return tab[fs_nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb))];
+}
+
+// Line r (0 <= r < N) of a slice: row J = r - NX + 1 (pixels consecutive in
+// I) or, for a slice marked cols, half of column I = r / 2 (pixels
+// consecutive in J; J >= 0 for even r, J < 0 for odd r).  Pixel k of the line
+// is (i0 + di k, j0 + dj k), k < cnt: the pixels of the line inside the half
+// disc of oneline.f's loops, so every pixel of the slice lies on exactly one
+// line in either order.  The host marks slices as the back-projection does
+// (bp.cu, insert_line_x4): eight pixels stepping along z scatter into eight
+// grid planes 2 MB apart at 256^3.  Only the insertions E^T follow the mark
+// (use_cols): at 256^3 with 8,192 slices it took E^T from 158.6 to 111.7 ms,
+// while the fused normal operators, which gather before they scatter, were
+// 2% slower with it (0.363 against 0.356 s per CG iteration in FP64).
+struct FsLine {
+  int i0, j0, di, dj, cnt;
+};
+__device__ __forceinline__ int fs_isqrt_below(int rem) {   // the largest m >= 0 with m * m < rem (rem > 0)
+  // approximate square root (no IEEE slow path); the two loops make m exact
+  float f;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(f) : "f"((float)(rem - 1)));
+  int m = (int)f;
+  while (m > 0 && m * m >= rem) --m;
+  while ((m + 1) * (m + 1) < rem) ++m;
+  return m;
+}
+__device__ __forceinline__ FsLine fs_line(const FsDesc& sd, int r, int nx, bool use_cols) {
+  const int NN4 = nx * nx;
+  FsLine l;
+  if (!(use_cols && sd.cols)) {
+    l.j0 = r - nx + 1; l.i0 = 0; l.di = 1; l.dj = 0;
+    l.cnt = (l.j0 * l.j0 < NN4) ? fs_isqrt_below(NN4 - l.j0 * l.j0) + 1 : 0;
+  } else {
+    l.i0 = r >> 1; l.di = 0;
+    const int jm = fs_isqrt_below(NN4 - l.i0 * l.i0);
+    if (r & 1) { l.j0 = -1; l.dj = -1; l.cnt = l.i0 == 0 ? 0 : jm; }
+    else { l.j0 = 0; l.dj = 1; l.cnt = jm + 1; }
+  }
+  return l;
 }
 
 // The tap window of pixel (I, J) for lane q of its four-lane group (lanes
@@ -177,16 +216,17 @@ __global__ void __launch_bounds__(256) fs_kernel(const float2* __restrict__ in, 
   for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < nitems;
        item += warps) {
     const int s = (int)(item / N);
-    const int J = (int)(item % N) - nx + 1;
     const FsDesc sd = slices[s];
-    const int JP = (J >= 0) ? J : N + J;
-    const size_t srow = (size_t)sd.img * plane + (size_t)JP * rowlen;
-    int I0 = 0;
-    for (; I0 <= nx && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
-      const int I = I0 + g;
-      FsWin w;
-      fs_window(sd, I, J, nx, tab, fltb, q, gl, w);
-      if (MODE == 0) {
+    if (MODE == 0) {
+      // rows only: every pixel of the row is written, zero outside the disc
+      const int J = (int)(item % N) - nx + 1;
+      const int JP = (J >= 0) ? J : N + J;
+      const size_t srow = (size_t)sd.img * plane + (size_t)JP * rowlen;
+      int I0 = 0;
+      for (; I0 <= nx && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+        const int I = I0 + g;
+        FsWin w;
+        fs_window(sd, I, J, nx, tab, fltb, q, gl, w);
         const float2 acc = group_sum4(fs_gather(in, w, q, nx));
         // BI_adj = acc (conj'ed for a flipped pixel); T = conj(BI_adj)
         if (q == 0 && I <= nx) {
@@ -194,22 +234,31 @@ __global__ void __launch_bounds__(256) fs_kernel(const float2* __restrict__ in, 
           if (I * I + J * J < NN4 && !(I == 0 && J < 0)) t = w.flipped ? acc : make_float2(acc.x, -acc.y);
           out[srow + I] = t;
         }
-      } else if (MODE == 1) {
-        // BTQ = BI = conj(T), or conj(BI) = T for a flipped pixel
-        float2 b = make_float2(0.0f, 0.0f);
-        if (w.ok) {
-          const float2 t = in[srow + I];
-          b = w.flipped ? t : make_float2(t.x, -t.y);
+      }
+      for (int I = I0 + lane; I <= nx; I += 32) out[srow + I] = make_float2(0.0f, 0.0f);
+    } else {
+      const FsLine ln = fs_line(sd, (int)(item % N), nx, MODE == 1);
+      for (int k0 = 0; k0 < ln.cnt; k0 += 8) {   // warp-uniform
+        const int k = k0 + g;
+        const int I = ln.i0 + ln.di * k, J = ln.j0 + ln.dj * k;
+        FsWin w;
+        fs_window(sd, I, J, nx, tab, fltb, q, gl, w);
+        if (MODE == 1) {
+          // BTQ = BI = conj(T), or conj(BI) = T for a flipped pixel
+          float2 b = make_float2(0.0f, 0.0f);
+          if (w.ok) {
+            const int JP = (J >= 0) ? J : N + J;
+            const float2 t = in[(size_t)sd.img * plane + (size_t)JP * rowlen + I];
+            b = w.flipped ? t : make_float2(t.x, -t.y);
+          }
+          fs_scatter(out, w, q, nx, b);
+        } else {
+          // extraction then insertion of the same pixel: the flips cancel
+          const float2 sum = group_sum4(fs_gather(in, w, q, nx));
+          fs_scatter(out, w, q, nx, sum);
         }
-        fs_scatter(out, w, q, nx, b);
-      } else {
-        // extraction then insertion of the same pixel: the flips cancel
-        const float2 sum = group_sum4(fs_gather(in, w, q, nx));
-        fs_scatter(out, w, q, nx, sum);
       }
     }
-    if (MODE == 0)   // the rest of the row lies outside the disk
-      for (int I = I0 + lane; I <= nx; I += 32) out[srow + I] = make_float2(0.0f, 0.0f);
   }
 }
 
@@ -269,7 +318,7 @@ __global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restr
   extern __shared__ float tab[];
   for (int i = threadIdx.x; i < 5000; i += blockDim.x) tab[i] = kbtab[i];
   __syncthreads();
-  const int N = 2 * nx, NN4 = N * N / 4;
+  const int N = 2 * nx;
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, q = lane & 3, gl = lane & ~3;
   const long long nitems = (long long)nslices * N;
@@ -277,13 +326,13 @@ __global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restr
   for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < nitems;
        item += warps) {
     const int s = (int)(item / N);
-    const int J = (int)(item % N) - nx + 1;
     const FsDesc sd = slices[s];
-    const int JP = (J >= 0) ? J : N + J;
-    const size_t srow = ((size_t)sd.img * N + JP) * (size_t)(nx + 1);
-    for (int I0 = 0; I0 <= nx && I0 * I0 + J * J < NN4; I0 += 8) {   // warp-uniform
+    const FsLine ln = fs_line(sd, (int)(item % N), nx, !NORMAL);
+    for (int k0 = 0; k0 < ln.cnt; k0 += 8) {   // warp-uniform
+      const int k = k0 + g;
+      const int I = ln.i0 + ln.di * k, J = ln.j0 + ln.dj * k;
       FsWin w;
-      fs_window(sd, I0 + g, J, nx, tab, fltb, q, gl, w);
+      fs_window(sd, I, J, nx, tab, fltb, q, gl, w);
       double2 v;
       if (NORMAL) {
         v = fs_gather64(in, w, q, nx);
@@ -294,7 +343,8 @@ __global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restr
       } else {   // BTQ = BI = conj(T), or T for a flipped pixel
         v = make_double2(0.0, 0.0);
         if (w.ok) {
-          const float2 t = sl_in[srow + I0 + g];
+          const int JP = (J >= 0) ? J : N + J;
+          const float2 t = sl_in[((size_t)sd.img * N + JP) * (size_t)(nx + 1) + I];
           v = make_double2((double)t.x, w.flipped ? (double)t.y : -(double)t.y);
         }
       }
@@ -452,12 +502,16 @@ int spi_fslice_plan_create(spi_ctx* ctx, int nx, const float* angles, int nang, 
                               "nonzero taps per axis", nx);
   }
   std::vector<FsDesc> hs(nang);
+  const char* ord = std::getenv("SPI_INSERT_ORDER");
+  const int order = !ord ? 1 : std::strcmp(ord, "rows") == 0 ? 0 : std::strcmp(ord, "cols") == 0 ? 2 : 1;
   for (int a = 0; a < nang; ++a) {
     float dm[9];
     cang(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dm);   // BUILDM1 (bp3f.f:1287)
     std::memcpy(hs[a].dm, dm, 6 * sizeof(float));
     hs[a].img = a;
-    hs[a].pad = 0;
+    // insertion order (FsLine): the in-plane axis with the smaller z
+    // component, for boxes above 192 (as the back-projection chooses)
+    hs[a].cols = (order == 2 || (order == 1 && nx > 192 && std::fabs(dm[5]) < std::fabs(dm[2]))) ? 1 : 0;
   }
   std::vector<float> wkb;
   windkb_table(nx, kb, wkb);
