@@ -377,14 +377,19 @@ __global__ void __launch_bounds__(128) wpro_adjoint_kernel(const float* __restri
 __global__ void __launch_bounds__(128) wpro_adjoint4_kernel(const float* __restrict__ proj, int nsam, int nrow,
                                                             int nslice, const PjRun* __restrict__ runs, int nruns,
                                                             const PjDM* __restrict__ dms, int nang, int ldpx,
-                                                            int ldpy, int ldpz, int zlo, int zhi,
+                                                            int ldpy, int ldpz, int zlo, int zhi, int order,
                                                             float4* __restrict__ q4) {
   const long long total = (long long)nruns * nang;
   const size_t sy = (size_t)nsam, sz = (size_t)nsam * nrow;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int a = (int)(t / nruns);
-    const PjRun r = runs[t % nruns];
     const PjDM dm = dms[a];
+    // neighbouring threads take neighbouring runs: in (z, y) order their
+    // walks lie DM(4:6) apart in the volume, in (y, z) order DM(7:9) apart
+    bool yz = order == 3;
+    if (order == 1) yz = fabsf(dm.d[6]) > fabsf(dm.d[3]);        // the larger x component
+    else if (order == 2) yz = fabsf(dm.d[8]) < fabsf(dm.d[5]);   // the smaller z component
+    const PjRun r = runs[(yz ? nruns : 0) + t % nruns];
     const float* b = proj + (size_t)a * nsam * nrow;
     const int k = r.y + ldpy;
     float xb = run_start(r, dm.d[0], dm.d[3], dm.d[6], ldpx);
@@ -477,10 +482,15 @@ int pj_common(spi_ctx* c, int nx, int ny, int nz, float ri, const float* angles,
   std::vector<PjDM> dms((size_t)std::max(nang, 1));
   for (int a = 0; a < nang; ++a)  // WPRO_N(PHI=reg3, THETA=reg2, PSI=reg1), writpro_n.f:214-216
     cang_pj(angles[3 * a + 2], angles[3 * a + 1], angles[3 * a + 0], dms[a].d);
-  SPI_TRY(c->pj_runs.ensure(std::max<size_t>(1, runs.size()) * sizeof(PjRun)));
+  // the runs twice: PREPCUB's (z, y) order, then (y, z) order (adjoint lanes, see pj_adjoint)
+  std::vector<PjRun> both(runs);
+  both.insert(both.end(), runs.begin(), runs.end());
+  std::stable_sort(both.begin() + runs.size(), both.end(),
+                   [](const PjRun& u, const PjRun& v) { return u.y != v.y ? u.y < v.y : u.z < v.z; });
+  SPI_TRY(c->pj_runs.ensure(std::max<size_t>(1, both.size()) * sizeof(PjRun)));
   SPI_TRY(c->pj_dm.ensure(dms.size() * sizeof(PjDM)));
-  if (!runs.empty())
-    SPI_CUDA(cudaMemcpyAsync(c->pj_runs.p, runs.data(), runs.size() * sizeof(PjRun), cudaMemcpyHostToDevice, c->stream));
+  if (!both.empty())
+    SPI_CUDA(cudaMemcpyAsync(c->pj_runs.p, both.data(), both.size() * sizeof(PjRun), cudaMemcpyHostToDevice, c->stream));
   SPI_CUDA(cudaMemcpyAsync(c->pj_dm.p, dms.data(), dms.size() * sizeof(PjDM), cudaMemcpyHostToDevice, c->stream));
   std::vector<PjRun> rowruns;
   std::vector<std::array<int, 4>> tasks;
@@ -565,6 +575,14 @@ static int pj_forward(spi_ctx* c, cudaStream_t st, const float* vol, int form, f
 // scalar atomics into vol.  Plans of 1,000 (192^3) and 500 (256^3)
 // projections: 30.6k and 12.7k projections/s in slabs (2 and 5), against
 // 13.1k and 5.6k with scalar atomics; at 128^3 one slab, 112k against 43k.
+// Order of the runs among the adjoint's threads (SPI_PJ_ADJ_ORDER): 0 (z, y),
+// 3 (y, z), 1 per projection the one whose neighbouring walks differ more
+// in x, 2 per projection the one whose neighbouring walks differ less in z.
+static int env_order() {
+  const char* e = std::getenv("SPI_PJ_ADJ_ORDER");
+  return e ? std::atoi(e) : 1;
+}
+
 static int pj_adjoint(spi_ctx* c, cudaStream_t st, const float* projs, float4* q4, int nx, int ny, int nz,
                       const PjRun* runs, int nruns, const PjDM* dms, int nang, float* vol) {
   const size_t nvox = (size_t)nx * ny * nz;
@@ -583,12 +601,13 @@ static int pj_adjoint(spi_ctx* c, cudaStream_t st, const float* projs, float4* q
     return 0;
   }
   SPI_CUDA(cudaMemsetAsync(q4, 0, nvox * sizeof(float4), st));
+  static const int adj_order = env_order();
   // cells have IOZ = 1 .. nz-1; S slabs of T planes each
   const int S = (int)std::max<size_t>(1, (nvox * sizeof(float4) + kSlabBytes - 1) / kSlabBytes);
   const int T = (nz - 1 + S - 1) / S;
   for (int zlo = 1; zlo < nz; zlo += T) {
     wpro_adjoint4_kernel<<<blocks, 128, 0, st>>>(projs, nx, ny, nz, runs, nruns, dms, nang, ldpx, ldpy, ldpz, zlo,
-                                                 std::min(nz, zlo + T), q4);
+                                                 std::min(nz, zlo + T), adj_order, q4);
     SPI_TRY(check_kernel("wpro_adjoint4_kernel"));
     c->count();
   }
@@ -678,7 +697,7 @@ struct spi_pj3q_plan {
   spi_ctx* ctx = nullptr;
   int device = 0, nx = 0, ny = 0, nz = 0, nang = 0, nruns = 0, ntasks = 0, form = 0;
   float ri = 0.0f;
-  PjRun* runs = nullptr;
+  PjRun* runs = nullptr;  // 2 x nruns: (z, y) order, then (y, z) order
   void* rows = nullptr;   // runs in (y, |z|) order, then the row tasks (forward)
   PjDM* dms = nullptr;
   float4* v4 = nullptr;   // packed volume of the forward projection (quads or cells, by form)
@@ -703,14 +722,14 @@ int spi_pj3q_plan_create(spi_ctx* c, int nx, int ny, int nz, float ri, const flo
   p->device = c->device;
   p->nx = nx; p->ny = ny; p->nz = nz; p->nang = nang; p->nruns = nruns; p->ntasks = ntasks; p->ri = ri;
   const size_t rows_bytes = pj_tasks_offset(nruns) + std::max(1, ntasks) * sizeof(int4);
-  cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, nruns) * sizeof(PjRun));
+  cudaError_t e = cudaMalloc(&p->runs, std::max<size_t>(1, 2 * (size_t)nruns) * sizeof(PjRun));
   if (e == cudaSuccess) e = cudaMalloc(&p->dms, (size_t)nang * sizeof(PjDM));
   if (e == cudaSuccess) e = cudaMalloc(&p->rows, rows_bytes);
   p->form = nruns ? form : kPjPlain;
   if (e == cudaSuccess && p->form != kPjPlain) e = cudaMalloc(&p->v4, pj_packed_bytes(p->form, nvox));
   if (e == cudaSuccess && nruns && nvox * sizeof(float4) <= quad_fwd_max()) e = cudaMalloc(&p->q4, nvox * sizeof(float4));
   if (e == cudaSuccess && nruns)
-    e = cudaMemcpyAsync(p->runs, c->pj_runs.p, (size_t)nruns * sizeof(PjRun), cudaMemcpyDeviceToDevice, c->stream);
+    e = cudaMemcpyAsync(p->runs, c->pj_runs.p, 2 * (size_t)nruns * sizeof(PjRun), cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(p->dms, c->pj_dm.p, (size_t)nang * sizeof(PjDM), cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess && nruns)
