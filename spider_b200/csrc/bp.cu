@@ -363,11 +363,13 @@ __global__ void to_bf16_kernel(const float2* __restrict__ in, __nv_bfloat162* __
 
 template <bool BF16>
 __device__ __forceinline__ float2 load_spec(const void* spec, size_t q) {
+  // read-only during the insertion: non-coherent global loads (the
+  // multi-class kernel's spectrum pointers come from shared memory)
   if (BF16) {
-    __nv_bfloat162 v = static_cast<const __nv_bfloat162*>(spec)[q];
+    __nv_bfloat162 v = __ldg(static_cast<const __nv_bfloat162*>(spec) + q);
     return make_float2(__low2float(v), __high2float(v));
   } else {
-    return static_cast<const float2*>(spec)[q];
+    return __ldg(static_cast<const float2*>(spec) + q);
   }
 }
 
@@ -621,6 +623,17 @@ __device__ __forceinline__ float kb_tap_cut(const float* tab, float v, int k, fl
   return tab[min(nint_pos(__fmul_rn(fabsf(__fsub_rn(v, (float)k)), fltb)), last)];
 }
 
+// G[i] += v as one 16-byte reduction in L2 (red.global.add.v4.f32).  The
+// address is converted to the global window explicitly: the multi-class
+// kernel takes its grid pointers from shared memory, and on such a generic
+// pointer atomicAdd(float4*) was not compiled to the vector reduction
+// (measured: 1.9x the instructions and no L2 reduction requests; 205
+// against 156 ms for the same 10,000 images at 256^3).
+__device__ __forceinline__ void red_add_v4(float4* p, float4 v) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(__cvta_generic_to_global(p)), "f"(v.x),
+               "f"(v.y), "f"(v.z), "f"(v.w));
+}
+
 // The largest m >= 0 with m * m < rem (rem > 0).
 __device__ __forceinline__ int isqrt_below(int rem) {
   // approximate square root (no IEEE slow path); the two loops make m exact
@@ -726,8 +739,8 @@ __device__ __forceinline__ void insert_line_x4(const void* __restrict__ spec, co
         const int iya = refl ? ((iyp > 0) ? N - iyp : -iyp) : ((iyp >= 0) ? iyp : N + iyp);
         const float wg = __fmul_rn(tx, tyz);
         if (wg != 0.0f)
-          atomicAdd(G + ((size_t)iza * N + iya) * rowlen + ixa,
-                    make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
+          red_add_v4(G + ((size_t)iza * N + iya) * rowlen + ixa,
+                     make_float4(__fmul_rn(br, wg), __fmul_rn(bis, wg), wg, 0.0f));
       }
     }
   }
@@ -808,8 +821,7 @@ __global__ void __launch_bounds__(512) insert_mc_kernel(const McClass* __restric
     const McClass& C = sc[c];
     const int N = 2 * C.nx;
     const long long local = item - C.item0;
-    const int s = (int)(local / N);
-    const SliceDesc sd = C.slices[s];
+    const SliceDesc sd = C.slices[local / N];
     insert_line_x4<BF16, kMcTab>(C.spec, sd, sd.grid ? C.g1 : C.g0, (int)(local % N), C.nx, tab + kMcTab * C.tab,
                                  sfl[C.tab], g, q, gl);
   }
