@@ -754,6 +754,18 @@ def run_ours(args):
             ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                             ctypes.c_void_p(grids[1].data_ptr())))
         hvol = [torch.empty((nx, nx, nx), dtype=torch.float32).pin_memory() for _ in range(3)]
+        # this box's pinned host-to-device bandwidth (the e2e rate depends on it)
+        probe = torch.empty_like(host_chunks[0], device=dev)
+        probe.copy_(host_chunks[0], non_blocking=True)
+        torch.cuda.synchronize()
+        h0 = torch.cuda.Event(enable_timing=True)
+        h1 = torch.cuda.Event(enable_timing=True)
+        h0.record()
+        probe.copy_(host_chunks[0], non_blocking=True)
+        h1.record()
+        h1.synchronize()
+        h2d_gbs = host_chunks[0].numel() * 4 / (h0.elapsed_time(h1) / 1e3) / 1e9
+        del probe
         # reopening at the same size zeroes the grids and keeps every buffer
         ctx.bp_open(nx, 2, bf16=args.bf16)
         ctx.bp_autotune()                   # cached choice
@@ -789,6 +801,7 @@ def run_ours(args):
         e2e = {"value": world * chunk * args.steps / (te / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": chunk * nx * nx * 4 + chunk * (12 + 1),
                "d2h_bytes_per_step": 3 * nx ** 3 * 4 / args.steps,
+               "h2d_gbs": h2d_gbs,
                "note": "spi_bp_insert on pinned host images per step, then one spi_bp_finish "
                        "to three host volumes; device-timed on the library stream"}
     ctx.bp_close()
