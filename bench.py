@@ -773,37 +773,50 @@ def run_ours(args):
             ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
                                       angles[i].ctypes.data_as(ctypes.c_void_p),
                                       halves[i].ctypes.data_as(ctypes.c_void_p), 0))
-        ctx.bp_open(nx, 2, bf16=args.bf16)
-        ctx.bp_autotune()
-        barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for i in range(args.warmup, nsteps):
-            ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
-                                      angles[i].ctypes.data_as(ctypes.c_void_p),
-                                      halves[i].ctypes.data_as(ctypes.c_void_p), 0))
-        if world > 1:
-            import torch.distributed as dist
-            ctx.bp_flush()             # the last insertions and folds are done on the library stream
-            for g in grids:
-                dist.all_reduce(g)
+
+        def e2e_pass():
+            ctx.bp_open(nx, 2, bf16=args.bf16)
+            ctx.bp_autotune()
+            barrier()
             torch.cuda.synchronize()
-        ops.check(L.spi_bp_finish(ctx.handle, ctypes.c_void_p(hvol[0].data_ptr()), ctypes.c_void_p(hvol[1].data_ptr()),
-                                  ctypes.c_void_p(hvol[2].data_ptr()), 0))
-        e1.record(stream)
-        e1.synchronize()
-        te = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([te], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+            th0 = time.perf_counter()
+            e0.record(stream)
+            for i in range(args.warmup, nsteps):
+                ops.check(L.spi_bp_insert(ctx.handle, ctypes.c_void_p(host_chunks[i % 2].data_ptr()), chunk,
+                                          angles[i].ctypes.data_as(ctypes.c_void_p),
+                                          halves[i].ctypes.data_as(ctypes.c_void_p), 0))
+            if world > 1:
+                import torch.distributed as dist
+                ctx.bp_flush()             # the last insertions and folds are done on the library stream
+                for g in grids:
+                    dist.all_reduce(g)
+                torch.cuda.synchronize()
+            ops.check(L.spi_bp_finish(ctx.handle, ctypes.c_void_p(hvol[0].data_ptr()),
+                                      ctypes.c_void_p(hvol[1].data_ptr()), ctypes.c_void_p(hvol[2].data_ptr()), 0))
+            e1.record(stream)
+            e1.synchronize()
+            th = (time.perf_counter() - th0) * 1e3
+            te = e0.elapsed_time(e1)
+            if world > 1:
+                import torch.distributed as dist
+                t = torch.tensor([te], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                te = float(t.item())
+            return te, th
+
+        # The same timed pass three times (each a fresh reconstruction of
+        # the same K steps): single passes of identical code on the same box
+        # were seen to vary by 20% (387 against 472 ms) with the box's H2D
+        # bandwidth unchanged, so the median pass is reported.
+        passes = [e2e_pass() for _ in range(3)]
+        te, th = sorted(passes)[1]
         e2e = {"value": world * chunk * args.steps / (te / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": chunk * nx * nx * 4 + chunk * (12 + 1),
                "d2h_bytes_per_step": 3 * nx ** 3 * 4 / args.steps,
-               "h2d_gbs": h2d_gbs,
+               "h2d_gbs": h2d_gbs, "host_clock_ms": th, "event_ms": te,
+               "passes_ms": [p[0] for p in passes],
                "note": "spi_bp_insert on pinned host images per step, then one spi_bp_finish "
-                       "to three host volumes; device-timed on the library stream"}
+                       "to three host volumes; device-timed on the library stream; median of three passes"}
     ctx.bp_close()
 
     cg = None
