@@ -601,7 +601,7 @@ static int pj_adjoint(spi_ctx* c, cudaStream_t st, const float* projs, float4* q
     return 0;
   }
   SPI_CUDA(cudaMemsetAsync(q4, 0, nvox * sizeof(float4), st));
-  static const int adj_order = env_order();
+  const int adj_order = env_order();
   // cells have IOZ = 1 .. nz-1; S slabs of T planes each
   const int S = (int)std::max<size_t>(1, (nvox * sizeof(float4) + kSlabBytes - 1) / kSlabBytes);
   const int T = (nz - 1 + S - 1) / S;

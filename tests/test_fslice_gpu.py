@@ -29,9 +29,13 @@ def _real(z):
     return torch.tensor(np.stack([z.real, z.imag], -1), dtype=torch.float32, device="cuda").contiguous()
 
 
-@pytest.mark.parametrize("nx", [24, 33])
-def test_fslice_operators_match_oracle(ctx, orc, nx):
+@pytest.mark.parametrize("nx,order", [(24, None), (33, None), (24, "cols")])
+def test_fslice_operators_match_oracle(ctx, orc, nx, order, monkeypatch):
+    """order "cols": the insertions E^T walk every slice by half columns (the
+    order boxes above 192 take per slice); the result is the same."""
     from spider_b200 import autograd
+    if order:
+        monkeypatch.setenv("SPI_INSERT_ORDER", order)
     rng = np.random.default_rng(300 + nx)
     n = 2 * nx
     ang = synth.so3_angles(40, rng)

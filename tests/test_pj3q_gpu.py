@@ -53,6 +53,27 @@ def test_pj3q_adjoint_exact(ctx):
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs))
 
 
+def test_pj3q_adjoint_run_orders(ctx, monkeypatch):
+    """The adjoint's threads take the runs in (z, y) order, (y, z) order or
+    per projection the one whose neighbouring walks differ more in x (the
+    default): every order adds the same weights to the same voxels."""
+    rng = np.random.default_rng(17)
+    n = 48
+    ang = synth.so3_angles(40, rng)
+    y = rng.standard_normal((40, n, n)).astype(np.float32)
+    x = rng.standard_normal((n, n, n)).astype(np.float32)
+    out = {}
+    for order in ("0", "3", "1", "2"):
+        monkeypatch.setenv("SPI_PJ_ADJ_ORDER", order)
+        out[order] = ops.pj3q_adjoint(y, ang, (n, n, n), ctx=ctx)
+    for order, v in out.items():
+        assert synth.rel_l2(v, out["0"]) <= 1e-6, order
+    ax = ops.pj3q(x, ang, ctx=ctx)
+    lhs = float(np.dot(ax.ravel().astype(np.float64), y.ravel()))
+    rhs = float(np.dot(x.ravel().astype(np.float64), out["1"].ravel()))
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs))
+
+
 def test_pj3q_device_tensors(ctx, orc):
     import torch
     rng = np.random.default_rng(9)
