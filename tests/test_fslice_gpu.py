@@ -29,13 +29,16 @@ def _real(z):
     return torch.tensor(np.stack([z.real, z.imag], -1), dtype=torch.float32, device="cuda").contiguous()
 
 
-@pytest.mark.parametrize("nx,order", [(24, None), (33, None), (24, "cols")])
+@pytest.mark.parametrize("nx,order", [(24, None), (33, None), (24, "cols"), (33, "lanes4")])
 def test_fslice_operators_match_oracle(ctx, orc, nx, order, monkeypatch):
     """order "cols": the insertions E^T walk every slice by half columns (the
-    order boxes above 192 take per slice); the result is the same."""
+    order boxes above 192 take per slice); "lanes4": the FP64 operators with
+    four lanes per pixel instead of eight.  The results are the same."""
     from spider_b200 import autograd
-    if order:
+    if order == "cols":
         monkeypatch.setenv("SPI_INSERT_ORDER", order)
+    elif order == "lanes4":
+        monkeypatch.setenv("SPI_FS_LANES", "4")
     rng = np.random.default_rng(300 + nx)
     n = 2 * nx
     ang = synth.so3_angles(40, rng)
