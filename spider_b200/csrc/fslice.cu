@@ -366,7 +366,9 @@ __global__ void __launch_bounds__(256) fs_normal64_kernel(const double2* __restr
 // Measured with 10,000 and 8,192 slices: 71.8 against 84.0 ms at 128^3,
 // 239 against 291 ms at 256^3.  The fused normal operator keeps four lanes: its
 // gather, with every weight and voxel index computed by two lanes here, made
-// it 1.7x slower in this form (0.159 against 0.0945 s per CG iteration).
+// it 1.7x slower in this form (0.159 against 0.0945 s per CG iteration), and
+// a four-lane gather followed by this scatter in two passes (the windows and
+// pixel sums moved across lanes by shuffles) 1.3x slower (0.123 s).
 __global__ void __launch_bounds__(256) fs_insert64w_kernel(const float2* __restrict__ sl_in, double* __restrict__ out,
                                                            const FsDesc* __restrict__ slices, int nslices, int nx,
                                                            const float* __restrict__ kbtab, float fltb) {
