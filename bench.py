@@ -657,7 +657,8 @@ def run_ours(args):
     if world > 1:
         gb = ctypes.c_longlong()
         L.spi_bp_grid_bytes(nx, ctypes.byref(gb))
-        grids = [torch.zeros(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
+        # spi_bp_open zeroes attached grids on the library stream, so no fill on torch's
+        grids = [torch.empty(gb.value // 4, dtype=torch.float32, device=dev) for _ in range(2)]
         ops.check(L.spi_bp_attach_grids(ctx.handle, ctypes.c_void_p(grids[0].data_ptr()),
                                         ctypes.c_void_p(grids[1].data_ptr())))
     ctx.bp_open(nx, 2, bf16=args.bf16)
