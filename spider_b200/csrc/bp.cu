@@ -17,6 +17,7 @@
 #include <map>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "../../include/spider_b200.h"
 #include "ctx.h"
@@ -277,6 +278,330 @@ __global__ void __launch_bounds__(256) colfft_kernel(const float2* __restrict__ 
   for (int q = threadIdx.x; q < n * kColTile; q += blockDim.x) {
     const int y = q / kColTile, cc = q % kColTile;
     if (cc < ncol) ob[(size_t)y * (h + 1) + k0 + cc] = a[cc * cs + y];
+  }
+}
+
+// ----------------------------------------------------------------------------
+// The same two passes with the transforms in registers (four-step FFT of H =
+// 32 P points over one warp: P-point DFTs in each lane's registers, a twiddle
+// W_H^(lane k2), then 32-point DFTs across the lanes by shuffles), one warp
+// per padded row (pass 1, H = n/2) or per column (pass 2, H = n).  A lane
+// starts with x[lane + 32 r], r < P, and ends with X[P brev5(lane) + k2],
+// k2 < P.  The radix-2 shared-memory form above is kept for n < 128 and
+// n > 512.
+
+// W_n^t for 0 <= t < n from the table of t < n/2 (W_n^(t + n/2) = -W_n^t)
+__device__ __forceinline__ float2 tw_full(const float2* tw, int t, int h) {
+  return t < h ? tw[t] : make_float2(-tw[t - h].x, -tw[t - h].y);
+}
+
+__host__ __device__ constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
+// bit reversal of V over BITS bits as a compile-time constant (register indices
+// must fold to constants, or the array goes to local memory)
+template <int V, int BITS>
+struct BrevT {
+  static constexpr int value = ((V & 1) << (BITS - 1)) | BrevT<(V >> 1), BITS - 1>::value;
+};
+template <int V>
+struct BrevT<V, 0> {
+  static constexpr int value = 0;
+};
+template <int K, int P, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (K < P) {
+    f(std::integral_constant<int, K>{});
+    static_for<K + 1, P>(f);
+  }
+}
+
+// P-point radix-2 decimation-in-frequency FFT in registers: natural order in,
+// a[brev(k)] = X[k] out; W_P^e = tw[e * (n / P)]
+template <int P>
+__device__ __forceinline__ void reg_fft_dif(float2 (&a)[P], const float2* tw, int n) {
+#pragma unroll
+  for (int h = P / 2; h >= 1; h >>= 1) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (i & h) continue;
+      const float2 u = a[i], v = a[i + h];
+      a[i] = make_float2(__fadd_rn(u.x, v.x), __fadd_rn(u.y, v.y));
+      const float2 d = make_float2(__fsub_rn(u.x, v.x), __fsub_rn(u.y, v.y));
+      const int e = (i & (h - 1)) * (P / (2 * h));
+      a[i + h] = e == 0 ? d : cmulf(tw[e * (n / P)], d);
+    }
+  }
+}
+
+// 32-point decimation-in-frequency FFT across the lanes, for each of the P
+// values of a lane: lane l ends with the output brev5(l)
+template <int P>
+__device__ __forceinline__ void warp_fft32_dif(float2 (&a)[P], const float2* tw, int n, int lane) {
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool top = (lane & h) == 0;
+    const float2 w = tw[(lane & (h - 1)) * (16 / h) * (n / 32)];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      const float px = __shfl_xor_sync(0xffffffffu, a[k].x, h);
+      const float py = __shfl_xor_sync(0xffffffffu, a[k].y, h);
+      if (top) a[k] = make_float2(__fadd_rn(a[k].x, px), __fadd_rn(a[k].y, py));
+      else a[k] = cmulf(w, make_float2(__fsub_rn(px, a[k].x), __fsub_rn(py, a[k].y)));
+    }
+  }
+}
+
+// H = 32 P point DFT (sign -1) of x[lane + 32 r] = z[r]; z[k2] = X[P brev5(lane) + k2] after
+template <int P>
+__device__ __forceinline__ void warp_fft(float2 (&z)[P], const float2* tw, int n, int lane) {
+  reg_fft_dif<P>(z, tw, n);
+  float2 y[P];
+  static_for<0, P>([&](auto kc) {
+    constexpr int k2 = decltype(kc)::value;
+    const float2 v = z[BrevT<k2, log2_c(P)>::value];
+    const int t = ((n / (32 * P)) * lane * k2) & (n - 1);   // W_H^(lane k2) = W_n^((n/H) lane k2)
+    y[k2] = k2 == 0 ? v : cmulf(tw_full(tw, t, n / 2), v);
+  });
+  warp_fft32_dif<P>(y, tw, n, lane);
+#pragma unroll
+  for (int k2 = 0; k2 < P; ++k2) z[k2] = y[k2];
+}
+
+__device__ __forceinline__ int brev5(int v) { return (int)(__brev((unsigned)v) >> 27); }
+
+// Pass 1, one warp per image row (P = n / 64): staging as stage_rowfft_kernel,
+// the real row as the complex sequence z[m] = in[2m] + i in[2m+1] of h = n/2
+// points, R[k] = E[k] + W_n^k O[k] for k <= h into inter[b][j][k].
+// the largest d >= 0 with d * d <= rem (rem >= 0)
+__device__ __forceinline__ int isqrt_floor(int rem) {
+  float f;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(f) : "f"((float)rem));
+  int d = (int)f;
+  while (d > 0 && d * d > rem) --d;
+  while ((d + 1) * (d + 1) <= rem) ++d;
+  return d;
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) stage_rowfft_w_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
+                                                             int nvalid, double klp, const float2* __restrict__ twg,
+                                                             float2* __restrict__ inter, size_t inter_stride) {
+  __shared__ float2 tw[512];
+  __shared__ double red[8];
+  __shared__ double qs_sh;
+  // per warp, a row's outputs R[k] at k + k / P (the lanes' values are P apart;
+  // this spreads them over the banks) before the row is written coalesced
+  __shared__ float2 rbuf[8][32 * P + 32 + 1];
+  const int h = n >> 1;   // = 32 P
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  const int b = blockIdx.x;
+  if (b >= nvalid) return;   // uniform per CTA
+  const float* img = imgs + (size_t)b * nx * nx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  {
+    // ASTA's border mean over the pixels outside the inscribed circle: row j
+    // (t = j + 1 - nc) keeps columns with t2 = i + 1 - nc, t^2 + t2^2 > r^2,
+    // i.e. all but the run |t2| <= isqrt(r^2 - t^2) (integers, exact)
+    const int r2 = (nx / 2) * (nx / 2), nc = nx / 2 + 1;
+    double sum = 0.0;
+    for (int j = warp; j < nx; j += nwarps) {
+      const int t = j + 1 - nc, rem = r2 - t * t;
+      const float* row = img + (size_t)j * nx;
+      int a0 = nx, b0 = nx;   // border: [0, a0) and [b0, nx)
+      if (rem >= 0) {
+        const int d = isqrt_floor(rem);
+        a0 = max(0, nc - 1 - d);
+        b0 = min(nx, nc + d);
+      }
+      for (int i = lane; i < a0; i += 32) sum += (double)__ldg(row + i);
+      for (int i = b0 + lane; i < nx; i += 32) sum += (double)__ldg(row + i);
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) red[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nwarps; ++w) t += red[w];
+      qs_sh = t / klp;
+    }
+    __syncthreads();
+  }
+  const double qs = qs_sh;
+  float2* ib = inter + (size_t)b * inter_stride;
+  const int j0 = (int)(((long long)nx * blockIdx.y) / gridDim.y), j1 = (int)(((long long)nx * (blockIdx.y + 1)) / gridDim.y);
+  const int k1 = brev5(lane);
+  const int lanec0 = brev5((32 - k1) & 31);   // the lane holding Z[h - P k1]
+  for (int j = j0 + warp; j < j1; j += nwarps) {   // warp-uniform
+    const float* irow = img + (size_t)j * nx;
+    float2 z[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      // padded columns 2m, 2m + 1 hold pixels i, i + 1 when i < nx (i even:
+      // nx - ip = nx / 2 is even for the sizes this kernel takes)
+      int i = 2 * (lane + 32 * r) + nx - ip;
+      if (i >= n) i -= n;
+      z[r] = make_float2(0.0f, 0.0f);
+      if (i < nx) {
+        const float2 p = __ldg(reinterpret_cast<const float2*>(irow + i));
+        z[r] = make_float2(__double2float_rn(__dsub_rn((double)p.x, qs)), __double2float_rn(__dsub_rn((double)p.y, qs)));
+      }
+    }
+    warp_fft<P>(z, tw, n, lane);   // the h-point FFT (tw is the table of W_n)
+    float2 zc[P];
+    zc[0] = make_float2(__shfl_sync(0xffffffffu, z[0].x, lanec0), __shfl_sync(0xffffffffu, z[0].y, lanec0));
+#pragma unroll
+    for (int k2 = 1; k2 < P; ++k2)
+      zc[k2] = make_float2(__shfl_sync(0xffffffffu, z[P - k2].x, 31 - lane),
+                           __shfl_sync(0xffffffffu, z[P - k2].y, 31 - lane));
+    float2* rb = rbuf[warp];
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+      const int k = P * k1 + k2;
+      const float2 zk = z[k2], c = zc[k2];
+      const float2 ev = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.x, c.x)), __fmul_rn(0.5f, __fsub_rn(zk.y, c.y)));
+      const float2 od = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.y, c.y)), __fmul_rn(-0.5f, __fsub_rn(zk.x, c.x)));
+      const float2 wo = cmulf(tw[k], od);
+      rb[(P + 1) * k1 + k2] = make_float2(__fadd_rn(ev.x, wo.x), __fadd_rn(ev.y, wo.y));
+      if (k == 0) {   // R[h] = E[0] - O[0]
+        rb[h + h / P] = make_float2(__fsub_rn(ev.x, od.x), __fsub_rn(ev.y, od.y));
+      }
+    }
+    __syncwarp();
+    float2* orow = ib + (size_t)j * (h + 1);
+    for (int k = lane; k <= h; k += 32) orow[k] = rb[k + k / P];
+    __syncwarp();
+  }
+}
+
+// Pass 2 at n = 128 and 256, one warp per column (P = n / 32; the shuffle
+// stages made it slower than colfft512_kernel's shared-memory transposes at
+// n = 512: 1.48 against 0.97 ms per 1,024 images): a CTA takes kColTileW columns k0..
+// of one image; the nx rows of those columns are read row by row (coalesced)
+// into shared memory, each warp transforms its columns (padded row y holds
+// image row j = (y - ip + nx) mod n when j < nx, else zero) into a second
+// tile, and the CTA writes that tile row by row.  256 threads (8 warps, two
+// columns each).
+constexpr int kColTileW = 16;
+template <int P>
+__global__ void __launch_bounds__(256) colfft_w_kernel(const float2* __restrict__ inter, size_t inter_stride, int nx,
+                                                       int n, int ip, int nvalid, const float2* __restrict__ twg,
+                                                       float2* __restrict__ out) {
+  extern __shared__ float2 fsm[];   // tw[n/2], inputs [kColTileW][nx + 1], outputs [kColTileW][so]
+  const int h = n >> 1;             // n = 32 P
+  const int tiles = (h + 1 + kColTileW - 1) / kColTileW;
+  const int b = blockIdx.x / tiles, k0 = (blockIdx.x % tiles) * kColTileW;
+  // Output y of column c sits at c * so + y + y / P: a warp's 32 lanes store
+  // rows P brev5(lane) + k2, P rows apart, which this spreads over the banks
+  // (so = n + n / P + 1 = n + 33, 1 mod 16, keeps the row-by-row reads apart
+  // too); the input columns have stride nx + 1 for the same reason.
+  const int si = nx + 1, so = n + n / P + 1;
+  float2* tw = fsm;
+  float2* ain = fsm + h;
+  float2* aout = ain + (size_t)kColTileW * si;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  if (b >= nvalid) return;          // uniform per CTA
+  const int ncol = min(kColTileW, h + 1 - k0);
+  const float2* ib = inter + (size_t)b * inter_stride;
+  for (int q = threadIdx.x; q < nx * kColTileW; q += blockDim.x) {
+    const int j = q / kColTileW, c = q % kColTileW;
+    if (c < ncol) ain[c * si + j] = ib[(size_t)j * (h + 1) + k0 + c];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int k1 = brev5(lane);
+  for (int c = warp; c < ncol; c += nwarps) {   // warp-uniform
+    float2 z[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      const int y = lane + 32 * r;
+      int j = y - ip + nx;
+      if (j >= n) j -= n;
+      z[r] = (j < nx) ? ain[c * si + j] : make_float2(0.0f, 0.0f);
+    }
+    warp_fft<P>(z, tw, n, lane);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) aout[c * so + (P + 1) * k1 + k2] = z[k2];   // y + y / P, y = P k1 + k2
+  }
+  __syncthreads();
+  float2* ob = out + (size_t)b * n * (h + 1);
+  for (int q = threadIdx.x; q < n * kColTileW; q += blockDim.x) {
+    const int y = q / kColTileW, c = q % kColTileW;
+    if (c < ncol) ob[(size_t)y * (h + 1) + k0 + c] = aout[c * so + y + y / P];
+  }
+}
+
+// Pass 2 at n = 512 (nx = 256), 64 threads per column, three register
+// radix-8 levels joined by two shared-memory transposes: level 1, thread t
+// takes x[t + 64 r], an 8-point DFT over r and W_512^(t k2) give S[k2][t];
+// level 2, thread (k2, u) takes S[k2][u + 8 r], an 8-point DFT over r and
+// W_64^(u m2) give T[k2][m2][u]; level 3, thread (k2, m2) takes T[k2][m2][u],
+// an 8-point DFT over u gives X[64 m1 + 8 m2 + k2].  A CTA of 256 threads does
+// 8 columns of one image (4 at a time).  Shared strides are chosen so that a
+// warp's accesses hit each bank at most twice (checked by enumeration).
+constexpr int kC512Cols = 8, kC512SI = 260, kC512SO = 580, kC512WB = 576;
+__global__ void __launch_bounds__(256) colfft512_kernel(const float2* __restrict__ inter, size_t inter_stride, int nx,
+                                                        int n, int ip, int nvalid, const float2* __restrict__ twg,
+                                                        float2* __restrict__ out) {
+  extern __shared__ float2 fsm[];   // tw[256], in [8][SI], out [8][SO], work [4][WB]
+  const int h = 256;
+  const int tiles = (h + 1 + kC512Cols - 1) / kC512Cols;
+  const int b = blockIdx.x / tiles, k0 = (blockIdx.x % tiles) * kC512Cols;
+  float2* tw = fsm;
+  float2* ain = tw + h;
+  float2* aout = ain + kC512Cols * kC512SI;
+  float2* work = aout + kC512Cols * kC512SO;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  if (b >= nvalid) return;          // uniform per CTA
+  const int ncol = min(kC512Cols, h + 1 - k0);
+  const float2* ib = inter + (size_t)b * inter_stride;
+  for (int q = threadIdx.x; q < nx * kC512Cols; q += blockDim.x) {
+    const int j = q / kC512Cols, c = q % kC512Cols;
+    ain[c * kC512SI + j] = (c < ncol) ? ib[(size_t)j * (h + 1) + k0 + c] : make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  const int grp = threadIdx.x >> 6, t = threadIdx.x & 63;
+  float2* S = work + grp * kC512WB;
+  const int g8 = t >> 3, l8 = t & 7;
+  for (int c = grp; c < kC512Cols; c += 4) {   // the same two rounds for every group
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int j = t + 64 * r - ip + nx;
+      if (j >= n) j -= n;
+      v[r] = (j < nx) ? ain[c * kC512SI + j] : make_float2(0.0f, 0.0f);
+    }
+    reg_fft_dif<8>(v, tw, n);
+    static_for<0, 8>([&](auto kc) {
+      constexpr int k2 = decltype(kc)::value;
+      const float2 val = v[BrevT<k2, 3>::value];
+      S[k2 * 68 + t] = k2 == 0 ? val : cmulf(tw_full(tw, t * k2, h), val);
+    });
+    __syncthreads();
+    float2 w[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) w[r] = S[g8 * 68 + l8 + 8 * r];   // k2 = g8, u = l8
+    reg_fft_dif<8>(w, tw, n);
+    __syncthreads();                                             // S read; T overwrites it
+    static_for<0, 8>([&](auto mc) {
+      constexpr int m2 = decltype(mc)::value;
+      const float2 val = w[BrevT<m2, 3>::value];
+      S[g8 * 72 + 9 * m2 + l8] = m2 == 0 ? val : cmulf(tw_full(tw, 8 * l8 * m2, h), val);
+    });
+    __syncthreads();
+    float2 qv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) qv[u] = S[g8 * 72 + 9 * l8 + u];   // k2 = g8, m2 = l8
+    reg_fft_dif<8>(qv, tw, n);
+    static_for<0, 8>([&](auto mc) {
+      constexpr int m1 = decltype(mc)::value;
+      const int y = 64 * m1 + 8 * l8 + g8;
+      aout[c * kC512SO + y + (y >> 3)] = qv[BrevT<m1, 3>::value];
+    });
+    __syncthreads();                                             // before the next round's S
+  }
+  float2* ob = out + (size_t)b * n * (h + 1);
+  for (int q = threadIdx.x; q < n * kC512Cols; q += blockDim.x) {
+    const int y = q / kC512Cols, c = q % kC512Cols;
+    if (c < ncol) ob[(size_t)y * (h + 1) + k0 + c] = aout[c * kC512SO + y + (y >> 3)];
   }
 }
 
@@ -1721,10 +2046,12 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
   {
     // the own two-pass R2C is opt-in (SPI_FFT=own): measured slower than
-    // staging + cuFFT at 256^3 (2.4 against 1.4 ms per 1,024 images)
+    // staging + cuFFT at 256^3 (1.64 against 1.36 ms per 1,024 images with
+    // the register-FFT passes; 2.37 with the radix-2 shared-memory passes,
+    // SPI_FFT=own2)
     const char* f = getenv("SPI_FFT");
     const bool pow2 = (c->n & (c->n - 1)) == 0 && c->n >= 16 && c->n <= 1024;
-    c->fft_own = (pow2 && f && strcmp(f, "own") == 0) ? 1 : 0;
+    c->fft_own = (pow2 && f && strcmp(f, "own") == 0) ? 1 : (pow2 && f && strcmp(f, "own2") == 0) ? 2 : 0;
   }
   c->chunk = ((chunk + sub - 1) / sub) * sub;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -1769,6 +2096,51 @@ int spi_bp_flush(spi_ctx* c) {
 }
 
 // Twiddles of the own R2C: W_n^t = e^(-2 pi i t / n), t < n/2, computed in FP64.
+// The register-FFT passes exist for n = 128, 256 and 512 (SPI_FFT=own; at n =
+// 512 the column pass is colfft512_kernel); the shared-memory radix-2 passes
+// take the other sizes (and SPI_FFT=own2).
+static bool fft_warp_form(const spi_ctx* c) { return c->fft_own == 1 && (c->n == 128 || c->n == 256 || c->n == 512); }
+
+static int launch_rowfft(spi_ctx* c, cudaStream_t st, const float* src, int np, int parts, double klp, float2* inter) {
+  const int nx = c->nx, n = c->n, ip = (n - nx) / 2 + nx % 2;
+  const float2* tw = c->fft_tw.as<float2>();
+  const size_t istride = (size_t)n * n / 2;
+  if (fft_warp_form(c)) {
+    const dim3 g(np, parts);
+    if (n == 128) stage_rowfft_w_kernel<2><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
+    else if (n == 256) stage_rowfft_w_kernel<4><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
+    else stage_rowfft_w_kernel<8><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
+    return check_kernel("stage_rowfft_w_kernel");
+  }
+  const size_t smem = (size_t)(n / 2) * 5 * sizeof(float2);
+  stage_rowfft_kernel<<<dim3(np, parts), 256, smem, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
+  return check_kernel("stage_rowfft_kernel");
+}
+
+static int launch_colfft(spi_ctx* c, cudaStream_t st, const float2* inter, int nvalid, float2* out) {
+  const int nx = c->nx, n = c->n, ip = (n - nx) / 2 + nx % 2;
+  const float2* tw = c->fft_tw.as<float2>();
+  const size_t istride = (size_t)n * n / 2;
+  if (fft_warp_form(c)) {
+    const int tiles = (n / 2 + 1 + kColTileW - 1) / kColTileW;
+    const size_t smem = ((size_t)(n / 2) + (size_t)kColTileW * ((nx + 1) + (n + 33))) * sizeof(float2);
+    if (n == 128) {
+      colfft_w_kernel<4><<<nvalid * tiles, 256, smem, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+    } else if (n == 256) {
+      colfft_w_kernel<8><<<nvalid * tiles, 256, smem, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+    } else {
+      const int t512 = (n / 2 + 1 + kC512Cols - 1) / kC512Cols;
+      const size_t sm512 = (size_t)(256 + kC512Cols * (kC512SI + kC512SO) + 4 * kC512WB) * sizeof(float2);
+      colfft512_kernel<<<nvalid * t512, 256, sm512, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+    }
+    return check_kernel("colfft_w_kernel");
+  }
+  const int tiles = (n / 2 + 1 + kColTile - 1) / kColTile;
+  const size_t smem = ((size_t)(n / 2) + (size_t)kColTile * (n + 1)) * sizeof(float2);
+  colfft_kernel<<<nvalid * tiles, 256, smem, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+  return check_kernel("colfft_kernel");
+}
+
 static int ensure_fft_twiddles(spi_ctx* c) {
   const int n = c->n, h = n / 2;
   if (c->fft_tw.p && c->fft_tw.bytes >= (size_t)h * sizeof(float2)) return 0;
@@ -1786,6 +2158,11 @@ static int ensure_fft_twiddles(spi_ctx* c) {
   if (!(done & bit)) {   // the column pass holds 16 columns of up to 1,024 points
     SPI_CUDA(cudaFuncSetAttribute(colfft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)((512 + kColTile * 1025) * sizeof(float2))));
+    const int wsm = (int)((128 + kColTileW * (129 + 256 + 33)) * sizeof(float2));   // n = 256
+    SPI_CUDA(cudaFuncSetAttribute(colfft_w_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+    SPI_CUDA(cudaFuncSetAttribute(colfft_w_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+    SPI_CUDA(cudaFuncSetAttribute(colfft512_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((256 + kC512Cols * (kC512SI + kC512SO) + 4 * kC512WB) * sizeof(float2))));
     done |= bit;
   }
   return 0;
@@ -2129,11 +2506,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
           // pass 1 of the own R2C: staged rows transformed into padded, used as
           // the row-spectrum buffer (n*n/2 complex slots per image)
           const int parts = std::max(1, std::min(8, (4 * c->sm_count + np - 1) / std::max(np, 1)));
-          const size_t smem = (size_t)(n / 2) * 5 * sizeof(float2);
-          stage_rowfft_kernel<<<dim3(np, parts), 256, smem, c->stream>>>(
-              src, nx, n, ip, np, klp, c->fft_tw.as<float2>(),
-              c->padded.as<float2>() + (size_t)(p0 - b0) * n * n / 2, (size_t)n * n / 2);
-          SPI_TRY(check_kernel("stage_rowfft_kernel"));
+          SPI_TRY(launch_rowfft(c, c->stream, src, np, parts, klp,
+                                c->padded.as<float2>() + (size_t)(p0 - b0) * n * n / 2));
         } else {
           // the last piece also zero-pads the unused tail of the FFT batch
           const int blocks = last ? c->sub - (p0 - b0) : np;
@@ -2150,11 +2524,7 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
       float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + (size_t)b0 * spec_plane;
       int ev = c->phase_begin(1);
       if (c->fft_own) {   // pass 2: the columns of the valid images
-        const int tiles = (n / 2 + 1 + kColTile - 1) / kColTile;
-        const size_t smem = ((size_t)(n / 2) + (size_t)kColTile * (n + 1)) * sizeof(float2);
-        colfft_kernel<<<nvalid * tiles, 256, smem, c->stream>>>(c->padded.as<float2>(), (size_t)n * n / 2, nx, n, ip,
-                                                                 nvalid, c->fft_tw.as<float2>(), fout);
-        SPI_TRY(check_kernel("colfft_kernel"));
+        SPI_TRY(launch_colfft(c, c->stream, c->padded.as<float2>(), nvalid, fout));
         c->count();
       } else {
         SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
