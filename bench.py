@@ -897,9 +897,8 @@ def multiclass_measure(args, steps=4):
     classes are timed, images resident on the device; the rate with one context and host thread per class (concurrent
     streams) is given beside it.  Several streams run at once in the second
     form, so both are timed by the host clock between synchronisations.
-    Each pass opens (allocates) and closes (frees) the classes' grids and FFT
-    plans, which varies by up to a second between passes on the same box, so
-    the minimum of four passes is reported."""
+    The contexts stay open across passes (a same-size open zeroes the grids
+    and keeps buffers and FFT plans); the minimum of four passes is reported."""
     import torch
     from spider_b200 import ops, synth
     _, _, local = dist_env()
@@ -921,7 +920,7 @@ def multiclass_measure(args, steps=4):
     ctx.close()
     torch.cuda.synchronize()
 
-    ctxs = [ops.Context(local) for _ in classes]      # kept across passes
+    ctxs = [ops.Context(local) for _ in classes]      # kept open across passes
 
     def one_pass(one_launch):
         torch.cuda.synchronize()
@@ -943,8 +942,8 @@ def multiclass_measure(args, steps=4):
             "config": {"workload": "multi-class BP 32F, boxes 96,128,160,192,192,224,256,256",
                        "images": args.mc_images, "per_class": [int(c[0].shape[0]) for c in classes],
                        "timing": "host clock around synchronised calls (open, insertion and finish of all eight "
-                                 "classes; the contexts are kept across passes, and each pass opens and closes "
-                                 f"the classes' grids, buffers and FFT plans), min over {max(steps, 1)} passes",
+                                 "classes; the contexts stay open across passes, so each pass's open zeroes the "
+                                 f"grids and reuses the buffers and FFT plans), min over {max(steps, 1)} passes",
                        "forms": "value: spi_bp_insert_multi (one insertion launch per round, one stream); "
                                 "threads_value: one context and host thread per class"}}
 

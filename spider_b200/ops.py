@@ -254,14 +254,18 @@ def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, 
             if autotune and not one_launch:   # launch shape per box size (cached per process)
                 c.bp_autotune()
 
-        if one_launch:
-            bp_insert_multi(ctxs, classes)
+        def finish_all():
             out = []
             for c in ctxs:
                 o = c.bp_finish(("all", "1", "2"), device=device_out)
                 out.append((o["all"], o["1"], o["2"]))
-                c.bp_close()
+                if own:   # caller contexts stay open: a same-size bp_open keeps their buffers and plans
+                    c.bp_close()
             return out
+
+        if one_launch:
+            bp_insert_multi(ctxs, classes)
+            return finish_all()
 
         def insert(k):
             imgs, ang, half = classes[k]
@@ -274,12 +278,7 @@ def bp32f_multiclass(classes, sym=None, *, device: int = 0, bf16: bool = False, 
         else:
             for k in range(len(classes)):
                 insert(k)
-        out = []
-        for c in ctxs:
-            o = c.bp_finish(("all", "1", "2"), device=device_out)
-            out.append((o["all"], o["1"], o["2"]))
-            c.bp_close()
-        return out
+        return finish_all()
     finally:
         if own:
             for c in ctxs:

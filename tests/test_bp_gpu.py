@@ -238,6 +238,29 @@ def test_bp32f_multiclass(orc, mode):
             assert synth.rel_l2(a, b) <= TOL
 
 
+@pytest.mark.parametrize("one_launch", [True, False])
+def test_bp32f_multiclass_reused_contexts(orc, one_launch):
+    """Caller contexts stay open between calls: the second call's same-size
+    open zeroes the grids and reuses buffers and FFT plans, and both calls
+    give the oracle's volumes."""
+    classes, refs = [], []
+    for k, (nx, nimg) in enumerate(((24, 90), (32, 120))):
+        _, pr, ang = _case(nx, nimg, 130 + k, noise=0.5)
+        half = synth.half_mask(nimg, np.random.default_rng(135 + k))
+        classes.append((pr, ang, half))
+        refs.append(orc.bp32f(pr, ang, half, prec=0, nthreads=1))
+    ctxs = [ops.Context(0) for _ in classes]
+    try:
+        for _ in range(2):
+            out = ops.bp32f_multiclass(classes, one_launch=one_launch, ctxs=ctxs)
+            for got, ref in zip(out, refs):
+                for a, b in zip(got, ref):
+                    assert synth.rel_l2(a, b) <= TOL
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_bp_insert_multi_rounds_and_errors(ctx, orc):
     """spi_bp_insert_multi with device images and FFT sub-batches smaller
     than the image counts (several rounds, classes running out at different
