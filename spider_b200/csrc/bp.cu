@@ -472,6 +472,138 @@ __global__ void __launch_bounds__(256) stage_rowfft_w_kernel(const float* __rest
   }
 }
 
+// Pass 1 at n = 512 (nx = 256): as stage_rowfft_w_kernel, one warp per row,
+// but the 256-point transform in three register levels joined by two
+// transposes through the warp's shared buffer instead of shuffles: level 1,
+// lane t takes x[t + 32 r], an 8-point DFT over r and W_256^(t k2) give
+// S[k2][t]; level 2, lane (k2, u) takes S[k2][u + 4 r], an 8-point DFT over r
+// and W_32^(u m2) give T[k2][m2][u]; level 3, lane (k2, m2, m2 + 1) takes
+// T[k2][m2][u], 4-point DFTs over u give X[64 m1 + 8 m2 + k2] into the buffer,
+// from which each lane forms R[k] = E[k] + W_512^k O[k] for k = lane + 32 i
+// and writes the row coalesced.  Strides and the swizzle of X (k + k / 4)
+// keep every warp access at most 3-way bank-conflicted (checked by
+// enumeration).
+constexpr int kR512SS = 36, kR512TS = 35, kR512TR = 4, kR512Buf = 320;
+__global__ void __launch_bounds__(256) stage_rowfft512_kernel(const float* __restrict__ imgs, int nx, int n, int ip,
+                                                              int nvalid, double klp, const float2* __restrict__ twg,
+                                                              float2* __restrict__ inter, size_t inter_stride) {
+  __shared__ float2 tw[256];
+  __shared__ double red[8];
+  __shared__ double qs_sh;
+  __shared__ float2 wbuf[8][kR512Buf];
+  const int h = 256;
+  for (int t = threadIdx.x; t < h; t += blockDim.x) tw[t] = twg[t];
+  const int b = blockIdx.x;
+  if (b >= nvalid) return;   // uniform per CTA
+  const float* img = imgs + (size_t)b * nx * nx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  {
+    const int r2 = (nx / 2) * (nx / 2), nc = nx / 2 + 1;
+    double sum = 0.0;
+    for (int j = warp; j < nx; j += nwarps) {
+      const int t = j + 1 - nc, rem = r2 - t * t;
+      const float* row = img + (size_t)j * nx;
+      int a0 = nx, b0 = nx;
+      if (rem >= 0) {
+        const int d = isqrt_floor(rem);
+        a0 = max(0, nc - 1 - d);
+        b0 = min(nx, nc + d);
+      }
+      for (int i = lane; i < a0; i += 32) sum += (double)__ldg(row + i);
+      for (int i = b0 + lane; i < nx; i += 32) sum += (double)__ldg(row + i);
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) red[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nwarps; ++w) t += red[w];
+      qs_sh = t / klp;
+    }
+    __syncthreads();
+  }
+  const double qs = qs_sh;
+  float2* ib = inter + (size_t)b * inter_stride;
+  float2* B = wbuf[warp];
+  const int k2l = lane >> 2, ul = lane & 3;
+  const int j0 = (int)(((long long)nx * blockIdx.y) / gridDim.y), j1 = (int)(((long long)nx * (blockIdx.y + 1)) / gridDim.y);
+  // padded columns 2m, 2m + 1 (m = lane + 32 r) hold pixels i, i + 1 when i < nx;
+  // a row's pixels are loaded one row ahead of its transform
+  auto load_row = [&](int jr, float2 (&pv)[8]) {
+    const float* irow = img + (size_t)jr * nx;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int i = 2 * (lane + 32 * r) + nx - ip;
+      if (i >= n) i -= n;
+      pv[r] = (i < nx) ? __ldg(reinterpret_cast<const float2*>(irow + i)) : make_float2(0.0f, 0.0f);
+    }
+  };
+  float2 pnext[8];
+  if (j0 + warp < j1) load_row(j0 + warp, pnext);
+  for (int j = j0 + warp; j < j1; j += nwarps) {   // warp-uniform
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int i = 2 * (lane + 32 * r) + nx - ip;
+      if (i >= n) i -= n;
+      v[r] = (i < nx) ? make_float2(__double2float_rn(__dsub_rn((double)pnext[r].x, qs)),
+                                    __double2float_rn(__dsub_rn((double)pnext[r].y, qs)))
+                      : make_float2(0.0f, 0.0f);
+    }
+    if (j + nwarps < j1) load_row(j + nwarps, pnext);
+    // level 1
+    reg_fft_dif<8>(v, tw, n);
+    static_for<0, 8>([&](auto kc) {
+      constexpr int k2 = decltype(kc)::value;
+      const float2 val = v[BrevT<k2, 3>::value];
+      B[k2 * kR512SS + lane] = k2 == 0 ? val : cmulf(tw_full(tw, 2 * lane * k2, h), val);   // W_256^(t k2)
+    });
+    __syncwarp();
+    // level 2
+    float2 w[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) w[r] = B[k2l * kR512SS + ul + 4 * r];
+    reg_fft_dif<8>(w, tw, n);
+    __syncwarp();
+    static_for<0, 8>([&](auto mc) {
+      constexpr int m2 = decltype(mc)::value;
+      const float2 val = w[BrevT<m2, 3>::value];
+      B[k2l * kR512TS + m2 * kR512TR + ul] = m2 == 0 ? val : cmulf(tw_full(tw, 16 * ul * m2, h), val);   // W_32^(u m2)
+    });
+    __syncwarp();
+    // level 3: lane takes (k2, m2) for m2 = 2 (lane & 3) and 2 (lane & 3) + 1
+    float2 q0[4], q1[4];
+    const int m2a = 2 * ul;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      q0[u] = B[k2l * kR512TS + m2a * kR512TR + u];
+      q1[u] = B[k2l * kR512TS + (m2a + 1) * kR512TR + u];
+    }
+    reg_fft_dif<4>(q0, tw, n);
+    reg_fft_dif<4>(q1, tw, n);
+    __syncwarp();
+    static_for<0, 4>([&](auto mc) {
+      constexpr int m1 = decltype(mc)::value;
+      const int y0 = 64 * m1 + 8 * m2a + k2l, y1 = y0 + 8;
+      B[y0 + (y0 >> 2)] = q0[BrevT<m1, 2>::value];
+      B[y1 + (y1 >> 2)] = q1[BrevT<m1, 2>::value];
+    });
+    __syncwarp();
+    float2* orow = ib + (size_t)j * (h + 1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int k = lane + 32 * i, kc = (h - k) & (h - 1);
+      const float2 zk = B[k + (k >> 2)], c = B[kc + (kc >> 2)];
+      const float2 ev = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.x, c.x)), __fmul_rn(0.5f, __fsub_rn(zk.y, c.y)));
+      const float2 od = make_float2(__fmul_rn(0.5f, __fadd_rn(zk.y, c.y)), __fmul_rn(-0.5f, __fsub_rn(zk.x, c.x)));
+      const float2 wo = cmulf(tw[k], od);
+      orow[k] = make_float2(__fadd_rn(ev.x, wo.x), __fadd_rn(ev.y, wo.y));
+      if (k == 0) orow[h] = make_float2(__fsub_rn(ev.x, od.x), __fsub_rn(ev.y, od.y));   // R[h] = E[0] - O[0]
+    }
+    __syncwarp();
+  }
+}
+
 // Pass 2 at n = 128 and 256, one warp per column (P = n / 32; the shuffle
 // stages made it slower than colfft512_kernel's shared-memory transposes at
 // n = 512: 1.48 against 0.97 ms per 1,024 images): a CTA takes kColTileW columns k0..
@@ -553,9 +685,20 @@ __global__ void __launch_bounds__(256) colfft512_kernel(const float2* __restrict
   if (b >= nvalid) return;          // uniform per CTA
   const int ncol = min(kC512Cols, h + 1 - k0);
   const float2* ib = inter + (size_t)b * inter_stride;
-  for (int q = threadIdx.x; q < nx * kC512Cols; q += blockDim.x) {
-    const int j = q / kC512Cols, c = q % kC512Cols;
-    ain[c * kC512SI + j] = (c < ncol) ? ib[(size_t)j * (h + 1) + k0 + c] : make_float2(0.0f, 0.0f);
+  {
+    // nx * 8 = 2,048 values, 8 per thread: all loads first, then the stores
+    constexpr int kPer = 256 * kC512Cols / 256;
+    float2 ld[kPer];
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int q = threadIdx.x + 256 * e, j = q / kC512Cols, c = q % kC512Cols;
+      ld[e] = (c < ncol) ? __ldg(ib + (size_t)j * (h + 1) + k0 + c) : make_float2(0.0f, 0.0f);
+    }
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int q = threadIdx.x + 256 * e, j = q / kC512Cols, c = q % kC512Cols;
+      ain[c * kC512SI + j] = ld[e];
+    }
   }
   __syncthreads();
   const int grp = threadIdx.x >> 6, t = threadIdx.x & 63;
@@ -2045,13 +2188,17 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   c->sub = sub;
   c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
   {
-    // the own two-pass R2C is opt-in (SPI_FFT=own): measured slower than
-    // staging + cuFFT at 256^3 (1.64 against 1.36 ms per 1,024 images with
-    // the register-FFT passes; 2.37 with the radix-2 shared-memory passes,
-    // SPI_FFT=own2)
+    // The own two-pass R2C is the default at n = 512 (nx = 256), where its
+    // register passes (stage_rowfft512_kernel + colfft512_kernel) measured
+    // 1.22 ms per 1,024 images against 1.36 ms for PADD2 + cuFFT; elsewhere
+    // PADD2 + cuFFT.  SPI_FFT=cufft / own / own2 choose explicitly (own: the
+    // register passes at n = 128-512, radix-2 elsewhere; own2: radix-2).
     const char* f = getenv("SPI_FFT");
     const bool pow2 = (c->n & (c->n - 1)) == 0 && c->n >= 16 && c->n <= 1024;
-    c->fft_own = (pow2 && f && strcmp(f, "own") == 0) ? 1 : (pow2 && f && strcmp(f, "own2") == 0) ? 2 : 0;
+    if (f && strcmp(f, "own") == 0) c->fft_own = pow2 ? 1 : 0;
+    else if (f && strcmp(f, "own2") == 0) c->fft_own = pow2 ? 2 : 0;
+    else if (f && strcmp(f, "cufft") == 0) c->fft_own = 0;
+    else c->fft_own = c->n == 512 ? 1 : 0;
   }
   c->chunk = ((chunk + sub - 1) / sub) * sub;
   SPI_CUDA(cudaStreamSynchronize(c->stream));
@@ -2109,7 +2256,7 @@ static int launch_rowfft(spi_ctx* c, cudaStream_t st, const float* src, int np, 
     const dim3 g(np, parts);
     if (n == 128) stage_rowfft_w_kernel<2><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
     else if (n == 256) stage_rowfft_w_kernel<4><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
-    else stage_rowfft_w_kernel<8><<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
+    else stage_rowfft512_kernel<<<g, 256, 0, st>>>(src, nx, n, ip, np, klp, tw, inter, istride);
     return check_kernel("stage_rowfft_w_kernel");
   }
   const size_t smem = (size_t)(n / 2) * 5 * sizeof(float2);

@@ -420,18 +420,22 @@ def test_own_r2c_matches_cufft_path(ctx, orc):
             assert synth.rel_l2(d, r) <= 5e-4
 
 
-@pytest.mark.parametrize("nx,mode", [(64, "own2"), (128, "own"), (128, "own2"), (256, "own")])
+@pytest.mark.parametrize("nx,mode", [(64, "own2"), (128, "own"), (128, "own2"), (256, "own"), (256, "own2")])
 def test_own_r2c_sizes(ctx, nx, mode):
-    """The register-FFT passes (SPI_FFT=own at padded sizes 128-512) and the
-    shared-memory radix-2 passes (own2) give the staging + cuFFT path's
-    volumes at the bench's sizes."""
+    """The register-FFT passes (SPI_FFT=own at padded sizes 128-512; the
+    default at 512) and the shared-memory radix-2 passes (own2) give the
+    volumes of PADD2 + cuFFT (SPI_FFT=cufft)."""
     rng = np.random.default_rng(700 + nx)
     nimg = 48
     vol = synth.blob_phantom(nx, 10, sigma=(2, 6), radius=0.35 * nx, rng=rng)
     ang = synth.so3_angles(nimg, rng)
     pr = ops.pj3q(vol, ang, ctx=ctx)
     half = synth.half_mask(nimg, rng)
-    base = ops.bp32f(pr, ang, half, ctx=ctx)
+    os.environ["SPI_FFT"] = "cufft"
+    try:
+        base = ops.bp32f(pr, ang, half, ctx=ctx)
+    finally:
+        del os.environ["SPI_FFT"]
     os.environ["SPI_FFT"] = mode
     try:
         own = ops.bp32f(pr, ang, half, ctx=ctx)
