@@ -2864,11 +2864,18 @@ static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* con
       }
       const int ip = (n - nx) / 2 + nx % 2;
       const int parts = std::max(1, std::min(8, (4 * c->sm_count + c->sub - 1) / c->sub));
-      stage_kernel<<<dim3(c->sub, parts), 256, 0, s2>>>(src, nx, n, ip, nb, klp[k], c->padded.as<float>());
-      SPI_TRY(check_kernel("stage_kernel"));
-      c->count();
       float2* fout = c->bf16 ? c->spec_tmp.as<float2>() : c->spectra.as<float2>() + hoff * plane;
-      SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      if (c->fft_own) {   // the own R2C (the class's box takes the same default as spi_bp_insert)
+        const int rparts = std::max(1, std::min(8, (4 * c->sm_count + nb - 1) / std::max(nb, 1)));
+        SPI_TRY(launch_rowfft(c, s2, src, nb, rparts, klp[k], c->padded.as<float2>()));
+        SPI_TRY(launch_colfft(c, s2, c->padded.as<float2>(), nb, fout));
+        c->count(2);
+      } else {
+        stage_kernel<<<dim3(c->sub, parts), 256, 0, s2>>>(src, nx, n, ip, nb, klp[k], c->padded.as<float>());
+        SPI_TRY(check_kernel("stage_kernel"));
+        c->count();
+        SPI_CUFFT(cufftExecR2C(c->plan2d, c->padded.as<cufftReal>(), reinterpret_cast<cufftComplex*>(fout)));
+      }
       if (c->bf16) {
         const size_t cntv = (size_t)nb * plane;
         to_bf16_kernel<<<grid_blocks(c, cntv, 256), 256, 0, s2>>>(

@@ -212,7 +212,7 @@ def test_rb3f_rb32f_match_oracle(ctx, orc):
     assert synth.rel_l2(z, ops.bp3f(pr, ang, ctx=ctx)) <= 2e-6
 
 
-@pytest.mark.parametrize("mode", ["one_launch", "one_launch:cols", "concurrent", "in_turn"])
+@pytest.mark.parametrize("mode", ["one_launch", "one_launch:cols", "one_launch:own", "concurrent", "in_turn"])
 def test_bp32f_multiclass(orc, mode):
     """Several classes of different box sizes (one odd, two equal) reconstructed
     from one image stream: all classes in one insertion launch per round
@@ -225,13 +225,16 @@ def test_bp32f_multiclass(orc, mode):
         half = synth.half_mask(nimg, np.random.default_rng(95 + k))
         classes.append((pr, ang, half))
         refs.append(orc.bp32f(pr, ang, half, prec=0, nthreads=1))
-    mode, _, order = mode.partition(":")
-    if order:
-        os.environ["SPI_INSERT_ORDER"] = order
+    mode, _, opt = mode.partition(":")
+    if opt == "cols":
+        os.environ["SPI_INSERT_ORDER"] = opt
+    elif opt == "own":   # the own R2C for the power-of-two padded box (32 -> 64), cuFFT for the others
+        os.environ["SPI_FFT"] = opt
     try:
         out = ops.bp32f_multiclass(classes, one_launch=mode == "one_launch", concurrent=mode == "concurrent")
     finally:
         os.environ.pop("SPI_INSERT_ORDER", None)
+        os.environ.pop("SPI_FFT", None)
     for got, ref in zip(out, refs):
         for a, b in zip(got, ref):
             assert a.shape == b.shape
