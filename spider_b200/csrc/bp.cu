@@ -2054,6 +2054,7 @@ int spi_ctx_create(int device, spi_ctx** out) {
     return st;
   }
   c->pipeline = env_int("SPI_PIPELINE", 1) ? 1 : 0;
+  c->first_piece = env_int("SPI_FIRST_PIECE", 1) ? 1 : 0;
   c->accum = env_int("SPI_BP_ACCUM", 1) ? 1 : 0;
   *out = c;
   return 0;
@@ -2187,6 +2188,7 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   sub = std::max(1, std::min(chunk, env_int("SPI_BP_SUB", sub)));
   c->sub = sub;
   c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
+  c->upload_images = std::max(0, env_int("SPI_UPLOAD_IMAGES", 0));   // 0: pieces of ~64 MB
   {
     // The own two-pass R2C is the default at n = 512 (nx = 256), where its
     // register passes (stage_rowfft512_kernel + colfft512_kernel) measured
@@ -2471,13 +2473,15 @@ static short line_cols(const spi_ctx* c, const float* dms) {
 // Slice descriptors of nimg images: CANG of each angle triple (BUILDM1,
 // bp3f.f:1287), its products with the symmetry matrices (bp3f.f:460-466) and
 // the grid its half-set mask routes it to; image index a % chunk.  With slice
-// ordering on, the slices of each group of `group` images within a chunk are
-// ordered by the normal of their central plane (boustrophedon over rings of
-// the polar angle), so the slices in flight together touch overlapping
-// voxels and their atomics hit in L2; the order only changes the FP32
-// summation order.
-static void build_slices(const spi_ctx* c, const float* angles, const uint8_t* half, int nimg, int chunk, int group,
-                         SliceDesc* hs) {
+// ordering on, the slices of each group of `group` images are ordered by the
+// normal of their central plane (boustrophedon over rings of the polar
+// angle), so the slices in flight together touch overlapping voxels and
+// their atomics hit in L2; the order only changes the FP32 summation order.
+// Groups lie inside the FFT sub-batches of a chunk (its first `first`
+// images, then `sub` at a time), so an insertion launch, which takes one
+// sub-batch, only meets slices of images it has staged.
+static void build_slices(const spi_ctx* c, const float* angles, const uint8_t* half, int nimg, int chunk, int first,
+                         int sub, int group, SliceDesc* hs) {
   const int nsym = c->nsym;
   for (int a = 0; a < nimg; ++a) {
     float dm[9];
@@ -2495,30 +2499,35 @@ static void build_slices(const spi_ctx* c, const float* angles, const uint8_t* h
     }
   }
   if (!c->slice_order) return;
-  for (int a0 = 0; a0 < nimg; a0 += chunk)
-    for (int b0 = a0; b0 < std::min(nimg, a0 + chunk); b0 += group) {
-      const int nb = std::min(group, std::min(nimg, a0 + chunk) - b0);
-      SliceDesc* base = hs + (size_t)b0 * nsym;
-      const int m = nb * nsym;
-      const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
-      std::vector<std::pair<double, int>> key(m);
-      for (int q = 0; q < m; ++q) {
-        const float* d = base[q].dm;
-        double cx = (double)d[1] * d[5] - (double)d[2] * d[4];
-        double cy = (double)d[2] * d[3] - (double)d[0] * d[5];
-        double cz = (double)d[0] * d[4] - (double)d[1] * d[3];
-        if (cz < 0 || (cz == 0 && (cy < 0 || (cy == 0 && cx < 0)))) { cx = -cx; cy = -cy; cz = -cz; }
-        const double th = std::acos(std::min(1.0, std::max(-1.0, cz)));      // 0..pi/2
-        const double ph = std::atan2(cy, cx);                                 // -pi..pi
-        int ring = std::min(rings - 1, (int)(th / (M_PI / 2) * rings));
-        double u = (ph + M_PI) / (2 * M_PI);
-        if (ring & 1) u = 1.0 - u;
-        key[q] = {ring + u, q};
+  for (int a0 = 0; a0 < nimg; a0 += chunk) {
+    const int a1 = std::min(nimg, a0 + chunk);
+    for (int s0 = a0, bi = 0; s0 < a1; s0 += (bi == 0 ? first : sub), ++bi) {
+      const int s1 = std::min(a1, s0 + (bi == 0 ? first : sub));
+      for (int b0 = s0; b0 < s1; b0 += group) {
+        const int nb = std::min(group, s1 - b0);
+        SliceDesc* base = hs + (size_t)b0 * nsym;
+        const int m = nb * nsym;
+        const int rings = std::max(1, (int)std::sqrt((double)m / 2.0));
+        std::vector<std::pair<double, int>> key(m);
+        for (int q = 0; q < m; ++q) {
+          const float* d = base[q].dm;
+          double cx = (double)d[1] * d[5] - (double)d[2] * d[4];
+          double cy = (double)d[2] * d[3] - (double)d[0] * d[5];
+          double cz = (double)d[0] * d[4] - (double)d[1] * d[3];
+          if (cz < 0 || (cz == 0 && (cy < 0 || (cy == 0 && cx < 0)))) { cx = -cx; cy = -cy; cz = -cz; }
+          const double th = std::acos(std::min(1.0, std::max(-1.0, cz)));      // 0..pi/2
+          const double ph = std::atan2(cy, cx);                                 // -pi..pi
+          int ring = std::min(rings - 1, (int)(th / (M_PI / 2) * rings));
+          double u = (ph + M_PI) / (2 * M_PI);
+          if (ring & 1) u = 1.0 - u;
+          key[q] = {ring + u, q};
+        }
+        std::sort(key.begin(), key.end());
+        std::vector<SliceDesc> tmp(base, base + m);
+        for (int q = 0; q < m; ++q) base[q] = tmp[key[q].second];
       }
-      std::sort(key.begin(), key.end());
-      std::vector<SliceDesc> tmp(base, base + m);
-      for (int q = 0; q < m; ++q) base[q] = tmp[key[q].second];
     }
+  }
 }
 
 static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* angles, const float* inplane,
@@ -2535,7 +2544,23 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   const size_t nsl = (size_t)nimg * nsym;
   SPI_TRY(c->hslices.ensure(nsl * sizeof(SliceDesc)));
   SliceDesc* hs = c->hslices.as<SliceDesc>();
-  build_slices(c, angles, half, nimg, c->chunk, c->sort_group, hs);
+  const bool copy_pipe = !imgs_on_device && c->pipeline;
+  // images per upload piece: at most ~64 MB unless the context sets a count
+  const int piece = c->upload_images > 0 ? c->upload_images
+                                         : (int)((64ull << 20) / ((size_t)nx * nx * sizeof(float)));
+  const int up = imgs_on_device ? c->sub : std::max(1, std::min(c->sub, piece));
+  // With host images in a call of one chunk, the first FFT sub-batch is one
+  // upload piece, so the first insertion starts once that piece has arrived
+  // rather than a whole sub-batch (at 256^3: 256 images, 1.2 ms of upload at
+  // 55 GB/s, instead of 1,024 images, 4.8 ms); the later sub-batches' uploads
+  // still run ahead under the compute.  Only where a sub-batch writes the
+  // spectra of its own images alone (the own R2C, or BF16 spectra through
+  // the FFT scratch): cuFFT's FP32 path transforms a full batch of c->sub
+  // images into the chunk's spectra, which a shifted last sub-batch would
+  // overrun.
+  const int first_sub =
+      (copy_pipe && c->first_piece && nimg <= c->chunk && (c->fft_own || c->bf16)) ? up : c->sub;
+  build_slices(c, angles, half, nimg, c->chunk, first_sub, c->sub, c->sort_group, hs);
   int klp_count = 0;
   {
     float rr = (float)(nx / 2) * (float)(nx / 2);
@@ -2584,10 +2609,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
   // was measured slower: each insertion launch took 21.1-21.3 instead of
   // 15.7-15.8 ms of 1,024 images at 256^3 while a transform ran beside it,
   // 46.2-46.6k instead of 57.5-58.3k images/s device-resident.)
-  const int nsubs = (c->chunk + c->sub - 1) / c->sub;
-  const bool copy_pipe = !imgs_on_device && c->pipeline;
-  const int up = imgs_on_device ? c->sub
-                                : std::max(1, std::min(c->sub, (int)((64ull << 20) / ((size_t)nx * nx * sizeof(float)))));
+  const int nsubs = (c->chunk + c->sub - 1) / c->sub + (first_sub < c->sub ? 1 : 0);
+  auto sub_len = [&](int bi) { return bi == 0 ? first_sub : c->sub; };   // images of sub-batch bi
   const int ppsub = (c->sub + up - 1) / up;
   SPI_TRY(ensure_pipeline_events(c, nsubs * ppsub));
   cudaStream_t cs = copy_pipe ? c->stream2 : c->stream;
@@ -2606,8 +2629,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
     SPI_CUDA(cudaMemcpyAsync(c->slices.p, hs + (size_t)a0 * nsym, (size_t)nb * nsym * sizeof(SliceDesc),
                              cudaMemcpyHostToDevice, c->stream));
     if (!imgs_on_device) {   // uploads of the whole chunk, ahead of the compute
-      for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
-        const int nvalid = std::min(c->sub, nb - b0);
+      for (int b0 = 0, bi = 0; b0 < nb; b0 += sub_len(bi), ++bi) {
+        const int nvalid = std::min(sub_len(bi), nb - b0);
         if (done_valid[bi]) SPI_CUDA(cudaStreamWaitEvent(cs, c->ev_done[bi], 0));
         for (int p0 = b0, pi = 0; p0 < b0 + nvalid; p0 += up, ++pi) {
           const int np = std::min(up, b0 + nvalid - p0);
@@ -2621,8 +2644,8 @@ static int bp_insert_impl(spi_ctx* c, const float* imgs, int nimg, const float* 
         }
       }
     }
-    for (int b0 = 0, bi = 0; b0 < nb; b0 += c->sub, ++bi) {
-      const int nvalid = std::min(c->sub, nb - b0);
+    for (int b0 = 0, bi = 0; b0 < nb; b0 += sub_len(bi), ++bi) {
+      const int nvalid = std::min(sub_len(bi), nb - b0);
       for (int p0 = b0, pi = 0; p0 < b0 + nvalid; p0 += up, ++pi) {
         const int np = std::min(up, b0 + nvalid - p0);
         const bool last = p0 + up >= b0 + nvalid;
@@ -2823,7 +2846,7 @@ static int bp_insert_multi_impl(spi_ctx* const* ctxs, int ncls, const float* con
     SPI_TRY(c->slices.ensure(two * c->nsym * sizeof(SliceDesc)));
     if (!imgs_on_device) SPI_TRY(c->imgs.ensure(two * c->nx * c->nx * sizeof(float)));
     if (nimg[k] > 0)
-      build_slices(c, angles[k], half ? half[k] : nullptr, nimg[k], c->sub, c->sub, hs_all + sl_off[k]);
+      build_slices(c, angles[k], half ? half[k] : nullptr, nimg[k], c->sub, c->sub, c->sub, c->sub, hs_all + sl_off[k]);
     const int nx = c->nx;
     int cnt = 0;
     const float rr = (float)(nx / 2) * (float)(nx / 2);

@@ -27,6 +27,7 @@ struct spi_ctx {
   int insert_threads = 256;           // threads per insert block
   int insert_blocks_per_sm = 0;       // 0 = as many as fit
   int pipeline = 1;                   // 1 = host-image uploads on stream2 under the compute
+  int first_piece = 1;                // 1 = a one-chunk host-image call's first FFT sub-batch is one upload piece
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_ready, ev_done;  // per FFT sub-batch slot
   int cg_fp64 = 2;                    // BP CG precision: 0 FP32, 1 FP64, 2-4 FP64 vectors + fixed-point projections
@@ -37,7 +38,8 @@ struct spi_ctx {
   spi::DevBuf rtsf_buf;               // RTSF scratch: FP64 FFT arrays + FBS2 tables
   int chunk = 0;                      // images per persistent insert launch
   int sub = 0;                        // images per batched 2D FFT (and per insert launch)
-  int sort_group = 0;                 // images per slice-ordering group (divides into sub)
+  int sort_group = 0;                 // images per slice-ordering group (groups stay inside FFT sub-batches)
+  int upload_images = 0;              // host images per upload piece (0 = ~64 MB)
   spi::KBTab kb;
   spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
   int accum = 1;                      // 1 = compensated: insert into part[], two-sum fold into grid + comp

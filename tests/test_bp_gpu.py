@@ -449,3 +449,26 @@ def test_own_r2c_sizes(ctx, nx, mode):
         print(f"own R2C ({mode}) nx={nx}: rel-L2 vs cuFFT path {e:.2e}")
         assert e <= TOL
 
+
+
+@pytest.mark.parametrize("fft,bf16", [("own", False), ("cufft", True), ("cufft", False)])
+def test_bp_host_upload_pieces(ctx, orc, fft, bf16, monkeypatch):
+    """Host images uploaded in small pieces (16 images, FFT sub-batches of 64):
+    a call of one chunk takes its first piece as the first sub-batch (own R2C
+    or BF16 spectra; with cuFFT's FP32 batches the sub-batches stay whole),
+    and slice-sorting groups of 24, which do not divide a sub-batch, stay
+    inside their sub-batch.  The volumes match the FP64 oracle."""
+    nx, nimg = 64, 150
+    _, pr, ang = _case(nx, nimg, 810)
+    half = synth.half_mask(nimg, np.random.default_rng(811))
+    ref = orc.bp32f(pr, ang, half, prec=1)
+    for k, v in (("SPI_BP_SUB", "64"), ("SPI_UPLOAD_IMAGES", "16"), ("SPI_SORT_GROUP", "24"), ("SPI_FFT", fft)):
+        monkeypatch.setenv(k, v)
+    out = ops.bp32f(pr, ang, half, ctx=ctx, bf16=bf16)
+    monkeypatch.setenv("SPI_FIRST_PIECE", "0")
+    whole = ops.bp32f(pr, ang, half, ctx=ctx, bf16=bf16)
+    for a, w, r in zip(out, whole, ref):
+        e = synth.rel_l2(a, r)
+        print(f"upload pieces ({fft}, bf16={bf16}): rel-L2 vs FP64 oracle {e:.2e}")
+        assert e <= (5e-4 if bf16 else TOL)
+        assert synth.rel_l2(a, w) <= (1e-4 if bf16 else TOL)
