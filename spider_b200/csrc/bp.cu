@@ -667,12 +667,16 @@ __global__ void __launch_bounds__(256) colfft_w_kernel(const float2* __restrict_
 // level 2, thread (k2, u) takes S[k2][u + 8 r], an 8-point DFT over r and
 // W_64^(u m2) give T[k2][m2][u]; level 3, thread (k2, m2) takes T[k2][m2][u],
 // an 8-point DFT over u gives X[64 m1 + 8 m2 + k2].  A CTA of 256 threads does
-// 8 columns of one image (4 at a time).  Shared strides are chosen so that a
-// warp's accesses hit each bank at most twice (checked by enumeration).
-constexpr int kC512Cols = 8, kC512SI = 260, kC512SO = 580, kC512WB = 576;
+// COLS (4 or 8) columns of one image, 4 at a time.  Shared strides are chosen
+// so that a warp's accesses hit each bank at most twice (checked by
+// enumeration for both column counts).
+constexpr int kC512SI = 260, kC512SO = 580, kC512WB = 576;
+constexpr size_t colfft512_smem(int cols) { return (size_t)(256 + cols * (kC512SI + kC512SO) + 4 * kC512WB) * 8; }
+template <int COLS>
 __global__ void __launch_bounds__(256) colfft512_kernel(const float2* __restrict__ inter, size_t inter_stride, int nx,
                                                         int n, int ip, int nvalid, const float2* __restrict__ twg,
                                                         float2* __restrict__ out) {
+  constexpr int kC512Cols = COLS;
   extern __shared__ float2 fsm[];   // tw[256], in [8][SI], out [8][SO], work [4][WB]
   const int h = 256;
   const int tiles = (h + 1 + kC512Cols - 1) / kC512Cols;
@@ -704,7 +708,7 @@ __global__ void __launch_bounds__(256) colfft512_kernel(const float2* __restrict
   const int grp = threadIdx.x >> 6, t = threadIdx.x & 63;
   float2* S = work + grp * kC512WB;
   const int g8 = t >> 3, l8 = t & 7;
-  for (int c = grp; c < kC512Cols; c += 4) {   // the same two rounds for every group
+  for (int c = grp; c < kC512Cols; c += 4) {   // COLS / 4 rounds, the same for every group
     float2 v[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -2189,6 +2193,10 @@ int spi_bp_open(spi_ctx* c, int nx, int ngrids, const float* sym_angles, int nsy
   c->sub = sub;
   c->sort_group = std::max(1, std::min(sub, env_int("SPI_SORT_GROUP", sub)));
   c->upload_images = std::max(0, env_int("SPI_UPLOAD_IMAGES", 0));   // 0: pieces of ~64 MB
+  // n = 512 column pass: 4 columns per CTA (47 KB of shared memory, 4 CTAs
+  // per SM) measured 69.64-69.69 ms per 4,096-image step against
+  // 69.96-70.32 ms with 8 (74 KB, 3 CTAs per SM), two alternations at 256^3
+  c->col512 = env_int("SPI_COLFFT_COLS", 4) == 8 ? 8 : 4;
   {
     // The own two-pass R2C is the default at n = 512 (nx = 256), where its
     // register passes (stage_rowfft512_kernel + colfft512_kernel) measured
@@ -2278,9 +2286,12 @@ static int launch_colfft(spi_ctx* c, cudaStream_t st, const float2* inter, int n
     } else if (n == 256) {
       colfft_w_kernel<8><<<nvalid * tiles, 256, smem, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
     } else {
-      const int t512 = (n / 2 + 1 + kC512Cols - 1) / kC512Cols;
-      const size_t sm512 = (size_t)(256 + kC512Cols * (kC512SI + kC512SO) + 4 * kC512WB) * sizeof(float2);
-      colfft512_kernel<<<nvalid * t512, 256, sm512, st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+      const int cols = c->col512;
+      const int t512 = (n / 2 + 1 + cols - 1) / cols;
+      if (cols == 4)
+        colfft512_kernel<4><<<nvalid * t512, 256, colfft512_smem(4), st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
+      else
+        colfft512_kernel<8><<<nvalid * t512, 256, colfft512_smem(8), st>>>(inter, istride, nx, n, ip, nvalid, tw, out);
     }
     return check_kernel("colfft_w_kernel");
   }
@@ -2310,8 +2321,10 @@ static int ensure_fft_twiddles(spi_ctx* c) {
     const int wsm = (int)((128 + kColTileW * (129 + 256 + 33)) * sizeof(float2));   // n = 256
     SPI_CUDA(cudaFuncSetAttribute(colfft_w_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
     SPI_CUDA(cudaFuncSetAttribute(colfft_w_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
-    SPI_CUDA(cudaFuncSetAttribute(colfft512_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((256 + kC512Cols * (kC512SI + kC512SO) + 4 * kC512WB) * sizeof(float2))));
+    SPI_CUDA(cudaFuncSetAttribute(colfft512_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)colfft512_smem(4)));
+    SPI_CUDA(cudaFuncSetAttribute(colfft512_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)colfft512_smem(8)));
     done |= bit;
   }
   return 0;

@@ -40,6 +40,7 @@ struct spi_ctx {
   int sub = 0;                        // images per batched 2D FFT (and per insert launch)
   int sort_group = 0;                 // images per slice-ordering group (groups stay inside FFT sub-batches)
   int upload_images = 0;              // host images per upload piece (0 = ~64 MB)
+  int col512 = 4;                     // columns per CTA of the n = 512 column FFT (4 or 8)
   spi::KBTab kb;
   spi::DevBuf grid[2];                // float4 {re, im, w, 0} [n][n][nx+1]
   int accum = 1;                      // 1 = compensated: insert into part[], two-sum fold into grid + comp

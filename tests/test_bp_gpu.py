@@ -423,11 +423,16 @@ def test_own_r2c_matches_cufft_path(ctx, orc):
             assert synth.rel_l2(d, r) <= 5e-4
 
 
-@pytest.mark.parametrize("nx,mode", [(64, "own2"), (128, "own"), (128, "own2"), (256, "own"), (256, "own2")])
-def test_own_r2c_sizes(ctx, nx, mode):
+@pytest.mark.parametrize("nx,mode", [(64, "own2"), (128, "own"), (128, "own2"), (256, "own"), (256, "own:cols8"),
+                                     (256, "own2")])
+def test_own_r2c_sizes(ctx, nx, mode, monkeypatch):
     """The register-FFT passes (SPI_FFT=own at padded sizes 128-512; the
-    default at 512) and the shared-memory radix-2 passes (own2) give the
-    volumes of PADD2 + cuFFT (SPI_FFT=cufft)."""
+    default at 512, its column pass with 4 (default) or 8 columns per CTA)
+    and the shared-memory radix-2 passes (own2) give the volumes of PADD2 +
+    cuFFT (SPI_FFT=cufft)."""
+    if mode.endswith(":cols8"):
+        monkeypatch.setenv("SPI_COLFFT_COLS", "8")
+        mode = "own"
     rng = np.random.default_rng(700 + nx)
     nimg = 48
     vol = synth.blob_phantom(nx, 10, sigma=(2, 6), radius=0.35 * nx, rng=rng)
